@@ -1,0 +1,299 @@
+// svdag_ctx.cu - context lifetime (one preallocated HBM pool), status, statistics, garbage collection.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <new>
+
+#include "svdag_edit.cuh"
+#include "svdag_host.hpp"
+
+using namespace svdag;
+
+namespace {
+
+constexpr unsigned long long kCtlBytes = 64 * 1024;
+
+// ---------------------------------------------------------------- garbage collection
+// MyGPUHashDAG::garbageCollect (my_gpu_hash_dag.cu:365-475) marks level by level from the root set
+// (the root and the level-0 fully-filled nodes) and, with CAPTURE_MEMORY_STATS_SLOW, frees the
+// unmarked slots (gpu_hash_table_base.cu:304-374). Here marking is a bitmap indexed by handle/2 (items
+// are at least two words long) and the frontier is deduplicated by the test-and-set on that bitmap.
+
+__device__ __forceinline__ bool mark_once(uint32_t* bits, uint32_t handle)
+{
+    const uint32_t b = handle >> 1;
+    const uint32_t m = 1u << (b & 31u);
+    return !(atomicOr(&bits[b >> 5], m) & m);
+}
+
+__global__ void k_gc_roots(DevDag d, uint32_t* bits, uint32_t* frontier, uint32_t* count)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0)
+        return;
+    uint32_t n = 0;
+    const uint32_t root = d.ctl->root;
+    if (root != kNone && mark_once(bits, root))
+        frontier[n++] = root;
+    for (uint32_t m = 0; m < SVDAG_NUM_MATERIALS; ++m) {
+        const uint32_t h = d.ctl->fullyFilled[0][m];
+        if (h != kNone && mark_once(bits, h))
+            frontier[n++] = h;
+    }
+    count[0] = n;
+}
+
+__global__ void k_gc_mark(DevDag d, uint32_t* bits, const uint32_t* in, const uint32_t* inCount, uint32_t* out, uint32_t* outCount,
+    unsigned long long outCap)
+{
+    const uint32_t n = *inCount;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t* node = d.items + in[i];
+        const uint32_t mask = node[0] & 0xFFu;
+        const uint32_t k = __popc(mask);
+        for (uint32_t j = 0; j < k; ++j) {
+            const uint32_t c = node[1 + j];
+            if (mark_once(bits, c)) {
+                const uint32_t at = atomicAdd(outCount, 1u);
+                if (at < outCap)
+                    out[at] = c;
+                else
+                    set_status(d.ctl, SVDAG_ERR_OOM);
+            }
+        }
+    }
+}
+
+// Clears unmarked occupied slots (tag and item words) of one table; returns freed items in *freed.
+__global__ void k_gc_sweep(DevDag d, DevTable t, const uint32_t* bits, unsigned long long* freed)
+{
+    unsigned long long nfreed = 0;
+    for (uint32_t c = 0; c < kNumClasses; ++c) {
+        const uint32_t k = c + 2;
+        for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < t.numBuckets[c]; b += gridDim.x * blockDim.x) {
+            uint32_t slab = t.bucketBase[c] + b * slab_words(k);
+            for (uint32_t steps = 0; steps < kMaxChain; ++steps) {
+                uint32_t* h = d.items + slab;
+                for (uint32_t s = 0; s < kSlots; ++s) {
+                    const uint32_t shift = 8u * (s / 7u);
+                    const uint32_t tag = (h[s % 7u] >> shift) & 0xFFu;
+                    if (tag == 0 || tag == kTagBusy)
+                        continue;
+                    const uint32_t item = slab + kHeaderWords + s * k;
+                    const uint32_t bit = item >> 1;
+                    if ((bits[bit >> 5] >> (bit & 31u)) & 1u)
+                        continue;
+                    for (uint32_t j = 0; j < k; ++j)
+                        d.items[item + j] = 0;
+                    h[s % 7u] &= ~(0xFFu << shift);
+                    ++nfreed;
+                }
+                if (h[7] == kEnd)
+                    break;
+                slab = h[7];
+            }
+        }
+    }
+    if (nfreed)
+        atomicAdd(freed, nfreed);
+}
+
+__global__ void k_gc_clear_history(Control* c)
+{
+    c->undoCount = 0;
+    c->redoCount = 0;
+}
+
+} // namespace
+
+extern "C" {
+
+uint32_t svdag_abi_version(void) { return SVDAG_ABI_VERSION; }
+
+const char* svdag_status_string(svdag_status s)
+{
+    switch (s) {
+    case SVDAG_OK:
+        return "ok";
+    case SVDAG_ERR_INVALID:
+        return "invalid argument";
+    case SVDAG_ERR_OOM:
+        return "out of memory (pool, item region or scratch arena)";
+    case SVDAG_ERR_TIMEOUT:
+        return "bounded device wait or retry loop gave up";
+    case SVDAG_ERR_CORRUPT:
+        return "structural invariant violated";
+    case SVDAG_ERR_CUDA:
+        return "CUDA runtime error";
+    case SVDAG_ERR_NO_DEVICE:
+        return "no usable sm_100 device";
+    case SVDAG_ERR_UNSUPPORTED:
+        return "unsupported";
+    case SVDAG_ERR_BUSY:
+        return "busy";
+    }
+    return "unknown status";
+}
+
+svdag_status svdag_create(const svdag_config* cfg, svdag_ctx** out)
+{
+    if (!cfg || !out || cfg->levels < SVDAG_MIN_LEVELS || cfg->levels > SVDAG_MAX_LEVELS || cfg->flags != 0)
+        return SVDAG_ERR_INVALID;
+    if (cfg->probe_lanes && cfg->probe_lanes != 1 && cfg->probe_lanes != 2 && cfg->probe_lanes != 4 && cfg->probe_lanes != 8
+        && cfg->probe_lanes != 16 && cfg->probe_lanes != 32)
+        return SVDAG_ERR_INVALID;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0 || cfg->device < 0 || cfg->device >= ndev) {
+        cudaGetLastError();
+        return SVDAG_ERR_NO_DEVICE;
+    }
+    cudaDeviceProp prop {};
+    SVDAG_CUDA(cudaGetDeviceProperties(&prop, cfg->device));
+    if (prop.major != 10)
+        return SVDAG_ERR_NO_DEVICE; // built for sm_100a only
+    SVDAG_CUDA(cudaSetDevice(cfg->device));
+    const unsigned long long pool = cfg->pool_bytes ? cfg->pool_bytes : (1ull << 30);
+    const unsigned long long scratch = cfg->scratch_bytes ? cfg->scratch_bytes : pool / 4;
+    if (scratch + kCtlBytes + (1ull << 20) > pool)
+        return SVDAG_ERR_INVALID;
+    auto* ctx = new (std::nothrow) svdag_ctx();
+    if (!ctx)
+        return SVDAG_ERR_OOM;
+    ctx->cfg = *cfg;
+    ctx->device = cfg->device;
+    ctx->probeLanes = cfg->probe_lanes ? cfg->probe_lanes : 8;
+    ctx->loadFactor = cfg->target_load_factor ? cfg->target_load_factor : 16;
+    ctx->cfg.undo_depth = cfg->undo_depth ? std::min<uint32_t>(cfg->undo_depth, 64) : 32;
+    if (cudaMalloc(&ctx->pool, pool) != cudaSuccess) {
+        cudaGetLastError();
+        delete ctx;
+        return SVDAG_ERR_OOM;
+    }
+    ctx->poolBytes = pool;
+    ctx->ctl = reinterpret_cast<Control*>(ctx->pool);
+    ctx->scratch = ctx->pool + kCtlBytes;
+    ctx->scratchBytes = scratch;
+    ctx->items = reinterpret_cast<uint32_t*>(ctx->pool + kCtlBytes + scratch);
+    ctx->itemWords = std::min<unsigned long long>((pool - kCtlBytes - scratch) / 4, kMaxHandle);
+    static_assert(sizeof(Control) <= kCtlBytes, "control block too large");
+    cudaError_t e = cudaMemset(ctx->pool, 0, pool);
+    if (e == cudaSuccess) {
+        Control init {};
+        init.root = kNone;
+        init.undoDepth = ctx->cfg.undo_depth;
+        init.savedRoot = kNone;
+        for (auto& lv : init.fullyFilled)
+            for (auto& m : lv)
+                m = kNone;
+        e = cudaMemcpy(ctx->ctl, &init, sizeof(init), cudaMemcpyHostToDevice);
+    }
+    if (e != cudaSuccess) {
+        cudaFree(ctx->pool);
+        delete ctx;
+        return cuda_status(e);
+    }
+    *out = ctx;
+    return SVDAG_OK;
+}
+
+svdag_status svdag_destroy(svdag_ctx* ctx)
+{
+    if (!ctx)
+        return SVDAG_ERR_INVALID;
+    cudaSetDevice(ctx->device);
+    for (auto* t : ctx->standalone)
+        delete t;
+    cudaFree(ctx->pool);
+    delete ctx;
+    return SVDAG_OK;
+}
+
+svdag_status svdag_sync(svdag_ctx* ctx, void* stream)
+{
+    if (!ctx)
+        return SVDAG_ERR_INVALID;
+    return read_status(ctx, as_stream(stream));
+}
+
+svdag_status svdag_get_root(svdag_ctx* ctx, uint32_t* root, void* stream)
+{
+    if (!ctx || !root)
+        return SVDAG_ERR_INVALID;
+    cudaStream_t s = as_stream(stream);
+    SVDAG_CUDA(cudaMemcpyAsync(root, &ctx->ctl->root, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    SVDAG_CUDA(cudaStreamSynchronize(s));
+    return SVDAG_OK;
+}
+
+svdag_status svdag_gc(svdag_ctx* ctx, void* stream)
+{
+    if (!ctx)
+        return SVDAG_ERR_INVALID;
+    cudaStream_t s = as_stream(stream);
+    SVDAG_TRY(ensure_level_tables(ctx, s));
+    unsigned long long top = 0;
+    SVDAG_CUDA(cudaMemcpyAsync(&top, &ctx->ctl->itemTop, sizeof(top), cudaMemcpyDeviceToHost, s));
+    SVDAG_CUDA(cudaStreamSynchronize(s));
+    const unsigned long long bitmapBytes = align256(((top / 2) + 32) / 8 + 8);
+    const unsigned long long rest = ctx->scratchBytes > bitmapBytes + 4096 ? ctx->scratchBytes - bitmapBytes - 4096 : 0;
+    const unsigned long long frontierCap = rest / 8; // two frontiers of u32
+    if (frontierCap < 1024)
+        return SVDAG_ERR_OOM;
+    auto* bits = reinterpret_cast<uint32_t*>(ctx->scratch);
+    auto* counts = reinterpret_cast<uint32_t*>(ctx->scratch + bitmapBytes);
+    auto* fa = reinterpret_cast<uint32_t*>(ctx->scratch + bitmapBytes + 4096);
+    auto* fb = fa + frontierCap;
+    SVDAG_CUDA(cudaMemsetAsync(ctx->scratch, 0, bitmapBytes + 4096, s));
+    const DevDag d = ctx->dag();
+    k_gc_roots<<<1, 32, 0, s>>>(d, bits, fa, counts + 0);
+    const uint32_t LL = d.leafLevel;
+    for (uint32_t level = 0; level < LL; ++level) {
+        uint32_t* in = (level & 1) ? fb : fa;
+        uint32_t* out = (level & 1) ? fa : fb;
+        k_gc_mark<<<grid_for(ctx, 1ull << 24, 256), 256, 0, s>>>(d, bits, in, counts + level, out, counts + level + 1, frontierCap);
+    }
+    unsigned long long* freed = reinterpret_cast<unsigned long long*>(counts + 64);
+    for (uint32_t level = 0; level <= LL; ++level) {
+        const DevTable t = ctx->levelTables[level].dev;
+        unsigned long long nb = 0;
+        for (uint32_t c = 0; c < kNumClasses; ++c)
+            nb = std::max<unsigned long long>(nb, t.numBuckets[c]);
+        k_gc_sweep<<<grid_for(ctx, nb, 256), 256, 0, s>>>(d, t, bits, freed);
+    }
+    k_gc_clear_history<<<1, 1, 0, s>>>(ctx->ctl);
+    SVDAG_CUDA(cudaGetLastError());
+    return read_status(ctx, s);
+}
+
+svdag_status svdag_get_stats(svdag_ctx* ctx, svdag_stats* out, void* stream)
+{
+    if (!ctx || !out)
+        return SVDAG_ERR_INVALID;
+    cudaStream_t s = as_stream(stream);
+    std::memset(out, 0, sizeof(*out));
+    Control c;
+    SVDAG_CUDA(cudaMemcpyAsync(&c, ctx->ctl, sizeof(c), cudaMemcpyDeviceToHost, s));
+    SVDAG_CUDA(cudaStreamSynchronize(s));
+    out->levels = ctx->cfg.levels;
+    out->root = c.root;
+    out->pool_bytes = ctx->poolBytes;
+    out->item_region_bytes = ctx->itemWords * 4;
+    out->item_region_used_bytes = c.itemTop * 4;
+    out->scratch_bytes = ctx->scratchBytes;
+    out->scratch_high_water_bytes = ctx->scratchHighWater;
+    out->undo_count = c.undoCount;
+    out->redo_count = c.redoCount;
+    for (uint32_t l = 0; l + 1 < ctx->cfg.levels; ++l) {
+        svdag_table& t = ctx->levelTables[l];
+        if (!t.ready)
+            continue;
+        svdag_table_stats ts {};
+        SVDAG_TRY(svdag_table_get_stats(&t, &ts, stream));
+        out->level_items[l] = ts.items;
+        out->level_buckets[l] = ts.buckets;
+    }
+    return SVDAG_OK;
+}
+
+} // extern "C"

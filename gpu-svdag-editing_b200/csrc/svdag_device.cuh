@@ -1,0 +1,525 @@
+// svdag_device.cuh - device-side data layout and the slab hash table probes.
+//
+// Item region: one word-addressed array inside the context's HBM pool. A handle is the 32-bit word
+// offset of an item, so decoding a handle is one add (the reference decodes through a table
+// descriptor and the slab allocator's super-block table, gpu_hash_table_base.h:275-294).
+//
+// Hash tables: one table per DAG level. A level table holds keys of 2..10 words; keys of one length
+// share a slab family (the "size class"), so slots have a fixed stride and the slot index gives the
+// item address. A slab of class k:
+//   words 0..6  : 28 one-byte tags, slot s at word (s % 7), byte (s / 7); 0 = free, 0xFF = being written
+//   word  7     : word offset of the next slab in the bucket's chain, 0 = end of chain (offset 0 is
+//                 always a bucket array, never an overflow slab)
+//   words 8..   : 28 items of k words (item s at 8 + s*k)
+// The 8 header words are one 32-byte sector, so a probe costs one sector per slab plus the candidate
+// item; the reference's header is 10 words (8 hash words + next + active mask) spanning two sectors
+// (compact_acceleration_hash_table.h:519-541). The first slab of each bucket sits in the bucket
+// array (HASH_TABLE_STORE_SLABS_IN_TABLE, gpu_hash_table_base.h:30-49); overflow slabs come from a
+// bump allocator over the same item region and are linked at the tail of the chain.
+#pragma once
+#include <cstdint>
+
+#include "../../include/svdag.h"
+
+namespace svdag {
+
+constexpr uint32_t kNone = 0xFFFFFFFFu; // empty child / missing handle
+constexpr uint32_t kEnd = 0u; // end of a slab chain
+constexpr uint32_t kFillMarker = 0xFFFFFF00u; // SVO child "canonical fully-filled node of material m" = kFillMarker | m
+constexpr uint32_t kMaxHandle = 0xFFFFFF00u; // item region limit in words (just under 16 GiB)
+constexpr uint32_t kSlots = 28;
+constexpr uint32_t kHeaderWords = 8;
+constexpr uint32_t kTagBusy = 0xFFu;
+constexpr uint32_t kMaxLevels = SVDAG_MAX_LEVELS;
+constexpr uint32_t kItemStride = 10; // padded stride of items in scratch arrays
+constexpr uint32_t kNumClasses = 9; // item sizes 2..10
+
+__host__ __device__ constexpr uint32_t slab_words(uint32_t k) { return ((kHeaderWords + kSlots * k) + 7u) & ~7u; }
+
+// Per-table descriptor, passed by value to kernels.
+struct DevTable {
+    uint32_t kind; // svdag_item_kind
+    uint32_t numBuckets[kNumClasses];
+    uint32_t bucketBase[kNumClasses]; // word offset of bucket 0's slab
+};
+
+// Device control block (lives at the start of the scratch side of the pool).
+struct EditCounters {
+    uint32_t count[kMaxLevels]; // intermediate SVO items per level
+    uint32_t ffCount[kMaxLevels]; // fully-filled items found per level
+    uint32_t ffRan[kMaxLevels]; // discovery ran at this level
+    uint32_t repCount[kMaxLevels]; // items left after intra-level dedup
+    uint32_t repPerClass[kMaxLevels][kNumClasses];
+    unsigned long long oldRead, added, edited;
+    unsigned long long offW[kMaxLevels]; // scratch byte offset of each level's work items
+    unsigned long long offN[kMaxLevels]; // scratch byte offset of each level's SVO items
+    unsigned long long buildTop; // end of the top-down allocations
+    uint32_t rootBefore, rootAfter;
+    uint32_t overflow; // scratch arena exhausted
+    uint32_t pad;
+};
+
+struct Control {
+    unsigned long long itemTop; // bump pointer of the item region, in words
+    uint32_t status; // latched svdag_status
+    uint32_t root; // current root handle (kNone = empty DAG)
+    uint32_t undo[64];
+    uint32_t redo[64];
+    uint32_t undoHead, undoCount, redoCount, undoDepth;
+    uint32_t savedRoot; // source root of a move (the DAG before its removal step)
+    uint32_t pad0;
+    uint32_t fullyFilled[kMaxLevels][SVDAG_NUM_MATERIALS];
+    EditCounters edit;
+};
+
+struct DevDag {
+    uint32_t* items;
+    unsigned long long itemWords; // capacity of the item region
+    Control* ctl;
+    uint32_t levels;
+    uint32_t leafLevel;
+};
+
+__device__ __forceinline__ void set_status(Control* ctl, uint32_t code)
+{
+    atomicCAS(&ctl->status, 0u, code);
+}
+
+// ---------------------------------------------------------------- hashing (ours; the bucket
+// function of the reference is xorHash32xN, utils.h:395-403, which uses a 32-bit modulo per word)
+
+__host__ __device__ __forceinline__ uint32_t fmix32(uint32_t h)
+{
+    h ^= h >> 16;
+    h *= 0x85ebca6bu;
+    h ^= h >> 13;
+    h *= 0xc2b2ae35u;
+    h ^= h >> 16;
+    return h;
+}
+__host__ __device__ __forceinline__ uint32_t word_hash_a(uint32_t w, uint32_t i)
+{
+    return fmix32(w ^ (i * 0x9E3779B9u + 0x7F4A7C15u));
+}
+__host__ __device__ __forceinline__ uint32_t word_hash_b(uint32_t w, uint32_t i)
+{
+    return fmix32(w + (i * 0x85EBCA6Bu + 0x165667B1u));
+}
+__host__ __device__ __forceinline__ uint32_t tag_of(uint32_t hb)
+{
+    uint32_t t = hb >> 24;
+    return t == 0 ? 1u : (t == 0xFFu ? 0xFEu : t);
+}
+__device__ __forceinline__ uint32_t bucket_of(uint32_t ha, uint32_t numBuckets) { return __umulhi(ha, numBuckets); }
+
+// Key length from the first words (my_gpu_base_dag.h:195-203).
+__host__ __device__ __forceinline__ uint32_t node_words(uint32_t header) { return 1u + __builtin_popcount(header & 0xFFu); }
+__host__ __device__ __forceinline__ uint32_t leaf_words(uint32_t lo, uint32_t hi)
+{
+    const uint32_t v = __builtin_popcount(lo) + __builtin_popcount(hi);
+    return 2u + ((v * 4u + 31u) >> 5);
+}
+__device__ __forceinline__ uint32_t dev_node_words(uint32_t header) { return 1u + __popc(header & 0xFFu); }
+__device__ __forceinline__ uint32_t dev_leaf_words(uint32_t lo, uint32_t hi) { return 2u + (((__popc(lo) + __popc(hi)) * 4u + 31u) >> 5); }
+
+// ---------------------------------------------------------------- cooperative groups of G lanes
+
+template <int G>
+struct Grp {
+    static constexpr int KW = (int(kItemStride) + G - 1) / G; // key words per lane
+    uint32_t lane; // 0..G-1
+    uint32_t mask; // warp lanes of this group
+    __device__ __forceinline__ Grp()
+    {
+        const uint32_t wl = threadIdx.x & 31u;
+        lane = wl % G;
+        mask = (G == 32) ? 0xFFFFFFFFu : (((1u << G) - 1u) << (wl / G * G));
+    }
+    __device__ __forceinline__ uint32_t bcast(uint32_t v, uint32_t src) const
+    {
+        if constexpr (G == 1)
+            return v;
+        else
+            return __shfl_sync(mask, v, src, G);
+    }
+    __device__ __forceinline__ uint32_t reduce_or(uint32_t v) const
+    {
+        if constexpr (G > 1) {
+#pragma unroll
+            for (int o = G / 2; o > 0; o >>= 1)
+                v |= __shfl_xor_sync(mask, v, o, G);
+        }
+        return v;
+    }
+    __device__ __forceinline__ uint32_t reduce_xor(uint32_t v) const
+    {
+        if constexpr (G > 1) {
+#pragma unroll
+            for (int o = G / 2; o > 0; o >>= 1)
+                v ^= __shfl_xor_sync(mask, v, o, G);
+        }
+        return v;
+    }
+    __device__ __forceinline__ bool all(bool p) const
+    {
+        if constexpr (G == 1)
+            return p;
+        else
+            return __all_sync(mask, p);
+    }
+    __device__ __forceinline__ void sync() const
+    {
+        if constexpr (G > 1)
+            __syncwarp(mask);
+    }
+};
+
+// A key spread over the lanes of a group: lane j holds words j, j+G, j+2G, ...
+template <int G>
+struct Key {
+    uint32_t w[Grp<G>::KW];
+    uint32_t n; // words
+    uint32_t ha, hb; // bucket hash, tag hash
+};
+
+// Loads a self-describing key (node or leaf) of at most 10 words; `limit` bounds the readable words.
+template <int G>
+__device__ __forceinline__ void load_key(const Grp<G>& g, const uint32_t* p, unsigned long long limit, uint32_t kind, Key<G>& key)
+{
+    uint32_t w0 = 0, w1 = 0;
+    if constexpr (G == 1) {
+        w0 = limit > 0 ? p[0] : 0u;
+        w1 = limit > 1 ? p[1] : 0u;
+    } else {
+        uint32_t v = (g.lane < 2 && g.lane < limit) ? p[g.lane] : 0u;
+        w0 = g.bcast(v, 0);
+        w1 = g.bcast(v, 1);
+    }
+    key.n = kind == SVDAG_KIND_NODE ? dev_node_words(w0) : dev_leaf_words(w0, w1);
+    uint32_t a = 0, b = 0;
+#pragma unroll
+    for (int i = 0; i < Grp<G>::KW; ++i) {
+        const uint32_t idx = g.lane + uint32_t(i) * G;
+        uint32_t v = 0;
+        if (idx < key.n && idx < limit)
+            v = p[idx];
+        key.w[i] = v;
+        if (idx < key.n) {
+            a ^= word_hash_a(v, idx);
+            b ^= word_hash_b(v, idx);
+        }
+    }
+    key.ha = g.reduce_xor(a);
+    key.hb = g.reduce_xor(b);
+}
+
+// Sets up a key already held in registers of a single thread (G == 1 paths of the pipeline).
+__device__ __forceinline__ void hash_words(const uint32_t* w, uint32_t n, uint32_t& ha, uint32_t& hb)
+{
+    uint32_t a = 0, b = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        a ^= word_hash_a(w[i], i);
+        b ^= word_hash_b(w[i], i);
+    }
+    ha = a;
+    hb = b;
+}
+
+// Loads the 8 header words of a slab; each lane ends up with the words it owns.
+// Returns the candidate mask of slots whose tag byte equals `tag` (28 bits) and the next pointer.
+template <int G, bool CG = false>
+__device__ __forceinline__ uint32_t probe_header(const Grp<G>& g, const uint32_t* slab, uint32_t tag, uint32_t& next,
+    uint32_t& emptyMask)
+{
+    const uint32_t tag4 = tag * 0x01010101u;
+    uint32_t cand = 0, empty = 0;
+    auto account = [&](uint32_t word, uint32_t x) {
+        if (word < 7) {
+            const uint32_t eq = __vcmpeq4(x, tag4);
+            const uint32_t ez = __vcmpeq4(x, 0u);
+#pragma unroll
+            for (uint32_t b = 0; b < 4; ++b) {
+                cand |= ((eq >> (8 * b)) & 1u) << (word + 7 * b);
+                empty |= ((ez >> (8 * b)) & 1u) << (word + 7 * b);
+            }
+        }
+    };
+    uint32_t nx = 0;
+    if constexpr (G == 1) {
+        const uint4 a = CG ? __ldcg(reinterpret_cast<const uint4*>(slab)) : reinterpret_cast<const uint4*>(slab)[0];
+        const uint4 b = CG ? __ldcg(reinterpret_cast<const uint4*>(slab) + 1) : reinterpret_cast<const uint4*>(slab)[1];
+        account(0, a.x);
+        account(1, a.y);
+        account(2, a.z);
+        account(3, a.w);
+        account(4, b.x);
+        account(5, b.y);
+        account(6, b.z);
+        nx = b.w;
+    } else if constexpr (G == 2) {
+        const uint4 a = CG ? __ldcg(reinterpret_cast<const uint4*>(slab) + g.lane) : reinterpret_cast<const uint4*>(slab)[g.lane];
+        account(4 * g.lane + 0, a.x);
+        account(4 * g.lane + 1, a.y);
+        account(4 * g.lane + 2, a.z);
+        account(4 * g.lane + 3, a.w);
+        nx = g.bcast(a.w, 1);
+    } else if constexpr (G == 4) {
+        const uint2 a = CG ? __ldcg(reinterpret_cast<const uint2*>(slab) + g.lane) : reinterpret_cast<const uint2*>(slab)[g.lane];
+        account(2 * g.lane + 0, a.x);
+        account(2 * g.lane + 1, a.y);
+        nx = g.bcast(a.y, 3);
+    } else {
+        uint32_t x = 0;
+        if (g.lane < 8)
+            x = CG ? __ldcg(slab + g.lane) : slab[g.lane];
+        if (g.lane < 8)
+            account(g.lane, x);
+        nx = g.bcast(x, 7);
+    }
+    next = nx;
+    emptyMask = g.reduce_or(empty);
+    return g.reduce_or(cand);
+}
+
+// Compares the key with the item at `item`; all lanes of the group get the same answer.
+template <int G, bool CG = false>
+__device__ __forceinline__ bool item_equals(const Grp<G>& g, const uint32_t* item, const Key<G>& key)
+{
+    bool eq = true;
+#pragma unroll
+    for (int i = 0; i < Grp<G>::KW; ++i) {
+        const uint32_t idx = g.lane + uint32_t(i) * G;
+        if (idx < key.n)
+            eq &= (CG ? __ldcg(item + idx) : item[idx]) == key.w[i];
+    }
+    return g.all(eq);
+}
+
+template <int G>
+__device__ __forceinline__ void write_item(const Grp<G>& g, uint32_t* item, const Key<G>& key)
+{
+#pragma unroll
+    for (int i = 0; i < Grp<G>::KW; ++i) {
+        const uint32_t idx = g.lane + uint32_t(i) * G;
+        if (idx < key.n)
+            item[idx] = key.w[i];
+    }
+}
+
+__device__ __forceinline__ uint32_t first_slab(const DevTable& t, uint32_t cls, uint32_t ha)
+{
+    return t.bucketBase[cls] + bucket_of(ha, t.numBuckets[cls]) * slab_words(cls + 2u);
+}
+
+// Allocates and initialises an overflow slab of class k; returns kNone when the region is full.
+template <int G>
+__device__ __forceinline__ uint32_t alloc_slab(const Grp<G>& g, const DevDag& d, uint32_t k)
+{
+    uint32_t off = kNone;
+    if (g.lane == 0) {
+        const unsigned long long w = slab_words(k);
+        const unsigned long long o = atomicAdd(&d.ctl->itemTop, w);
+        if (o + w <= d.itemWords && o + w <= kMaxHandle)
+            off = (uint32_t)o;
+        else
+            set_status(d.ctl, SVDAG_ERR_OOM);
+    }
+    off = g.bcast(off, 0);
+    if (off != kNone) {
+        // Free slots keep zero words (a valid key is never all zero), so the whole slab is cleared.
+        const uint32_t sw = slab_words(k);
+        for (uint32_t i = g.lane * 4; i < sw; i += G * 4)
+            *reinterpret_cast<uint4*>(d.items + off + i) = make_uint4(0, 0, 0, 0);
+        __threadfence();
+        g.sync();
+    }
+    return off;
+}
+
+// Links `fresh` behind `slab`; returns the slab that follows `slab` afterwards (ours or a racer's).
+__device__ __forceinline__ uint32_t link_slab(uint32_t* items, uint32_t slab, uint32_t fresh)
+{
+    const uint32_t prev = atomicCAS(&items[slab + 7], kEnd, fresh);
+    return prev == kEnd ? fresh : prev;
+}
+
+constexpr uint32_t kMaxChain = 1u << 20; // bound on chain walks (a longer walk means a corrupt chain)
+
+// Read-only lookup (CompactAccelerationHashTable::findAsWarp, compact_acceleration_hash_table.h:233-280).
+template <int G>
+__device__ __forceinline__ uint32_t table_find(const Grp<G>& g, const DevDag& d, const DevTable& t, const Key<G>& key)
+{
+    const uint32_t cls = key.n - 2u;
+    if (key.n < 2u || key.n > 10u || t.numBuckets[cls] == 0)
+        return kNone;
+    const uint32_t tag = tag_of(key.hb);
+    uint32_t slab = first_slab(t, cls, key.ha);
+    for (uint32_t steps = 0;; ++steps) {
+        if (steps >= kMaxChain) {
+            set_status(d.ctl, SVDAG_ERR_CORRUPT);
+            return kNone;
+        }
+        uint32_t next, empty;
+        uint32_t cand = probe_header<G>(g, d.items + slab, tag, next, empty);
+        while (cand) {
+            const uint32_t s = __ffs(cand) - 1u;
+            cand &= cand - 1u;
+            const uint32_t item = slab + kHeaderWords + s * key.n;
+            if (item_equals<G>(g, d.items + item, key))
+                return item;
+        }
+        if (next == kEnd)
+            return kNone;
+        slab = next;
+    }
+}
+
+// Claims a free slot of `slab` for the key; returns the item offset or kNone when the slab is full.
+// `busy` claims with the in-flight tag (published later), otherwise with the final tag.
+template <int G>
+__device__ __forceinline__ uint32_t claim_in_slab(const Grp<G>& g, const DevDag& d, uint32_t slab, uint32_t emptyMask,
+    uint32_t tag, uint32_t n, bool busy)
+{
+    while (emptyMask) {
+        const uint32_t s = __ffs(emptyMask) - 1u;
+        const uint32_t word = s % 7u, shift = 8u * (s / 7u);
+        uint32_t got = 0;
+        if (g.lane == 0) {
+            uint32_t* p = d.items + slab + word;
+            uint32_t cur = *reinterpret_cast<volatile uint32_t*>(p);
+            for (;;) {
+                if ((cur >> shift) & 0xFFu)
+                    break; // taken meanwhile
+                const uint32_t want = cur | ((busy ? kTagBusy : tag) << shift);
+                const uint32_t old = atomicCAS(p, cur, want);
+                if (old == cur) {
+                    got = 1;
+                    break;
+                }
+                cur = old;
+            }
+        }
+        got = g.bcast(got, 0);
+        if (got)
+            return slab + kHeaderWords + s * n;
+        emptyMask &= emptyMask - 1u;
+    }
+    return kNone;
+}
+
+// Unconditional insert (CompactAccelerationHashTable::addAsWarp, compact_acceleration_hash_table.h:63-121):
+// the key gets a fresh slot even when an equal key is stored already.
+template <int G>
+__device__ __forceinline__ uint32_t table_add(const Grp<G>& g, const DevDag& d, const DevTable& t, const Key<G>& key, uint32_t& spare)
+{
+    const uint32_t cls = key.n - 2u;
+    if (key.n < 2u || key.n > 10u || t.numBuckets[cls] == 0) {
+        set_status(d.ctl, SVDAG_ERR_INVALID);
+        return kNone;
+    }
+    const uint32_t tag = tag_of(key.hb);
+    uint32_t slab = first_slab(t, cls, key.ha);
+    for (uint32_t steps = 0; steps < kMaxChain; ++steps) {
+        uint32_t next, empty;
+        probe_header<G>(g, d.items + slab, tag, next, empty);
+        const uint32_t item = claim_in_slab<G>(g, d, slab, empty, tag, key.n, false);
+        if (item != kNone) {
+            write_item<G>(g, d.items + item, key);
+            return item;
+        }
+        if (next == kEnd) {
+            if (spare == kNone)
+                spare = alloc_slab<G>(g, d, key.n);
+            if (spare == kNone)
+                return kNone;
+            uint32_t linked = kNone;
+            if (g.lane == 0)
+                linked = link_slab(d.items, slab, spare);
+            linked = g.bcast(linked, 0);
+            if (linked == spare)
+                spare = kNone;
+            next = linked;
+        }
+        slab = next;
+    }
+    set_status(d.ctl, SVDAG_ERR_TIMEOUT);
+    return kNone;
+}
+
+// Find-or-insert for keys that no other group of the same launch looks up (the DAG merge inserts
+// each distinct item once). A slot is claimed with the in-flight tag, the item written, then the
+// final tag published, so concurrent probes of other keys never compare a half-written item.
+template <int G>
+__device__ __forceinline__ uint32_t table_find_or_insert(const Grp<G>& g, const DevDag& d, const DevTable& t, const Key<G>& key,
+    uint32_t& spare, bool& inserted)
+{
+    inserted = false;
+    const uint32_t cls = key.n - 2u;
+    if (key.n < 2u || key.n > 10u || t.numBuckets[cls] == 0) {
+        set_status(d.ctl, SVDAG_ERR_INVALID);
+        return kNone;
+    }
+    const uint32_t tag = tag_of(key.hb);
+    uint32_t slab = first_slab(t, cls, key.ha);
+    uint32_t tail = slab, tailEmpty = 0;
+    for (uint32_t steps = 0;; ++steps) {
+        if (steps >= kMaxChain) {
+            set_status(d.ctl, SVDAG_ERR_CORRUPT);
+            return kNone;
+        }
+        uint32_t next, empty;
+        uint32_t cand = probe_header<G, true>(g, d.items + slab, tag, next, empty);
+        while (cand) {
+            const uint32_t s = __ffs(cand) - 1u;
+            cand &= cand - 1u;
+            const uint32_t item = slab + kHeaderWords + s * key.n;
+            if (item_equals<G, true>(g, d.items + item, key))
+                return item;
+        }
+        tail = slab;
+        tailEmpty = empty;
+        if (next == kEnd)
+            break;
+        slab = next;
+    }
+    // Not present: claim a slot at the tail of the chain (earlier slabs were full or hold other keys).
+    slab = tail;
+    uint32_t empty = tailEmpty;
+    for (uint32_t steps = 0; steps < kMaxChain; ++steps) {
+        const uint32_t item = claim_in_slab<G>(g, d, slab, empty, tag, key.n, true);
+        if (item != kNone) {
+            write_item<G>(g, d.items + item, key);
+            __threadfence();
+            g.sync();
+            if (g.lane == 0) {
+                const uint32_t s = (item - slab - kHeaderWords) / key.n;
+                atomicXor(&d.items[slab + s % 7u], (kTagBusy ^ tag) << (8u * (s / 7u)));
+            }
+            inserted = true;
+            return item;
+        }
+        uint32_t next;
+        probe_header<G, true>(g, d.items + slab, tag, next, empty);
+        if (empty)
+            continue; // a slot was freed up meanwhile (cannot happen during edits, kept for safety)
+        if (next == kEnd) {
+            if (spare == kNone)
+                spare = alloc_slab<G>(g, d, key.n);
+            if (spare == kNone)
+                return kNone;
+            uint32_t linked = kNone;
+            if (g.lane == 0)
+                linked = link_slab(d.items, slab, spare);
+            linked = g.bcast(linked, 0);
+            if (linked == spare)
+                spare = kNone;
+            next = linked;
+        }
+        slab = next;
+        probe_header<G, true>(g, d.items + slab, tag, next, empty);
+    }
+    set_status(d.ctl, SVDAG_ERR_TIMEOUT);
+    return kNone;
+}
+
+} // namespace svdag

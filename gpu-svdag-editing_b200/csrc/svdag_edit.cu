@@ -1,0 +1,1185 @@
+// svdag_edit.cu - the per-edit pipeline: top-down intermediate-SVO construction and bottom-up
+// dedup/merge into the level tables, the procedural scene builder, undo/redo.
+//
+// Reference path (mathijs727/GPU-SVDAG-Editing): editMyHashDag (my_gpu_hash_dag_edits.cu:633-671) ->
+// create_edit_intermediate_svo (create_edit_svo.cu:548-646) -> mergeDag_CUDA (my_gpu_hash_dag_edits.cu:495-631).
+//
+// B200 design: the whole edit is a fixed launch sequence over device-resident counts (no host round
+// trip per level, unlike the reference's per-level cudaMemcpy of counts and the size-histogram sync),
+// every kernel sizes itself from counters written by its predecessor, and the scratch arena layout is
+// recomputed on the device from those counts. Intra-level dedup is one open-addressing pass; the DAG
+// insert is a fused find-or-insert (the reference runs find and insert as two kernels).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "svdag_edit.cuh"
+#include "svdag_host.hpp"
+
+namespace svdag {
+
+// ---------------------------------------------------------------- device editors
+
+__device__ __forceinline__ float sqf(float f) { return f * f; }
+__device__ __forceinline__ float cmaxf(float a, float b) { return a > b ? a : b; } // constexpr_max (cuda_math.h:13)
+__device__ __forceinline__ float cminf(float a, float b) { return a < b ? a : b; } // constexpr_min (cuda_math.h:17)
+__device__ __forceinline__ float stdmaxf(float a, float b) { return a < b ? b : a; } // std::max
+
+__device__ __forceinline__ bool box_overlap(const DevEditor& e, const float* nmin, const float* nmax)
+{ // MyGpuBoxEditorBase::test_node_overlap, my_gpu_dag_editors.h:64-67
+    return !(e.bmin[0] >= nmax[0] || e.bmin[1] >= nmax[1] || e.bmin[2] >= nmax[2] || e.bmax[0] <= nmin[0] || e.bmax[1] <= nmin[1]
+        || e.bmax[2] <= nmin[2] || nmin[0] >= e.bmax[0] || nmin[1] >= e.bmax[1] || nmin[2] >= e.bmax[2] || nmax[0] <= e.bmin[0]
+        || nmax[1] <= e.bmin[1] || nmax[2] <= e.bmin[2]);
+}
+__device__ __forceinline__ bool box_contained(const DevEditor& e, const float* nmin, const float* nmax)
+{ // :76-79
+    return e.bmin[0] <= nmin[0] && e.bmin[1] <= nmin[1] && e.bmin[2] <= nmin[2] && e.bmax[0] >= nmax[0] && e.bmax[1] >= nmax[1]
+        && e.bmax[2] >= nmax[2];
+}
+__device__ __forceinline__ bool sphere_overlap(const DevEditor& e, const float* nmin, const float* nmax)
+{ // MyGpuSphereEditorBase::test_node_overlap, :420-440
+    float dist = e.radiusSquared;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if (e.center[a] < nmin[a])
+            dist -= sqf(e.center[a] - nmin[a]);
+        else if (e.center[a] > nmax[a])
+            dist -= sqf(e.center[a] - nmax[a]);
+    }
+    return dist > 0;
+}
+__device__ __forceinline__ bool sphere_contained(const DevEditor& e, const float* nmin, const float* nmax)
+{ // :442-454
+    return stdmaxf(sqf(nmin[0] - e.center[0]), sqf(nmax[0] - e.center[0])) + stdmaxf(sqf(nmin[1] - e.center[1]), sqf(nmax[1] - e.center[1]))
+        + stdmaxf(sqf(nmin[2] - e.center[2]), sqf(nmax[2] - e.center[2]))
+        < e.radiusSquared;
+}
+
+// ---- procedural terrain (integer value-noise fBm; identical to the oracle's Terrain)
+
+__device__ __forceinline__ uint32_t terrain_lattice(const DevEditor& e, uint32_t ix, uint32_t iz, uint32_t o)
+{
+    uint32_t h = fmix32(e.terrain.seed * 0x9E3779B9u ^ (o * 0x85EBCA6Bu) ^ 0x68E31DA4u);
+    h = fmix32(h ^ (ix * 0xC2B2AE35u));
+    h = fmix32(h ^ (iz * 0x27D4EB2Fu));
+    return h >> 16;
+}
+__device__ __forceinline__ long long smooth16(long long t) { return (t * t * (3 * 65536 - 2 * t)) >> 32; }
+__device__ __forceinline__ long long lerp16(long long a, long long b, long long t) { return a + (((b - a) * t) >> 16); }
+__device__ __forceinline__ uint32_t terrain_cell_log2(const DevEditor& e, uint32_t o) { return e.terrainBaseLog2 > o ? e.terrainBaseLog2 - o : 0u; }
+__device__ __forceinline__ uint32_t terrain_height_from_fbm(const DevEditor& e, long long f)
+{
+    const long long G = 1ll << e.levels;
+    const long long base = G * e.terrain.min_height_pct / 100;
+    const long long range = G * (long long)(e.terrain.max_height_pct - e.terrain.min_height_pct) / 100;
+    const long long norm = ((1ll << e.terrain.octaves) - 1) * 65536;
+    return (uint32_t)(base + (range * f) / norm);
+}
+__device__ uint32_t terrain_height(const DevEditor& e, uint32_t x, uint32_t z)
+{
+    long long f = 0;
+    for (uint32_t o = 0; o < e.terrain.octaves; ++o) {
+        const uint32_t c = terrain_cell_log2(e, o);
+        const uint32_t ix = x >> c, iz = z >> c, m = (1u << c) - 1u;
+        const long long fx = c <= 16 ? (long long)((x & m) << (16 - c)) : (long long)((x & m) >> (c - 16));
+        const long long fz = c <= 16 ? (long long)((z & m) << (16 - c)) : (long long)((z & m) >> (c - 16));
+        const long long sx = smooth16(fx), sz = smooth16(fz);
+        const long long a = lerp16(terrain_lattice(e, ix, iz, o), terrain_lattice(e, ix + 1, iz, o), sx);
+        const long long b = lerp16(terrain_lattice(e, ix, iz + 1, o), terrain_lattice(e, ix + 1, iz + 1, o), sx);
+        f += lerp16(a, b, sz) << (e.terrain.octaves - 1 - o);
+    }
+    return terrain_height_from_fbm(e, f);
+}
+__device__ void terrain_bounds(const DevEditor& e, uint32_t x0, uint32_t z0, uint32_t s, uint32_t& hlo, uint32_t& hhi)
+{
+    long long lo = 0, hi = 0;
+    for (uint32_t o = 0; o < e.terrain.octaves; ++o) {
+        const uint32_t c = terrain_cell_log2(e, o);
+        const uint32_t ix0 = x0 >> c, iz0 = z0 >> c;
+        const uint32_t ix1 = ((x0 + s - 1) >> c) + 1, iz1 = ((z0 + s - 1) >> c) + 1;
+        long long vlo = 65535, vhi = 0;
+        if ((unsigned long long)(ix1 - ix0 + 1) * (iz1 - iz0 + 1) > 64) {
+            vlo = 0;
+            vhi = 65535;
+        } else {
+            for (uint32_t iz = iz0; iz <= iz1; ++iz)
+                for (uint32_t ix = ix0; ix <= ix1; ++ix) {
+                    const long long v = terrain_lattice(e, ix, iz, o);
+                    vlo = v < vlo ? v : vlo;
+                    vhi = v > vhi ? v : vhi;
+                }
+        }
+        lo += vlo << (e.terrain.octaves - 1 - o);
+        hi += vhi << (e.terrain.octaves - 1 - o);
+    }
+    hlo = terrain_height_from_fbm(e, lo);
+    hhi = terrain_height_from_fbm(e, hi);
+}
+__device__ __forceinline__ uint32_t terrain_material(const DevEditor& e, uint32_t y)
+{
+    return (uint32_t)(((unsigned long long)y * e.terrain.num_materials) >> e.levels);
+}
+
+// ---- 3D value noise material (box noise paint), identical to the oracle's noise_material
+__device__ __forceinline__ uint32_t lattice3(uint32_t seed, uint32_t x, uint32_t y, uint32_t z)
+{
+    uint32_t h = fmix32(seed * 0x9E3779B9u ^ 0x5bd1e995u);
+    h = fmix32(h ^ (x * 0xC2B2AE35u));
+    h = fmix32(h ^ (y * 0x27D4EB2Fu));
+    h = fmix32(h ^ (z * 0x165667B1u));
+    return h >> 16;
+}
+__device__ uint32_t noise_material(uint32_t seed, uint32_t cl, uint32_t x, uint32_t y, uint32_t z)
+{
+    const uint32_t m = (1u << cl) - 1u;
+    const auto frac = [&](uint32_t v) -> long long {
+        const uint32_t f = v & m;
+        return cl <= 16 ? (long long)(f << (16 - cl)) : (long long)(f >> (cl - 16));
+    };
+    const uint32_t ix = x >> cl, iy = y >> cl, iz = z >> cl;
+    const long long sx = smooth16(frac(x)), sy = smooth16(frac(y)), sz = smooth16(frac(z));
+    const long long x00 = lerp16(lattice3(seed, ix, iy, iz), lattice3(seed, ix + 1, iy, iz), sx);
+    const long long x10 = lerp16(lattice3(seed, ix, iy + 1, iz), lattice3(seed, ix + 1, iy + 1, iz), sx);
+    const long long x01 = lerp16(lattice3(seed, ix, iy, iz + 1), lattice3(seed, ix + 1, iy, iz + 1), sx);
+    const long long x11 = lerp16(lattice3(seed, ix, iy + 1, iz + 1), lattice3(seed, ix + 1, iy + 1, iz + 1), sx);
+    const long long y0 = lerp16(x00, x10, sy), y1 = lerp16(x01, x11, sy);
+    return (uint32_t)(lerp16(y0, y1, sz) >> 12) & 0xFu;
+}
+
+// Stateless should_edit of every tool (the node is [p << depth, +2^depth)^3).
+template <uint32_t TOOL>
+__device__ __forceinline__ uint32_t should_edit(const DevEditor& e, uint32_t px, uint32_t py, uint32_t pz, uint32_t depth, uint32_t state,
+    uint32_t& fillMaterial)
+{
+    const float nmin[3] = { float(px << depth), float(py << depth), float(pz << depth) }; // Path::as_position
+    const float size = float(1u << depth);
+    const float nmax[3] = { nmin[0] + size, nmin[1] + size, nmin[2] + size };
+    if constexpr (TOOL == SVDAG_TOOL_BOX_ADD || TOOL == SVDAG_TOOL_BOX_REMOVE) { // :94-110
+        if (box_contained(e, nmin, nmax)) {
+            fillMaterial = e.material;
+            return TOOL == SVDAG_TOOL_BOX_ADD ? OP_FILL : OP_EMPTY;
+        }
+        return box_overlap(e, nmin, nmax) ? OP_SUBDIVIDE : OP_KEEP;
+    } else if constexpr (TOOL == SVDAG_TOOL_SPHERE_ADD || TOOL == SVDAG_TOOL_SPHERE_REMOVE) { // :467-487
+        const bool overlaps = sphere_overlap(e, nmin, nmax);
+        const float smin[3] = { nmin[0] + 1.0f, nmin[1] + 1.0f, nmin[2] + 1.0f };
+        const float smax[3] = { nmax[0] - 1.0f, nmax[1] - 1.0f, nmax[2] - 1.0f };
+        const bool fully = sphere_contained(e, smin, smax);
+        if (!overlaps)
+            return OP_KEEP;
+        if (fully) {
+            fillMaterial = e.material;
+            return TOOL == SVDAG_TOOL_SPHERE_ADD ? OP_FILL : OP_EMPTY;
+        }
+        return OP_SUBDIVIDE;
+    } else if constexpr (TOOL == SVDAG_TOOL_SPHERE_PAINT) { // :509-530
+        const bool overlaps = sphere_overlap(e, nmin, nmax);
+        const bool fully = sphere_contained(e, nmin, nmax);
+        if (!overlaps)
+            return OP_KEEP;
+        if (fully && state == ST_FILLED) {
+            fillMaterial = e.material;
+            return OP_FILL;
+        }
+        if (state == ST_EMPTY)
+            return OP_EMPTY;
+        return OP_SUBDIVIDE;
+    } else if constexpr (TOOL == SVDAG_TOOL_BOX_PAINT_NOISE) {
+        if (!box_overlap(e, nmin, nmax))
+            return OP_KEEP;
+        return state == ST_EMPTY ? OP_EMPTY : OP_SUBDIVIDE;
+    } else if constexpr (TOOL == SVDAG_TOOL_COPY) { // stateless form, :166-172 (used for voxels)
+        return box_overlap(e, nmin, nmax) ? OP_SUBDIVIDE : OP_KEEP;
+    } else if constexpr (TOOL == kToolTerrain) {
+        const uint32_t s = 1u << depth;
+        uint32_t hlo, hhi;
+        terrain_bounds(e, px << depth, pz << depth, s, hlo, hhi);
+        const uint32_t y0 = py << depth;
+        if (y0 >= hhi)
+            return OP_EMPTY;
+        if (y0 + s <= hlo) {
+            const uint32_t m0 = terrain_material(e, y0), m1 = terrain_material(e, y0 + s - 1);
+            if (m0 == m1) {
+                fillMaterial = m0;
+                return OP_FILL;
+            }
+        }
+        return OP_SUBDIVIDE;
+    } else {
+        return OP_KEEP;
+    }
+}
+
+// MyGpuCopyEditor::should_edit with state (the "#if 1" form, my_gpu_dag_editors.h:173-217).
+__device__ uint32_t copy_should_edit(const DevEditor& e, const DevDag& d, uint32_t px, uint32_t py, uint32_t pz, uint32_t depth,
+    const CopyParent* in, CopyParent* out)
+{
+    const float nmin[3] = { float(px << depth), float(py << depth), float(pz << depth) };
+    const float nodeSize = float(1u << depth);
+    const float nmax[3] = { nmin[0] + nodeSize, nmin[1] + nodeSize, nmin[2] + nodeSize };
+    if (!box_overlap(e, nmin, nmax))
+        return OP_KEEP;
+    float smin[3], smax[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        smin[a] = cmaxf(nmin[a], e.bmin[a]) + e.fDestToSource[a];
+        smax[a] = cminf(smin[a] + nodeSize, e.bmax[a] + e.fDestToSource[a]);
+    }
+    const uint32_t parentLevel = e.levels - depth - 1;
+    (void)parentLevel;
+    uint32_t numOut = 0;
+    for (uint32_t p = 0; p < 8; ++p) {
+        const CopyParent par = in[p];
+        if (par.handle == kNone)
+            break;
+        const uint32_t* node = d.items + par.handle;
+        const uint32_t mask = node[0] & 0xFFu;
+        for (uint32_t c = 0; c < 8; ++c) {
+            if (!(mask & (1u << c)))
+                continue;
+            const uint32_t cx = (par.x << 1) | ((c >> 2) & 1u), cy = (par.y << 1) | ((c >> 1) & 1u), cz = (par.z << 1) | (c & 1u);
+            const float cmn[3] = { float(cx << depth), float(cy << depth), float(cz << depth) };
+            const float cmx[3] = { cmn[0] + nodeSize, cmn[1] + nodeSize, cmn[2] + nodeSize };
+            // aabbOverlap, :121-125
+            const bool ov = !(cmn[0] >= smax[0] || cmn[1] >= smax[1] || cmn[2] >= smax[2] || cmx[0] <= smin[0] || cmx[1] <= smin[1]
+                || cmx[2] <= smin[2] || smin[0] >= cmx[0] || smin[1] >= cmx[1] || smin[2] >= cmx[2] || smax[0] <= cmn[0]
+                || smax[1] <= cmn[1] || smax[2] <= cmn[2]);
+            if (ov && numOut < 8) {
+                out[numOut].handle = node[1 + __popc(mask & ((1u << c) - 1u))];
+                out[numOut].x = cx;
+                out[numOut].y = cy;
+                out[numOut].z = cz;
+                ++numOut;
+            }
+        }
+    }
+    if (numOut != 8)
+        out[numOut].handle = kNone;
+    return numOut == 0 ? OP_KEEP : OP_SUBDIVIDE;
+}
+
+// material of voxel `v` of the leaf at `leaf` (get_material, my_gpu_base_dag.h:293-316)
+__device__ __forceinline__ bool leaf_get_material(uint32_t lo, uint32_t hi, const uint32_t* leaf, uint32_t v, uint32_t& out)
+{
+    const unsigned long long mask = (unsigned long long)lo | ((unsigned long long)hi << 32);
+    if (!((mask >> v) & 1ull))
+        return false;
+    const uint32_t bit = __popcll(mask & ((1ull << v) - 1ull)) * 4u;
+    out = (leaf[2 + (bit >> 5)] >> (bit & 31u)) & 0xFu;
+    return true;
+}
+
+// ---------------------------------------------------------------- kernels
+
+__device__ __forceinline__ unsigned long long work_stride(uint32_t tool) { return tool == SVDAG_TOOL_COPY ? 16ull + 128ull : 16ull; }
+
+__global__ void k_edit_begin(DevDag d, DevEditor e, char* scratch)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0)
+        return;
+    Control* c = d.ctl;
+    EditCounters& E = c->edit;
+    const uint32_t root = c->root;
+    E.rootBefore = root;
+    if (!e.builder) { // MyGPUHashDAGUndoRedo::add_frame (my_gpu_base_dag.h:23-34), ring of undoDepth frames
+        const bool same = c->undoCount > 0 && c->undo[(c->undoHead + 63u) & 63u] == root;
+        if (!same) {
+            c->redoCount = 0;
+            c->undo[c->undoHead] = root;
+            c->undoHead = (c->undoHead + 1u) & 63u;
+            c->undoCount = c->undoCount < c->undoDepth ? c->undoCount + 1u : c->undoDepth;
+        }
+    }
+    E.count[0] = 1;
+    E.offW[0] = 0;
+    WorkItem* w = reinterpret_cast<WorkItem*>(scratch);
+    w[0] = WorkItem { 0, 0, 0, root };
+    if (e.tool == SVDAG_TOOL_COPY) { // createInitialState, my_gpu_dag_editors.h:148-155
+        CopyParent* st = reinterpret_cast<CopyParent*>(scratch + 16);
+        for (int i = 0; i < 8; ++i)
+            st[i] = CopyParent { 0, 0, 0, 0 };
+        st[0].handle = e.useSavedSource ? c->savedRoot : root;
+        st[1].handle = kNone;
+    }
+}
+
+// One 8-lane group per work item, lane c evaluates child c
+// (createIntermediateSvoStructure_innerNode_warp, create_edit_svo.cu:168-303).
+template <uint32_t TOOL>
+__global__ void __launch_bounds__(256) k_build_level(DevDag d, DevEditor e, uint32_t level, char* scratch, unsigned long long scratchBytes)
+{
+    EditCounters& E = d.ctl->edit;
+    const unsigned long long stride = work_stride(TOOL);
+    const uint32_t n = E.count[level];
+    const unsigned long long offW = E.offW[level];
+    const unsigned long long offN = align256(offW + n * stride);
+    const unsigned long long offWn = align256(offN + (unsigned long long)n * 4 * kItemStride);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        E.offN[level] = offN;
+        E.offW[level + 1] = offWn;
+    }
+    if (E.overflow || n == 0)
+        return;
+    if (offN + (unsigned long long)n * 4 * kItemStride > scratchBytes) {
+        if (threadIdx.x == 0)
+            atomicExch(&E.overflow, 1u);
+        return;
+    }
+    const uint32_t lane = threadIdx.x & 31u, c = lane & 7u, grp = lane >> 3;
+    const uint32_t childLevel = level + 1, childDepth = d.levels - childLevel;
+    const uint32_t warpsTotal = gridDim.x * (blockDim.x >> 5);
+    unsigned long long edited = 0, oldRead = 0;
+    for (uint32_t base = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 4; base < n; base += warpsTotal * 4) {
+        const uint32_t i = base + grp;
+        const bool active = i < n;
+        WorkItem w { 0, 0, 0, kNone };
+        if (active)
+            w = *reinterpret_cast<const WorkItem*>(scratch + offW + i * stride);
+        uint32_t child = kNone, state = ST_EMPTY, fillMat = 0;
+        if (active && w.handle != kNone) {
+            const uint32_t* node = d.items + w.handle;
+            const uint32_t mask = node[0] & 0xFFu;
+            if (mask & (1u << c)) {
+                child = node[1 + __popc(mask & ((1u << c) - 1u))];
+                if (childLevel == d.leafLevel)
+                    state = ST_PARTIAL;
+                else
+                    state = ((d.items[child] >> 8) & 1u) ? ST_FILLED : ST_PARTIAL;
+            }
+            if (c == 0)
+                ++oldRead;
+        }
+        const uint32_t cx = (w.x << 1) | ((c >> 2) & 1u), cy = (w.y << 1) | ((c >> 1) & 1u), cz = (w.z << 1) | (c & 1u);
+        uint32_t op = OP_KEEP;
+        CopyParent childState[8];
+        if (active) {
+            if constexpr (TOOL == SVDAG_TOOL_COPY) {
+                const CopyParent* in = reinterpret_cast<const CopyParent*>(scratch + offW + i * stride + 16);
+                op = copy_should_edit(e, d, cx, cy, cz, childDepth, in, childState);
+            } else {
+                op = should_edit<TOOL>(e, cx, cy, cz, childDepth, state, fillMat);
+            }
+        }
+        if (op == OP_FILL || op == OP_EMPTY)
+            edited += 1ull << (3 * childDepth);
+        const bool subdivide = op == OP_SUBDIVIDE;
+        // One atomicAdd per warp for the children to subdivide.
+        const uint32_t bal = __ballot_sync(0xFFFFFFFFu, subdivide);
+        uint32_t idx0 = 0;
+        if (lane == 0 && bal)
+            idx0 = atomicAdd(&E.count[childLevel], __popc(bal));
+        idx0 = __shfl_sync(0xFFFFFFFFu, idx0, 0);
+        if (subdivide) {
+            const uint32_t idx = idx0 + __popc(bal & ((1u << lane) - 1u));
+            const unsigned long long at = offWn + (unsigned long long)idx * stride;
+            if (at + stride <= scratchBytes) {
+                *reinterpret_cast<WorkItem*>(scratch + at) = WorkItem { cx, cy, cz, child };
+                if constexpr (TOOL == SVDAG_TOOL_COPY) {
+                    CopyParent* out = reinterpret_cast<CopyParent*>(scratch + at + 16);
+                    for (int p = 0; p < 8; ++p)
+                        out[p] = childState[p];
+                }
+            } else {
+                atomicExch(&E.overflow, 1u);
+            }
+            child = idx;
+        } else if (op == OP_EMPTY) {
+            child = kNone;
+        } else if (op == OP_FILL) {
+            child = kFillMarker | fillMat;
+        }
+        const uint32_t present = __ballot_sync(0xFFFFFFFFu, active && child != kNone);
+        const uint32_t interm = bal;
+        const uint32_t outMask = (present >> (grp * 8)) & 0xFFu;
+        const uint32_t intMask = (interm >> (grp * 8)) & 0xFFu;
+        if (active) {
+            uint32_t* node = reinterpret_cast<uint32_t*>(scratch + offN) + (size_t)i * kItemStride;
+            const uint32_t np = __popc(outMask);
+            if (c == 0) {
+                node[0] = outMask ? (outMask | (intMask << 13)) : 0u; // encode_node_header_with_payload
+                node[9] = 0;
+            }
+            // Present children fill words 1..np in child order; words np+1..8 are cleared so that equal
+            // nodes are equal word for word (create_edit_svo.cu:285-290).
+            if (child != kNone)
+                node[1 + __popc(outMask & ((1u << c) - 1u))] = child;
+            if (c >= np)
+                node[1 + c] = 0;
+        }
+    }
+    // warp-aggregated counters
+    for (int o = 16; o > 0; o >>= 1) {
+        edited += __shfl_xor_sync(0xFFFFFFFFu, edited, o);
+        oldRead += __shfl_xor_sync(0xFFFFFFFFu, oldRead, o);
+    }
+    if (lane == 0) {
+        if (edited)
+            atomicAdd(&E.edited, edited);
+        if (oldRead)
+            atomicAdd(&E.oldRead, oldRead);
+    }
+}
+
+// One warp per leaf; lane l owns voxels l and l+32 (createIntermediateSvoStructure_leaf_workgroup,
+// create_edit_svo.cu:321-426, which uses a 64-thread block per leaf).
+template <uint32_t TOOL>
+__global__ void __launch_bounds__(256) k_build_leaves(DevDag d, DevEditor e, char* scratch, unsigned long long scratchBytes)
+{
+    EditCounters& E = d.ctl->edit;
+    const uint32_t LL = d.leafLevel;
+    const unsigned long long stride = work_stride(TOOL);
+    const uint32_t n = E.count[LL];
+    const unsigned long long offW = E.offW[LL];
+    const unsigned long long offN = align256(offW + n * stride);
+    const unsigned long long buildTop = align256(offN + (unsigned long long)n * 4 * kItemStride);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        E.offN[LL] = offN;
+        E.buildTop = buildTop;
+    }
+    if (E.overflow || n == 0)
+        return;
+    // Reserve and clear the dedup tables of every level for the bottom-up phase.
+    const MergeLayout top = merge_layout(E.count, buildTop, 0, LL);
+    if (top.end > scratchBytes) {
+        if (threadIdx.x == 0)
+            atomicExch(&E.overflow, 1u);
+        return;
+    }
+    const unsigned long long tid = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
+    const unsigned long long nthreads = (unsigned long long)gridDim.x * blockDim.x;
+    for (uint32_t l = 0; l <= LL; ++l) {
+        const MergeLayout m = merge_layout(E.count, buildTop, l, LL);
+        uint4* t = reinterpret_cast<uint4*>(scratch + m.table);
+        for (unsigned long long j = tid; j < m.cap / 2; j += nthreads)
+            t[j] = make_uint4(0, 0, 0, 0);
+    }
+
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warpsTotal = gridDim.x * (blockDim.x >> 5);
+    unsigned long long edited = 0, oldRead = 0;
+    uint32_t fullLeaves = 0;
+    for (uint32_t i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warpsTotal) {
+        const WorkItem w = *reinterpret_cast<const WorkItem*>(scratch + offW + i * stride);
+        // old leaf words (lanes 0..9)
+        uint32_t ow = 0, lo = 0, hi = 0;
+        if (w.handle != kNone) {
+            const uint32_t* leaf = d.items + w.handle;
+            const uint32_t a = lane < 2 ? leaf[lane] : 0u;
+            lo = __shfl_sync(0xFFFFFFFFu, a, 0);
+            hi = __shfl_sync(0xFFFFFFFFu, a, 1);
+            const uint32_t nw = dev_leaf_words(lo, hi);
+            ow = lane < nw ? leaf[lane] : 0u;
+            if (lane == 0)
+                ++oldRead;
+        }
+        uint32_t th = 0; // terrain: column heights in lanes 0..15
+        if constexpr (TOOL == kToolTerrain) {
+            if (lane < 16)
+                th = terrain_height(e, (w.x << 2) + (lane >> 2), (w.z << 2) + (lane & 3u));
+        }
+        uint32_t newMat[2];
+        bool set[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const uint32_t v = lane + 32u * h;
+            const unsigned long long mask = (unsigned long long)lo | ((unsigned long long)hi << 32);
+            bool hasOld = (mask >> v) & 1ull;
+            uint32_t oldMat = 0;
+            {
+                const uint32_t bit = __popcll(mask & ((1ull << v) - 1ull)) * 4u;
+                const uint32_t word = __shfl_sync(0xFFFFFFFFu, ow, 2 + ((bit >> 5) & 7u));
+                oldMat = (word >> (bit & 31u)) & 0xFu;
+            }
+            const uint32_t cc = v >> 3, f = v & 7u;
+            const uint32_t dx = ((cc >> 2) & 1u) * 2 + ((f >> 2) & 1u), dy = ((cc >> 1) & 1u) * 2 + ((f >> 1) & 1u),
+                           dz = (cc & 1u) * 2 + (f & 1u);
+            const uint32_t vx = (w.x << 2) | dx, vy = (w.y << 2) | dy, vz = (w.z << 2) | dz;
+            bool out = false;
+            uint32_t mat = 0;
+            if constexpr (TOOL == kToolTerrain) {
+                const uint32_t colH = __shfl_sync(0xFFFFFFFFu, th, dx * 4 + dz);
+                out = vy < colH;
+                mat = terrain_material(e, vy);
+                ++edited;
+            } else {
+                uint32_t fm = 0;
+                const uint32_t op = should_edit<TOOL>(e, vx, vy, vz, 0, hasOld ? ST_FILLED : ST_EMPTY, fm);
+                if (op != OP_KEEP)
+                    ++edited;
+                if (op == OP_FILL || op == OP_SUBDIVIDE) {
+                    if constexpr (TOOL == SVDAG_TOOL_BOX_ADD || TOOL == SVDAG_TOOL_SPHERE_ADD || TOOL == SVDAG_TOOL_SPHERE_PAINT) {
+                        out = true;
+                        mat = e.material;
+                    } else if constexpr (TOOL == SVDAG_TOOL_BOX_PAINT_NOISE) {
+                        out = true;
+                        mat = noise_material(e.noiseSeed, e.noiseCellLog2, vx, vy, vz);
+                    } else if constexpr (TOOL == SVDAG_TOOL_COPY) { // get_new_value(uint3, optional, State), :225-252
+                        out = hasOld;
+                        mat = oldMat;
+                        int sx = (int)vx + e.iDestToSource[0], sy = (int)vy + e.iDestToSource[1], sz = (int)vz + e.iDestToSource[2];
+                        sx = sx > 0 ? sx : 0;
+                        sy = sy > 0 ? sy : 0;
+                        sz = sz > 0 ? sz : 0;
+                        const uint32_t ux = (uint32_t)sx, uy = (uint32_t)sy, uz = (uint32_t)sz;
+                        const CopyParent* st = reinterpret_cast<const CopyParent*>(scratch + offW + i * stride + 16);
+                        uint32_t found = kNone;
+                        for (int p = 0; p < 8; ++p) {
+                            const CopyParent par = st[p];
+                            if (par.handle == kNone)
+                                break;
+                            if (par.x == (ux >> 2) && par.y == (uy >> 2) && par.z == (uz >> 2))
+                                found = par.handle;
+                        }
+                        if (found != kNone) {
+                            const uint32_t* src = d.items + found;
+                            const uint32_t bitIdx = ((ux & 1u) ? 4u : 0u) | ((uy & 1u) ? 2u : 0u) | ((uz & 1u) ? 1u : 0u) | ((ux & 2u) ? 32u : 0u)
+                                | ((uy & 2u) ? 16u : 0u) | ((uz & 2u) ? 8u : 0u);
+                            uint32_t m;
+                            if (leaf_get_material(src[0], src[1], src, bitIdx, m)) {
+                                out = true;
+                                mat = m;
+                            }
+                        }
+                    } else { // removal tools
+                        out = false;
+                    }
+                } else if (op == OP_KEEP) {
+                    out = hasOld;
+                    mat = oldMat;
+                }
+            }
+            set[h] = out;
+            newMat[h] = mat;
+        }
+        const uint32_t nlo = __ballot_sync(0xFFFFFFFFu, set[0]);
+        const uint32_t nhi = __ballot_sync(0xFFFFFFFFu, set[1]);
+        const uint32_t below = (1u << lane) - 1u;
+        const uint32_t off0 = __popc(nlo & below), off1 = __popc(nlo) + __popc(nhi & below);
+        uint32_t words[8];
+#pragma unroll
+        for (uint32_t wd = 0; wd < 8; ++wd) {
+            uint32_t v = 0;
+            if (set[0] && (off0 >> 3) == wd)
+                v |= newMat[0] << (4u * (off0 & 7u));
+            if (set[1] && (off1 >> 3) == wd)
+                v |= newMat[1] << (4u * (off1 & 7u));
+            words[wd] = __reduce_or_sync(0xFFFFFFFFu, v);
+        }
+        uint32_t* outLeaf = reinterpret_cast<uint32_t*>(scratch + offN) + (size_t)i * kItemStride;
+        uint32_t mine = 0;
+#pragma unroll
+        for (uint32_t wd = 0; wd < 8; ++wd)
+            if (lane == 2 + wd)
+                mine = words[wd];
+        if (lane == 0)
+            mine = nlo;
+        if (lane == 1)
+            mine = nhi;
+        if (lane < kItemStride)
+            outLeaf[lane] = mine;
+        if (lane == 0 && nlo == 0xFFFFFFFFu && nhi == 0xFFFFFFFFu) { // is_leaf_fully_filled (my_gpu_hash_dag.h:143-166)
+            const uint32_t m = (words[0] & 0xFu) * 0x11111111u;
+            bool full = true;
+            for (int wd = 0; wd < 8; ++wd)
+                full &= words[wd] == m;
+            fullLeaves += full ? 1u : 0u;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        edited += __shfl_xor_sync(0xFFFFFFFFu, edited, o);
+        oldRead += __shfl_xor_sync(0xFFFFFFFFu, oldRead, o);
+    }
+    if (lane == 0) {
+        if (edited)
+            atomicAdd(&E.edited, edited);
+        if (oldRead)
+            atomicAdd(&E.oldRead, oldRead);
+        if (fullLeaves)
+            atomicAdd(&E.ffCount[LL], fullLeaves);
+    }
+}
+
+__device__ __forceinline__ bool merge_live(const DevDag& d)
+{
+    const EditCounters& E = d.ctl->edit;
+    return E.count[d.leafLevel] != 0 && !E.overflow;
+}
+
+// updateChildPointers + discover_fully_filled (my_gpu_hash_dag_edits.cu:44-150), thread per node.
+__global__ void __launch_bounds__(256) k_fix_level(DevDag d, uint32_t level, uint32_t builder, char* scratch)
+{
+    EditCounters& E = d.ctl->edit;
+    if (!merge_live(d))
+        return;
+    const uint32_t LL = d.leafLevel;
+    const uint32_t n = E.count[level];
+    // Discovery at this level runs only if it ran one level down (always at the leaf level) and found
+    // fully-filled items there (my_gpu_hash_dag_edits.cu:337-351, hasFullyFilledNodes starts true at :589).
+    bool gate = true;
+    if (!builder) {
+        const bool ranBelow = (level + 1 == LL) || E.ffRan[level + 1] != 0;
+        gate = ranBelow && E.ffCount[level + 1] > 0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        E.ffRan[level] = gate ? 1u : 0u;
+    const MergeLayout ch = merge_layout(E.count, E.buildTop, level + 1, LL);
+    const uint32_t* repC = reinterpret_cast<const uint32_t*>(scratch + ch.rep);
+    const uint32_t* hC = reinterpret_cast<const uint32_t*>(scratch + ch.handle);
+    uint32_t* nodes = reinterpret_cast<uint32_t*>(scratch + E.offN[level]);
+    uint32_t full = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t* node = nodes + (size_t)i * kItemStride;
+        uint32_t w[kItemStride];
+#pragma unroll
+        for (uint32_t j = 0; j < kItemStride; ++j)
+            w[j] = node[j];
+        uint32_t mask = w[0] & 0xFFu;
+        const uint32_t interm = w[0] >> 13;
+        uint32_t outW[8];
+        uint32_t in = 1, out = 0;
+        for (uint32_t c = 0; c < 8; ++c) {
+            if (!(mask & (1u << c)))
+                continue;
+            uint32_t h = w[in++];
+            if (interm & (1u << c)) {
+                const uint32_t r = repC[h];
+                h = r == kEmptyRep ? kNone : hC[r];
+            } else if (h >= kFillMarker && h != kNone) {
+                h = d.ctl->fullyFilled[level + 1][h & 0xFu];
+            }
+            if (h != kNone)
+                outW[out++] = h;
+            else
+                mask ^= 1u << c;
+        }
+        uint32_t header = mask;
+        if (gate && mask == 0xFFu) {
+            bool all = true;
+            uint32_t mat = 0;
+            for (uint32_t c = 0; c < 8 && all; ++c) {
+                const uint32_t* p = d.items + outW[c];
+                uint32_t cm;
+                if (level + 1 == LL) {
+                    all = p[0] == 0xFFFFFFFFu && p[1] == 0xFFFFFFFFu;
+                    cm = p[2] & 0xFu;
+                    for (uint32_t j = 2; j < 10 && all; ++j)
+                        all = p[j] == cm * 0x11111111u;
+                } else {
+                    const uint32_t hh = p[0];
+                    all = (hh >> 8) & 1u;
+                    cm = (hh >> 9) & 0xFu;
+                }
+                if (c == 0)
+                    mat = cm;
+                all = all && cm == mat;
+            }
+            if (all) {
+                header = 0xFFu | (1u << 8) | (mat << 9);
+                ++full;
+            }
+        }
+        node[0] = header;
+        for (uint32_t j = 0; j < 8; ++j)
+            node[1 + j] = j < out ? outW[j] : 0u;
+        node[9] = 0;
+    }
+    if (full)
+        atomicAdd(&E.ffCount[level], full);
+}
+
+// Intra-level dedup (insertDuplicatesIntoHashTableAsWarp + findUniqueInHashTableAsWarp_kernel1,
+// my_gpu_hash_dag_edits.cu:164-218) as one open-addressing pass; rep[i] = index of the item's
+// representative, kEmptyRep for an empty item.
+__global__ void __launch_bounds__(256) k_dedup_level(DevDag d, uint32_t level, char* scratch)
+{
+    EditCounters& E = d.ctl->edit;
+    if (!merge_live(d))
+        return;
+    const uint32_t LL = d.leafLevel;
+    const uint32_t n = E.count[level];
+    const MergeLayout m = merge_layout(E.count, E.buildTop, level, LL);
+    uint32_t* rep = reinterpret_cast<uint32_t*>(scratch + m.rep);
+    unsigned long long* table = reinterpret_cast<unsigned long long*>(scratch + m.table);
+    const uint32_t* items = reinterpret_cast<const uint32_t*>(scratch + E.offN[level]);
+    const uint32_t capMask = m.cap - 1u;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t* it = items + (size_t)i * kItemStride;
+        uint32_t w[kItemStride];
+#pragma unroll
+        for (uint32_t j = 0; j < kItemStride; ++j)
+            w[j] = it[j];
+        const bool isEmpty = level == LL ? (w[0] == 0 && w[1] == 0) : ((w[0] & 0xFFu) == 0);
+        if (isEmpty) {
+            rep[i] = kEmptyRep;
+            continue;
+        }
+        const uint32_t nw = level == LL ? dev_leaf_words(w[0], w[1]) : dev_node_words(w[0]);
+        uint32_t ha, hb;
+        hash_words(w, nw, ha, hb);
+        const unsigned long long entry = ((unsigned long long)hb << 32) | (unsigned long long)(i + 1u);
+        uint32_t slot = ha & capMask, r = i;
+        for (uint32_t probe = 0; probe <= capMask; ++probe) {
+            unsigned long long e = table[slot];
+            if (e == 0) {
+                e = atomicCAS(&table[slot], 0ull, entry);
+                if (e == 0)
+                    break;
+            }
+            if ((uint32_t)(e >> 32) == hb) {
+                const uint32_t j = (uint32_t)e - 1u;
+                const uint32_t* q = items + (size_t)j * kItemStride;
+                bool same = true;
+                for (uint32_t k = 0; k < nw && same; ++k)
+                    same = q[k] == w[k];
+                if (same) {
+                    r = j;
+                    break;
+                }
+            }
+            slot = (slot + 1u) & capMask;
+        }
+        rep[i] = r;
+        if (r == i) {
+            atomicAdd(&E.repCount[level], 1u);
+            atomicAdd(&E.repPerClass[level][nw - 2], 1u);
+        }
+    }
+}
+
+// Find-or-insert of each representative into the level table (findUniqueInHashTableAsWarp_kernel2 +
+// insertUniqueInHashTableAsWarp_kernel, my_gpu_hash_dag_edits.cu:220-280, fused).
+template <int G>
+__global__ void __launch_bounds__(256) k_insert_level(DevDag d, DevTable t, uint32_t level, char* scratch)
+{
+    EditCounters& E = d.ctl->edit;
+    if (!merge_live(d))
+        return;
+    const uint32_t n = E.count[level];
+    const MergeLayout m = merge_layout(E.count, E.buildTop, level, d.leafLevel);
+    const uint32_t* rep = reinterpret_cast<const uint32_t*>(scratch + m.rep);
+    uint32_t* handle = reinterpret_cast<uint32_t*>(scratch + m.handle);
+    const uint32_t* items = reinterpret_cast<const uint32_t*>(scratch + E.offN[level]);
+    Grp<G> g;
+    const uint32_t groupsPerBlock = blockDim.x / G;
+    uint32_t spare = kNone, added = 0;
+    for (uint32_t i = blockIdx.x * groupsPerBlock + threadIdx.x / G; i < n; i += gridDim.x * groupsPerBlock) {
+        if (rep[i] != i)
+            continue;
+        Key<G> key;
+        load_key<G>(g, items + (size_t)i * kItemStride, kItemStride, t.kind, key);
+        bool ins = false;
+        const uint32_t h = table_find_or_insert<G>(g, d, t, key, spare, ins);
+        if (g.lane == 0) {
+            handle[i] = h;
+            added += ins ? 1u : 0u;
+        }
+    }
+    if (added)
+        atomicAdd(&E.added, (unsigned long long)added);
+}
+
+__global__ void k_edit_end(DevDag d, char* scratch, uint32_t builder)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0)
+        return;
+    Control* c = d.ctl;
+    EditCounters& E = c->edit;
+    if (E.overflow) {
+        set_status(c, SVDAG_ERR_OOM);
+    } else if (E.count[d.leafLevel] != 0 && c->status == 0) {
+        const MergeLayout m = merge_layout(E.count, E.buildTop, 0, d.leafLevel);
+        const uint32_t r = reinterpret_cast<const uint32_t*>(scratch + m.rep)[0];
+        c->root = r == kEmptyRep ? kNone : reinterpret_cast<const uint32_t*>(scratch + m.handle)[r];
+    } else if (builder && E.count[d.leafLevel] == 0) {
+        c->root = kNone;
+    }
+    E.rootAfter = c->root;
+}
+
+__global__ void k_undo_redo(Control* c, uint32_t redo)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0)
+        return;
+    if (!redo) { // MyGPUHashDAGUndoRedo::undo, my_gpu_base_dag.h:35-49
+        if (c->undoCount == 0)
+            return;
+        c->undoHead = (c->undoHead + 63u) & 63u;
+        const uint32_t f = c->undo[c->undoHead];
+        c->undoCount--;
+        if (c->redoCount < 64)
+            c->redo[c->redoCount++] = c->root;
+        c->root = f;
+    } else { // redo, :50-64
+        if (c->redoCount == 0)
+            return;
+        const uint32_t f = c->redo[--c->redoCount];
+        c->undo[c->undoHead] = c->root;
+        c->undoHead = (c->undoHead + 1u) & 63u;
+        c->undoCount = c->undoCount < c->undoDepth ? c->undoCount + 1u : c->undoDepth;
+        c->root = f;
+    }
+}
+
+__global__ void k_save_root(Control* c) { c->savedRoot = c->root; }
+
+// ---------------------------------------------------------------- host orchestration
+
+namespace {
+
+DevEditor make_editor(const svdag_ctx* ctx, const svdag_edit& e)
+{
+    DevEditor d {};
+    d.tool = e.tool;
+    d.material = e.material;
+    d.levels = ctx->cfg.levels;
+    const float c[3] = { e.center[0], e.center[1], e.center[2] };
+    auto box = [&](const float* center, float r) { // MyGpuBoxEditorBase constructor, my_gpu_dag_editors.h:50-55
+        for (int a = 0; a < 3; ++a) {
+            d.bmin[a] = center[a] - r;
+            d.bmax[a] = r == 0 ? center[a] + 1.0f : center[a] + r;
+        }
+    };
+    switch (e.tool) {
+    case SVDAG_TOOL_BOX_ADD:
+    case SVDAG_TOOL_BOX_REMOVE:
+    case SVDAG_TOOL_BOX_PAINT_NOISE:
+        box(c, e.radius);
+        d.noiseSeed = e.noise_seed;
+        d.noiseCellLog2 = e.noise_cell_log2;
+        break;
+    case SVDAG_TOOL_SPHERE_ADD:
+    case SVDAG_TOOL_SPHERE_REMOVE:
+    case SVDAG_TOOL_SPHERE_PAINT: // MyGpuSphereEditorBase constructor, :406-411
+        for (int a = 0; a < 3; ++a)
+            d.center[a] = c[a] + 0.5f;
+        d.radius = std::max(e.radius, 0.1f);
+        d.radiusSquared = d.radius * d.radius;
+        break;
+    case SVDAG_TOOL_COPY: { // MyGpuCopyEditor constructor, :157-164
+        float center[3];
+        for (int a = 0; a < 3; ++a) {
+            center[a] = e.dst[a] + (c[a] - e.src[a]);
+            d.fDestToSource[a] = -e.dst[a] + e.src[a];
+            d.iDestToSource[a] = (int32_t)d.fDestToSource[a];
+        }
+        box(center, e.radius);
+    } break;
+    default:
+        break;
+    }
+    return d;
+}
+
+template <uint32_t TOOL>
+svdag_status launch_build(svdag_ctx* ctx, const DevEditor& ed, cudaStream_t s)
+{
+    const DevDag d = ctx->dag();
+    const uint32_t LL = d.leafLevel;
+    for (uint32_t level = 0; level < LL; ++level) {
+        const unsigned long long bound = level < 8 ? (1ull << (3 * level)) : (1ull << 24);
+        k_build_level<TOOL><<<grid_for(ctx, bound * 8, 256), 256, 0, s>>>(d, ed, level, ctx->scratch, ctx->scratchBytes);
+    }
+    const unsigned long long bound = LL < 8 ? (1ull << (3 * LL)) : (1ull << 24);
+    k_build_leaves<TOOL><<<grid_for(ctx, bound * 32, 256), 256, 0, s>>>(d, ed, ctx->scratch, ctx->scratchBytes);
+    SVDAG_CUDA(cudaGetLastError());
+    return SVDAG_OK;
+}
+
+svdag_status launch_build_any(svdag_ctx* ctx, const DevEditor& ed, cudaStream_t s)
+{
+    switch (ed.tool) {
+    case SVDAG_TOOL_SPHERE_ADD:
+        return launch_build<SVDAG_TOOL_SPHERE_ADD>(ctx, ed, s);
+    case SVDAG_TOOL_SPHERE_REMOVE:
+        return launch_build<SVDAG_TOOL_SPHERE_REMOVE>(ctx, ed, s);
+    case SVDAG_TOOL_BOX_ADD:
+        return launch_build<SVDAG_TOOL_BOX_ADD>(ctx, ed, s);
+    case SVDAG_TOOL_BOX_REMOVE:
+        return launch_build<SVDAG_TOOL_BOX_REMOVE>(ctx, ed, s);
+    case SVDAG_TOOL_SPHERE_PAINT:
+        return launch_build<SVDAG_TOOL_SPHERE_PAINT>(ctx, ed, s);
+    case SVDAG_TOOL_COPY:
+        return launch_build<SVDAG_TOOL_COPY>(ctx, ed, s);
+    case SVDAG_TOOL_BOX_PAINT_NOISE:
+        return launch_build<SVDAG_TOOL_BOX_PAINT_NOISE>(ctx, ed, s);
+    case kToolTerrain:
+        return launch_build<kToolTerrain>(ctx, ed, s);
+    default:
+        return SVDAG_ERR_INVALID;
+    }
+}
+
+svdag_status launch_insert(svdag_ctx* ctx, uint32_t level, unsigned long long bound, cudaStream_t s)
+{
+    const DevDag d = ctx->dag();
+    const DevTable t = ctx->levelTables[level].dev;
+    const uint32_t G = ctx->probeLanes;
+    const int grid = grid_for(ctx, bound * G, 256);
+    switch (G) {
+    case 1:
+        k_insert_level<1><<<grid, 256, 0, s>>>(d, t, level, ctx->scratch);
+        break;
+    case 2:
+        k_insert_level<2><<<grid, 256, 0, s>>>(d, t, level, ctx->scratch);
+        break;
+    case 4:
+        k_insert_level<4><<<grid, 256, 0, s>>>(d, t, level, ctx->scratch);
+        break;
+    case 16:
+        k_insert_level<16><<<grid, 256, 0, s>>>(d, t, level, ctx->scratch);
+        break;
+    case 32:
+        k_insert_level<32><<<grid, 256, 0, s>>>(d, t, level, ctx->scratch);
+        break;
+    default:
+        k_insert_level<8><<<grid, 256, 0, s>>>(d, t, level, ctx->scratch);
+        break;
+    }
+    SVDAG_CUDA(cudaGetLastError());
+    return SVDAG_OK;
+}
+
+unsigned long long level_bound(uint32_t level) { return level < 8 ? (1ull << (3 * level)) : (1ull << 24); }
+
+} // namespace
+
+svdag_status launch_pipeline(svdag_ctx* ctx, const DevEditor& ed, cudaStream_t s)
+{
+    const DevDag d = ctx->dag();
+    SVDAG_CUDA(cudaMemsetAsync(&ctx->ctl->edit, 0, sizeof(EditCounters), s));
+    k_edit_begin<<<1, 32, 0, s>>>(d, ed, ctx->scratch);
+    SVDAG_TRY(launch_build_any(ctx, ed, s));
+    const uint32_t LL = d.leafLevel;
+    for (int level = (int)LL; level >= 0; --level) {
+        if (level < (int)LL)
+            k_fix_level<<<grid_for(ctx, level_bound(level), 256), 256, 0, s>>>(d, level, 0, ctx->scratch);
+        k_dedup_level<<<grid_for(ctx, level_bound(level), 256), 256, 0, s>>>(d, level, ctx->scratch);
+        SVDAG_TRY(launch_insert(ctx, level, level_bound(level), s));
+    }
+    k_edit_end<<<1, 32, 0, s>>>(d, ctx->scratch, 0);
+    SVDAG_CUDA(cudaGetLastError());
+    return SVDAG_OK;
+}
+
+svdag_status run_edit(svdag_ctx* ctx, const svdag_edit* e, cudaStream_t s)
+{
+    SVDAG_TRY(ensure_level_tables(ctx, s));
+    if (e->tool == SVDAG_TOOL_MOVE) { // clear the source box, then paste from the DAG before the clear
+        k_save_root<<<1, 1, 0, s>>>(ctx->ctl);
+        svdag_edit rm = *e;
+        rm.tool = SVDAG_TOOL_BOX_REMOVE;
+        SVDAG_TRY(launch_pipeline(ctx, make_editor(ctx, rm), s));
+        svdag_edit cp = *e;
+        cp.tool = SVDAG_TOOL_COPY;
+        DevEditor ed = make_editor(ctx, cp);
+        ed.useSavedSource = 1;
+        return launch_pipeline(ctx, ed, s);
+    }
+    return launch_pipeline(ctx, make_editor(ctx, *e), s);
+}
+
+// Scene construction: the terrain runs through the same pipeline as an edit of an empty DAG, with
+// fully-filled discovery on every level (the factory's create_dag_cpu propagates the fully-filled
+// bits everywhere, my_gpu_hash_dag_factory.cpp:350-353) and each level table sized from the exact
+// number of distinct items of that level (the reference resizes with setLoadFactor afterwards,
+// my_gpu_hash_dag.cu:139-155).
+svdag_status run_terrain_build(svdag_ctx* ctx, const svdag_terrain_params* p, cudaStream_t s)
+{
+    // Reset the DAG: empty item region, no tables, empty history.
+    reset_level_tables(ctx);
+    {
+        Control init {};
+        init.root = kNone;
+        init.undoDepth = ctx->cfg.undo_depth ? std::min<uint32_t>(ctx->cfg.undo_depth, 64) : 32;
+        for (auto& lv : init.fullyFilled)
+            for (auto& m : lv)
+                m = kNone;
+        init.savedRoot = kNone;
+        SVDAG_CUDA(cudaMemcpyAsync(ctx->ctl, &init, sizeof(init), cudaMemcpyHostToDevice, s));
+    }
+    DevEditor ed {};
+    ed.tool = kToolTerrain;
+    ed.terrain = *p;
+    ed.levels = ctx->cfg.levels;
+    ed.terrainBaseLog2 = ctx->cfg.levels - 2;
+    ed.builder = 1;
+    const DevDag d = ctx->dag();
+    SVDAG_CUDA(cudaMemsetAsync(&ctx->ctl->edit, 0, sizeof(EditCounters), s));
+    k_edit_begin<<<1, 32, 0, s>>>(d, ed, ctx->scratch);
+    SVDAG_TRY(launch_build_any(ctx, ed, s));
+    const uint32_t LL = d.leafLevel;
+    for (int level = (int)LL; level >= 0; --level) {
+        if (level < (int)LL)
+            k_fix_level<<<grid_for(ctx, level_bound(level), 256), 256, 0, s>>>(d, level, 1, ctx->scratch);
+        k_dedup_level<<<grid_for(ctx, level_bound(level), 256), 256, 0, s>>>(d, level, ctx->scratch);
+        SVDAG_CUDA(cudaGetLastError());
+        uint32_t reps[kNumClasses];
+        SVDAG_CUDA(cudaMemcpyAsync(reps, &ctx->ctl->edit.repPerClass[level][0], sizeof(reps), cudaMemcpyDeviceToHost, s));
+        uint32_t overflow = 0;
+        SVDAG_CUDA(cudaMemcpyAsync(&overflow, &ctx->ctl->edit.overflow, sizeof(overflow), cudaMemcpyDeviceToHost, s));
+        SVDAG_CUDA(cudaStreamSynchronize(s));
+        if (overflow)
+            return SVDAG_ERR_OOM;
+        uint32_t buckets[kNumClasses];
+        for (uint32_t c = 0; c < kNumClasses; ++c) {
+            const unsigned long long items = (unsigned long long)reps[c] + SVDAG_NUM_MATERIALS;
+            buckets[c] = (uint32_t)std::max<unsigned long long>(1, (items + ctx->loadFactor - 1) / ctx->loadFactor);
+        }
+        svdag_table& t = ctx->levelTables[level];
+        SVDAG_TRY(alloc_table(ctx, &t, level == (int)LL ? SVDAG_KIND_LEAF : SVDAG_KIND_NODE, buckets, s));
+        t.level = level;
+        SVDAG_TRY(insert_canonical(ctx, (uint32_t)level, s));
+        SVDAG_TRY(launch_insert(ctx, level, level_bound(level), s));
+    }
+    k_edit_end<<<1, 32, 0, s>>>(d, ctx->scratch, 1);
+    SVDAG_CUDA(cudaGetLastError());
+    return read_status(ctx, s);
+}
+
+} // namespace svdag
+
+using namespace svdag;
+
+extern "C" {
+
+svdag_status svdag_build_terrain(svdag_ctx* ctx, const svdag_terrain_params* p, void* stream)
+{
+    if (!ctx || !p || p->octaves == 0 || p->octaves > 16 || p->num_materials == 0 || p->num_materials > SVDAG_NUM_MATERIALS
+        || p->max_height_pct > 100 || p->min_height_pct > p->max_height_pct)
+        return SVDAG_ERR_INVALID;
+    if (p->num_structures != 0)
+        return SVDAG_ERR_UNSUPPORTED;
+    return run_terrain_build(ctx, p, as_stream(stream));
+}
+
+svdag_status svdag_edit_apply(svdag_ctx* ctx, const svdag_edit* e, void* stream)
+{
+    if (!ctx || !e || e->tool >= SVDAG_NUM_TOOLS || e->material >= SVDAG_NUM_MATERIALS)
+        return SVDAG_ERR_INVALID;
+    if (e->tool == SVDAG_TOOL_BOX_PAINT_NOISE && e->noise_cell_log2 > 20)
+        return SVDAG_ERR_INVALID;
+    for (int a = 0; a < 3; ++a)
+        if (!std::isfinite(e->center[a]) || !std::isfinite(e->src[a]) || !std::isfinite(e->dst[a]))
+            return SVDAG_ERR_INVALID;
+    if (!std::isfinite(e->radius) || e->radius < 0)
+        return SVDAG_ERR_INVALID;
+    return run_edit(ctx, e, as_stream(stream));
+}
+
+svdag_status svdag_edit_apply_many(svdag_ctx* ctx, const svdag_edit* edits, uint32_t count, void* stream)
+{
+    if (!ctx || (count && !edits))
+        return SVDAG_ERR_INVALID;
+    for (uint32_t i = 0; i < count; ++i)
+        SVDAG_TRY(svdag_edit_apply(ctx, &edits[i], stream));
+    return SVDAG_OK;
+}
+
+svdag_status svdag_last_edit_stats(svdag_ctx* ctx, svdag_edit_stats* out, void* stream)
+{
+    if (!ctx || !out)
+        return SVDAG_ERR_INVALID;
+    cudaStream_t s = as_stream(stream);
+    EditCounters E;
+    SVDAG_CUDA(cudaMemcpyAsync(&E, &ctx->ctl->edit, sizeof(E), cudaMemcpyDeviceToHost, s));
+    uint32_t status = 0;
+    SVDAG_CUDA(cudaMemcpyAsync(&status, &ctx->ctl->status, sizeof(status), cudaMemcpyDeviceToHost, s));
+    SVDAG_CUDA(cudaStreamSynchronize(s));
+    std::memset(out, 0, sizeof(*out));
+    unsigned long long reps = 0;
+    for (uint32_t l = 0; l < kMaxLevels; ++l) {
+        out->svo_nodes[l] = E.count[l];
+        reps += E.repCount[l];
+    }
+    out->old_items_read = E.oldRead;
+    out->unique_items = reps;
+    out->new_items = E.added;
+    out->edited_voxels = E.edited;
+    out->root_before = E.rootBefore;
+    out->root_after = E.rootAfter;
+    out->status = E.overflow ? SVDAG_ERR_OOM : status;
+    const unsigned long long used = E.count[ctx->cfg.levels - 2] ? merge_layout(E.count, E.buildTop, 0, ctx->cfg.levels - 2).end : E.buildTop;
+    ctx->scratchHighWater = std::max(ctx->scratchHighWater, used);
+    return SVDAG_OK;
+}
+
+svdag_status svdag_edit_sphere(svdag_ctx* ctx, float cx, float cy, float cz, float r, uint32_t material, int add, void* stream)
+{
+    svdag_edit e {};
+    e.tool = add ? SVDAG_TOOL_SPHERE_ADD : SVDAG_TOOL_SPHERE_REMOVE;
+    e.material = material;
+    e.center[0] = cx;
+    e.center[1] = cy;
+    e.center[2] = cz;
+    e.radius = r;
+    return svdag_edit_apply(ctx, &e, stream);
+}
+svdag_status svdag_edit_box(svdag_ctx* ctx, float cx, float cy, float cz, float h, uint32_t material, int add, void* stream)
+{
+    svdag_edit e {};
+    e.tool = add ? SVDAG_TOOL_BOX_ADD : SVDAG_TOOL_BOX_REMOVE;
+    e.material = material;
+    e.center[0] = cx;
+    e.center[1] = cy;
+    e.center[2] = cz;
+    e.radius = h;
+    return svdag_edit_apply(ctx, &e, stream);
+}
+svdag_status svdag_edit_paint(svdag_ctx* ctx, float cx, float cy, float cz, float r, uint32_t material, void* stream)
+{
+    svdag_edit e {};
+    e.tool = SVDAG_TOOL_SPHERE_PAINT;
+    e.material = material;
+    e.center[0] = cx;
+    e.center[1] = cy;
+    e.center[2] = cz;
+    e.radius = r;
+    return svdag_edit_apply(ctx, &e, stream);
+}
+svdag_status svdag_edit_paint_noise(svdag_ctx* ctx, float cx, float cy, float cz, float h, uint32_t seed, uint32_t cellLog2, void* stream)
+{
+    svdag_edit e {};
+    e.tool = SVDAG_TOOL_BOX_PAINT_NOISE;
+    e.center[0] = cx;
+    e.center[1] = cy;
+    e.center[2] = cz;
+    e.radius = h;
+    e.noise_seed = seed;
+    e.noise_cell_log2 = cellLog2;
+    return svdag_edit_apply(ctx, &e, stream);
+}
+svdag_status svdag_edit_copy(svdag_ctx* ctx, const float src[3], const float dst[3], const float center[3], float radius, void* stream)
+{
+    if (!src || !dst || !center)
+        return SVDAG_ERR_INVALID;
+    svdag_edit e {};
+    e.tool = SVDAG_TOOL_COPY;
+    for (int a = 0; a < 3; ++a) {
+        e.src[a] = src[a];
+        e.dst[a] = dst[a];
+        e.center[a] = center[a];
+    }
+    e.radius = radius;
+    return svdag_edit_apply(ctx, &e, stream);
+}
+
+svdag_status svdag_undo(svdag_ctx* ctx, void* stream)
+{
+    if (!ctx)
+        return SVDAG_ERR_INVALID;
+    k_undo_redo<<<1, 1, 0, as_stream(stream)>>>(ctx->ctl, 0);
+    SVDAG_CUDA(cudaGetLastError());
+    return SVDAG_OK;
+}
+svdag_status svdag_redo(svdag_ctx* ctx, void* stream)
+{
+    if (!ctx)
+        return SVDAG_ERR_INVALID;
+    k_undo_redo<<<1, 1, 0, as_stream(stream)>>>(ctx->ctl, 1);
+    SVDAG_CUDA(cudaGetLastError());
+    return SVDAG_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,69 @@
+// svdag_edit.cuh - device editors and the per-edit scratch layout.
+//
+// The editors restate the reference tools' predicates with the same float expressions
+// (my_gpu_dag_editors.h). The library is built with -fmad=false so no expression is contracted:
+// Fill/Empty/Subdivide decisions, and so the DAG structure, are then bit-identical to the
+// uncontracted IEEE evaluation the oracle performs on the CPU.
+#pragma once
+#include "svdag_device.cuh"
+
+namespace svdag {
+
+enum : uint32_t { OP_SUBDIVIDE = 0, OP_FILL = 1, OP_EMPTY = 2, OP_KEEP = 3 };
+enum : uint32_t { ST_PARTIAL = 0, ST_FILLED = 1, ST_EMPTY = 2 };
+constexpr uint32_t kToolTerrain = 100; // internal: the procedural scene builder
+constexpr uint32_t kEmptyRep = 0xFFFFFFFEu; // dedup result of an empty SVO item
+
+struct DevEditor {
+    uint32_t tool;
+    uint32_t material;
+    float bmin[3], bmax[3]; // box, copy destination box, noise box (MyGpuBoxEditorBase)
+    float center[3]; // sphere centre (+0.5 applied)
+    float radius, radiusSquared;
+    float fDestToSource[3];
+    int32_t iDestToSource[3];
+    uint32_t noiseSeed, noiseCellLog2;
+    svdag_terrain_params terrain;
+    uint32_t terrainBaseLog2;
+    uint32_t levels;
+    uint32_t useSavedSource; // copy: read the source from the saved root (move)
+    uint32_t builder; // scene build: fully-filled discovery on every level, no undo frame
+};
+
+struct WorkItem { // CreateIntermediateWorkItem (create_edit_svo.cu:55-65)
+    uint32_t x, y, z, handle;
+};
+struct CopyParent {
+    uint32_t x, y, z, handle;
+};
+
+__host__ __device__ inline unsigned long long align256(unsigned long long v) { return (v + 255ull) & ~255ull; }
+
+struct MergeLayout {
+    unsigned long long rep, handle, table, end;
+    uint32_t cap;
+};
+
+// Scratch layout of the bottom-up phase; every thread recomputes it from the final level counts.
+__host__ __device__ inline MergeLayout merge_layout(const uint32_t* count, unsigned long long buildTop, uint32_t level, uint32_t leafLevel)
+{
+    unsigned long long off = buildTop;
+    MergeLayout m {};
+    for (int l = (int)leafLevel; l >= 0; --l) {
+        const unsigned long long n = count[l];
+        uint32_t cap = 2;
+        while (cap < 2ull * n)
+            cap <<= 1;
+        m.rep = off;
+        m.handle = align256(m.rep + 4 * n);
+        m.table = align256(m.handle + 4 * n);
+        m.end = align256(m.table + 8ull * cap);
+        m.cap = cap;
+        if ((uint32_t)l == level)
+            return m;
+        off = m.end;
+    }
+    return m;
+}
+
+} // namespace svdag

@@ -1,0 +1,78 @@
+// svdag_host.hpp - host-side context of libsvdag (shared by the .cu translation units).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <vector>
+
+#include "svdag_device.cuh"
+
+struct svdag_table {
+    svdag_ctx* ctx = nullptr;
+    svdag::DevTable dev {};
+    int level = -1; // -1 for standalone tables
+    bool ready = false;
+    unsigned long long words = 0; // words of the bucket arrays
+};
+
+struct svdag_ctx {
+    svdag_config cfg {};
+    int device = 0;
+    char* pool = nullptr;
+    size_t poolBytes = 0;
+    svdag::Control* ctl = nullptr; // device control block
+    char* scratch = nullptr; // per-edit arena
+    unsigned long long scratchBytes = 0;
+    uint32_t* items = nullptr; // item region
+    unsigned long long itemWords = 0;
+    svdag_table levelTables[svdag::kMaxLevels];
+    std::vector<svdag_table*> standalone;
+    uint32_t probeLanes = 8;
+    uint32_t loadFactor = 16;
+    unsigned long long scratchHighWater = 0;
+    svdag::DevDag dag() const { return svdag::DevDag { items, itemWords, ctl, cfg.levels, cfg.levels - 2 }; }
+};
+
+namespace svdag {
+
+// Maps a CUDA error to a status (and remembers nothing: CUDA errors are reported where they occur).
+inline svdag_status cuda_status(cudaError_t e)
+{
+    if (e == cudaSuccess)
+        return SVDAG_OK;
+    std::fprintf(stderr, "libsvdag: CUDA error %s\n", cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? SVDAG_ERR_OOM : SVDAG_ERR_CUDA;
+}
+
+#define SVDAG_CUDA(call)                                      \
+    do {                                                      \
+        const cudaError_t e_ = (call);                        \
+        if (e_ != cudaSuccess)                                \
+            return ::svdag::cuda_status(e_);                  \
+    } while (0)
+#define SVDAG_TRY(call)                                       \
+    do {                                                      \
+        const svdag_status s_ = (call);                       \
+        if (s_ != SVDAG_OK)                                   \
+            return s_;                                        \
+    } while (0)
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Number of resident-CTA-sized grid for grid-stride kernels: a multiple of the SM count.
+int grid_for(const svdag_ctx* ctx, unsigned long long work, int threadsPerBlock, int blocksPerSm = 8);
+
+// Table management (svdag_tables.cu).
+svdag_status alloc_table(svdag_ctx* ctx, svdag_table* t, uint32_t kind, const uint32_t* bucketsPerClass, cudaStream_t s);
+svdag_status ensure_level_tables(svdag_ctx* ctx, cudaStream_t s);
+svdag_status insert_canonical(svdag_ctx* ctx, uint32_t level, cudaStream_t s);
+svdag_status upload_tables(svdag_ctx* ctx, cudaStream_t s);
+svdag_status read_status(svdag_ctx* ctx, cudaStream_t s);
+void reset_level_tables(svdag_ctx* ctx);
+
+// Edit machinery (svdag_edit.cu).
+svdag_status run_edit(svdag_ctx* ctx, const svdag_edit* e, cudaStream_t s);
+svdag_status run_terrain_build(svdag_ctx* ctx, const svdag_terrain_params* p, cudaStream_t s);
+
+} // namespace svdag

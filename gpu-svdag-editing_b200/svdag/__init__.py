@@ -1,0 +1,451 @@
+"""Python host binding of libsvdag (C ABI declared in include/svdag.h).
+
+The names mirror the reference's EDag::MyGpuDag interface (mathijs727/GPU-SVDAG-Editing):
+``MyGPUHashDAG`` (my_gpu_hash_dag.h), the tool classes of my_gpu_dag_editors.h, ``editMyHashDag``
+(my_gpu_hash_dag_edits.h:12-13), ``MyGPUHashDAGUndoRedo`` (my_gpu_base_dag.h:16-82) and
+``DAGTracer.resolve_paths`` (dag_tracer.h:33). Every call goes through the CUDA library; there is no
+CPU path: importing this module on a machine where libsvdag.so is missing raises, and creating a
+context without an sm_100 device raises ``SvdagError(SVDAG_ERR_NO_DEVICE)``.
+
+Device buffers and streams are plain CUDA pointers; torch tensors are accepted for convenience
+(``.data_ptr()`` / ``torch.cuda.Stream.cuda_stream``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG_ROOT = os.path.dirname(HERE)
+LIB_PATH = os.path.join(PKG_ROOT, "libsvdag.so")
+
+MAX_LEVELS = 17
+MAX_ITEM_WORDS = 10
+NUM_SIZE_CLASSES = 9
+NUM_MATERIALS = 16
+INVALID_HANDLE = 0xFFFFFFFF
+NO_MATERIAL = 0xFFFFFFFF
+
+KIND_NODE, KIND_LEAF = 0, 1
+
+TOOL_SPHERE_ADD, TOOL_SPHERE_REMOVE, TOOL_BOX_ADD, TOOL_BOX_REMOVE = 0, 1, 2, 3
+TOOL_SPHERE_PAINT, TOOL_COPY, TOOL_BOX_PAINT_NOISE, TOOL_MOVE = 4, 5, 6, 7
+
+STATUS = {0: "SVDAG_OK", 1: "SVDAG_ERR_INVALID", 2: "SVDAG_ERR_OOM", 3: "SVDAG_ERR_TIMEOUT",
+          4: "SVDAG_ERR_CORRUPT", 5: "SVDAG_ERR_CUDA", 6: "SVDAG_ERR_NO_DEVICE", 7: "SVDAG_ERR_UNSUPPORTED",
+          8: "SVDAG_ERR_BUSY"}
+
+
+class SvdagError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        self.status = status
+        super().__init__(f"{what}: {STATUS.get(status, status)}")
+
+
+class Config(C.Structure):
+    _fields_ = [("levels", C.c_uint32), ("device", C.c_int32), ("pool_bytes", C.c_uint64),
+                ("scratch_bytes", C.c_uint64), ("target_load_factor", C.c_uint32), ("probe_lanes", C.c_uint32),
+                ("undo_depth", C.c_uint32), ("flags", C.c_uint32)]
+
+
+class TerrainParams(C.Structure):
+    _fields_ = [("seed", C.c_uint32), ("octaves", C.c_uint32), ("num_materials", C.c_uint32),
+                ("min_height_pct", C.c_uint32), ("max_height_pct", C.c_uint32),
+                ("num_structures", C.c_uint32), ("structure_seed", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class Edit(C.Structure):
+    _fields_ = [("tool", C.c_uint32), ("material", C.c_uint32), ("center", C.c_float * 3),
+                ("radius", C.c_float), ("src", C.c_float * 3), ("dst", C.c_float * 3),
+                ("noise_seed", C.c_uint32), ("noise_cell_log2", C.c_uint32)]
+
+
+class EditStats(C.Structure):
+    _fields_ = [("svo_nodes", C.c_uint64 * MAX_LEVELS), ("old_items_read", C.c_uint64),
+                ("unique_items", C.c_uint64), ("new_items", C.c_uint64), ("edited_voxels", C.c_uint64),
+                ("root_before", C.c_uint32), ("root_after", C.c_uint32), ("status", C.c_uint32),
+                ("reserved", C.c_uint32)]
+
+
+class TraceParams(C.Structure):
+    _fields_ = [("camera", C.c_double * 3), ("ray_min", C.c_double * 3), ("ray_ddx", C.c_double * 3),
+                ("ray_ddy", C.c_double * 3), ("width", C.c_uint32), ("height", C.c_uint32)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("levels", C.c_uint32), ("root", C.c_uint32), ("pool_bytes", C.c_uint64),
+                ("item_region_bytes", C.c_uint64), ("item_region_used_bytes", C.c_uint64),
+                ("scratch_bytes", C.c_uint64), ("scratch_high_water_bytes", C.c_uint64),
+                ("level_items", C.c_uint64 * MAX_LEVELS), ("level_buckets", C.c_uint64 * MAX_LEVELS),
+                ("undo_count", C.c_uint32), ("redo_count", C.c_uint32)]
+
+
+class TableStats(C.Structure):
+    _fields_ = [("items", C.c_uint64), ("buckets", C.c_uint64), ("overflow_slabs", C.c_uint64),
+                ("bytes", C.c_uint64)]
+
+
+# Tracer::SurfaceInteraction (tracer.h:95-110), 68 bytes.
+HIT_DTYPE = np.dtype([("path", "<u4", (3,)), ("material", "u1"), ("pad", "u1", (3,)),
+                      ("position", "<f4", (3,)), ("normal", "<f4", (3,)), ("dpdu", "<f4", (3,)),
+                      ("dpdv", "<f4", (3,)), ("color", "<u4")])
+assert HIT_DTYPE.itemsize == 68
+
+_P = C.c_void_p
+_U32, _U64 = C.c_uint32, C.c_uint64
+_PROTOS = {
+    "svdag_create": [C.POINTER(Config), C.POINTER(_P)],
+    "svdag_destroy": [_P],
+    "svdag_sync": [_P, _P],
+    "svdag_status_string": [C.c_int],
+    "svdag_abi_version": [],
+    "svdag_build_terrain": [_P, C.POINTER(TerrainParams), _P],
+    "svdag_edit_apply": [_P, C.POINTER(Edit), _P],
+    "svdag_edit_apply_many": [_P, C.POINTER(Edit), _U32, _P],
+    "svdag_last_edit_stats": [_P, C.POINTER(EditStats), _P],
+    "svdag_edit_sphere": [_P, C.c_float, C.c_float, C.c_float, C.c_float, _U32, C.c_int, _P],
+    "svdag_edit_box": [_P, C.c_float, C.c_float, C.c_float, C.c_float, _U32, C.c_int, _P],
+    "svdag_edit_paint": [_P, C.c_float, C.c_float, C.c_float, C.c_float, _U32, _P],
+    "svdag_edit_paint_noise": [_P, C.c_float, C.c_float, C.c_float, C.c_float, _U32, _U32, _P],
+    "svdag_edit_copy": [_P, _P, _P, _P, C.c_float, _P],
+    "svdag_undo": [_P, _P],
+    "svdag_redo": [_P, _P],
+    "svdag_gc": [_P, _P],
+    "svdag_get_root": [_P, C.POINTER(_U32), _P],
+    "svdag_trace_primary": [_P, C.POINTER(TraceParams), _P, _P],
+    "svdag_sample_voxels": [_P, _P, _U32, _P, _P],
+    "svdag_level_table": [_P, _U32, C.POINTER(_P)],
+    "svdag_table_create": [_P, _U32, _P, C.POINTER(_P)],
+    "svdag_table_destroy": [_P],
+    "svdag_table_add": [_P, _P, _P, _U32, _U64, _P, _U32, _P],
+    "svdag_table_find": [_P, _P, _P, _U32, _U64, _P, _U32, _P],
+    "svdag_table_find_or_add": [_P, _P, _P, _U32, _U64, _P, _U32, _P],
+    "svdag_table_read": [_P, _P, _U32, _P, _P],
+    "svdag_table_get_stats": [_P, C.POINTER(TableStats), _P],
+    "svdag_get_stats": [_P, C.POINTER(Stats), _P],
+    "svdag_export_level": [_P, _U32, _P, _P, _U64, C.POINTER(_U64), _P],
+}
+EXPORTED = tuple(_PROTOS)
+
+_lib = None
+
+
+def lib():
+    """Loads the in-tree libsvdag.so (never a CPU substitute)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with gpu-svdag-editing_b200/build.py")
+        L = C.CDLL(LIB_PATH)
+        for name, args in _PROTOS.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = C.c_int
+        L.svdag_status_string.restype = C.c_char_p
+        L.svdag_abi_version.restype = C.c_uint32
+        _lib = L
+    return _lib
+
+
+def _check(status: int, what: str):
+    if status != 0:
+        raise SvdagError(status, what)
+
+
+def ptr(x) -> int:
+    """Device or host pointer of a torch tensor / numpy array / int."""
+    if x is None:
+        return 0
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    if isinstance(x, np.ndarray):
+        return x.ctypes.data
+    raise TypeError(type(x))
+
+
+def stream_ptr(stream) -> int:
+    if stream is None:
+        return 0
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+# ------------------------------------------------------------------ tools (my_gpu_dag_editors.h)
+
+@dataclass
+class MyGpuSphereEditor:
+    """MyGpuSphereEditor<isAdding> (my_gpu_dag_editors.h:457-496)."""
+    center: tuple
+    radius: float
+    material: int
+    is_adding: bool = True
+
+    def to_edit(self) -> Edit:
+        e = Edit(tool=TOOL_SPHERE_ADD if self.is_adding else TOOL_SPHERE_REMOVE, material=self.material)
+        e.center[:] = [float(v) for v in self.center]
+        e.radius = float(self.radius)
+        return e
+
+
+@dataclass
+class MyGpuBoxEditor:
+    """MyGpuBoxEditor<isAdding> (my_gpu_dag_editors.h:82-119); radius = half extent."""
+    center: tuple
+    radius: float
+    material: int
+    is_adding: bool = True
+
+    def to_edit(self) -> Edit:
+        e = Edit(tool=TOOL_BOX_ADD if self.is_adding else TOOL_BOX_REMOVE, material=self.material)
+        e.center[:] = [float(v) for v in self.center]
+        e.radius = float(self.radius)
+        return e
+
+
+@dataclass
+class MyGpuSpherePaintEditor:
+    """MyGpuSpherePaintEditor (my_gpu_dag_editors.h:498-536); the paint colour only shades."""
+    center: tuple
+    radius: float
+    paint_color: tuple
+    material: int
+
+    def to_edit(self) -> Edit:
+        e = Edit(tool=TOOL_SPHERE_PAINT, material=self.material)
+        e.center[:] = [float(v) for v in self.center]
+        e.radius = float(self.radius)
+        return e
+
+
+@dataclass
+class MyGpuCopyEditor:
+    """MyGpuCopyEditor (my_gpu_dag_editors.h:129-253): pastes the box of half extent `radius` around
+    `center` from `source` to `dest` (voxels that are empty in the source keep their old value)."""
+    source: tuple
+    dest: tuple
+    center: tuple
+    radius: float
+    move: bool = False
+
+    def to_edit(self) -> Edit:
+        e = Edit(tool=TOOL_MOVE if self.move else TOOL_COPY, material=0)
+        e.src[:] = [float(v) for v in self.source]
+        e.dst[:] = [float(v) for v in self.dest]
+        e.center[:] = [float(v) for v in self.center]
+        e.radius = float(self.radius)
+        return e
+
+
+@dataclass
+class MyGpuBoxNoisePaintEditor:
+    """Box paint whose material comes from 3D value noise (lattice cell 2^cell_log2 voxels)."""
+    center: tuple
+    radius: float
+    seed: int = 0
+    cell_log2: int = 5
+
+    def to_edit(self) -> Edit:
+        e = Edit(tool=TOOL_BOX_PAINT_NOISE, material=0, noise_seed=self.seed, noise_cell_log2=self.cell_log2)
+        e.center[:] = [float(v) for v in self.center]
+        e.radius = float(self.radius)
+        return e
+
+
+# ------------------------------------------------------------------ DAG context
+
+class MyGPUHashDAG:
+    """One context: one HBM pool, one slab hash table per level, the root and the undo history."""
+
+    def __init__(self, levels: int, pool_bytes: int = 1 << 30, scratch_bytes: int = 0, device: int = 0,
+                 load_factor: int = 0, probe_lanes: int = 0, undo_depth: int = 0):
+        cfg = Config(levels=levels, device=device, pool_bytes=pool_bytes, scratch_bytes=scratch_bytes,
+                     target_load_factor=load_factor, probe_lanes=probe_lanes, undo_depth=undo_depth, flags=0)
+        h = C.c_void_p()
+        _check(lib().svdag_create(C.byref(cfg), C.byref(h)), "svdag_create")
+        self.h = h
+        self.levels = levels
+
+    def free(self):
+        if getattr(self, "h", None):
+            lib().svdag_destroy(self.h)
+            self.h = None
+
+    __del__ = free
+
+    def leaf_level(self) -> int:
+        return self.levels - 2
+
+    def sync(self, stream=None):
+        _check(lib().svdag_sync(self.h, stream_ptr(stream)), "svdag_sync")
+
+    def build_terrain(self, seed=0, octaves=5, num_materials=8, min_height_pct=40, max_height_pct=70, stream=None):
+        p = TerrainParams(seed=seed, octaves=octaves, num_materials=num_materials, min_height_pct=min_height_pct,
+                          max_height_pct=max_height_pct)
+        _check(lib().svdag_build_terrain(self.h, C.byref(p), stream_ptr(stream)), "svdag_build_terrain")
+
+    def edit(self, editor, stream=None):
+        e = editor if isinstance(editor, Edit) else editor.to_edit()
+        _check(lib().svdag_edit_apply(self.h, C.byref(e), stream_ptr(stream)), "svdag_edit_apply")
+
+    def last_edit_stats(self, stream=None) -> EditStats:
+        st = EditStats()
+        _check(lib().svdag_last_edit_stats(self.h, C.byref(st), stream_ptr(stream)), "svdag_last_edit_stats")
+        return st
+
+    def get_first_node_index(self, stream=None) -> int:
+        r = C.c_uint32()
+        _check(lib().svdag_get_root(self.h, C.byref(r), stream_ptr(stream)), "svdag_get_root")
+        return r.value
+
+    def undo(self, stream=None):
+        _check(lib().svdag_undo(self.h, stream_ptr(stream)), "svdag_undo")
+
+    def redo(self, stream=None):
+        _check(lib().svdag_redo(self.h, stream_ptr(stream)), "svdag_redo")
+
+    def garbage_collect(self, stream=None):
+        _check(lib().svdag_gc(self.h, stream_ptr(stream)), "svdag_gc")
+
+    def stats(self, stream=None) -> Stats:
+        s = Stats()
+        _check(lib().svdag_get_stats(self.h, C.byref(s), stream_ptr(stream)), "svdag_get_stats")
+        return s
+
+    def table(self, level: int) -> "HashTable":
+        t = C.c_void_p()
+        _check(lib().svdag_level_table(self.h, level, C.byref(t)), "svdag_level_table")
+        return HashTable(self, t, KIND_LEAF if level == self.leaf_level() else KIND_NODE, owned=False)
+
+    def create_table(self, kind: int, buckets_per_size) -> "HashTable":
+        b = np.ascontiguousarray(buckets_per_size, dtype=np.uint32)
+        assert b.size == NUM_SIZE_CLASSES
+        t = C.c_void_p()
+        _check(lib().svdag_table_create(self.h, kind, b.ctypes.data, C.byref(t)), "svdag_table_create")
+        return HashTable(self, t, kind, owned=True)
+
+    def trace(self, params: TraceParams, out, stream=None):
+        """Writes width*height hit records into the device buffer `out` (68 bytes each)."""
+        _check(lib().svdag_trace_primary(self.h, C.byref(params), ptr(out), stream_ptr(stream)), "svdag_trace_primary")
+
+    def sample_voxels(self, xyz_dev, count: int, out_dev, stream=None):
+        _check(lib().svdag_sample_voxels(self.h, ptr(xyz_dev), count, ptr(out_dev), stream_ptr(stream)),
+               "svdag_sample_voxels")
+
+    def export_level(self, level: int):
+        """(handles uint32[n], words uint32[n, 10]) of every item in the level table."""
+        n = C.c_uint64()
+        _check(lib().svdag_export_level(self.h, level, None, None, 0, C.byref(n), None), "svdag_export_level")
+        cap = n.value
+        handles = np.zeros(cap, dtype=np.uint32)
+        words = np.zeros((cap, MAX_ITEM_WORDS), dtype=np.uint32)
+        if cap:
+            _check(lib().svdag_export_level(self.h, level, handles.ctypes.data, words.ctypes.data, cap, C.byref(n),
+                                            None), "svdag_export_level")
+        return handles[: n.value], words[: n.value]
+
+
+class HashTable:
+    """Batched find/add over one slab hash table (MyGPUHashDAG::find_/add_{node,leaf}_as_warp)."""
+
+    def __init__(self, dag: MyGPUHashDAG, handle, kind: int, owned: bool):
+        self.dag, self.h, self.kind, self.owned = dag, handle, kind, owned
+
+    def _op(self, fn, keys, offsets, count, total_words, out, lanes, stream):
+        _check(fn(self.h, ptr(keys), ptr(offsets), count, total_words, ptr(out), lanes, stream_ptr(stream)), fn.__name__)
+
+    def add(self, keys, offsets, count, total_words, out, lanes=0, stream=None):
+        self._op(lib().svdag_table_add, keys, offsets, count, total_words, out, lanes, stream)
+
+    def find(self, keys, offsets, count, total_words, out, lanes=0, stream=None):
+        self._op(lib().svdag_table_find, keys, offsets, count, total_words, out, lanes, stream)
+
+    def find_or_add(self, keys, offsets, count, total_words, out, lanes=0, stream=None):
+        self._op(lib().svdag_table_find_or_add, keys, offsets, count, total_words, out, lanes, stream)
+
+    def read(self, handles, count, out_words, stream=None):
+        _check(lib().svdag_table_read(self.h, ptr(handles), count, ptr(out_words), stream_ptr(stream)),
+               "svdag_table_read")
+
+    def stats(self, stream=None) -> TableStats:
+        s = TableStats()
+        _check(lib().svdag_table_get_stats(self.h, C.byref(s), stream_ptr(stream)), "svdag_table_get_stats")
+        return s
+
+    def destroy(self):
+        if self.owned and self.h:
+            lib().svdag_table_destroy(self.h)
+            self.h = None
+
+
+class MyGPUHashDAGUndoRedo:
+    """MyGPUHashDAGUndoRedo (my_gpu_base_dag.h:16-82); the history itself lives on the device."""
+
+    def undo(self, dag: MyGPUHashDAG, stream=None):
+        dag.undo(stream)
+
+    def redo(self, dag: MyGPUHashDAG, stream=None):
+        dag.redo(stream)
+
+    def garbageCollect(self, dag: MyGPUHashDAG, stream=None):
+        dag.garbage_collect(stream)
+
+
+def editMyHashDag(editor, dag: MyGPUHashDAG, undoRedo: MyGPUHashDAGUndoRedo | None = None, stream=None):
+    """editMyHashDag<Editor> (my_gpu_hash_dag_edits.h:12-13): applies one tool; the undo frame is
+    recorded on the device, so `undoRedo` is accepted only for signature compatibility."""
+    dag.edit(editor, stream)
+
+
+# ------------------------------------------------------------------ camera (dag_tracer.cu:59-101)
+
+def get_trace_params(position, target, width: int, height: int, fov_degrees: float = 60.0,
+                     levels: int | None = None, bounds_min=(0.0, 0.0, 0.0), bounds_max=None) -> TraceParams:
+    """Ray basis of a look-at camera in double precision. With bounds given, world coordinates are
+    scaled to the [0, 2^levels) voxel grid as get_trace_params does; by default they already are voxels."""
+    pos = np.asarray(position, dtype=np.float64)
+    f = np.asarray(target, dtype=np.float64) - pos
+    f = f / math.sqrt(float(np.dot(f, f)))
+    wu = np.array([0.0, 0.0, 1.0]) if abs(f[1]) > 0.999 else np.array([0.0, 1.0, 0.0])
+    r = np.cross(f, wu)
+    r = r / math.sqrt(float(np.dot(r, r)))
+    u = np.cross(r, f)
+    fov = fov_degrees / 2.0 * (math.pi / 180.0)
+    aspect = float(width) / float(height)
+    X = r * math.sin(fov) * aspect
+    Y = u * math.sin(fov)
+    Z = f * math.cos(fov)
+    bl, br, tl = pos + Z - Y - X, pos + Z - Y + X, pos + Z + Y - X
+    if bounds_max is not None:
+        bmin, bmax = np.asarray(bounds_min, dtype=np.float64), np.asarray(bounds_max, dtype=np.float64)
+        scale = float(1 << levels) / (bmax - bmin)
+        pos, bl, br, tl = [(v - bmin) * scale for v in (pos, bl, br, tl)]
+    p = TraceParams()
+    p.camera[:] = list(pos)
+    p.ray_min[:] = list(bl)
+    p.ray_ddx[:] = list((br - bl) * (1.0 / width))
+    p.ray_ddy[:] = list((tl - bl) * (1.0 / height))
+    p.width, p.height = width, height
+    return p
+
+
+class DAGTracer:
+    """DAGTracer (dag_tracer.h): owns the per-pixel hit buffer (a device tensor of 68-byte records)."""
+
+    def __init__(self, width: int, height: int, device: str = "cuda"):
+        import torch
+        self.width, self.height = width, height
+        self.hits = torch.empty(width * height * HIT_DTYPE.itemsize, dtype=torch.uint8, device=device)
+
+    def resolve_paths(self, params: TraceParams, dag: MyGPUHashDAG, stream=None):
+        assert params.width == self.width and params.height == self.height
+        dag.trace(params, self.hits, stream)
+
+    def hits_numpy(self) -> np.ndarray:
+        return self.hits.cpu().numpy().view(HIT_DTYPE)

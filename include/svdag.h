@@ -1,0 +1,273 @@
+/*
+ * svdag.h - C ABI of libsvdag, a B200-native (sm_100a) SVDAG editing back-end and DAG ray tracer.
+ *
+ * The entry points replace the C++ template interface of the reference's EDag::MyGpuDag path
+ * (mathijs727/GPU-SVDAG-Editing). Each declaration names the reference interface it stands in for.
+ *
+ * Conventions
+ *  - Every function returns an svdag_status (0 = SVDAG_OK) and never aborts the process.
+ *  - Device pointers are marked *_dev; everything else is host memory owned by the caller.
+ *  - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *  - Calls on one context are not thread-safe; the serving loop (svdag_serve_*) is the
+ *    thread-safe way to feed a context from several producers.
+ *  - Asynchronous failures (device-side capacity or iteration-limit errors) are latched in a
+ *    device status word; svdag_sync() and every call that synchronises report them.
+ */
+#ifndef SVDAG_H
+#define SVDAG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SVDAG_ABI_VERSION 1u
+
+typedef enum svdag_status {
+    SVDAG_OK = 0,
+    SVDAG_ERR_INVALID = 1, /* bad argument */
+    SVDAG_ERR_OOM = 2, /* pool, slab region or scratch arena exhausted */
+    SVDAG_ERR_TIMEOUT = 3, /* a bounded device-side wait or retry loop gave up */
+    SVDAG_ERR_CORRUPT = 4, /* structural invariant violated (bad handle, bad size) */
+    SVDAG_ERR_CUDA = 5, /* CUDA runtime error */
+    SVDAG_ERR_NO_DEVICE = 6, /* no usable sm_100 device */
+    SVDAG_ERR_UNSUPPORTED = 7,
+    SVDAG_ERR_BUSY = 8 /* serving queue full / admission refused */
+} svdag_status;
+
+/* Item handles are 32-bit word offsets of the item inside the context's item region. */
+#define SVDAG_INVALID_HANDLE 0xFFFFFFFFu
+/* Voxel sampling and hit records use this value for "no voxel". */
+#define SVDAG_NO_MATERIAL 0xFFFFFFFFu
+
+#define SVDAG_MAX_LEVELS 17u /* total octree depth (reference MAX_LEVELS) */
+#define SVDAG_MIN_LEVELS 4u
+#define SVDAG_MATERIAL_BITS 4u /* reference HASH_DAG_MATERIAL_BITS */
+#define SVDAG_NUM_MATERIALS 16u
+#define SVDAG_MIN_ITEM_WORDS 2u /* node: header + 1 child */
+#define SVDAG_MAX_ITEM_WORDS 10u /* leaf: 2 mask words + 8 material words */
+#define SVDAG_NUM_SIZE_CLASSES 9u /* item sizes 2..10 words */
+
+/* Table kinds: a node key's length is 1 + popcount(child mask); a leaf key's length is
+ * 2 + ceil(4 * popcount(64-bit voxel mask) / 32). Keys are self-describing. */
+typedef enum svdag_item_kind { SVDAG_KIND_NODE = 0, SVDAG_KIND_LEAF = 1 } svdag_item_kind;
+
+typedef struct svdag_config {
+    uint32_t levels; /* octree depth, SVDAG_MIN_LEVELS..SVDAG_MAX_LEVELS (1 << levels voxels per axis) */
+    int32_t device; /* CUDA device ordinal */
+    uint64_t pool_bytes; /* the single preallocated HBM pool (item region + scratch arena) */
+    uint64_t scratch_bytes; /* part of the pool reserved for per-edit temporaries */
+    uint32_t target_load_factor; /* items per bucket when a level table is sized; 0 = default (16) */
+    uint32_t probe_lanes; /* lanes cooperating on one key: 1, 4, 8, 16 or 32; 0 = autotuned default */
+    uint32_t undo_depth; /* undo history ring size; 0 = default (32) */
+    uint32_t flags; /* reserved, must be 0 */
+} svdag_config;
+
+typedef struct svdag_ctx svdag_ctx;
+typedef struct svdag_table svdag_table;
+
+/* ---------------------------------------------------------------- context */
+
+/* Replaces MyGPUHashDAG<GPU_Malloc>::allocate (my_gpu_hash_dag.cu:24-66): one HBM pool, one table
+ * per level, the canonical fully-filled node of every (level, material) inserted up front. */
+svdag_status svdag_create(const svdag_config* config, svdag_ctx** out_ctx);
+/* Replaces MyGPUHashDAG::free (my_gpu_hash_dag.cu:68-76). */
+svdag_status svdag_destroy(svdag_ctx* ctx);
+/* Waits for all work of the context on `stream` and returns the latched device status (then clears it). */
+svdag_status svdag_sync(svdag_ctx* ctx, void* stream);
+const char* svdag_status_string(svdag_status status);
+uint32_t svdag_abi_version(void);
+
+/* ---------------------------------------------------------------- scene construction */
+
+typedef struct svdag_terrain_params {
+    uint32_t seed; /* lattice hash seed */
+    uint32_t octaves; /* fBm octaves */
+    uint32_t num_materials; /* height bands -> materials [0, num_materials) (8 or 16) */
+    uint32_t min_height_pct; /* surface height range, in percent of the grid height */
+    uint32_t max_height_pct;
+    uint32_t num_structures; /* random boxes/spheres unioned on the surface (0 = none) */
+    uint32_t structure_seed;
+    uint32_t reserved;
+} svdag_terrain_params;
+
+/* Builds a procedural heightfield terrain into an empty context; stands in for the reference's
+ * scene load MyGPUHashDAGFactory::load_from_DAG (my_gpu_hash_dag_factory.cpp:427-500). Every
+ * uniformly filled node carries the fully-filled header bits, as the factory's create_dag_cpu does. */
+svdag_status svdag_build_terrain(svdag_ctx* ctx, const svdag_terrain_params* params, void* stream);
+
+/* ---------------------------------------------------------------- edits */
+
+typedef enum svdag_tool {
+    SVDAG_TOOL_SPHERE_ADD = 0, /* MyGpuSphereEditor<true>   (my_gpu_dag_editors.h:457-496) */
+    SVDAG_TOOL_SPHERE_REMOVE = 1, /* MyGpuSphereEditor<false> */
+    SVDAG_TOOL_BOX_ADD = 2, /* MyGpuBoxEditor<true>      (my_gpu_dag_editors.h:82-119) */
+    SVDAG_TOOL_BOX_REMOVE = 3, /* MyGpuBoxEditor<false> */
+    SVDAG_TOOL_SPHERE_PAINT = 4, /* MyGpuSpherePaintEditor    (my_gpu_dag_editors.h:498-536) */
+    SVDAG_TOOL_COPY = 5, /* MyGpuCopyEditor           (my_gpu_dag_editors.h:129-253) */
+    SVDAG_TOOL_BOX_PAINT_NOISE = 6, /* box paint with a per-voxel material from 3D value noise */
+    SVDAG_TOOL_MOVE = 7, /* copy followed by removal of the source box */
+    SVDAG_NUM_TOOLS = 8
+} svdag_tool;
+
+typedef struct svdag_edit {
+    uint32_t tool; /* svdag_tool */
+    uint32_t material; /* fill / paint material, < SVDAG_NUM_MATERIALS */
+    float center[3]; /* voxel coordinates; sphere centre or box centre */
+    float radius; /* sphere radius, or box half extent */
+    float src[3]; /* copy/move: source anchor */
+    float dst[3]; /* copy/move: destination anchor */
+    uint32_t noise_seed; /* BOX_PAINT_NOISE: lattice seed */
+    uint32_t noise_cell_log2; /* BOX_PAINT_NOISE: lattice cell size = 1 << noise_cell_log2 voxels */
+} svdag_edit;
+
+/* Per-edit counters (exact, from the device) used for the algorithmic-byte roofline. */
+typedef struct svdag_edit_stats {
+    uint64_t svo_nodes[SVDAG_MAX_LEVELS]; /* intermediate SVO items per level (leaf level = leaves) */
+    uint64_t old_items_read; /* existing DAG nodes read by the top-down pass */
+    uint64_t unique_items; /* items left after intra-SVO dedup */
+    uint64_t new_items; /* items inserted into the DAG tables */
+    uint64_t edited_voxels; /* voxels whose operation is not Keep (Fill/Empty regions count fully) */
+    uint32_t root_before;
+    uint32_t root_after;
+    uint32_t status;
+    uint32_t reserved;
+} svdag_edit_stats;
+
+/* Replaces editMyHashDag<Editor>(editor, dag, undoRedo, stats, memPool, stream)
+ * (my_gpu_hash_dag_edits.h:12-13, body my_gpu_hash_dag_edits.cu:633-671). Asynchronous on
+ * `stream`; the root handle, undo history and counters stay on the device. */
+svdag_status svdag_edit_apply(svdag_ctx* ctx, const svdag_edit* edit, void* stream);
+/* Applies edits one after another with one launch sequence per edit level phase. */
+svdag_status svdag_edit_apply_many(svdag_ctx* ctx, const svdag_edit* edits, uint32_t count, void* stream);
+/* Copies the counters of the most recent edit to the host (synchronises `stream`). */
+svdag_status svdag_last_edit_stats(svdag_ctx* ctx, svdag_edit_stats* out, void* stream);
+
+/* Convenience forms mirroring the reference tool constructors. */
+svdag_status svdag_edit_sphere(svdag_ctx* ctx, float cx, float cy, float cz, float radius,
+    uint32_t material, int add, void* stream);
+svdag_status svdag_edit_box(svdag_ctx* ctx, float cx, float cy, float cz, float half_extent,
+    uint32_t material, int add, void* stream);
+svdag_status svdag_edit_paint(svdag_ctx* ctx, float cx, float cy, float cz, float radius,
+    uint32_t material, void* stream);
+svdag_status svdag_edit_paint_noise(svdag_ctx* ctx, float cx, float cy, float cz, float half_extent,
+    uint32_t seed, uint32_t cell_log2, void* stream);
+svdag_status svdag_edit_copy(svdag_ctx* ctx, const float src[3], const float dst[3],
+    const float center[3], float radius, void* stream);
+
+/* MyGPUHashDAGUndoRedo::undo / redo (my_gpu_base_dag.h:35-64): swap the root with the history. */
+svdag_status svdag_undo(svdag_ctx* ctx, void* stream);
+svdag_status svdag_redo(svdag_ctx* ctx, void* stream);
+/* MyGPUHashDAGUndoRedo::garbageCollect (my_gpu_base_dag.h:66-77) -> MyGPUHashDAG::garbageCollect
+ * (my_gpu_hash_dag.cu:365-475): clears the history, marks everything reachable from the root and
+ * the canonical fully-filled nodes, frees the rest. Synchronous. */
+svdag_status svdag_gc(svdag_ctx* ctx, void* stream);
+/* MyGPUHashDAG::get_first_node_index (my_gpu_hash_dag.h:290-293); synchronises `stream`. */
+svdag_status svdag_get_root(svdag_ctx* ctx, uint32_t* out_root, void* stream);
+
+/* ---------------------------------------------------------------- tracing and sampling */
+
+/* Tracer::TracePathsParams (tracer.h:112-121) as produced by get_trace_params (dag_tracer.cu:59-101),
+ * already in voxel coordinates of the [0, 2^levels)^3 grid. */
+typedef struct svdag_trace_params {
+    double camera[3];
+    double ray_min[3];
+    double ray_ddx[3];
+    double ray_ddy[3];
+    uint32_t width;
+    uint32_t height;
+} svdag_trace_params;
+
+/* Layout-compatible with Tracer::SurfaceInteraction (tracer.h:95-110): 68 bytes. A miss has
+ * path (0,0,0); material 0xFF means "no material". */
+typedef struct svdag_hit {
+    uint32_t path[3];
+    uint8_t material;
+    uint8_t pad[3];
+    float position[3];
+    float normal[3];
+    float dpdu[3];
+    float dpdv[3];
+    uint32_t color;
+} svdag_hit;
+
+/* Replaces DAGTracer::resolve_paths -> Tracer::trace_paths<MyGPUHashDAG> (dag_tracer.cu:112-134,
+ * tracer.cu:391-411). Writes width*height hit records, row (height-1-y) for pixel row y. */
+svdag_status svdag_trace_primary(svdag_ctx* ctx, const svdag_trace_params* params,
+    svdag_hit* out_dev, void* stream);
+
+/* Replaces DAGTracer::get_voxel_values -> getVoxelValues_kernel (dag_tracer.cu:361-390): material of
+ * each voxel (x,y,z triplets) or SVDAG_NO_MATERIAL. */
+svdag_status svdag_sample_voxels(svdag_ctx* ctx, const uint32_t* xyz_dev, uint32_t count,
+    uint32_t* out_dev, void* stream);
+
+/* ---------------------------------------------------------------- hash tables */
+
+/* The table of one DAG level (level leaf_level = levels-2 holds leaves). The handle stays owned by
+ * the context. Mirrors MyGPUHashDAG::find_/add_{node,leaf}[_as_warp] (my_gpu_hash_dag.h:168-283). */
+svdag_status svdag_level_table(svdag_ctx* ctx, uint32_t level, svdag_table** out_table);
+/* A standalone table (microbenchmarks, tests): buckets_per_size[i] = bucket count for keys of
+ * 2+i words (0 = no keys of that size). Replaces CompactAccelerationHashTable::allocate
+ * (compact_acceleration_hash_table.cu:10). */
+svdag_status svdag_table_create(svdag_ctx* ctx, uint32_t kind, const uint32_t* buckets_per_size,
+    svdag_table** out_table);
+svdag_status svdag_table_destroy(svdag_table* table);
+
+/* Batched add (CompactAccelerationHashTable::add / addAsWarp, compact_acceleration_hash_table.h:27-121):
+ * every key is stored in a fresh slot, duplicates included, as the reference does. keys_dev holds
+ * the packed key words; offsets_dev[i] is the word offset of key i; total_words bounds the reads.
+ * lanes = lanes cooperating on one key (1 = thread per key, 8, 32 = warp per key; 0 = default). */
+svdag_status svdag_table_add(svdag_table* table, const uint32_t* keys_dev, const uint32_t* offsets_dev,
+    uint32_t count, uint64_t total_words, uint32_t* handles_dev, uint32_t lanes, void* stream);
+/* Batched find (find / findAsWarp, compact_acceleration_hash_table.h:205-280): handle of a stored
+ * copy of each key, or SVDAG_INVALID_HANDLE. */
+svdag_status svdag_table_find(svdag_table* table, const uint32_t* keys_dev, const uint32_t* offsets_dev,
+    uint32_t count, uint64_t total_words, uint32_t* handles_dev, uint32_t lanes, void* stream);
+/* Find-or-add: one slot per distinct key even when a batch holds duplicates (the DAG insert path). */
+svdag_status svdag_table_find_or_add(svdag_table* table, const uint32_t* keys_dev,
+    const uint32_t* offsets_dev, uint32_t count, uint64_t total_words, uint32_t* handles_dev,
+    uint32_t lanes, void* stream);
+/* decodePointer (compact_acceleration_hash_table.h:398-402): copies the words of each handle into
+ * out_words_dev[i * SVDAG_MAX_ITEM_WORDS ...], zero padded. */
+svdag_status svdag_table_read(svdag_table* table, const uint32_t* handles_dev, uint32_t count,
+    uint32_t* out_words_dev, void* stream);
+
+typedef struct svdag_table_stats {
+    uint64_t items; /* occupied slots */
+    uint64_t buckets; /* base slabs */
+    uint64_t overflow_slabs; /* chained slabs taken from the slab allocator */
+    uint64_t bytes; /* bytes of slab storage (base + overflow) */
+} svdag_table_stats;
+svdag_status svdag_table_get_stats(svdag_table* table, svdag_table_stats* out, void* stream);
+
+/* ---------------------------------------------------------------- inspection */
+
+typedef struct svdag_stats {
+    uint32_t levels;
+    uint32_t root;
+    uint64_t pool_bytes;
+    uint64_t item_region_bytes;
+    uint64_t item_region_used_bytes;
+    uint64_t scratch_bytes;
+    uint64_t scratch_high_water_bytes;
+    uint64_t level_items[SVDAG_MAX_LEVELS];
+    uint64_t level_buckets[SVDAG_MAX_LEVELS];
+    uint32_t undo_count;
+    uint32_t redo_count;
+} svdag_stats;
+/* MyGPUHashDAG::report (my_gpu_hash_dag.cu:217-230). Synchronises `stream`. */
+svdag_status svdag_get_stats(svdag_ctx* ctx, svdag_stats* out, void* stream);
+
+/* Dumps every occupied item of a level table: out_handles[i] and out_words[i*SVDAG_MAX_ITEM_WORDS..]
+ * (zero padded). With capacity 0 only *out_count is written. Synchronous; used for structural
+ * comparison (MyGPUHashDAG::copy<CPU>, my_gpu_hash_dag.h:106-127). */
+svdag_status svdag_export_level(svdag_ctx* ctx, uint32_t level, uint32_t* out_handles, uint32_t* out_words,
+    uint64_t capacity, uint64_t* out_count, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SVDAG_H */

@@ -1,0 +1,60 @@
+"""The C ABI library builds, loads and exports every entry point include/svdag.h declares."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "svdag.h")).read()
+    return sorted(set(re.findall(r"^\s*(?:svdag_status|const char\*|uint32_t)\s+(svdag_\w+)\s*\(", text, re.M)))
+
+
+def test_every_declared_symbol_is_exported(svdag_lib):
+    names = declared_symbols()
+    assert len(names) >= 25
+    out = subprocess.check_output(["nm", "-D", "--defined-only", svdag_lib.LIB_PATH], text=True)
+    exported = set(re.findall(r" T (svdag_\w+)", out))
+    missing = [n for n in names if n not in exported]
+    assert not missing, missing
+    assert set(names) == set(svdag_lib.EXPORTED)
+
+
+def test_library_loads_and_reports_version(svdag_lib):
+    L = svdag_lib.lib()
+    assert L.svdag_abi_version() == 1
+    assert L.svdag_status_string(2).decode().startswith("out of memory")
+
+
+def test_struct_layouts(svdag_lib):
+    s = svdag_lib
+    assert s.HIT_DTYPE.itemsize == 68  # Tracer::SurfaceInteraction
+    assert C.sizeof(s.Edit) == 56
+    assert C.sizeof(s.Config) == 40
+    assert C.sizeof(s.TraceParams) == 104
+    assert C.sizeof(s.TerrainParams) == 32
+
+
+def test_invalid_arguments_are_rejected(svdag_lib):
+    L = svdag_lib.lib()
+    cfg = svdag_lib.Config(levels=3)  # below SVDAG_MIN_LEVELS
+    h = C.c_void_p()
+    assert L.svdag_create(C.byref(cfg), C.byref(h)) == 1
+    cfg = svdag_lib.Config(levels=10, probe_lanes=3)
+    assert L.svdag_create(C.byref(cfg), C.byref(h)) == 1
+    assert L.svdag_destroy(None) == 1
+    assert L.svdag_edit_apply(None, None, None) == 1
+
+
+def test_no_cpu_fallback_without_device(svdag_lib):
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(svdag_lib.SvdagError) as e:
+        svdag_lib.MyGPUHashDAG(10)
+    assert e.value.status == 6  # SVDAG_ERR_NO_DEVICE
