@@ -16,9 +16,7 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
-import tempfile
 import time
 
 import numpy as np
@@ -66,53 +64,72 @@ def c0_edits(n, seed=EDIT_SEED):
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+    """SM clock and clock-event reasons polled through NVML every 5 ms during the timed region
+    (the per-edit steps are far shorter than nvidia-smi's 200 ms sampling period)."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "sw_power_cap": 0x4, "hw_power_brake_slowdown": 0x80}
 
-    def __init__(self, device_index: int):
-        self.dev = device_index
-        self.path = tempfile.mktemp(suffix=".csv")
-        self.proc = None
+    def __init__(self, cuda_device: int):
+        self.cuda_device = cuda_device
+        self.samples = []
+        self.max_mhz = None
+        self.handle = None
+        self._stop = None
+
+    def _open(self):
+        import pynvml
+
+        pynvml.nvmlInit()
+        try:
+            import torch
+
+            pr = torch.cuda.get_device_properties(self.cuda_device)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0".upper()
+            self.handle = pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
+        except Exception:
+            self.handle = pynvml.nvmlDeviceGetHandleByIndex(0)
+        self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM)
+        return pynvml
 
     def __enter__(self):
+        import threading
+
         try:
-            self.f = open(self.path, "w")
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
-                                         stderr=subprocess.DEVNULL)
+            nv = self._open()
         except Exception:
-            self.proc = None
+            return self
+        self._stop = threading.Event()
+
+        def loop():
+            while not self._stop.is_set():
+                try:
+                    mhz = nv.nvmlDeviceGetClockInfo(self.handle, nv.NVML_CLOCK_SM)
+                    try:
+                        rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.handle)
+                    except Exception:
+                        rs = nv.nvmlDeviceGetCurrentClocksThrottleReasons(self.handle)
+                    self.samples.append((mhz, rs))
+                except Exception:
+                    pass
+                self._stop.wait(0.005)
+
+        self.thread = threading.Thread(target=loop, daemon=True)
+        self.thread.start()
         return self
 
     def __exit__(self, *a):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except Exception:
-                self.proc.kill()
-            self.f.close()
+        if self._stop is not None:
+            self._stop.set()
+            self.thread.join(timeout=2)
 
     def summary(self):
-        try:
-            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
-        except Exception:
-            rows = []
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = set()
-        for r in rows:
-            for i, n in enumerate(names):
-                if len(r) > 5 + i and r[5 + i].strip().lower() == "active":
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(rows)}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"], "samples": 0}
+        mhz = [m for m, _ in self.samples]
+        reasons = sorted({n for _, r in self.samples for n, bit in self.REASONS.items() if r & bit})
+        return {"sm_mhz": statistics.median(mhz), "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                "samples": len(self.samples), "source": "nvml, 5 ms"}
 
 
 # ------------------------------------------------------------------ C1 hash microbenchmark
@@ -142,7 +159,7 @@ def gather_keys(words, offs, sizes, order):
     return words[idx], o.astype(np.uint32), s
 
 
-def run_hash_bench(svdag, torch, stream, n_total=1 << 24, load_factor=20, lanes=8, reps=3):
+def run_hash_bench(svdag, torch, stream, n_total=1 << 24, load_factor=20, lanes=8, reps=3, pool=6 << 30):
     """Insert 2^24 keys (50% duplicates, stored twice as the reference's add does), then 2^24 finds
     (50% hits). Algorithmic bytes (per key of k words): find 4k + 32 + 4k*hit + 4, insert 4k + 32 + 4k + 4."""
     n_unique = n_total // 2
@@ -168,10 +185,9 @@ def run_hash_bench(svdag, torch, stream, n_total=1 << 24, load_factor=20, lanes=
     buckets = np.maximum(1, cls_items // load_factor + 1).astype(np.uint32)
     ins_bytes = float(np.sum(4 * isz + 32 + 4 * isz + 4))
     find_bytes = float(np.sum(4 * fsz + 32 + 4 * fsz * is_hit + 4))
-    pool = 6 << 30
     res = {"insert_ms": [], "find_ms": []}
     for r in range(reps):
-        dag = svdag.MyGPUHashDAG(10, pool_bytes=pool, scratch_bytes=1 << 30)
+        dag = svdag.MyGPUHashDAG(10, pool_bytes=pool, scratch_bytes=min(1 << 30, pool // 4))
         tbl = dag.create_table(0, buckets)
         torch.cuda.synchronize()
         e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))

@@ -48,11 +48,15 @@ __global__ void k_gc_mark(DevDag d, uint32_t* bits, const uint32_t* in, const ui
 {
     const uint32_t n = *inCount;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t* node = d.items + in[i];
+        const uint32_t* node = item_ptr(d, in[i]);
         const uint32_t mask = node[0] & 0xFFu;
         const uint32_t k = __popc(mask);
         for (uint32_t j = 0; j < k; ++j) {
             const uint32_t c = node[1 + j];
+            if (!handle_ok(d, c)) {
+                set_status(d.ctl, SVDAG_ERR_CORRUPT);
+                continue;
+            }
             if (mark_once(bits, c)) {
                 const uint32_t at = atomicAdd(outCount, 1u);
                 if (at < outCap)
@@ -90,6 +94,10 @@ __global__ void k_gc_sweep(DevDag d, DevTable t, const uint32_t* bits, unsigned 
                 }
                 if (h[7] == kEnd)
                     break;
+                if (!handle_ok(d, h[7])) {
+                    set_status(d.ctl, SVDAG_ERR_CORRUPT);
+                    break;
+                }
                 slab = h[7];
             }
         }
@@ -162,7 +170,7 @@ svdag_status svdag_create(const svdag_config* cfg, svdag_ctx** out)
         return SVDAG_ERR_OOM;
     ctx->cfg = *cfg;
     ctx->device = cfg->device;
-    ctx->probeLanes = cfg->probe_lanes ? cfg->probe_lanes : 8;
+    ctx->probeLanes = cfg->probe_lanes ? cfg->probe_lanes : 1; // thread per key: measured fastest on B200
     ctx->loadFactor = cfg->target_load_factor ? cfg->target_load_factor : 16;
     ctx->cfg.undo_depth = cfg->undo_depth ? std::min<uint32_t>(cfg->undo_depth, 64) : 32;
     if (cudaMalloc(&ctx->pool, pool) != cudaSuccess) {
@@ -175,7 +183,7 @@ svdag_status svdag_create(const svdag_config* cfg, svdag_ctx** out)
     ctx->scratch = ctx->pool + kCtlBytes;
     ctx->scratchBytes = scratch;
     ctx->items = reinterpret_cast<uint32_t*>(ctx->pool + kCtlBytes + scratch);
-    ctx->itemWords = std::min<unsigned long long>((pool - kCtlBytes - scratch) / 4, kMaxHandle);
+    ctx->itemWords = std::min<unsigned long long>((pool - kCtlBytes - scratch) / 4 - 64, kMaxHandle);
     static_assert(sizeof(Control) <= kCtlBytes, "control block too large");
     cudaError_t e = cudaMemset(ctx->pool, 0, pool);
     if (e == cudaSuccess) {

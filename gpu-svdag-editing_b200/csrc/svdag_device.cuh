@@ -85,6 +85,21 @@ __device__ __forceinline__ void set_status(Control* ctl, uint32_t code)
     atomicCAS(&ctl->status, 0u, code);
 }
 
+// Every handle read from memory is checked before it is dereferenced: a bad handle (which only a
+// bug could produce) latches SVDAG_ERR_CORRUPT and reads a zero item instead of faulting.
+__device__ const uint32_t kZeroItem[16] = {};
+__device__ __forceinline__ bool handle_ok(const DevDag& d, uint32_t h)
+{
+    return (unsigned long long)h + 16ull <= d.itemWords;
+}
+__device__ __forceinline__ const uint32_t* item_ptr(const DevDag& d, uint32_t h)
+{
+    if (handle_ok(d, h))
+        return d.items + h;
+    set_status(d.ctl, SVDAG_ERR_CORRUPT);
+    return kZeroItem;
+}
+
 // ---------------------------------------------------------------- hashing (ours; the bucket
 // function of the reference is xorHash32xN, utils.h:395-403, which uses a 32-bit modulo per word)
 
@@ -343,7 +358,14 @@ __device__ __forceinline__ uint32_t link_slab(uint32_t* items, uint32_t slab, ui
     return prev == kEnd ? fresh : prev;
 }
 
-constexpr uint32_t kMaxChain = 1u << 20; // bound on chain walks (a longer walk means a corrupt chain)
+// An overflow slab allocated by a group that lost the race to link it; it may only be linked into a
+// chain of the same size class later.
+struct Spare {
+    uint32_t slab = kNone;
+    uint32_t k = 0;
+};
+
+constexpr uint32_t kMaxChain = 1u << 14; // bound on chain walks (16K slabs in one bucket only happens on a corrupt chain)
 
 // Read-only lookup (CompactAccelerationHashTable::findAsWarp, compact_acceleration_hash_table.h:233-280).
 template <int G>
@@ -370,6 +392,10 @@ __device__ __forceinline__ uint32_t table_find(const Grp<G>& g, const DevDag& d,
         }
         if (next == kEnd)
             return kNone;
+        if (!handle_ok(d, next)) {
+            set_status(d.ctl, SVDAG_ERR_CORRUPT);
+            return kNone;
+        }
         slab = next;
     }
 }
@@ -410,7 +436,7 @@ __device__ __forceinline__ uint32_t claim_in_slab(const Grp<G>& g, const DevDag&
 // Unconditional insert (CompactAccelerationHashTable::addAsWarp, compact_acceleration_hash_table.h:63-121):
 // the key gets a fresh slot even when an equal key is stored already.
 template <int G>
-__device__ __forceinline__ uint32_t table_add(const Grp<G>& g, const DevDag& d, const DevTable& t, const Key<G>& key, uint32_t& spare)
+__device__ __forceinline__ uint32_t table_add(const Grp<G>& g, const DevDag& d, const DevTable& t, const Key<G>& key, Spare& spare)
 {
     const uint32_t cls = key.n - 2u;
     if (key.n < 2u || key.n > 10u || t.numBuckets[cls] == 0) {
@@ -428,17 +454,23 @@ __device__ __forceinline__ uint32_t table_add(const Grp<G>& g, const DevDag& d, 
             return item;
         }
         if (next == kEnd) {
-            if (spare == kNone)
-                spare = alloc_slab<G>(g, d, key.n);
-            if (spare == kNone)
+            if (spare.slab == kNone || spare.k != key.n) {
+                spare.slab = alloc_slab<G>(g, d, key.n); // a spare of another class is abandoned
+                spare.k = key.n;
+            }
+            if (spare.slab == kNone)
                 return kNone;
             uint32_t linked = kNone;
             if (g.lane == 0)
-                linked = link_slab(d.items, slab, spare);
+                linked = link_slab(d.items, slab, spare.slab);
             linked = g.bcast(linked, 0);
-            if (linked == spare)
-                spare = kNone;
+            if (linked == spare.slab)
+                spare.slab = kNone;
             next = linked;
+        }
+        if (!handle_ok(d, next)) {
+            set_status(d.ctl, SVDAG_ERR_CORRUPT);
+            return kNone;
         }
         slab = next;
     }
@@ -451,7 +483,7 @@ __device__ __forceinline__ uint32_t table_add(const Grp<G>& g, const DevDag& d, 
 // final tag published, so concurrent probes of other keys never compare a half-written item.
 template <int G>
 __device__ __forceinline__ uint32_t table_find_or_insert(const Grp<G>& g, const DevDag& d, const DevTable& t, const Key<G>& key,
-    uint32_t& spare, bool& inserted)
+    Spare& spare, bool& inserted)
 {
     inserted = false;
     const uint32_t cls = key.n - 2u;
@@ -480,6 +512,10 @@ __device__ __forceinline__ uint32_t table_find_or_insert(const Grp<G>& g, const 
         tailEmpty = empty;
         if (next == kEnd)
             break;
+        if (!handle_ok(d, next)) {
+            set_status(d.ctl, SVDAG_ERR_CORRUPT);
+            return kNone;
+        }
         slab = next;
     }
     // Not present: claim a slot at the tail of the chain (earlier slabs were full or hold other keys).
@@ -503,17 +539,23 @@ __device__ __forceinline__ uint32_t table_find_or_insert(const Grp<G>& g, const 
         if (empty)
             continue; // a slot was freed up meanwhile (cannot happen during edits, kept for safety)
         if (next == kEnd) {
-            if (spare == kNone)
-                spare = alloc_slab<G>(g, d, key.n);
-            if (spare == kNone)
+            if (spare.slab == kNone || spare.k != key.n) {
+                spare.slab = alloc_slab<G>(g, d, key.n); // a spare of another class is abandoned
+                spare.k = key.n;
+            }
+            if (spare.slab == kNone)
                 return kNone;
             uint32_t linked = kNone;
             if (g.lane == 0)
-                linked = link_slab(d.items, slab, spare);
+                linked = link_slab(d.items, slab, spare.slab);
             linked = g.bcast(linked, 0);
-            if (linked == spare)
-                spare = kNone;
+            if (linked == spare.slab)
+                spare.slab = kNone;
             next = linked;
+        }
+        if (!handle_ok(d, next)) {
+            set_status(d.ctl, SVDAG_ERR_CORRUPT);
+            return kNone;
         }
         slab = next;
         probe_header<G, true>(g, d.items + slab, tag, next, empty);

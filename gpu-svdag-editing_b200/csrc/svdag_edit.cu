@@ -77,19 +77,22 @@ __device__ __forceinline__ uint32_t terrain_height_from_fbm(const DevEditor& e, 
     const long long norm = ((1ll << e.terrain.octaves) - 1) * 65536;
     return (uint32_t)(base + (range * f) / norm);
 }
+__device__ long long terrain_octave(const DevEditor& e, uint32_t x, uint32_t z, uint32_t o)
+{
+    const uint32_t c = terrain_cell_log2(e, o);
+    const uint32_t ix = x >> c, iz = z >> c, m = (1u << c) - 1u;
+    const long long fx = c <= 16 ? (long long)((x & m) << (16 - c)) : (long long)((x & m) >> (c - 16));
+    const long long fz = c <= 16 ? (long long)((z & m) << (16 - c)) : (long long)((z & m) >> (c - 16));
+    const long long sx = smooth16(fx), sz = smooth16(fz);
+    const long long a = lerp16(terrain_lattice(e, ix, iz, o), terrain_lattice(e, ix + 1, iz, o), sx);
+    const long long b = lerp16(terrain_lattice(e, ix, iz + 1, o), terrain_lattice(e, ix + 1, iz + 1, o), sx);
+    return lerp16(a, b, sz);
+}
 __device__ uint32_t terrain_height(const DevEditor& e, uint32_t x, uint32_t z)
 {
     long long f = 0;
-    for (uint32_t o = 0; o < e.terrain.octaves; ++o) {
-        const uint32_t c = terrain_cell_log2(e, o);
-        const uint32_t ix = x >> c, iz = z >> c, m = (1u << c) - 1u;
-        const long long fx = c <= 16 ? (long long)((x & m) << (16 - c)) : (long long)((x & m) >> (c - 16));
-        const long long fz = c <= 16 ? (long long)((z & m) << (16 - c)) : (long long)((z & m) >> (c - 16));
-        const long long sx = smooth16(fx), sz = smooth16(fz);
-        const long long a = lerp16(terrain_lattice(e, ix, iz, o), terrain_lattice(e, ix + 1, iz, o), sx);
-        const long long b = lerp16(terrain_lattice(e, ix, iz + 1, o), terrain_lattice(e, ix + 1, iz + 1, o), sx);
-        f += lerp16(a, b, sz) << (e.terrain.octaves - 1 - o);
-    }
+    for (uint32_t o = 0; o < e.terrain.octaves; ++o)
+        f += terrain_octave(e, x, z, o) << (e.terrain.octaves - 1 - o);
     return terrain_height_from_fbm(e, f);
 }
 __device__ void terrain_bounds(const DevEditor& e, uint32_t x0, uint32_t z0, uint32_t s, uint32_t& hlo, uint32_t& hhi)
@@ -100,7 +103,17 @@ __device__ void terrain_bounds(const DevEditor& e, uint32_t x0, uint32_t z0, uin
         const uint32_t ix0 = x0 >> c, iz0 = z0 >> c;
         const uint32_t ix1 = ((x0 + s - 1) >> c) + 1, iz1 = ((z0 + s - 1) >> c) + 1;
         long long vlo = 65535, vhi = 0;
-        if ((unsigned long long)(ix1 - ix0 + 1) * (iz1 - iz0 + 1) > 64) {
+        if (s <= (1u << c)) {
+            // Footprint inside one lattice cell: extremes at the footprint corners, up to 2 units of
+            // integer truncation below the real bilinear value (same rule as the oracle).
+            const uint32_t x1 = x0 + s - 1, z1 = z0 + s - 1;
+            const long long v0 = terrain_octave(e, x0, z0, o), v1 = terrain_octave(e, x1, z0, o);
+            const long long v2 = terrain_octave(e, x0, z1, o), v3 = terrain_octave(e, x1, z1, o);
+            vlo = min(min(v0, v1), min(v2, v3)) - 2;
+            vhi = max(max(v0, v1), max(v2, v3)) + 2;
+            vlo = vlo < 0 ? 0 : vlo;
+            vhi = vhi > 65535 ? 65535 : vhi;
+        } else if ((unsigned long long)(ix1 - ix0 + 1) * (iz1 - iz0 + 1) > 64) {
             vlo = 0;
             vhi = 65535;
         } else {
@@ -234,7 +247,7 @@ __device__ uint32_t copy_should_edit(const DevEditor& e, const DevDag& d, uint32
         const CopyParent par = in[p];
         if (par.handle == kNone)
             break;
-        const uint32_t* node = d.items + par.handle;
+        const uint32_t* node = item_ptr(d, par.handle);
         const uint32_t mask = node[0] & 0xFFu;
         for (uint32_t c = 0; c < 8; ++c) {
             if (!(mask & (1u << c)))
@@ -339,14 +352,14 @@ __global__ void __launch_bounds__(256) k_build_level(DevDag d, DevEditor e, uint
             w = *reinterpret_cast<const WorkItem*>(scratch + offW + i * stride);
         uint32_t child = kNone, state = ST_EMPTY, fillMat = 0;
         if (active && w.handle != kNone) {
-            const uint32_t* node = d.items + w.handle;
+            const uint32_t* node = item_ptr(d, w.handle);
             const uint32_t mask = node[0] & 0xFFu;
             if (mask & (1u << c)) {
                 child = node[1 + __popc(mask & ((1u << c) - 1u))];
                 if (childLevel == d.leafLevel)
                     state = ST_PARTIAL;
                 else
-                    state = ((d.items[child] >> 8) & 1u) ? ST_FILLED : ST_PARTIAL;
+                    state = ((item_ptr(d, child)[0] >> 8) & 1u) ? ST_FILLED : ST_PARTIAL;
             }
             if (c == 0)
                 ++oldRead;
@@ -465,7 +478,7 @@ __global__ void __launch_bounds__(256) k_build_leaves(DevDag d, DevEditor e, cha
         // old leaf words (lanes 0..9)
         uint32_t ow = 0, lo = 0, hi = 0;
         if (w.handle != kNone) {
-            const uint32_t* leaf = d.items + w.handle;
+            const uint32_t* leaf = item_ptr(d, w.handle);
             const uint32_t a = lane < 2 ? leaf[lane] : 0u;
             lo = __shfl_sync(0xFFFFFFFFu, a, 0);
             hi = __shfl_sync(0xFFFFFFFFu, a, 1);
@@ -533,7 +546,7 @@ __global__ void __launch_bounds__(256) k_build_leaves(DevDag d, DevEditor e, cha
                                 found = par.handle;
                         }
                         if (found != kNone) {
-                            const uint32_t* src = d.items + found;
+                            const uint32_t* src = item_ptr(d, found);
                             const uint32_t bitIdx = ((ux & 1u) ? 4u : 0u) | ((uy & 1u) ? 2u : 0u) | ((uz & 1u) ? 1u : 0u) | ((ux & 2u) ? 32u : 0u)
                                 | ((uy & 2u) ? 16u : 0u) | ((uz & 2u) ? 8u : 0u);
                             uint32_t m;
@@ -659,7 +672,7 @@ __global__ void __launch_bounds__(256) k_fix_level(DevDag d, uint32_t level, uin
             bool all = true;
             uint32_t mat = 0;
             for (uint32_t c = 0; c < 8 && all; ++c) {
-                const uint32_t* p = d.items + outW[c];
+                const uint32_t* p = item_ptr(d, outW[c]);
                 uint32_t cm;
                 if (level + 1 == LL) {
                     all = p[0] == 0xFFFFFFFFu && p[1] == 0xFFFFFFFFu;
@@ -763,7 +776,8 @@ __global__ void __launch_bounds__(256) k_insert_level(DevDag d, DevTable t, uint
     const uint32_t* items = reinterpret_cast<const uint32_t*>(scratch + E.offN[level]);
     Grp<G> g;
     const uint32_t groupsPerBlock = blockDim.x / G;
-    uint32_t spare = kNone, added = 0;
+    Spare spare;
+    uint32_t added = 0;
     for (uint32_t i = blockIdx.x * groupsPerBlock + threadIdx.x / G; i < n; i += gridDim.x * groupsPerBlock) {
         if (rep[i] != i)
             continue;

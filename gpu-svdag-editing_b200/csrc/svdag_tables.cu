@@ -68,7 +68,7 @@ __global__ void k_insert_canonical(DevDag d, DevTable t, uint32_t level)
     if (threadIdx.x != 0 || blockIdx.x != 0)
         return;
     Grp<1> g;
-    uint32_t spare = kNone;
+    Spare spare;
     for (uint32_t m = 0; m < SVDAG_NUM_MATERIALS; ++m) {
         Key<1> key;
         if (level == d.leafLevel) { // fully filled leaf of material m (my_gpu_hash_dag.cu:40-49)
@@ -140,11 +140,17 @@ __global__ void __launch_bounds__(256) k_table_op(DevDag d, DevTable t, const ui
     Grp<G> g;
     const uint32_t groupsPerBlock = blockDim.x / G;
     const uint32_t stride = gridDim.x * groupsPerBlock;
-    uint32_t spare = kNone;
+    Spare spare;
     for (uint32_t i = blockIdx.x * groupsPerBlock + threadIdx.x / G; i < n; i += stride) {
         if (reps && reps[i] != i)
             continue;
         const uint32_t off = offsets[i];
+        if (off >= totalWords) {
+            if (g.lane == 0)
+                out[i] = kNone;
+            set_status(d.ctl, SVDAG_ERR_INVALID);
+            continue;
+        }
         Key<G> key;
         load_key<G>(g, keys + off, totalWords - off, t.kind, key);
         uint32_t h;
@@ -168,6 +174,11 @@ __global__ void __launch_bounds__(256) k_batch_dedup(const uint32_t* __restrict_
 {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t off = offsets[i];
+        if (off >= totalWords) {
+            reps[i] = i;
+            set_status(ctl, SVDAG_ERR_INVALID);
+            continue;
+        }
         const uint32_t* p = keys + off;
         const unsigned long long lim = totalWords - off;
         uint32_t w[kItemStride] = {};
@@ -195,9 +206,10 @@ __global__ void __launch_bounds__(256) k_batch_dedup(const uint32_t* __restrict_
             if ((uint32_t)(e >> 32) == hb) {
                 const uint32_t j = (uint32_t)e - 1u;
                 const uint32_t* q = keys + offsets[j];
+                const unsigned long long qlim = totalWords - offsets[j];
                 bool same = true;
                 for (uint32_t k = 0; k < nw && same; ++k)
-                    same = q[k] == w[k];
+                    same = k < qlim && q[k] == w[k];
                 if (same) {
                     rep = j;
                     break;
@@ -221,7 +233,7 @@ __global__ void k_table_read(DevDag d, uint32_t kind, const uint32_t* handles, u
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t h = handles[i];
         uint32_t* o = out + (size_t)i * kItemStride;
-        if (h == kNone || h + 2ull > d.itemWords) {
+        if (h == kNone || h + 16ull > d.itemWords) {
             for (uint32_t j = 0; j < kItemStride; ++j)
                 o[j] = 0;
             continue;
@@ -263,6 +275,10 @@ __global__ void k_table_walk(DevDag d, DevTable t, unsigned long long* counters,
                 const uint32_t next = h[7];
                 if (next == kEnd)
                     break;
+                if (!handle_ok(d, next)) {
+                    set_status(d.ctl, SVDAG_ERR_CORRUPT);
+                    break;
+                }
                 ++slabs;
                 slab = next;
             }

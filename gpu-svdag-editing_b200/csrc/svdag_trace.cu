@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(256) k_trace(DevDag d, svdag_trace_params p, s
     const uint32_t root = d.ctl->root;
     if (root != kNone) {
         uint32_t cIndex = root;
-        uint32_t cChild = d.items[root] & 0xFFu;
+        uint32_t cChild = item_ptr(d, root)[0] & 0xFFu;
         uint32_t cVisit = cChild & intersection_mask(true, 0, 0, 0, 0, levels, r);
         for (;;) {
             {
@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(256) k_trace(DevDag d, svdag_trace_params p, s
             if (level == levels) {
                 const uint32_t voxel = ((px & 1u) ? 4u : 0u) | ((py & 1u) ? 2u : 0u) | ((pz & 1u) ? 1u : 0u) | ((px & 2u) ? 32u : 0u)
                     | ((py & 2u) ? 16u : 0u) | ((pz & 2u) ? 8u : 0u); // mortonU32() & 63
-                const uint32_t* leaf = d.items + addr;
+                const uint32_t* leaf = item_ptr(d, addr);
                 const unsigned long long m = (unsigned long long)leafLo | ((unsigned long long)leafHi << 32);
                 if ((m >> voxel) & 1ull) {
                     const uint32_t bit = __popcll(m & ((1ull << voxel) - 1ull)) * 4u;
@@ -186,16 +186,17 @@ __global__ void __launch_bounds__(256) k_trace(DevDag d, svdag_trace_params p, s
                 break;
             }
             if (level < LL) {
-                const uint32_t* node = d.items + cIndex;
+                const uint32_t* node = item_ptr(d, cIndex);
                 cIndex = node[1 + __popc(cChild & ((1u << nextChild) - 1u))];
-                cChild = d.items[cIndex] & 0xFFu;
+                cChild = item_ptr(d, cIndex)[0] & 0xFFu;
                 cVisit = cChild & intersection_mask(false, level, px, py, pz, levels, r);
             } else {
                 uint32_t childMask;
                 if (level == LL) {
-                    const uint32_t* node = d.items + cIndex;
+                    const uint32_t* node = item_ptr(d, cIndex);
                     addr = node[1 + __popc(cChild & ((1u << nextChild) - 1u))];
-                    const uint2 lh = make_uint2(d.items[addr], d.items[addr + 1]);
+                    const uint32_t* lp = item_ptr(d, addr);
+                    const uint2 lh = make_uint2(lp[0], lp[1]);
                     leafLo = lh.x;
                     leafHi = lh.y;
                     childMask = first_child_mask(leafLo, leafHi);
@@ -257,7 +258,7 @@ __global__ void k_sample(DevDag d, const uint32_t* xyz, uint32_t n, uint32_t* ou
             for (uint32_t level = 0; level < d.leafLevel; ++level) {
                 const uint32_t s = d.levels - (level + 1);
                 const uint32_t child = (((x >> s) & 1u) << 2) | (((y >> s) & 1u) << 1) | ((z >> s) & 1u);
-                const uint32_t* node = d.items + h;
+                const uint32_t* node = item_ptr(d, h);
                 const uint32_t mask = node[0] & 0xFFu;
                 if (!(mask & (1u << child))) {
                     h = kNone;
@@ -268,7 +269,7 @@ __global__ void k_sample(DevDag d, const uint32_t* xyz, uint32_t n, uint32_t* ou
             if (h != kNone) {
                 const uint32_t v = ((x & 1u) ? 4u : 0u) | ((y & 1u) ? 2u : 0u) | ((z & 1u) ? 1u : 0u) | ((x & 2u) ? 32u : 0u) | ((y & 2u) ? 16u : 0u)
                     | ((z & 2u) ? 8u : 0u);
-                const uint32_t* leaf = d.items + h;
+                const uint32_t* leaf = item_ptr(d, h);
                 const unsigned long long m = (unsigned long long)leaf[0] | ((unsigned long long)leaf[1] << 32);
                 if ((m >> v) & 1ull) {
                     const uint32_t bit = __popcll(m & ((1ull << v) - 1ull)) * 4u;

@@ -274,7 +274,10 @@ class MyGPUHashDAG:
 
     def free(self):
         if getattr(self, "h", None):
-            lib().svdag_destroy(self.h)
+            try:
+                lib().svdag_destroy(self.h)
+            except Exception:  # interpreter shutdown
+                pass
             self.h = None
 
     __del__ = free

@@ -60,7 +60,7 @@ typedef struct svdag_config {
     uint64_t pool_bytes; /* the single preallocated HBM pool (item region + scratch arena) */
     uint64_t scratch_bytes; /* part of the pool reserved for per-edit temporaries */
     uint32_t target_load_factor; /* items per bucket when a level table is sized; 0 = default (16) */
-    uint32_t probe_lanes; /* lanes cooperating on one key: 1, 4, 8, 16 or 32; 0 = autotuned default */
+    uint32_t probe_lanes; /* lanes cooperating on one key: 1, 2, 4, 8, 16 or 32; 0 = default (1) */
     uint32_t undo_depth; /* undo history ring size; 0 = default (32) */
     uint32_t flags; /* reserved, must be 0 */
 } svdag_config;

@@ -139,7 +139,10 @@ class OracleDag:
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().oracle_destroy(self.h)
+            try:
+                lib().oracle_destroy(self.h)
+            except Exception:  # interpreter shutdown
+                pass
             self.h = None
 
     @property

@@ -910,7 +910,19 @@ struct Terrain {
             const uint32_t ix0 = x0 >> c, iz0 = z0 >> c;
             const uint32_t ix1 = ((x0 + s - 1) >> c) + 1, iz1 = ((z0 + s - 1) >> c) + 1;
             int64_t vlo = 65535, vhi = 0;
-            if ((uint64_t)(ix1 - ix0 + 1) * (iz1 - iz0 + 1) > 64) {
+            if (s <= (1u << c)) {
+                // Footprint inside one lattice cell: the field is bilinear in the (monotone) smoothstep
+                // weights, so its extremes sit at the footprint corners; integer truncation of the
+                // three lerps moves a value by at most 2 units below the real bilinear value.
+                const uint32_t x1 = x0 + s - 1, z1 = z0 + s - 1;
+                const int64_t v[4] = { octave_value(x0, z0, o), octave_value(x1, z0, o), octave_value(x0, z1, o), octave_value(x1, z1, o) };
+                for (int64_t t : v) {
+                    vlo = std::min(vlo, t);
+                    vhi = std::max(vhi, t);
+                }
+                vlo = std::max<int64_t>(0, vlo - 2);
+                vhi = std::min<int64_t>(65535, vhi + 2);
+            } else if ((uint64_t)(ix1 - ix0 + 1) * (iz1 - iz0 + 1) > 64) {
                 vlo = 0;
                 vhi = 65535;
             } else {

@@ -12,7 +12,7 @@ from gpu_util import (TERRAIN, compare_hits, gpu_canon, gpu_sample, gpu_trace, r
 pytestmark = pytest.mark.gpu
 
 
-def make_pair(svdag_lib, oracle_mod, levels, terrain=TERRAIN, pool=1 << 30):
+def make_pair(svdag_lib, oracle_mod, levels, terrain=TERRAIN, pool=2 << 30):
     g = svdag_lib.MyGPUHashDAG(levels, pool_bytes=pool)
     g.build_terrain(**terrain)
     o = oracle_mod.OracleDag(levels)
