@@ -303,7 +303,22 @@ def run_mine(args):
     torch.cuda.synchronize()
     e2e_ms = e_start.elapsed_time(e_end)
 
-    hash_res = run_hash_bench(svdag, torch, stream)
+    # batched form: the same K edits (after the same warm-up) in one persistent launch
+    b_dag = svdag.MyGPUHashDAG(LEVELS, pool_bytes=4 << 30, scratch_bytes=1 << 30)
+    b_dag.build_terrain(**TERRAIN, stream=stream)
+    for i in range(args.warmup):
+        b_dag.edit(mk(i), stream=stream)
+    stream.synchronize()
+    b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    b0.record(stream)
+    nrec = b_dag.edit_batch([mk(args.warmup + k) for k in range(args.steps)], stream=stream)
+    b1.record(stream)
+    torch.cuda.synchronize()
+    b_ms = b0.elapsed_time(b1)
+    b_edited = sum(r.edited_voxels for r in b_dag.edit_records(nrec, stream))
+    b_dag.free()
+
+    hash_res = run_hash_bench(svdag, torch, stream, lanes=args.hash_lanes, load_factor=args.hash_lf)
     t_max = total_ms
     if dist:
         t = torch.tensor([total_ms, e2e_ms], device="cuda")
@@ -334,9 +349,11 @@ def run_mine(args):
         "edit_status": int(status),
         "e2e": {"value": e2e_edited / (e2e_ms / 1e3) / 1e6, "unit": "edited Mvox/s",
                 "h2d_bytes_per_step": 56, "d2h_bytes_per_step": FRAME * FRAME * 68 + 264},
-        "roofline": {"bound": "hbm", "kernel": "slab-hash find (C1, 2^24 keys, 8 lanes/key)",
+        "roofline": {"bound": "hbm", "kernel": f"slab-hash find (C1, 2^24 keys, {args.hash_lanes} lane(s)/key)",
                      "achieved": find_gbs, "peak": peak, "unit": "GB/s", "frac": find_gbs / peak,
                      "peak_source": peak_kind, "traffic": None},
+        "batched": {"edits": args.steps, "ms": b_ms, "ms_per_edit": b_ms / args.steps,
+                    "edited_mvox_s": b_edited / (b_ms / 1e3) / 1e6, "note": "edits only, one persistent launch"},
         "hash_c1": hash_res,
         "clocks": clocks.summary(),
         "gpu_launches": args.steps * (4 * (LEVELS - 2) + 6),
@@ -419,18 +436,73 @@ def run_reference(args):
     }))
 
 
+def run_mode_hash(args):
+    """Only the C1 slab-hash microbenchmark (profiling entry point)."""
+    import torch
+
+    import svdag
+
+    r = run_hash_bench(svdag, torch, torch.cuda.Stream(), n_total=args.hash_keys, lanes=args.hash_lanes,
+                       load_factor=args.hash_lf, reps=args.hash_reps, pool=args.hash_pool)
+    print(json.dumps({k: v for k, v in r.items()}))
+
+
+def run_mode_edit(args):
+    """Only the per-edit path: depth-10 terrain, warm-up edits, then K edits each followed by a frame
+    (profiling entry point)."""
+    import torch
+
+    import svdag
+
+    edits = c0_edits(max(args.warmup + args.steps, 64))
+    dag = svdag.MyGPUHashDAG(LEVELS, pool_bytes=4 << 30, scratch_bytes=1 << 30)
+    dag.build_terrain(**TERRAIN)
+    params = svdag.get_trace_params((512.0, 900.0, 512.0), (512.0, 512.0, 512.0), FRAME, FRAME)
+    hits = torch.empty(FRAME * FRAME * 68, dtype=torch.uint8, device="cuda")
+    te, tt = [], []
+    for i in range(args.warmup + args.steps):
+        tool, mat, c, r = edits[i % len(edits)]
+        e = svdag.Edit(tool=tool, material=mat)
+        e.center[:] = list(c)
+        e.radius = r
+        a, b, d = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        a.record()
+        dag.edit(e)
+        b.record()
+        dag.trace(params, hits)
+        d.record()
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            te.append(a.elapsed_time(b))
+            tt.append(b.elapsed_time(d))
+    dag.sync()
+    print(json.dumps({"edit_ms_median": statistics.median(te), "trace_ms_median": statistics.median(tt),
+                      "edit_ms": te, "trace_ms": tt}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=48)
     ap.add_argument("--warmup", type=int, default=8)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
+    ap.add_argument("--mode", default="full", choices=["full", "hash", "edit"],
+                    help="full = the benchmark line; hash / edit run one sub-workload (profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--hash-keys", type=int, default=1 << 24)
+    ap.add_argument("--hash-lanes", type=int, default=1)
+    ap.add_argument("--hash-lf", type=int, default=20)
+    ap.add_argument("--hash-reps", type=int, default=3)
+    ap.add_argument("--hash-pool", type=int, default=6 << 30)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.mode == "hash":
+        run_mode_hash(args)
+    elif args.mode == "edit":
+        run_mode_edit(args)
     else:
         run_mine(args)
 

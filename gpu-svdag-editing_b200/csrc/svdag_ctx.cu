@@ -13,6 +13,7 @@ using namespace svdag;
 namespace {
 
 constexpr unsigned long long kCtlBytes = 64 * 1024;
+constexpr unsigned long long kBatchBytes = 2 * 1024 * 1024;
 
 // ---------------------------------------------------------------- garbage collection
 // MyGPUHashDAG::garbageCollect (my_gpu_hash_dag.cu:365-475) marks level by level from the root set
@@ -163,7 +164,7 @@ svdag_status svdag_create(const svdag_config* cfg, svdag_ctx** out)
     SVDAG_CUDA(cudaSetDevice(cfg->device));
     const unsigned long long pool = cfg->pool_bytes ? cfg->pool_bytes : (1ull << 30);
     const unsigned long long scratch = cfg->scratch_bytes ? cfg->scratch_bytes : pool / 4;
-    if (scratch + kCtlBytes + (1ull << 20) > pool)
+    if (scratch + kCtlBytes + kBatchBytes + (1ull << 20) > pool)
         return SVDAG_ERR_INVALID;
     auto* ctx = new (std::nothrow) svdag_ctx();
     if (!ctx)
@@ -180,10 +181,12 @@ svdag_status svdag_create(const svdag_config* cfg, svdag_ctx** out)
     }
     ctx->poolBytes = pool;
     ctx->ctl = reinterpret_cast<Control*>(ctx->pool);
-    ctx->scratch = ctx->pool + kCtlBytes;
+    ctx->batch = ctx->pool + kCtlBytes;
+    ctx->batchBytes = kBatchBytes;
+    ctx->scratch = ctx->pool + kCtlBytes + kBatchBytes;
     ctx->scratchBytes = scratch;
-    ctx->items = reinterpret_cast<uint32_t*>(ctx->pool + kCtlBytes + scratch);
-    ctx->itemWords = std::min<unsigned long long>((pool - kCtlBytes - scratch) / 4 - 64, kMaxHandle);
+    ctx->items = reinterpret_cast<uint32_t*>(ctx->pool + kCtlBytes + kBatchBytes + scratch);
+    ctx->itemWords = std::min<unsigned long long>((pool - kCtlBytes - kBatchBytes - scratch) / 4 - 64, kMaxHandle);
     static_assert(sizeof(Control) <= kCtlBytes, "control block too large");
     cudaError_t e = cudaMemset(ctx->pool, 0, pool);
     if (e == cudaSuccess) {

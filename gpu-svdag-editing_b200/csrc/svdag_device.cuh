@@ -69,6 +69,7 @@ struct Control {
     uint32_t savedRoot; // source root of a move (the DAG before its removal step)
     uint32_t pad0;
     uint32_t fullyFilled[kMaxLevels][SVDAG_NUM_MATERIALS];
+    DevTable tables[kMaxLevels]; // the level tables (copied here by the host whenever they change)
     EditCounters edit;
 };
 

@@ -9,14 +9,18 @@
 // every kernel sizes itself from counters written by its predecessor, and the scratch arena layout is
 // recomputed on the device from those counts. Intra-level dedup is one open-addressing pass; the DAG
 // insert is a fused find-or-insert (the reference runs find and insert as two kernels).
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "svdag_edit.cuh"
 #include "svdag_host.hpp"
+
+namespace cg = cooperative_groups;
 
 namespace svdag {
 
@@ -288,11 +292,13 @@ __device__ __forceinline__ bool leaf_get_material(uint32_t lo, uint32_t hi, cons
 
 __device__ __forceinline__ unsigned long long work_stride(uint32_t tool) { return tool == SVDAG_TOOL_COPY ? 16ull + 128ull : 16ull; }
 
-__global__ void k_edit_begin(DevDag d, DevEditor e, char* scratch)
+__device__ void ph_edit_begin(const DevDag& d, const DevEditor& e, char* scratch)
 {
     if (threadIdx.x != 0 || blockIdx.x != 0)
         return;
     Control* c = d.ctl;
+    if (e.saveRoot)
+        c->savedRoot = c->root;
     EditCounters& E = c->edit;
     const uint32_t root = c->root;
     E.rootBefore = root;
@@ -321,7 +327,7 @@ __global__ void k_edit_begin(DevDag d, DevEditor e, char* scratch)
 // One 8-lane group per work item, lane c evaluates child c
 // (createIntermediateSvoStructure_innerNode_warp, create_edit_svo.cu:168-303).
 template <uint32_t TOOL>
-__global__ void __launch_bounds__(256) k_build_level(DevDag d, DevEditor e, uint32_t level, char* scratch, unsigned long long scratchBytes)
+__device__ void ph_build_level(const DevDag& d, const DevEditor& e, uint32_t level, char* scratch, unsigned long long scratchBytes)
 {
     EditCounters& E = d.ctl->edit;
     const unsigned long long stride = work_stride(TOOL);
@@ -438,7 +444,7 @@ __global__ void __launch_bounds__(256) k_build_level(DevDag d, DevEditor e, uint
 // One warp per leaf; lane l owns voxels l and l+32 (createIntermediateSvoStructure_leaf_workgroup,
 // create_edit_svo.cu:321-426, which uses a 64-thread block per leaf).
 template <uint32_t TOOL>
-__global__ void __launch_bounds__(256) k_build_leaves(DevDag d, DevEditor e, char* scratch, unsigned long long scratchBytes)
+__device__ void ph_build_leaves(const DevDag& d, const DevEditor& e, char* scratch, unsigned long long scratchBytes)
 {
     EditCounters& E = d.ctl->edit;
     const uint32_t LL = d.leafLevel;
@@ -621,7 +627,7 @@ __device__ __forceinline__ bool merge_live(const DevDag& d)
 }
 
 // updateChildPointers + discover_fully_filled (my_gpu_hash_dag_edits.cu:44-150), thread per node.
-__global__ void __launch_bounds__(256) k_fix_level(DevDag d, uint32_t level, uint32_t builder, char* scratch)
+__device__ void ph_fix_level(const DevDag& d, uint32_t level, uint32_t builder, char* scratch)
 {
     EditCounters& E = d.ctl->edit;
     if (!merge_live(d))
@@ -705,7 +711,7 @@ __global__ void __launch_bounds__(256) k_fix_level(DevDag d, uint32_t level, uin
 // Intra-level dedup (insertDuplicatesIntoHashTableAsWarp + findUniqueInHashTableAsWarp_kernel1,
 // my_gpu_hash_dag_edits.cu:164-218) as one open-addressing pass; rep[i] = index of the item's
 // representative, kEmptyRep for an empty item.
-__global__ void __launch_bounds__(256) k_dedup_level(DevDag d, uint32_t level, char* scratch)
+__device__ void ph_dedup_level(const DevDag& d, uint32_t level, char* scratch)
 {
     EditCounters& E = d.ctl->edit;
     if (!merge_live(d))
@@ -764,7 +770,7 @@ __global__ void __launch_bounds__(256) k_dedup_level(DevDag d, uint32_t level, c
 // Find-or-insert of each representative into the level table (findUniqueInHashTableAsWarp_kernel2 +
 // insertUniqueInHashTableAsWarp_kernel, my_gpu_hash_dag_edits.cu:220-280, fused).
 template <int G>
-__global__ void __launch_bounds__(256) k_insert_level(DevDag d, DevTable t, uint32_t level, char* scratch)
+__device__ void ph_insert_level(const DevDag& d, const DevTable& t, uint32_t level, char* scratch)
 {
     EditCounters& E = d.ctl->edit;
     if (!merge_live(d))
@@ -794,7 +800,7 @@ __global__ void __launch_bounds__(256) k_insert_level(DevDag d, DevTable t, uint
         atomicAdd(&E.added, (unsigned long long)added);
 }
 
-__global__ void k_edit_end(DevDag d, char* scratch, uint32_t builder)
+__device__ void ph_edit_end(const DevDag& d, char* scratch, uint32_t builder, EditRecord* record)
 {
     if (threadIdx.x != 0 || blockIdx.x != 0)
         return;
@@ -810,6 +816,123 @@ __global__ void k_edit_end(DevDag d, char* scratch, uint32_t builder)
         c->root = kNone;
     }
     E.rootAfter = c->root;
+    if (record) {
+        record->rootBefore = E.rootBefore;
+        record->rootAfter = E.rootAfter;
+        record->status = E.overflow ? (uint32_t)SVDAG_ERR_OOM : c->status;
+        record->edited = E.edited;
+        record->added = E.added;
+        unsigned long long svo = 0, reps = 0;
+        for (uint32_t l = 0; l < kMaxLevels; ++l) {
+            svo += E.count[l];
+            reps += E.repCount[l];
+        }
+        record->svoItems = svo;
+        record->unique = reps;
+    }
+}
+
+__device__ void ph_reset_counters(const DevDag& d)
+{
+    if (blockIdx.x != 0)
+        return;
+    uint32_t* w = reinterpret_cast<uint32_t*>(&d.ctl->edit);
+    for (uint32_t i = threadIdx.x; i < sizeof(EditCounters) / 4; i += blockDim.x)
+        w[i] = 0;
+}
+
+// ---------------------------------------------------------------- kernel wrappers (one launch per phase)
+
+__global__ void k_edit_begin(DevDag d, DevEditor e, char* scratch) { ph_edit_begin(d, e, scratch); }
+template <uint32_t TOOL>
+__global__ void __launch_bounds__(256) k_build_level(DevDag d, DevEditor e, uint32_t level, char* scratch, unsigned long long scratchBytes)
+{
+    ph_build_level<TOOL>(d, e, level, scratch, scratchBytes);
+}
+template <uint32_t TOOL>
+__global__ void __launch_bounds__(256) k_build_leaves(DevDag d, DevEditor e, char* scratch, unsigned long long scratchBytes)
+{
+    ph_build_leaves<TOOL>(d, e, scratch, scratchBytes);
+}
+__global__ void __launch_bounds__(256) k_fix_level(DevDag d, uint32_t level, uint32_t builder, char* scratch)
+{
+    ph_fix_level(d, level, builder, scratch);
+}
+__global__ void __launch_bounds__(256) k_dedup_level(DevDag d, uint32_t level, char* scratch) { ph_dedup_level(d, level, scratch); }
+template <int G>
+__global__ void __launch_bounds__(256) k_insert_level(DevDag d, DevTable t, uint32_t level, char* scratch)
+{
+    ph_insert_level<G>(d, t, level, scratch);
+}
+__global__ void k_edit_end(DevDag d, char* scratch, uint32_t builder) { ph_edit_end(d, scratch, builder, nullptr); }
+
+// ---------------------------------------------------------------- persistent form
+// One cooperative launch runs whole edits: every phase above is a grid-stride loop over the
+// device-resident counts, separated by grid-wide barriers instead of kernel boundaries. All
+// threads reach every barrier (phases only return early, never skip a barrier).
+
+template <uint32_t TOOL>
+__device__ __forceinline__ void fused_edit(cg::grid_group& grid, const DevDag& d, const DevEditor& ed, char* scratch,
+    unsigned long long scratchBytes, EditRecord* record)
+{
+    const uint32_t LL = d.leafLevel;
+    ph_reset_counters(d);
+    grid.sync();
+    ph_edit_begin(d, ed, scratch);
+    grid.sync();
+    for (uint32_t level = 0; level < LL; ++level) {
+        ph_build_level<TOOL>(d, ed, level, scratch, scratchBytes);
+        grid.sync();
+    }
+    ph_build_leaves<TOOL>(d, ed, scratch, scratchBytes);
+    grid.sync();
+    for (int level = (int)LL; level >= 0; --level) {
+        if (level < (int)LL) {
+            ph_fix_level(d, (uint32_t)level, ed.builder, scratch);
+            grid.sync();
+        }
+        ph_dedup_level(d, (uint32_t)level, scratch);
+        grid.sync();
+        ph_insert_level<1>(d, d.ctl->tables[level], (uint32_t)level, scratch);
+        grid.sync();
+    }
+    ph_edit_end(d, scratch, ed.builder, record);
+    grid.sync();
+}
+
+__global__ void __launch_bounds__(256) k_edit_fused(DevDag d, DevEditor single, const DevEditor* eds, uint32_t numEdits, char* scratch,
+    unsigned long long scratchBytes, EditRecord* records)
+{
+    cg::grid_group grid = cg::this_grid();
+    for (uint32_t k = 0; k < numEdits; ++k) {
+        const DevEditor ed = eds ? eds[k] : single;
+        EditRecord* rec = records ? &records[k] : nullptr;
+        switch (ed.tool) {
+        case SVDAG_TOOL_SPHERE_ADD:
+            fused_edit<SVDAG_TOOL_SPHERE_ADD>(grid, d, ed, scratch, scratchBytes, rec);
+            break;
+        case SVDAG_TOOL_SPHERE_REMOVE:
+            fused_edit<SVDAG_TOOL_SPHERE_REMOVE>(grid, d, ed, scratch, scratchBytes, rec);
+            break;
+        case SVDAG_TOOL_BOX_ADD:
+            fused_edit<SVDAG_TOOL_BOX_ADD>(grid, d, ed, scratch, scratchBytes, rec);
+            break;
+        case SVDAG_TOOL_BOX_REMOVE:
+            fused_edit<SVDAG_TOOL_BOX_REMOVE>(grid, d, ed, scratch, scratchBytes, rec);
+            break;
+        case SVDAG_TOOL_SPHERE_PAINT:
+            fused_edit<SVDAG_TOOL_SPHERE_PAINT>(grid, d, ed, scratch, scratchBytes, rec);
+            break;
+        case SVDAG_TOOL_COPY:
+            fused_edit<SVDAG_TOOL_COPY>(grid, d, ed, scratch, scratchBytes, rec);
+            break;
+        case SVDAG_TOOL_BOX_PAINT_NOISE:
+            fused_edit<SVDAG_TOOL_BOX_PAINT_NOISE>(grid, d, ed, scratch, scratchBytes, rec);
+            break;
+        default:
+            break;
+        }
+    }
 }
 
 __global__ void k_undo_redo(Control* c, uint32_t redo)
@@ -836,7 +959,6 @@ __global__ void k_undo_redo(Control* c, uint32_t redo)
     }
 }
 
-__global__ void k_save_root(Control* c) { c->savedRoot = c->root; }
 
 // ---------------------------------------------------------------- host orchestration
 
@@ -977,21 +1099,98 @@ svdag_status launch_pipeline(svdag_ctx* ctx, const DevEditor& ed, cudaStream_t s
     return SVDAG_OK;
 }
 
+// Expands a tool into device editors (a move is a box removal that saves the root, then a copy
+// from the saved root).
+int expand_edit(const svdag_ctx* ctx, const svdag_edit& e, DevEditor* out)
+{
+    if (e.tool == SVDAG_TOOL_MOVE) {
+        svdag_edit rm = e;
+        rm.tool = SVDAG_TOOL_BOX_REMOVE;
+        out[0] = make_editor(ctx, rm);
+        out[0].saveRoot = 1;
+        svdag_edit cp = e;
+        cp.tool = SVDAG_TOOL_COPY;
+        out[1] = make_editor(ctx, cp);
+        out[1].useSavedSource = 1;
+        return 2;
+    }
+    out[0] = make_editor(ctx, e);
+    return 1;
+}
+
+int fused_grid(svdag_ctx* ctx)
+{
+    if (ctx->fusedGrid < 0) {
+        int perSm = 0, sms = 0, coop = 0;
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ctx->device);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+        if (coop && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_edit_fused, 256, 0) == cudaSuccess)
+            ctx->fusedGrid = perSm * sms;
+        else
+            ctx->fusedGrid = 0;
+        cudaGetLastError();
+    }
+    return ctx->fusedGrid;
+}
+
+svdag_status launch_fused(svdag_ctx* ctx, const DevEditor* eds, uint32_t n, bool recordEdits, cudaStream_t s)
+{
+    const int grid = fused_grid(ctx);
+    if (grid <= 0)
+        return SVDAG_ERR_UNSUPPORTED;
+    DevDag d = ctx->dag();
+    DevEditor single = eds[0];
+    const DevEditor* devEds = nullptr;
+    EditRecord* records = nullptr;
+    if (n > 1 || recordEdits) {
+        const size_t edBytes = align256((size_t)n * sizeof(DevEditor));
+        if (edBytes + (size_t)n * sizeof(EditRecord) > ctx->batchBytes)
+            return SVDAG_ERR_INVALID;
+        SVDAG_CUDA(cudaMemcpyAsync(ctx->batch, eds, (size_t)n * sizeof(DevEditor), cudaMemcpyHostToDevice, s));
+        devEds = reinterpret_cast<const DevEditor*>(ctx->batch);
+        records = reinterpret_cast<EditRecord*>(ctx->batch + edBytes);
+        ctx->lastBatch = n;
+    }
+    char* scratch = ctx->scratch;
+    unsigned long long scratchBytes = ctx->scratchBytes;
+    void* args[] = { &d, &single, &devEds, &n, &scratch, &scratchBytes, &records };
+    SVDAG_CUDA(cudaLaunchCooperativeKernel((const void*)k_edit_fused, dim3(grid), dim3(256), args, 0, s));
+    return SVDAG_OK;
+}
+
 svdag_status run_edit(svdag_ctx* ctx, const svdag_edit* e, cudaStream_t s)
 {
     SVDAG_TRY(ensure_level_tables(ctx, s));
-    if (e->tool == SVDAG_TOOL_MOVE) { // clear the source box, then paste from the DAG before the clear
-        k_save_root<<<1, 1, 0, s>>>(ctx->ctl);
-        svdag_edit rm = *e;
-        rm.tool = SVDAG_TOOL_BOX_REMOVE;
-        SVDAG_TRY(launch_pipeline(ctx, make_editor(ctx, rm), s));
-        svdag_edit cp = *e;
-        cp.tool = SVDAG_TOOL_COPY;
-        DevEditor ed = make_editor(ctx, cp);
-        ed.useSavedSource = 1;
-        return launch_pipeline(ctx, ed, s);
+    DevEditor eds[2];
+    const int n = expand_edit(ctx, *e, eds);
+    if (fused_grid(ctx) > 0)
+        return launch_fused(ctx, eds, (uint32_t)n, false, s);
+    for (int i = 0; i < n; ++i)
+        SVDAG_TRY(launch_pipeline(ctx, eds[i], s));
+    return SVDAG_OK;
+}
+
+svdag_status run_edit_batch(svdag_ctx* ctx, const svdag_edit* edits, uint32_t count, cudaStream_t s)
+{
+    SVDAG_TRY(ensure_level_tables(ctx, s));
+    std::vector<DevEditor> eds;
+    eds.reserve(2 * (size_t)count);
+    for (uint32_t i = 0; i < count; ++i) {
+        DevEditor tmp[2];
+        const int n = expand_edit(ctx, edits[i], tmp);
+        eds.insert(eds.end(), tmp, tmp + n);
     }
-    return launch_pipeline(ctx, make_editor(ctx, *e), s);
+    if (eds.empty())
+        return SVDAG_OK;
+    if (fused_grid(ctx) > 0) {
+        const uint32_t maxPerLaunch = (uint32_t)(ctx->batchBytes / (sizeof(DevEditor) + sizeof(EditRecord) + 8));
+        for (size_t i = 0; i < eds.size(); i += maxPerLaunch)
+            SVDAG_TRY(launch_fused(ctx, eds.data() + i, (uint32_t)std::min<size_t>(maxPerLaunch, eds.size() - i), true, s));
+        return SVDAG_OK;
+    }
+    for (const auto& ed : eds)
+        SVDAG_TRY(launch_pipeline(ctx, ed, s));
+    return SVDAG_OK;
 }
 
 // Scene construction: the terrain runs through the same pipeline as an edit of an empty DAG, with
@@ -1044,6 +1243,7 @@ svdag_status run_terrain_build(svdag_ctx* ctx, const svdag_terrain_params* p, cu
         svdag_table& t = ctx->levelTables[level];
         SVDAG_TRY(alloc_table(ctx, &t, level == (int)LL ? SVDAG_KIND_LEAF : SVDAG_KIND_NODE, buckets, s));
         t.level = level;
+        SVDAG_TRY(upload_tables(ctx, s));
         SVDAG_TRY(insert_canonical(ctx, (uint32_t)level, s));
         SVDAG_TRY(launch_insert(ctx, level, level_bound(level), s));
     }
@@ -1086,8 +1286,39 @@ svdag_status svdag_edit_apply_many(svdag_ctx* ctx, const svdag_edit* edits, uint
 {
     if (!ctx || (count && !edits))
         return SVDAG_ERR_INVALID;
-    for (uint32_t i = 0; i < count; ++i)
-        SVDAG_TRY(svdag_edit_apply(ctx, &edits[i], stream));
+    for (uint32_t i = 0; i < count; ++i) {
+        const svdag_edit* e = &edits[i];
+        if (e->tool >= SVDAG_NUM_TOOLS || e->material >= SVDAG_NUM_MATERIALS || !std::isfinite(e->radius) || e->radius < 0
+            || (e->tool == SVDAG_TOOL_BOX_PAINT_NOISE && e->noise_cell_log2 > 20))
+            return SVDAG_ERR_INVALID;
+        for (int a = 0; a < 3; ++a)
+            if (!std::isfinite(e->center[a]) || !std::isfinite(e->src[a]) || !std::isfinite(e->dst[a]))
+                return SVDAG_ERR_INVALID;
+    }
+    return run_edit_batch(ctx, edits, count, as_stream(stream));
+}
+
+svdag_status svdag_edit_records(svdag_ctx* ctx, svdag_edit_record* out, uint32_t count, void* stream)
+{
+    if (!ctx || (count && !out) || count > ctx->lastBatch)
+        return SVDAG_ERR_INVALID;
+    if (!count)
+        return SVDAG_OK;
+    cudaStream_t s = as_stream(stream);
+    const size_t edBytes = align256((size_t)ctx->lastBatch * sizeof(DevEditor));
+    std::vector<EditRecord> rec(count);
+    SVDAG_CUDA(cudaMemcpyAsync(rec.data(), ctx->batch + edBytes, count * sizeof(EditRecord), cudaMemcpyDeviceToHost, s));
+    SVDAG_CUDA(cudaStreamSynchronize(s));
+    for (uint32_t i = 0; i < count; ++i) {
+        out[i].root_before = rec[i].rootBefore;
+        out[i].root_after = rec[i].rootAfter;
+        out[i].status = rec[i].status;
+        out[i].reserved = 0;
+        out[i].edited_voxels = rec[i].edited;
+        out[i].new_items = rec[i].added;
+        out[i].unique_items = rec[i].unique;
+        out[i].svo_items = rec[i].svoItems;
+    }
     return SVDAG_OK;
 }
 

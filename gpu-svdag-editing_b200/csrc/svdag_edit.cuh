@@ -27,7 +27,14 @@ struct DevEditor {
     uint32_t terrainBaseLog2;
     uint32_t levels;
     uint32_t useSavedSource; // copy: read the source from the saved root (move)
+    uint32_t saveRoot; // remember the root before this edit as the source of a later copy (move)
     uint32_t builder; // scene build: fully-filled discovery on every level, no undo frame
+};
+
+// Summary of one edit of a batch (written on the device, read by the host after the batch).
+struct EditRecord {
+    uint32_t rootBefore, rootAfter, status, pad;
+    unsigned long long edited, added, unique, svoItems;
 };
 
 struct WorkItem { // CreateIntermediateWorkItem (create_edit_svo.cu:55-65)

@@ -24,6 +24,10 @@ struct svdag_ctx {
     svdag::Control* ctl = nullptr; // device control block
     char* scratch = nullptr; // per-edit arena
     unsigned long long scratchBytes = 0;
+    char* batch = nullptr; // editors and per-edit records of a persistent batch launch
+    unsigned long long batchBytes = 0;
+    int fusedGrid = -1; // co-resident blocks of the persistent edit kernel (0 = unavailable)
+    uint32_t lastBatch = 0;
     uint32_t* items = nullptr; // item region
     unsigned long long itemWords = 0;
     svdag_table levelTables[svdag::kMaxLevels];
@@ -73,6 +77,7 @@ void reset_level_tables(svdag_ctx* ctx);
 
 // Edit machinery (svdag_edit.cu).
 svdag_status run_edit(svdag_ctx* ctx, const svdag_edit* e, cudaStream_t s);
+svdag_status run_edit_batch(svdag_ctx* ctx, const svdag_edit* edits, uint32_t count, cudaStream_t s);
 svdag_status run_terrain_build(svdag_ctx* ctx, const svdag_terrain_params* p, cudaStream_t s);
 
 } // namespace svdag

@@ -107,6 +107,7 @@ void reset_level_tables(svdag_ctx* ctx)
 svdag_status ensure_level_tables(svdag_ctx* ctx, cudaStream_t s)
 {
     const uint32_t leaf = ctx->cfg.levels - 2;
+    bool created = false;
     for (int level = (int)leaf; level >= 0; --level) {
         svdag_table& t = ctx->levelTables[level];
         if (t.ready)
@@ -118,11 +119,20 @@ svdag_status ensure_level_tables(svdag_ctx* ctx, cudaStream_t s)
         SVDAG_TRY(alloc_table(ctx, &t, level == (int)leaf ? SVDAG_KIND_LEAF : SVDAG_KIND_NODE, buckets, s));
         t.level = level;
         SVDAG_TRY(insert_canonical(ctx, (uint32_t)level, s));
+        created = true;
     }
-    return SVDAG_OK;
+    return created ? upload_tables(ctx, s) : SVDAG_OK;
 }
 
-svdag_status upload_tables(svdag_ctx*, cudaStream_t) { return SVDAG_OK; }
+svdag_status upload_tables(svdag_ctx* ctx, cudaStream_t s)
+{
+    DevTable t[kMaxLevels];
+    for (uint32_t l = 0; l < kMaxLevels; ++l)
+        t[l] = ctx->levelTables[l].dev;
+    SVDAG_CUDA(cudaMemcpyAsync(ctx->ctl->tables, t, sizeof(t), cudaMemcpyHostToDevice, s));
+    SVDAG_CUDA(cudaStreamSynchronize(s));
+    return SVDAG_OK;
+}
 
 } // namespace svdag
 

@@ -71,6 +71,12 @@ class EditStats(C.Structure):
                 ("reserved", C.c_uint32)]
 
 
+class EditRecord(C.Structure):
+    _fields_ = [("root_before", C.c_uint32), ("root_after", C.c_uint32), ("status", C.c_uint32),
+                ("reserved", C.c_uint32), ("edited_voxels", C.c_uint64), ("new_items", C.c_uint64),
+                ("unique_items", C.c_uint64), ("svo_items", C.c_uint64)]
+
+
 class TraceParams(C.Structure):
     _fields_ = [("camera", C.c_double * 3), ("ray_min", C.c_double * 3), ("ray_ddx", C.c_double * 3),
                 ("ray_ddy", C.c_double * 3), ("width", C.c_uint32), ("height", C.c_uint32)]
@@ -107,6 +113,7 @@ _PROTOS = {
     "svdag_edit_apply": [_P, C.POINTER(Edit), _P],
     "svdag_edit_apply_many": [_P, C.POINTER(Edit), _U32, _P],
     "svdag_last_edit_stats": [_P, C.POINTER(EditStats), _P],
+    "svdag_edit_records": [_P, C.POINTER(EditRecord), _U32, _P],
     "svdag_edit_sphere": [_P, C.c_float, C.c_float, C.c_float, C.c_float, _U32, C.c_int, _P],
     "svdag_edit_box": [_P, C.c_float, C.c_float, C.c_float, C.c_float, _U32, C.c_int, _P],
     "svdag_edit_paint": [_P, C.c_float, C.c_float, C.c_float, C.c_float, _U32, _P],
@@ -296,6 +303,18 @@ class MyGPUHashDAG:
     def edit(self, editor, stream=None):
         e = editor if isinstance(editor, Edit) else editor.to_edit()
         _check(lib().svdag_edit_apply(self.h, C.byref(e), stream_ptr(stream)), "svdag_edit_apply")
+
+    def edit_batch(self, editors, stream=None) -> int:
+        """Batched form: all edits in one persistent launch. Returns the number of records
+        (a move yields two)."""
+        arr = (Edit * len(editors))(*[e if isinstance(e, Edit) else e.to_edit() for e in editors])
+        _check(lib().svdag_edit_apply_many(self.h, arr, len(editors), stream_ptr(stream)), "svdag_edit_apply_many")
+        return sum(2 if e.tool == TOOL_MOVE else 1 for e in arr)
+
+    def edit_records(self, count: int, stream=None):
+        out = (EditRecord * count)()
+        _check(lib().svdag_edit_records(self.h, out, count, stream_ptr(stream)), "svdag_edit_records")
+        return list(out)
 
     def last_edit_stats(self, stream=None) -> EditStats:
         st = EditStats()

@@ -140,8 +140,23 @@ typedef struct svdag_edit_stats {
  * (my_gpu_hash_dag_edits.h:12-13, body my_gpu_hash_dag_edits.cu:633-671). Asynchronous on
  * `stream`; the root handle, undo history and counters stay on the device. */
 svdag_status svdag_edit_apply(svdag_ctx* ctx, const svdag_edit* edit, void* stream);
-/* Applies edits one after another with one launch sequence per edit level phase. */
+/* Batched form: applies the edits in order inside one persistent cooperative launch (phases separated
+ * by grid-wide barriers, no host round trip between edits); the result equals applying them one by
+ * one. Each edit gets an svdag_edit_record. A move counts as two records (removal, then paste). */
 svdag_status svdag_edit_apply_many(svdag_ctx* ctx, const svdag_edit* edits, uint32_t count, void* stream);
+
+typedef struct svdag_edit_record {
+    uint32_t root_before;
+    uint32_t root_after;
+    uint32_t status;
+    uint32_t reserved;
+    uint64_t edited_voxels;
+    uint64_t new_items;
+    uint64_t unique_items;
+    uint64_t svo_items;
+} svdag_edit_record;
+/* Copies the records of the first `count` edits of the most recent svdag_edit_apply_many (synchronises `stream`). */
+svdag_status svdag_edit_records(svdag_ctx* ctx, svdag_edit_record* out, uint32_t count, void* stream);
 /* Copies the counters of the most recent edit to the host (synchronises `stream`). */
 svdag_status svdag_last_edit_stats(svdag_ctx* ctx, svdag_edit_stats* out, void* stream);
 

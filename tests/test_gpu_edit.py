@@ -129,3 +129,48 @@ def test_trace_misses_and_empty_dag(svdag_lib, oracle_mod):
     o.build_terrain(oracle_mod.TerrainParams(**TERRAIN))
     compare_hits(gpu_trace(svdag_lib, g, p), o.trace(po))
     g.free()
+
+
+def test_batched_form_equals_sequential(svdag_lib, oracle_mod):
+    """One persistent launch over a mixed batch gives the same DAG as the oracle applying the same
+    edits one by one, and per-edit records match the oracle's per-edit counters."""
+    levels = 8
+    g, o = make_pair(svdag_lib, oracle_mod, levels)
+    rng = np.random.default_rng(77)
+    batch, oracle_edits = [], []
+    for i, (tool, mat, c, r) in enumerate(sphere_edits(oracle_mod, levels, 24, seed=13, rmin=2, rmax=24, near=10)):
+        kind = i % 6
+        kw = {}
+        if kind == 2:
+            tool = 2 if rng.integers(0, 2) else 3  # box add / remove
+        elif kind == 3:
+            tool = 4  # sphere paint
+        elif kind == 4:
+            tool, kw = 6, {"noise_seed": 5, "noise_cell_log2": 2}
+        elif kind == 5:
+            tool, kw = (5 if rng.integers(0, 2) else 7), {"src": c, "dst": (c[0] + 9.0, c[1] + 3.0, c[2] - 7.0)}
+        batch.append(to_svdag_edit(svdag_lib, tool, mat, c, r, **kw))
+        oracle_edits.append(to_oracle_edit(oracle_mod, tool, mat, c, r, **kw))
+    nrec = g.edit_batch(batch)
+    recs = g.edit_records(nrec)
+    ri = 0
+    for e in oracle_edits:
+        if e.tool == 7:  # a move is a removal then a paste: compare the final DAG only
+            o.edit(e)
+            ri += 2
+            continue
+        st = o.edit(e)
+        assert recs[ri].status == 0
+        assert recs[ri].edited_voxels == st.edited_voxels, ri
+        assert recs[ri].new_items == st.new_items, ri
+        assert recs[ri].unique_items == st.unique_items, ri
+        assert recs[ri].svo_items == sum(st.svo_nodes), ri
+        ri += 1
+    assert ri == nrec
+    g.sync()
+    assert gpu_canon(oracle_mod, g) == o.canon()
+    # the undo history holds one frame per edit (two per move), as with single calls
+    g.undo()
+    o.undo()
+    assert gpu_canon(oracle_mod, g) == o.canon()
+    g.free()
