@@ -2,7 +2,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
+#include <mutex>
 
 #include "svdag_host.hpp"
 
@@ -426,6 +428,81 @@ svdag_status svdag_table_find_or_add(svdag_table* t, const uint32_t* keys, const
     SVDAG_CUDA(cudaGetLastError());
     return SVDAG_OK;
 }
+
+} // extern "C"
+
+// ---------------------------------------------------------------- allocation-free find-or-add
+// Some callers cannot allocate GPU memory while they run: code recording a CUDA graph, real-time
+// loops that must not hit the driver's allocator, or hosts whose memory is owned by another runtime.
+// This entry point does the same work as svdag_table_find_or_add, but its dedup scratch is a fixed
+// array compiled into the library instead of the context's arena, so a call allocates nothing.
+// The array lives in every GPU that loads the library until the process exits.
+
+constexpr uint32_t kStaticMaxKeys = 65536; // largest batch the fixed scratch holds
+constexpr uint32_t kStaticTableEntries = 2 * kStaticMaxKeys; // open-addressing entries (power of two)
+constexpr size_t kStaticScratchBytes = kStaticTableEntries * sizeof(unsigned long long) + kStaticMaxKeys * sizeof(uint32_t);
+
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+namespace {
+std::mutex g_static_mutex;
+void* g_static_ptr[64] = {}; // device address of g_static_scratch, per device ordinal
+
+// The symbol's device address, looked up once per device with that device current.
+svdag_status static_scratch(int device, unsigned char** out)
+{
+    if (device < 0 || device >= 64)
+        return SVDAG_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(g_static_mutex);
+    if (!g_static_ptr[device]) {
+        int prev = 0;
+        SVDAG_CUDA(cudaGetDevice(&prev));
+        if (prev != device)
+            SVDAG_CUDA(cudaSetDevice(device));
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (prev != device)
+            cudaSetDevice(prev);
+        if (e != cudaSuccess)
+            return cuda_status(e);
+        g_static_ptr[device] = p;
+    }
+    *out = static_cast<unsigned char*>(g_static_ptr[device]);
+    return SVDAG_OK;
+}
+} // namespace
+
+extern "C" svdag_status svdag_table_find_or_add_static(svdag_table* t, const uint32_t* keys, const uint32_t* offsets, uint32_t n,
+    uint64_t totalWords, uint32_t* handles, uint32_t lanes, void* stream)
+{
+    if (!valid_table(t) || (n && (!keys || !offsets || !handles)))
+        return SVDAG_ERR_INVALID;
+    if (n > kStaticMaxKeys) {
+        std::fprintf(stderr, "svdag_table_find_or_add_static: %u keys exceed the fixed scratch limit of %u keys\n", n, kStaticMaxKeys);
+        return SVDAG_ERR_INVALID;
+    }
+    if (!n)
+        return SVDAG_OK;
+    svdag_ctx* ctx = t->ctx;
+    unsigned char* base = nullptr;
+    SVDAG_TRY(static_scratch(ctx->device, &base));
+    cudaStream_t s = as_stream(stream);
+    uint32_t cap = 2;
+    while (cap < 2ull * n)
+        cap <<= 1; // <= kStaticTableEntries because n <= kStaticMaxKeys
+    auto* table = reinterpret_cast<unsigned long long*>(base);
+    auto* reps = reinterpret_cast<uint32_t*>(base + kStaticTableEntries * sizeof(unsigned long long));
+    // The array keeps the previous call's contents: the probe table must start empty.
+    SVDAG_CUDA(cudaMemsetAsync(table, 0, (size_t)cap * sizeof(unsigned long long), s));
+    k_batch_dedup<<<grid_for(ctx, n, 256), 256, 0, s>>>(keys, offsets, n, totalWords, t->dev.kind, table, cap - 1, reps, ctx->ctl);
+    SVDAG_CUDA(cudaGetLastError());
+    SVDAG_TRY(launch_table_op<OP_FIND_OR_INSERT>(t, keys, offsets, n, totalWords, reps, handles, lanes, s));
+    k_gather<<<grid_for(ctx, n, 256), 256, 0, s>>>(reps, n, handles);
+    SVDAG_CUDA(cudaGetLastError());
+    return SVDAG_OK;
+}
+
+extern "C" {
 
 svdag_status svdag_table_read(svdag_table* t, const uint32_t* handles, uint32_t n, uint32_t* out, void* stream)
 {

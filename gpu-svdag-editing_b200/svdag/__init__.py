@@ -131,6 +131,7 @@ _PROTOS = {
     "svdag_table_add": [_P, _P, _P, _U32, _U64, _P, _U32, _P],
     "svdag_table_find": [_P, _P, _P, _U32, _U64, _P, _U32, _P],
     "svdag_table_find_or_add": [_P, _P, _P, _U32, _U64, _P, _U32, _P],
+    "svdag_table_find_or_add_static": [_P, _P, _P, _U32, _U64, _P, _U32, _P],
     "svdag_table_read": [_P, _P, _U32, _P, _P],
     "svdag_table_get_stats": [_P, C.POINTER(TableStats), _P],
     "svdag_get_stats": [_P, C.POINTER(Stats), _P],
@@ -390,6 +391,11 @@ class HashTable:
 
     def find_or_add(self, keys, offsets, count, total_words, out, lanes=0, stream=None):
         self._op(lib().svdag_table_find_or_add, keys, offsets, count, total_words, out, lanes, stream)
+
+    def find_or_add_static(self, keys, offsets, count, total_words, out, lanes=0, stream=None):
+        """find_or_add without any allocation: scratch is a fixed array inside the library
+        (at most 65536 keys per call; calls that overlap on the GPU must be serialised)."""
+        self._op(lib().svdag_table_find_or_add_static, keys, offsets, count, total_words, out, lanes, stream)
 
     def read(self, handles, count, out_words, stream=None):
         _check(lib().svdag_table_read(self.h, ptr(handles), count, ptr(out_words), stream_ptr(stream)),

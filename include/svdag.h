@@ -244,6 +244,18 @@ svdag_status svdag_table_find(svdag_table* table, const uint32_t* keys_dev, cons
 svdag_status svdag_table_find_or_add(svdag_table* table, const uint32_t* keys_dev,
     const uint32_t* offsets_dev, uint32_t count, uint64_t total_words, uint32_t* handles_dev,
     uint32_t lanes, void* stream);
+/* Allocation-free form of svdag_table_find_or_add, with no counterpart in the reference. It is for
+ * callers that must not allocate GPU memory during the call (for example while recording a CUDA graph,
+ * or inside a real-time loop that may not reach the driver's allocator): its dedup scratch is a fixed
+ * 1.25 MiB array compiled into the library, which every GPU that loads the library keeps until the
+ * process exits. At most 65536 keys per call; larger batches are rejected with SVDAG_ERR_INVALID.
+ * The first call on a device looks up the array's address (with that device made current), so make
+ * that first call before any stream capture. All calls share the one array: calls whose work
+ * overlaps on the GPU (different streams, or different contexts on the same device) race on it and
+ * must be serialised by the caller. Results are the same as svdag_table_find_or_add's. */
+svdag_status svdag_table_find_or_add_static(svdag_table* table, const uint32_t* keys_dev,
+    const uint32_t* offsets_dev, uint32_t count, uint64_t total_words, uint32_t* handles_dev,
+    uint32_t lanes, void* stream);
 /* decodePointer (compact_acceleration_hash_table.h:398-402): copies the words of each handle into
  * out_words_dev[i * SVDAG_MAX_ITEM_WORDS ...], zero padded. */
 svdag_status svdag_table_read(svdag_table* table, const uint32_t* handles_dev, uint32_t count,
