@@ -459,7 +459,7 @@ def run_mode_edit(args):
     dag.build_terrain(**TERRAIN)
     params = svdag.get_trace_params((512.0, 900.0, 512.0), (512.0, 512.0, 512.0), FRAME, FRAME)
     hits = torch.empty(FRAME * FRAME * 68, dtype=torch.uint8, device="cuda")
-    te, tt = [], []
+    te, tt, phases = [], [], []
     for i in range(args.warmup + args.steps):
         tool, mat, c, r = edits[i % len(edits)]
         e = svdag.Edit(tool=tool, material=mat)
@@ -475,9 +475,11 @@ def run_mode_edit(args):
         if i >= args.warmup:
             te.append(a.elapsed_time(b))
             tt.append(b.elapsed_time(d))
+            pt = dag.last_edit_phase_times()
+            phases.append([round(float(x - pt[0]) / 1e3, 2) for x in pt])
     dag.sync()
     print(json.dumps({"edit_ms_median": statistics.median(te), "trace_ms_median": statistics.median(tt),
-                      "edit_ms": te, "trace_ms": tt}))
+                      "edit_ms": te, "trace_ms": tt, "phase_us": phases[:4]}))
 
 
 def main():

@@ -71,6 +71,9 @@ struct Control {
     uint32_t fullyFilled[kMaxLevels][SVDAG_NUM_MATERIALS];
     DevTable tables[kMaxLevels]; // the level tables (copied here by the host whenever they change)
     EditCounters edit;
+    unsigned long long phaseTimes[64]; // GPU global-timer stamps at the phase barriers of the last fused edit
+    uint32_t phaseCount;
+    uint32_t pad1;
 };
 
 struct DevDag {
@@ -198,16 +201,30 @@ struct Key {
     uint32_t ha, hb; // bucket hash, tag hash
 };
 
+// Load flavours: default caching, L2 only (__ldcg: coherent with other SMs' stores of the same
+// launch) and streaming (__ldcs: evict-first in L1 and L2, for data read once).
+enum : int { LD_DEFAULT = 0, LD_L2 = 1, LD_STREAM = 2 };
+template <int MODE>
+__device__ __forceinline__ uint32_t ld(const uint32_t* p)
+{
+    if constexpr (MODE == LD_L2)
+        return __ldcg(p);
+    else if constexpr (MODE == LD_STREAM)
+        return __ldcs(p);
+    else
+        return *p;
+}
+
 // Loads a self-describing key (node or leaf) of at most 10 words; `limit` bounds the readable words.
-template <int G>
+template <int G, int MODE = LD_DEFAULT>
 __device__ __forceinline__ void load_key(const Grp<G>& g, const uint32_t* p, unsigned long long limit, uint32_t kind, Key<G>& key)
 {
     uint32_t w0 = 0, w1 = 0;
     if constexpr (G == 1) {
-        w0 = limit > 0 ? p[0] : 0u;
-        w1 = limit > 1 ? p[1] : 0u;
+        w0 = limit > 0 ? ld<MODE>(p) : 0u;
+        w1 = limit > 1 ? ld<MODE>(p + 1) : 0u;
     } else {
-        uint32_t v = (g.lane < 2 && g.lane < limit) ? p[g.lane] : 0u;
+        uint32_t v = (g.lane < 2 && g.lane < limit) ? ld<MODE>(p + g.lane) : 0u;
         w0 = g.bcast(v, 0);
         w1 = g.bcast(v, 1);
     }
@@ -218,7 +235,7 @@ __device__ __forceinline__ void load_key(const Grp<G>& g, const uint32_t* p, uns
         const uint32_t idx = g.lane + uint32_t(i) * G;
         uint32_t v = 0;
         if (idx < key.n && idx < limit)
-            v = p[idx];
+            v = (G == 1 && idx < 2) ? (idx == 0 ? w0 : w1) : ld<MODE>(p + idx);
         key.w[i] = v;
         if (idx < key.n) {
             a ^= word_hash_a(v, idx);
@@ -233,9 +250,12 @@ __device__ __forceinline__ void load_key(const Grp<G>& g, const uint32_t* p, uns
 __device__ __forceinline__ void hash_words(const uint32_t* w, uint32_t n, uint32_t& ha, uint32_t& hb)
 {
     uint32_t a = 0, b = 0;
-    for (uint32_t i = 0; i < n; ++i) {
-        a ^= word_hash_a(w[i], i);
-        b ^= word_hash_b(w[i], i);
+#pragma unroll
+    for (uint32_t i = 0; i < kItemStride; ++i) { // fixed trip count keeps w[] in registers
+        if (i < n) {
+            a ^= word_hash_a(w[i], i);
+            b ^= word_hash_b(w[i], i);
+        }
     }
     ha = a;
     hb = b;
@@ -298,7 +318,7 @@ __device__ __forceinline__ uint32_t probe_header(const Grp<G>& g, const uint32_t
 }
 
 // Compares the key with the item at `item`; all lanes of the group get the same answer.
-template <int G, bool CG = false>
+template <int G, int MODE = LD_DEFAULT>
 __device__ __forceinline__ bool item_equals(const Grp<G>& g, const uint32_t* item, const Key<G>& key)
 {
     bool eq = true;
@@ -306,7 +326,7 @@ __device__ __forceinline__ bool item_equals(const Grp<G>& g, const uint32_t* ite
     for (int i = 0; i < Grp<G>::KW; ++i) {
         const uint32_t idx = g.lane + uint32_t(i) * G;
         if (idx < key.n)
-            eq &= (CG ? __ldcg(item + idx) : item[idx]) == key.w[i];
+            eq &= ld<MODE>(item + idx) == key.w[i];
     }
     return g.all(eq);
 }
@@ -369,6 +389,7 @@ struct Spare {
 constexpr uint32_t kMaxChain = 1u << 14; // bound on chain walks (16K slabs in one bucket only happens on a corrupt chain)
 
 // Read-only lookup (CompactAccelerationHashTable::findAsWarp, compact_acceleration_hash_table.h:233-280).
+// Candidate items are streamed (read once) so that the slab header sectors stay resident in L2.
 template <int G>
 __device__ __forceinline__ uint32_t table_find(const Grp<G>& g, const DevDag& d, const DevTable& t, const Key<G>& key)
 {
@@ -388,7 +409,7 @@ __device__ __forceinline__ uint32_t table_find(const Grp<G>& g, const DevDag& d,
             const uint32_t s = __ffs(cand) - 1u;
             cand &= cand - 1u;
             const uint32_t item = slab + kHeaderWords + s * key.n;
-            if (item_equals<G>(g, d.items + item, key))
+            if (item_equals<G, LD_STREAM>(g, d.items + item, key))
                 return item;
         }
         if (next == kEnd)
@@ -506,7 +527,7 @@ __device__ __forceinline__ uint32_t table_find_or_insert(const Grp<G>& g, const 
             const uint32_t s = __ffs(cand) - 1u;
             cand &= cand - 1u;
             const uint32_t item = slab + kHeaderWords + s * key.n;
-            if (item_equals<G, true>(g, d.items + item, key))
+            if (item_equals<G, LD_L2>(g, d.items + item, key))
                 return item;
         }
         tail = slab;

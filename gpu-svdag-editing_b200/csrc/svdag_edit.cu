@@ -460,7 +460,12 @@ __device__ void ph_build_leaves(const DevDag& d, const DevEditor& e, char* scrat
     if (E.overflow || n == 0)
         return;
     // Reserve and clear the dedup tables of every level for the bottom-up phase.
-    const MergeLayout top = merge_layout(E.count, buildTop, 0, LL);
+    // The dedup tables of all levels form one contiguous run per level; walk the layout once (from
+    // the leaf level up, the order merge_layout assigns) instead of recomputing it per level.
+    uint32_t cnt[kMaxLevels];
+    for (uint32_t l = 0; l <= LL; ++l)
+        cnt[l] = E.count[l];
+    const MergeLayout top = merge_layout(cnt, buildTop, 0, LL);
     if (top.end > scratchBytes) {
         if (threadIdx.x == 0)
             atomicExch(&E.overflow, 1u);
@@ -468,11 +473,19 @@ __device__ void ph_build_leaves(const DevDag& d, const DevEditor& e, char* scrat
     }
     const unsigned long long tid = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
     const unsigned long long nthreads = (unsigned long long)gridDim.x * blockDim.x;
-    for (uint32_t l = 0; l <= LL; ++l) {
-        const MergeLayout m = merge_layout(E.count, buildTop, l, LL);
-        uint4* t = reinterpret_cast<uint4*>(scratch + m.table);
-        for (unsigned long long j = tid; j < m.cap / 2; j += nthreads)
-            t[j] = make_uint4(0, 0, 0, 0);
+    {
+        unsigned long long off = buildTop;
+        for (int l = (int)LL; l >= 0; --l) {
+            const unsigned long long nl = cnt[l];
+            uint32_t cap = 2;
+            while (cap < 2ull * nl)
+                cap <<= 1;
+            const unsigned long long table = align256(align256(off + 4 * nl) + 4 * nl);
+            uint4* t = reinterpret_cast<uint4*>(scratch + table);
+            for (unsigned long long j = tid; j < cap / 2; j += nthreads)
+                t[j] = make_uint4(0, 0, 0, 0);
+            off = align256(table + 8ull * cap);
+        }
     }
 
     const uint32_t lane = threadIdx.x & 31u;
@@ -626,7 +639,105 @@ __device__ __forceinline__ bool merge_live(const DevDag& d)
     return E.count[d.leafLevel] != 0 && !E.overflow;
 }
 
-// updateChildPointers + discover_fully_filled (my_gpu_hash_dag_edits.cu:44-150), thread per node.
+// Discovery at `level` runs only if it ran one level down (always at the leaf level) and found
+// fully-filled items there (my_gpu_hash_dag_edits.cu:337-351, hasFullyFilledNodes starts true at :589).
+__device__ __forceinline__ bool discovery_gate(const EditCounters& E, uint32_t level, uint32_t LL, uint32_t builder)
+{
+    if (builder)
+        return true;
+    const bool ranBelow = (level + 1 == LL) || E.ffRan[level + 1] != 0;
+    return ranBelow && E.ffCount[level + 1] > 0;
+}
+
+// updateChildPointers + discover_fully_filled for one node held in registers
+// (my_gpu_hash_dag_edits.cu:44-150). Returns true when the node was found fully filled.
+__device__ __forceinline__ bool fix_node(const DevDag& d, uint32_t level, bool gate, const uint32_t* repC, const uint32_t* hC,
+    uint32_t* w)
+{
+    const uint32_t LL = d.leafLevel;
+    uint32_t mask = w[0] & 0xFFu;
+    const uint32_t interm = w[0] >> 13;
+    uint32_t outW[8];
+    uint32_t in = 1, out = 0;
+    for (uint32_t c = 0; c < 8; ++c) {
+        if (!(mask & (1u << c)))
+            continue;
+        uint32_t h = w[in++];
+        if (interm & (1u << c)) {
+            const uint32_t r = repC[h];
+            h = r == kEmptyRep ? kNone : hC[r];
+        } else if (h >= kFillMarker && h != kNone) {
+            h = d.ctl->fullyFilled[level + 1][h & 0xFu];
+        }
+        if (h != kNone)
+            outW[out++] = h;
+        else
+            mask ^= 1u << c;
+    }
+    uint32_t header = mask;
+    bool full = false;
+    if (gate && mask == 0xFFu) {
+        bool all = true;
+        uint32_t mat = 0;
+        for (uint32_t c = 0; c < 8 && all; ++c) {
+            const uint32_t* p = item_ptr(d, outW[c]);
+            uint32_t cm;
+            if (level + 1 == LL) {
+                all = p[0] == 0xFFFFFFFFu && p[1] == 0xFFFFFFFFu;
+                cm = p[2] & 0xFu;
+                for (uint32_t j = 2; j < 10 && all; ++j)
+                    all = p[j] == cm * 0x11111111u;
+            } else {
+                const uint32_t hh = p[0];
+                all = (hh >> 8) & 1u;
+                cm = (hh >> 9) & 0xFu;
+            }
+            if (c == 0)
+                mat = cm;
+            all = all && cm == mat;
+        }
+        if (all) {
+            header = 0xFFu | (1u << 8) | (mat << 9);
+            full = true;
+        }
+    }
+    w[0] = header;
+    for (uint32_t j = 0; j < 8; ++j)
+        w[1 + j] = j < out ? outW[j] : 0u;
+    w[9] = 0;
+    return full;
+}
+
+// Inserts item i into the level's open-addressing dedup table and returns its representative. Other
+// items are read through L2 (__ldcg): in the fused merge phase they were rewritten in this launch.
+__device__ __forceinline__ uint32_t dedup_item(unsigned long long* table, uint32_t capMask, const uint32_t* items, uint32_t i,
+    const uint32_t* w, uint32_t nw, uint32_t ha, uint32_t hb)
+{
+    const unsigned long long entry = ((unsigned long long)hb << 32) | (unsigned long long)(i + 1u);
+    uint32_t slot = ha & capMask;
+    for (uint32_t probe = 0; probe <= capMask; ++probe) {
+        unsigned long long e = __ldcg(&table[slot]);
+        if (e == 0) {
+            e = atomicCAS(&table[slot], 0ull, entry);
+            if (e == 0)
+                return i;
+        }
+        if ((uint32_t)(e >> 32) == hb) {
+            const uint32_t j = (uint32_t)e - 1u;
+            const uint32_t* q = items + (size_t)j * kItemStride;
+            bool same = true;
+#pragma unroll
+            for (uint32_t k = 0; k < kItemStride; ++k)
+                if (k < nw)
+                    same &= __ldcg(q + k) == w[k];
+            if (same)
+                return j;
+        }
+        slot = (slot + 1u) & capMask;
+    }
+    return i;
+}
+
 __device__ void ph_fix_level(const DevDag& d, uint32_t level, uint32_t builder, char* scratch)
 {
     EditCounters& E = d.ctl->edit;
@@ -634,13 +745,7 @@ __device__ void ph_fix_level(const DevDag& d, uint32_t level, uint32_t builder, 
         return;
     const uint32_t LL = d.leafLevel;
     const uint32_t n = E.count[level];
-    // Discovery at this level runs only if it ran one level down (always at the leaf level) and found
-    // fully-filled items there (my_gpu_hash_dag_edits.cu:337-351, hasFullyFilledNodes starts true at :589).
-    bool gate = true;
-    if (!builder) {
-        const bool ranBelow = (level + 1 == LL) || E.ffRan[level + 1] != 0;
-        gate = ranBelow && E.ffCount[level + 1] > 0;
-    }
+    const bool gate = discovery_gate(E, level, LL, builder);
     if (blockIdx.x == 0 && threadIdx.x == 0)
         E.ffRan[level] = gate ? 1u : 0u;
     const MergeLayout ch = merge_layout(E.count, E.buildTop, level + 1, LL);
@@ -654,55 +759,10 @@ __device__ void ph_fix_level(const DevDag& d, uint32_t level, uint32_t builder, 
 #pragma unroll
         for (uint32_t j = 0; j < kItemStride; ++j)
             w[j] = node[j];
-        uint32_t mask = w[0] & 0xFFu;
-        const uint32_t interm = w[0] >> 13;
-        uint32_t outW[8];
-        uint32_t in = 1, out = 0;
-        for (uint32_t c = 0; c < 8; ++c) {
-            if (!(mask & (1u << c)))
-                continue;
-            uint32_t h = w[in++];
-            if (interm & (1u << c)) {
-                const uint32_t r = repC[h];
-                h = r == kEmptyRep ? kNone : hC[r];
-            } else if (h >= kFillMarker && h != kNone) {
-                h = d.ctl->fullyFilled[level + 1][h & 0xFu];
-            }
-            if (h != kNone)
-                outW[out++] = h;
-            else
-                mask ^= 1u << c;
-        }
-        uint32_t header = mask;
-        if (gate && mask == 0xFFu) {
-            bool all = true;
-            uint32_t mat = 0;
-            for (uint32_t c = 0; c < 8 && all; ++c) {
-                const uint32_t* p = item_ptr(d, outW[c]);
-                uint32_t cm;
-                if (level + 1 == LL) {
-                    all = p[0] == 0xFFFFFFFFu && p[1] == 0xFFFFFFFFu;
-                    cm = p[2] & 0xFu;
-                    for (uint32_t j = 2; j < 10 && all; ++j)
-                        all = p[j] == cm * 0x11111111u;
-                } else {
-                    const uint32_t hh = p[0];
-                    all = (hh >> 8) & 1u;
-                    cm = (hh >> 9) & 0xFu;
-                }
-                if (c == 0)
-                    mat = cm;
-                all = all && cm == mat;
-            }
-            if (all) {
-                header = 0xFFu | (1u << 8) | (mat << 9);
-                ++full;
-            }
-        }
-        node[0] = header;
-        for (uint32_t j = 0; j < 8; ++j)
-            node[1 + j] = j < out ? outW[j] : 0u;
-        node[9] = 0;
+        full += fix_node(d, level, gate, repC, hC, w) ? 1u : 0u;
+#pragma unroll
+        for (uint32_t j = 0; j < kItemStride; ++j)
+            node[j] = w[j];
     }
     if (full)
         atomicAdd(&E.ffCount[level], full);
@@ -722,7 +782,6 @@ __device__ void ph_dedup_level(const DevDag& d, uint32_t level, char* scratch)
     uint32_t* rep = reinterpret_cast<uint32_t*>(scratch + m.rep);
     unsigned long long* table = reinterpret_cast<unsigned long long*>(scratch + m.table);
     const uint32_t* items = reinterpret_cast<const uint32_t*>(scratch + E.offN[level]);
-    const uint32_t capMask = m.cap - 1u;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t* it = items + (size_t)i * kItemStride;
         uint32_t w[kItemStride];
@@ -737,34 +796,77 @@ __device__ void ph_dedup_level(const DevDag& d, uint32_t level, char* scratch)
         const uint32_t nw = level == LL ? dev_leaf_words(w[0], w[1]) : dev_node_words(w[0]);
         uint32_t ha, hb;
         hash_words(w, nw, ha, hb);
-        const unsigned long long entry = ((unsigned long long)hb << 32) | (unsigned long long)(i + 1u);
-        uint32_t slot = ha & capMask, r = i;
-        for (uint32_t probe = 0; probe <= capMask; ++probe) {
-            unsigned long long e = table[slot];
-            if (e == 0) {
-                e = atomicCAS(&table[slot], 0ull, entry);
-                if (e == 0)
-                    break;
-            }
-            if ((uint32_t)(e >> 32) == hb) {
-                const uint32_t j = (uint32_t)e - 1u;
-                const uint32_t* q = items + (size_t)j * kItemStride;
-                bool same = true;
-                for (uint32_t k = 0; k < nw && same; ++k)
-                    same = q[k] == w[k];
-                if (same) {
-                    r = j;
-                    break;
-                }
-            }
-            slot = (slot + 1u) & capMask;
-        }
+        const uint32_t r = dedup_item(table, m.cap - 1u, items, i, w, nw, ha, hb);
         rep[i] = r;
         if (r == i) {
             atomicAdd(&E.repCount[level], 1u);
             atomicAdd(&E.repPerClass[level][nw - 2], 1u);
         }
     }
+}
+
+// One bottom-up level in a single pass (used by edits): child fix-up and gated discovery, intra-level
+// dedup, and find-or-insert of the representative in the level table. Duplicates only record their
+// representative; the parent level reads the representative's handle after the next barrier.
+__device__ void ph_merge_level(const DevDag& d, uint32_t level, char* scratch)
+{
+    EditCounters& E = d.ctl->edit;
+    if (!merge_live(d))
+        return;
+    const uint32_t LL = d.leafLevel;
+    const uint32_t n = E.count[level];
+    const bool isLeaf = level == LL;
+    const bool gate = isLeaf ? false : discovery_gate(E, level, LL, 0);
+    if (!isLeaf && blockIdx.x == 0 && threadIdx.x == 0)
+        E.ffRan[level] = gate ? 1u : 0u;
+    const MergeLayout m = merge_layout(E.count, E.buildTop, level, LL);
+    const MergeLayout ch = isLeaf ? m : merge_layout(E.count, E.buildTop, level + 1, LL);
+    const uint32_t* repC = reinterpret_cast<const uint32_t*>(scratch + ch.rep);
+    const uint32_t* hC = reinterpret_cast<const uint32_t*>(scratch + ch.handle);
+    uint32_t* rep = reinterpret_cast<uint32_t*>(scratch + m.rep);
+    uint32_t* handle = reinterpret_cast<uint32_t*>(scratch + m.handle);
+    unsigned long long* table = reinterpret_cast<unsigned long long*>(scratch + m.table);
+    uint32_t* items = reinterpret_cast<uint32_t*>(scratch + E.offN[level]);
+    const DevTable t = d.ctl->tables[level];
+    Grp<1> g;
+    Spare spare;
+    uint32_t full = 0, reps = 0, added = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t* it = items + (size_t)i * kItemStride;
+        Key<1> key;
+#pragma unroll
+        for (uint32_t j = 0; j < kItemStride; ++j)
+            key.w[j] = it[j];
+        if (!isLeaf) {
+            full += fix_node(d, level, gate, repC, hC, key.w) ? 1u : 0u;
+#pragma unroll
+            for (uint32_t j = 0; j < kItemStride; ++j)
+                it[j] = key.w[j];
+            __threadfence(); // the content is visible before the dedup entry that points at it
+        }
+        const bool isEmpty = isLeaf ? (key.w[0] == 0 && key.w[1] == 0) : ((key.w[0] & 0xFFu) == 0);
+        if (isEmpty) {
+            rep[i] = kEmptyRep;
+            continue;
+        }
+        key.n = isLeaf ? dev_leaf_words(key.w[0], key.w[1]) : dev_node_words(key.w[0]);
+        hash_words(key.w, key.n, key.ha, key.hb);
+        const uint32_t r = dedup_item(table, m.cap - 1u, items, i, key.w, key.n, key.ha, key.hb);
+        rep[i] = r;
+        if (r != i)
+            continue;
+        ++reps;
+        atomicAdd(&E.repPerClass[level][key.n - 2], 1u);
+        bool ins = false;
+        handle[i] = table_find_or_insert<1>(g, d, t, key, spare, ins);
+        added += ins ? 1u : 0u;
+    }
+    if (full)
+        atomicAdd(&E.ffCount[level], full);
+    if (reps)
+        atomicAdd(&E.repCount[level], reps);
+    if (added)
+        atomicAdd(&E.added, (unsigned long long)added);
 }
 
 // Find-or-insert of each representative into the level table (findUniqueInHashTableAsWarp_kernel2 +
@@ -859,6 +961,7 @@ __global__ void __launch_bounds__(256) k_fix_level(DevDag d, uint32_t level, uin
     ph_fix_level(d, level, builder, scratch);
 }
 __global__ void __launch_bounds__(256) k_dedup_level(DevDag d, uint32_t level, char* scratch) { ph_dedup_level(d, level, scratch); }
+__global__ void __launch_bounds__(256) k_merge_level(DevDag d, uint32_t level, char* scratch) { ph_merge_level(d, level, scratch); }
 template <int G>
 __global__ void __launch_bounds__(256) k_insert_level(DevDag d, DevTable t, uint32_t level, char* scratch)
 {
@@ -871,33 +974,45 @@ __global__ void k_edit_end(DevDag d, char* scratch, uint32_t builder) { ph_edit_
 // device-resident counts, separated by grid-wide barriers instead of kernel boundaries. All
 // threads reach every barrier (phases only return early, never skip a barrier).
 
+__device__ __forceinline__ void stamp(const DevDag& d, uint32_t& k)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        unsigned long long t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        if (k < 64)
+            d.ctl->phaseTimes[k] = t;
+        d.ctl->phaseCount = ++k;
+    }
+}
+
 template <uint32_t TOOL>
 __device__ __forceinline__ void fused_edit(cg::grid_group& grid, const DevDag& d, const DevEditor& ed, char* scratch,
     unsigned long long scratchBytes, EditRecord* record)
 {
     const uint32_t LL = d.leafLevel;
+    uint32_t k = 0;
+    stamp(d, k);
     ph_reset_counters(d);
     grid.sync();
     ph_edit_begin(d, ed, scratch);
     grid.sync();
+    stamp(d, k);
     for (uint32_t level = 0; level < LL; ++level) {
         ph_build_level<TOOL>(d, ed, level, scratch, scratchBytes);
         grid.sync();
+        stamp(d, k);
     }
     ph_build_leaves<TOOL>(d, ed, scratch, scratchBytes);
     grid.sync();
+    stamp(d, k);
     for (int level = (int)LL; level >= 0; --level) {
-        if (level < (int)LL) {
-            ph_fix_level(d, (uint32_t)level, ed.builder, scratch);
-            grid.sync();
-        }
-        ph_dedup_level(d, (uint32_t)level, scratch);
+        ph_merge_level(d, (uint32_t)level, scratch);
         grid.sync();
-        ph_insert_level<1>(d, d.ctl->tables[level], (uint32_t)level, scratch);
-        grid.sync();
+        stamp(d, k);
     }
     ph_edit_end(d, scratch, ed.builder, record);
     grid.sync();
+    stamp(d, k);
 }
 
 __global__ void __launch_bounds__(256) k_edit_fused(DevDag d, DevEditor single, const DevEditor* eds, uint32_t numEdits, char* scratch,
@@ -1088,12 +1203,8 @@ svdag_status launch_pipeline(svdag_ctx* ctx, const DevEditor& ed, cudaStream_t s
     k_edit_begin<<<1, 32, 0, s>>>(d, ed, ctx->scratch);
     SVDAG_TRY(launch_build_any(ctx, ed, s));
     const uint32_t LL = d.leafLevel;
-    for (int level = (int)LL; level >= 0; --level) {
-        if (level < (int)LL)
-            k_fix_level<<<grid_for(ctx, level_bound(level), 256), 256, 0, s>>>(d, level, 0, ctx->scratch);
-        k_dedup_level<<<grid_for(ctx, level_bound(level), 256), 256, 0, s>>>(d, level, ctx->scratch);
-        SVDAG_TRY(launch_insert(ctx, level, level_bound(level), s));
-    }
+    for (int level = (int)LL; level >= 0; --level)
+        k_merge_level<<<grid_for(ctx, level_bound(level), 256), 256, 0, s>>>(d, level, ctx->scratch);
     k_edit_end<<<1, 32, 0, s>>>(d, ctx->scratch, 0);
     SVDAG_CUDA(cudaGetLastError());
     return SVDAG_OK;
@@ -1408,6 +1519,23 @@ svdag_status svdag_edit_copy(svdag_ctx* ctx, const float src[3], const float dst
     }
     e.radius = radius;
     return svdag_edit_apply(ctx, &e, stream);
+}
+
+svdag_status svdag_last_edit_phase_times(svdag_ctx* ctx, uint64_t* out_ns, uint32_t capacity, uint32_t* out_count, void* stream)
+{
+    if (!ctx || !out_count || (capacity && !out_ns))
+        return SVDAG_ERR_INVALID;
+    cudaStream_t s = as_stream(stream);
+    unsigned long long t[64];
+    uint32_t n = 0;
+    SVDAG_CUDA(cudaMemcpyAsync(t, ctx->ctl->phaseTimes, sizeof(t), cudaMemcpyDeviceToHost, s));
+    SVDAG_CUDA(cudaMemcpyAsync(&n, &ctx->ctl->phaseCount, sizeof(n), cudaMemcpyDeviceToHost, s));
+    SVDAG_CUDA(cudaStreamSynchronize(s));
+    n = std::min<uint32_t>(n, 64);
+    *out_count = n;
+    for (uint32_t i = 0; i < n && i < capacity; ++i)
+        out_ns[i] = t[i];
+    return SVDAG_OK;
 }
 
 svdag_status svdag_undo(svdag_ctx* ctx, void* stream)

@@ -114,6 +114,7 @@ _PROTOS = {
     "svdag_edit_apply_many": [_P, C.POINTER(Edit), _U32, _P],
     "svdag_last_edit_stats": [_P, C.POINTER(EditStats), _P],
     "svdag_edit_records": [_P, C.POINTER(EditRecord), _U32, _P],
+    "svdag_last_edit_phase_times": [_P, _P, _U32, C.POINTER(_U32), _P],
     "svdag_edit_sphere": [_P, C.c_float, C.c_float, C.c_float, C.c_float, _U32, C.c_int, _P],
     "svdag_edit_box": [_P, C.c_float, C.c_float, C.c_float, C.c_float, _U32, C.c_int, _P],
     "svdag_edit_paint": [_P, C.c_float, C.c_float, C.c_float, C.c_float, _U32, _P],
@@ -316,6 +317,14 @@ class MyGPUHashDAG:
         out = (EditRecord * count)()
         _check(lib().svdag_edit_records(self.h, out, count, stream_ptr(stream)), "svdag_edit_records")
         return list(out)
+
+    def last_edit_phase_times(self, stream=None):
+        """GPU timestamps (ns) at the phase barriers of the last persistent-kernel edit."""
+        buf = np.zeros(64, dtype=np.uint64)
+        n = C.c_uint32()
+        _check(lib().svdag_last_edit_phase_times(self.h, buf.ctypes.data, 64, C.byref(n), stream_ptr(stream)),
+               "svdag_last_edit_phase_times")
+        return buf[: n.value].copy()
 
     def last_edit_stats(self, stream=None) -> EditStats:
         st = EditStats()

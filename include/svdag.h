@@ -160,6 +160,13 @@ svdag_status svdag_edit_records(svdag_ctx* ctx, svdag_edit_record* out, uint32_t
 /* Copies the counters of the most recent edit to the host (synchronises `stream`). */
 svdag_status svdag_last_edit_stats(svdag_ctx* ctx, svdag_edit_stats* out, void* stream);
 
+/* Profiling: GPU global-timer stamps (ns) taken at the phase barriers of the most recent edit run by
+ * the persistent kernel: start, after begin, after each top-down level, after the leaves, after each
+ * bottom-up level, after the end. Plays the role of the reference's GPUTimingsManager scopes
+ * (timings.h). Synchronises `stream`. */
+svdag_status svdag_last_edit_phase_times(svdag_ctx* ctx, uint64_t* out_ns, uint32_t capacity, uint32_t* out_count,
+    void* stream);
+
 /* Convenience forms mirroring the reference tool constructors. */
 svdag_status svdag_edit_sphere(svdag_ctx* ctx, float cx, float cy, float cz, float radius,
     uint32_t material, int add, void* stream);
