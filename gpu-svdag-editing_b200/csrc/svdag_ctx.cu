@@ -18,14 +18,13 @@ constexpr unsigned long long kBatchBytes = 2 * 1024 * 1024;
 // ---------------------------------------------------------------- garbage collection
 // MyGPUHashDAG::garbageCollect (my_gpu_hash_dag.cu:365-475) marks level by level from the root set
 // (the root and the level-0 fully-filled nodes) and, with CAPTURE_MEMORY_STATS_SLOW, frees the
-// unmarked slots (gpu_hash_table_base.cu:304-374). Here marking is a bitmap indexed by handle/2 (items
-// are at least two words long) and the frontier is deduplicated by the test-and-set on that bitmap.
+// unmarked slots (gpu_hash_table_base.cu:304-374). Here marking is a bitmap with one bit per handle
+// (an 8-byte unit of the item region) and the frontier is deduplicated by the test-and-set on it.
 
 __device__ __forceinline__ bool mark_once(uint32_t* bits, uint32_t handle)
 {
-    const uint32_t b = handle >> 1;
-    const uint32_t m = 1u << (b & 31u);
-    return !(atomicOr(&bits[b >> 5], m) & m);
+    const uint32_t m = 1u << (handle & 31u);
+    return !(atomicOr(&bits[handle >> 5], m) & m);
 }
 
 __global__ void k_gc_roots(DevDag d, uint32_t* bits, uint32_t* frontier, uint32_t* count)
@@ -76,26 +75,26 @@ __global__ void k_gc_sweep(DevDag d, DevTable t, const uint32_t* bits, unsigned 
     for (uint32_t c = 0; c < kNumClasses; ++c) {
         const uint32_t k = c + 2;
         for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < t.numBuckets[c]; b += gridDim.x * blockDim.x) {
-            uint32_t slab = t.bucketBase[c] + b * slab_words(k);
+            uint32_t slab = t.bucketBase[c] + b * slab_sectors(k);
             for (uint32_t steps = 0; steps < kMaxChain; ++steps) {
-                uint32_t* h = d.items + slab;
+                uint32_t* h = slab_ptr(d, slab);
                 for (uint32_t s = 0; s < kSlots; ++s) {
                     const uint32_t shift = 8u * (s / 7u);
                     const uint32_t tag = (h[s % 7u] >> shift) & 0xFFu;
                     if (tag == 0 || tag == kTagBusy)
                         continue;
-                    const uint32_t item = slab + kHeaderWords + s * k;
-                    const uint32_t bit = item >> 1;
-                    if ((bits[bit >> 5] >> (bit & 31u)) & 1u)
+                    const uint32_t item = slot_handle(slab, s, k);
+                    if ((bits[item >> 5] >> (item & 31u)) & 1u)
                         continue;
+                    uint32_t* ip = handle_ptr(d, item);
                     for (uint32_t j = 0; j < k; ++j)
-                        d.items[item + j] = 0;
+                        ip[j] = 0;
                     h[s % 7u] &= ~(0xFFu << shift);
                     ++nfreed;
                 }
                 if (h[7] == kEnd)
                     break;
-                if (!handle_ok(d, h[7])) {
+                if (!slab_ok(d, h[7])) {
                     set_status(d.ctl, SVDAG_ERR_CORRUPT);
                     break;
                 }
@@ -186,7 +185,7 @@ svdag_status svdag_create(const svdag_config* cfg, svdag_ctx** out)
     ctx->scratch = ctx->pool + kCtlBytes + kBatchBytes;
     ctx->scratchBytes = scratch;
     ctx->items = reinterpret_cast<uint32_t*>(ctx->pool + kCtlBytes + kBatchBytes + scratch);
-    ctx->itemWords = std::min<unsigned long long>((pool - kCtlBytes - kBatchBytes - scratch) / 4 - 64, kMaxHandle);
+    ctx->itemWords = std::min<unsigned long long>((pool - kCtlBytes - kBatchBytes - scratch) / 4 - 64, kMaxItemWords) & ~7ull;
     static_assert(sizeof(Control) <= kCtlBytes, "control block too large");
     cudaError_t e = cudaMemset(ctx->pool, 0, pool);
     if (e == cudaSuccess) {
@@ -246,7 +245,7 @@ svdag_status svdag_gc(svdag_ctx* ctx, void* stream)
     unsigned long long top = 0;
     SVDAG_CUDA(cudaMemcpyAsync(&top, &ctx->ctl->itemTop, sizeof(top), cudaMemcpyDeviceToHost, s));
     SVDAG_CUDA(cudaStreamSynchronize(s));
-    const unsigned long long bitmapBytes = align256(((top / 2) + 32) / 8 + 8);
+    const unsigned long long bitmapBytes = align256(((top / 2) + 64) / 8 + 8); // one bit per 8-byte unit
     const unsigned long long rest = ctx->scratchBytes > bitmapBytes + 4096 ? ctx->scratchBytes - bitmapBytes - 4096 : 0;
     const unsigned long long frontierCap = rest / 8; // two frontiers of u32
     if (frontierCap < 1024)

@@ -1,16 +1,18 @@
 // svdag_device.cuh - device-side data layout and the slab hash table probes.
 //
-// Item region: one word-addressed array inside the context's HBM pool. A handle is the 32-bit word
-// offset of an item, so decoding a handle is one add (the reference decodes through a table
-// descriptor and the slab allocator's super-block table, gpu_hash_table_base.h:275-294).
+// Item region: one array inside the context's HBM pool. A handle is the index of an item in 8-byte
+// units (items are 8-byte aligned), so decoding a handle is a shift and an add and 32-bit handles
+// reach 32 GiB (the reference decodes through a table descriptor and the slab allocator's super-block
+// table, gpu_hash_table_base.h:275-294). Slabs are 32-byte aligned and named by their index in
+// 32-byte units (the "slab id").
 //
 // Hash tables: one table per DAG level. A level table holds keys of 2..10 words; keys of one length
 // share a slab family (the "size class"), so slots have a fixed stride and the slot index gives the
 // item address. A slab of class k:
 //   words 0..6  : 28 one-byte tags, slot s at word (s % 7), byte (s / 7); 0 = free, 0xFF = being written
-//   word  7     : word offset of the next slab in the bucket's chain, 0 = end of chain (offset 0 is
-//                 always a bucket array, never an overflow slab)
-//   words 8..   : 28 items of k words (item s at 8 + s*k)
+//   word  7     : slab id of the next slab in the bucket's chain, 0 = end of chain (slab 0 is always
+//                 a bucket array, never an overflow slab)
+//   words 8..   : 28 items of k words at a stride of k rounded up to even (item s at 8 + s*stride)
 // The 8 header words are one 32-byte sector, so a probe costs one sector per slab plus the candidate
 // item; the reference's header is 10 words (8 hash words + next + active mask) spanning two sectors
 // (compact_acceleration_hash_table.h:519-541). The first slab of each bucket sits in the bucket
@@ -26,7 +28,7 @@ namespace svdag {
 constexpr uint32_t kNone = 0xFFFFFFFFu; // empty child / missing handle
 constexpr uint32_t kEnd = 0u; // end of a slab chain
 constexpr uint32_t kFillMarker = 0xFFFFFF00u; // SVO child "canonical fully-filled node of material m" = kFillMarker | m
-constexpr uint32_t kMaxHandle = 0xFFFFFF00u; // item region limit in words (just under 16 GiB)
+constexpr unsigned long long kMaxItemWords = 2ull * 0xFFFFFF00ull - 64; // item region limit (just under 32 GiB)
 constexpr uint32_t kSlots = 28;
 constexpr uint32_t kHeaderWords = 8;
 constexpr uint32_t kTagBusy = 0xFFu;
@@ -34,13 +36,20 @@ constexpr uint32_t kMaxLevels = SVDAG_MAX_LEVELS;
 constexpr uint32_t kItemStride = 10; // padded stride of items in scratch arrays
 constexpr uint32_t kNumClasses = 9; // item sizes 2..10
 
-__host__ __device__ constexpr uint32_t slab_words(uint32_t k) { return ((kHeaderWords + kSlots * k) + 7u) & ~7u; }
+__host__ __device__ constexpr uint32_t item_stride(uint32_t k) { return (k + 1u) & ~1u; } // words, even
+__host__ __device__ constexpr uint32_t slab_words(uint32_t k) { return ((kHeaderWords + kSlots * item_stride(k)) + 7u) & ~7u; }
+__host__ __device__ constexpr uint32_t slab_sectors(uint32_t k) { return slab_words(k) >> 3; }
+// Handle of slot s of the slab with id `slab` for items of k words.
+__host__ __device__ constexpr uint32_t slot_handle(uint32_t slab, uint32_t s, uint32_t k)
+{
+    return (slab << 2) + 4u + s * (item_stride(k) >> 1);
+}
 
 // Per-table descriptor, passed by value to kernels.
 struct DevTable {
     uint32_t kind; // svdag_item_kind
     uint32_t numBuckets[kNumClasses];
-    uint32_t bucketBase[kNumClasses]; // word offset of bucket 0's slab
+    uint32_t bucketBase[kNumClasses]; // slab id of bucket 0
 };
 
 // Device control block (lives at the start of the scratch side of the pool).
@@ -94,15 +103,21 @@ __device__ __forceinline__ void set_status(Control* ctl, uint32_t code)
 __device__ const uint32_t kZeroItem[16] = {};
 __device__ __forceinline__ bool handle_ok(const DevDag& d, uint32_t h)
 {
-    return (unsigned long long)h + 16ull <= d.itemWords;
+    return 2ull * h + 16ull <= d.itemWords;
 }
 __device__ __forceinline__ const uint32_t* item_ptr(const DevDag& d, uint32_t h)
 {
     if (handle_ok(d, h))
-        return d.items + h;
+        return d.items + 2ull * h;
     set_status(d.ctl, SVDAG_ERR_CORRUPT);
     return kZeroItem;
 }
+__device__ __forceinline__ bool slab_ok(const DevDag& d, uint32_t slab)
+{
+    return 8ull * slab + 8ull <= d.itemWords;
+}
+__device__ __forceinline__ uint32_t* slab_ptr(const DevDag& d, uint32_t slab) { return d.items + 8ull * slab; }
+__device__ __forceinline__ uint32_t* handle_ptr(const DevDag& d, uint32_t h) { return d.items + 2ull * h; }
 
 // ---------------------------------------------------------------- hashing (ours; the bucket
 // function of the reference is xorHash32xN, utils.h:395-403, which uses a 32-bit modulo per word)
@@ -344,7 +359,7 @@ __device__ __forceinline__ void write_item(const Grp<G>& g, uint32_t* item, cons
 
 __device__ __forceinline__ uint32_t first_slab(const DevTable& t, uint32_t cls, uint32_t ha)
 {
-    return t.bucketBase[cls] + bucket_of(ha, t.numBuckets[cls]) * slab_words(cls + 2u);
+    return t.bucketBase[cls] + bucket_of(ha, t.numBuckets[cls]) * slab_sectors(cls + 2u);
 }
 
 // Allocates and initialises an overflow slab of class k; returns kNone when the region is full.
@@ -355,8 +370,8 @@ __device__ __forceinline__ uint32_t alloc_slab(const Grp<G>& g, const DevDag& d,
     if (g.lane == 0) {
         const unsigned long long w = slab_words(k);
         const unsigned long long o = atomicAdd(&d.ctl->itemTop, w);
-        if (o + w <= d.itemWords && o + w <= kMaxHandle)
-            off = (uint32_t)o;
+        if (o + w <= d.itemWords)
+            off = (uint32_t)(o >> 3); // itemTop stays a multiple of 8 words
         else
             set_status(d.ctl, SVDAG_ERR_OOM);
     }
@@ -364,8 +379,9 @@ __device__ __forceinline__ uint32_t alloc_slab(const Grp<G>& g, const DevDag& d,
     if (off != kNone) {
         // Free slots keep zero words (a valid key is never all zero), so the whole slab is cleared.
         const uint32_t sw = slab_words(k);
+        uint32_t* p = slab_ptr(d, off);
         for (uint32_t i = g.lane * 4; i < sw; i += G * 4)
-            *reinterpret_cast<uint4*>(d.items + off + i) = make_uint4(0, 0, 0, 0);
+            *reinterpret_cast<uint4*>(p + i) = make_uint4(0, 0, 0, 0);
         __threadfence();
         g.sync();
     }
@@ -373,9 +389,9 @@ __device__ __forceinline__ uint32_t alloc_slab(const Grp<G>& g, const DevDag& d,
 }
 
 // Links `fresh` behind `slab`; returns the slab that follows `slab` afterwards (ours or a racer's).
-__device__ __forceinline__ uint32_t link_slab(uint32_t* items, uint32_t slab, uint32_t fresh)
+__device__ __forceinline__ uint32_t link_slab(const DevDag& d, uint32_t slab, uint32_t fresh)
 {
-    const uint32_t prev = atomicCAS(&items[slab + 7], kEnd, fresh);
+    const uint32_t prev = atomicCAS(slab_ptr(d, slab) + 7, kEnd, fresh);
     return prev == kEnd ? fresh : prev;
 }
 
@@ -404,17 +420,17 @@ __device__ __forceinline__ uint32_t table_find(const Grp<G>& g, const DevDag& d,
             return kNone;
         }
         uint32_t next, empty;
-        uint32_t cand = probe_header<G>(g, d.items + slab, tag, next, empty);
+        uint32_t cand = probe_header<G>(g, slab_ptr(d, slab), tag, next, empty);
         while (cand) {
             const uint32_t s = __ffs(cand) - 1u;
             cand &= cand - 1u;
-            const uint32_t item = slab + kHeaderWords + s * key.n;
-            if (item_equals<G, LD_STREAM>(g, d.items + item, key))
+            const uint32_t item = slot_handle(slab, s, key.n);
+            if (item_equals<G, LD_STREAM>(g, handle_ptr(d, item), key))
                 return item;
         }
         if (next == kEnd)
             return kNone;
-        if (!handle_ok(d, next)) {
+        if (!slab_ok(d, next)) {
             set_status(d.ctl, SVDAG_ERR_CORRUPT);
             return kNone;
         }
@@ -433,7 +449,7 @@ __device__ __forceinline__ uint32_t claim_in_slab(const Grp<G>& g, const DevDag&
         const uint32_t word = s % 7u, shift = 8u * (s / 7u);
         uint32_t got = 0;
         if (g.lane == 0) {
-            uint32_t* p = d.items + slab + word;
+            uint32_t* p = slab_ptr(d, slab) + word;
             uint32_t cur = *reinterpret_cast<volatile uint32_t*>(p);
             for (;;) {
                 if ((cur >> shift) & 0xFFu)
@@ -449,7 +465,7 @@ __device__ __forceinline__ uint32_t claim_in_slab(const Grp<G>& g, const DevDag&
         }
         got = g.bcast(got, 0);
         if (got)
-            return slab + kHeaderWords + s * n;
+            return slot_handle(slab, s, n);
         emptyMask &= emptyMask - 1u;
     }
     return kNone;
@@ -469,10 +485,10 @@ __device__ __forceinline__ uint32_t table_add(const Grp<G>& g, const DevDag& d, 
     uint32_t slab = first_slab(t, cls, key.ha);
     for (uint32_t steps = 0; steps < kMaxChain; ++steps) {
         uint32_t next, empty;
-        probe_header<G>(g, d.items + slab, tag, next, empty);
+        probe_header<G>(g, slab_ptr(d, slab), tag, next, empty);
         const uint32_t item = claim_in_slab<G>(g, d, slab, empty, tag, key.n, false);
         if (item != kNone) {
-            write_item<G>(g, d.items + item, key);
+            write_item<G>(g, handle_ptr(d, item), key);
             return item;
         }
         if (next == kEnd) {
@@ -484,13 +500,13 @@ __device__ __forceinline__ uint32_t table_add(const Grp<G>& g, const DevDag& d, 
                 return kNone;
             uint32_t linked = kNone;
             if (g.lane == 0)
-                linked = link_slab(d.items, slab, spare.slab);
+                linked = link_slab(d, slab, spare.slab);
             linked = g.bcast(linked, 0);
             if (linked == spare.slab)
                 spare.slab = kNone;
             next = linked;
         }
-        if (!handle_ok(d, next)) {
+        if (!slab_ok(d, next)) {
             set_status(d.ctl, SVDAG_ERR_CORRUPT);
             return kNone;
         }
@@ -522,19 +538,19 @@ __device__ __forceinline__ uint32_t table_find_or_insert(const Grp<G>& g, const 
             return kNone;
         }
         uint32_t next, empty;
-        uint32_t cand = probe_header<G, true>(g, d.items + slab, tag, next, empty);
+        uint32_t cand = probe_header<G, true>(g, slab_ptr(d, slab), tag, next, empty);
         while (cand) {
             const uint32_t s = __ffs(cand) - 1u;
             cand &= cand - 1u;
-            const uint32_t item = slab + kHeaderWords + s * key.n;
-            if (item_equals<G, LD_L2>(g, d.items + item, key))
+            const uint32_t item = slot_handle(slab, s, key.n);
+            if (item_equals<G, LD_L2>(g, handle_ptr(d, item), key))
                 return item;
         }
         tail = slab;
         tailEmpty = empty;
         if (next == kEnd)
             break;
-        if (!handle_ok(d, next)) {
+        if (!slab_ok(d, next)) {
             set_status(d.ctl, SVDAG_ERR_CORRUPT);
             return kNone;
         }
@@ -546,18 +562,18 @@ __device__ __forceinline__ uint32_t table_find_or_insert(const Grp<G>& g, const 
     for (uint32_t steps = 0; steps < kMaxChain; ++steps) {
         const uint32_t item = claim_in_slab<G>(g, d, slab, empty, tag, key.n, true);
         if (item != kNone) {
-            write_item<G>(g, d.items + item, key);
+            write_item<G>(g, handle_ptr(d, item), key);
             __threadfence();
             g.sync();
             if (g.lane == 0) {
-                const uint32_t s = (item - slab - kHeaderWords) / key.n;
-                atomicXor(&d.items[slab + s % 7u], (kTagBusy ^ tag) << (8u * (s / 7u)));
+                const uint32_t s = (item - (slab << 2) - 4u) / (item_stride(key.n) >> 1);
+                atomicXor(slab_ptr(d, slab) + s % 7u, (kTagBusy ^ tag) << (8u * (s / 7u)));
             }
             inserted = true;
             return item;
         }
         uint32_t next;
-        probe_header<G, true>(g, d.items + slab, tag, next, empty);
+        probe_header<G, true>(g, slab_ptr(d, slab), tag, next, empty);
         if (empty)
             continue; // a slot was freed up meanwhile (cannot happen during edits, kept for safety)
         if (next == kEnd) {
@@ -569,18 +585,18 @@ __device__ __forceinline__ uint32_t table_find_or_insert(const Grp<G>& g, const 
                 return kNone;
             uint32_t linked = kNone;
             if (g.lane == 0)
-                linked = link_slab(d.items, slab, spare.slab);
+                linked = link_slab(d, slab, spare.slab);
             linked = g.bcast(linked, 0);
             if (linked == spare.slab)
                 spare.slab = kNone;
             next = linked;
         }
-        if (!handle_ok(d, next)) {
+        if (!slab_ok(d, next)) {
             set_status(d.ctl, SVDAG_ERR_CORRUPT);
             return kNone;
         }
         slab = next;
-        probe_header<G, true>(g, d.items + slab, tag, next, empty);
+        probe_header<G, true>(g, slab_ptr(d, slab), tag, next, empty);
     }
     set_status(d.ctl, SVDAG_ERR_TIMEOUT);
     return kNone;

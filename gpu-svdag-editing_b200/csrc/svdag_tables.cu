@@ -49,10 +49,10 @@ svdag_status alloc_table(svdag_ctx* ctx, svdag_table* t, uint32_t kind, const ui
     unsigned long long words = 0;
     for (uint32_t c = 0; c < kNumClasses; ++c) {
         dev.numBuckets[c] = bucketsPerClass[c];
-        dev.bucketBase[c] = (uint32_t)(top + words);
+        dev.bucketBase[c] = (uint32_t)((top + words) >> 3); // slab id (top and slab sizes are multiples of 8 words)
         words += (unsigned long long)bucketsPerClass[c] * slab_words(c + 2);
     }
-    if (top + words > ctx->itemWords || top + words > kMaxHandle)
+    if (top + words > ctx->itemWords)
         return SVDAG_ERR_OOM;
     SVDAG_CUDA(cudaMemsetAsync(ctx->items + top, 0, words * 4, s));
     const unsigned long long newTop = top + words;
@@ -245,12 +245,12 @@ __global__ void k_table_read(DevDag d, uint32_t kind, const uint32_t* handles, u
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t h = handles[i];
         uint32_t* o = out + (size_t)i * kItemStride;
-        if (h == kNone || h + 16ull > d.itemWords) {
+        if (h == kNone || !handle_ok(d, h)) {
             for (uint32_t j = 0; j < kItemStride; ++j)
                 o[j] = 0;
             continue;
         }
-        const uint32_t* p = d.items + h;
+        const uint32_t* p = handle_ptr(d, h);
         const uint32_t nw = kind == SVDAG_KIND_NODE ? dev_node_words(p[0]) : dev_leaf_words(p[0], p[1]);
         for (uint32_t j = 0; j < kItemStride; ++j)
             o[j] = j < nw ? p[j] : 0u;
@@ -265,10 +265,10 @@ __global__ void k_table_walk(DevDag d, DevTable t, unsigned long long* counters,
         const uint32_t k = c + 2;
         const uint32_t nb = t.numBuckets[c];
         for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
-            uint32_t slab = t.bucketBase[c] + b * slab_words(k);
+            uint32_t slab = t.bucketBase[c] + b * slab_sectors(k);
             unsigned long long items = 0, slabs = 0;
             for (uint32_t steps = 0; steps < kMaxChain; ++steps) {
-                const uint32_t* h = d.items + slab;
+                const uint32_t* h = slab_ptr(d, slab);
                 for (uint32_t s = 0; s < kSlots; ++s) {
                     const uint32_t tag = (h[s % 7u] >> (8u * (s / 7u))) & 0xFFu;
                     if (tag == 0 || tag == kTagBusy)
@@ -277,17 +277,18 @@ __global__ void k_table_walk(DevDag d, DevTable t, unsigned long long* counters,
                     if (outHandles) {
                         const unsigned long long pos = atomicAdd(&counters[2], 1ull);
                         if (pos < capacity) {
-                            const uint32_t item = slab + kHeaderWords + s * k;
+                            const uint32_t item = slot_handle(slab, s, k);
                             outHandles[pos] = item;
+                            const uint32_t* ip = handle_ptr(d, item);
                             for (uint32_t j = 0; j < kItemStride; ++j)
-                                outWords[pos * kItemStride + j] = j < k ? d.items[item + j] : 0u;
+                                outWords[pos * kItemStride + j] = j < k ? ip[j] : 0u;
                         }
                     }
                 }
                 const uint32_t next = h[7];
                 if (next == kEnd)
                     break;
-                if (!handle_ok(d, next)) {
+                if (!slab_ok(d, next)) {
                     set_status(d.ctl, SVDAG_ERR_CORRUPT);
                     break;
                 }

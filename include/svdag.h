@@ -37,7 +37,7 @@ typedef enum svdag_status {
     SVDAG_ERR_BUSY = 8 /* serving queue full / admission refused */
 } svdag_status;
 
-/* Item handles are 32-bit word offsets of the item inside the context's item region. */
+/* Item handles are 32-bit indices of items in 8-byte units of the context's item region (up to 32 GiB). */
 #define SVDAG_INVALID_HANDLE 0xFFFFFFFFu
 /* Voxel sampling and hit records use this value for "no voxel". */
 #define SVDAG_NO_MATERIAL 0xFFFFFFFFu
