@@ -65,6 +65,8 @@ struct EditCounters {
     unsigned long long buildTop; // end of the top-down allocations
     uint32_t rootBefore, rootAfter;
     uint32_t overflow; // scratch arena exhausted
+    uint32_t builder; // scene build: merge even without leaves, discovery on every level
+    uint32_t startLevel;
     uint32_t pad;
 };
 

@@ -61,84 +61,6 @@ __device__ __forceinline__ bool sphere_contained(const DevEditor& e, const float
         < e.radiusSquared;
 }
 
-// ---- procedural terrain (integer value-noise fBm; identical to the oracle's Terrain)
-
-__device__ __forceinline__ uint32_t terrain_lattice(const DevEditor& e, uint32_t ix, uint32_t iz, uint32_t o)
-{
-    uint32_t h = fmix32(e.terrain.seed * 0x9E3779B9u ^ (o * 0x85EBCA6Bu) ^ 0x68E31DA4u);
-    h = fmix32(h ^ (ix * 0xC2B2AE35u));
-    h = fmix32(h ^ (iz * 0x27D4EB2Fu));
-    return h >> 16;
-}
-__device__ __forceinline__ long long smooth16(long long t) { return (t * t * (3 * 65536 - 2 * t)) >> 32; }
-__device__ __forceinline__ long long lerp16(long long a, long long b, long long t) { return a + (((b - a) * t) >> 16); }
-__device__ __forceinline__ uint32_t terrain_cell_log2(const DevEditor& e, uint32_t o) { return e.terrainBaseLog2 > o ? e.terrainBaseLog2 - o : 0u; }
-__device__ __forceinline__ uint32_t terrain_height_from_fbm(const DevEditor& e, long long f)
-{
-    const long long G = 1ll << e.levels;
-    const long long base = G * e.terrain.min_height_pct / 100;
-    const long long range = G * (long long)(e.terrain.max_height_pct - e.terrain.min_height_pct) / 100;
-    const long long norm = ((1ll << e.terrain.octaves) - 1) * 65536;
-    return (uint32_t)(base + (range * f) / norm);
-}
-__device__ long long terrain_octave(const DevEditor& e, uint32_t x, uint32_t z, uint32_t o)
-{
-    const uint32_t c = terrain_cell_log2(e, o);
-    const uint32_t ix = x >> c, iz = z >> c, m = (1u << c) - 1u;
-    const long long fx = c <= 16 ? (long long)((x & m) << (16 - c)) : (long long)((x & m) >> (c - 16));
-    const long long fz = c <= 16 ? (long long)((z & m) << (16 - c)) : (long long)((z & m) >> (c - 16));
-    const long long sx = smooth16(fx), sz = smooth16(fz);
-    const long long a = lerp16(terrain_lattice(e, ix, iz, o), terrain_lattice(e, ix + 1, iz, o), sx);
-    const long long b = lerp16(terrain_lattice(e, ix, iz + 1, o), terrain_lattice(e, ix + 1, iz + 1, o), sx);
-    return lerp16(a, b, sz);
-}
-__device__ uint32_t terrain_height(const DevEditor& e, uint32_t x, uint32_t z)
-{
-    long long f = 0;
-    for (uint32_t o = 0; o < e.terrain.octaves; ++o)
-        f += terrain_octave(e, x, z, o) << (e.terrain.octaves - 1 - o);
-    return terrain_height_from_fbm(e, f);
-}
-__device__ void terrain_bounds(const DevEditor& e, uint32_t x0, uint32_t z0, uint32_t s, uint32_t& hlo, uint32_t& hhi)
-{
-    long long lo = 0, hi = 0;
-    for (uint32_t o = 0; o < e.terrain.octaves; ++o) {
-        const uint32_t c = terrain_cell_log2(e, o);
-        const uint32_t ix0 = x0 >> c, iz0 = z0 >> c;
-        const uint32_t ix1 = ((x0 + s - 1) >> c) + 1, iz1 = ((z0 + s - 1) >> c) + 1;
-        long long vlo = 65535, vhi = 0;
-        if (s <= (1u << c)) {
-            // Footprint inside one lattice cell: extremes at the footprint corners, up to 2 units of
-            // integer truncation below the real bilinear value (same rule as the oracle).
-            const uint32_t x1 = x0 + s - 1, z1 = z0 + s - 1;
-            const long long v0 = terrain_octave(e, x0, z0, o), v1 = terrain_octave(e, x1, z0, o);
-            const long long v2 = terrain_octave(e, x0, z1, o), v3 = terrain_octave(e, x1, z1, o);
-            vlo = min(min(v0, v1), min(v2, v3)) - 2;
-            vhi = max(max(v0, v1), max(v2, v3)) + 2;
-            vlo = vlo < 0 ? 0 : vlo;
-            vhi = vhi > 65535 ? 65535 : vhi;
-        } else if ((unsigned long long)(ix1 - ix0 + 1) * (iz1 - iz0 + 1) > 64) {
-            vlo = 0;
-            vhi = 65535;
-        } else {
-            for (uint32_t iz = iz0; iz <= iz1; ++iz)
-                for (uint32_t ix = ix0; ix <= ix1; ++ix) {
-                    const long long v = terrain_lattice(e, ix, iz, o);
-                    vlo = v < vlo ? v : vlo;
-                    vhi = v > vhi ? v : vhi;
-                }
-        }
-        lo += vlo << (e.terrain.octaves - 1 - o);
-        hi += vhi << (e.terrain.octaves - 1 - o);
-    }
-    hlo = terrain_height_from_fbm(e, lo);
-    hhi = terrain_height_from_fbm(e, hi);
-}
-__device__ __forceinline__ uint32_t terrain_material(const DevEditor& e, uint32_t y)
-{
-    return (uint32_t)(((unsigned long long)y * e.terrain.num_materials) >> e.levels);
-}
-
 // ---- 3D value noise material (box noise paint), identical to the oracle's noise_material
 __device__ __forceinline__ uint32_t lattice3(uint32_t seed, uint32_t x, uint32_t y, uint32_t z)
 {
@@ -210,20 +132,8 @@ __device__ __forceinline__ uint32_t should_edit(const DevEditor& e, uint32_t px,
     } else if constexpr (TOOL == SVDAG_TOOL_COPY) { // stateless form, :166-172 (used for voxels)
         return box_overlap(e, nmin, nmax) ? OP_SUBDIVIDE : OP_KEEP;
     } else if constexpr (TOOL == kToolTerrain) {
-        const uint32_t s = 1u << depth;
-        uint32_t hlo, hhi;
-        terrain_bounds(e, px << depth, pz << depth, s, hlo, hhi);
-        const uint32_t y0 = py << depth;
-        if (y0 >= hhi)
-            return OP_EMPTY;
-        if (y0 + s <= hlo) {
-            const uint32_t m0 = terrain_material(e, y0), m1 = terrain_material(e, y0 + s - 1);
-            if (m0 == m1) {
-                fillMaterial = m0;
-                return OP_FILL;
-            }
-        }
-        return OP_SUBDIVIDE;
+        const uint32_t c = scene_classify(e.scene, px, py, pz, depth, fillMaterial);
+        return c == 1 ? OP_FILL : (c == 2 ? OP_EMPTY : OP_SUBDIVIDE);
     } else {
         return OP_KEEP;
     }
@@ -311,10 +221,13 @@ __device__ void ph_edit_begin(const DevDag& d, const DevEditor& e, char* scratch
             c->undoCount = c->undoCount < c->undoDepth ? c->undoCount + 1u : c->undoDepth;
         }
     }
-    E.count[0] = 1;
-    E.offW[0] = 0;
+    const uint32_t L0 = e.startLevel;
+    E.builder = e.builder;
+    E.startLevel = L0;
+    E.count[L0] = 1;
+    E.offW[L0] = 0;
     WorkItem* w = reinterpret_cast<WorkItem*>(scratch);
-    w[0] = WorkItem { 0, 0, 0, root };
+    w[0] = WorkItem { e.startPath[0], e.startPath[1], e.startPath[2], L0 == 0 ? root : kNone };
     if (e.tool == SVDAG_TOOL_COPY) { // createInitialState, my_gpu_dag_editors.h:148-155
         CopyParent* st = reinterpret_cast<CopyParent*>(scratch + 16);
         for (int i = 0; i < 8; ++i)
@@ -457,7 +370,7 @@ __device__ void ph_build_leaves(const DevDag& d, const DevEditor& e, char* scrat
         E.offN[LL] = offN;
         E.buildTop = buildTop;
     }
-    if (E.overflow || n == 0)
+    if (E.overflow || (n == 0 && !E.builder))
         return;
     // Reserve and clear the dedup tables of every level for the bottom-up phase.
     // The dedup tables of all levels form one contiguous run per level; walk the layout once (from
@@ -506,10 +419,10 @@ __device__ void ph_build_leaves(const DevDag& d, const DevEditor& e, char* scrat
             if (lane == 0)
                 ++oldRead;
         }
-        uint32_t th = 0; // terrain: column heights in lanes 0..15
+        uint32_t th = 0; // scene: terrain column heights in lanes 0..15
         if constexpr (TOOL == kToolTerrain) {
             if (lane < 16)
-                th = terrain_height(e, (w.x << 2) + (lane >> 2), (w.z << 2) + (lane & 3u));
+                th = terrain_height(e.scene, (w.x << 2) + (lane >> 2), (w.z << 2) + (lane & 3u));
         }
         uint32_t newMat[2];
         bool set[2];
@@ -532,8 +445,8 @@ __device__ void ph_build_leaves(const DevDag& d, const DevEditor& e, char* scrat
             uint32_t mat = 0;
             if constexpr (TOOL == kToolTerrain) {
                 const uint32_t colH = __shfl_sync(0xFFFFFFFFu, th, dx * 4 + dz);
-                out = vy < colH;
-                mat = terrain_material(e, vy);
+                mat = scene_voxel(e.scene, vx, vy, vz, colH);
+                out = mat != SVDAG_NO_MATERIAL;
                 ++edited;
             } else {
                 uint32_t fm = 0;
@@ -633,10 +546,12 @@ __device__ void ph_build_leaves(const DevDag& d, const DevEditor& e, char* scrat
     }
 }
 
+// The bottom-up phase runs when the SVO reached the leaf level (an edit without leaves leaves the DAG
+// untouched, my_gpu_hash_dag_edits.cu:651) or, for the scene builder, always.
 __device__ __forceinline__ bool merge_live(const DevDag& d)
 {
     const EditCounters& E = d.ctl->edit;
-    return E.count[d.leafLevel] != 0 && !E.overflow;
+    return (E.count[d.leafLevel] != 0 || E.builder) && !E.overflow;
 }
 
 // Discovery at `level` runs only if it ran one level down (always at the leaf level) and found
@@ -816,7 +731,7 @@ __device__ void ph_merge_level(const DevDag& d, uint32_t level, char* scratch)
     const uint32_t LL = d.leafLevel;
     const uint32_t n = E.count[level];
     const bool isLeaf = level == LL;
-    const bool gate = isLeaf ? false : discovery_gate(E, level, LL, 0);
+    const bool gate = isLeaf ? false : discovery_gate(E, level, LL, E.builder);
     if (!isLeaf && blockIdx.x == 0 && threadIdx.x == 0)
         E.ffRan[level] = gate ? 1u : 0u;
     const MergeLayout m = merge_layout(E.count, E.buildTop, level, LL);
@@ -902,7 +817,7 @@ __device__ void ph_insert_level(const DevDag& d, const DevTable& t, uint32_t lev
         atomicAdd(&E.added, (unsigned long long)added);
 }
 
-__device__ void ph_edit_end(const DevDag& d, char* scratch, uint32_t builder, EditRecord* record)
+__device__ void ph_edit_end(const DevDag& d, char* scratch, uint32_t builder, uint32_t* tileOut, EditRecord* record)
 {
     if (threadIdx.x != 0 || blockIdx.x != 0)
         return;
@@ -910,12 +825,14 @@ __device__ void ph_edit_end(const DevDag& d, char* scratch, uint32_t builder, Ed
     EditCounters& E = c->edit;
     if (E.overflow) {
         set_status(c, SVDAG_ERR_OOM);
-    } else if (E.count[d.leafLevel] != 0 && c->status == 0) {
-        const MergeLayout m = merge_layout(E.count, E.buildTop, 0, d.leafLevel);
+    } else if ((E.count[d.leafLevel] != 0 || builder) && c->status == 0) {
+        const MergeLayout m = merge_layout(E.count, E.buildTop, E.startLevel, d.leafLevel);
         const uint32_t r = reinterpret_cast<const uint32_t*>(scratch + m.rep)[0];
-        c->root = r == kEmptyRep ? kNone : reinterpret_cast<const uint32_t*>(scratch + m.handle)[r];
-    } else if (builder && E.count[d.leafLevel] == 0) {
-        c->root = kNone;
+        const uint32_t h = r == kEmptyRep ? kNone : reinterpret_cast<const uint32_t*>(scratch + m.handle)[r];
+        if (tileOut)
+            *tileOut = h;
+        else
+            c->root = h;
     }
     E.rootAfter = c->root;
     if (record) {
@@ -967,7 +884,7 @@ __global__ void __launch_bounds__(256) k_insert_level(DevDag d, DevTable t, uint
 {
     ph_insert_level<G>(d, t, level, scratch);
 }
-__global__ void k_edit_end(DevDag d, char* scratch, uint32_t builder) { ph_edit_end(d, scratch, builder, nullptr); }
+__global__ void k_edit_end(DevDag d, char* scratch, uint32_t builder, uint32_t* tileOut) { ph_edit_end(d, scratch, builder, tileOut, nullptr); }
 
 // ---------------------------------------------------------------- persistent form
 // One cooperative launch runs whole edits: every phase above is a grid-stride loop over the
@@ -1010,7 +927,7 @@ __device__ __forceinline__ void fused_edit(cg::grid_group& grid, const DevDag& d
         grid.sync();
         stamp(d, k);
     }
-    ph_edit_end(d, scratch, ed.builder, record);
+    ph_edit_end(d, scratch, ed.builder, ed.tileOut, record);
     grid.sync();
     stamp(d, k);
 }
@@ -1048,6 +965,15 @@ __global__ void __launch_bounds__(256) k_edit_fused(DevDag d, DevEditor single, 
             break;
         }
     }
+}
+
+// Scene tiles: builder edits of subtrees, one after another in one persistent launch.
+__global__ void __launch_bounds__(256) k_scene_fused(DevDag d, const DevEditor* eds, uint32_t numEdits, char* scratch,
+    unsigned long long scratchBytes)
+{
+    cg::grid_group grid = cg::this_grid();
+    for (uint32_t k = 0; k < numEdits; ++k)
+        fused_edit<kToolTerrain>(grid, d, eds[k], scratch, scratchBytes, nullptr);
 }
 
 __global__ void k_undo_redo(Control* c, uint32_t redo)
@@ -1205,7 +1131,7 @@ svdag_status launch_pipeline(svdag_ctx* ctx, const DevEditor& ed, cudaStream_t s
     const uint32_t LL = d.leafLevel;
     for (int level = (int)LL; level >= 0; --level)
         k_merge_level<<<grid_for(ctx, level_bound(level), 256), 256, 0, s>>>(d, level, ctx->scratch);
-    k_edit_end<<<1, 32, 0, s>>>(d, ctx->scratch, 0);
+    k_edit_end<<<1, 32, 0, s>>>(d, ctx->scratch, ed.builder, ed.tileOut);
     SVDAG_CUDA(cudaGetLastError());
     return SVDAG_OK;
 }
@@ -1304,31 +1230,29 @@ svdag_status run_edit_batch(svdag_ctx* ctx, const svdag_edit* edits, uint32_t co
     return SVDAG_OK;
 }
 
-// Scene construction: the terrain runs through the same pipeline as an edit of an empty DAG, with
-// fully-filled discovery on every level (the factory's create_dag_cpu propagates the fully-filled
-// bits everywhere, my_gpu_hash_dag_factory.cpp:350-353) and each level table sized from the exact
-// number of distinct items of that level (the reference resizes with setLoadFactor afterwards,
-// my_gpu_hash_dag.cu:139-155).
-svdag_status run_terrain_build(svdag_ctx* ctx, const svdag_terrain_params* p, cudaStream_t s)
+svdag_status reset_dag(svdag_ctx* ctx, cudaStream_t s)
 {
-    // Reset the DAG: empty item region, no tables, empty history.
     reset_level_tables(ctx);
-    {
-        Control init {};
-        init.root = kNone;
-        init.undoDepth = ctx->cfg.undo_depth ? std::min<uint32_t>(ctx->cfg.undo_depth, 64) : 32;
-        for (auto& lv : init.fullyFilled)
-            for (auto& m : lv)
-                m = kNone;
-        init.savedRoot = kNone;
-        SVDAG_CUDA(cudaMemcpyAsync(ctx->ctl, &init, sizeof(init), cudaMemcpyHostToDevice, s));
-    }
-    DevEditor ed {};
-    ed.tool = kToolTerrain;
-    ed.terrain = *p;
-    ed.levels = ctx->cfg.levels;
-    ed.terrainBaseLog2 = ctx->cfg.levels - 2;
-    ed.builder = 1;
+    Control init {};
+    init.root = kNone;
+    init.undoDepth = ctx->cfg.undo_depth ? std::min<uint32_t>(ctx->cfg.undo_depth, 64) : 32;
+    for (auto& lv : init.fullyFilled)
+        for (auto& m : lv)
+            m = kNone;
+    init.savedRoot = kNone;
+    SVDAG_CUDA(cudaMemcpyAsync(ctx->ctl, &init, sizeof(init), cudaMemcpyHostToDevice, s));
+    SVDAG_CUDA(cudaStreamSynchronize(s));
+    return SVDAG_OK;
+}
+
+// Scene construction in one pass: the scene runs through the same pipeline as an edit of an empty
+// DAG, with fully-filled discovery on every level (the factory's create_dag_cpu propagates the
+// fully-filled bits everywhere, my_gpu_hash_dag_factory.cpp:350-353) and each level table sized from
+// the exact number of distinct items of that level (the reference resizes with setLoadFactor
+// afterwards, my_gpu_hash_dag.cu:139-155).
+svdag_status build_scene_untiled(svdag_ctx* ctx, const DevEditor& ed, cudaStream_t s)
+{
+    SVDAG_TRY(reset_dag(ctx, s));
     const DevDag d = ctx->dag();
     SVDAG_CUDA(cudaMemsetAsync(&ctx->ctl->edit, 0, sizeof(EditCounters), s));
     k_edit_begin<<<1, 32, 0, s>>>(d, ed, ctx->scratch);
@@ -1358,9 +1282,43 @@ svdag_status run_terrain_build(svdag_ctx* ctx, const svdag_terrain_params* p, cu
         SVDAG_TRY(insert_canonical(ctx, (uint32_t)level, s));
         SVDAG_TRY(launch_insert(ctx, level, level_bound(level), s));
     }
-    k_edit_end<<<1, 32, 0, s>>>(d, ctx->scratch, 1);
+    k_edit_end<<<1, 32, 0, s>>>(d, ctx->scratch, 1, nullptr);
     SVDAG_CUDA(cudaGetLastError());
     return read_status(ctx, s);
+}
+
+// Tiles of a scene: every tile is a builder edit of the subtree under one node, all tiles of a call
+// in one persistent launch (the level tables exist already; the merge phase finds or inserts).
+svdag_status launch_scene_tiles(svdag_ctx* ctx, const DevEditor* eds, uint32_t n, cudaStream_t s)
+{
+    if (ctx->sceneGrid < 0) {
+        int perSm = 0, sms = 0, coop = 0;
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ctx->device);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+        if (coop && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_scene_fused, 256, 0) == cudaSuccess)
+            ctx->sceneGrid = perSm * sms;
+        else
+            ctx->sceneGrid = 0;
+        cudaGetLastError();
+    }
+    if (ctx->sceneGrid <= 0) {
+        for (uint32_t i = 0; i < n; ++i)
+            SVDAG_TRY(launch_pipeline(ctx, eds[i], s));
+        return SVDAG_OK;
+    }
+    const uint32_t perLaunch = (uint32_t)(ctx->batchBytes / sizeof(DevEditor));
+    for (uint32_t i = 0; i < n; i += perLaunch) {
+        uint32_t m = std::min(perLaunch, n - i);
+        SVDAG_CUDA(cudaMemcpyAsync(ctx->batch, eds + i, (size_t)m * sizeof(DevEditor), cudaMemcpyHostToDevice, s));
+        DevDag d = ctx->dag();
+        const DevEditor* devEds = reinterpret_cast<const DevEditor*>(ctx->batch);
+        char* scratch = ctx->scratch;
+        unsigned long long scratchBytes = ctx->scratchBytes;
+        void* args[] = { &d, &devEds, &m, &scratch, &scratchBytes };
+        SVDAG_CUDA(cudaLaunchCooperativeKernel((const void*)k_scene_fused, dim3(ctx->sceneGrid), dim3(256), args, 0, s));
+        SVDAG_CUDA(cudaStreamSynchronize(s)); // the batch region is reused by the next launch
+    }
+    return SVDAG_OK;
 }
 
 } // namespace svdag
@@ -1374,9 +1332,9 @@ svdag_status svdag_build_terrain(svdag_ctx* ctx, const svdag_terrain_params* p, 
     if (!ctx || !p || p->octaves == 0 || p->octaves > 16 || p->num_materials == 0 || p->num_materials > SVDAG_NUM_MATERIALS
         || p->max_height_pct > 100 || p->min_height_pct > p->max_height_pct)
         return SVDAG_ERR_INVALID;
-    if (p->num_structures != 0)
-        return SVDAG_ERR_UNSUPPORTED;
-    return run_terrain_build(ctx, p, as_stream(stream));
+    if (p->num_structures > 65536 || p->tile_level > std::min<uint32_t>(ctx->cfg.levels - 3, 6))
+        return SVDAG_ERR_INVALID;
+    return run_scene_build(ctx, p, as_stream(stream));
 }
 
 svdag_status svdag_edit_apply(svdag_ctx* ctx, const svdag_edit* e, void* stream)

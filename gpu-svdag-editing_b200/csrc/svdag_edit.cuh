@@ -6,6 +6,7 @@
 // uncontracted IEEE evaluation the oracle performs on the CPU.
 #pragma once
 #include "svdag_device.cuh"
+#include "svdag_scene.cuh"
 
 namespace svdag {
 
@@ -23,9 +24,11 @@ struct DevEditor {
     float fDestToSource[3];
     int32_t iDestToSource[3];
     uint32_t noiseSeed, noiseCellLog2;
-    svdag_terrain_params terrain;
-    uint32_t terrainBaseLog2;
+    SceneParams scene; // scene builder: heightfield and structures
     uint32_t levels;
+    uint32_t startLevel; // the edit covers the subtree of the node (startLevel, startPath); 0 = whole DAG
+    uint32_t startPath[3];
+    uint32_t* tileOut; // scene builder tiles: the subtree's handle goes here instead of the root
     uint32_t useSavedSource; // copy: read the source from the saved root (move)
     uint32_t saveRoot; // remember the root before this edit as the source of a later copy (move)
     uint32_t builder; // scene build: fully-filled discovery on every level, no undo frame

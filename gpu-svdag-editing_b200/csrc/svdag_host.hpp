@@ -27,6 +27,7 @@ struct svdag_ctx {
     char* batch = nullptr; // editors and per-edit records of a persistent batch launch
     unsigned long long batchBytes = 0;
     int fusedGrid = -1; // co-resident blocks of the persistent edit kernel (0 = unavailable)
+    int sceneGrid = -1; // same for the scene tile kernel
     uint32_t lastBatch = 0;
     uint32_t* items = nullptr; // item region
     unsigned long long itemWords = 0;
@@ -74,10 +75,23 @@ svdag_status insert_canonical(svdag_ctx* ctx, uint32_t level, cudaStream_t s);
 svdag_status upload_tables(svdag_ctx* ctx, cudaStream_t s);
 svdag_status read_status(svdag_ctx* ctx, cudaStream_t s);
 void reset_level_tables(svdag_ctx* ctx);
+// Find-or-insert of keys that are pairwise distinct (no batch dedup) into a level table.
+svdag_status find_or_insert_distinct(svdag_ctx* ctx, uint32_t level, const uint32_t* keys, const uint32_t* offsets, uint32_t n,
+    unsigned long long totalWords, uint32_t* out, cudaStream_t s);
+// Items per size class of a table (`scratch`: 9 device words).
+svdag_status table_class_counts(svdag_ctx* ctx, const svdag_table& t, unsigned long long* perClass, unsigned long long* scratch, cudaStream_t s);
 
 // Edit machinery (svdag_edit.cu).
 svdag_status run_edit(svdag_ctx* ctx, const svdag_edit* e, cudaStream_t s);
 svdag_status run_edit_batch(svdag_ctx* ctx, const svdag_edit* edits, uint32_t count, cudaStream_t s);
-svdag_status run_terrain_build(svdag_ctx* ctx, const svdag_terrain_params* p, cudaStream_t s);
+struct DevEditor;
+// Resets the DAG to empty: no items, no tables, empty history.
+svdag_status reset_dag(svdag_ctx* ctx, cudaStream_t s);
+// Scene build in one pass over the whole grid, level tables sized exactly per level (svdag_edit.cu).
+svdag_status build_scene_untiled(svdag_ctx* ctx, const DevEditor& ed, cudaStream_t s);
+// Builds the subtrees of scene tiles, one builder editor per tile (svdag_edit.cu).
+svdag_status launch_scene_tiles(svdag_ctx* ctx, const DevEditor* eds, uint32_t n, cudaStream_t s);
+// Procedural scene construction (svdag_scene.cu).
+svdag_status run_scene_build(svdag_ctx* ctx, const svdag_terrain_params* p, cudaStream_t s);
 
 } // namespace svdag

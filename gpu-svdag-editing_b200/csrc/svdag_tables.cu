@@ -580,3 +580,60 @@ svdag_status svdag_export_level(svdag_ctx* ctx, uint32_t level, uint32_t* outHan
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------- helpers of the scene builder
+
+namespace {
+
+// Items per size class of a table: one thread per bucket walks its chain.
+__global__ void k_table_class_counts(DevDag d, DevTable t, unsigned long long* perClass)
+{
+    for (uint32_t c = 0; c < kNumClasses; ++c) {
+        const uint32_t k = c + 2;
+        unsigned long long items = 0;
+        for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < t.numBuckets[c]; b += gridDim.x * blockDim.x) {
+            uint32_t slab = t.bucketBase[c] + b * slab_sectors(k);
+            for (uint32_t steps = 0; steps < kMaxChain; ++steps) {
+                const uint32_t* h = slab_ptr(d, slab);
+                for (uint32_t s = 0; s < kSlots; ++s) {
+                    const uint32_t tag = (h[s % 7u] >> (8u * (s / 7u))) & 0xFFu;
+                    items += (tag != 0 && tag != kTagBusy) ? 1u : 0u;
+                }
+                const uint32_t next = h[7];
+                if (next == kEnd)
+                    break;
+                if (!slab_ok(d, next)) {
+                    set_status(d.ctl, SVDAG_ERR_CORRUPT);
+                    break;
+                }
+                slab = next;
+            }
+        }
+        if (items)
+            atomicAdd(&perClass[c], items);
+    }
+}
+
+} // namespace
+
+namespace svdag {
+
+svdag_status find_or_insert_distinct(svdag_ctx* ctx, uint32_t level, const uint32_t* keys, const uint32_t* offsets, uint32_t n,
+    unsigned long long totalWords, uint32_t* out, cudaStream_t s)
+{
+    if (!n)
+        return SVDAG_OK;
+    return launch_table_op<OP_FIND_OR_INSERT>(&ctx->levelTables[level], keys, offsets, n, totalWords, nullptr, out, 1, s);
+}
+
+svdag_status table_class_counts(svdag_ctx* ctx, const svdag_table& t, unsigned long long* perClass, unsigned long long* scratch, cudaStream_t s)
+{
+    SVDAG_CUDA(cudaMemsetAsync(scratch, 0, kNumClasses * sizeof(unsigned long long), s));
+    k_table_class_counts<<<grid_for(ctx, 1u << 20, 256), 256, 0, s>>>(ctx->dag(), t.dev, scratch);
+    SVDAG_CUDA(cudaGetLastError());
+    SVDAG_CUDA(cudaMemcpyAsync(perClass, scratch, kNumClasses * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    SVDAG_CUDA(cudaStreamSynchronize(s));
+    return SVDAG_OK;
+}
+
+} // namespace svdag

@@ -55,7 +55,7 @@ class Config(C.Structure):
 class TerrainParams(C.Structure):
     _fields_ = [("seed", C.c_uint32), ("octaves", C.c_uint32), ("num_materials", C.c_uint32),
                 ("min_height_pct", C.c_uint32), ("max_height_pct", C.c_uint32),
-                ("num_structures", C.c_uint32), ("structure_seed", C.c_uint32), ("reserved", C.c_uint32)]
+                ("num_structures", C.c_uint32), ("structure_seed", C.c_uint32), ("tile_level", C.c_uint32)]
 
 
 class Edit(C.Structure):
@@ -297,9 +297,11 @@ class MyGPUHashDAG:
     def sync(self, stream=None):
         _check(lib().svdag_sync(self.h, stream_ptr(stream)), "svdag_sync")
 
-    def build_terrain(self, seed=0, octaves=5, num_materials=8, min_height_pct=40, max_height_pct=70, stream=None):
+    def build_terrain(self, seed=0, octaves=5, num_materials=8, min_height_pct=40, max_height_pct=70,
+                      num_structures=0, structure_seed=0, tile_level=0, stream=None):
         p = TerrainParams(seed=seed, octaves=octaves, num_materials=num_materials, min_height_pct=min_height_pct,
-                          max_height_pct=max_height_pct)
+                          max_height_pct=max_height_pct, num_structures=num_structures,
+                          structure_seed=structure_seed, tile_level=tile_level)
         _check(lib().svdag_build_terrain(self.h, C.byref(p), stream_ptr(stream)), "svdag_build_terrain")
 
     def edit(self, editor, stream=None):

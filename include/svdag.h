@@ -88,10 +88,25 @@ typedef struct svdag_terrain_params {
     uint32_t num_materials; /* height bands -> materials [0, num_materials) (8 or 16) */
     uint32_t min_height_pct; /* surface height range, in percent of the grid height */
     uint32_t max_height_pct;
-    uint32_t num_structures; /* random boxes/spheres unioned on the surface (0 = none) */
+    uint32_t num_structures; /* random boxes/spheres unioned on the surface (0 = none), at most 65536 */
     uint32_t structure_seed;
-    uint32_t reserved;
+    uint32_t tile_level; /* level (at most min(levels - 3, 6)) at which the build is cut into
+                            independently built tiles; 0 = automatic (levels - 13 above depth 13,
+                            untiled otherwise) */
 } svdag_terrain_params;
+
+/* The scene. Voxel (x, y, z) of a 2^levels grid is solid when y < height(x, z) or when a structure
+ * contains it; its material is that of the highest-index structure containing it, else the height
+ * band (y * num_materials) >> levels. height(x, z) is integer value-noise fBm: octave o has lattice
+ * cells of 2^max(levels-2-o, 0) voxels, lattice values fmix32-hashed from (seed, o, ix, iz) in
+ * [0, 65535], smoothstep-weighted bilinear interpolation in 16.16 fixed point, weight 2^(octaves-1-o);
+ * the sum maps linearly onto [min_height_pct, max_height_pct] of the grid height.
+ *
+ * Structure i (i = 0 .. num_structures-1) draws from one splitmix64 stream seeded with
+ * structure_seed, in this order: x = next % 2^levels, z = next % 2^levels, kind = next & 1
+ * (0 box, 1 sphere), material = next % 16, size = next; with h = height(x, z):
+ *   box: side = 16 + size % 497, voxels [x - side/2, x - side/2 + side) (same for y around h, z);
+ *   sphere: radius r = 8 + size % 249, voxels v with |v - (x, h, z)|^2 <= r^2. */
 
 /* Builds a procedural heightfield terrain into an empty context; stands in for the reference's
  * scene load MyGPUHashDAGFactory::load_from_DAG (my_gpu_hash_dag_factory.cpp:427-500). Every

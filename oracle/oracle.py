@@ -34,7 +34,7 @@ def build(force: bool = False) -> str:
 class TerrainParams(C.Structure):
     _fields_ = [("seed", C.c_uint32), ("octaves", C.c_uint32), ("num_materials", C.c_uint32),
                 ("min_height_pct", C.c_uint32), ("max_height_pct", C.c_uint32),
-                ("num_structures", C.c_uint32), ("structure_seed", C.c_uint32), ("reserved", C.c_uint32)]
+                ("num_structures", C.c_uint32), ("structure_seed", C.c_uint32), ("tile_level", C.c_uint32)]
 
 
 class Edit(C.Structure):
@@ -102,6 +102,10 @@ def lib():
                                           C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
         L.oracle_canonicalize.argtypes = [P, C.POINTER(Canon)]
         L.oracle_canonicalize_dump.argtypes = [C.c_uint32, C.c_uint32, P, P, P, C.POINTER(Canon)]
+        L.oracle_canonicalize_dump_at.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, P, P, P, C.POINTER(Canon)]
+        L.oracle_canonicalize_at.argtypes = [P, C.c_uint32, C.c_uint32, C.POINTER(Canon)]
+        L.oracle_build_scene_subtree.argtypes = [P, C.POINTER(TerrainParams), C.c_uint32, P, C.POINTER(C.c_uint32)]
+        L.oracle_scene_voxels.argtypes = [C.POINTER(TerrainParams), C.c_uint32, P, C.c_uint64, P]
         L.oracle_encode_node_header.restype = C.c_uint32
         L.oracle_encode_node_header.argtypes = [C.c_uint32, C.c_uint32]
         L.oracle_header_child_mask.restype = C.c_uint32
@@ -154,6 +158,20 @@ class OracleDag:
         if r:
             raise RuntimeError(f"oracle_build_terrain -> {r}")
 
+    def build_scene_subtree(self, params: TerrainParams, level: int, path) -> int:
+        """Builds only the subtree of scene node (level, path); returns its handle at `level`."""
+        p = np.ascontiguousarray(path, dtype=np.uint32)
+        h = C.c_uint32()
+        r = lib().oracle_build_scene_subtree(self.h, C.byref(params), level, _ptr(p), C.byref(h))
+        if r:
+            raise RuntimeError(f"oracle_build_scene_subtree -> {r}")
+        return h.value
+
+    def canon_at(self, level: int, handle: int) -> dict:
+        c = Canon()
+        lib().oracle_canonicalize_at(self.h, level, handle, C.byref(c))
+        return c.as_dict(self.levels)
+
     def build_box(self, bmin: float, bmax: float, material: int):
         lib().oracle_build_box(self.h, bmin, bmax, material)
 
@@ -201,8 +219,17 @@ class OracleDag:
         return c.as_dict(self.levels)
 
 
-def canonicalize_dump(levels: int, root: int, dumps) -> dict:
-    """dumps[l] = (handles uint32[n], words uint32[n, 10]) for every level 0..levels-2."""
+def scene_voxels(params: TerrainParams, levels: int, xyz: np.ndarray) -> np.ndarray:
+    """Voxels of the scene straight from its definition (no DAG)."""
+    xyz = np.ascontiguousarray(xyz, dtype=np.uint32).reshape(-1, 3)
+    out = np.empty(len(xyz), dtype=np.uint32)
+    lib().oracle_scene_voxels(C.byref(params), levels, _ptr(xyz), len(xyz), _ptr(out))
+    return out
+
+
+def canonicalize_dump(levels: int, root: int, dumps, level: int = 0) -> dict:
+    """dumps[l] = (handles uint32[n], words uint32[n, 10]) for every level 0..levels-2; `root` is an
+    item of `level`."""
     n = levels - 1
     hs = [np.ascontiguousarray(d[0], dtype=np.uint32) for d in dumps]
     ws = [np.ascontiguousarray(d[1], dtype=np.uint32) for d in dumps]
@@ -210,7 +237,7 @@ def canonicalize_dump(levels: int, root: int, dumps) -> dict:
     wp = (C.c_void_p * n)(*[w.ctypes.data for w in ws])
     counts = np.array([len(h) for h in hs], dtype=np.uint64)
     c = Canon()
-    r = lib().oracle_canonicalize_dump(levels, root, hp, wp, _ptr(counts), C.byref(c))
+    r = lib().oracle_canonicalize_dump_at(levels, level, root, hp, wp, _ptr(counts), C.byref(c))
     if r:
         raise RuntimeError("dump references a handle that is not in the dump")
     return c.as_dict(levels)

@@ -942,6 +942,80 @@ struct Terrain {
     uint32_t material(uint32_t y) const { return (uint32_t)(((uint64_t)y * p.num_materials) >> levels); }
 };
 
+// Boxes and spheres unioned on the terrain surface, drawn from one splitmix64 stream in the order
+// the svdag_terrain_params documentation gives.
+struct Scene {
+    struct Structure {
+        int64_t lo[3], hi[3]; // voxel bounding box [lo, hi)
+        int64_t c[3];
+        int64_t r2;
+        bool sphere;
+        uint32_t material;
+    };
+    Terrain t;
+    std::vector<Structure> s;
+
+    static uint64_t splitmix(uint64_t& x)
+    {
+        x += 0x9E3779B97F4A7C15ull;
+        uint64_t z = x;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    }
+    Scene(const svdag_terrain_params& p, uint32_t levels) : t { p, levels, levels - 2, {} }
+    {
+        const uint64_t G = uint64_t(1) << levels;
+        uint64_t st = p.structure_seed;
+        for (uint32_t i = 0; i < p.num_structures; ++i) {
+            const uint64_t x = splitmix(st) % G, z = splitmix(st) % G;
+            const bool sphere = splitmix(st) & 1u;
+            const uint32_t material = (uint32_t)(splitmix(st) % 16);
+            const uint64_t size = splitmix(st);
+            const int64_t c[3] = { (int64_t)x, (int64_t)t.height((uint32_t)x, (uint32_t)z), (int64_t)z };
+            Structure q {};
+            q.sphere = sphere;
+            q.material = material;
+            if (!sphere) {
+                const int64_t side = 16 + (int64_t)(size % 497);
+                for (int a = 0; a < 3; ++a) {
+                    q.lo[a] = c[a] - side / 2;
+                    q.hi[a] = q.lo[a] + side;
+                }
+            } else {
+                const int64_t r = 8 + (int64_t)(size % 249);
+                q.r2 = r * r;
+                for (int a = 0; a < 3; ++a) {
+                    q.c[a] = c[a];
+                    q.lo[a] = c[a] - r;
+                    q.hi[a] = c[a] + r + 1;
+                }
+            }
+            s.push_back(q);
+        }
+    }
+    bool contains(const Structure& q, int64_t x, int64_t y, int64_t z) const
+    {
+        if (q.sphere) {
+            const int64_t dx = x - q.c[0], dy = y - q.c[1], dz = z - q.c[2];
+            return dx * dx + dy * dy + dz * dz <= q.r2;
+        }
+        return x >= q.lo[0] && x < q.hi[0] && y >= q.lo[1] && y < q.hi[1] && z >= q.lo[2] && z < q.hi[2];
+    }
+    bool touches(const Structure& q, int64_t x0, int64_t y0, int64_t z0, int64_t n) const
+    {
+        return x0 < q.hi[0] && x0 + n > q.lo[0] && y0 < q.hi[1] && y0 + n > q.lo[1] && z0 < q.hi[2] && z0 + n > q.lo[2];
+    }
+    // Material of a voxel (kSentinel = empty), among the structures listed in `active`.
+    uint32_t voxel(uint32_t x, uint32_t y, uint32_t z, uint32_t height, const std::vector<uint32_t>& active) const
+    {
+        for (size_t k = active.size(); k-- > 0;)
+            if (contains(s[active[k]], x, y, z))
+                return s[active[k]].material;
+        return y < height ? t.material(y) : kSentinel;
+    }
+};
+
 struct BuildResult {
     uint32_t handle;
     uint32_t fillMaterial; // kSentinel unless uniformly filled
@@ -950,19 +1024,28 @@ struct BuildResult {
 // Factory-style recursive construction (create_dag_cpu, my_gpu_hash_dag_factory.cpp:317-409):
 // children first, fully-filled bits wherever all 8 children are filled with one material,
 // find-then-add per item. Height bounds only prune uniform subtrees (they are conservative).
-BuildResult build_terrain_rec(Dag& dag, const Terrain& t, uint32_t level, const Path& path, std::vector<uint32_t>& col)
+// Structures only add subdivision: a node that any structure's bounding box touches is subdivided
+// down to the leaves, where every voxel is evaluated.
+BuildResult build_terrain_rec(Dag& dag, const Scene& sc, uint32_t level, const Path& path, const std::vector<uint32_t>& parentActive)
 {
+    const Terrain& t = sc.t;
     const uint32_t depth = dag.levels - level;
     const uint32_t s = 1u << depth;
     const uint32_t x0 = path.x << depth, y0 = path.y << depth, z0 = path.z << depth;
-    uint32_t hlo, hhi;
-    t.bounds(x0, z0, s, hlo, hhi);
-    if (y0 >= hhi)
-        return { kSentinel, kSentinel };
-    if (y0 + s <= hlo) {
-        const uint32_t m0 = t.material(y0), m1 = t.material(y0 + s - 1);
-        if (m0 == m1)
-            return { dag.fullyFilled[level][m0], m0 };
+    std::vector<uint32_t> active;
+    for (uint32_t i : parentActive)
+        if (sc.touches(sc.s[i], x0, y0, z0, s))
+            active.push_back(i);
+    if (active.empty()) {
+        uint32_t hlo, hhi;
+        t.bounds(x0, z0, s, hlo, hhi);
+        if (y0 >= hhi)
+            return { kSentinel, kSentinel };
+        if (y0 + s <= hlo) {
+            const uint32_t m0 = t.material(y0), m1 = t.material(y0 + s - 1);
+            if (m0 == m1)
+                return { dag.fullyFilled[level][m0], m0 };
+        }
     }
     if (level == dag.leaf_level()) {
         uint32_t h[4][4];
@@ -979,8 +1062,8 @@ BuildResult build_terrain_rec(Dag& dag, const Terrain& t, uint32_t level, const 
             const uint32_t dx = ((c >> 2) & 1u) * 2 + ((f >> 2) & 1u);
             const uint32_t dy = ((c >> 1) & 1u) * 2 + ((f >> 1) & 1u);
             const uint32_t dz = (c & 1u) * 2 + (f & 1u);
-            if (y0 + dy < h[dx][dz]) {
-                const uint32_t m = t.material(y0 + dy);
+            const uint32_t m = sc.voxel(x0 + dx, y0 + dy, z0 + dz, h[dx][dz], active);
+            if (m != kSentinel) {
                 b.set(m);
                 mask |= 1ull << v;
                 if (v == 0)
@@ -1002,7 +1085,7 @@ BuildResult build_terrain_rec(Dag& dag, const Terrain& t, uint32_t level, const 
     for (uint32_t c = 0; c < 8; ++c) {
         Path cp = path;
         cp.descend(c);
-        const BuildResult r = build_terrain_rec(dag, t, level + 1, cp, col);
+        const BuildResult r = build_terrain_rec(dag, sc, level + 1, cp, active);
         fills[c] = r.fillMaterial;
         if (r.handle != kSentinel) {
             mask |= 1u << c;
@@ -1352,7 +1435,7 @@ struct Canon {
         vox = v;
         return h;
     }
-    void run(uint32_t root, oracle_canon* out)
+    void run(uint32_t root, oracle_canon* out, uint32_t startLevel = 0)
     {
         std::memset(out, 0, sizeof(*out));
         digest.assign(levels, {});
@@ -1360,7 +1443,7 @@ struct Canon {
         if (root == kSentinel)
             return;
         __uint128_t total = 0;
-        out->root_digest = visit(0, root, total);
+        out->root_digest = visit(startLevel, root, total);
         out->voxel_count_lo = (uint64_t)total;
         out->voxel_count_hi = (uint64_t)(total >> 64);
         for (uint32_t l = 0; l + 1 < levels; ++l) {
@@ -1402,12 +1485,44 @@ int oracle_build_terrain(oracle_dag* d, const svdag_terrain_params* params)
     if (!d || !params || params->octaves == 0 || params->num_materials == 0 || params->num_materials > kNumMaterials
         || params->max_height_pct > 100 || params->min_height_pct > params->max_height_pct)
         return SVDAG_ERR_INVALID;
-    if (params->num_structures != 0)
-        return SVDAG_ERR_UNSUPPORTED;
     d->dag.init(d->dag.levels);
-    Terrain t { *params, d->dag.levels, d->dag.levels - 2, {} };
-    std::vector<uint32_t> col;
-    d->dag.root = build_terrain_rec(d->dag, t, 0, Path {}, col).handle;
+    const Scene sc(*params, d->dag.levels);
+    std::vector<uint32_t> all(sc.s.size());
+    for (uint32_t i = 0; i < all.size(); ++i)
+        all[i] = i;
+    d->dag.root = build_terrain_rec(d->dag, sc, 0, Path {}, all).handle;
+    return SVDAG_OK;
+}
+
+int oracle_build_scene_subtree(oracle_dag* d, const svdag_terrain_params* params, uint32_t level, const uint32_t path[3], uint32_t* out_handle)
+{
+    if (!d || !params || !path || !out_handle || level >= d->dag.leaf_level() || params->octaves == 0 || params->num_materials == 0)
+        return SVDAG_ERR_INVALID;
+    d->dag.init(d->dag.levels);
+    const Scene sc(*params, d->dag.levels);
+    std::vector<uint32_t> all(sc.s.size());
+    for (uint32_t i = 0; i < all.size(); ++i)
+        all[i] = i;
+    Path p {};
+    p.x = path[0];
+    p.y = path[1];
+    p.z = path[2];
+    *out_handle = build_terrain_rec(d->dag, sc, level, p, all).handle;
+    return SVDAG_OK;
+}
+
+int oracle_scene_voxels(const svdag_terrain_params* params, uint32_t levels, const uint32_t* xyz, uint64_t count, uint32_t* out)
+{
+    if (!params || !xyz || !out || params->octaves == 0 || params->num_materials == 0)
+        return SVDAG_ERR_INVALID;
+    const Scene sc(*params, levels);
+    std::vector<uint32_t> all(sc.s.size());
+    for (uint32_t i = 0; i < all.size(); ++i)
+        all[i] = i;
+    for (uint64_t i = 0; i < count; ++i) {
+        const uint32_t x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2];
+        out[i] = sc.voxel(x, y, z, sc.t.height_uncached(x, z), all);
+    }
     return SVDAG_OK;
 }
 
@@ -1592,8 +1707,27 @@ int oracle_canonicalize(const oracle_dag* d, oracle_canon* out)
     return SVDAG_OK;
 }
 
+int oracle_canonicalize_at(const oracle_dag* d, uint32_t level, uint32_t handle, oracle_canon* out)
+{
+    Canon c;
+    c.levels = d->dag.levels;
+    const Dag* dag = &d->dag;
+    c.fetch = [dag](uint32_t l, uint32_t h) { return dag->ptr(l, h); };
+    c.run(handle, out, level);
+    return SVDAG_OK;
+}
+
+int oracle_canonicalize_dump_at(uint32_t levels, uint32_t level, uint32_t root, const uint32_t* const* handles,
+    const uint32_t* const* words, const uint64_t* counts, oracle_canon* out);
+
 int oracle_canonicalize_dump(uint32_t levels, uint32_t root, const uint32_t* const* handles, const uint32_t* const* words,
     const uint64_t* counts, oracle_canon* out)
+{
+    return oracle_canonicalize_dump_at(levels, 0, root, handles, words, counts, out);
+}
+
+int oracle_canonicalize_dump_at(uint32_t levels, uint32_t level, uint32_t root, const uint32_t* const* handles,
+    const uint32_t* const* words, const uint64_t* counts, oracle_canon* out)
 {
     std::vector<std::unordered_map<uint32_t, uint64_t>> where(levels);
     for (uint32_t l = 0; l + 1 < levels; ++l)
@@ -1611,7 +1745,7 @@ int oracle_canonicalize_dump(uint32_t levels, uint32_t root, const uint32_t* con
         }
         return &words[level][it->second * SVDAG_MAX_ITEM_WORDS];
     };
-    c.run(root, out);
+    c.run(root, out, level);
     return bad ? SVDAG_ERR_CORRUPT : SVDAG_OK;
 }
 

@@ -39,6 +39,12 @@ int oracle_is_empty(const oracle_dag* dag);
 int oracle_build_terrain(oracle_dag* dag, const svdag_terrain_params* params);
 /* The reference test scene of gpu_hash_dag_tests.cpp:35-89 (createBoxDag): an axis-aligned box. */
 int oracle_build_box(oracle_dag* dag, float bmin, float bmax, uint32_t material);
+/* Builds only the subtree of the scene node (level, path) into an emptied DAG; *out_handle is its
+ * handle at `level` (0xFFFFFFFF = empty). */
+int oracle_build_scene_subtree(oracle_dag* dag, const svdag_terrain_params* params, uint32_t level, const uint32_t path[3],
+    uint32_t* out_handle);
+/* The scene's voxels straight from its definition (no DAG): material or 0xFFFFFFFF. */
+int oracle_scene_voxels(const svdag_terrain_params* params, uint32_t levels, const uint32_t* xyz, uint64_t count, uint32_t* out);
 
 int oracle_edit(oracle_dag* dag, const svdag_edit* edit, svdag_edit_stats* out_stats);
 int oracle_undo(oracle_dag* dag);
@@ -56,6 +62,10 @@ int oracle_trace_counts(const oracle_dag* dag, const svdag_trace_params* params,
 int oracle_canonicalize(const oracle_dag* dag, oracle_canon* out);
 /* Canonicalises a DAG given as per-level dumps of (handle, 10 padded words) records, as produced
  * by svdag_export_level. handles[l]/words[l] have counts[l] entries. */
+/* Canonical form of the subtree under the item `handle` of `level`. */
+int oracle_canonicalize_at(const oracle_dag* dag, uint32_t level, uint32_t handle, oracle_canon* out);
+int oracle_canonicalize_dump_at(uint32_t levels, uint32_t level, uint32_t root, const uint32_t* const* handles,
+    const uint32_t* const* words, const uint64_t* counts, oracle_canon* out);
 int oracle_canonicalize_dump(uint32_t levels, uint32_t root, const uint32_t* const* handles,
     const uint32_t* const* words, const uint64_t* counts, oracle_canon* out);
 

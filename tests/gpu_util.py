@@ -13,6 +13,50 @@ def gpu_canon(oracle_mod, dag):
     return oracle_mod.canonicalize_dump(levels, root, dumps)
 
 
+def gpu_read(dag, level, handles):
+    """Item words (n, 10) of the given handles of one level."""
+    import torch
+
+    h = torch.from_numpy(np.ascontiguousarray(handles, dtype=np.uint32).view(np.int32)).cuda()
+    out = torch.empty((len(handles), 10), dtype=torch.int32, device="cuda")
+    dag.table(level).read(h, len(handles), out)
+    torch.cuda.synchronize()
+    return out.cpu().numpy().view(np.uint32)
+
+
+def gpu_node_at(dag, level, path):
+    """Handle of the node (level, path) of the GPU DAG, or None where the subtree is empty."""
+    h = dag.get_first_node_index()
+    for l in range(level):
+        if h == 0xFFFFFFFF:
+            return None
+        w = gpu_read(dag, l, [h])[0]
+        s = level - l - 1
+        c = (((path[0] >> s) & 1) << 2) | (((path[1] >> s) & 1) << 1) | ((path[2] >> s) & 1)
+        mask = int(w[0]) & 0xFF
+        if not (mask >> c) & 1:
+            return None
+        h = int(w[1 + bin(mask & ((1 << c) - 1)).count("1")])
+    return h
+
+
+def gpu_subtree_canon(oracle_mod, dag, level, handle):
+    """Canonical form of the GPU DAG's subtree under `handle` (an item of `level`), read item by item."""
+    levels = dag.levels
+    empty = (np.zeros(0, np.uint32), np.zeros((0, 10), np.uint32))
+    dumps = [empty] * (levels - 1)
+    frontier = np.array([handle], dtype=np.uint32)
+    for l in range(level, levels - 1):
+        words = gpu_read(dag, l, frontier)
+        dumps[l] = (frontier, words)
+        if l == levels - 2:
+            break
+        pc = np.array([bin(int(m) & 0xFF).count("1") for m in words[:, 0]])
+        kids = np.concatenate([words[i, 1:1 + pc[i]] for i in range(len(frontier))])
+        frontier = np.unique(kids).astype(np.uint32)
+    return oracle_mod.canonicalize_dump(levels, handle, dumps, level)
+
+
 def random_bricks(rng, levels, n, size=16):
     g = 1 << levels
     lo = rng.integers(0, g - size, size=(n, 3))
