@@ -1,14 +1,22 @@
-"""Benchmark of the per-edit SVDAG editing path on B200 (one JSON line on rank 0).
+"""Benchmark of the SVDAG editing path on B200 (one JSON line on rank 0).
 
-Step = one edit of the seeded C0 stream (sphere add/remove near the surface of a depth-10 fBm
-terrain, radius U{4..64}) followed by one 256x256 primary-ray frame (edit-to-visible).
-value = edited voxels per second over the timed steps (Mvox/s), with p50/p99 edit-to-visible
-latency beside it; `e2e` repeats the steps through the C ABI with the edit read from host memory
-and the hit buffer copied back to pinned host memory every step. The slab-hash find/insert kernels
-are measured on the 2^24-key microbenchmark and give the `roofline` object.
+Default workload (--mode serve): the served edit stream on the at-scale scene. The scene is the
+depth-17 (131072^3) fBm terrain with 8 octaves and 4096 boxes/spheres on the surface, built on the
+GPU; the stream is Poisson edit arrivals (add / remove / paint / copy 35/35/20/10, radius
+log-uniform 2..2048, centres on the surface) with 1920x1080 frame requests at 60 Hz, undo history 32
+deep, admission under a 120 GB cap. The same timed request stream is replayed against the serving
+form (continuous batching) and against the plain per-edit path (one request at a time, an edit then a
+frame); `value` is the served p99 edit-to-visible latency, with the plain path's beside it.
+`e2e` repeats the served replay with every frame copied to pinned host memory.
 
---impl reference times the reference algorithm on the host cores (the CPU oracle restatement of the
-MyGpuDag pipeline; the reference has no CPU implementation of that pipeline) on the same config.
+A step is one window of `--window` seconds of the stream; W windows are replayed untimed first, then
+K windows in one continuous replay. Other modes (profiling entry points): c0 (depth-10 per-edit
+path), c2 (the at-scale edit sequence), c3 (256 uneven edits, batched vs plain), hash (the 2^24-key
+slab-hash microbenchmark).
+
+--impl reference times the reference algorithm on the host cores: the CPU restatement of the
+MyGpuDag pipeline (the reference has no CPU implementation of it) on a bounded sample of the same
+stream, each edit on the scene clipped to its footprint.
 """
 from __future__ import annotations
 
@@ -27,12 +35,10 @@ for p in (ROOT, PKG):
     if p not in sys.path:
         sys.path.insert(0, p)
 
-LEVELS = 10
-TERRAIN = dict(seed=0, octaves=5, num_materials=8, min_height_pct=40, max_height_pct=70)
-EDIT_SEED = 2024
-FRAME = 256
 METRIC = "p99 edit latency & edited Mvox/s, served vs per-edit, bit-exact DAG, 1 B200"
 HBM_FALLBACK_GBS = 6650.0
+POOL_CAP = 120 << 30
+C0_FRAME = 256
 
 
 def measured_peak_gbs():
@@ -43,29 +49,12 @@ def measured_peak_gbs():
         return HBM_FALLBACK_GBS, "fallback"
 
 
-def c0_edits(n, seed=EDIT_SEED):
-    """Sphere edits of config 0: centre within +-32 voxels of the surface, radius U{4..64},
-    50% add / 50% remove, add material U[0,8). Heights come from the terrain definition."""
-    from oracle import oracle  # the terrain height function is shared with the checker
-
-    L = oracle.lib()
-    p = oracle.TerrainParams(**TERRAIN)
-    rng = np.random.default_rng(seed)
-    g = 1 << LEVELS
-    out = []
-    for _ in range(n):
-        x, z = (int(v) for v in rng.integers(0, g, 2))
-        h = L.oracle_terrain_height(p, LEVELS, x, z)
-        c = (float(x + rng.integers(-32, 33)), float(h + rng.integers(-32, 33)), float(z + rng.integers(-32, 33)))
-        r = float(rng.integers(4, 65))
-        add = bool(rng.integers(0, 2))
-        out.append((0 if add else 1, int(rng.integers(0, 8)), c, r))
-    return out
+def pct(a, q):
+    return float(np.percentile(np.asarray(a, dtype=np.float64), q)) if len(a) else None
 
 
 class ClockSampler:
-    """SM clock and clock-event reasons polled through NVML every 5 ms during the timed region
-    (the per-edit steps are far shorter than nvidia-smi's 200 ms sampling period)."""
+    """SM clock and clock-event reasons polled through NVML every 5 ms during the timed region."""
 
     REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
                "sw_power_cap": 0x4, "hw_power_brake_slowdown": 0x80}
@@ -159,7 +148,7 @@ def gather_keys(words, offs, sizes, order):
     return words[idx], o.astype(np.uint32), s
 
 
-def run_hash_bench(svdag, torch, stream, n_total=1 << 24, load_factor=20, lanes=8, reps=3, pool=6 << 30):
+def run_hash_bench(svdag, torch, stream, n_total=1 << 24, load_factor=20, lanes=1, reps=3, pool=6 << 30):
     """Insert 2^24 keys (50% duplicates, stored twice as the reference's add does), then 2^24 finds
     (50% hits). Algorithmic bytes (per key of k words): find 4k + 32 + 4k*hit + 4, insert 4k + 32 + 4k + 4."""
     n_unique = n_total // 2
@@ -180,7 +169,6 @@ def run_hash_bench(svdag, torch, stream, n_total=1 << 24, load_factor=20, lanes=
     dev = lambda a: torch.from_numpy(np.ascontiguousarray(a).astype(np.uint32).view(np.int32)).cuda()
     d_iw, d_io, d_fw, d_fo = dev(iw), dev(io), dev(fw), dev(fo)
     out = torch.empty(n_total, dtype=torch.int32, device="cuda")
-    # buckets per size class ~ items of that class / load factor (stored items = 2^24)
     cls_items = np.bincount(isz - 2, minlength=9)[:9]
     buckets = np.maximum(1, cls_items // load_factor + 1).astype(np.uint32)
     ins_bytes = float(np.sum(4 * isz + 32 + 4 * isz + 4))
@@ -222,12 +210,56 @@ def run_hash_bench(svdag, torch, stream, n_total=1 << 24, load_factor=20, lanes=
     }
 
 
-# ------------------------------------------------------------------ per-edit path
+# ------------------------------------------------------------------ the served stream (C4 on the C2 scene)
 
-def run_mine(args):
+def c2_camera(svdag, levels, width=1920, height=1080):
+    g = float(1 << levels)
+    return svdag.get_trace_params((0.5 * g - 6000.0 * g / 131072, 0.62 * g, 0.5 * g - 6000.0 * g / 131072),
+                                  (0.5 * g, 0.52 * g, 0.5 * g), width, height)
+
+
+def make_scene(svdag, w, levels, phase_kernels=False):
+    dag = svdag.MyGPUHashDAG(levels, pool_bytes=min(POOL_CAP, 52 << 30), scratch_bytes=16 << 30, undo_depth=32,
+                             phase_kernels=phase_kernels)
+    terrain = make_terrain(w, levels)
+    dag.build_terrain(**terrain)
+    dag.sync()
+    return dag, terrain
+
+
+def summarize(res, n_edits):
+    """Latency (ms) and throughput of a replay; res = edits then frames."""
+    ed = res[:n_edits]
+    lat = (ed["visible_s"] - ed["submit_s"]) * 1e3
+    fr = res[n_edits:]
+    flat = (fr["visible_s"] - fr["submit_s"]) * 1e3
+    span = float(res["visible_s"].max() - res["submit_s"].min()) if len(res) else 0.0
+    vox = float(ed["edited_voxels"].sum())
+    launches = len(set(res["launch"].tolist()))
+    return {"edits": int(n_edits), "ok": int((ed["status"] == 0).sum()), "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99),
+            "max_ms": float(lat.max()) if len(lat) else None, "frame_p99_ms": pct(flat, 99),
+            "edited_mvox_s": vox / span / 1e6 if span > 0 else None, "launches": launches,
+            "mean_edits_per_launch": float(n_edits) / max(1, len(set(ed["launch"].tolist()))), "span_s": span}
+
+
+def replay(svdag, dag, cam, edits, times, frames, plain=False, copy_frames=False):
+    with svdag.Server(dag, cam, max_batch=256, max_inflight=2, memory_cap_bytes=POOL_CAP, plain=plain,
+                      copy_frames=copy_frames) as srv:
+        return srv.replay(edits, times, frames)
+
+
+def edit_algorithmic_bytes(records):
+    """Per edit: every intermediate SVO item written by the top-down phases and read by the bottom-up
+    ones (44 + 44 bytes with its representative and handle), one table find per distinct item (a
+    32-byte slab header and a 40-byte candidate), 40 bytes per inserted item."""
+    return float(sum(r.svo_items * 88 + r.unique_items * 72 + r.new_items * 40 for r in records))
+
+
+def run_serve(args):
     import torch
 
     import svdag
+    import svdag.workloads as w
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -235,236 +267,225 @@ def run_mine(args):
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
-        import torch.distributed as dist
         import datetime
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    stream = torch.cuda.Stream()
-    n_edits = args.warmup + args.steps
-    edits = c0_edits(max(n_edits, 64))
-    dag = svdag.MyGPUHashDAG(LEVELS, pool_bytes=4 << 30, scratch_bytes=1 << 30)
-    dag.build_terrain(**TERRAIN, stream=stream)
-    params = svdag.get_trace_params((512.0, 900.0, 512.0), (512.0, 512.0, 512.0), FRAME, FRAME)
-    hits = torch.empty(FRAME * FRAME * 68, dtype=torch.uint8, device="cuda")
-    host_hits = torch.empty(FRAME * FRAME * 68, dtype=torch.uint8, pin_memory=True)
+        import torch.distributed as dist
 
-    def mk(i):
-        tool, mat, c, r = edits[i % len(edits)]
-        e = svdag.Edit(tool=tool, material=mat)
-        e.center[:] = list(c)
-        e.radius = r
-        return e
-
-    # warm-up (also collects per-edit edited-voxel counts of the whole stream on a scratch replay)
-    for i in range(args.warmup):
-        dag.edit(mk(i), stream=stream)
-        dag.trace(params, hits, stream=stream)
-    stream.synchronize()
-    dag.sync(stream)
-
-    # device-resident timed region: K edits + K frames
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    edited = 0
-    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clocks:
-        t_start.record(stream)
-        for k in range(args.steps):
-            ev[k][0].record(stream)
-            dag.edit(mk(args.warmup + k), stream=stream)
-            dag.trace(params, hits, stream=stream)
-            ev[k][1].record(stream)
-            edited += dag.last_edit_stats(stream).edited_voxels  # host read of the step's counters
-        t_end.record(stream)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    levels = args.levels
+    rmax = 2048.0 * (1 << levels) / 131072
+    dur_w, dur_k = args.warmup * args.window, args.steps * args.window
+    # warm-up and timed streams (different seeds, so the timed edits are new work)
+    tw, ew, fw = w.c4_stream(args.rate, dur_w, seed=40 + rank, levels=levels, rmax=rmax,
+                             terrain=make_terrain(w, levels), copy_offset=int(1024 * (1 << levels) / 131072))
+    tk, ek, fk = w.c4_stream(args.rate, dur_k, seed=4 + rank, levels=levels, rmax=rmax,
+                             terrain=make_terrain(w, levels), copy_offset=int(1024 * (1 << levels) / 131072))
+    cam = c2_camera(svdag, levels)
+    out = {}
+    # served and plain paths, each on its own copy of the scene
+    for name, plain in (("served", False), ("plain", True)):
+        dag, _ = make_scene(svdag, w, levels)
+        replay(svdag, dag, cam, ew, tw, fw, plain=plain)
+        if dist:
+            dist.barrier()
         torch.cuda.synchronize()
-    total_ms = t_start.elapsed_time(t_end)
-    lat = sorted(a.elapsed_time(b) for a, b in ev)
-    status = dag.last_edit_stats(stream).status
-
-    # e2e: same steps through the C ABI with the edit from host memory and the hit buffer read back
-    e2e_dag = svdag.MyGPUHashDAG(LEVELS, pool_bytes=4 << 30, scratch_bytes=1 << 30)
-    e2e_dag.build_terrain(**TERRAIN, stream=stream)
-    for i in range(args.warmup):
-        e2e_dag.edit(mk(i), stream=stream)
-    stream.synchronize()
-    e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e2e_edited = 0
-    torch.cuda.synchronize()
-    e_start.record(stream)
-    for k in range(args.steps):
-        e2e_dag.edit(mk(args.warmup + k), stream=stream)
-        e2e_dag.trace(params, hits, stream=stream)
-        with torch.cuda.stream(stream):
-            host_hits.copy_(hits, non_blocking=True)
-        e2e_edited += e2e_dag.last_edit_stats(stream).edited_voxels
-    e_end.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = e_start.elapsed_time(e_end)
-
-    # batched form: the same K edits (after the same warm-up) in one persistent launch
-    b_dag = svdag.MyGPUHashDAG(LEVELS, pool_bytes=4 << 30, scratch_bytes=1 << 30)
-    b_dag.build_terrain(**TERRAIN, stream=stream)
-    for i in range(args.warmup):
-        b_dag.edit(mk(i), stream=stream)
-    stream.synchronize()
-    b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    b0.record(stream)
-    nrec = b_dag.edit_batch([mk(args.warmup + k) for k in range(args.steps)], stream=stream)
-    b1.record(stream)
-    torch.cuda.synchronize()
-    b_ms = b0.elapsed_time(b1)
-    b_edited = sum(r.edited_voxels for r in b_dag.edit_records(nrec, stream))
-    b_dag.free()
-
-    hash_res = run_hash_bench(svdag, torch, stream, lanes=args.hash_lanes, load_factor=args.hash_lf)
-    t_max = total_ms
+        with ClockSampler(local) as clocks:
+            t0 = time.perf_counter()
+            res = replay(svdag, dag, cam, ek, tk, fk, plain=plain)
+            wall = time.perf_counter() - t0
+        torch.cuda.synchronize()
+        out[name] = summarize(res, len(ek))
+        out[name]["wall_s"] = wall
+        if name == "served":
+            out["clocks"] = clocks.summary()
+            out["launches_timed"] = out[name]["launches"]
+            # e2e: the same timed stream again (after GC) with every frame copied to pinned host memory
+            dag.garbage_collect()
+            replay(svdag, dag, cam, ew, tw, fw)
+            res_e2e = replay(svdag, dag, cam, ek, tk, fk, copy_frames=True)
+            out["e2e"] = summarize(res_e2e, len(ek))
+            # the dominant kernel: one window of the stream as one persistent batched launch
+            dag.garbage_collect()
+            nwin = max(1, len(ek) // max(1, args.steps))
+            batch = ek[:nwin]
+            stream = torch.cuda.Stream()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            a.record(stream)
+            nrec = dag.edit_batch(batch, stream=stream.cuda_stream)
+            b.record(stream)
+            torch.cuda.synchronize()
+            recs = dag.edit_records(nrec)
+            out["batch"] = {"edits": len(batch), "ms": a.elapsed_time(b), "bytes": edit_algorithmic_bytes(recs),
+                            "svo_items": int(sum(r.svo_items for r in recs))}
+            out["used_gb"] = dag.stats().item_region_used_bytes / 1e9
+        dag.free()
+        del dag
+    hash_res = None
+    if not args.no_hash:
+        hash_res = run_hash_bench(svdag, torch, torch.cuda.Stream(), lanes=args.hash_lanes, load_factor=args.hash_lf)
+    p99 = out["served"]["p99_ms"]
     if dist:
-        t = torch.tensor([total_ms, e2e_ms], device="cuda")
+        t = torch.tensor([p99, out["plain"]["p99_ms"], out["e2e"]["p99_ms"]], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max, e2e_ms = float(t[0]), float(t[1])
-        cnt = torch.tensor([float(edited), float(e2e_edited)], device="cuda", dtype=torch.float64)
-        dist.all_reduce(cnt)
-        edited, e2e_edited = cnt[0].item(), cnt[1].item()
+        p99, out["plain"]["p99_ms"], out["e2e"]["p99_ms"] = (float(x) for x in t)
     peak, peak_kind = measured_peak_gbs()
-    find_gbs = hash_res["find_gbs"]
+    bt = out["batch"]
+    achieved = bt["bytes"] / (bt["ms"] / 1e3) / 1e9
+    frame_bytes = cam.width * cam.height * 68
+    n_frames_e2e = out["e2e"]["launches"]
     line = {
         "metric": METRIC,
-        "value": edited / (t_max / 1e3) / 1e6,
-        "unit": "edited Mvox/s",
+        "value": p99,
+        "unit": "ms (served p99 edit-to-visible)",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": t_max / args.steps,
-        "higher_is_better": True,
+        "ms_per_step": out["served"]["wall_s"] * 1e3 / args.steps,
+        "higher_is_better": False,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "u32",
-        "data": "synthetic (seeded procedural fBm terrain and seeded edit stream)",
-        "config": {"workload": "c0 per-edit: depth-10 (1024^3) fBm terrain, sphere add/remove r U{4..64} "
-                               "near the surface, 256x256 primary-ray frame after each edit",
-                   "levels": LEVELS, "frame": [FRAME, FRAME], "parallelism": f"replicas x{world}",
-                   "l2": "DAG and tables resident; steps edit different regions"},
-        "p50_edit_to_visible_ms": lat[len(lat) // 2],
-        "p99_edit_to_visible_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
-        "edit_status": int(status),
-        "e2e": {"value": e2e_edited / (e2e_ms / 1e3) / 1e6, "unit": "edited Mvox/s",
-                "h2d_bytes_per_step": 56, "d2h_bytes_per_step": FRAME * FRAME * 68 + 264},
-        "roofline": {"bound": "hbm", "kernel": f"slab-hash find (C1, 2^24 keys, {args.hash_lanes} lane(s)/key)",
-                     "achieved": find_gbs, "peak": peak, "unit": "GB/s", "frac": find_gbs / peak,
-                     "peak_source": peak_kind, "traffic": None},
-        "batched": {"edits": args.steps, "ms": b_ms, "ms_per_edit": b_ms / args.steps,
-                    "edited_mvox_s": b_edited / (b_ms / 1e3) / 1e6, "note": "edits only, one persistent launch"},
-        "hash_c1": hash_res,
-        "clocks": clocks.summary(),
-        "gpu_launches": args.steps * (4 * (LEVELS - 2) + 6),
+        "data": "synthetic (seeded procedural scene and seeded Poisson request stream)",
+        "config": {"workload": f"c4 served stream on the c2 scene: depth-{levels} fBm terrain (8 octaves) + "
+                               f"{make_terrain(w, levels)['num_structures']} boxes/spheres, Poisson {args.rate:g} edits/s "
+                               "add/remove/paint/copy 35/35/20/10, radius log-uniform 2..2048, 1920x1080 frames "
+                               "at 60 Hz, undo depth 32, 120 GB cap",
+                   "levels": levels, "rate_edits_per_s": args.rate, "window_s": args.window,
+                   "frame": [cam.width, cam.height], "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (the DAG holds > 20 GB; edits land at random places)"},
+        "served": out["served"], "plain": out["plain"],
+        "p99_served_over_plain": p99 / out["plain"]["p99_ms"] if out["plain"]["p99_ms"] else None,
+        "edited_mvox_s_served": out["served"]["edited_mvox_s"],
+        "e2e": {"value": out["e2e"]["p99_ms"], "unit": "ms (served p99 edit-to-visible, frames copied to host)",
+                "h2d_bytes_per_step": int(56 * len(ek) / args.steps),
+                "d2h_bytes_per_step": int((n_frames_e2e * frame_bytes + 48 * len(ek)) / args.steps),
+                "detail": out["e2e"]},
+        "roofline": {"bound": "hbm", "kernel": "k_edit_fused (one window of the stream as one persistent launch)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_kind, "traffic": None, "launch": bt},
+        "clocks": out["clocks"],
+        "gpu_launches": 2 * out["launches_timed"],
+        "item_region_used_gb": out["used_gb"],
     }
+    if hash_res:
+        line["hash_c1"] = hash_res
+        line["hash_roofline"] = {"kernel": f"slab-hash find (2^24 keys, {args.hash_lanes} lane(s)/key)",
+                                 "achieved": hash_res["find_gbs"], "peak": peak, "unit": "GB/s",
+                                 "frac": hash_res["find_gbs"] / peak}
     if rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(args)
+        line["cpu_baseline"] = cpu_sample(args, levels)["cpu_baseline"]
     if rank == 0:
         print(json.dumps(line))
-    dag.free()
-    e2e_dag.free()
     if dist:
         dist.destroy_process_group()
 
 
-def cpu_baseline(args, sample_edits=64):
-    """The oracle restatement of the MyGpuDag pipeline on one host core, on the same C0 stream."""
+def make_terrain(w, levels):
+    if levels == w.C2_LEVELS:
+        return w.C2_TERRAIN
+    return dict(w.C2_TERRAIN, num_structures=max(16, 4096 >> (2 * (w.C2_LEVELS - levels))))
+
+
+# ------------------------------------------------------------------ CPU baseline / reference arm
+
+def edit_box(e):
+    """Voxel box the edit can read or change (copies: source and destination)."""
+    c, r = np.array(e.center, dtype=np.float64), float(e.radius) + 2.0
+    if e.tool in (5, 7):
+        d = np.array(e.dst, dtype=np.float64) + c - np.array(e.src, dtype=np.float64)
+        lo, hi = np.minimum(c, d) - r, np.maximum(c, d) + r
+    else:
+        lo, hi = c - r, c + r
+    return [int(np.floor(v)) for v in lo], [int(np.ceil(v)) + 1 for v in hi]
+
+
+def cpu_sample(args, levels, budget_s=25.0):
+    """The oracle (CPU restatement of the reference pipeline, one core) on the leading edits of the
+    timed stream, each on the scene clipped to the edit's box (the result inside the box equals the
+    full scene's: edits are local). Times the edit only; the region build is not timed."""
+    import svdag.workloads as w
     from oracle import oracle
 
-    d = oracle.OracleDag(LEVELS)
-    d.build_terrain(oracle.TerrainParams(**TERRAIN))
-    edits = c0_edits(max(args.warmup + args.steps, 64))
-    edited = 0
-    t0 = time.perf_counter()
-    for i in range(sample_edits):
-        tool, mat, c, r = edits[i]
-        e = oracle.Edit(tool=tool, material=mat)
-        e.center[:] = list(c)
-        e.radius = r
-        edited += d.edit(e).edited_voxels
-    dt = time.perf_counter() - t0
-    return {"value": edited / dt / 1e6, "unit": "edited Mvox/s", "cores": 1, "kind": "port",
-            "sample": f"first {sample_edits} edits of the C0 stream on the depth-10 terrain (edits only, no frames)"}
+    rmax = 2048.0 * (1 << levels) / 131072
+    tk, ek, _ = w.c4_stream(args.rate, args.steps * args.window, seed=4, levels=levels, rmax=rmax,
+                            terrain=make_terrain(w, levels), copy_offset=int(1024 * (1 << levels) / 131072))
+    params = oracle.TerrainParams(**make_terrain(w, levels))
+    lat, vox, radii = [], 0, []
+    start = time.perf_counter()
+    for e in ek:
+        if time.perf_counter() - start > budget_s and len(lat) >= 8:
+            break
+        d = oracle.OracleDag(levels)
+        lo, hi = edit_box(e)
+        d.build_scene_region(params, lo, hi)
+        oe = oracle.Edit(tool=e.tool, material=e.material, radius=e.radius, noise_seed=e.noise_seed,
+                         noise_cell_log2=e.noise_cell_log2)
+        oe.center[:], oe.src[:], oe.dst[:] = list(e.center), list(e.src), list(e.dst)
+        t0 = time.perf_counter()
+        st = d.edit(oe)
+        lat.append((time.perf_counter() - t0) * 1e3)
+        vox += st.edited_voxels
+        radii.append(float(e.radius))
+        del d
+    p99 = pct(lat, 99)
+    return {"p99_ms": p99, "p50_ms": pct(lat, 50), "mean_ms": float(np.mean(lat)), "edits": len(lat),
+            "edited_mvox_s": vox / (sum(lat) / 1e3) / 1e6,
+            "cpu_baseline": {"value": p99, "unit": "ms (p99 edit latency, edit only)", "cores": 1, "kind": "port",
+                             "sample": f"first {len(lat)} edits of the timed stream (radius {min(radii):.0f}..{max(radii):.0f}), "
+                                       "each on the scene clipped to its box; edit time only, no frame, no queueing",
+                             "p50_ms": pct(lat, 50)}}
 
 
 def run_reference(args):
-    """Reference arm: the CPU restatement of the reference path (the reference's MyGpuDag pipeline has
-    no CPU implementation) timed on the host, rank 0 only."""
+    """Reference arm: the CPU restatement of the reference path timed on the host, rank 0 only."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from oracle import oracle
-
-    d = oracle.OracleDag(LEVELS)
-    d.build_terrain(oracle.TerrainParams(**TERRAIN))
-    edits = c0_edits(max(args.warmup + args.steps, 64))
-    params = oracle.camera_params([512.0, 900.0, 512.0], [512.0, 512.0, 512.0], 60.0, FRAME, FRAME)
-    threads = os.cpu_count() or 1
-
-    def step(i):
-        tool, mat, c, r = edits[i % len(edits)]
-        e = oracle.Edit(tool=tool, material=mat)
-        e.center[:] = list(c)
-        e.radius = r
-        st = d.edit(e)
-        d.trace(params, threads=threads)
-        return st.edited_voxels
-
-    for i in range(args.warmup):
-        step(i)
-    lat, edited = [], 0
-    t0 = time.perf_counter()
-    for k in range(args.steps):
-        s = time.perf_counter()
-        edited += step(args.warmup + k)
-        lat.append((time.perf_counter() - s) * 1e3)
-    dt = time.perf_counter() - t0
-    lat.sort()
-    v = edited / dt / 1e6
+    r = cpu_sample(args, args.levels)
+    cb = r["cpu_baseline"]
+    cb["cores"] = 1
     print(json.dumps({
-        "impl": "reference", "metric": METRIC, "value": v, "unit": "edited Mvox/s",
+        "impl": "reference", "metric": METRIC, "value": r["p99_ms"], "unit": "ms (p99 edit latency, edit only)",
         "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "u32", "data": "synthetic (seeded procedural fBm terrain and seeded edit stream)",
-        "config": {"workload": "c0 per-edit: depth-10 (1024^3) fBm terrain, sphere add/remove r U{4..64} "
-                               "near the surface, 256x256 primary-ray frame after each edit", "levels": LEVELS},
-        "p50_edit_to_visible_ms": lat[len(lat) // 2], "p99_edit_to_visible_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
-        "cpu_baseline": {"value": v, "unit": "edited Mvox/s", "cores": threads, "kind": "port",
-                         "sample": "the timed steps themselves (edit single-threaded, frame on all cores)"},
-        "e2e": {"value": v, "unit": "edited Mvox/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "ms_per_step": r["mean_ms"], "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded procedural scene and seeded request stream)",
+        "config": {"workload": f"c4 stream edits on the c2 scene (depth {args.levels}), one at a time on the CPU",
+                   "levels": args.levels, "rate_edits_per_s": args.rate},
+        "p50_ms": r["p50_ms"], "edits": r["edits"], "edited_mvox_s": r["edited_mvox_s"],
+        "cpu_baseline": cb,
+        "e2e": {"value": r["p99_ms"], "unit": "ms (p99 edit latency, edit only)", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
     }))
 
 
+# ------------------------------------------------------------------ profiling entry points
+
 def run_mode_hash(args):
-    """Only the C1 slab-hash microbenchmark (profiling entry point)."""
+    """Only the 2^24-key slab-hash microbenchmark."""
     import torch
 
     import svdag
 
     r = run_hash_bench(svdag, torch, torch.cuda.Stream(), n_total=args.hash_keys, lanes=args.hash_lanes,
                        load_factor=args.hash_lf, reps=args.hash_reps, pool=args.hash_pool)
-    print(json.dumps({k: v for k, v in r.items()}))
+    print(json.dumps(r))
 
 
-def run_mode_edit(args):
-    """Only the per-edit path: depth-10 terrain, warm-up edits, then K edits each followed by a frame
-    (profiling entry point)."""
+def run_mode_c0(args):
+    """Depth-10 terrain, then K sphere edits of the C0 stream each followed by a 256x256 frame."""
     import torch
 
     import svdag
+    import svdag.workloads as w
 
-    edits = c0_edits(max(args.warmup + args.steps, 64))
-    dag = svdag.MyGPUHashDAG(LEVELS, pool_bytes=4 << 30, scratch_bytes=1 << 30)
-    dag.build_terrain(**TERRAIN)
-    params = svdag.get_trace_params((512.0, 900.0, 512.0), (512.0, 512.0, 512.0), FRAME, FRAME)
-    hits = torch.empty(FRAME * FRAME * 68, dtype=torch.uint8, device="cuda")
-    te, tt, phases = [], [], []
+    edits = w.c0_edits(max(args.warmup + args.steps, 64))
+    dag = svdag.MyGPUHashDAG(w.C0_LEVELS, pool_bytes=4 << 30, scratch_bytes=1 << 30, phase_kernels=args.phase_kernels)
+    dag.build_terrain(**w.C0_TERRAIN)
+    params = svdag.get_trace_params((512.0, 900.0, 512.0), (512.0, 512.0, 512.0), C0_FRAME, C0_FRAME)
+    hits = torch.empty(C0_FRAME * C0_FRAME * 68, dtype=torch.uint8, device="cuda")
+    te, tt = [], []
     for i in range(args.warmup + args.steps):
         tool, mat, c, r = edits[i % len(edits)]
-        e = svdag.Edit(tool=tool, material=mat)
-        e.center[:] = list(c)
-        e.radius = r
+        e = w.make_edit(tool, mat, c, r)
         a, b, d = (torch.cuda.Event(enable_timing=True) for _ in range(3))
         a.record()
         dag.edit(e)
@@ -475,38 +496,100 @@ def run_mode_edit(args):
         if i >= args.warmup:
             te.append(a.elapsed_time(b))
             tt.append(b.elapsed_time(d))
-            pt = dag.last_edit_phase_times()
-            phases.append([round(float(x - pt[0]) / 1e3, 2) for x in pt])
     dag.sync()
-    print(json.dumps({"edit_ms_median": statistics.median(te), "trace_ms_median": statistics.median(tt),
-                      "edit_ms": te, "trace_ms": tt, "phase_us": phases[:4]}))
+    print(json.dumps({"edit_ms_p50": pct(te, 50), "edit_ms_p99": pct(te, 99), "trace_ms_p50": pct(tt, 50)}))
+
+
+def run_mode_c2(args):
+    """The at-scale sequence (carve, copy, noise paint) timed per edit with its phase timestamps."""
+    import torch
+
+    import svdag
+    import svdag.workloads as w
+
+    dag, terrain = make_scene(svdag, w, args.levels, phase_kernels=args.phase_kernels)
+    out = []
+    for e in w.c2_edits(args.levels, terrain):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record()
+        dag.edit(e)
+        b.record()
+        torch.cuda.synchronize()
+        st = dag.last_edit_stats()
+        pt = [] if args.phase_kernels else dag.last_edit_phase_times()
+        out.append({"tool": int(e.tool), "ms": a.elapsed_time(b), "status": int(st.status),
+                    "edited_mvox": st.edited_voxels / 1e6, "svo_items": int(sum(st.svo_nodes)), "new_items": int(st.new_items),
+                    "phase_us": [round(float(pt[i + 1] - pt[i]) / 1e3, 1) for i in range(len(pt) - 1)]})
+    dag.free()
+    print(json.dumps({"levels": args.levels, "edits": out}))
+
+
+def run_mode_c3(args):
+    """256 edits of uneven footprint: one batched persistent launch against the plain per-edit path,
+    each on its own copy of the scene; the stored item sets must be equal."""
+    import torch
+
+    import svdag
+    import svdag.workloads as w
+
+    edits = w.c3_edits(levels=args.levels, terrain=make_terrain(w, args.levels), rmax=4096.0 * (1 << args.levels) / 131072)
+    res = {}
+    items = {}
+    for name in ("plain", "batched"):
+        dag, _ = make_scene(svdag, w, args.levels)
+        stream = torch.cuda.Stream()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        if name == "plain":
+            for e in edits:
+                dag.edit(e, stream=stream.cuda_stream)
+        else:
+            dag.edit_batch(edits, stream=stream.cuda_stream)
+        b.record(stream)
+        torch.cuda.synchronize()
+        dag.sync()
+        res[name] = a.elapsed_time(b)
+        items[name] = [dag.table(l).stats().items for l in range(args.levels - 1)]
+        dag.free()
+    print(json.dumps({"edits": len(edits), "plain_ms": res["plain"], "batched_ms": res["batched"],
+                      "items_equal": items["plain"] == items["batched"]}))
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=48)
-    ap.add_argument("--warmup", type=int, default=8)
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
-    ap.add_argument("--mode", default="full", choices=["full", "hash", "edit"],
-                    help="full = the benchmark line; hash / edit run one sub-workload (profiling)")
+    ap.add_argument("--mode", default="serve", choices=["serve", "c0", "c2", "c3", "hash"],
+                    help="serve = the benchmark line; the others run one sub-workload (profiling)")
+    ap.add_argument("--rate", type=float, default=1000.0, help="edit arrivals per second")
+    ap.add_argument("--window", type=float, default=0.5, help="seconds of the stream per step")
+    ap.add_argument("--levels", type=int, default=17)
+    ap.add_argument("--phase-kernels", action="store_true", help="one launch per edit phase (profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-hash", action="store_true")
     ap.add_argument("--hash-keys", type=int, default=1 << 24)
     ap.add_argument("--hash-lanes", type=int, default=1)
     ap.add_argument("--hash-lf", type=int, default=20)
     ap.add_argument("--hash-reps", type=int, default=3)
     ap.add_argument("--hash-pool", type=int, default=6 << 30)
     args = ap.parse_args()
-    if args.warmup < 3:
-        args.warmup = 3
+    args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         run_reference(args)
     elif args.mode == "hash":
         run_mode_hash(args)
-    elif args.mode == "edit":
-        run_mode_edit(args)
+    elif args.mode == "c0":
+        run_mode_c0(args)
+    elif args.mode == "c2":
+        run_mode_c2(args)
+    elif args.mode == "c3":
+        run_mode_c3(args)
     else:
-        run_mine(args)
+        run_serve(args)
 
 
 if __name__ == "__main__":

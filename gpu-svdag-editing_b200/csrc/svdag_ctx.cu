@@ -145,7 +145,7 @@ const char* svdag_status_string(svdag_status s)
 
 svdag_status svdag_create(const svdag_config* cfg, svdag_ctx** out)
 {
-    if (!cfg || !out || cfg->levels < SVDAG_MIN_LEVELS || cfg->levels > SVDAG_MAX_LEVELS || cfg->flags != 0)
+    if (!cfg || !out || cfg->levels < SVDAG_MIN_LEVELS || cfg->levels > SVDAG_MAX_LEVELS || (cfg->flags & ~SVDAG_FLAG_PHASE_KERNELS) != 0)
         return SVDAG_ERR_INVALID;
     if (cfg->probe_lanes && cfg->probe_lanes != 1 && cfg->probe_lanes != 2 && cfg->probe_lanes != 4 && cfg->probe_lanes != 8
         && cfg->probe_lanes != 16 && cfg->probe_lanes != 32)

@@ -67,7 +67,7 @@ struct EditCounters {
     uint32_t overflow; // scratch arena exhausted
     uint32_t builder; // scene build: merge even without leaves, discovery on every level
     uint32_t startLevel;
-    uint32_t pad;
+    uint32_t err; // first error status raised while this edit ran (0 = none)
 };
 
 struct Control {
@@ -95,9 +95,12 @@ struct DevDag {
     uint32_t leafLevel;
 };
 
+// Latches the first error of the context (reported by svdag_sync) and of the running edit (which
+// then leaves the root unchanged).
 __device__ __forceinline__ void set_status(Control* ctl, uint32_t code)
 {
     atomicCAS(&ctl->status, 0u, code);
+    atomicCAS(&ctl->edit.err, 0u, code);
 }
 
 // Every handle read from memory is checked before it is dereferenced: a bad handle (which only a

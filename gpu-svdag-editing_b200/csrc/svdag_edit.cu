@@ -86,6 +86,23 @@ __device__ uint32_t noise_material(uint32_t seed, uint32_t cl, uint32_t x, uint3
     const long long y0 = lerp16(x00, x10, sy), y1 = lerp16(x01, x11, sy);
     return (uint32_t)(lerp16(y0, y1, sz) >> 12) & 0xFu;
 }
+// The same value when the eight lattice corners of the voxel's cell are given (L[k] for corner
+// (k >> 2 & 1, k >> 1 & 1, k & 1)): a 4^3 leaf lies in one cell when cells are 4 voxels or larger.
+__device__ __forceinline__ uint32_t noise_from_corners(const uint32_t* L, uint32_t cl, uint32_t x, uint32_t y, uint32_t z)
+{
+    const uint32_t m = (1u << cl) - 1u;
+    const auto frac = [&](uint32_t v) -> long long {
+        const uint32_t f = v & m;
+        return cl <= 16 ? (long long)(f << (16 - cl)) : (long long)(f >> (cl - 16));
+    };
+    const long long sx = smooth16(frac(x)), sy = smooth16(frac(y)), sz = smooth16(frac(z));
+    const long long x00 = lerp16(L[0], L[4], sx);
+    const long long x10 = lerp16(L[2], L[6], sx);
+    const long long x01 = lerp16(L[1], L[5], sx);
+    const long long x11 = lerp16(L[3], L[7], sx);
+    const long long y0 = lerp16(x00, x10, sy), y1 = lerp16(x01, x11, sy);
+    return (uint32_t)(lerp16(y0, y1, sz) >> 12) & 0xFu;
+}
 
 // Stateless should_edit of every tool (the node is [p << depth, +2^depth)^3).
 template <uint32_t TOOL>
@@ -375,9 +392,7 @@ __device__ void ph_build_leaves(const DevDag& d, const DevEditor& e, char* scrat
     // Reserve and clear the dedup tables of every level for the bottom-up phase.
     // The dedup tables of all levels form one contiguous run per level; walk the layout once (from
     // the leaf level up, the order merge_layout assigns) instead of recomputing it per level.
-    uint32_t cnt[kMaxLevels];
-    for (uint32_t l = 0; l <= LL; ++l)
-        cnt[l] = E.count[l];
+    const uint32_t* cnt = E.count; // final: the top-down phases are done
     const MergeLayout top = merge_layout(cnt, buildTop, 0, LL);
     if (top.end > scratchBytes) {
         if (threadIdx.x == 0)
@@ -405,17 +420,26 @@ __device__ void ph_build_leaves(const DevDag& d, const DevEditor& e, char* scrat
     const uint32_t warpsTotal = gridDim.x * (blockDim.x >> 5);
     unsigned long long edited = 0, oldRead = 0;
     uint32_t fullLeaves = 0;
-    for (uint32_t i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warpsTotal) {
-        const WorkItem w = *reinterpret_cast<const WorkItem*>(scratch + offW + i * stride);
+    // Software pipeline over the warp's leaves: the work item two ahead and the old leaf one ahead are
+    // in flight while a leaf is computed (every valid handle has 16 readable words, so the ten words
+    // of a leaf are fetched at once and trimmed to its size afterwards).
+    auto work_at = [&](uint32_t k) {
+        return k < n ? *reinterpret_cast<const WorkItem*>(scratch + offW + k * stride) : WorkItem { 0, 0, 0, kNone };
+    };
+    auto leaf_word = [&](uint32_t h) { return (h != kNone && lane < kItemStride) ? item_ptr(d, h)[lane] : 0u; };
+    uint32_t i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    WorkItem w = work_at(i), wn = work_at(i + warpsTotal);
+    uint32_t owRaw = leaf_word(w.handle);
+    for (; i < n; i += warpsTotal) {
+        const WorkItem wnn = work_at(i + 2 * warpsTotal);
+        const uint32_t owNext = leaf_word(wn.handle);
         // old leaf words (lanes 0..9)
         uint32_t ow = 0, lo = 0, hi = 0;
         if (w.handle != kNone) {
-            const uint32_t* leaf = item_ptr(d, w.handle);
-            const uint32_t a = lane < 2 ? leaf[lane] : 0u;
-            lo = __shfl_sync(0xFFFFFFFFu, a, 0);
-            hi = __shfl_sync(0xFFFFFFFFu, a, 1);
+            lo = __shfl_sync(0xFFFFFFFFu, owRaw, 0);
+            hi = __shfl_sync(0xFFFFFFFFu, owRaw, 1);
             const uint32_t nw = dev_leaf_words(lo, hi);
-            ow = lane < nw ? leaf[lane] : 0u;
+            ow = lane < nw ? owRaw : 0u;
             if (lane == 0)
                 ++oldRead;
         }
@@ -423,6 +447,17 @@ __device__ void ph_build_leaves(const DevDag& d, const DevEditor& e, char* scrat
         if constexpr (TOOL == kToolTerrain) {
             if (lane < 16)
                 th = terrain_height(e.scene, (w.x << 2) + (lane >> 2), (w.z << 2) + (lane & 3u));
+        }
+        uint32_t corners[8] = {}; // noise paint: lattice corners of the leaf's cell, one per lane 0..7
+        if constexpr (TOOL == SVDAG_TOOL_BOX_PAINT_NOISE) {
+            if (e.noiseCellLog2 >= 2) {
+                const uint32_t cl = e.noiseCellLog2;
+                const uint32_t mine = lattice3(e.noiseSeed, ((w.x << 2) >> cl) + ((lane >> 2) & 1u), ((w.y << 2) >> cl) + ((lane >> 1) & 1u),
+                    ((w.z << 2) >> cl) + (lane & 1u));
+#pragma unroll
+                for (uint32_t k = 0; k < 8; ++k)
+                    corners[k] = __shfl_sync(0xFFFFFFFFu, mine, k);
+            }
         }
         uint32_t newMat[2];
         bool set[2];
@@ -459,7 +494,8 @@ __device__ void ph_build_leaves(const DevDag& d, const DevEditor& e, char* scrat
                         mat = e.material;
                     } else if constexpr (TOOL == SVDAG_TOOL_BOX_PAINT_NOISE) {
                         out = true;
-                        mat = noise_material(e.noiseSeed, e.noiseCellLog2, vx, vy, vz);
+                        mat = e.noiseCellLog2 >= 2 ? noise_from_corners(corners, e.noiseCellLog2, vx, vy, vz)
+                                                   : noise_material(e.noiseSeed, e.noiseCellLog2, vx, vy, vz);
                     } else if constexpr (TOOL == SVDAG_TOOL_COPY) { // get_new_value(uint3, optional, State), :225-252
                         out = hasOld;
                         mat = oldMat;
@@ -531,6 +567,9 @@ __device__ void ph_build_leaves(const DevDag& d, const DevEditor& e, char* scrat
                 full &= words[wd] == m;
             fullLeaves += full ? 1u : 0u;
         }
+        w = wn;
+        wn = wnn;
+        owRaw = owNext;
     }
     for (int o = 16; o > 0; o >>= 1) {
         edited += __shfl_xor_sync(0xFFFFFFFFu, edited, o);
@@ -564,61 +603,108 @@ __device__ __forceinline__ bool discovery_gate(const EditCounters& E, uint32_t l
     return ranBelow && E.ffCount[level + 1] > 0;
 }
 
+// Value of slot j (0..7) of a register array without dynamic indexing (which would put the array in
+// local memory).
+__device__ __forceinline__ uint32_t sel8(const uint32_t (&v)[8], uint32_t j)
+{
+    uint32_t r = v[0];
+#pragma unroll
+    for (uint32_t k = 1; k < 8; ++k)
+        r = j == k ? v[k] : r;
+    return r;
+}
+
 // updateChildPointers + discover_fully_filled for one node held in registers
-// (my_gpu_hash_dag_edits.cu:44-150). Returns true when the node was found fully filled.
+// (my_gpu_hash_dag_edits.cu:44-150). Returns true when the node was found fully filled. Every slot is
+// handled with static indices and the loads of all children are issued together, stage by stage.
 __device__ __forceinline__ bool fix_node(const DevDag& d, uint32_t level, bool gate, const uint32_t* repC, const uint32_t* hC,
     uint32_t* w)
 {
     const uint32_t LL = d.leafLevel;
-    uint32_t mask = w[0] & 0xFFu;
+    const uint32_t mask = w[0] & 0xFFu;
     const uint32_t interm = w[0] >> 13;
-    uint32_t outW[8];
-    uint32_t in = 1, out = 0;
-    for (uint32_t c = 0; c < 8; ++c) {
-        if (!(mask & (1u << c)))
-            continue;
-        uint32_t h = w[in++];
-        if (interm & (1u << c)) {
-            const uint32_t r = repC[h];
-            h = r == kEmptyRep ? kNone : hC[r];
-        } else if (h >= kFillMarker && h != kNone) {
-            h = d.ctl->fullyFilled[level + 1][h & 0xFu];
-        }
-        if (h != kNone)
-            outW[out++] = h;
-        else
-            mask ^= 1u << c;
+    const uint32_t n = __popc(mask);
+    uint32_t cbit[8], h[8];
+    uint32_t rem = mask;
+#pragma unroll
+    for (uint32_t j = 0; j < 8; ++j) {
+        cbit[j] = rem ? (uint32_t)__ffs(rem) - 1u : 0u;
+        rem &= rem - 1u;
+        h[j] = w[1 + j];
     }
-    uint32_t header = mask;
+    // Children built in this edit: their representative, then its handle.
+    uint32_t r[8];
+#pragma unroll
+    for (uint32_t j = 0; j < 8; ++j)
+        r[j] = (j < n && ((interm >> cbit[j]) & 1u)) ? repC[h[j]] : kEmptyRep;
+    const uint32_t* ff = d.ctl->fullyFilled[level + 1];
+#pragma unroll
+    for (uint32_t j = 0; j < 8; ++j) {
+        if (j >= n)
+            h[j] = kNone;
+        else if ((interm >> cbit[j]) & 1u)
+            h[j] = r[j] == kEmptyRep ? kNone : hC[r[j]];
+        else if (h[j] >= kFillMarker && h[j] != kNone)
+            h[j] = ff[h[j] & 0xFu];
+    }
+    // Drop emptied children, keep the others in child order.
+    uint32_t newMask = 0, keep = 0;
+#pragma unroll
+    for (uint32_t j = 0; j < 8; ++j)
+        if (h[j] != kNone) {
+            newMask |= 1u << cbit[j];
+            keep |= 1u << j;
+        }
+    uint32_t outW[8];
+#pragma unroll
+    for (uint32_t p = 0; p < 8; ++p) {
+        const uint32_t j = (uint32_t)__fns(keep, 0, (int)p + 1);
+        outW[p] = j < 8 ? sel8(h, j) : 0u;
+    }
+    uint32_t header = newMask;
     bool full = false;
-    if (gate && mask == 0xFFu) {
+    if (gate && newMask == 0xFFu) {
+        // All eight children present: fully filled with one material?
+        uint32_t head[8], cm[8];
         bool all = true;
-        uint32_t mat = 0;
-        for (uint32_t c = 0; c < 8 && all; ++c) {
-            const uint32_t* p = item_ptr(d, outW[c]);
-            uint32_t cm;
-            if (level + 1 == LL) {
-                all = p[0] == 0xFFFFFFFFu && p[1] == 0xFFFFFFFFu;
-                cm = p[2] & 0xFu;
-                for (uint32_t j = 2; j < 10 && all; ++j)
-                    all = p[j] == cm * 0x11111111u;
-            } else {
-                const uint32_t hh = p[0];
-                all = (hh >> 8) & 1u;
-                cm = (hh >> 9) & 0xFu;
+        if (level + 1 == LL) {
+#pragma unroll
+            for (uint32_t c = 0; c < 8; ++c) {
+                const uint32_t* p = item_ptr(d, outW[c]);
+                head[c] = p[0] & p[1];
+                cm[c] = p[2];
             }
-            if (c == 0)
-                mat = cm;
-            all = all && cm == mat;
+#pragma unroll
+            for (uint32_t c = 0; c < 8; ++c)
+                all = all && head[c] == 0xFFFFFFFFu && (cm[c] & 0xFu) * 0x11111111u == cm[c] && (cm[c] & 0xFu) == (cm[0] & 0xFu);
+            if (all) { // the remaining material words of full leaves
+#pragma unroll
+                for (uint32_t c = 0; c < 8; ++c) {
+                    const uint32_t* p = item_ptr(d, outW[c]);
+#pragma unroll
+                    for (uint32_t k = 3; k < 10; ++k)
+                        all = all && p[k] == cm[c];
+                }
+            }
+            cm[0] &= 0xFu;
+        } else {
+#pragma unroll
+            for (uint32_t c = 0; c < 8; ++c)
+                head[c] = item_ptr(d, outW[c])[0];
+#pragma unroll
+            for (uint32_t c = 0; c < 8; ++c)
+                all = all && ((head[c] >> 8) & 1u) && ((head[c] >> 9) & 0xFu) == ((head[0] >> 9) & 0xFu);
+            cm[0] = (head[0] >> 9) & 0xFu;
         }
         if (all) {
-            header = 0xFFu | (1u << 8) | (mat << 9);
+            header = 0xFFu | (1u << 8) | (cm[0] << 9);
             full = true;
         }
     }
     w[0] = header;
+#pragma unroll
     for (uint32_t j = 0; j < 8; ++j)
-        w[1 + j] = j < out ? outW[j] : 0u;
+        w[1 + j] = outW[j];
     w[9] = 0;
     return full;
 }
@@ -771,7 +857,8 @@ __device__ void ph_merge_level(const DevDag& d, uint32_t level, char* scratch)
         if (r != i)
             continue;
         ++reps;
-        atomicAdd(&E.repPerClass[level][key.n - 2], 1u);
+        if (E.builder) // the scene builder sizes the level tables from these
+            atomicAdd(&E.repPerClass[level][key.n - 2], 1u);
         bool ins = false;
         handle[i] = table_find_or_insert<1>(g, d, t, key, spare, ins);
         added += ins ? 1u : 0u;
@@ -823,9 +910,11 @@ __device__ void ph_edit_end(const DevDag& d, char* scratch, uint32_t builder, ui
         return;
     Control* c = d.ctl;
     EditCounters& E = c->edit;
+    // An edit that failed (scratch exhausted, or an error raised while it ran) leaves the root as it
+    // was; later edits of a batch still run.
     if (E.overflow) {
         set_status(c, SVDAG_ERR_OOM);
-    } else if ((E.count[d.leafLevel] != 0 || builder) && c->status == 0) {
+    } else if ((E.count[d.leafLevel] != 0 || builder) && E.err == 0) {
         const MergeLayout m = merge_layout(E.count, E.buildTop, E.startLevel, d.leafLevel);
         const uint32_t r = reinterpret_cast<const uint32_t*>(scratch + m.rep)[0];
         const uint32_t h = r == kEmptyRep ? kNone : reinterpret_cast<const uint32_t*>(scratch + m.handle)[r];
@@ -838,7 +927,7 @@ __device__ void ph_edit_end(const DevDag& d, char* scratch, uint32_t builder, ui
     if (record) {
         record->rootBefore = E.rootBefore;
         record->rootAfter = E.rootAfter;
-        record->status = E.overflow ? (uint32_t)SVDAG_ERR_OOM : c->status;
+        record->status = E.overflow ? (uint32_t)SVDAG_ERR_OOM : E.err;
         record->edited = E.edited;
         record->added = E.added;
         unsigned long long svo = 0, reps = 0;
@@ -1136,6 +1225,17 @@ svdag_status launch_pipeline(svdag_ctx* ctx, const DevEditor& ed, cudaStream_t s
     return SVDAG_OK;
 }
 
+bool valid_edit(const svdag_edit* e)
+{
+    if (!e || e->tool >= SVDAG_NUM_TOOLS || e->material >= SVDAG_NUM_MATERIALS || !std::isfinite(e->radius) || e->radius < 0
+        || (e->tool == SVDAG_TOOL_BOX_PAINT_NOISE && e->noise_cell_log2 > 20))
+        return false;
+    for (int a = 0; a < 3; ++a)
+        if (!std::isfinite(e->center[a]) || !std::isfinite(e->src[a]) || !std::isfinite(e->dst[a]))
+            return false;
+    return true;
+}
+
 // Expands a tool into device editors (a move is a box removal that saves the root, then a copy
 // from the saved root).
 int expand_edit(const svdag_ctx* ctx, const svdag_edit& e, DevEditor* out)
@@ -1157,6 +1257,8 @@ int expand_edit(const svdag_ctx* ctx, const svdag_edit& e, DevEditor* out)
 
 int fused_grid(svdag_ctx* ctx)
 {
+    if (ctx->cfg.flags & SVDAG_FLAG_PHASE_KERNELS)
+        return 0;
     if (ctx->fusedGrid < 0) {
         int perSm = 0, sms = 0, coop = 0;
         cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ctx->device);
@@ -1170,8 +1272,32 @@ int fused_grid(svdag_ctx* ctx)
     return ctx->fusedGrid;
 }
 
+svdag_status launch_fused_at(svdag_ctx* ctx, const DevEditor* eds, uint32_t n, char* region, size_t regionBytes, cudaStream_t s)
+{
+    const int grid = fused_grid(ctx);
+    if (grid <= 0)
+        return SVDAG_ERR_UNSUPPORTED;
+    DevDag d = ctx->dag();
+    DevEditor single = eds[0];
+    const size_t edBytes = align256((size_t)n * sizeof(DevEditor));
+    if (edBytes + (size_t)n * sizeof(EditRecord) > regionBytes)
+        return SVDAG_ERR_INVALID;
+    SVDAG_CUDA(cudaMemcpyAsync(region, eds, (size_t)n * sizeof(DevEditor), cudaMemcpyHostToDevice, s));
+    const DevEditor* devEds = reinterpret_cast<const DevEditor*>(region);
+    EditRecord* records = reinterpret_cast<EditRecord*>(region + edBytes);
+    char* scratch = ctx->scratch;
+    unsigned long long scratchBytes = ctx->scratchBytes;
+    void* args[] = { &d, &single, &devEds, &n, &scratch, &scratchBytes, &records };
+    SVDAG_CUDA(cudaLaunchCooperativeKernel((const void*)k_edit_fused, dim3(grid), dim3(256), args, 0, s));
+    return SVDAG_OK;
+}
+
 svdag_status launch_fused(svdag_ctx* ctx, const DevEditor* eds, uint32_t n, bool recordEdits, cudaStream_t s)
 {
+    if (n > 1 || recordEdits) {
+        ctx->lastBatch = n;
+        return launch_fused_at(ctx, eds, n, ctx->batch, ctx->batchBytes, s);
+    }
     const int grid = fused_grid(ctx);
     if (grid <= 0)
         return SVDAG_ERR_UNSUPPORTED;
@@ -1179,15 +1305,6 @@ svdag_status launch_fused(svdag_ctx* ctx, const DevEditor* eds, uint32_t n, bool
     DevEditor single = eds[0];
     const DevEditor* devEds = nullptr;
     EditRecord* records = nullptr;
-    if (n > 1 || recordEdits) {
-        const size_t edBytes = align256((size_t)n * sizeof(DevEditor));
-        if (edBytes + (size_t)n * sizeof(EditRecord) > ctx->batchBytes)
-            return SVDAG_ERR_INVALID;
-        SVDAG_CUDA(cudaMemcpyAsync(ctx->batch, eds, (size_t)n * sizeof(DevEditor), cudaMemcpyHostToDevice, s));
-        devEds = reinterpret_cast<const DevEditor*>(ctx->batch);
-        records = reinterpret_cast<EditRecord*>(ctx->batch + edBytes);
-        ctx->lastBatch = n;
-    }
     char* scratch = ctx->scratch;
     unsigned long long scratchBytes = ctx->scratchBytes;
     void* args[] = { &d, &single, &devEds, &n, &scratch, &scratchBytes, &records };
@@ -1355,15 +1472,9 @@ svdag_status svdag_edit_apply_many(svdag_ctx* ctx, const svdag_edit* edits, uint
 {
     if (!ctx || (count && !edits))
         return SVDAG_ERR_INVALID;
-    for (uint32_t i = 0; i < count; ++i) {
-        const svdag_edit* e = &edits[i];
-        if (e->tool >= SVDAG_NUM_TOOLS || e->material >= SVDAG_NUM_MATERIALS || !std::isfinite(e->radius) || e->radius < 0
-            || (e->tool == SVDAG_TOOL_BOX_PAINT_NOISE && e->noise_cell_log2 > 20))
+    for (uint32_t i = 0; i < count; ++i)
+        if (!valid_edit(&edits[i]))
             return SVDAG_ERR_INVALID;
-        for (int a = 0; a < 3; ++a)
-            if (!std::isfinite(e->center[a]) || !std::isfinite(e->src[a]) || !std::isfinite(e->dst[a]))
-                return SVDAG_ERR_INVALID;
-    }
     return run_edit_batch(ctx, edits, count, as_stream(stream));
 }
 

@@ -91,6 +91,12 @@ svdag_status reset_dag(svdag_ctx* ctx, cudaStream_t s);
 svdag_status build_scene_untiled(svdag_ctx* ctx, const DevEditor& ed, cudaStream_t s);
 // Builds the subtrees of scene tiles, one builder editor per tile (svdag_edit.cu).
 svdag_status launch_scene_tiles(svdag_ctx* ctx, const DevEditor* eds, uint32_t n, cudaStream_t s);
+// Edit validation, expansion into device editors (a move gives two) and the persistent launch of
+// expanded editors with their editors and records in `region` (svdag_edit.cu).
+bool valid_edit(const svdag_edit* e);
+int expand_edit(const svdag_ctx* ctx, const svdag_edit& e, DevEditor* out);
+int fused_grid(svdag_ctx* ctx);
+svdag_status launch_fused_at(svdag_ctx* ctx, const DevEditor* eds, uint32_t n, char* region, size_t regionBytes, cudaStream_t s);
 // Procedural scene construction (svdag_scene.cu).
 svdag_status run_scene_build(svdag_ctx* ctx, const svdag_terrain_params* p, cudaStream_t s);
 

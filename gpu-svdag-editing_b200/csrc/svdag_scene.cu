@@ -393,3 +393,14 @@ svdag_status run_scene_build(svdag_ctx* ctx, const svdag_terrain_params* p, cuda
 }
 
 } // namespace svdag
+
+extern "C" uint32_t svdag_scene_height(const svdag_terrain_params* params, uint32_t levels, uint32_t x, uint32_t z)
+{
+    if (!params || levels < SVDAG_MIN_LEVELS || levels > SVDAG_MAX_LEVELS || params->octaves == 0 || params->octaves > 16)
+        return 0;
+    svdag::SceneParams p {};
+    p.terrain = *params;
+    p.levels = levels;
+    p.baseLog2 = levels - 2;
+    return svdag::terrain_height(p, x, z);
+}

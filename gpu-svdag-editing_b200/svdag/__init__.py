@@ -82,6 +82,24 @@ class TraceParams(C.Structure):
                 ("ray_ddy", C.c_double * 3), ("width", C.c_uint32), ("height", C.c_uint32)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("max_batch", C.c_uint32), ("max_inflight", C.c_uint32), ("memory_cap_bytes", C.c_uint64),
+                ("frame", TraceParams), ("flags", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class RequestResult(C.Structure):
+    _fields_ = [("ticket", C.c_uint64), ("kind", C.c_uint32), ("status", C.c_uint32), ("root_after", C.c_uint32),
+                ("launch", C.c_uint32), ("edited_voxels", C.c_uint64), ("submit_s", C.c_double),
+                ("visible_s", C.c_double)]
+
+
+RESULT_DTYPE = np.dtype([("ticket", "<u8"), ("kind", "<u4"), ("status", "<u4"), ("root_after", "<u4"),
+                         ("launch", "<u4"), ("edited_voxels", "<u8"), ("submit_s", "<f8"), ("visible_s", "<f8")])
+assert RESULT_DTYPE.itemsize == C.sizeof(RequestResult) == 48
+
+SERVE_PLAIN, SERVE_COPY_FRAMES = 1, 2
+
+
 class Stats(C.Structure):
     _fields_ = [("levels", C.c_uint32), ("root", C.c_uint32), ("pool_bytes", C.c_uint64),
                 ("item_region_bytes", C.c_uint64), ("item_region_used_bytes", C.c_uint64),
@@ -110,6 +128,7 @@ _PROTOS = {
     "svdag_status_string": [C.c_int],
     "svdag_abi_version": [],
     "svdag_build_terrain": [_P, C.POINTER(TerrainParams), _P],
+    "svdag_scene_height": [C.POINTER(TerrainParams), _U32, _U32, _U32],
     "svdag_edit_apply": [_P, C.POINTER(Edit), _P],
     "svdag_edit_apply_many": [_P, C.POINTER(Edit), _U32, _P],
     "svdag_last_edit_stats": [_P, C.POINTER(EditStats), _P],
@@ -137,6 +156,13 @@ _PROTOS = {
     "svdag_table_get_stats": [_P, C.POINTER(TableStats), _P],
     "svdag_get_stats": [_P, C.POINTER(Stats), _P],
     "svdag_export_level": [_P, _U32, _P, _P, _U64, C.POINTER(_U64), _P],
+    "svdag_server_create": [_P, C.POINTER(ServerConfig), C.POINTER(_P)],
+    "svdag_server_destroy": [_P],
+    "svdag_submit_edit": [_P, C.POINTER(Edit), C.POINTER(_U64)],
+    "svdag_submit_frame": [_P, C.POINTER(TraceParams), C.POINTER(_U64)],
+    "svdag_poll": [_P, _U64, C.c_int, C.POINTER(RequestResult)],
+    "svdag_server_frame": [_P, _P, _U64],
+    "svdag_server_replay": [_P, C.POINTER(Edit), _P, _U32, _P, _U32, _P],
 }
 EXPORTED = tuple(_PROTOS)
 
@@ -156,8 +182,14 @@ def lib():
             f.restype = C.c_int
         L.svdag_status_string.restype = C.c_char_p
         L.svdag_abi_version.restype = C.c_uint32
+        L.svdag_scene_height.restype = C.c_uint32
         _lib = L
     return _lib
+
+
+def scene_height(levels: int, x: int, z: int, **terrain) -> int:
+    """Surface height of column (x, z) of the procedural terrain (svdag_scene_height)."""
+    return lib().svdag_scene_height(C.byref(TerrainParams(**terrain)), levels, x, z)
 
 
 def _check(status: int, what: str):
@@ -273,9 +305,10 @@ class MyGPUHashDAG:
     """One context: one HBM pool, one slab hash table per level, the root and the undo history."""
 
     def __init__(self, levels: int, pool_bytes: int = 1 << 30, scratch_bytes: int = 0, device: int = 0,
-                 load_factor: int = 0, probe_lanes: int = 0, undo_depth: int = 0):
+                 load_factor: int = 0, probe_lanes: int = 0, undo_depth: int = 0, phase_kernels: bool = False):
         cfg = Config(levels=levels, device=device, pool_bytes=pool_bytes, scratch_bytes=scratch_bytes,
-                     target_load_factor=load_factor, probe_lanes=probe_lanes, undo_depth=undo_depth, flags=0)
+                     target_load_factor=load_factor, probe_lanes=probe_lanes, undo_depth=undo_depth,
+                     flags=1 if phase_kernels else 0)
         h = C.c_void_p()
         _check(lib().svdag_create(C.byref(cfg), C.byref(h)), "svdag_create")
         self.h = h
@@ -488,3 +521,67 @@ class DAGTracer:
 
     def hits_numpy(self) -> np.ndarray:
         return self.hits.cpu().numpy().view(HIT_DTYPE)
+
+
+class Server:
+    """The serving form: a native request loop over a resident DAG (svdag_server_*). With
+    plain=True it is the per-edit baseline: one request at a time, each edit followed by a frame."""
+
+    def __init__(self, dag: MyGPUHashDAG, frame: TraceParams, max_batch: int = 256, max_inflight: int = 2,
+                 memory_cap_bytes: int = 0, plain: bool = False, copy_frames: bool = False):
+        self.dag = dag
+        self.frame_params = frame
+        cfg = ServerConfig(max_batch=max_batch, max_inflight=max_inflight, memory_cap_bytes=memory_cap_bytes,
+                           frame=frame, flags=(SERVE_PLAIN if plain else 0) | (SERVE_COPY_FRAMES if copy_frames else 0))
+        h = C.c_void_p()
+        _check(lib().svdag_server_create(dag.h, C.byref(cfg), C.byref(h)), "svdag_server_create")
+        self.h = h
+
+    def submit_edit(self, editor) -> int:
+        e = editor if isinstance(editor, Edit) else editor.to_edit()
+        t = C.c_uint64()
+        _check(lib().svdag_submit_edit(self.h, C.byref(e), C.byref(t)), "svdag_submit_edit")
+        return t.value
+
+    def submit_frame(self, params: TraceParams | None = None) -> int:
+        t = C.c_uint64()
+        _check(lib().svdag_submit_frame(self.h, C.byref(params) if params is not None else None, C.byref(t)),
+               "svdag_submit_frame")
+        return t.value
+
+    def poll(self, ticket: int, wait: bool = True):
+        """RequestResult, or None while not visible (wait=False)."""
+        r = RequestResult()
+        st = lib().svdag_poll(self.h, ticket, 1 if wait else 0, C.byref(r))
+        if st == 8 and not wait:
+            return None
+        _check(st, "svdag_poll")
+        return r
+
+    def frame(self) -> np.ndarray:
+        n = self.frame_params.width * self.frame_params.height
+        out = np.zeros(n, dtype=HIT_DTYPE)
+        _check(lib().svdag_server_frame(self.h, out.ctypes.data, n), "svdag_server_frame")
+        return out
+
+    def replay(self, edits, edit_times, frame_times=()) -> np.ndarray:
+        """Submits edit i at edit_times[i] s and frame j at frame_times[j] s after the call starts;
+        returns the results (edits first, then frames) once all are visible."""
+        arr = (Edit * max(len(edits), 1))(*[e if isinstance(e, Edit) else e.to_edit() for e in edits])
+        et = np.ascontiguousarray(edit_times, dtype=np.float64)
+        ft = np.ascontiguousarray(frame_times, dtype=np.float64)
+        out = np.zeros(len(edits) + len(ft), dtype=RESULT_DTYPE)
+        _check(lib().svdag_server_replay(self.h, arr, et.ctypes.data, len(edits), ft.ctypes.data, len(ft),
+                                         out.ctypes.data), "svdag_server_replay")
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            h, self.h = self.h, None
+            _check(lib().svdag_server_destroy(h), "svdag_server_destroy")
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

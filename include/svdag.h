@@ -54,6 +54,10 @@ typedef enum svdag_status {
  * 2 + ceil(4 * popcount(64-bit voxel mask) / 32). Keys are self-describing. */
 typedef enum svdag_item_kind { SVDAG_KIND_NODE = 0, SVDAG_KIND_LEAF = 1 } svdag_item_kind;
 
+/* Run every edit phase as its own kernel launch instead of one persistent cooperative launch per
+ * edit or batch (for profiling single phases; slower for small edits). */
+#define SVDAG_FLAG_PHASE_KERNELS 1u
+
 typedef struct svdag_config {
     uint32_t levels; /* octree depth, SVDAG_MIN_LEVELS..SVDAG_MAX_LEVELS (1 << levels voxels per axis) */
     int32_t device; /* CUDA device ordinal */
@@ -62,7 +66,7 @@ typedef struct svdag_config {
     uint32_t target_load_factor; /* items per bucket when a level table is sized; 0 = default (16) */
     uint32_t probe_lanes; /* lanes cooperating on one key: 1, 2, 4, 8, 16 or 32; 0 = default (1) */
     uint32_t undo_depth; /* undo history ring size; 0 = default (32) */
-    uint32_t flags; /* reserved, must be 0 */
+    uint32_t flags; /* SVDAG_FLAG_* */
 } svdag_config;
 
 typedef struct svdag_ctx svdag_ctx;
@@ -112,6 +116,9 @@ typedef struct svdag_terrain_params {
  * scene load MyGPUHashDAGFactory::load_from_DAG (my_gpu_hash_dag_factory.cpp:427-500). Every
  * uniformly filled node carries the fully-filled header bits, as the factory's create_dag_cpu does. */
 svdag_status svdag_build_terrain(svdag_ctx* ctx, const svdag_terrain_params* params, void* stream);
+/* Surface height of column (x, z) of the terrain of a 2^levels grid (host function, for placing
+ * edits on the surface). No counterpart in the reference, whose scenes are loaded from files. */
+uint32_t svdag_scene_height(const svdag_terrain_params* params, uint32_t levels, uint32_t x, uint32_t z);
 
 /* ---------------------------------------------------------------- edits */
 
@@ -314,6 +321,61 @@ svdag_status svdag_get_stats(svdag_ctx* ctx, svdag_stats* out, void* stream);
  * comparison (MyGPUHashDAG::copy<CPU>, my_gpu_hash_dag.h:106-127). */
 svdag_status svdag_export_level(svdag_ctx* ctx, uint32_t level, uint32_t* out_handles, uint32_t* out_words,
     uint64_t capacity, uint64_t* out_count, void* stream);
+
+/* ---------------------------------------------------------------- serving form
+ *
+ * A request loop on its own host thread keeps the DAG, its tables and the undo history resident and
+ * serves edit and frame requests as they arrive. Edits that arrive while earlier launches are on the
+ * GPU are coalesced into the next batched persistent launch (continuous batching: up to max_inflight
+ * launches are queued on the GPU ahead of their completion); every launch is followed by a frame of
+ * the new state, which makes its edits visible and answers every frame request pending at launch.
+ * An edit is admitted when the item-region bytes in use plus those reserved by admitted, unfinished
+ * edits (an upper estimate from the tool's footprint) stay under the memory cap; a queue head that
+ * does not fit waits until launches complete. With SVDAG_SERVE_PLAIN the same loop serves one request
+ * at a time, synchronously, as the reference's engine does (an edit, then a frame: engine.h:104-163,
+ * engine.cpp:627-629): the per-edit baseline. No counterpart in the reference beyond that loop. */
+
+#define SVDAG_SERVE_PLAIN 1u /* one request per launch, synchronously */
+#define SVDAG_SERVE_COPY_FRAMES 2u /* copy every rendered frame to host memory (svdag_server_frame) */
+
+typedef struct svdag_server_config {
+    uint32_t max_batch; /* edits per launch; 0 = 256 */
+    uint32_t max_inflight; /* launches queued on the GPU; 0 = 2 */
+    uint64_t memory_cap_bytes; /* item-region budget for admission; 0 = the whole item region */
+    svdag_trace_params frame; /* camera and resolution of the frames rendered after each launch */
+    uint32_t flags; /* SVDAG_SERVE_* */
+    uint32_t reserved;
+} svdag_server_config;
+
+typedef struct svdag_server svdag_server;
+
+typedef struct svdag_request_result {
+    uint64_t ticket;
+    uint32_t kind; /* 0 edit, 1 frame */
+    uint32_t status; /* svdag_status of the edit (frames: 0) */
+    uint32_t root_after; /* edits: root after this edit */
+    uint32_t launch; /* sequence number of the launch that carried the request */
+    uint64_t edited_voxels;
+    double submit_s; /* host clock, seconds since the server started */
+    double visible_s; /* completion of the frame that shows the request */
+} svdag_request_result;
+
+svdag_status svdag_server_create(svdag_ctx* ctx, const svdag_server_config* config, svdag_server** out);
+/* Serves every request submitted so far, then stops the loop and frees the server (not the context). */
+svdag_status svdag_server_destroy(svdag_server* server);
+svdag_status svdag_submit_edit(svdag_server* server, const svdag_edit* edit, uint64_t* out_ticket);
+/* `params` may be NULL (the configured camera). */
+svdag_status svdag_submit_frame(svdag_server* server, const svdag_trace_params* params, uint64_t* out_ticket);
+/* Result of a request: with wait = 0 returns SVDAG_ERR_BUSY while it is not visible yet. A result is
+ * handed out once. */
+svdag_status svdag_poll(svdag_server* server, uint64_t ticket, int wait, svdag_request_result* out);
+/* Copies the most recent frame (SVDAG_SERVE_COPY_FRAMES) to `out` (width * height hits). */
+svdag_status svdag_server_frame(svdag_server* server, svdag_hit* out, uint64_t capacity);
+/* Replays a timed request stream (the reference's replay of recorded edits, replay.h): edit i is
+ * submitted edit_times[i] seconds after the call starts, frame j at frame_times[j]; returns when all
+ * are visible, with results[0 .. n_edits) for the edits and results[n_edits ..) for the frames. */
+svdag_status svdag_server_replay(svdag_server* server, const svdag_edit* edits, const double* edit_times, uint32_t n_edits,
+    const double* frame_times, uint32_t n_frames, svdag_request_result* results);
 
 #ifdef __cplusplus
 }

@@ -37,6 +37,8 @@ def test_struct_layouts(svdag_lib):
     assert C.sizeof(s.Config) == 40
     assert C.sizeof(s.TraceParams) == 104
     assert C.sizeof(s.TerrainParams) == 32
+    assert C.sizeof(s.ServerConfig) == 128
+    assert C.sizeof(s.RequestResult) == 48
 
 
 def test_invalid_arguments_are_rejected(svdag_lib):
