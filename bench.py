@@ -219,8 +219,12 @@ def c2_camera(svdag, levels, width=1920, height=1080):
 
 
 def make_scene(svdag, w, levels, phase_kernels=False):
-    dag = svdag.MyGPUHashDAG(levels, pool_bytes=min(POOL_CAP, 52 << 30), scratch_bytes=16 << 30, undo_depth=32,
-                             phase_kernels=phase_kernels)
+    # 52 GB at depth 17 (a 32 GiB item region, 16 GiB scratch); smaller scenes get a share of it by
+    # surface area (4^(levels-17)), at least 2 GB
+    shrink = 4 ** max(0, w.C2_LEVELS - levels)
+    pool = max(2 << 30, min(POOL_CAP, 52 << 30) // shrink)
+    dag = svdag.MyGPUHashDAG(levels, pool_bytes=pool, scratch_bytes=max(512 << 20, (16 << 30) // shrink),
+                             undo_depth=32, phase_kernels=phase_kernels)
     terrain = make_terrain(w, levels)
     dag.build_terrain(**terrain)
     dag.sync()
@@ -565,7 +569,7 @@ def main():
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--mode", default="serve", choices=["serve", "c0", "c2", "c3", "hash"],
                     help="serve = the benchmark line; the others run one sub-workload (profiling)")
-    ap.add_argument("--rate", type=float, default=1000.0, help="edit arrivals per second")
+    ap.add_argument("--rate", type=float, default=500.0, help="edit arrivals per second")
     ap.add_argument("--window", type=float, default=0.5, help="seconds of the stream per step")
     ap.add_argument("--levels", type=int, default=17)
     ap.add_argument("--phase-kernels", action="store_true", help="one launch per edit phase (profiling)")

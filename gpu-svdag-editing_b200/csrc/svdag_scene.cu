@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <map>
 #include <vector>
@@ -346,7 +347,15 @@ svdag_status run_scene_build(svdag_ctx* ctx, const svdag_terrain_params* p, cuda
     const uint32_t levels = ctx->cfg.levels;
     HostScene hs;
     make_scene(levels, *p, hs);
-    const uint32_t T = p->tile_level ? p->tile_level : (levels > 13 ? levels - 13 : 0);
+    // Automatic tile level: the smallest whose tiles' intermediate SVO fits half the scratch arena,
+    // at about 3 * 4^(depth of a tile - 2) leaves (a heightfield surface with structures) of ~200
+    // bytes each with their work items and dedup entries.
+    uint32_t T = p->tile_level;
+    if (!T) {
+        const double fit = std::log(std::max(1.0, (double)ctx->scratchBytes / 2.0 / (3.0 * 200.0))) / std::log(4.0);
+        const double t = std::ceil((double)levels - 2.0 - fit);
+        T = t <= 0.0 ? 0u : std::min<uint32_t>((uint32_t)t, std::min<uint32_t>(levels - 3, 6));
+    }
     // Top of the scratch arena: scene arrays, tile results and key staging (at most 8^T tiles).
     const unsigned long long sceneBytes = scene_device_bytes(hs);
     const unsigned long long topBytes = T ? align256((1ull << (3 * T)) * 4) + (64ull << 10) * 4 * 11 : 0;

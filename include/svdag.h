@@ -95,8 +95,8 @@ typedef struct svdag_terrain_params {
     uint32_t num_structures; /* random boxes/spheres unioned on the surface (0 = none), at most 65536 */
     uint32_t structure_seed;
     uint32_t tile_level; /* level (at most min(levels - 3, 6)) at which the build is cut into
-                            independently built tiles; 0 = automatic (levels - 13 above depth 13,
-                            untiled otherwise) */
+                            independently built tiles; 0 = automatic (the smallest level whose
+                            tiles fit the scratch arena; untiled when the whole scene fits) */
 } svdag_terrain_params;
 
 /* The scene. Voxel (x, y, z) of a 2^levels grid is solid when y < height(x, z) or when a structure
