@@ -218,13 +218,13 @@ def c2_camera(svdag, levels, width=1920, height=1080):
                                   (0.5 * g, 0.52 * g, 0.5 * g), width, height)
 
 
-def make_scene(svdag, w, levels, phase_kernels=False):
+def make_scene(svdag, w, levels, phase_kernels=False, pool_gb=0.0, persistent=False):
     # 52 GB at depth 17 (a 32 GiB item region, 16 GiB scratch); smaller scenes get a share of it by
     # surface area (4^(levels-17)), at least 2 GB
     shrink = 4 ** max(0, w.C2_LEVELS - levels)
-    pool = max(2 << 30, min(POOL_CAP, 52 << 30) // shrink)
+    pool = int(pool_gb * (1 << 30)) if pool_gb else max(2 << 30, min(POOL_CAP, 52 << 30) // shrink)
     dag = svdag.MyGPUHashDAG(levels, pool_bytes=pool, scratch_bytes=max(512 << 20, (16 << 30) // shrink),
-                             undo_depth=32, phase_kernels=phase_kernels)
+                             undo_depth=32, phase_kernels=phase_kernels, persistent=persistent)
     terrain = make_terrain(w, levels)
     dag.build_terrain(**terrain)
     dag.sync()
@@ -288,7 +288,7 @@ def run_serve(args):
     out = {}
     # served and plain paths, each on its own copy of the scene
     for name, plain in (("served", False), ("plain", True)):
-        dag, _ = make_scene(svdag, w, levels)
+        dag, _ = make_scene(svdag, w, levels, persistent=args.persistent)
         replay(svdag, dag, cam, ew, tw, fw, plain=plain)
         if dist:
             dist.barrier()
@@ -482,7 +482,8 @@ def run_mode_c0(args):
     import svdag.workloads as w
 
     edits = w.c0_edits(max(args.warmup + args.steps, 64))
-    dag = svdag.MyGPUHashDAG(w.C0_LEVELS, pool_bytes=4 << 30, scratch_bytes=1 << 30, phase_kernels=args.phase_kernels)
+    dag = svdag.MyGPUHashDAG(w.C0_LEVELS, pool_bytes=4 << 30, scratch_bytes=1 << 30, phase_kernels=args.phase_kernels,
+                             persistent=args.persistent)
     dag.build_terrain(**w.C0_TERRAIN)
     params = svdag.get_trace_params((512.0, 900.0, 512.0), (512.0, 512.0, 512.0), C0_FRAME, C0_FRAME)
     hits = torch.empty(C0_FRAME * C0_FRAME * 68, dtype=torch.uint8, device="cuda")
@@ -511,7 +512,10 @@ def run_mode_c2(args):
     import svdag
     import svdag.workloads as w
 
-    dag, terrain = make_scene(svdag, w, args.levels, phase_kernels=args.phase_kernels)
+    t0 = time.perf_counter()
+    dag, terrain = make_scene(svdag, w, args.levels, phase_kernels=args.phase_kernels, pool_gb=args.pool_gb,
+                              persistent=args.persistent)
+    build_s = time.perf_counter() - t0
     out = []
     for e in w.c2_edits(args.levels, terrain):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -526,7 +530,7 @@ def run_mode_c2(args):
                     "edited_mvox": st.edited_voxels / 1e6, "svo_items": int(sum(st.svo_nodes)), "new_items": int(st.new_items),
                     "phase_us": [round(float(pt[i + 1] - pt[i]) / 1e3, 1) for i in range(len(pt) - 1)]})
     dag.free()
-    print(json.dumps({"levels": args.levels, "edits": out}))
+    print(json.dumps({"levels": args.levels, "build_s": build_s, "edits": out}))
 
 
 def run_mode_c3(args):
@@ -573,6 +577,8 @@ def main():
     ap.add_argument("--window", type=float, default=0.5, help="seconds of the stream per step")
     ap.add_argument("--levels", type=int, default=17)
     ap.add_argument("--phase-kernels", action="store_true", help="one launch per edit phase (profiling)")
+    ap.add_argument("--persistent", action="store_true", help="small edits in the persistent cooperative kernel")
+    ap.add_argument("--pool-gb", type=float, default=0.0, help="pool size of the c2 mode's scene (0 = by depth)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-hash", action="store_true")
     ap.add_argument("--hash-keys", type=int, default=1 << 24)

@@ -145,7 +145,7 @@ const char* svdag_status_string(svdag_status s)
 
 svdag_status svdag_create(const svdag_config* cfg, svdag_ctx** out)
 {
-    if (!cfg || !out || cfg->levels < SVDAG_MIN_LEVELS || cfg->levels > SVDAG_MAX_LEVELS || (cfg->flags & ~SVDAG_FLAG_PHASE_KERNELS) != 0)
+    if (!cfg || !out || cfg->levels < SVDAG_MIN_LEVELS || cfg->levels > SVDAG_MAX_LEVELS || (cfg->flags & ~(SVDAG_FLAG_PHASE_KERNELS | SVDAG_FLAG_PERSISTENT)) != 0)
         return SVDAG_ERR_INVALID;
     if (cfg->probe_lanes && cfg->probe_lanes != 1 && cfg->probe_lanes != 2 && cfg->probe_lanes != 4 && cfg->probe_lanes != 8
         && cfg->probe_lanes != 16 && cfg->probe_lanes != 32)
@@ -181,7 +181,9 @@ svdag_status svdag_create(const svdag_config* cfg, svdag_ctx** out)
     ctx->poolBytes = pool;
     ctx->ctl = reinterpret_cast<Control*>(ctx->pool);
     ctx->batch = ctx->pool + kCtlBytes;
-    ctx->batchBytes = kBatchBytes;
+    ctx->batchBytes = kBatchBytes - 4096; // the last 4 KiB hold the editor queue of the phase launches
+    ctx->queue = reinterpret_cast<EditQueue*>(ctx->batch + ctx->batchBytes);
+    static_assert(sizeof(EditQueue) <= 4096, "editor queue too large");
     ctx->scratch = ctx->pool + kCtlBytes + kBatchBytes;
     ctx->scratchBytes = scratch;
     ctx->items = reinterpret_cast<uint32_t*>(ctx->pool + kCtlBytes + kBatchBytes + scratch);
@@ -214,6 +216,10 @@ svdag_status svdag_destroy(svdag_ctx* ctx)
     cudaSetDevice(ctx->device);
     for (auto* t : ctx->standalone)
         delete t;
+    for (auto& g : ctx->graphs)
+        if (g)
+            cudaGraphExecDestroy(g);
+    cudaDeviceSynchronize();
     cudaFree(ctx->pool);
     delete ctx;
     return SVDAG_OK;

@@ -951,15 +951,29 @@ __device__ void ph_reset_counters(const DevDag& d)
 
 // ---------------------------------------------------------------- kernel wrappers (one launch per phase)
 
-__global__ void k_edit_begin(DevDag d, DevEditor e, char* scratch) { ph_edit_begin(d, e, scratch); }
-template <uint32_t TOOL>
-__global__ void __launch_bounds__(256) k_build_level(DevDag d, DevEditor e, uint32_t level, char* scratch, unsigned long long scratchBytes)
+__global__ void k_edit_begin(DevDag d, EditQueue* q, char* scratch)
 {
+    if (q->eds) { // next editor of the batch into the slot
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(q->eds + q->cursor);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(&q->slot);
+        for (uint32_t i = threadIdx.x; i < sizeof(DevEditor) / 4; i += blockDim.x)
+            dst[i] = src[i];
+        __syncwarp();
+    }
+    ph_reset_counters(d);
+    __syncwarp();
+    ph_edit_begin(d, q->slot, scratch);
+}
+template <uint32_t TOOL>
+__global__ void __launch_bounds__(256) k_build_level(DevDag d, const EditQueue* q, uint32_t level, char* scratch, unsigned long long scratchBytes)
+{
+    const DevEditor e = q->slot;
     ph_build_level<TOOL>(d, e, level, scratch, scratchBytes);
 }
 template <uint32_t TOOL>
-__global__ void __launch_bounds__(256) k_build_leaves(DevDag d, DevEditor e, char* scratch, unsigned long long scratchBytes)
+__global__ void __launch_bounds__(256) k_build_leaves(DevDag d, const EditQueue* q, char* scratch, unsigned long long scratchBytes)
 {
+    const DevEditor e = q->slot;
     ph_build_leaves<TOOL>(d, e, scratch, scratchBytes);
 }
 __global__ void __launch_bounds__(256) k_fix_level(DevDag d, uint32_t level, uint32_t builder, char* scratch)
@@ -973,7 +987,12 @@ __global__ void __launch_bounds__(256) k_insert_level(DevDag d, DevTable t, uint
 {
     ph_insert_level<G>(d, t, level, scratch);
 }
-__global__ void k_edit_end(DevDag d, char* scratch, uint32_t builder, uint32_t* tileOut) { ph_edit_end(d, scratch, builder, tileOut, nullptr); }
+__global__ void k_edit_end(DevDag d, char* scratch, EditQueue* q)
+{
+    ph_edit_end(d, scratch, q->slot.builder, q->slot.tileOut, q->slot.record);
+    if (threadIdx.x == 0 && q->eds)
+        ++q->cursor;
+}
 
 // ---------------------------------------------------------------- persistent form
 // One cooperative launch runs whole edits: every phase above is a grid-stride loop over the
@@ -1139,39 +1158,40 @@ DevEditor make_editor(const svdag_ctx* ctx, const svdag_edit& e)
 }
 
 template <uint32_t TOOL>
-svdag_status launch_build(svdag_ctx* ctx, const DevEditor& ed, cudaStream_t s)
+svdag_status launch_build(svdag_ctx* ctx, cudaStream_t s)
 {
     const DevDag d = ctx->dag();
+    const EditQueue* q = ctx->queue;
     const uint32_t LL = d.leafLevel;
     for (uint32_t level = 0; level < LL; ++level) {
         const unsigned long long bound = level < 8 ? (1ull << (3 * level)) : (1ull << 24);
-        k_build_level<TOOL><<<grid_for(ctx, bound * 8, 256), 256, 0, s>>>(d, ed, level, ctx->scratch, ctx->scratchBytes);
+        k_build_level<TOOL><<<grid_for(ctx, bound * 8, 256), 256, 0, s>>>(d, q, level, ctx->scratch, ctx->scratchBytes);
     }
     const unsigned long long bound = LL < 8 ? (1ull << (3 * LL)) : (1ull << 24);
-    k_build_leaves<TOOL><<<grid_for(ctx, bound * 32, 256), 256, 0, s>>>(d, ed, ctx->scratch, ctx->scratchBytes);
+    k_build_leaves<TOOL><<<grid_for(ctx, bound * 32, 256), 256, 0, s>>>(d, q, ctx->scratch, ctx->scratchBytes);
     SVDAG_CUDA(cudaGetLastError());
     return SVDAG_OK;
 }
 
-svdag_status launch_build_any(svdag_ctx* ctx, const DevEditor& ed, cudaStream_t s)
+svdag_status launch_build_any(svdag_ctx* ctx, uint32_t tool, cudaStream_t s)
 {
-    switch (ed.tool) {
+    switch (tool) {
     case SVDAG_TOOL_SPHERE_ADD:
-        return launch_build<SVDAG_TOOL_SPHERE_ADD>(ctx, ed, s);
+        return launch_build<SVDAG_TOOL_SPHERE_ADD>(ctx, s);
     case SVDAG_TOOL_SPHERE_REMOVE:
-        return launch_build<SVDAG_TOOL_SPHERE_REMOVE>(ctx, ed, s);
+        return launch_build<SVDAG_TOOL_SPHERE_REMOVE>(ctx, s);
     case SVDAG_TOOL_BOX_ADD:
-        return launch_build<SVDAG_TOOL_BOX_ADD>(ctx, ed, s);
+        return launch_build<SVDAG_TOOL_BOX_ADD>(ctx, s);
     case SVDAG_TOOL_BOX_REMOVE:
-        return launch_build<SVDAG_TOOL_BOX_REMOVE>(ctx, ed, s);
+        return launch_build<SVDAG_TOOL_BOX_REMOVE>(ctx, s);
     case SVDAG_TOOL_SPHERE_PAINT:
-        return launch_build<SVDAG_TOOL_SPHERE_PAINT>(ctx, ed, s);
+        return launch_build<SVDAG_TOOL_SPHERE_PAINT>(ctx, s);
     case SVDAG_TOOL_COPY:
-        return launch_build<SVDAG_TOOL_COPY>(ctx, ed, s);
+        return launch_build<SVDAG_TOOL_COPY>(ctx, s);
     case SVDAG_TOOL_BOX_PAINT_NOISE:
-        return launch_build<SVDAG_TOOL_BOX_PAINT_NOISE>(ctx, ed, s);
+        return launch_build<SVDAG_TOOL_BOX_PAINT_NOISE>(ctx, s);
     case kToolTerrain:
-        return launch_build<kToolTerrain>(ctx, ed, s);
+        return launch_build<kToolTerrain>(ctx, s);
     default:
         return SVDAG_ERR_INVALID;
     }
@@ -1211,17 +1231,135 @@ unsigned long long level_bound(uint32_t level) { return level < 8 ? (1ull << (3 
 
 } // namespace
 
-svdag_status launch_pipeline(svdag_ctx* ctx, const DevEditor& ed, cudaStream_t s)
+// The phases of the editor in the queue slot, one launch each.
+svdag_status launch_phases(svdag_ctx* ctx, uint32_t tool, cudaStream_t s)
 {
     const DevDag d = ctx->dag();
-    SVDAG_CUDA(cudaMemsetAsync(&ctx->ctl->edit, 0, sizeof(EditCounters), s));
-    k_edit_begin<<<1, 32, 0, s>>>(d, ed, ctx->scratch);
-    SVDAG_TRY(launch_build_any(ctx, ed, s));
+    k_edit_begin<<<1, 32, 0, s>>>(d, ctx->queue, ctx->scratch);
+    SVDAG_TRY(launch_build_any(ctx, tool, s));
     const uint32_t LL = d.leafLevel;
     for (int level = (int)LL; level >= 0; --level)
         k_merge_level<<<grid_for(ctx, level_bound(level), 256), 256, 0, s>>>(d, level, ctx->scratch);
-    k_edit_end<<<1, 32, 0, s>>>(d, ctx->scratch, ed.builder, ed.tileOut);
+    k_edit_end<<<1, 32, 0, s>>>(d, ctx->scratch, ctx->queue);
     SVDAG_CUDA(cudaGetLastError());
+    return SVDAG_OK;
+}
+
+// Runs the editor in the queue slot: through the tool's CUDA graph of the phase launches (captured
+// on first use), or launch by launch with SVDAG_FLAG_PHASE_KERNELS and while a scene build has
+// lent part of the scratch arena.
+svdag_status run_phases(svdag_ctx* ctx, uint32_t tool, cudaStream_t s, bool graphOk)
+{
+    const int g = tool == kToolTerrain ? kNumGraphs - 1 : (int)tool;
+    if (!graphOk || (ctx->cfg.flags & SVDAG_FLAG_PHASE_KERNELS) || g < 0 || g >= kNumGraphs)
+        return launch_phases(ctx, tool, s);
+    if (!ctx->graphs[g]) {
+        cudaStream_t cs;
+        SVDAG_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        cudaGraph_t graph = nullptr;
+        svdag_status st = SVDAG_OK;
+        if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            st = launch_phases(ctx, tool, cs);
+            const cudaError_t e = cudaStreamEndCapture(cs, &graph);
+            if (st == SVDAG_OK && e != cudaSuccess)
+                st = cuda_status(e);
+        } else {
+            st = SVDAG_ERR_CUDA;
+        }
+        if (st == SVDAG_OK && cudaGraphInstantiate(&ctx->graphs[g], graph, 0) != cudaSuccess)
+            st = SVDAG_ERR_CUDA;
+        if (graph)
+            cudaGraphDestroy(graph);
+        cudaStreamDestroy(cs);
+        if (st != SVDAG_OK) {
+            ctx->graphs[g] = nullptr;
+            return st;
+        }
+    }
+    SVDAG_CUDA(cudaGraphLaunch(ctx->graphs[g], s));
+    return SVDAG_OK;
+}
+
+// One editor: copied into the queue slot from host memory, then its phases.
+svdag_status launch_pipeline(svdag_ctx* ctx, const DevEditor& ed, cudaStream_t s, EditRecord* record, bool graphOk)
+{
+    EditQueue h {};
+    h.eds = nullptr;
+    h.slot = ed;
+    h.slot.record = record;
+    SVDAG_CUDA(cudaMemcpyAsync(ctx->queue, &h, sizeof(h), cudaMemcpyHostToDevice, s));
+    return run_phases(ctx, ed.tool, s, graphOk);
+}
+
+// Upper estimate of the leaves of an editor's intermediate SVO: the bounding volume in 4^3 bricks or,
+// for sphere and box add/remove, a shell of three bricks around the surface (interiors are filled or
+// emptied whole); the noise paint and the copy subdivide their whole box.
+double estimate_leaves(const DevEditor& e)
+{
+    double side;
+    switch (e.tool) {
+    case SVDAG_TOOL_SPHERE_ADD:
+    case SVDAG_TOOL_SPHERE_REMOVE:
+    case SVDAG_TOOL_SPHERE_PAINT: {
+        const double r = e.radius / 4.0 + 1.0;
+        return std::min(8.0 * r * r * r, 12.0 * M_PI * r * r);
+    }
+    case kToolTerrain:
+        return 1e12;
+    default:
+        side = std::max({ e.bmax[0] - e.bmin[0], e.bmax[1] - e.bmin[1], e.bmax[2] - e.bmin[2] }) / 4.0 + 2.0;
+        if (e.tool == SVDAG_TOOL_BOX_ADD || e.tool == SVDAG_TOOL_BOX_REMOVE)
+            return std::min(side * side * side, 18.0 * side * side);
+        return side * side * side;
+    }
+}
+
+// Launches expanded editors with their editors and records in `region`: runs of small edits in one
+// persistent launch each (grid barriers are cheaper than launches for small SVOs), large edits as one
+// launch per phase at full occupancy (the persistent kernel holds 16 warps per SM).
+svdag_status launch_edits_at(svdag_ctx* ctx, const DevEditor* eds, uint32_t n, char* region, size_t regionBytes, cudaStream_t s)
+{
+    const size_t edBytes = align256((size_t)n * sizeof(DevEditor));
+    if (edBytes + (size_t)n * sizeof(EditRecord) > regionBytes)
+        return SVDAG_ERR_INVALID;
+    const DevEditor* devEds = reinterpret_cast<const DevEditor*>(region);
+    EditRecord* records = reinterpret_cast<EditRecord*>(region + edBytes);
+    {
+        std::vector<DevEditor> withRecords(eds, eds + n);
+        for (uint32_t k = 0; k < n; ++k)
+            withRecords[k].record = records + k;
+        // a pageable source is staged before the call returns, so the vector may go
+        SVDAG_CUDA(cudaMemcpyAsync(region, withRecords.data(), (size_t)n * sizeof(DevEditor), cudaMemcpyHostToDevice, s));
+    }
+    const int grid = (ctx->cfg.flags & SVDAG_FLAG_PERSISTENT) ? fused_grid(ctx) : 0;
+    auto small = [&](uint32_t k) { return grid > 0 && estimate_leaves(eds[k]) <= ctx->bigEditLeaves; };
+    uint32_t i = 0;
+    while (i < n) {
+        if (!small(i)) { // a run of editors through the queue: the first phase takes eds[cursor]
+            uint32_t j = i + 1;
+            while (j < n && !small(j))
+                ++j;
+            const EditQueue head { devEds + i, 0, 0, {} };
+            SVDAG_CUDA(cudaMemcpyAsync(ctx->queue, &head, offsetof(EditQueue, slot), cudaMemcpyHostToDevice, s));
+            for (uint32_t k = i; k < j; ++k)
+                SVDAG_TRY(run_phases(ctx, eds[k].tool, s, true));
+            i = j;
+            continue;
+        }
+        uint32_t j = i + 1;
+        while (j < n && small(j))
+            ++j;
+        DevDag d = ctx->dag();
+        DevEditor single = eds[i];
+        const DevEditor* segEds = devEds + i;
+        EditRecord* segRec = records + i;
+        uint32_t m = j - i;
+        char* scratch = ctx->scratch;
+        unsigned long long scratchBytes = ctx->scratchBytes;
+        void* args[] = { &d, &single, &segEds, &m, &scratch, &scratchBytes, &segRec };
+        SVDAG_CUDA(cudaLaunchCooperativeKernel((const void*)k_edit_fused, dim3(grid), dim3(256), args, 0, s));
+        i = j;
+    }
     return SVDAG_OK;
 }
 
@@ -1272,39 +1410,15 @@ int fused_grid(svdag_ctx* ctx)
     return ctx->fusedGrid;
 }
 
-svdag_status launch_fused_at(svdag_ctx* ctx, const DevEditor* eds, uint32_t n, char* region, size_t regionBytes, cudaStream_t s)
+// One small edit as one persistent launch, its editor passed by value.
+svdag_status launch_single_fused(svdag_ctx* ctx, const DevEditor& ed, cudaStream_t s)
 {
     const int grid = fused_grid(ctx);
-    if (grid <= 0)
-        return SVDAG_ERR_UNSUPPORTED;
     DevDag d = ctx->dag();
-    DevEditor single = eds[0];
-    const size_t edBytes = align256((size_t)n * sizeof(DevEditor));
-    if (edBytes + (size_t)n * sizeof(EditRecord) > regionBytes)
-        return SVDAG_ERR_INVALID;
-    SVDAG_CUDA(cudaMemcpyAsync(region, eds, (size_t)n * sizeof(DevEditor), cudaMemcpyHostToDevice, s));
-    const DevEditor* devEds = reinterpret_cast<const DevEditor*>(region);
-    EditRecord* records = reinterpret_cast<EditRecord*>(region + edBytes);
-    char* scratch = ctx->scratch;
-    unsigned long long scratchBytes = ctx->scratchBytes;
-    void* args[] = { &d, &single, &devEds, &n, &scratch, &scratchBytes, &records };
-    SVDAG_CUDA(cudaLaunchCooperativeKernel((const void*)k_edit_fused, dim3(grid), dim3(256), args, 0, s));
-    return SVDAG_OK;
-}
-
-svdag_status launch_fused(svdag_ctx* ctx, const DevEditor* eds, uint32_t n, bool recordEdits, cudaStream_t s)
-{
-    if (n > 1 || recordEdits) {
-        ctx->lastBatch = n;
-        return launch_fused_at(ctx, eds, n, ctx->batch, ctx->batchBytes, s);
-    }
-    const int grid = fused_grid(ctx);
-    if (grid <= 0)
-        return SVDAG_ERR_UNSUPPORTED;
-    DevDag d = ctx->dag();
-    DevEditor single = eds[0];
+    DevEditor single = ed;
     const DevEditor* devEds = nullptr;
     EditRecord* records = nullptr;
+    uint32_t n = 1;
     char* scratch = ctx->scratch;
     unsigned long long scratchBytes = ctx->scratchBytes;
     void* args[] = { &d, &single, &devEds, &n, &scratch, &scratchBytes, &records };
@@ -1317,10 +1431,12 @@ svdag_status run_edit(svdag_ctx* ctx, const svdag_edit* e, cudaStream_t s)
     SVDAG_TRY(ensure_level_tables(ctx, s));
     DevEditor eds[2];
     const int n = expand_edit(ctx, *e, eds);
-    if (fused_grid(ctx) > 0)
-        return launch_fused(ctx, eds, (uint32_t)n, false, s);
-    for (int i = 0; i < n; ++i)
-        SVDAG_TRY(launch_pipeline(ctx, eds[i], s));
+    for (int i = 0; i < n; ++i) {
+        if ((ctx->cfg.flags & SVDAG_FLAG_PERSISTENT) && fused_grid(ctx) > 0 && estimate_leaves(eds[i]) <= ctx->bigEditLeaves)
+            SVDAG_TRY(launch_single_fused(ctx, eds[i], s));
+        else
+            SVDAG_TRY(launch_pipeline(ctx, eds[i], s, nullptr, true));
+    }
     return SVDAG_OK;
 }
 
@@ -1336,14 +1452,12 @@ svdag_status run_edit_batch(svdag_ctx* ctx, const svdag_edit* edits, uint32_t co
     }
     if (eds.empty())
         return SVDAG_OK;
-    if (fused_grid(ctx) > 0) {
-        const uint32_t maxPerLaunch = (uint32_t)(ctx->batchBytes / (sizeof(DevEditor) + sizeof(EditRecord) + 8));
-        for (size_t i = 0; i < eds.size(); i += maxPerLaunch)
-            SVDAG_TRY(launch_fused(ctx, eds.data() + i, (uint32_t)std::min<size_t>(maxPerLaunch, eds.size() - i), true, s));
-        return SVDAG_OK;
+    const uint32_t maxPerLaunch = (uint32_t)((ctx->batchBytes - 256) / (sizeof(DevEditor) + sizeof(EditRecord)));
+    for (size_t i = 0; i < eds.size(); i += maxPerLaunch) {
+        const uint32_t m = (uint32_t)std::min<size_t>(maxPerLaunch, eds.size() - i);
+        ctx->lastBatch = m;
+        SVDAG_TRY(launch_edits_at(ctx, eds.data() + i, m, ctx->batch, ctx->batchBytes, s));
     }
-    for (const auto& ed : eds)
-        SVDAG_TRY(launch_pipeline(ctx, ed, s));
     return SVDAG_OK;
 }
 
@@ -1371,9 +1485,13 @@ svdag_status build_scene_untiled(svdag_ctx* ctx, const DevEditor& ed, cudaStream
 {
     SVDAG_TRY(reset_dag(ctx, s));
     const DevDag d = ctx->dag();
-    SVDAG_CUDA(cudaMemsetAsync(&ctx->ctl->edit, 0, sizeof(EditCounters), s));
-    k_edit_begin<<<1, 32, 0, s>>>(d, ed, ctx->scratch);
-    SVDAG_TRY(launch_build_any(ctx, ed, s));
+    {
+        EditQueue h {};
+        h.slot = ed;
+        SVDAG_CUDA(cudaMemcpyAsync(ctx->queue, &h, sizeof(h), cudaMemcpyHostToDevice, s));
+    }
+    k_edit_begin<<<1, 32, 0, s>>>(d, ctx->queue, ctx->scratch);
+    SVDAG_TRY(launch_build_any(ctx, kToolTerrain, s));
     const uint32_t LL = d.leafLevel;
     for (int level = (int)LL; level >= 0; --level) {
         if (level < (int)LL)
@@ -1399,7 +1517,7 @@ svdag_status build_scene_untiled(svdag_ctx* ctx, const DevEditor& ed, cudaStream
         SVDAG_TRY(insert_canonical(ctx, (uint32_t)level, s));
         SVDAG_TRY(launch_insert(ctx, level, level_bound(level), s));
     }
-    k_edit_end<<<1, 32, 0, s>>>(d, ctx->scratch, 1, nullptr);
+    k_edit_end<<<1, 32, 0, s>>>(d, ctx->scratch, ctx->queue);
     SVDAG_CUDA(cudaGetLastError());
     return read_status(ctx, s);
 }
@@ -1418,9 +1536,9 @@ svdag_status launch_scene_tiles(svdag_ctx* ctx, const DevEditor* eds, uint32_t n
             ctx->sceneGrid = 0;
         cudaGetLastError();
     }
-    if (ctx->sceneGrid <= 0) {
+    if (ctx->sceneGrid <= 0 || (ctx->cfg.flags & SVDAG_FLAG_PHASE_KERNELS)) {
         for (uint32_t i = 0; i < n; ++i)
-            SVDAG_TRY(launch_pipeline(ctx, eds[i], s));
+            SVDAG_TRY(launch_pipeline(ctx, eds[i], s, nullptr, false));
         return SVDAG_OK;
     }
     const uint32_t perLaunch = (uint32_t)(ctx->batchBytes / sizeof(DevEditor));

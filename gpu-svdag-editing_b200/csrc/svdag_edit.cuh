@@ -14,6 +14,9 @@ enum : uint32_t { OP_SUBDIVIDE = 0, OP_FILL = 1, OP_EMPTY = 2, OP_KEEP = 3 };
 enum : uint32_t { ST_PARTIAL = 0, ST_FILLED = 1, ST_EMPTY = 2 };
 constexpr uint32_t kToolTerrain = 100; // internal: the procedural scene builder
 constexpr uint32_t kEmptyRep = 0xFFFFFFFEu; // dedup result of an empty SVO item
+constexpr int kNumGraphs = 8; // CUDA graphs of the phase launches: one per tool, the last for the scene builder
+
+struct EditRecord;
 
 struct DevEditor {
     uint32_t tool;
@@ -29,6 +32,7 @@ struct DevEditor {
     uint32_t startLevel; // the edit covers the subtree of the node (startLevel, startPath); 0 = whole DAG
     uint32_t startPath[3];
     uint32_t* tileOut; // scene builder tiles: the subtree's handle goes here instead of the root
+    EditRecord* record; // per-edit record of a batch (or null)
     uint32_t useSavedSource; // copy: read the source from the saved root (move)
     uint32_t saveRoot; // remember the root before this edit as the source of a later copy (move)
     uint32_t builder; // scene build: fully-filled discovery on every level, no undo frame
@@ -38,6 +42,16 @@ struct DevEditor {
 struct EditRecord {
     uint32_t rootBefore, rootAfter, status, pad;
     unsigned long long edited, added, unique, svoItems;
+};
+
+// Editor of the running edit for the one-launch-per-phase form (and its CUDA graphs): the phase
+// kernels read `slot`; with `eds` set, the first phase copies eds[cursor] into the slot and the
+// last one advances the cursor, so one captured graph per tool serves every edit of a batch.
+struct EditQueue {
+    const DevEditor* eds;
+    uint32_t cursor;
+    uint32_t pad;
+    DevEditor slot;
 };
 
 struct WorkItem { // CreateIntermediateWorkItem (create_edit_svo.cu:55-65)

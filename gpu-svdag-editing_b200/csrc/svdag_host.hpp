@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "svdag_device.cuh"
+#include "svdag_edit.cuh"
 
 struct svdag_table {
     svdag_ctx* ctx = nullptr;
@@ -28,12 +29,15 @@ struct svdag_ctx {
     unsigned long long batchBytes = 0;
     int fusedGrid = -1; // co-resident blocks of the persistent edit kernel (0 = unavailable)
     int sceneGrid = -1; // same for the scene tile kernel
+    svdag::EditQueue* queue = nullptr; // editor slot of the one-launch-per-phase form (end of the batch region)
+    cudaGraphExec_t graphs[svdag::kNumGraphs] = {}; // per tool: the phase launches of one edit
     uint32_t lastBatch = 0;
     uint32_t* items = nullptr; // item region
     unsigned long long itemWords = 0;
     svdag_table levelTables[svdag::kMaxLevels];
     std::vector<svdag_table*> standalone;
     uint32_t probeLanes = 8;
+    double bigEditLeaves = 16384; // edits whose SVO may exceed this many leaves run one launch per phase
     uint32_t loadFactor = 16;
     unsigned long long scratchHighWater = 0;
     svdag::DevDag dag() const { return svdag::DevDag { items, itemWords, ctl, cfg.levels, cfg.levels - 2 }; }
@@ -96,7 +100,7 @@ svdag_status launch_scene_tiles(svdag_ctx* ctx, const DevEditor* eds, uint32_t n
 bool valid_edit(const svdag_edit* e);
 int expand_edit(const svdag_ctx* ctx, const svdag_edit& e, DevEditor* out);
 int fused_grid(svdag_ctx* ctx);
-svdag_status launch_fused_at(svdag_ctx* ctx, const DevEditor* eds, uint32_t n, char* region, size_t regionBytes, cudaStream_t s);
+svdag_status launch_edits_at(svdag_ctx* ctx, const DevEditor* eds, uint32_t n, char* region, size_t regionBytes, cudaStream_t s);
 // Procedural scene construction (svdag_scene.cu).
 svdag_status run_scene_build(svdag_ctx* ctx, const svdag_terrain_params* p, cudaStream_t s);
 

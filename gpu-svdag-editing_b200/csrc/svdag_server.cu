@@ -130,7 +130,7 @@ struct svdag_server {
         }
         char* region = ctx->batch + (size_t)f.slot * slotBytes;
         if (!eds.empty()) {
-            SVDAG_TRY(launch_fused_at(ctx, eds.data(), (uint32_t)eds.size(), region, slotBytes, stream));
+            SVDAG_TRY(launch_edits_at(ctx, eds.data(), (uint32_t)eds.size(), region, slotBytes, stream));
             const size_t edBytes = align256(eds.size() * sizeof(DevEditor));
             SVDAG_CUDA(cudaMemcpyAsync(hostRecords[f.slot], region + edBytes, eds.size() * sizeof(EditRecord), cudaMemcpyDeviceToHost,
                 stream));
@@ -282,8 +282,6 @@ svdag_status svdag_server_create(svdag_ctx* ctx, const svdag_server_config* conf
     SVDAG_CUDA(cudaSetDevice(ctx->device));
     SVDAG_TRY(ensure_level_tables(ctx, nullptr));
     SVDAG_CUDA(cudaStreamSynchronize(nullptr));
-    if (fused_grid(ctx) <= 0)
-        return SVDAG_ERR_UNSUPPORTED;
     auto* s = new svdag_server();
     s->ctx = ctx;
     s->cfg = *config;

@@ -305,10 +305,11 @@ class MyGPUHashDAG:
     """One context: one HBM pool, one slab hash table per level, the root and the undo history."""
 
     def __init__(self, levels: int, pool_bytes: int = 1 << 30, scratch_bytes: int = 0, device: int = 0,
-                 load_factor: int = 0, probe_lanes: int = 0, undo_depth: int = 0, phase_kernels: bool = False):
+                 load_factor: int = 0, probe_lanes: int = 0, undo_depth: int = 0, phase_kernels: bool = False,
+                 persistent: bool = False):
         cfg = Config(levels=levels, device=device, pool_bytes=pool_bytes, scratch_bytes=scratch_bytes,
                      target_load_factor=load_factor, probe_lanes=probe_lanes, undo_depth=undo_depth,
-                     flags=1 if phase_kernels else 0)
+                     flags=(1 if phase_kernels else 0) | (2 if persistent else 0))
         h = C.c_void_p()
         _check(lib().svdag_create(C.byref(cfg), C.byref(h)), "svdag_create")
         self.h = h

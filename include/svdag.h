@@ -54,9 +54,12 @@ typedef enum svdag_status {
  * 2 + ceil(4 * popcount(64-bit voxel mask) / 32). Keys are self-describing. */
 typedef enum svdag_item_kind { SVDAG_KIND_NODE = 0, SVDAG_KIND_LEAF = 1 } svdag_item_kind;
 
-/* Run every edit phase as its own kernel launch instead of one persistent cooperative launch per
- * edit or batch (for profiling single phases; slower for small edits). */
+/* Launch every edit phase directly instead of replaying the tool's captured CUDA graph of the phase
+ * launches (for profiling single phases). */
 #define SVDAG_FLAG_PHASE_KERNELS 1u
+/* Run edits whose intermediate SVO is estimated small in one persistent cooperative launch (grid-wide
+ * barriers between phases) instead of the per-tool CUDA graph of the phase launches. */
+#define SVDAG_FLAG_PERSISTENT 2u
 
 typedef struct svdag_config {
     uint32_t levels; /* octree depth, SVDAG_MIN_LEVELS..SVDAG_MAX_LEVELS (1 << levels voxels per axis) */

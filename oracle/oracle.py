@@ -106,6 +106,9 @@ def lib():
         L.oracle_canonicalize_at.argtypes = [P, C.c_uint32, C.c_uint32, C.POINTER(Canon)]
         L.oracle_build_scene_subtree.argtypes = [P, C.POINTER(TerrainParams), C.c_uint32, P, C.POINTER(C.c_uint32)]
         L.oracle_scene_voxels.argtypes = [C.POINTER(TerrainParams), C.c_uint32, P, C.c_uint64, P]
+        L.oracle_build_scene_region.argtypes = [P, C.POINTER(TerrainParams), P, P]
+        L.oracle_node_at.restype = C.c_uint32
+        L.oracle_node_at.argtypes = [P, C.c_uint32, P]
         L.oracle_encode_node_header.restype = C.c_uint32
         L.oracle_encode_node_header.argtypes = [C.c_uint32, C.c_uint32]
         L.oracle_header_child_mask.restype = C.c_uint32
@@ -166,6 +169,20 @@ class OracleDag:
         if r:
             raise RuntimeError(f"oracle_build_scene_subtree -> {r}")
         return h.value
+
+    def build_scene_region(self, params: TerrainParams, lo, hi):
+        """Builds the scene with every voxel outside the box [lo, hi) empty."""
+        a = np.ascontiguousarray(lo, dtype=np.int64)
+        b = np.ascontiguousarray(hi, dtype=np.int64)
+        r = lib().oracle_build_scene_region(self.h, C.byref(params), _ptr(a), _ptr(b))
+        if r:
+            raise RuntimeError(f"oracle_build_scene_region -> {r}")
+
+    def node_at(self, level: int, path):
+        """Handle of node (level, path), or None where the DAG is empty."""
+        p = np.ascontiguousarray(path, dtype=np.uint32)
+        h = lib().oracle_node_at(self.h, level, _ptr(p))
+        return None if h == 0xFFFFFFFF else h
 
     def canon_at(self, level: int, handle: int) -> dict:
         c = Canon()

@@ -954,6 +954,22 @@ struct Scene {
     };
     Terrain t;
     std::vector<Structure> s;
+    bool clipped = false; // restrict the scene to the voxel box [rlo, rhi)
+    int64_t rlo[3] = {}, rhi[3] = {};
+    // 0 = node outside the region, 1 = partly inside, 2 = inside (always 2 without a region)
+    int region(int64_t x0, int64_t y0, int64_t z0, int64_t n) const
+    {
+        if (!clipped)
+            return 2;
+        const int64_t b[3] = { x0, y0, z0 };
+        bool inside = true;
+        for (int a = 0; a < 3; ++a) {
+            if (b[a] + n <= rlo[a] || b[a] >= rhi[a])
+                return 0;
+            inside = inside && b[a] >= rlo[a] && b[a] + n <= rhi[a];
+        }
+        return inside ? 2 : 1;
+    }
 
     static uint64_t splitmix(uint64_t& x)
     {
@@ -1032,11 +1048,14 @@ BuildResult build_terrain_rec(Dag& dag, const Scene& sc, uint32_t level, const P
     const uint32_t depth = dag.levels - level;
     const uint32_t s = 1u << depth;
     const uint32_t x0 = path.x << depth, y0 = path.y << depth, z0 = path.z << depth;
+    const int inRegion = sc.region(x0, y0, z0, s);
+    if (inRegion == 0)
+        return { kSentinel, kSentinel };
     std::vector<uint32_t> active;
     for (uint32_t i : parentActive)
         if (sc.touches(sc.s[i], x0, y0, z0, s))
             active.push_back(i);
-    if (active.empty()) {
+    if (active.empty() && inRegion == 2) {
         uint32_t hlo, hhi;
         t.bounds(x0, z0, s, hlo, hhi);
         if (y0 >= hhi)
@@ -1062,7 +1081,7 @@ BuildResult build_terrain_rec(Dag& dag, const Scene& sc, uint32_t level, const P
             const uint32_t dx = ((c >> 2) & 1u) * 2 + ((f >> 2) & 1u);
             const uint32_t dy = ((c >> 1) & 1u) * 2 + ((f >> 1) & 1u);
             const uint32_t dz = (c & 1u) * 2 + (f & 1u);
-            const uint32_t m = sc.voxel(x0 + dx, y0 + dy, z0 + dz, h[dx][dz], active);
+            const uint32_t m = sc.region(x0 + dx, y0 + dy, z0 + dz, 1) ? sc.voxel(x0 + dx, y0 + dy, z0 + dz, h[dx][dz], active) : kSentinel;
             if (m != kSentinel) {
                 b.set(m);
                 mask |= 1ull << v;
@@ -1509,6 +1528,39 @@ int oracle_build_scene_subtree(oracle_dag* d, const svdag_terrain_params* params
     p.z = path[2];
     *out_handle = build_terrain_rec(d->dag, sc, level, p, all).handle;
     return SVDAG_OK;
+}
+
+int oracle_build_scene_region(oracle_dag* d, const svdag_terrain_params* params, const int64_t lo[3], const int64_t hi[3])
+{
+    if (!d || !params || !lo || !hi || params->octaves == 0 || params->num_materials == 0)
+        return SVDAG_ERR_INVALID;
+    d->dag.init(d->dag.levels);
+    Scene sc(*params, d->dag.levels);
+    sc.clipped = true;
+    for (int a = 0; a < 3; ++a) {
+        sc.rlo[a] = lo[a];
+        sc.rhi[a] = hi[a];
+    }
+    std::vector<uint32_t> all(sc.s.size());
+    for (uint32_t i = 0; i < all.size(); ++i)
+        all[i] = i;
+    d->dag.root = build_terrain_rec(d->dag, sc, 0, Path {}, all).handle;
+    return SVDAG_OK;
+}
+
+uint32_t oracle_node_at(const oracle_dag* d, uint32_t level, const uint32_t path[3])
+{
+    uint32_t h = d->dag.root;
+    for (uint32_t l = 0; l < level && h != kSentinel; ++l) {
+        const uint32_t* n = d->dag.ptr(l, h);
+        const uint32_t sh = level - l - 1;
+        const uint32_t c = (((path[0] >> sh) & 1u) << 2) | (((path[1] >> sh) & 1u) << 1) | ((path[2] >> sh) & 1u);
+        const uint32_t mask = header_child_mask(n[0]);
+        if (!((mask >> c) & 1u))
+            return kSentinel;
+        h = n[1 + child_offset(mask, c)];
+    }
+    return h;
 }
 
 int oracle_scene_voxels(const svdag_terrain_params* params, uint32_t levels, const uint32_t* xyz, uint64_t count, uint32_t* out)

@@ -43,6 +43,11 @@ int oracle_build_box(oracle_dag* dag, float bmin, float bmax, uint32_t material)
  * handle at `level` (0xFFFFFFFF = empty). */
 int oracle_build_scene_subtree(oracle_dag* dag, const svdag_terrain_params* params, uint32_t level, const uint32_t path[3],
     uint32_t* out_handle);
+/* Builds the scene with every voxel outside [lo, hi) left empty (regions of scenes too large for
+ * the oracle; nodes wholly inside the region equal those of the full scene). */
+int oracle_build_scene_region(oracle_dag* dag, const svdag_terrain_params* params, const int64_t lo[3], const int64_t hi[3]);
+/* Handle of the node (level, path), 0xFFFFFFFF where the DAG is empty there. */
+uint32_t oracle_node_at(const oracle_dag* dag, uint32_t level, const uint32_t path[3]);
 /* The scene's voxels straight from its definition (no DAG): material or 0xFFFFFFFF. */
 int oracle_scene_voxels(const svdag_terrain_params* params, uint32_t levels, const uint32_t* xyz, uint64_t count, uint32_t* out);
 
