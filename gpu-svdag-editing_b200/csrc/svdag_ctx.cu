@@ -75,21 +75,25 @@ __global__ void k_gc_sweep(DevDag d, DevTable t, const uint32_t* bits, unsigned 
     for (uint32_t c = 0; c < kNumClasses; ++c) {
         const uint32_t k = c + 2;
         for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < t.numBuckets[c]; b += gridDim.x * blockDim.x) {
-            uint32_t slab = t.bucketBase[c] + b * slab_sectors(k);
+            uint32_t slab = t.bucketBase[c] + b;
             for (uint32_t steps = 0; steps < kMaxChain; ++steps) {
                 uint32_t* h = slab_ptr(d, slab);
+                const uint32_t body = h[6];
                 for (uint32_t s = 0; s < kSlots; ++s) {
-                    const uint32_t shift = 8u * (s / 7u);
-                    const uint32_t tag = (h[s % 7u] >> shift) & 0xFFu;
+                    const uint32_t tag = header_tag(h, s);
                     if (tag == 0 || tag == kTagBusy)
                         continue;
-                    const uint32_t item = slot_handle(slab, s, k);
+                    const uint32_t item = slot_handle(body, s, k);
                     if ((bits[item >> 5] >> (item & 31u)) & 1u)
                         continue;
+                    if (!handle_ok(d, item)) {
+                        set_status(d.ctl, SVDAG_ERR_CORRUPT);
+                        continue;
+                    }
                     uint32_t* ip = handle_ptr(d, item);
                     for (uint32_t j = 0; j < k; ++j)
                         ip[j] = 0;
-                    h[s % 7u] &= ~(0xFFu << shift);
+                    h[s >> 2] &= ~(0xFFu << (8u * (s & 3u)));
                     ++nfreed;
                 }
                 if (h[7] == kEnd)
@@ -162,7 +166,7 @@ svdag_status svdag_create(const svdag_config* cfg, svdag_ctx** out)
         return SVDAG_ERR_NO_DEVICE; // built for sm_100a only
     SVDAG_CUDA(cudaSetDevice(cfg->device));
     const unsigned long long pool = cfg->pool_bytes ? cfg->pool_bytes : (1ull << 30);
-    const unsigned long long scratch = cfg->scratch_bytes ? cfg->scratch_bytes : pool / 4;
+    const unsigned long long scratch = (cfg->scratch_bytes ? cfg->scratch_bytes : pool / 4) & ~255ull;
     if (scratch + kCtlBytes + kBatchBytes + (1ull << 20) > pool)
         return SVDAG_ERR_INVALID;
     auto* ctx = new (std::nothrow) svdag_ctx();
@@ -186,12 +190,18 @@ svdag_status svdag_create(const svdag_config* cfg, svdag_ctx** out)
     static_assert(sizeof(EditQueue) <= 4096, "editor queue too large");
     ctx->scratch = ctx->pool + kCtlBytes + kBatchBytes;
     ctx->scratchBytes = scratch;
-    ctx->items = reinterpret_cast<uint32_t*>(ctx->pool + kCtlBytes + kBatchBytes + scratch);
-    ctx->itemWords = std::min<unsigned long long>((pool - kCtlBytes - kBatchBytes - scratch) / 4 - 64, kMaxItemWords) & ~7ull;
+    // The rest: slab headers (a ninth: 32 bytes per slab of 24 items of 2..10 words) then items.
+    const unsigned long long rest = pool - kCtlBytes - kBatchBytes - scratch;
+    const unsigned long long headerBytes = align256(rest / 9);
+    ctx->headers = reinterpret_cast<uint32_t*>(ctx->pool + kCtlBytes + kBatchBytes + scratch);
+    ctx->headerCount = std::min<unsigned long long>(headerBytes / 32, 0xFFFFFFF0ull);
+    ctx->items = reinterpret_cast<uint32_t*>(ctx->pool + kCtlBytes + kBatchBytes + scratch + headerBytes);
+    ctx->itemWords = std::min<unsigned long long>((rest - headerBytes) / 4 - 64, kMaxItemWords) & ~7ull;
     static_assert(sizeof(Control) <= kCtlBytes, "control block too large");
     cudaError_t e = cudaMemset(ctx->pool, 0, pool);
     if (e == cudaSuccess) {
         Control init {};
+        init.headerTop = 1;
         init.root = kNone;
         init.undoDepth = ctx->cfg.undo_depth;
         init.savedRoot = kNone;
@@ -294,8 +304,8 @@ svdag_status svdag_get_stats(svdag_ctx* ctx, svdag_stats* out, void* stream)
     out->levels = ctx->cfg.levels;
     out->root = c.root;
     out->pool_bytes = ctx->poolBytes;
-    out->item_region_bytes = ctx->itemWords * 4;
-    out->item_region_used_bytes = c.itemTop * 4;
+    out->item_region_bytes = ctx->itemWords * 4 + ctx->headerCount * 32;
+    out->item_region_used_bytes = c.itemTop * 4 + c.headerTop * 32;
     out->scratch_bytes = ctx->scratchBytes;
     out->scratch_high_water_bytes = ctx->scratchHighWater;
     out->undo_count = c.undoCount;

@@ -8,16 +8,18 @@
 //
 // Hash tables: one table per DAG level. A level table holds keys of 2..10 words; keys of one length
 // share a slab family (the "size class"), so slots have a fixed stride and the slot index gives the
-// item address. A slab of class k:
-//   words 0..6  : 28 one-byte tags, slot s at word (s % 7), byte (s / 7); 0 = free, 0xFF = being written
-//   word  7     : slab id of the next slab in the bucket's chain, 0 = end of chain (slab 0 is always
-//                 a bucket array, never an overflow slab)
-//   words 8..   : 28 items of k words at a stride of k rounded up to even (item s at 8 + s*stride)
-// The 8 header words are one 32-byte sector, so a probe costs one sector per slab plus the candidate
-// item; the reference's header is 10 words (8 hash words + next + active mask) spanning two sectors
-// (compact_acceleration_hash_table.h:519-541). The first slab of each bucket sits in the bucket
-// array (HASH_TABLE_STORE_SLABS_IN_TABLE, gpu_hash_table_base.h:30-49); overflow slabs come from a
-// bump allocator over the same item region and are linked at the tail of the chain.
+// item address. A slab is a 32-byte header in the header region plus a body of 24 items in the item
+// region:
+//   header words 0..5 : 24 one-byte tags, slot s at word s / 4, byte s % 4; 0 = free, 0xFF = being written
+//   header word 6     : handle of the body (item of slot 0)
+//   header word 7     : header id of the next slab in the bucket's chain, 0 = end (header 0 is unused)
+//   body              : 24 items of k words at a stride of k rounded up to even (slot s at body + s*stride)
+// A probe reads one 32-byte header sector per slab plus the candidate item. Headers are dense (a
+// table's headers are about a tenth of its bytes), so the headers a lookup stream touches stay in
+// the 126 MB L2 while the items it compares are read once; the reference interleaves a 10-word
+// header with each slab's items (compact_acceleration_hash_table.h:519-541). The first slab of each
+// bucket is allocated with the table (HASH_TABLE_STORE_SLABS_IN_TABLE, gpu_hash_table_base.h:30-49);
+// overflow slabs come from bump allocators over the two regions and are linked at the chain's tail.
 #pragma once
 #include <cstdint>
 
@@ -29,7 +31,7 @@ constexpr uint32_t kNone = 0xFFFFFFFFu; // empty child / missing handle
 constexpr uint32_t kEnd = 0u; // end of a slab chain
 constexpr uint32_t kFillMarker = 0xFFFFFF00u; // SVO child "canonical fully-filled node of material m" = kFillMarker | m
 constexpr unsigned long long kMaxItemWords = 2ull * 0xFFFFFF00ull - 64; // item region limit (just under 32 GiB)
-constexpr uint32_t kSlots = 28;
+constexpr uint32_t kSlots = 24;
 constexpr uint32_t kHeaderWords = 8;
 constexpr uint32_t kTagBusy = 0xFFu;
 constexpr uint32_t kMaxLevels = SVDAG_MAX_LEVELS;
@@ -37,19 +39,17 @@ constexpr uint32_t kItemStride = 10; // padded stride of items in scratch arrays
 constexpr uint32_t kNumClasses = 9; // item sizes 2..10
 
 __host__ __device__ constexpr uint32_t item_stride(uint32_t k) { return (k + 1u) & ~1u; } // words, even
-__host__ __device__ constexpr uint32_t slab_words(uint32_t k) { return ((kHeaderWords + kSlots * item_stride(k)) + 7u) & ~7u; }
-__host__ __device__ constexpr uint32_t slab_sectors(uint32_t k) { return slab_words(k) >> 3; }
-// Handle of slot s of the slab with id `slab` for items of k words.
-__host__ __device__ constexpr uint32_t slot_handle(uint32_t slab, uint32_t s, uint32_t k)
-{
-    return (slab << 2) + 4u + s * (item_stride(k) >> 1);
-}
+__host__ __device__ constexpr uint32_t body_words(uint32_t k) { return kSlots * item_stride(k); } // a multiple of 8
+// Handle of slot s of the slab whose body starts at handle `body`, for items of k words.
+__host__ __device__ constexpr uint32_t slot_handle(uint32_t body, uint32_t s, uint32_t k) { return body + s * (item_stride(k) >> 1); }
+__host__ __device__ inline uint32_t header_tag(const uint32_t* h, uint32_t s) { return (h[s >> 2] >> (8u * (s & 3u))) & 0xFFu; }
 
 // Per-table descriptor, passed by value to kernels.
 struct DevTable {
     uint32_t kind; // svdag_item_kind
     uint32_t numBuckets[kNumClasses];
-    uint32_t bucketBase[kNumClasses]; // slab id of bucket 0
+    uint32_t bucketBase[kNumClasses]; // header id of bucket 0
+    uint32_t bodyBase[kNumClasses]; // body handle of bucket 0 (bucket b's body follows at b * body size)
 };
 
 // Device control block (lives at the start of the scratch side of the pool).
@@ -72,6 +72,7 @@ struct EditCounters {
 
 struct Control {
     unsigned long long itemTop; // bump pointer of the item region, in words
+    unsigned long long headerTop; // bump pointer of the header region, in headers (0 is never used)
     uint32_t status; // latched svdag_status
     uint32_t root; // current root handle (kNone = empty DAG)
     uint32_t undo[64];
@@ -90,6 +91,8 @@ struct Control {
 struct DevDag {
     uint32_t* items;
     unsigned long long itemWords; // capacity of the item region
+    uint32_t* headers; // slab headers, 8 words each
+    unsigned long long headerCount; // capacity of the header region
     Control* ctl;
     uint32_t levels;
     uint32_t leafLevel;
@@ -117,11 +120,8 @@ __device__ __forceinline__ const uint32_t* item_ptr(const DevDag& d, uint32_t h)
     set_status(d.ctl, SVDAG_ERR_CORRUPT);
     return kZeroItem;
 }
-__device__ __forceinline__ bool slab_ok(const DevDag& d, uint32_t slab)
-{
-    return 8ull * slab + 8ull <= d.itemWords;
-}
-__device__ __forceinline__ uint32_t* slab_ptr(const DevDag& d, uint32_t slab) { return d.items + 8ull * slab; }
+__device__ __forceinline__ bool slab_ok(const DevDag& d, uint32_t slab) { return slab != 0 && slab < d.headerCount; }
+__device__ __forceinline__ uint32_t* slab_ptr(const DevDag& d, uint32_t slab) { return d.headers + 8ull * slab; }
 __device__ __forceinline__ uint32_t* handle_ptr(const DevDag& d, uint32_t h) { return d.items + 2ull * h; }
 
 // ---------------------------------------------------------------- hashing (ours; the bucket
@@ -281,58 +281,58 @@ __device__ __forceinline__ void hash_words(const uint32_t* w, uint32_t n, uint32
     hb = b;
 }
 
-// Loads the 8 header words of a slab; each lane ends up with the words it owns.
-// Returns the candidate mask of slots whose tag byte equals `tag` (28 bits) and the next pointer.
+// Loads the 8 header words of a slab. Returns the candidate mask of slots whose tag byte equals
+// `tag` (24 bits), with the body handle, the next header id and the mask of free slots.
 template <int G, bool CG = false>
-__device__ __forceinline__ uint32_t probe_header(const Grp<G>& g, const uint32_t* slab, uint32_t tag, uint32_t& next,
+__device__ __forceinline__ uint32_t probe_header(const Grp<G>& g, const uint32_t* hdr, uint32_t tag, uint32_t& next, uint32_t& body,
     uint32_t& emptyMask)
 {
     const uint32_t tag4 = tag * 0x01010101u;
     uint32_t cand = 0, empty = 0;
+    auto bytes = [](uint32_t v) { return ((v >> 7) & 1u) | ((v >> 14) & 2u) | ((v >> 21) & 4u) | ((v >> 28) & 8u); };
     auto account = [&](uint32_t word, uint32_t x) {
-        if (word < 7) {
-            const uint32_t eq = __vcmpeq4(x, tag4);
-            const uint32_t ez = __vcmpeq4(x, 0u);
-#pragma unroll
-            for (uint32_t b = 0; b < 4; ++b) {
-                cand |= ((eq >> (8 * b)) & 1u) << (word + 7 * b);
-                empty |= ((ez >> (8 * b)) & 1u) << (word + 7 * b);
-            }
+        if (word < 6) {
+            cand |= bytes(__vcmpeq4(x, tag4)) << (4 * word);
+            empty |= bytes(__vcmpeq4(x, 0u)) << (4 * word);
         }
     };
-    uint32_t nx = 0;
+    uint32_t nx = 0, bd = 0;
     if constexpr (G == 1) {
-        const uint4 a = CG ? __ldcg(reinterpret_cast<const uint4*>(slab)) : reinterpret_cast<const uint4*>(slab)[0];
-        const uint4 b = CG ? __ldcg(reinterpret_cast<const uint4*>(slab) + 1) : reinterpret_cast<const uint4*>(slab)[1];
+        const uint4 a = CG ? __ldcg(reinterpret_cast<const uint4*>(hdr)) : reinterpret_cast<const uint4*>(hdr)[0];
+        const uint4 b = CG ? __ldcg(reinterpret_cast<const uint4*>(hdr) + 1) : reinterpret_cast<const uint4*>(hdr)[1];
         account(0, a.x);
         account(1, a.y);
         account(2, a.z);
         account(3, a.w);
         account(4, b.x);
         account(5, b.y);
-        account(6, b.z);
+        bd = b.z;
         nx = b.w;
     } else if constexpr (G == 2) {
-        const uint4 a = CG ? __ldcg(reinterpret_cast<const uint4*>(slab) + g.lane) : reinterpret_cast<const uint4*>(slab)[g.lane];
+        const uint4 a = CG ? __ldcg(reinterpret_cast<const uint4*>(hdr) + g.lane) : reinterpret_cast<const uint4*>(hdr)[g.lane];
         account(4 * g.lane + 0, a.x);
         account(4 * g.lane + 1, a.y);
         account(4 * g.lane + 2, a.z);
         account(4 * g.lane + 3, a.w);
+        bd = g.bcast(a.z, 1);
         nx = g.bcast(a.w, 1);
     } else if constexpr (G == 4) {
-        const uint2 a = CG ? __ldcg(reinterpret_cast<const uint2*>(slab) + g.lane) : reinterpret_cast<const uint2*>(slab)[g.lane];
+        const uint2 a = CG ? __ldcg(reinterpret_cast<const uint2*>(hdr) + g.lane) : reinterpret_cast<const uint2*>(hdr)[g.lane];
         account(2 * g.lane + 0, a.x);
         account(2 * g.lane + 1, a.y);
+        bd = g.bcast(a.x, 3);
         nx = g.bcast(a.y, 3);
     } else {
         uint32_t x = 0;
         if (g.lane < 8)
-            x = CG ? __ldcg(slab + g.lane) : slab[g.lane];
+            x = CG ? __ldcg(hdr + g.lane) : hdr[g.lane];
         if (g.lane < 8)
             account(g.lane, x);
+        bd = g.bcast(x, 6);
         nx = g.bcast(x, 7);
     }
     next = nx;
+    body = bd;
     emptyMask = g.reduce_or(empty);
     return g.reduce_or(cand);
 }
@@ -364,33 +364,43 @@ __device__ __forceinline__ void write_item(const Grp<G>& g, uint32_t* item, cons
 
 __device__ __forceinline__ uint32_t first_slab(const DevTable& t, uint32_t cls, uint32_t ha)
 {
-    return t.bucketBase[cls] + bucket_of(ha, t.numBuckets[cls]) * slab_sectors(cls + 2u);
+    return t.bucketBase[cls] + bucket_of(ha, t.numBuckets[cls]);
 }
 
-// Allocates and initialises an overflow slab of class k; returns kNone when the region is full.
+// Allocates and initialises an overflow slab of class k (a header and a cleared body); returns its
+// header id, or kNone when a region is full.
 template <int G>
 __device__ __forceinline__ uint32_t alloc_slab(const Grp<G>& g, const DevDag& d, uint32_t k)
 {
-    uint32_t off = kNone;
+    uint32_t id = kNone, body = 0;
     if (g.lane == 0) {
-        const unsigned long long w = slab_words(k);
+        const unsigned long long hid = atomicAdd(&d.ctl->headerTop, 1ull);
+        const unsigned long long w = body_words(k);
         const unsigned long long o = atomicAdd(&d.ctl->itemTop, w);
-        if (o + w <= d.itemWords)
-            off = (uint32_t)(o >> 3); // itemTop stays a multiple of 8 words
-        else
+        if (hid < d.headerCount && o + w <= d.itemWords) {
+            id = (uint32_t)hid;
+            body = (uint32_t)(o >> 1); // itemTop stays a multiple of 8 words
+        } else {
             set_status(d.ctl, SVDAG_ERR_OOM);
+        }
     }
-    off = g.bcast(off, 0);
-    if (off != kNone) {
-        // Free slots keep zero words (a valid key is never all zero), so the whole slab is cleared.
-        const uint32_t sw = slab_words(k);
-        uint32_t* p = slab_ptr(d, off);
-        for (uint32_t i = g.lane * 4; i < sw; i += G * 4)
+    id = g.bcast(id, 0);
+    body = g.bcast(body, 0);
+    if (id != kNone) {
+        // Free slots keep zero words (a valid key is never all zero), so the whole body is cleared.
+        const uint32_t bw = body_words(k);
+        uint32_t* p = handle_ptr(d, body);
+        for (uint32_t i = g.lane * 4; i < bw; i += G * 4)
             *reinterpret_cast<uint4*>(p + i) = make_uint4(0, 0, 0, 0);
+        if (g.lane == 0) {
+            uint32_t* h = slab_ptr(d, id);
+            reinterpret_cast<uint4*>(h)[0] = make_uint4(0, 0, 0, 0);
+            reinterpret_cast<uint4*>(h)[1] = make_uint4(0, 0, body, kEnd);
+        }
         __threadfence();
         g.sync();
     }
-    return off;
+    return id;
 }
 
 // Links `fresh` behind `slab`; returns the slab that follows `slab` afterwards (ours or a racer's).
@@ -424,12 +434,12 @@ __device__ __forceinline__ uint32_t table_find(const Grp<G>& g, const DevDag& d,
             set_status(d.ctl, SVDAG_ERR_CORRUPT);
             return kNone;
         }
-        uint32_t next, empty;
-        uint32_t cand = probe_header<G>(g, slab_ptr(d, slab), tag, next, empty);
+        uint32_t next, body, empty;
+        uint32_t cand = probe_header<G>(g, slab_ptr(d, slab), tag, next, body, empty);
         while (cand) {
             const uint32_t s = __ffs(cand) - 1u;
             cand &= cand - 1u;
-            const uint32_t item = slot_handle(slab, s, key.n);
+            const uint32_t item = slot_handle(body, s, key.n);
             if (item_equals<G, LD_STREAM>(g, handle_ptr(d, item), key))
                 return item;
         }
@@ -446,12 +456,12 @@ __device__ __forceinline__ uint32_t table_find(const Grp<G>& g, const DevDag& d,
 // Claims a free slot of `slab` for the key; returns the item offset or kNone when the slab is full.
 // `busy` claims with the in-flight tag (published later), otherwise with the final tag.
 template <int G>
-__device__ __forceinline__ uint32_t claim_in_slab(const Grp<G>& g, const DevDag& d, uint32_t slab, uint32_t emptyMask,
-    uint32_t tag, uint32_t n, bool busy)
+__device__ __forceinline__ uint32_t claim_in_slab(const Grp<G>& g, const DevDag& d, uint32_t slab, uint32_t body, uint32_t emptyMask,
+    uint32_t tag, uint32_t n, bool busy, uint32_t& slot)
 {
     while (emptyMask) {
         const uint32_t s = __ffs(emptyMask) - 1u;
-        const uint32_t word = s % 7u, shift = 8u * (s / 7u);
+        const uint32_t word = s >> 2, shift = 8u * (s & 3u);
         uint32_t got = 0;
         if (g.lane == 0) {
             uint32_t* p = slab_ptr(d, slab) + word;
@@ -469,8 +479,10 @@ __device__ __forceinline__ uint32_t claim_in_slab(const Grp<G>& g, const DevDag&
             }
         }
         got = g.bcast(got, 0);
-        if (got)
-            return slot_handle(slab, s, n);
+        if (got) {
+            slot = s;
+            return slot_handle(body, s, n);
+        }
         emptyMask &= emptyMask - 1u;
     }
     return kNone;
@@ -489,9 +501,9 @@ __device__ __forceinline__ uint32_t table_add(const Grp<G>& g, const DevDag& d, 
     const uint32_t tag = tag_of(key.hb);
     uint32_t slab = first_slab(t, cls, key.ha);
     for (uint32_t steps = 0; steps < kMaxChain; ++steps) {
-        uint32_t next, empty;
-        probe_header<G>(g, slab_ptr(d, slab), tag, next, empty);
-        const uint32_t item = claim_in_slab<G>(g, d, slab, empty, tag, key.n, false);
+        uint32_t next, body, empty, slot;
+        probe_header<G>(g, slab_ptr(d, slab), tag, next, body, empty);
+        const uint32_t item = claim_in_slab<G>(g, d, slab, body, empty, tag, key.n, false, slot);
         if (item != kNone) {
             write_item<G>(g, handle_ptr(d, item), key);
             return item;
@@ -536,23 +548,24 @@ __device__ __forceinline__ uint32_t table_find_or_insert(const Grp<G>& g, const 
     }
     const uint32_t tag = tag_of(key.hb);
     uint32_t slab = first_slab(t, cls, key.ha);
-    uint32_t tail = slab, tailEmpty = 0;
+    uint32_t tail = slab, tailEmpty = 0, tailBody = 0;
     for (uint32_t steps = 0;; ++steps) {
         if (steps >= kMaxChain) {
             set_status(d.ctl, SVDAG_ERR_CORRUPT);
             return kNone;
         }
-        uint32_t next, empty;
-        uint32_t cand = probe_header<G, true>(g, slab_ptr(d, slab), tag, next, empty);
+        uint32_t next, body, empty;
+        uint32_t cand = probe_header<G, true>(g, slab_ptr(d, slab), tag, next, body, empty);
         while (cand) {
             const uint32_t s = __ffs(cand) - 1u;
             cand &= cand - 1u;
-            const uint32_t item = slot_handle(slab, s, key.n);
+            const uint32_t item = slot_handle(body, s, key.n);
             if (item_equals<G, LD_L2>(g, handle_ptr(d, item), key))
                 return item;
         }
         tail = slab;
         tailEmpty = empty;
+        tailBody = body;
         if (next == kEnd)
             break;
         if (!slab_ok(d, next)) {
@@ -563,22 +576,21 @@ __device__ __forceinline__ uint32_t table_find_or_insert(const Grp<G>& g, const 
     }
     // Not present: claim a slot at the tail of the chain (earlier slabs were full or hold other keys).
     slab = tail;
-    uint32_t empty = tailEmpty;
+    uint32_t empty = tailEmpty, body = tailBody;
     for (uint32_t steps = 0; steps < kMaxChain; ++steps) {
-        const uint32_t item = claim_in_slab<G>(g, d, slab, empty, tag, key.n, true);
+        uint32_t s = 0;
+        const uint32_t item = claim_in_slab<G>(g, d, slab, body, empty, tag, key.n, true, s);
         if (item != kNone) {
             write_item<G>(g, handle_ptr(d, item), key);
             __threadfence();
             g.sync();
-            if (g.lane == 0) {
-                const uint32_t s = (item - (slab << 2) - 4u) / (item_stride(key.n) >> 1);
-                atomicXor(slab_ptr(d, slab) + s % 7u, (kTagBusy ^ tag) << (8u * (s / 7u)));
-            }
+            if (g.lane == 0)
+                atomicXor(slab_ptr(d, slab) + (s >> 2), (kTagBusy ^ tag) << (8u * (s & 3u)));
             inserted = true;
             return item;
         }
         uint32_t next;
-        probe_header<G, true>(g, slab_ptr(d, slab), tag, next, empty);
+        probe_header<G, true>(g, slab_ptr(d, slab), tag, next, body, empty);
         if (empty)
             continue; // a slot was freed up meanwhile (cannot happen during edits, kept for safety)
         if (next == kEnd) {
@@ -601,7 +613,7 @@ __device__ __forceinline__ uint32_t table_find_or_insert(const Grp<G>& g, const 
             return kNone;
         }
         slab = next;
-        probe_header<G, true>(g, slab_ptr(d, slab), tag, next, empty);
+        probe_header<G, true>(g, slab_ptr(d, slab), tag, next, body, empty);
     }
     set_status(d.ctl, SVDAG_ERR_TIMEOUT);
     return kNone;

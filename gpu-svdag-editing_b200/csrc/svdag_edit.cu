@@ -1465,6 +1465,7 @@ svdag_status reset_dag(svdag_ctx* ctx, cudaStream_t s)
 {
     reset_level_tables(ctx);
     Control init {};
+    init.headerTop = 1;
     init.root = kNone;
     init.undoDepth = ctx->cfg.undo_depth ? std::min<uint32_t>(ctx->cfg.undo_depth, 64) : 32;
     for (auto& lv : init.fullyFilled)

@@ -34,13 +34,15 @@ struct svdag_ctx {
     uint32_t lastBatch = 0;
     uint32_t* items = nullptr; // item region
     unsigned long long itemWords = 0;
+    uint32_t* headers = nullptr; // slab header region
+    unsigned long long headerCount = 0;
     svdag_table levelTables[svdag::kMaxLevels];
     std::vector<svdag_table*> standalone;
     uint32_t probeLanes = 8;
     double bigEditLeaves = 16384; // edits whose SVO may exceed this many leaves run one launch per phase
     uint32_t loadFactor = 16;
     unsigned long long scratchHighWater = 0;
-    svdag::DevDag dag() const { return svdag::DevDag { items, itemWords, ctl, cfg.levels, cfg.levels - 2 }; }
+    svdag::DevDag dag() const { return svdag::DevDag { items, itemWords, headers, headerCount, ctl, cfg.levels, cfg.levels - 2 }; }
 };
 
 namespace svdag {

@@ -38,30 +38,49 @@ svdag_status read_status(svdag_ctx* ctx, cudaStream_t s)
     return (svdag_status)st;
 }
 
-// Reserves the bucket arrays of a table at the top of the item region and clears them.
+// Writes the body handle of every bucket header of a table (the rest of each header is cleared).
+__global__ void k_init_bucket_headers(DevDag d, DevTable t)
+{
+    for (uint32_t c = 0; c < kNumClasses; ++c) {
+        const uint32_t units = body_words(c + 2) >> 1;
+        for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < t.numBuckets[c]; b += gridDim.x * blockDim.x) {
+            uint4* h = reinterpret_cast<uint4*>(slab_ptr(d, t.bucketBase[c] + b));
+            h[0] = make_uint4(0, 0, 0, 0);
+            h[1] = make_uint4(0, 0, t.bodyBase[c] + b * units, kEnd);
+        }
+    }
+}
+
+// Reserves a table's bucket headers at the top of the header region and its first slab bodies at the
+// top of the item region, clears them and links each header to its body.
 svdag_status alloc_table(svdag_ctx* ctx, svdag_table* t, uint32_t kind, const uint32_t* bucketsPerClass, cudaStream_t s)
 {
-    unsigned long long top = 0;
-    SVDAG_CUDA(cudaMemcpyAsync(&top, &ctx->ctl->itemTop, sizeof(top), cudaMemcpyDeviceToHost, s));
+    unsigned long long tops[2] = { 0, 0 }; // itemTop (words), headerTop (headers)
+    SVDAG_CUDA(cudaMemcpyAsync(tops, &ctx->ctl->itemTop, sizeof(tops), cudaMemcpyDeviceToHost, s));
     SVDAG_CUDA(cudaStreamSynchronize(s));
     DevTable dev {};
     dev.kind = kind;
-    unsigned long long words = 0;
+    unsigned long long words = 0, headers = 0, buckets = 0;
     for (uint32_t c = 0; c < kNumClasses; ++c) {
         dev.numBuckets[c] = bucketsPerClass[c];
-        dev.bucketBase[c] = (uint32_t)((top + words) >> 3); // slab id (top and slab sizes are multiples of 8 words)
-        words += (unsigned long long)bucketsPerClass[c] * slab_words(c + 2);
+        dev.bucketBase[c] = (uint32_t)(tops[1] + headers);
+        dev.bodyBase[c] = (uint32_t)((tops[0] + words) >> 1); // tops[0] and body sizes are multiples of 8 words
+        words += (unsigned long long)bucketsPerClass[c] * body_words(c + 2);
+        headers += bucketsPerClass[c];
+        buckets = std::max<unsigned long long>(buckets, bucketsPerClass[c]);
     }
-    if (top + words > ctx->itemWords)
+    if (tops[0] + words > ctx->itemWords || tops[1] + headers > ctx->headerCount)
         return SVDAG_ERR_OOM;
-    SVDAG_CUDA(cudaMemsetAsync(ctx->items + top, 0, words * 4, s));
-    const unsigned long long newTop = top + words;
-    SVDAG_CUDA(cudaMemcpyAsync(&ctx->ctl->itemTop, &newTop, sizeof(newTop), cudaMemcpyHostToDevice, s));
+    SVDAG_CUDA(cudaMemsetAsync(ctx->items + tops[0], 0, words * 4, s));
+    k_init_bucket_headers<<<grid_for(ctx, buckets, 256), 256, 0, s>>>(ctx->dag(), dev);
+    SVDAG_CUDA(cudaGetLastError());
+    const unsigned long long newTops[2] = { tops[0] + words, tops[1] + headers };
+    SVDAG_CUDA(cudaMemcpyAsync(&ctx->ctl->itemTop, newTops, sizeof(newTops), cudaMemcpyHostToDevice, s));
     SVDAG_CUDA(cudaStreamSynchronize(s));
     t->ctx = ctx;
     t->dev = dev;
     t->ready = true;
-    t->words = words;
+    t->words = words + headers * kHeaderWords;
     return SVDAG_OK;
 }
 
@@ -265,19 +284,19 @@ __global__ void k_table_walk(DevDag d, DevTable t, unsigned long long* counters,
         const uint32_t k = c + 2;
         const uint32_t nb = t.numBuckets[c];
         for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
-            uint32_t slab = t.bucketBase[c] + b * slab_sectors(k);
+            uint32_t slab = t.bucketBase[c] + b;
             unsigned long long items = 0, slabs = 0;
             for (uint32_t steps = 0; steps < kMaxChain; ++steps) {
                 const uint32_t* h = slab_ptr(d, slab);
                 for (uint32_t s = 0; s < kSlots; ++s) {
-                    const uint32_t tag = (h[s % 7u] >> (8u * (s / 7u))) & 0xFFu;
+                    const uint32_t tag = header_tag(h, s);
                     if (tag == 0 || tag == kTagBusy)
                         continue;
                     ++items;
                     if (outHandles) {
                         const unsigned long long pos = atomicAdd(&counters[2], 1ull);
                         if (pos < capacity) {
-                            const uint32_t item = slot_handle(slab, s, k);
+                            const uint32_t item = slot_handle(h[6], s, k);
                             outHandles[pos] = item;
                             const uint32_t* ip = handle_ptr(d, item);
                             for (uint32_t j = 0; j < kItemStride; ++j)
@@ -534,7 +553,7 @@ svdag_status svdag_table_get_stats(svdag_table* t, svdag_table_stats* out, void*
     unsigned long long buckets = 0, bytes = 0;
     for (uint32_t c = 0; c < kNumClasses; ++c) {
         buckets += t->dev.numBuckets[c];
-        bytes += (unsigned long long)t->dev.numBuckets[c] * slab_words(c + 2) * 4;
+        bytes += (unsigned long long)t->dev.numBuckets[c] * (body_words(c + 2) + kHeaderWords) * 4;
     }
     // Overflow slabs are counted per class by the walk only in total; bytes use the mean class size.
     out->buckets = buckets;
@@ -589,14 +608,13 @@ namespace {
 __global__ void k_table_class_counts(DevDag d, DevTable t, unsigned long long* perClass)
 {
     for (uint32_t c = 0; c < kNumClasses; ++c) {
-        const uint32_t k = c + 2;
         unsigned long long items = 0;
         for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < t.numBuckets[c]; b += gridDim.x * blockDim.x) {
-            uint32_t slab = t.bucketBase[c] + b * slab_sectors(k);
+            uint32_t slab = t.bucketBase[c] + b;
             for (uint32_t steps = 0; steps < kMaxChain; ++steps) {
                 const uint32_t* h = slab_ptr(d, slab);
                 for (uint32_t s = 0; s < kSlots; ++s) {
-                    const uint32_t tag = (h[s % 7u] >> (8u * (s / 7u))) & 0xFFu;
+                    const uint32_t tag = header_tag(h, s);
                     items += (tag != 0 && tag != kTagBusy) ? 1u : 0u;
                 }
                 const uint32_t next = h[7];

@@ -307,7 +307,7 @@ typedef struct svdag_stats {
     uint32_t levels;
     uint32_t root;
     uint64_t pool_bytes;
-    uint64_t item_region_bytes;
+    uint64_t item_region_bytes; /* items and slab headers */
     uint64_t item_region_used_bytes;
     uint64_t scratch_bytes;
     uint64_t scratch_high_water_bytes;
