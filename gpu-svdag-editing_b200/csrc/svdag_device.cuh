@@ -136,14 +136,15 @@ __host__ __device__ __forceinline__ uint32_t fmix32(uint32_t h)
     h ^= h >> 16;
     return h;
 }
-__host__ __device__ __forceinline__ uint32_t word_hash_a(uint32_t w, uint32_t i)
+// Per-word term of the key hash: an odd multiply of the word offset by a position constant (a
+// bijection of the word; the terms of a key are combined by XOR, so lanes that hold different words
+// of one key can combine theirs). The finalisers below turn the sum into the bucket and tag hashes.
+__host__ __device__ __forceinline__ uint32_t word_term(uint32_t w, uint32_t i)
 {
-    return fmix32(w ^ (i * 0x9E3779B9u + 0x7F4A7C15u));
+    return (w ^ (i * 0x9E3779B9u + 0x7F4A7C15u)) * (0x85EBCA6Bu + 2u * i);
 }
-__host__ __device__ __forceinline__ uint32_t word_hash_b(uint32_t w, uint32_t i)
-{
-    return fmix32(w + (i * 0x85EBCA6Bu + 0x165667B1u));
-}
+__host__ __device__ __forceinline__ uint32_t bucket_hash(uint32_t acc) { return fmix32(acc); }
+__host__ __device__ __forceinline__ uint32_t tag_hash(uint32_t acc) { return fmix32(acc ^ 0x5BD1E995u); }
 __host__ __device__ __forceinline__ uint32_t tag_of(uint32_t hb)
 {
     uint32_t t = hb >> 24;
@@ -249,7 +250,7 @@ __device__ __forceinline__ void load_key(const Grp<G>& g, const uint32_t* p, uns
         w1 = g.bcast(v, 1);
     }
     key.n = kind == SVDAG_KIND_NODE ? dev_node_words(w0) : dev_leaf_words(w0, w1);
-    uint32_t a = 0, b = 0;
+    uint32_t a = 0;
 #pragma unroll
     for (int i = 0; i < Grp<G>::KW; ++i) {
         const uint32_t idx = g.lane + uint32_t(i) * G;
@@ -257,28 +258,24 @@ __device__ __forceinline__ void load_key(const Grp<G>& g, const uint32_t* p, uns
         if (idx < key.n && idx < limit)
             v = (G == 1 && idx < 2) ? (idx == 0 ? w0 : w1) : ld<MODE>(p + idx);
         key.w[i] = v;
-        if (idx < key.n) {
-            a ^= word_hash_a(v, idx);
-            b ^= word_hash_b(v, idx);
-        }
+        if (idx < key.n)
+            a ^= word_term(v, idx);
     }
-    key.ha = g.reduce_xor(a);
-    key.hb = g.reduce_xor(b);
+    a = g.reduce_xor(a);
+    key.ha = bucket_hash(a);
+    key.hb = tag_hash(a);
 }
 
 // Sets up a key already held in registers of a single thread (G == 1 paths of the pipeline).
 __device__ __forceinline__ void hash_words(const uint32_t* w, uint32_t n, uint32_t& ha, uint32_t& hb)
 {
-    uint32_t a = 0, b = 0;
+    uint32_t a = 0;
 #pragma unroll
-    for (uint32_t i = 0; i < kItemStride; ++i) { // fixed trip count keeps w[] in registers
-        if (i < n) {
-            a ^= word_hash_a(w[i], i);
-            b ^= word_hash_b(w[i], i);
-        }
-    }
-    ha = a;
-    hb = b;
+    for (uint32_t i = 0; i < kItemStride; ++i) // fixed trip count keeps w[] in registers
+        if (i < n)
+            a ^= word_term(w[i], i);
+    ha = bucket_hash(a);
+    hb = tag_hash(a);
 }
 
 // Loads the 8 header words of a slab. Returns the candidate mask of slots whose tag byte equals
@@ -289,7 +286,8 @@ __device__ __forceinline__ uint32_t probe_header(const Grp<G>& g, const uint32_t
 {
     const uint32_t tag4 = tag * 0x01010101u;
     uint32_t cand = 0, empty = 0;
-    auto bytes = [](uint32_t v) { return ((v >> 7) & 1u) | ((v >> 14) & 2u) | ((v >> 21) & 4u) | ((v >> 28) & 8u); };
+    // bytes of 0xFF/0x00 -> 4-bit mask: the multiply gathers bit 7 of every byte into bits 28..31
+    auto bytes = [](uint32_t v) { return ((v & 0x80808080u) * 0x00204081u) >> 28; };
     auto account = [&](uint32_t word, uint32_t x) {
         if (word < 6) {
             cand |= bytes(__vcmpeq4(x, tag4)) << (4 * word);
