@@ -240,6 +240,24 @@ __device__ __forceinline__ uint32_t ld(const uint32_t* p)
 template <int G, int MODE = LD_DEFAULT>
 __device__ __forceinline__ void load_key(const Grp<G>& g, const uint32_t* p, unsigned long long limit, uint32_t kind, Key<G>& key)
 {
+    if constexpr (G == 1) {
+        // All ten words are requested at once (one memory round trip instead of two: the length is
+        // only known from the first words) and trimmed to the key's length afterwards.
+        uint32_t v[kItemStride];
+#pragma unroll
+        for (uint32_t i = 0; i < kItemStride; ++i)
+            v[i] = i < limit ? ld<MODE>(p + i) : 0u;
+        key.n = kind == SVDAG_KIND_NODE ? dev_node_words(v[0]) : dev_leaf_words(v[0], v[1]);
+        uint32_t a = 0;
+#pragma unroll
+        for (uint32_t i = 0; i < kItemStride; ++i) {
+            key.w[i] = i < key.n ? v[i] : 0u;
+            a ^= i < key.n ? word_term(v[i], i) : 0u;
+        }
+        key.ha = bucket_hash(a);
+        key.hb = tag_hash(a);
+        return;
+    }
     uint32_t w0 = 0, w1 = 0;
     if constexpr (G == 1) {
         w0 = limit > 0 ? ld<MODE>(p) : 0u;
