@@ -456,7 +456,7 @@ __device__ __forceinline__ uint32_t table_find(const Grp<G>& g, const DevDag& d,
             const uint32_t s = __ffs(cand) - 1u;
             cand &= cand - 1u;
             const uint32_t item = slot_handle(body, s, key.n);
-            if (item_equals<G, LD_STREAM>(g, handle_ptr(d, item), key))
+            if (item_equals<G, LD_DEFAULT>(g, handle_ptr(d, item), key))
                 return item;
         }
         if (next == kEnd)
