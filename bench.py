@@ -573,7 +573,7 @@ def main():
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--mode", default="serve", choices=["serve", "c0", "c2", "c3", "hash"],
                     help="serve = the benchmark line; the others run one sub-workload (profiling)")
-    ap.add_argument("--rate", type=float, default=500.0, help="edit arrivals per second")
+    ap.add_argument("--rate", type=float, default=1000.0, help="edit arrivals per second")
     ap.add_argument("--window", type=float, default=0.5, help="seconds of the stream per step")
     ap.add_argument("--levels", type=int, default=17)
     ap.add_argument("--phase-kernels", action="store_true", help="one launch per edit phase (profiling)")

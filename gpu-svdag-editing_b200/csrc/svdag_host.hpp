@@ -103,6 +103,8 @@ bool valid_edit(const svdag_edit* e);
 int expand_edit(const svdag_ctx* ctx, const svdag_edit& e, DevEditor* out);
 int fused_grid(svdag_ctx* ctx);
 svdag_status launch_edits_at(svdag_ctx* ctx, const DevEditor* eds, uint32_t n, char* region, size_t regionBytes, cudaStream_t s);
+// A frame of the root stored at `root` (device word) instead of the current one (svdag_trace.cu).
+svdag_status trace_frame(svdag_ctx* ctx, const svdag_trace_params* p, svdag_hit* out, const uint32_t* root, cudaStream_t s);
 // Procedural scene construction (svdag_scene.cu).
 svdag_status run_scene_build(svdag_ctx* ctx, const svdag_terrain_params* p, cudaStream_t s);
 

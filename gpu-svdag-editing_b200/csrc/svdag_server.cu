@@ -1,7 +1,8 @@
 // svdag_server.cu - the serving form: a request loop on its own host thread with continuous batching
-// of edits into persistent launches, a frame after every launch (edit-to-visible), admission by
-// reserved item-region memory, and a timed replay driver. SVDAG_SERVE_PLAIN turns the same loop into
-// the per-edit baseline (one request at a time, synchronously).
+// of edits into batched launches on one stream, frames on a second stream (one in flight at a time,
+// each behind every batch launched before it, so the GPU renders while the next batch edits),
+// admission by reserved item-region memory, and a timed replay driver. SVDAG_SERVE_PLAIN turns the
+// loop into the per-edit baseline (one request at a time: an edit, then its frame, synchronously).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -33,16 +34,17 @@ struct Request {
     unsigned long long reserve; // admission estimate (edits)
 };
 
-struct Flight {
+// An edit launch: its requests, where its records are, and what they said once it finished.
+struct Batch {
     std::vector<Request> reqs;
-    std::vector<uint32_t> lastRecord; // per request: index of its last record (edits), or ~0u
+    std::vector<uint32_t> lastRecord; // per request: index of its last record
+    std::vector<EditRecord> records; // copied from the slot's pinned buffer when the launch finished
     uint32_t slot = 0;
     uint32_t launch = 0;
     unsigned long long reserved = 0;
     cudaEvent_t done = nullptr;
+    bool finished = false;
 };
-
-constexpr uint32_t kNoRecord = 0xFFFFFFFFu;
 
 // Upper estimate of the item-region bytes an edit can add: its intermediate SVO bounds the new items.
 // Leaves: the footprint's bounding volume in 4^3 bricks, or for spheres and boxes whose volume is
@@ -83,7 +85,8 @@ struct svdag_server {
     svdag_ctx* ctx = nullptr;
     svdag_server_config cfg {};
     Clock::time_point t0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr; // edit launches
+    cudaStream_t frameStream = nullptr; // frames
     svdag_hit* hits = nullptr; // device frame
     svdag_hit* hostHits = nullptr; // pinned copy (SVDAG_SERVE_COPY_FRAMES)
     size_t frameHits = 0;
@@ -91,9 +94,11 @@ struct svdag_server {
     size_t slotBytes = 0;
     std::vector<EditRecord*> hostRecords; // pinned, one array per slot
     std::vector<unsigned long long*> hostTop; // pinned item-region top after each launch
-    std::vector<cudaEvent_t> events;
+    std::vector<cudaEvent_t> events; // one per slot
+    cudaEvent_t frameDone = nullptr;
+    uint32_t* frameRoot = nullptr; // root the frame in flight shows (batches may commit meanwhile)
     unsigned long long capBytes = 0;
-    unsigned long long usedBytes = 0; // item region in use after the last completed launch
+    unsigned long long usedBytes = 0; // item region in use after the last finished launch
 
     std::mutex m;
     std::condition_variable cv, doneCv;
@@ -102,94 +107,131 @@ struct svdag_server {
     uint64_t nextTicket = 1;
     bool stop = false;
     svdag_status fatal = SVDAG_OK;
-    std::deque<Flight> inflight; // touched by the worker thread only
+    // Worker-thread state: launched batches not yet shown by a finished frame, the frame in flight
+    // (it shows every batch launched before it) and the frame requests it will answer.
+    std::deque<Batch> batches;
+    bool frameActive = false;
+    uint32_t frameCovers = 0; // batches with launch < frameCovers are shown by the frame in flight
+    uint32_t covered = 0; // batches with launch < covered have a frame launched behind them
+    std::vector<Request> frameReqs, pendingFrames;
+    svdag_trace_params lastFrame {};
     uint32_t launches = 0;
     std::thread worker;
 
     bool plain() const { return cfg.flags & SVDAG_SERVE_PLAIN; }
 
-    svdag_status launch(std::vector<Request>& reqs, unsigned long long reserved)
+    svdag_status launch_batch(std::vector<Request>& reqs, unsigned long long reserved)
     {
-        Flight f;
-        f.slot = launches % nslots;
-        f.launch = launches++;
-        f.reserved = reserved;
-        f.done = events[f.slot];
+        Batch b;
+        b.slot = launches % nslots;
+        b.launch = launches++;
+        b.reserved = reserved;
+        b.done = events[b.slot];
         std::vector<DevEditor> eds;
-        svdag_trace_params frame = cfg.frame;
         for (auto& r : reqs) {
-            if (r.kind == 0) {
-                DevEditor tmp[2];
-                const int n = expand_edit(ctx, r.edit, tmp);
-                eds.insert(eds.end(), tmp, tmp + n);
-                f.lastRecord.push_back((uint32_t)eds.size() - 1);
-            } else {
-                frame = r.frame;
-                f.lastRecord.push_back(kNoRecord);
-            }
+            DevEditor tmp[2];
+            const int n = expand_edit(ctx, r.edit, tmp);
+            eds.insert(eds.end(), tmp, tmp + n);
+            b.lastRecord.push_back((uint32_t)eds.size() - 1);
         }
-        char* region = ctx->batch + (size_t)f.slot * slotBytes;
-        if (!eds.empty()) {
-            SVDAG_TRY(launch_edits_at(ctx, eds.data(), (uint32_t)eds.size(), region, slotBytes, stream));
-            const size_t edBytes = align256(eds.size() * sizeof(DevEditor));
-            SVDAG_CUDA(cudaMemcpyAsync(hostRecords[f.slot], region + edBytes, eds.size() * sizeof(EditRecord), cudaMemcpyDeviceToHost,
-                stream));
-            SVDAG_CUDA(cudaMemcpyAsync(hostTop[f.slot], &ctx->ctl->itemTop, sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream));
-        }
-        // The frame of the new state: edit-to-visible ends when it completes.
+        char* region = ctx->batch + (size_t)b.slot * slotBytes;
+        SVDAG_TRY(launch_edits_at(ctx, eds.data(), (uint32_t)eds.size(), region, slotBytes, stream));
+        const size_t edBytes = align256(eds.size() * sizeof(DevEditor));
+        b.records.resize(eds.size());
+        SVDAG_CUDA(cudaMemcpyAsync(hostRecords[b.slot], region + edBytes, eds.size() * sizeof(EditRecord), cudaMemcpyDeviceToHost, stream));
+        SVDAG_CUDA(cudaMemcpyAsync(hostTop[b.slot], &ctx->ctl->itemTop, sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream));
+        SVDAG_CUDA(cudaEventRecord(b.done, stream));
+        b.reqs = std::move(reqs);
+        batches.push_back(std::move(b));
+        return SVDAG_OK;
+    }
+
+    // A frame of the newest state, behind every batch launched so far.
+    svdag_status launch_frame()
+    {
+        if (!batches.empty() && batches.back().launch >= covered)
+            SVDAG_CUDA(cudaStreamWaitEvent(frameStream, batches.back().done, 0));
+        svdag_trace_params frame = cfg.frame;
+        for (auto& r : pendingFrames)
+            frame = r.frame;
         if ((size_t)frame.width * frame.height > frameHits)
             frame = cfg.frame;
-        SVDAG_TRY((svdag_status)svdag_trace_primary(ctx, &frame, hits, stream));
+        SVDAG_CUDA(cudaMemcpyAsync(frameRoot, &ctx->ctl->root, sizeof(uint32_t), cudaMemcpyDeviceToDevice, frameStream));
+        SVDAG_TRY(trace_frame(ctx, &frame, hits, frameRoot, frameStream));
         if (cfg.flags & SVDAG_SERVE_COPY_FRAMES)
             SVDAG_CUDA(cudaMemcpyAsync(hostHits, hits, (size_t)frame.width * frame.height * sizeof(svdag_hit), cudaMemcpyDeviceToHost,
-                stream));
-        SVDAG_CUDA(cudaEventRecord(f.done, stream));
-        f.reqs = std::move(reqs);
-        inflight.push_back(std::move(f));
+                frameStream));
+        SVDAG_CUDA(cudaEventRecord(frameDone, frameStream));
+        frameActive = true;
+        frameCovers = covered = launches;
+        frameReqs = std::move(pendingFrames);
+        pendingFrames.clear();
         return SVDAG_OK;
     }
 
-    // Waits for the oldest launch and hands out its results.
-    svdag_status complete_oldest()
+    void finish_batch(Batch& b)
     {
-        SVDAG_CUDA(cudaEventSynchronize(inflight.front().done));
+        if (b.finished)
+            return;
+        std::memcpy(b.records.data(), hostRecords[b.slot], b.records.size() * sizeof(EditRecord));
+        usedBytes = *hostTop[b.slot] * 4ull;
+        b.finished = true;
+    }
+
+    // Results of the batches the finished frame shows and of the frame requests it answers.
+    void complete_frame()
+    {
         const double t = now_since(t0);
-        Flight f = std::move(inflight.front());
-        inflight.pop_front();
-        const EditRecord* rec = hostRecords[f.slot];
         std::lock_guard<std::mutex> lk(m);
-        bool anyEdit = false;
-        for (size_t i = 0; i < f.reqs.size(); ++i) {
-            const Request& r = f.reqs[i];
-            svdag_request_result out {};
-            out.ticket = r.ticket;
-            out.kind = r.kind;
-            out.launch = f.launch;
-            out.submit_s = r.submit;
-            out.visible_s = t;
-            if (f.lastRecord[i] != kNoRecord) {
-                anyEdit = true;
-                const EditRecord& e = rec[f.lastRecord[i]];
+        while (!batches.empty() && batches.front().launch < frameCovers) {
+            Batch& b = batches.front();
+            finish_batch(b); // its event completed before the frame ran
+            for (size_t i = 0; i < b.reqs.size(); ++i) {
+                const Request& r = b.reqs[i];
+                const EditRecord& e = b.records[b.lastRecord[i]];
+                svdag_request_result out {};
+                out.ticket = r.ticket;
+                out.kind = 0;
+                out.launch = b.launch;
+                out.submit_s = r.submit;
+                out.visible_s = t;
                 out.status = e.status;
-                if (r.edit.tool == SVDAG_TOOL_MOVE && f.lastRecord[i] > 0 && rec[f.lastRecord[i] - 1].status)
-                    out.status = rec[f.lastRecord[i] - 1].status;
+                if (r.edit.tool == SVDAG_TOOL_MOVE && b.lastRecord[i] > 0 && b.records[b.lastRecord[i] - 1].status)
+                    out.status = b.records[b.lastRecord[i] - 1].status;
                 out.root_after = e.rootAfter;
                 out.edited_voxels = e.edited;
+                done[r.ticket] = out;
             }
+            batches.pop_front();
+        }
+        for (auto& r : frameReqs) {
+            svdag_request_result out {};
+            out.ticket = r.ticket;
+            out.kind = 1;
+            out.launch = frameCovers;
+            out.submit_s = r.submit;
+            out.visible_s = t;
             done[r.ticket] = out;
         }
-        if (anyEdit)
-            usedBytes = *hostTop[f.slot] * 4ull;
+        frameReqs.clear();
+        frameActive = false;
         doneCv.notify_all();
-        return SVDAG_OK;
     }
 
-    unsigned long long reserved_in_flight()
+    unsigned long long reserved_in_flight() const
     {
         unsigned long long s = 0;
-        for (auto& f : inflight)
-            s += f.reserved;
+        for (auto& b : batches)
+            if (!b.finished)
+                s += b.reserved;
         return s;
+    }
+    uint32_t unfinished() const
+    {
+        uint32_t n = 0;
+        for (auto& b : batches)
+            n += b.finished ? 0u : 1u;
+        return n;
     }
 
     // Hands out failed results for requests that will never become visible.
@@ -207,67 +249,120 @@ struct svdag_server {
         }
         doneCv.notify_all();
     }
+    void fail_everything(svdag_status st)
+    {
+        std::lock_guard<std::mutex> lk(m);
+        fatal = st;
+        for (auto& b : batches)
+            fail_requests(b.reqs, st);
+        batches.clear();
+        fail_requests(frameReqs, st);
+        fail_requests(pendingFrames, st);
+        frameReqs.clear();
+        pendingFrames.clear();
+        frameActive = false;
+    }
+
+    // The per-edit baseline: one request, then its frame, synchronously.
+    void run_plain()
+    {
+        for (;;) {
+            Request r;
+            {
+                std::unique_lock<std::mutex> lk(m);
+                cv.wait(lk, [&] { return stop || !queue.empty(); });
+                if (queue.empty())
+                    break;
+                r = queue.front();
+                queue.pop_front();
+            }
+            std::vector<Request> one { r };
+            svdag_status st = SVDAG_OK;
+            if (r.kind == 0)
+                st = launch_batch(one, r.reserve);
+            else
+                pendingFrames.push_back(r);
+            if (st == SVDAG_OK)
+                st = launch_frame();
+            if (st == SVDAG_OK && cudaEventSynchronize(frameDone) != cudaSuccess)
+                st = SVDAG_ERR_CUDA;
+            if (st != SVDAG_OK) {
+                if (r.kind == 0 && batches.empty()) {
+                    std::lock_guard<std::mutex> lk(m);
+                    fail_requests(one, st);
+                }
+                fail_everything(st);
+                continue;
+            }
+            complete_frame();
+        }
+    }
 
     void run()
     {
-        const uint32_t maxBatch = plain() ? 1u : (cfg.max_batch ? cfg.max_batch : 256u);
-        const uint32_t maxInflight = plain() ? 1u : std::min<uint32_t>(cfg.max_inflight ? cfg.max_inflight : 2u, nslots - 1);
+        if (plain()) {
+            run_plain();
+            return;
+        }
+        const uint32_t maxBatch = cfg.max_batch ? cfg.max_batch : 256u;
+        const uint32_t maxInflight = std::min<uint32_t>(cfg.max_inflight ? cfg.max_inflight : 2u, nslots - 1);
         for (;;) {
-            // Results of finished launches.
-            while (!inflight.empty() && cudaEventQuery(inflight.front().done) == cudaSuccess)
-                if (complete_oldest() != SVDAG_OK)
-                    break;
+            // Finished launches (records, memory in use), then a finished frame.
+            for (auto& b : batches)
+                if (!b.finished && cudaEventQuery(b.done) == cudaSuccess)
+                    finish_batch(b);
+            if (frameActive && cudaEventQuery(frameDone) == cudaSuccess)
+                complete_frame();
             std::vector<Request> take;
             unsigned long long reserve = 0;
             {
                 std::unique_lock<std::mutex> lk(m);
-                if (stop && queue.empty() && inflight.empty())
+                if (stop && queue.empty() && batches.empty() && !frameActive && pendingFrames.empty())
                     break;
-                if (inflight.size() < maxInflight && !queue.empty()) {
-                    const unsigned long long inUse = usedBytes + reserved_in_flight();
-                    uint32_t edits = 0;
-                    while (!queue.empty()) {
-                        Request& r = queue.front();
-                        if (r.kind == 0) {
-                            if (edits == maxBatch)
-                                break;
-                            const bool first = inflight.empty() && edits == 0; // always make progress
-                            if (!first && inUse + reserve + r.reserve > capBytes)
-                                break;
-                            reserve += r.reserve;
-                            ++edits;
-                        }
-                        take.push_back(r);
-                        queue.pop_front();
-                        if (plain())
-                            break;
+                const bool canLaunch = unfinished() < maxInflight;
+                const unsigned long long inUse = usedBytes + reserved_in_flight();
+                uint32_t edits = 0;
+                for (auto it = queue.begin(); it != queue.end();) {
+                    if (it->kind == 1) { // answered by the next frame
+                        pendingFrames.push_back(*it);
+                        it = queue.erase(it);
+                        continue;
                     }
+                    if (!canLaunch || edits == maxBatch)
+                        break;
+                    const bool first = unfinished() == 0 && edits == 0; // always make progress
+                    if (!first && inUse + reserve + it->reserve > capBytes)
+                        break;
+                    reserve += it->reserve;
+                    ++edits;
+                    take.push_back(*it);
+                    it = queue.erase(it);
                 }
             }
+            bool launched = false;
             if (!take.empty()) {
-                const svdag_status st = launch(take, reserve);
-                if (st != SVDAG_OK) {
+                if (launch_batch(take, reserve) != SVDAG_OK) {
                     std::lock_guard<std::mutex> lk(m);
-                    fatal = st;
-                    fail_requests(take, st);
+                    fail_requests(take, SVDAG_ERR_CUDA);
+                    continue;
                 }
-                continue;
+                launched = true;
             }
-            if (!inflight.empty() && inflight.size() >= maxInflight) {
-                // Full: wait for the oldest launch.
-                if (complete_oldest() != SVDAG_OK) {
-                    std::lock_guard<std::mutex> lk(m);
-                    fatal = SVDAG_ERR_CUDA;
-                    for (auto& f : inflight)
-                        fail_requests(f.reqs, SVDAG_ERR_CUDA);
-                    inflight.clear();
+            // One frame in flight at a time, behind everything launched so far.
+            const bool uncovered = !batches.empty() && batches.back().launch >= covered;
+            if (!frameActive && (uncovered || !pendingFrames.empty())) {
+                if (launch_frame() != SVDAG_OK) {
+                    fail_everything(SVDAG_ERR_CUDA);
+                    continue;
                 }
-                continue;
+                launched = true;
             }
+            if (launched)
+                continue;
             std::unique_lock<std::mutex> lk(m);
-            if (inflight.empty())
+            if (batches.empty() && !frameActive && pendingFrames.empty())
                 cv.wait(lk, [&] { return stop || !queue.empty(); });
-            else // a launch is on the GPU: wake for new requests or to look at it again
+            else // work on the GPU: wake for new requests or to look at it again
                 cv.wait_for(lk, std::chrono::microseconds(20), [&] { return stop || !queue.empty(); });
         }
     }
@@ -298,6 +393,9 @@ svdag_status svdag_server_create(svdag_ctx* ctx, const svdag_server_config* conf
             st = cuda_status(e);
     };
     fail(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    fail(cudaStreamCreateWithFlags(&s->frameStream, cudaStreamNonBlocking));
+    fail(cudaEventCreateWithFlags(&s->frameDone, cudaEventDisableTiming));
+    fail(cudaMalloc(&s->frameRoot, 256));
     fail(cudaMalloc(&s->hits, s->frameHits * sizeof(svdag_hit)));
     if (config->flags & SVDAG_SERVE_COPY_FRAMES)
         fail(cudaMallocHost(&s->hostHits, s->frameHits * sizeof(svdag_hit)));
@@ -346,6 +444,8 @@ svdag_status svdag_server_destroy(svdag_server* s)
         s->worker.join();
     if (s->stream)
         cudaStreamSynchronize(s->stream);
+    if (s->frameStream)
+        cudaStreamSynchronize(s->frameStream);
     for (auto* r : s->hostRecords)
         cudaFreeHost(r);
     for (auto* t : s->hostTop)
@@ -356,8 +456,14 @@ svdag_status svdag_server_destroy(svdag_server* s)
         cudaFreeHost(s->hostHits);
     if (s->hits)
         cudaFree(s->hits);
+    if (s->frameRoot)
+        cudaFree(s->frameRoot);
+    if (s->frameDone)
+        cudaEventDestroy(s->frameDone);
     if (s->stream)
         cudaStreamDestroy(s->stream);
+    if (s->frameStream)
+        cudaStreamDestroy(s->frameStream);
     const svdag_status st = s->fatal;
     delete s;
     return st;

@@ -4,9 +4,9 @@
 // (tracer.cu:28-411), ray setup from DAGTracer::resolve_paths (dag_tracer.cu:112-134), voxel queries
 // from getVoxelValues_kernel -> DAGUtils::get_value (dag_tracer.cu:361-372, dag_utils.h:146-182).
 // Float and double arithmetic follow the reference expression by expression; with -fmad=false nothing
-// is contracted, so hits equal the oracle's bit for bit. A child fetch is one load: handles are word
-// offsets of the items, so the traversal reads the header and the child handle without a slab-table
-// decode.
+// is contracted, so hits equal the oracle's bit for bit. A child fetch is one load: handles are
+// offsets of the items (8-byte units), so the traversal reads the header and the child handle without
+// a slab-table decode.
 #include <cuda_runtime.h>
 
 #include "svdag_host.hpp"
@@ -111,7 +111,7 @@ __device__ __forceinline__ uint32_t first_child_mask(uint32_t lo, uint32_t hi) /
     return out;
 }
 
-__global__ void __launch_bounds__(256) k_trace(DevDag d, svdag_trace_params p, svdag_hit* out)
+__global__ void __launch_bounds__(256) k_trace(DevDag d, svdag_trace_params p, svdag_hit* out, const uint32_t* rootPtr)
 {
     const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t y = blockIdx.y * blockDim.y + threadIdx.y;
@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(256) k_trace(DevDag d, svdag_trace_params p, s
     uint32_t stackMasks[kMaxLevels]; // childMask | visitMask << 8
     uint32_t level = 0, addr = 0, px = 0, py = 0, pz = 0, leafLo = 0, leafHi = 0;
     uint32_t material = 0xFFFFFFFFu;
-    const uint32_t root = d.ctl->root;
+    const uint32_t root = rootPtr ? *rootPtr : d.ctl->root;
     if (root != kNone) {
         uint32_t cIndex = root;
         uint32_t cChild = item_ptr(d, root)[0] & 0xFFu;
@@ -282,6 +282,16 @@ __global__ void k_sample(DevDag d, const uint32_t* xyz, uint32_t n, uint32_t* ou
 }
 
 } // namespace
+
+svdag_status trace_frame(svdag_ctx* ctx, const svdag_trace_params* p, svdag_hit* out, const uint32_t* root, cudaStream_t s)
+{
+    const dim3 block(32, 8);
+    const dim3 grid((p->width + block.x - 1) / block.x, (p->height + block.y - 1) / block.y);
+    k_trace<<<grid, block, 0, s>>>(ctx->dag(), *p, out, root);
+    SVDAG_CUDA(cudaGetLastError());
+    return SVDAG_OK;
+}
+
 } // namespace svdag
 
 using namespace svdag;
@@ -294,7 +304,7 @@ svdag_status svdag_trace_primary(svdag_ctx* ctx, const svdag_trace_params* p, sv
         return SVDAG_ERR_INVALID;
     const dim3 block(32, 8);
     const dim3 grid((p->width + block.x - 1) / block.x, (p->height + block.y - 1) / block.y);
-    k_trace<<<grid, block, 0, as_stream(stream)>>>(ctx->dag(), *p, out);
+    k_trace<<<grid, block, 0, as_stream(stream)>>>(ctx->dag(), *p, out, nullptr);
     SVDAG_CUDA(cudaGetLastError());
     return SVDAG_OK;
 }

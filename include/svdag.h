@@ -329,9 +329,10 @@ svdag_status svdag_export_level(svdag_ctx* ctx, uint32_t level, uint32_t* out_ha
  *
  * A request loop on its own host thread keeps the DAG, its tables and the undo history resident and
  * serves edit and frame requests as they arrive. Edits that arrive while earlier launches are on the
- * GPU are coalesced into the next batched persistent launch (continuous batching: up to max_inflight
- * launches are queued on the GPU ahead of their completion); every launch is followed by a frame of
- * the new state, which makes its edits visible and answers every frame request pending at launch.
+ * GPU are coalesced into the next batched launch (continuous batching: up to max_inflight launches
+ * are queued on the GPU ahead of their completion). Frames run on a second stream, one at a time,
+ * each behind every batch launched before it: its completion makes those edits visible and answers
+ * the frame requests pending when it started, and the next batch edits while it renders.
  * An edit is admitted when the item-region bytes in use plus those reserved by admitted, unfinished
  * edits (an upper estimate from the tool's footprint) stay under the memory cap; a queue head that
  * does not fit waits until launches complete. With SVDAG_SERVE_PLAIN the same loop serves one request
