@@ -533,6 +533,33 @@ def run_mode_c2(args):
     print(json.dumps({"levels": args.levels, "build_s": build_s, "edits": out}))
 
 
+def run_mode_trace(args):
+    """1920x1080 primary-ray frames of the at-scale scene (at --levels), CUDA-event timed."""
+    import torch
+
+    import svdag
+    import svdag.workloads as w
+
+    dag, _ = make_scene(svdag, w, args.levels, pool_gb=args.pool_gb)
+    cam = c2_camera(svdag, args.levels)
+    tracer = svdag.DAGTracer(cam.width, cam.height)
+    stream = torch.cuda.Stream()
+    for _ in range(args.warmup):
+        tracer.resolve_paths(cam, dag, stream=stream.cuda_stream)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    for a, b in ev:
+        a.record(stream)
+        tracer.resolve_paths(cam, dag, stream=stream.cuda_stream)
+        b.record(stream)
+    torch.cuda.synchronize()
+    ms = [a.elapsed_time(b) for a, b in ev]
+    hits = tracer.hits_numpy()
+    dag.free()
+    print(json.dumps({"levels": args.levels, "frame_ms_p50": pct(ms, 50), "mrays_s": cam.width * cam.height / pct(ms, 50) / 1e3,
+                      "hit_fraction": float((hits["material"] != 255).mean())}))
+
+
 def run_mode_c3(args):
     """256 edits of uneven footprint: one batched persistent launch against the plain per-edit path,
     each on its own copy of the scene; the stored item sets must be equal."""
@@ -571,7 +598,7 @@ def main():
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
-    ap.add_argument("--mode", default="serve", choices=["serve", "c0", "c2", "c3", "hash"],
+    ap.add_argument("--mode", default="serve", choices=["serve", "c0", "c2", "c3", "hash", "trace"],
                     help="serve = the benchmark line; the others run one sub-workload (profiling)")
     ap.add_argument("--rate", type=float, default=1000.0, help="edit arrivals per second")
     ap.add_argument("--window", type=float, default=0.5, help="seconds of the stream per step")
@@ -598,6 +625,8 @@ def main():
         run_mode_c2(args)
     elif args.mode == "c3":
         run_mode_c3(args)
+    elif args.mode == "trace":
+        run_mode_trace(args)
     else:
         run_serve(args)
 

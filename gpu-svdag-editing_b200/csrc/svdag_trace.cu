@@ -48,56 +48,37 @@ __device__ __forceinline__ uint32_t intersection_mask(bool isRoot, uint32_t leve
         mask = 1u << (((x >= rx) ? 4u : 0u) + ((y >= ry) ? 2u : 0u) + ((z >= rz) ? 1u : 0u));
     }
     const float eps = 1e-4f;
-    if (tmin <= tmx && tmx <= tmax) {
+    // The three plane tests as selects (no divergent branches; same comparisons and operands).
+    {
         const float y = tmx * r.dy, z = tmx * r.dz;
-        uint32_t A = 0, B = 0;
-        if (y >= ry - eps)
-            A |= 0xCC;
-        if (y <= ry + eps)
-            A |= 0x33;
-        if (z >= rz - eps)
-            B |= 0xAA;
-        if (z <= rz + eps)
-            B |= 0x55;
-        mask |= A & B;
+        const uint32_t A = ((y >= ry - eps) ? 0xCCu : 0u) | ((y <= ry + eps) ? 0x33u : 0u);
+        const uint32_t B = ((z >= rz - eps) ? 0xAAu : 0u) | ((z <= rz + eps) ? 0x55u : 0u);
+        mask |= (tmin <= tmx && tmx <= tmax) ? (A & B) : 0u;
     }
-    if (tmin <= tmy && tmy <= tmax) {
+    {
         const float x = tmy * r.dx, z = tmy * r.dz;
-        uint32_t C = 0, D = 0;
-        if (x >= rx - eps)
-            C |= 0xF0;
-        if (x <= rx + eps)
-            C |= 0x0F;
-        if (z >= rz - eps)
-            D |= 0xAA;
-        if (z <= rz + eps)
-            D |= 0x55;
-        mask |= C & D;
+        const uint32_t C = ((x >= rx - eps) ? 0xF0u : 0u) | ((x <= rx + eps) ? 0x0Fu : 0u);
+        const uint32_t D = ((z >= rz - eps) ? 0xAAu : 0u) | ((z <= rz + eps) ? 0x55u : 0u);
+        mask |= (tmin <= tmy && tmy <= tmax) ? (C & D) : 0u;
     }
-    if (tmin <= tmz && tmz <= tmax) {
+    {
         const float x = tmz * r.dx, y = tmz * r.dy;
-        uint32_t E = 0, F = 0;
-        if (x >= rx - eps)
-            E |= 0xF0;
-        if (x <= rx + eps)
-            E |= 0x0F;
-        if (y >= ry - eps)
-            F |= 0xCC;
-        if (y <= ry + eps)
-            F |= 0x33;
-        mask |= E & F;
+        const uint32_t E = ((x >= rx - eps) ? 0xF0u : 0u) | ((x <= rx + eps) ? 0x0Fu : 0u);
+        const uint32_t F = ((y >= ry - eps) ? 0xCCu : 0u) | ((y <= ry + eps) ? 0x33u : 0u);
+        mask |= (tmin <= tmz && tmz <= tmax) ? (E & F) : 0u;
     }
     return mask & 0xFFu;
 }
 
-__device__ __forceinline__ uint32_t next_child(uint32_t order, uint32_t mask) // tracer.cu:45-54
+// The first child ci = c ^ order (c = 0, 1, ...) whose bit is set (tracer.cu:45-54; mask != 0): the
+// mask is permuted so that bit c holds bit c ^ order, then the lowest set bit is taken.
+__device__ __forceinline__ uint32_t next_child(uint32_t order, uint32_t mask)
 {
-    for (uint32_t c = 0; c < 8; ++c) {
-        const uint32_t ci = c ^ order;
-        if (mask & (1u << ci))
-            return ci;
-    }
-    return 0;
+    uint32_t m = mask;
+    m = (order & 1u) ? (((m & 0x55u) << 1) | ((m >> 1) & 0x55u)) : m;
+    m = (order & 2u) ? (((m & 0x33u) << 2) | ((m >> 2) & 0x33u)) : m;
+    m = (order & 4u) ? (((m & 0x0Fu) << 4) | ((m >> 4) & 0x0Fu)) : m;
+    return ((uint32_t)__ffs(m) - 1u) ^ order;
 }
 
 __device__ __forceinline__ uint32_t first_child_mask(uint32_t lo, uint32_t hi) // Leaf::get_first_child_mask, base_dag.h:16-52
@@ -138,8 +119,10 @@ __global__ void __launch_bounds__(256) k_trace(DevDag d, svdag_trace_params p, s
     // intersect_ray, tracer.cu:186-273.
     const uint32_t levels = d.levels, LL = d.leafLevel;
     const uint32_t order = (r.dx < 0.f ? 4u : 0u) + (r.dy < 0.f ? 2u : 0u) + (r.dz < 0.f ? 1u : 0u);
-    uint32_t stackIndex[kMaxLevels];
-    uint32_t stackMasks[kMaxLevels]; // childMask | visitMask << 8
+    // Traversal stack in shared memory, [level][thread] so that a warp's accesses hit distinct banks.
+    __shared__ uint32_t sIndex[kMaxLevels][256];
+    __shared__ uint32_t sMasks[kMaxLevels][256]; // childMask | visitMask << 8
+    const uint32_t tix = threadIdx.y * blockDim.x + threadIdx.x;
     uint32_t level = 0, addr = 0, px = 0, py = 0, pz = 0, leafLo = 0, leafHi = 0;
     uint32_t material = 0xFFFFFFFFu;
     const uint32_t root = rootPtr ? *rootPtr : d.ctl->root;
@@ -152,9 +135,9 @@ __global__ void __launch_bounds__(256) k_trace(DevDag d, svdag_trace_params p, s
                 uint32_t newLevel = level;
                 while (newLevel > 0 && !cVisit) {
                     newLevel--;
-                    cIndex = stackIndex[newLevel];
-                    cChild = stackMasks[newLevel] & 0xFFu;
-                    cVisit = stackMasks[newLevel] >> 8;
+                    cIndex = sIndex[newLevel][tix];
+                    cChild = sMasks[newLevel][tix] & 0xFFu;
+                    cVisit = sMasks[newLevel][tix] >> 8;
                 }
                 if (newLevel == 0 && !cVisit) {
                     px = py = pz = 0;
@@ -171,8 +154,8 @@ __global__ void __launch_bounds__(256) k_trace(DevDag d, svdag_trace_params p, s
             px = (px << 1) | ((nextChild >> 2) & 1u);
             py = (py << 1) | ((nextChild >> 1) & 1u);
             pz = (pz << 1) | (nextChild & 1u);
-            stackIndex[level] = cIndex;
-            stackMasks[level] = cChild | (cVisit << 8);
+            sIndex[level][tix] = cIndex;
+            sMasks[level][tix] = cChild | (cVisit << 8);
             level++;
             if (level == levels) {
                 const uint32_t voxel = ((px & 1u) ? 4u : 0u) | ((py & 1u) ? 2u : 0u) | ((pz & 1u) ? 1u : 0u) | ((px & 2u) ? 32u : 0u)
