@@ -376,6 +376,7 @@ __device__ void ph_build_level(const DevDag& d, const DevEditor& e, uint32_t lev
 template <uint32_t TOOL>
 __device__ void ph_build_leaves(const DevDag& d, const DevEditor& e, char* scratch, unsigned long long scratchBytes)
 {
+    __shared__ __align__(16) uint32_t packBuf[8][16]; // per warp of a 256-thread block: 64 material bytes
     EditCounters& E = d.ctl->edit;
     const uint32_t LL = d.leafLevel;
     const unsigned long long stride = work_stride(TOOL);
@@ -538,35 +539,36 @@ __device__ void ph_build_leaves(const DevDag& d, const DevEditor& e, char* scrat
         const uint32_t nhi = __ballot_sync(0xFFFFFFFFu, set[1]);
         const uint32_t below = (1u << lane) - 1u;
         const uint32_t off0 = __popc(nlo & below), off1 = __popc(nlo) + __popc(nhi & below);
-        uint32_t words[8];
-#pragma unroll
-        for (uint32_t wd = 0; wd < 8; ++wd) {
-            uint32_t v = 0;
-            if (set[0] && (off0 >> 3) == wd)
-                v |= newMat[0] << (4u * (off0 & 7u));
-            if (set[1] && (off1 >> 3) == wd)
-                v |= newMat[1] << (4u * (off1 & 7u));
-            words[wd] = __reduce_or_sync(0xFFFFFFFFu, v);
+        // Pack the materials in voxel order through the warp's 64-byte slice of shared memory: clear,
+        // scatter one byte per set voxel at its rank, then lanes 2..9 each fold 8 bytes into a word of
+        // nibbles (LeafBuilder, my_gpu_base_dag.h:102-150).
+        uint32_t* pw = packBuf[threadIdx.x >> 5];
+        uint8_t* pb = reinterpret_cast<uint8_t*>(pw);
+        if (lane < 16)
+            pw[lane] = 0u;
+        __syncwarp();
+        if (set[0])
+            pb[off0] = (uint8_t)newMat[0];
+        if (set[1])
+            pb[off1] = (uint8_t)newMat[1];
+        __syncwarp();
+        uint32_t mine = lane == 0 ? nlo : nhi;
+        if (lane >= 2 && lane < kItemStride) {
+            unsigned long long x = reinterpret_cast<const unsigned long long*>(pw)[lane - 2];
+            x = (x | (x >> 4)) & 0x00FF00FF00FF00FFull;
+            x = (x | (x >> 8)) & 0x0000FFFF0000FFFFull;
+            x = (x | (x >> 16)) & 0x00000000FFFFFFFFull;
+            mine = (uint32_t)x;
         }
+        const uint32_t m0 = (uint32_t)pb[0] * 0x11111111u;
+        __syncwarp(); // the buffer is reused by the next leaf
         uint32_t* outLeaf = reinterpret_cast<uint32_t*>(scratch + offN) + (size_t)i * kItemStride;
-        uint32_t mine = 0;
-#pragma unroll
-        for (uint32_t wd = 0; wd < 8; ++wd)
-            if (lane == 2 + wd)
-                mine = words[wd];
-        if (lane == 0)
-            mine = nlo;
-        if (lane == 1)
-            mine = nhi;
         if (lane < kItemStride)
             outLeaf[lane] = mine;
-        if (lane == 0 && nlo == 0xFFFFFFFFu && nhi == 0xFFFFFFFFu) { // is_leaf_fully_filled (my_gpu_hash_dag.h:143-166)
-            const uint32_t m = (words[0] & 0xFu) * 0x11111111u;
-            bool full = true;
-            for (int wd = 0; wd < 8; ++wd)
-                full &= words[wd] == m;
-            fullLeaves += full ? 1u : 0u;
-        }
+        // is_leaf_fully_filled (my_gpu_hash_dag.h:143-166): all 64 voxels set, one material
+        const uint32_t same = __ballot_sync(0xFFFFFFFFu, lane >= 2 && lane < kItemStride && mine == m0);
+        if (lane == 0 && nlo == 0xFFFFFFFFu && nhi == 0xFFFFFFFFu && (same & 0x3FCu) == 0x3FCu)
+            ++fullLeaves;
         w = wn;
         wn = wnn;
         owRaw = owNext;
