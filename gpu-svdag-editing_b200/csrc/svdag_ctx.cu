@@ -176,6 +176,7 @@ svdag_status svdag_create(const svdag_config* cfg, svdag_ctx** out)
     ctx->device = cfg->device;
     ctx->probeLanes = cfg->probe_lanes ? cfg->probe_lanes : 1; // thread per key: measured fastest on B200
     ctx->loadFactor = cfg->target_load_factor ? cfg->target_load_factor : 16;
+    ctx->persistentLeaves = (cfg->flags & SVDAG_FLAG_PERSISTENT) ? 16384.0 : 0.0;
     ctx->cfg.undo_depth = cfg->undo_depth ? std::min<uint32_t>(cfg->undo_depth, 64) : 32;
     if (cudaMalloc(&ctx->pool, pool) != cudaSuccess) {
         cudaGetLastError();

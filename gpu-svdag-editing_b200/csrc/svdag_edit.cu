@@ -1333,8 +1333,8 @@ svdag_status launch_edits_at(svdag_ctx* ctx, const DevEditor* eds, uint32_t n, c
         // a pageable source is staged before the call returns, so the vector may go
         SVDAG_CUDA(cudaMemcpyAsync(region, withRecords.data(), (size_t)n * sizeof(DevEditor), cudaMemcpyHostToDevice, s));
     }
-    const int grid = (ctx->cfg.flags & SVDAG_FLAG_PERSISTENT) ? fused_grid(ctx) : 0;
-    auto small = [&](uint32_t k) { return grid > 0 && estimate_leaves(eds[k]) <= ctx->bigEditLeaves; };
+    const int grid = ctx->persistentLeaves > 0 ? fused_grid(ctx) : 0;
+    auto small = [&](uint32_t k) { return grid > 0 && estimate_leaves(eds[k]) <= ctx->persistentLeaves; };
     uint32_t i = 0;
     while (i < n) {
         if (!small(i)) { // a run of editors through the queue: the first phase takes eds[cursor]
@@ -1434,7 +1434,7 @@ svdag_status run_edit(svdag_ctx* ctx, const svdag_edit* e, cudaStream_t s)
     DevEditor eds[2];
     const int n = expand_edit(ctx, *e, eds);
     for (int i = 0; i < n; ++i) {
-        if ((ctx->cfg.flags & SVDAG_FLAG_PERSISTENT) && fused_grid(ctx) > 0 && estimate_leaves(eds[i]) <= ctx->bigEditLeaves)
+        if (ctx->persistentLeaves > 0 && fused_grid(ctx) > 0 && estimate_leaves(eds[i]) <= ctx->persistentLeaves)
             SVDAG_TRY(launch_single_fused(ctx, eds[i], s));
         else
             SVDAG_TRY(launch_pipeline(ctx, eds[i], s, nullptr, true));

@@ -39,7 +39,7 @@ struct svdag_ctx {
     svdag_table levelTables[svdag::kMaxLevels];
     std::vector<svdag_table*> standalone;
     uint32_t probeLanes = 8;
-    double bigEditLeaves = 16384; // edits whose SVO may exceed this many leaves run one launch per phase
+    double persistentLeaves = 0; // edits estimated at or below this many SVO leaves run in the persistent kernel (0 = none)
     uint32_t loadFactor = 16;
     unsigned long long scratchHighWater = 0;
     svdag::DevDag dag() const { return svdag::DevDag { items, itemWords, headers, headerCount, ctl, cfg.levels, cfg.levels - 2 }; }
@@ -102,6 +102,14 @@ svdag_status launch_scene_tiles(svdag_ctx* ctx, const DevEditor* eds, uint32_t n
 bool valid_edit(const svdag_edit* e);
 int expand_edit(const svdag_ctx* ctx, const svdag_edit& e, DevEditor* out);
 int fused_grid(svdag_ctx* ctx);
+double estimate_leaves(const DevEditor& e);
+svdag_status launch_single_fused(svdag_ctx* ctx, const DevEditor& ed, cudaStream_t s);
+svdag_status launch_pipeline(svdag_ctx* ctx, const DevEditor& ed, cudaStream_t s, EditRecord* record, bool graphOk);
+// The batched table operations of the public API, by lane count (svdag_tables.cu).
+svdag_status table_add_lanes(svdag_table* t, const uint32_t* keys, const uint32_t* offsets, uint32_t n, unsigned long long totalWords,
+    uint32_t* out, uint32_t lanes, cudaStream_t s);
+svdag_status table_find_lanes(svdag_table* t, const uint32_t* keys, const uint32_t* offsets, uint32_t n, unsigned long long totalWords,
+    uint32_t* out, uint32_t lanes, cudaStream_t s);
 svdag_status launch_edits_at(svdag_ctx* ctx, const DevEditor* eds, uint32_t n, char* region, size_t regionBytes, cudaStream_t s);
 // A frame of the root stored at `root` (device word) instead of the current one (svdag_trace.cu).
 svdag_status trace_frame(svdag_ctx* ctx, const svdag_trace_params* p, svdag_hit* out, const uint32_t* root, cudaStream_t s);

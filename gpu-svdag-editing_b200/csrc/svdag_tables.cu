@@ -600,6 +600,21 @@ svdag_status svdag_export_level(svdag_ctx* ctx, uint32_t level, uint32_t* outHan
 
 } // extern "C"
 
+namespace svdag {
+
+svdag_status table_add_lanes(svdag_table* t, const uint32_t* keys, const uint32_t* offsets, uint32_t n, unsigned long long totalWords,
+    uint32_t* out, uint32_t lanes, cudaStream_t s)
+{
+    return n ? launch_table_op<OP_ADD>(t, keys, offsets, n, totalWords, nullptr, out, lanes, s) : SVDAG_OK;
+}
+svdag_status table_find_lanes(svdag_table* t, const uint32_t* keys, const uint32_t* offsets, uint32_t n, unsigned long long totalWords,
+    uint32_t* out, uint32_t lanes, cudaStream_t s)
+{
+    return n ? launch_table_op<OP_FIND>(t, keys, offsets, n, totalWords, nullptr, out, lanes, s) : SVDAG_OK;
+}
+
+} // namespace svdag
+
 // ---------------------------------------------------------------- helpers of the scene builder
 
 namespace {

@@ -100,6 +100,12 @@ assert RESULT_DTYPE.itemsize == C.sizeof(RequestResult) == 48
 SERVE_PLAIN, SERVE_COPY_FRAMES = 1, 2
 
 
+class Tuning(C.Structure):
+    _fields_ = [("probe_lanes", C.c_uint32), ("load_factor", C.c_uint32), ("persistent_leaves", C.c_uint32),
+                ("trials", C.c_uint32), ("table_ns_per_key", C.c_double), ("graph_us_small", C.c_double),
+                ("persistent_us_small", C.c_double)]
+
+
 class Stats(C.Structure):
     _fields_ = [("levels", C.c_uint32), ("root", C.c_uint32), ("pool_bytes", C.c_uint64),
                 ("item_region_bytes", C.c_uint64), ("item_region_used_bytes", C.c_uint64),
@@ -156,6 +162,9 @@ _PROTOS = {
     "svdag_table_get_stats": [_P, C.POINTER(TableStats), _P],
     "svdag_get_stats": [_P, C.POINTER(Stats), _P],
     "svdag_export_level": [_P, _U32, _P, _P, _U64, C.POINTER(_U64), _P],
+    "svdag_autotune": [_P, C.POINTER(Edit), _U32, _P, _P, _U32, _U64, _U32, C.POINTER(Tuning), _P],
+    "svdag_get_tuning": [_P, C.POINTER(Tuning)],
+    "svdag_set_tuning": [_P, C.POINTER(Tuning)],
     "svdag_server_create": [_P, C.POINTER(ServerConfig), C.POINTER(_P)],
     "svdag_server_destroy": [_P],
     "svdag_submit_edit": [_P, C.POINTER(Edit), C.POINTER(_U64)],
@@ -405,6 +414,23 @@ class MyGPUHashDAG:
     def sample_voxels(self, xyz_dev, count: int, out_dev, stream=None):
         _check(lib().svdag_sample_voxels(self.h, ptr(xyz_dev), count, ptr(out_dev), stream_ptr(stream)),
                "svdag_sample_voxels")
+
+    def autotune(self, edits=(), keys=None, offsets=None, n_keys=0, total_words=0, kind=0, stream=None) -> "Tuning":
+        """Autotuner (svdag_autotune): key sample -> load factor and lanes per key; edit sample (applied
+        for real) -> which small edits use the persistent kernel."""
+        arr = (Edit * max(len(edits), 1))(*[e if isinstance(e, Edit) else e.to_edit() for e in edits])
+        t = Tuning()
+        _check(lib().svdag_autotune(self.h, arr, len(edits), ptr(keys), ptr(offsets), n_keys, total_words, kind,
+                                    C.byref(t), stream_ptr(stream)), "svdag_autotune")
+        return t
+
+    def tuning(self) -> "Tuning":
+        t = Tuning()
+        _check(lib().svdag_get_tuning(self.h, C.byref(t)), "svdag_get_tuning")
+        return t
+
+    def set_tuning(self, t: "Tuning"):
+        _check(lib().svdag_set_tuning(self.h, C.byref(t)), "svdag_set_tuning")
 
     def export_level(self, level: int):
         """(handles uint32[n], words uint32[n, 10]) of every item in the level table."""

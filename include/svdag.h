@@ -325,6 +325,34 @@ svdag_status svdag_get_stats(svdag_ctx* ctx, svdag_stats* out, void* stream);
 svdag_status svdag_export_level(svdag_ctx* ctx, uint32_t level, uint32_t* out_handles, uint32_t* out_words,
     uint64_t capacity, uint64_t* out_count, void* stream);
 
+/* ---------------------------------------------------------------- autotuner
+ *
+ * Picks the settings of the batched form by measuring them on the device (no counterpart in the
+ * reference, whose table sizes, slab layout and thread mapping are compile-time constants):
+ *  - with a key sample: for each load factor (items per bucket of the tables sized from then on:
+ *    8, 12, 16, 24, 32) and lane count per key (1, 2, 4, 8), a scratch table sized for the sample is
+ *    filled with it and searched for it, timed with CUDA events; the fastest pair is kept. The
+ *    scratch tables' space is given back afterwards.
+ *  - with an edit sample: the edits are applied in order (for real, each pushing its undo frame),
+ *    alternately through the per-tool CUDA graph of the phase launches and through the persistent
+ *    cooperative kernel, each timed with CUDA events; per size bucket of the estimated SVO leaves the
+ *    faster form wins and the persistent kernel is kept for the buckets, from the smallest up, where
+ *    it wins.
+ * Synchronous; no other call may use the context meanwhile. */
+typedef struct svdag_tuning {
+    uint32_t probe_lanes; /* lanes per key of the table kernels */
+    uint32_t load_factor; /* items per bucket of tables sized from now on */
+    uint32_t persistent_leaves; /* edits estimated at or below this many SVO leaves use the persistent kernel (0 = none) */
+    uint32_t trials; /* measurements taken */
+    double table_ns_per_key; /* best fill + search time per key of the key sample */
+    double graph_us_small; /* mean time of the sample's edits estimated below 4096 leaves: graph form */
+    double persistent_us_small; /* the same through the persistent kernel */
+} svdag_tuning;
+svdag_status svdag_autotune(svdag_ctx* ctx, const svdag_edit* edits, uint32_t n_edits, const uint32_t* keys_dev,
+    const uint32_t* offsets_dev, uint32_t n_keys, uint64_t total_words, uint32_t kind, svdag_tuning* out, void* stream);
+svdag_status svdag_get_tuning(svdag_ctx* ctx, svdag_tuning* out);
+svdag_status svdag_set_tuning(svdag_ctx* ctx, const svdag_tuning* tuning);
+
 /* ---------------------------------------------------------------- serving form
  *
  * A request loop on its own host thread keeps the DAG, its tables and the undo history resident and

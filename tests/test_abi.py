@@ -39,6 +39,7 @@ def test_struct_layouts(svdag_lib):
     assert C.sizeof(s.TerrainParams) == 32
     assert C.sizeof(s.ServerConfig) == 128
     assert C.sizeof(s.RequestResult) == 48
+    assert C.sizeof(s.Tuning) == 40
 
 
 def test_invalid_arguments_are_rejected(svdag_lib):
