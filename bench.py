@@ -231,6 +231,17 @@ def make_scene(svdag, w, levels, phase_kernels=False, pool_gb=0.0, persistent=Fa
     return dag, terrain
 
 
+def max_over_ranks(values, dist=None, device="cuda"):
+    """Element-wise max of floats over all ranks: a replica job's latency is its slowest rank's."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return [float(v) for v in values]
+    import torch
+
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.cpu()]
+
+
 def summarize(res, n_edits):
     """Latency (ms) and throughput of a replay; res = edits then frames."""
     ed = res[:n_edits]
@@ -333,10 +344,7 @@ def run_serve(args):
     if not args.no_hash:
         hash_res = run_hash_bench(svdag, torch, torch.cuda.Stream(), lanes=args.hash_lanes, load_factor=args.hash_lf)
     p99 = out["served"]["p99_ms"]
-    if dist:
-        t = torch.tensor([p99, out["plain"]["p99_ms"], out["e2e"]["p99_ms"]], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        p99, out["plain"]["p99_ms"], out["e2e"]["p99_ms"] = (float(x) for x in t)
+    p99, out["plain"]["p99_ms"], out["e2e"]["p99_ms"] = max_over_ranks([p99, out["plain"]["p99_ms"], out["e2e"]["p99_ms"]], dist)
     peak, peak_kind = measured_peak_gbs()
     bt = out["batch"]
     achieved = bt["bytes"] / (bt["ms"] / 1e3) / 1e9
