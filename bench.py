@@ -375,7 +375,8 @@ def run_serve(args):
                 "h2d_bytes_per_step": int(56 * len(ek) / args.steps),
                 "d2h_bytes_per_step": int((n_frames_e2e * frame_bytes + 48 * len(ek)) / args.steps),
                 "detail": out["e2e"]},
-        "roofline": {"bound": "hbm", "kernel": "k_edit_fused (one window of the stream as one persistent launch)",
+        "roofline": {"bound": "hbm", "kernel": "edit pipeline: one window of the stream as one batch (per-tool CUDA graphs of "
+                               "the phase kernels, small edits in the single-CTA persistent kernel)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind, "traffic": None, "launch": bt},
         "clocks": out["clocks"],

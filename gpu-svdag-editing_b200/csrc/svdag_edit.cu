@@ -9,7 +9,6 @@
 // every kernel sizes itself from counters written by its predecessor, and the scratch arena layout is
 // recomputed on the device from those counts. Intra-level dedup is one open-addressing pass; the DAG
 // insert is a fused find-or-insert (the reference runs find and insert as two kernels).
-#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -20,7 +19,6 @@
 #include "svdag_edit.cuh"
 #include "svdag_host.hpp"
 
-namespace cg = cooperative_groups;
 
 namespace svdag {
 
@@ -376,7 +374,7 @@ __device__ void ph_build_level(const DevDag& d, const DevEditor& e, uint32_t lev
 template <uint32_t TOOL>
 __device__ void ph_build_leaves(const DevDag& d, const DevEditor& e, char* scratch, unsigned long long scratchBytes)
 {
-    __shared__ __align__(16) uint32_t packBuf[8][16]; // per warp of a 256-thread block: 64 material bytes
+    __shared__ __align__(16) uint32_t packBuf[16][16]; // per warp of a block of up to 512 threads: 64 material bytes
     EditCounters& E = d.ctl->edit;
     const uint32_t LL = d.leafLevel;
     const unsigned long long stride = work_stride(TOOL);
@@ -997,9 +995,12 @@ __global__ void k_edit_end(DevDag d, char* scratch, EditQueue* q)
 }
 
 // ---------------------------------------------------------------- persistent form
-// One cooperative launch runs whole edits: every phase above is a grid-stride loop over the
-// device-resident counts, separated by grid-wide barriers instead of kernel boundaries. All
-// threads reach every barrier (phases only return early, never skip a barrier).
+// The persistent form for small edits: one CTA of 512 threads runs whole edits, one after another,
+// every phase above being a block-stride loop over the device-resident counts and the phases
+// separated by block barriers. Small SVOs thus cost one launch per batch instead of ~35 launches
+// per edit. All threads reach every barrier (phases only return early, never skip a barrier).
+
+constexpr uint32_t kBlockThreads = 512;
 
 __device__ __forceinline__ void stamp(const DevDag& d, uint32_t& k)
 {
@@ -1013,77 +1014,67 @@ __device__ __forceinline__ void stamp(const DevDag& d, uint32_t& k)
 }
 
 template <uint32_t TOOL>
-__device__ __forceinline__ void fused_edit(cg::grid_group& grid, const DevDag& d, const DevEditor& ed, char* scratch,
-    unsigned long long scratchBytes, EditRecord* record)
+__device__ __forceinline__ void block_edit(const DevDag& d, const DevEditor& ed, char* scratch, unsigned long long scratchBytes,
+    EditRecord* record)
 {
     const uint32_t LL = d.leafLevel;
     uint32_t k = 0;
     stamp(d, k);
     ph_reset_counters(d);
-    grid.sync();
+    __syncthreads();
     ph_edit_begin(d, ed, scratch);
-    grid.sync();
+    __syncthreads();
     stamp(d, k);
     for (uint32_t level = 0; level < LL; ++level) {
         ph_build_level<TOOL>(d, ed, level, scratch, scratchBytes);
-        grid.sync();
+        __syncthreads();
         stamp(d, k);
     }
     ph_build_leaves<TOOL>(d, ed, scratch, scratchBytes);
-    grid.sync();
+    __syncthreads();
     stamp(d, k);
     for (int level = (int)LL; level >= 0; --level) {
         ph_merge_level(d, (uint32_t)level, scratch);
-        grid.sync();
+        __syncthreads();
         stamp(d, k);
     }
     ph_edit_end(d, scratch, ed.builder, ed.tileOut, record);
-    grid.sync();
+    __syncthreads();
     stamp(d, k);
 }
 
-__global__ void __launch_bounds__(256) k_edit_fused(DevDag d, DevEditor single, const DevEditor* eds, uint32_t numEdits, char* scratch,
-    unsigned long long scratchBytes, EditRecord* records)
+__global__ void __launch_bounds__(kBlockThreads, 1) k_edit_block(DevDag d, DevEditor single, const DevEditor* eds, uint32_t numEdits,
+    char* scratch, unsigned long long scratchBytes, EditRecord* records)
 {
-    cg::grid_group grid = cg::this_grid();
     for (uint32_t k = 0; k < numEdits; ++k) {
         const DevEditor ed = eds ? eds[k] : single;
         EditRecord* rec = records ? &records[k] : nullptr;
         switch (ed.tool) {
         case SVDAG_TOOL_SPHERE_ADD:
-            fused_edit<SVDAG_TOOL_SPHERE_ADD>(grid, d, ed, scratch, scratchBytes, rec);
+            block_edit<SVDAG_TOOL_SPHERE_ADD>(d, ed, scratch, scratchBytes, rec);
             break;
         case SVDAG_TOOL_SPHERE_REMOVE:
-            fused_edit<SVDAG_TOOL_SPHERE_REMOVE>(grid, d, ed, scratch, scratchBytes, rec);
+            block_edit<SVDAG_TOOL_SPHERE_REMOVE>(d, ed, scratch, scratchBytes, rec);
             break;
         case SVDAG_TOOL_BOX_ADD:
-            fused_edit<SVDAG_TOOL_BOX_ADD>(grid, d, ed, scratch, scratchBytes, rec);
+            block_edit<SVDAG_TOOL_BOX_ADD>(d, ed, scratch, scratchBytes, rec);
             break;
         case SVDAG_TOOL_BOX_REMOVE:
-            fused_edit<SVDAG_TOOL_BOX_REMOVE>(grid, d, ed, scratch, scratchBytes, rec);
+            block_edit<SVDAG_TOOL_BOX_REMOVE>(d, ed, scratch, scratchBytes, rec);
             break;
         case SVDAG_TOOL_SPHERE_PAINT:
-            fused_edit<SVDAG_TOOL_SPHERE_PAINT>(grid, d, ed, scratch, scratchBytes, rec);
+            block_edit<SVDAG_TOOL_SPHERE_PAINT>(d, ed, scratch, scratchBytes, rec);
             break;
         case SVDAG_TOOL_COPY:
-            fused_edit<SVDAG_TOOL_COPY>(grid, d, ed, scratch, scratchBytes, rec);
+            block_edit<SVDAG_TOOL_COPY>(d, ed, scratch, scratchBytes, rec);
             break;
         case SVDAG_TOOL_BOX_PAINT_NOISE:
-            fused_edit<SVDAG_TOOL_BOX_PAINT_NOISE>(grid, d, ed, scratch, scratchBytes, rec);
+            block_edit<SVDAG_TOOL_BOX_PAINT_NOISE>(d, ed, scratch, scratchBytes, rec);
             break;
         default:
             break;
         }
     }
-}
-
-// Scene tiles: builder edits of subtrees, one after another in one persistent launch.
-__global__ void __launch_bounds__(256) k_scene_fused(DevDag d, const DevEditor* eds, uint32_t numEdits, char* scratch,
-    unsigned long long scratchBytes)
-{
-    cg::grid_group grid = cg::this_grid();
-    for (uint32_t k = 0; k < numEdits; ++k)
-        fused_edit<kToolTerrain>(grid, d, eds[k], scratch, scratchBytes, nullptr);
 }
 
 __global__ void k_undo_redo(Control* c, uint32_t redo)
@@ -1333,8 +1324,7 @@ svdag_status launch_edits_at(svdag_ctx* ctx, const DevEditor* eds, uint32_t n, c
         // a pageable source is staged before the call returns, so the vector may go
         SVDAG_CUDA(cudaMemcpyAsync(region, withRecords.data(), (size_t)n * sizeof(DevEditor), cudaMemcpyHostToDevice, s));
     }
-    const int grid = ctx->persistentLeaves > 0 ? fused_grid(ctx) : 0;
-    auto small = [&](uint32_t k) { return grid > 0 && estimate_leaves(eds[k]) <= ctx->persistentLeaves; };
+    auto small = [&](uint32_t k) { return ctx->persistentLeaves > 0 && estimate_leaves(eds[k]) <= ctx->persistentLeaves; };
     uint32_t i = 0;
     while (i < n) {
         if (!small(i)) { // a run of editors through the queue: the first phase takes eds[cursor]
@@ -1358,8 +1348,8 @@ svdag_status launch_edits_at(svdag_ctx* ctx, const DevEditor* eds, uint32_t n, c
         uint32_t m = j - i;
         char* scratch = ctx->scratch;
         unsigned long long scratchBytes = ctx->scratchBytes;
-        void* args[] = { &d, &single, &segEds, &m, &scratch, &scratchBytes, &segRec };
-        SVDAG_CUDA(cudaLaunchCooperativeKernel((const void*)k_edit_fused, dim3(grid), dim3(256), args, 0, s));
+        k_edit_block<<<1, kBlockThreads, 0, s>>>(d, single, segEds, m, scratch, scratchBytes, segRec);
+        SVDAG_CUDA(cudaGetLastError());
         i = j;
     }
     return SVDAG_OK;
@@ -1395,36 +1385,11 @@ int expand_edit(const svdag_ctx* ctx, const svdag_edit& e, DevEditor* out)
     return 1;
 }
 
-int fused_grid(svdag_ctx* ctx)
-{
-    if (ctx->cfg.flags & SVDAG_FLAG_PHASE_KERNELS)
-        return 0;
-    if (ctx->fusedGrid < 0) {
-        int perSm = 0, sms = 0, coop = 0;
-        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ctx->device);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-        if (coop && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_edit_fused, 256, 0) == cudaSuccess)
-            ctx->fusedGrid = perSm * sms;
-        else
-            ctx->fusedGrid = 0;
-        cudaGetLastError();
-    }
-    return ctx->fusedGrid;
-}
-
 // One small edit as one persistent launch, its editor passed by value.
 svdag_status launch_single_fused(svdag_ctx* ctx, const DevEditor& ed, cudaStream_t s)
 {
-    const int grid = fused_grid(ctx);
-    DevDag d = ctx->dag();
-    DevEditor single = ed;
-    const DevEditor* devEds = nullptr;
-    EditRecord* records = nullptr;
-    uint32_t n = 1;
-    char* scratch = ctx->scratch;
-    unsigned long long scratchBytes = ctx->scratchBytes;
-    void* args[] = { &d, &single, &devEds, &n, &scratch, &scratchBytes, &records };
-    SVDAG_CUDA(cudaLaunchCooperativeKernel((const void*)k_edit_fused, dim3(grid), dim3(256), args, 0, s));
+    k_edit_block<<<1, kBlockThreads, 0, s>>>(ctx->dag(), ed, nullptr, 1, ctx->scratch, ctx->scratchBytes, nullptr);
+    SVDAG_CUDA(cudaGetLastError());
     return SVDAG_OK;
 }
 
@@ -1434,7 +1399,7 @@ svdag_status run_edit(svdag_ctx* ctx, const svdag_edit* e, cudaStream_t s)
     DevEditor eds[2];
     const int n = expand_edit(ctx, *e, eds);
     for (int i = 0; i < n; ++i) {
-        if (ctx->persistentLeaves > 0 && fused_grid(ctx) > 0 && estimate_leaves(eds[i]) <= ctx->persistentLeaves)
+        if (ctx->persistentLeaves > 0 && estimate_leaves(eds[i]) <= ctx->persistentLeaves)
             SVDAG_TRY(launch_single_fused(ctx, eds[i], s));
         else
             SVDAG_TRY(launch_pipeline(ctx, eds[i], s, nullptr, true));
@@ -1529,33 +1494,8 @@ svdag_status build_scene_untiled(svdag_ctx* ctx, const DevEditor& ed, cudaStream
 // in one persistent launch (the level tables exist already; the merge phase finds or inserts).
 svdag_status launch_scene_tiles(svdag_ctx* ctx, const DevEditor* eds, uint32_t n, cudaStream_t s)
 {
-    if (ctx->sceneGrid < 0) {
-        int perSm = 0, sms = 0, coop = 0;
-        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ctx->device);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-        if (coop && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_scene_fused, 256, 0) == cudaSuccess)
-            ctx->sceneGrid = perSm * sms;
-        else
-            ctx->sceneGrid = 0;
-        cudaGetLastError();
-    }
-    if (ctx->sceneGrid <= 0 || (ctx->cfg.flags & SVDAG_FLAG_PHASE_KERNELS)) {
-        for (uint32_t i = 0; i < n; ++i)
-            SVDAG_TRY(launch_pipeline(ctx, eds[i], s, nullptr, false));
-        return SVDAG_OK;
-    }
-    const uint32_t perLaunch = (uint32_t)(ctx->batchBytes / sizeof(DevEditor));
-    for (uint32_t i = 0; i < n; i += perLaunch) {
-        uint32_t m = std::min(perLaunch, n - i);
-        SVDAG_CUDA(cudaMemcpyAsync(ctx->batch, eds + i, (size_t)m * sizeof(DevEditor), cudaMemcpyHostToDevice, s));
-        DevDag d = ctx->dag();
-        const DevEditor* devEds = reinterpret_cast<const DevEditor*>(ctx->batch);
-        char* scratch = ctx->scratch;
-        unsigned long long scratchBytes = ctx->scratchBytes;
-        void* args[] = { &d, &devEds, &m, &scratch, &scratchBytes };
-        SVDAG_CUDA(cudaLaunchCooperativeKernel((const void*)k_scene_fused, dim3(ctx->sceneGrid), dim3(256), args, 0, s));
-        SVDAG_CUDA(cudaStreamSynchronize(s)); // the batch region is reused by the next launch
-    }
+    for (uint32_t i = 0; i < n; ++i) // tiles are large: one launch per phase at full occupancy
+        SVDAG_TRY(launch_pipeline(ctx, eds[i], s, nullptr, false));
     return SVDAG_OK;
 }
 

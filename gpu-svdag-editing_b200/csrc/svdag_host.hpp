@@ -27,8 +27,6 @@ struct svdag_ctx {
     unsigned long long scratchBytes = 0;
     char* batch = nullptr; // editors and per-edit records of a persistent batch launch
     unsigned long long batchBytes = 0;
-    int fusedGrid = -1; // co-resident blocks of the persistent edit kernel (0 = unavailable)
-    int sceneGrid = -1; // same for the scene tile kernel
     svdag::EditQueue* queue = nullptr; // editor slot of the one-launch-per-phase form (end of the batch region)
     cudaGraphExec_t graphs[svdag::kNumGraphs] = {}; // per tool: the phase launches of one edit
     uint32_t lastBatch = 0;
@@ -101,7 +99,6 @@ svdag_status launch_scene_tiles(svdag_ctx* ctx, const DevEditor* eds, uint32_t n
 // expanded editors with their editors and records in `region` (svdag_edit.cu).
 bool valid_edit(const svdag_edit* e);
 int expand_edit(const svdag_ctx* ctx, const svdag_edit& e, DevEditor* out);
-int fused_grid(svdag_ctx* ctx);
 double estimate_leaves(const DevEditor& e);
 svdag_status launch_single_fused(svdag_ctx* ctx, const DevEditor& ed, cudaStream_t s);
 svdag_status launch_pipeline(svdag_ctx* ctx, const DevEditor& ed, cudaStream_t s, EditRecord* record, bool graphOk);

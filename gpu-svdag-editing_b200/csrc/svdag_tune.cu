@@ -108,11 +108,6 @@ svdag_status tune_tables(svdag_ctx* ctx, const uint32_t* keys, const uint32_t* o
 svdag_status tune_edits(svdag_ctx* ctx, const svdag_edit* edits, uint32_t n, svdag_tuning& out, cudaStream_t s)
 {
     SVDAG_TRY(ensure_level_tables(ctx, s));
-    if (fused_grid(ctx) <= 0) { // no cooperative launch: graphs only
-        out.persistent_leaves = 0;
-        ctx->persistentLeaves = 0;
-        return SVDAG_OK;
-    }
     // Size buckets of the estimated SVO leaves: [0, 1K), [1K, 4K), [4K, 16K), [16K, 64K), [64K, inf).
     constexpr int kBuckets = 5;
     const double upper[kBuckets] = { 1024, 4096, 16384, 65536, 1e300 };
