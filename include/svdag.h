@@ -57,8 +57,9 @@ typedef enum svdag_item_kind { SVDAG_KIND_NODE = 0, SVDAG_KIND_LEAF = 1 } svdag_
 /* Launch every edit phase directly instead of replaying the tool's captured CUDA graph of the phase
  * launches (for profiling single phases). */
 #define SVDAG_FLAG_PHASE_KERNELS 1u
-/* Run edits whose intermediate SVO is estimated small in one persistent cooperative launch (grid-wide
- * barriers between phases) instead of the per-tool CUDA graph of the phase launches. */
+/* Run edits whose intermediate SVO is estimated small (up to 16384 leaves) in the persistent kernel
+ * (one CTA, block barriers between phases; a run of such edits is one launch) instead of the tool's
+ * CUDA graph of the phase launches. svdag_autotune chooses the threshold by measurement. */
 #define SVDAG_FLAG_PERSISTENT 2u
 
 typedef struct svdag_config {
@@ -165,9 +166,10 @@ typedef struct svdag_edit_stats {
  * (my_gpu_hash_dag_edits.h:12-13, body my_gpu_hash_dag_edits.cu:633-671). Asynchronous on
  * `stream`; the root handle, undo history and counters stay on the device. */
 svdag_status svdag_edit_apply(svdag_ctx* ctx, const svdag_edit* edit, void* stream);
-/* Batched form: applies the edits in order inside one persistent cooperative launch (phases separated
- * by grid-wide barriers, no host round trip between edits); the result equals applying them one by
- * one. Each edit gets an svdag_edit_record. A move counts as two records (removal, then paste). */
+/* Batched form: applies the edits in order with no host round trip between them (runs of small edits
+ * in one persistent launch, the others replayed through the tool's CUDA graph, all reading their
+ * editors from device memory); the result equals applying them one by one. Each edit gets an
+ * svdag_edit_record. A move counts as two records (removal, then paste). */
 svdag_status svdag_edit_apply_many(svdag_ctx* ctx, const svdag_edit* edits, uint32_t count, void* stream);
 
 typedef struct svdag_edit_record {
@@ -335,9 +337,8 @@ svdag_status svdag_export_level(svdag_ctx* ctx, uint32_t level, uint32_t* out_ha
  *    scratch tables' space is given back afterwards.
  *  - with an edit sample: the edits are applied in order (for real, each pushing its undo frame),
  *    alternately through the per-tool CUDA graph of the phase launches and through the persistent
- *    cooperative kernel, each timed with CUDA events; per size bucket of the estimated SVO leaves the
- *    faster form wins and the persistent kernel is kept for the buckets, from the smallest up, where
- *    it wins.
+ *    single-CTA kernel, each timed with CUDA events; the persistent kernel is kept for the size
+ *    buckets of the estimated SVO leaves, from the smallest up, where it is faster.
  * Synchronous; no other call may use the context meanwhile. */
 typedef struct svdag_tuning {
     uint32_t probe_lanes; /* lanes per key of the table kernels */
