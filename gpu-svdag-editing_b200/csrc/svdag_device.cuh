@@ -98,6 +98,11 @@ struct DevDag {
     uint32_t leafLevel;
 };
 
+// Release fence at GPU scope: stores before it are visible to other SMs before stores after it (the
+// writers' half of publishing data through a flag or table entry; readers depend on the published
+// value's address, which orders their loads).
+__device__ __forceinline__ void fence_release() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
 // Latches the first error of the context (reported by svdag_sync) and of the running edit (which
 // then leaves the root unchanged).
 __device__ __forceinline__ void set_status(Control* ctl, uint32_t code)

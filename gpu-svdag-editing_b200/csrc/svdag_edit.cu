@@ -843,7 +843,7 @@ __device__ void ph_merge_level(const DevDag& d, uint32_t level, char* scratch)
 #pragma unroll
             for (uint32_t j = 0; j < kItemStride; ++j)
                 it[j] = key.w[j];
-            __threadfence(); // the content is visible before the dedup entry that points at it
+            fence_release(); // the content is visible before the dedup entry that points at it
         }
         const bool isEmpty = isLeaf ? (key.w[0] == 0 && key.w[1] == 0) : ((key.w[0] & 0xFFu) == 0);
         if (isEmpty) {
