@@ -478,10 +478,14 @@ __device__ __forceinline__ uint32_t table_find(const Grp<G>& g, const DevDag& d,
 // `busy` claims with the in-flight tag (published later), otherwise with the final tag.
 template <int G>
 __device__ __forceinline__ uint32_t claim_in_slab(const Grp<G>& g, const DevDag& d, uint32_t slab, uint32_t body, uint32_t emptyMask,
-    uint32_t tag, uint32_t n, bool busy, uint32_t& slot)
+    uint32_t tag, uint32_t n, bool busy, uint32_t& slot, uint32_t spread)
 {
+    // Claimants of one slab start at different free slots (`spread` is a hash of the key), so that
+    // they do not all race for the first free slot of the same snapshot.
+    const uint32_t start = spread % kSlots;
     while (emptyMask) {
-        const uint32_t s = __ffs(emptyMask) - 1u;
+        const uint32_t up = emptyMask >> start;
+        const uint32_t s = up ? start + (uint32_t)__ffs(up) - 1u : (uint32_t)__ffs(emptyMask) - 1u;
         const uint32_t word = s >> 2, shift = 8u * (s & 3u);
         uint32_t got = 0;
         if (g.lane == 0) {
@@ -504,7 +508,7 @@ __device__ __forceinline__ uint32_t claim_in_slab(const Grp<G>& g, const DevDag&
             slot = s;
             return slot_handle(body, s, n);
         }
-        emptyMask &= emptyMask - 1u;
+        emptyMask &= ~(1u << s);
     }
     return kNone;
 }
@@ -524,7 +528,7 @@ __device__ __forceinline__ uint32_t table_add(const Grp<G>& g, const DevDag& d, 
     for (uint32_t steps = 0; steps < kMaxChain; ++steps) {
         uint32_t next, body, empty, slot;
         probe_header<G>(g, slab_ptr(d, slab), tag, next, body, empty);
-        const uint32_t item = claim_in_slab<G>(g, d, slab, body, empty, tag, key.n, false, slot);
+        const uint32_t item = claim_in_slab<G>(g, d, slab, body, empty, tag, key.n, false, slot, key.ha >> 8);
         if (item != kNone) {
             write_item<G>(g, handle_ptr(d, item), key);
             return item;
@@ -600,7 +604,7 @@ __device__ __forceinline__ uint32_t table_find_or_insert(const Grp<G>& g, const 
     uint32_t empty = tailEmpty, body = tailBody;
     for (uint32_t steps = 0; steps < kMaxChain; ++steps) {
         uint32_t s = 0;
-        const uint32_t item = claim_in_slab<G>(g, d, slab, body, empty, tag, key.n, true, s);
+        const uint32_t item = claim_in_slab<G>(g, d, slab, body, empty, tag, key.n, true, s, key.ha >> 8);
         if (item != kNone) {
             write_item<G>(g, handle_ptr(d, item), key);
             __threadfence();
