@@ -27,7 +27,7 @@ using Clock = std::chrono::steady_clock;
 
 struct Request {
     uint64_t ticket;
-    uint32_t kind; // 0 edit, 1 frame
+    uint32_t kind; // 0 edit, 1 frame, 2 undo, 3 redo
     svdag_edit edit;
     svdag_trace_params frame;
     double submit;
@@ -41,6 +41,7 @@ struct Batch {
     std::vector<EditRecord> records; // copied from the slot's pinned buffer when the launch finished
     uint32_t slot = 0;
     uint32_t launch = 0;
+    uint32_t root = 0; // undo/redo launches: the root they left
     unsigned long long reserved = 0;
     cudaEvent_t done = nullptr;
     bool finished = false;
@@ -94,6 +95,7 @@ struct svdag_server {
     size_t slotBytes = 0;
     std::vector<EditRecord*> hostRecords; // pinned, one array per slot
     std::vector<unsigned long long*> hostTop; // pinned item-region top after each launch
+    std::vector<uint32_t*> hostRoot; // pinned root after each undo/redo launch
     std::vector<cudaEvent_t> events; // one per slot
     cudaEvent_t frameDone = nullptr;
     uint32_t* frameRoot = nullptr; // root the frame in flight shows (batches may commit meanwhile)
@@ -127,6 +129,15 @@ struct svdag_server {
         b.launch = launches++;
         b.reserved = reserved;
         b.done = events[b.slot];
+        if (reqs.size() == 1 && reqs[0].kind >= 2) { // an undo or redo is a launch of its own
+            SVDAG_TRY(reqs[0].kind == 2 ? svdag_undo(ctx, stream) : svdag_redo(ctx, stream));
+            SVDAG_CUDA(cudaMemcpyAsync(hostRoot[b.slot], &ctx->ctl->root, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+            SVDAG_CUDA(cudaMemcpyAsync(hostTop[b.slot], &ctx->ctl->itemTop, sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream));
+            SVDAG_CUDA(cudaEventRecord(b.done, stream));
+            b.reqs = std::move(reqs);
+            batches.push_back(std::move(b));
+            return SVDAG_OK;
+        }
         std::vector<DevEditor> eds;
         for (auto& r : reqs) {
             DevEditor tmp[2];
@@ -174,6 +185,8 @@ struct svdag_server {
         if (b.finished)
             return;
         std::memcpy(b.records.data(), hostRecords[b.slot], b.records.size() * sizeof(EditRecord));
+        if (b.records.empty())
+            b.root = *hostRoot[b.slot];
         usedBytes = *hostTop[b.slot] * 4ull;
         b.finished = true;
     }
@@ -188,13 +201,18 @@ struct svdag_server {
             finish_batch(b); // its event completed before the frame ran
             for (size_t i = 0; i < b.reqs.size(); ++i) {
                 const Request& r = b.reqs[i];
-                const EditRecord& e = b.records[b.lastRecord[i]];
                 svdag_request_result out {};
                 out.ticket = r.ticket;
-                out.kind = 0;
+                out.kind = r.kind;
                 out.launch = b.launch;
                 out.submit_s = r.submit;
                 out.visible_s = t;
+                if (r.kind >= 2) {
+                    out.root_after = b.root;
+                    done[r.ticket] = out;
+                    continue;
+                }
+                const EditRecord& e = b.records[b.lastRecord[i]];
                 out.status = e.status;
                 if (r.edit.tool == SVDAG_TOOL_MOVE && b.lastRecord[i] > 0 && b.records[b.lastRecord[i] - 1].status)
                     out.status = b.records[b.lastRecord[i] - 1].status;
@@ -328,6 +346,13 @@ struct svdag_server {
                         it = queue.erase(it);
                         continue;
                     }
+                    if (it->kind >= 2) { // undo/redo: a launch of its own, after the edits before it
+                        if (canLaunch && edits == 0) {
+                            take.push_back(*it);
+                            queue.erase(it);
+                        }
+                        break;
+                    }
                     if (!canLaunch || edits == maxBatch)
                         break;
                     const bool first = unfinished() == 0 && edits == 0; // always make progress
@@ -403,12 +428,15 @@ svdag_status svdag_server_create(svdag_ctx* ctx, const svdag_server_config* conf
     for (uint32_t i = 0; i < s->nslots; ++i) {
         EditRecord* r = nullptr;
         unsigned long long* t = nullptr;
+        uint32_t* root = nullptr;
         cudaEvent_t ev = nullptr;
         fail(cudaMallocHost(&r, maxRecords * sizeof(EditRecord)));
         fail(cudaMallocHost(&t, sizeof(unsigned long long)));
+        fail(cudaMallocHost(&root, sizeof(uint32_t)));
         fail(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
         s->hostRecords.push_back(r);
         s->hostTop.push_back(t);
+        s->hostRoot.push_back(root);
         s->events.push_back(ev);
     }
     {
@@ -450,6 +478,8 @@ svdag_status svdag_server_destroy(svdag_server* s)
         cudaFreeHost(r);
     for (auto* t : s->hostTop)
         cudaFreeHost(t);
+    for (auto* r : s->hostRoot)
+        cudaFreeHost(r);
     for (auto ev : s->events)
         cudaEventDestroy(ev);
     if (s->hostHits)
@@ -565,6 +595,64 @@ svdag_status svdag_server_replay(svdag_server* s, const svdag_edit* edits, const
     }
     for (uint32_t i = 0; i < nEdits + nFrames; ++i)
         SVDAG_TRY(svdag_poll(s, tickets[i], 1, &results[i]));
+    return SVDAG_OK;
+}
+
+svdag_status svdag_submit_undo(svdag_server* s, int redo, uint64_t* ticket)
+{
+    if (!s || !ticket)
+        return SVDAG_ERR_INVALID;
+    Request r {};
+    r.kind = redo ? 3u : 2u;
+    {
+        std::lock_guard<std::mutex> lk(s->m);
+        if (s->stop)
+            return SVDAG_ERR_INVALID;
+        r.ticket = s->nextTicket++;
+        r.submit = now_since(s->t0);
+        s->queue.push_back(r);
+    }
+    s->cv.notify_one();
+    *ticket = r.ticket;
+    return SVDAG_OK;
+}
+
+svdag_status svdag_server_replay_actions(svdag_server* s, const svdag_replay_action* actions, uint64_t n, double period,
+    const svdag_trace_params* frames, svdag_request_result* results)
+{
+    if (!s || !results || (n && !actions) || !(period >= 0.0))
+        return SVDAG_ERR_INVALID;
+    for (uint64_t i = 0; i < n; ++i)
+        if (actions[i].kind == SVDAG_REPLAY_EDIT && !valid_edit(&actions[i].edit))
+            return SVDAG_ERR_INVALID;
+    std::vector<uint64_t> tickets(n, 0);
+    const Clock::time_point start = Clock::now();
+    uint64_t frame = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        switch (actions[i].kind) {
+        case SVDAG_REPLAY_EDIT:
+            SVDAG_TRY(svdag_submit_edit(s, &actions[i].edit, &tickets[i]));
+            break;
+        case SVDAG_REPLAY_UNDO:
+        case SVDAG_REPLAY_REDO:
+            SVDAG_TRY(svdag_submit_undo(s, actions[i].kind == SVDAG_REPLAY_REDO, &tickets[i]));
+            break;
+        case SVDAG_REPLAY_END_FRAME:
+            SVDAG_TRY(svdag_submit_frame(s, frames ? &frames[frame] : nullptr, &tickets[i]));
+            ++frame;
+            std::this_thread::sleep_until(
+                start + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double>(period * (double)frame)));
+            break;
+        default:
+            break;
+        }
+    }
+    for (uint64_t i = 0; i < n; ++i) {
+        if (tickets[i])
+            SVDAG_TRY(svdag_poll(s, tickets[i], 1, &results[i]));
+        else
+            results[i] = svdag_request_result {};
+    }
     return SVDAG_OK;
 }
 

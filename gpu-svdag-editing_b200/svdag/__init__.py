@@ -93,6 +93,15 @@ class RequestResult(C.Structure):
                 ("visible_s", C.c_double)]
 
 
+class ReplayAction(C.Structure):
+    """svdag_replay_action: one line of a reference replay file (replay.h)."""
+    _fields_ = [("kind", C.c_uint32), ("edit", Edit), ("camera", C.c_float * 9)]
+
+
+REPLAY_OTHER, REPLAY_EDIT, REPLAY_UNDO, REPLAY_REDO, REPLAY_END_FRAME = 0, 1, 2, 3, 4
+REPLAY_CAMERA_LOCATION, REPLAY_CAMERA_ROTATION = 5, 6
+RESULT_EDIT, RESULT_FRAME, RESULT_UNDO, RESULT_REDO = 0, 1, 2, 3
+
 RESULT_DTYPE = np.dtype([("ticket", "<u8"), ("kind", "<u4"), ("status", "<u4"), ("root_after", "<u4"),
                          ("launch", "<u4"), ("edited_voxels", "<u8"), ("submit_s", "<f8"), ("visible_s", "<f8")])
 assert RESULT_DTYPE.itemsize == C.sizeof(RequestResult) == 48
@@ -172,6 +181,9 @@ _PROTOS = {
     "svdag_poll": [_P, _U64, C.c_int, C.POINTER(RequestResult)],
     "svdag_server_frame": [_P, _P, _U64],
     "svdag_server_replay": [_P, C.POINTER(Edit), _P, _U32, _P, _U32, _P],
+    "svdag_submit_undo": [_P, C.c_int, C.POINTER(_U64)],
+    "svdag_replay_parse": [C.c_char_p, _U64, C.c_float, _P, _U64, C.POINTER(_U64), C.POINTER(_U64)],
+    "svdag_server_replay_actions": [_P, _P, _U64, C.c_double, _P, _P],
 }
 EXPORTED = tuple(_PROTOS)
 
@@ -602,6 +614,26 @@ class Server:
                                          out.ctypes.data), "svdag_server_replay")
         return out
 
+    def submit_undo(self, redo: bool = False) -> int:
+        t = C.c_uint64()
+        _check(lib().svdag_submit_undo(self.h, 1 if redo else 0, C.byref(t)), "svdag_submit_undo")
+        return t.value
+
+    def replay_actions(self, actions, frame_period_s: float = 0.0, frames=None) -> np.ndarray:
+        """Serves parsed replay actions (parse_replay), one recorded frame every frame_period_s
+        seconds; `frames` (one TraceParams per EndFrame, e.g. replay_frames) overrides the configured
+        camera. Returns one result per action (ticket 0 for actions that are not requests)."""
+        n = len(actions)
+        out = np.zeros(n, dtype=RESULT_DTYPE)
+        fr = None
+        if frames is not None:
+            fr = (TraceParams * max(len(frames), 1))(*frames)
+            if len(frames) < sum(1 for a in actions if a.kind == REPLAY_END_FRAME):
+                raise SvdagError(1, "replay_actions: one frame per EndFrame")
+        _check(lib().svdag_server_replay_actions(self.h, C.addressof(actions) if n else None, n, float(frame_period_s), fr,
+                                                 out.ctypes.data), "svdag_server_replay_actions")
+        return out
+
     def close(self):
         if getattr(self, "h", None):
             h, self.h = self.h, None
@@ -612,3 +644,66 @@ class Server:
 
     def __exit__(self, *exc):
         self.close()
+
+
+# ---------------------------------------------------------------- recorded edit sessions
+
+def replay_scale(scene_depth: int, replay_depth: int) -> float:
+    """scalingFactor of replay.cpp:10: replay positions are voxels of a 2^replay_depth grid."""
+    return float(np.float32(float(1 << scene_depth)) / np.float32(float(1 << replay_depth)))
+
+
+def parse_replay(text, scale: float = 1.0):
+    """Parses a reference replay file's text (ReplayManager::load_csv, replay.h:650-683) into a
+    ctypes array of ReplayAction, edits scaled by `scale` (svdag_replay_parse)."""
+    data = text.encode() if isinstance(text, str) else bytes(text)
+    count, bad = C.c_uint64(), C.c_uint64()
+    st = lib().svdag_replay_parse(data, len(data), scale, None, 0, C.byref(count), C.byref(bad))
+    if st != 0:
+        raise SvdagError(st, f"svdag_replay_parse (line {bad.value})")
+    arr = (ReplayAction * max(count.value, 1))()
+    _check(lib().svdag_replay_parse(data, len(data), scale, C.addressof(arr), count.value, C.byref(count), None),
+           "svdag_replay_parse")
+    return (ReplayAction * count.value).from_buffer(arr) if count.value else (ReplayAction * 0)()
+
+
+def view_trace_params(position, rotation, width: int, height: int, levels: int, bounds_min, bounds_max,
+                      fov_degrees: float = 60.0) -> TraceParams:
+    """Trace parameters of the reference's CameraView (camera_view.h: right = -row 0, up = row 1,
+    forward = row 2 of the rotation) through get_trace_params (dag_tracer.cu:59-101), world
+    coordinates mapped from [bounds_min, bounds_max] onto the 2^levels voxel grid."""
+    pos = np.asarray(position, dtype=np.float32).astype(np.float64)
+    m = np.asarray(rotation, dtype=np.float32).reshape(3, 3).astype(np.float64)
+    right, up, fwd = -m[0], m[1], m[2]
+    fov = fov_degrees / 2.0 * (math.pi / 180.0)
+    aspect = float(width) / float(height)
+    X = right * math.sin(fov) * aspect
+    Y = up * math.sin(fov)
+    Z = fwd * math.cos(fov)
+    bl, br, tl = pos + Z - Y - X, pos + Z - Y + X, pos + Z + Y - X
+    bmin, bmax = np.asarray(bounds_min, dtype=np.float64), np.asarray(bounds_max, dtype=np.float64)
+    scale = float(1 << levels) / (bmax - bmin)
+    pos, bl, br, tl = [(v - bmin) * scale for v in (pos, bl, br, tl)]
+    p = TraceParams()
+    p.camera[:] = list(pos)
+    p.ray_min[:] = list(bl)
+    p.ray_ddx[:] = list((br - bl) * (1.0 / width))
+    p.ray_ddy[:] = list((tl - bl) * (1.0 / height))
+    p.width, p.height = width, height
+    return p
+
+
+def replay_frames(actions, width: int, height: int, levels: int, bounds_min, bounds_max, position=(0.0, 0.0, 0.0),
+                  rotation=(1, 0, 0, 0, 1, 0, 0, 0, 1)) -> list:
+    """One TraceParams per EndFrame, from the camera the SetLocation/SetRotation actions before it
+    left (the reference's view starts at the origin with the identity rotation, camera_view.h)."""
+    pos, rot = list(position), list(rotation)
+    out = []
+    for a in actions:
+        if a.kind == REPLAY_CAMERA_LOCATION:
+            pos = list(a.camera[:3])
+        elif a.kind == REPLAY_CAMERA_ROTATION:
+            rot = list(a.camera[:9])
+        elif a.kind == REPLAY_END_FRAME:
+            out.append(view_trace_params(pos, rot, width, height, levels, bounds_min, bounds_max))
+    return out

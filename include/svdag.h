@@ -409,6 +409,48 @@ svdag_status svdag_server_frame(svdag_server* server, svdag_hit* out, uint64_t c
  * are visible, with results[0 .. n_edits) for the edits and results[n_edits ..) for the frames. */
 svdag_status svdag_server_replay(svdag_server* server, const svdag_edit* edits, const double* edit_times, uint32_t n_edits,
     const double* frame_times, uint32_t n_frames, svdag_request_result* results);
+/* An undo (redo = 0) or redo (redo = 1) request: MyGPUHashDAGUndoRedo::undo/redo
+ * (my_gpu_base_dag.h:35-64) applied after every edit submitted before it and before every edit
+ * submitted after it. Its result has kind 2 (undo) or 3 (redo) and the root it left. */
+svdag_status svdag_submit_undo(svdag_server* server, int redo, uint64_t* out_ticket);
+
+/* ---------------------------------------------------------------- recorded edit sessions */
+
+/* The reference's replay files (ReplayManager::load_csv, replay.h:650-683): one action per line, the
+ * action name then comma-separated values, trailing empty cells ignored; text after the last newline
+ * is ignored, as load_csv ignores it. */
+typedef enum svdag_replay_kind {
+    SVDAG_REPLAY_OTHER = 0, /* SetToolParameters, EditFill (CPU HashDAG only): no GPU request */
+    SVDAG_REPLAY_EDIT = 1, /* EditSphere, EditCube, EditPaint, EditCopy */
+    SVDAG_REPLAY_UNDO = 2,
+    SVDAG_REPLAY_REDO = 3,
+    SVDAG_REPLAY_END_FRAME = 4,
+    SVDAG_REPLAY_CAMERA_LOCATION = 5, /* SetLocation: camera[0..3) world position */
+    SVDAG_REPLAY_CAMERA_ROTATION = 6 /* SetRotation: camera[0..9) rows D00..D22 of the view matrix */
+} svdag_replay_kind;
+
+typedef struct svdag_replay_action {
+    uint32_t kind; /* svdag_replay_kind */
+    svdag_edit edit; /* SVDAG_REPLAY_EDIT: the editor the reference's apply() builds (replay.cpp:52-134) */
+    float camera[9];
+} svdag_replay_action;
+
+/* Parses a replay file held in memory. Edit positions and radii are multiplied by `scale` (the
+ * reference's scalingFactor = 2^SCENE_DEPTH / 2^REPLAY_DEPTH, replay.cpp:10), colours are dropped
+ * (the DAG stores materials), materials default to 1 as in the reference's loaders (replay.h:288-541).
+ * Writes min(count, capacity) actions; *count is the number parsed. A line the reference's loaders
+ * would reject (unknown action, wrong cell count, a number or boolean that does not parse) or a
+ * material >= SVDAG_NUM_MATERIALS gives SVDAG_ERR_INVALID with its 0-based index in *bad_line (may
+ * be NULL); more actions than a nonzero capacity gives SVDAG_ERR_OOM. */
+svdag_status svdag_replay_parse(const char* text, uint64_t length, float scale, svdag_replay_action* out, uint64_t capacity,
+    uint64_t* count, uint64_t* bad_line);
+/* Serves a parsed replay: the actions of recorded frame f (those before its EndFrame) are submitted
+ * f * frame_period_s seconds after the call starts, in order (edits, undos, redos), and each EndFrame
+ * submits a frame request (the camera frames[f] when frames is not NULL, one per EndFrame, else the
+ * configured one), as ReplayManager::replay_frame does (replay.h:583-596). Returns when every request
+ * is visible; results[i] belongs to actions[i] (ticket 0 for actions that are not requests). */
+svdag_status svdag_server_replay_actions(svdag_server* server, const svdag_replay_action* actions, uint64_t n_actions,
+    double frame_period_s, const svdag_trace_params* frames, svdag_request_result* results);
 
 #ifdef __cplusplus
 }
