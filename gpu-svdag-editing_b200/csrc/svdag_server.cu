@@ -165,7 +165,7 @@ struct svdag_server {
         svdag_trace_params frame = cfg.frame;
         for (auto& r : pendingFrames)
             frame = r.frame;
-        if ((size_t)frame.width * frame.height > frameHits)
+        if ((size_t)frame.width * frame.height > frameHits || frame.width == 0 || frame.height == 0)
             frame = cfg.frame;
         SVDAG_CUDA(cudaMemcpyAsync(frameRoot, &ctx->ctl->root, sizeof(uint32_t), cudaMemcpyDeviceToDevice, frameStream));
         SVDAG_TRY(trace_frame(ctx, &frame, hits, frameRoot, frameStream));
@@ -296,7 +296,7 @@ struct svdag_server {
             }
             std::vector<Request> one { r };
             svdag_status st = SVDAG_OK;
-            if (r.kind == 0)
+            if (r.kind != 1) // an edit, undo or redo
                 st = launch_batch(one, r.reserve);
             else
                 pendingFrames.push_back(r);
@@ -305,7 +305,7 @@ struct svdag_server {
             if (st == SVDAG_OK && cudaEventSynchronize(frameDone) != cudaSuccess)
                 st = SVDAG_ERR_CUDA;
             if (st != SVDAG_OK) {
-                if (r.kind == 0 && batches.empty()) {
+                if (r.kind != 1 && batches.empty()) {
                     std::lock_guard<std::mutex> lk(m);
                     fail_requests(one, st);
                 }
