@@ -21,6 +21,8 @@
 // bucket is allocated with the table (HASH_TABLE_STORE_SLABS_IN_TABLE, gpu_hash_table_base.h:30-49);
 // overflow slabs come from bump allocators over the two regions and are linked at the chain's tail.
 #pragma once
+#include <cooperative_groups.h>
+#include <cooperative_groups/scan.h>
 #include <cstdint>
 
 #include "../../include/svdag.h"
@@ -301,11 +303,32 @@ __device__ __forceinline__ void hash_words(const uint32_t* w, uint32_t n, uint32
     hb = tag_hash(a);
 }
 
+// The tag words of a probed header as the lanes of a group loaded them: with G lanes, lane l holds
+// words first(l) .. first(l) + N - 1 (G = 1: all six; G >= 8: word l). A claim starts its
+// compare-and-swap from the probed value instead of reading the word again.
+template <int G>
+struct HdrSnap {
+    static constexpr int N = G == 1 ? 6 : (G == 2 ? 4 : (G == 4 ? 2 : 1));
+    uint32_t w[N];
+    static __device__ __forceinline__ uint32_t first(uint32_t lane) { return G == 1 ? 0u : (G == 2 ? 4u * lane : (G == 4 ? 2u * lane : lane)); }
+    static __device__ __forceinline__ uint32_t owner(uint32_t word) { return G == 1 ? 0u : (G == 2 ? word / 4u : (G == 4 ? word / 2u : word)); }
+    __device__ __forceinline__ uint32_t get(uint32_t word, uint32_t lane) const
+    {
+        const uint32_t j = word - first(lane);
+        uint32_t v = 0;
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+            v = j == uint32_t(i) ? w[i] : v;
+        return v;
+    }
+};
+
 // Loads the 8 header words of a slab. Returns the candidate mask of slots whose tag byte equals
-// `tag` (24 bits), with the body handle, the next header id and the mask of free slots.
+// `tag` (24 bits), with the body handle, the next header id and the mask of free slots; `snap`
+// (optional) receives the tag words.
 template <int G, bool CG = false>
 __device__ __forceinline__ uint32_t probe_header(const Grp<G>& g, const uint32_t* hdr, uint32_t tag, uint32_t& next, uint32_t& body,
-    uint32_t& emptyMask)
+    uint32_t& emptyMask, HdrSnap<G>* snap = nullptr)
 {
     const uint32_t tag4 = tag * 0x01010101u;
     uint32_t cand = 0, empty = 0;
@@ -329,6 +352,14 @@ __device__ __forceinline__ uint32_t probe_header(const Grp<G>& g, const uint32_t
         account(5, b.y);
         bd = b.z;
         nx = b.w;
+        if (snap) {
+            snap->w[0] = a.x;
+            snap->w[1] = a.y;
+            snap->w[2] = a.z;
+            snap->w[3] = a.w;
+            snap->w[4] = b.x;
+            snap->w[5] = b.y;
+        }
     } else if constexpr (G == 2) {
         const uint4 a = CG ? __ldcg(reinterpret_cast<const uint4*>(hdr) + g.lane) : reinterpret_cast<const uint4*>(hdr)[g.lane];
         account(4 * g.lane + 0, a.x);
@@ -337,12 +368,22 @@ __device__ __forceinline__ uint32_t probe_header(const Grp<G>& g, const uint32_t
         account(4 * g.lane + 3, a.w);
         bd = g.bcast(a.z, 1);
         nx = g.bcast(a.w, 1);
+        if (snap) {
+            snap->w[0] = a.x;
+            snap->w[1] = a.y;
+            snap->w[2 % HdrSnap<G>::N] = a.z;
+            snap->w[3 % HdrSnap<G>::N] = a.w;
+        }
     } else if constexpr (G == 4) {
         const uint2 a = CG ? __ldcg(reinterpret_cast<const uint2*>(hdr) + g.lane) : reinterpret_cast<const uint2*>(hdr)[g.lane];
         account(2 * g.lane + 0, a.x);
         account(2 * g.lane + 1, a.y);
         bd = g.bcast(a.x, 3);
         nx = g.bcast(a.y, 3);
+        if (snap) {
+            snap->w[0] = a.x;
+            snap->w[1 % HdrSnap<G>::N] = a.y;
+        }
     } else {
         uint32_t x = 0;
         if (g.lane < 8)
@@ -351,6 +392,8 @@ __device__ __forceinline__ uint32_t probe_header(const Grp<G>& g, const uint32_t
             account(g.lane, x);
         bd = g.bcast(x, 6);
         nx = g.bcast(x, 7);
+        if (snap)
+            snap->w[0] = x;
     }
     next = nx;
     body = bd;
@@ -375,11 +418,18 @@ __device__ __forceinline__ bool item_equals(const Grp<G>& g, const uint32_t* ite
 template <int G>
 __device__ __forceinline__ void write_item(const Grp<G>& g, uint32_t* item, const Key<G>& key)
 {
+    if constexpr (G == 1) { // word pairs; the pad word of an odd-length item is written as zero
 #pragma unroll
-    for (int i = 0; i < Grp<G>::KW; ++i) {
-        const uint32_t idx = g.lane + uint32_t(i) * G;
-        if (idx < key.n)
-            item[idx] = key.w[i];
+        for (uint32_t i = 0; i < kItemStride; i += 2)
+            if (i < key.n)
+                *reinterpret_cast<uint2*>(item + i) = make_uint2(key.w[i], i + 1 < key.n ? key.w[i + 1] : 0u);
+    } else {
+#pragma unroll
+        for (int i = 0; i < Grp<G>::KW; ++i) {
+            const uint32_t idx = g.lane + uint32_t(i) * G;
+            if (idx < key.n)
+                item[idx] = key.w[i];
+        }
     }
 }
 
@@ -395,9 +445,20 @@ __device__ __forceinline__ uint32_t alloc_slab(const Grp<G>& g, const DevDag& d,
 {
     uint32_t id = kNone, body = 0;
     if (g.lane == 0) {
-        const unsigned long long hid = atomicAdd(&d.ctl->headerTop, 1ull);
+        // The groups of a warp that allocate at the same time share one atomic per region (the
+        // bump pointers are single addresses every allocation in the launch goes through).
+        namespace cg = cooperative_groups;
+        const cg::coalesced_group leaders = cg::coalesced_threads();
         const unsigned long long w = body_words(k);
-        const unsigned long long o = atomicAdd(&d.ctl->itemTop, w);
+        const unsigned long long before = cg::exclusive_scan(leaders, w);
+        const unsigned long long total = leaders.shfl(before + w, leaders.num_threads() - 1);
+        unsigned long long hbase = 0, obase = 0;
+        if (leaders.thread_rank() == 0) {
+            hbase = atomicAdd(&d.ctl->headerTop, (unsigned long long)leaders.num_threads());
+            obase = atomicAdd(&d.ctl->itemTop, total);
+        }
+        const unsigned long long hid = leaders.shfl(hbase, 0) + leaders.thread_rank();
+        const unsigned long long o = leaders.shfl(obase, 0) + before;
         if (hid < d.headerCount && o + w <= d.itemWords) {
             id = (uint32_t)hid;
             body = (uint32_t)(o >> 1); // itemTop stays a multiple of 8 words
@@ -478,7 +539,7 @@ __device__ __forceinline__ uint32_t table_find(const Grp<G>& g, const DevDag& d,
 // `busy` claims with the in-flight tag (published later), otherwise with the final tag.
 template <int G>
 __device__ __forceinline__ uint32_t claim_in_slab(const Grp<G>& g, const DevDag& d, uint32_t slab, uint32_t body, uint32_t emptyMask,
-    uint32_t tag, uint32_t n, bool busy, uint32_t& slot, uint32_t spread)
+    uint32_t tag, uint32_t n, bool busy, uint32_t& slot, uint32_t spread, const HdrSnap<G>* snap = nullptr)
 {
     // Claimants of one slab start at different free slots (`spread` is a hash of the key), so that
     // they do not all race for the first free slot of the same snapshot.
@@ -488,9 +549,12 @@ __device__ __forceinline__ uint32_t claim_in_slab(const Grp<G>& g, const DevDag&
         const uint32_t s = up ? start + (uint32_t)__ffs(up) - 1u : (uint32_t)__ffs(emptyMask) - 1u;
         const uint32_t word = s >> 2, shift = 8u * (s & 3u);
         uint32_t got = 0;
-        if (g.lane == 0) {
+        // The lane that probed the tag word claims (its probed value is the first guess; a stale
+        // guess only costs one failed compare-and-swap, which returns the current word).
+        const uint32_t claimer = snap ? HdrSnap<G>::owner(word) : 0u;
+        if (g.lane == claimer) {
             uint32_t* p = slab_ptr(d, slab) + word;
-            uint32_t cur = *reinterpret_cast<volatile uint32_t*>(p);
+            uint32_t cur = snap ? snap->get(word, g.lane) : *reinterpret_cast<volatile uint32_t*>(p);
             for (;;) {
                 if ((cur >> shift) & 0xFFu)
                     break; // taken meanwhile
@@ -503,7 +567,7 @@ __device__ __forceinline__ uint32_t claim_in_slab(const Grp<G>& g, const DevDag&
                 cur = old;
             }
         }
-        got = g.bcast(got, 0);
+        got = g.bcast(got, claimer);
         if (got) {
             slot = s;
             return slot_handle(body, s, n);
@@ -527,8 +591,9 @@ __device__ __forceinline__ uint32_t table_add(const Grp<G>& g, const DevDag& d, 
     uint32_t slab = first_slab(t, cls, key.ha);
     for (uint32_t steps = 0; steps < kMaxChain; ++steps) {
         uint32_t next, body, empty, slot;
-        probe_header<G>(g, slab_ptr(d, slab), tag, next, body, empty);
-        const uint32_t item = claim_in_slab<G>(g, d, slab, body, empty, tag, key.n, false, slot, key.ha >> 8);
+        HdrSnap<G> snap;
+        probe_header<G>(g, slab_ptr(d, slab), tag, next, body, empty, &snap);
+        const uint32_t item = claim_in_slab<G>(g, d, slab, body, empty, tag, key.n, false, slot, key.ha >> 8, &snap);
         if (item != kNone) {
             write_item<G>(g, handle_ptr(d, item), key);
             return item;
@@ -574,13 +639,14 @@ __device__ __forceinline__ uint32_t table_find_or_insert(const Grp<G>& g, const 
     const uint32_t tag = tag_of(key.hb);
     uint32_t slab = first_slab(t, cls, key.ha);
     uint32_t tail = slab, tailEmpty = 0, tailBody = 0;
+    HdrSnap<G> snap;
     for (uint32_t steps = 0;; ++steps) {
         if (steps >= kMaxChain) {
             set_status(d.ctl, SVDAG_ERR_CORRUPT);
             return kNone;
         }
         uint32_t next, body, empty;
-        uint32_t cand = probe_header<G, true>(g, slab_ptr(d, slab), tag, next, body, empty);
+        uint32_t cand = probe_header<G, true>(g, slab_ptr(d, slab), tag, next, body, empty, &snap);
         while (cand) {
             const uint32_t s = __ffs(cand) - 1u;
             cand &= cand - 1u;
@@ -604,7 +670,7 @@ __device__ __forceinline__ uint32_t table_find_or_insert(const Grp<G>& g, const 
     uint32_t empty = tailEmpty, body = tailBody;
     for (uint32_t steps = 0; steps < kMaxChain; ++steps) {
         uint32_t s = 0;
-        const uint32_t item = claim_in_slab<G>(g, d, slab, body, empty, tag, key.n, true, s, key.ha >> 8);
+        const uint32_t item = claim_in_slab<G>(g, d, slab, body, empty, tag, key.n, true, s, key.ha >> 8, &snap);
         if (item != kNone) {
             write_item<G>(g, handle_ptr(d, item), key);
             __threadfence();
@@ -615,7 +681,7 @@ __device__ __forceinline__ uint32_t table_find_or_insert(const Grp<G>& g, const 
             return item;
         }
         uint32_t next;
-        probe_header<G, true>(g, slab_ptr(d, slab), tag, next, body, empty);
+        probe_header<G, true>(g, slab_ptr(d, slab), tag, next, body, empty, &snap);
         if (empty)
             continue; // a slot was freed up meanwhile (cannot happen during edits, kept for safety)
         if (next == kEnd) {
@@ -638,7 +704,7 @@ __device__ __forceinline__ uint32_t table_find_or_insert(const Grp<G>& g, const 
             return kNone;
         }
         slab = next;
-        probe_header<G, true>(g, slab_ptr(d, slab), tag, next, body, empty);
+        probe_header<G, true>(g, slab_ptr(d, slab), tag, next, body, empty, &snap);
     }
     set_status(d.ctl, SVDAG_ERR_TIMEOUT);
     return kNone;

@@ -170,9 +170,9 @@ __global__ void __launch_bounds__(256) k_table_op(DevDag d, DevTable t, const ui
 {
     Grp<G> g;
     const uint32_t groupsPerBlock = blockDim.x / G;
-    const uint32_t stride = gridDim.x * groupsPerBlock;
+    const unsigned long long stride = (unsigned long long)gridDim.x * groupsPerBlock;
     Spare spare;
-    for (uint32_t i = blockIdx.x * groupsPerBlock + threadIdx.x / G; i < n; i += stride) {
+    for (unsigned long long i = blockIdx.x * groupsPerBlock + threadIdx.x / G; i < n; i += stride) {
         if (reps && reps[i] != i)
             continue;
         const uint32_t off = offsets[i];
