@@ -166,9 +166,9 @@ def gather_keys(words, offs, sizes, order):
     return words[idx], o.astype(np.uint32), s
 
 
-def run_hash_bench(svdag, torch, stream, n_total=1 << 24, load_factor=20, lanes=1, reps=3, pool=6 << 30):
+def run_hash_bench(svdag, torch, stream, n_total=1 << 24, load_factor=16, lanes=1, reps=3, pool=6 << 30):
     """Insert 2^24 keys (50% duplicates, stored twice as the reference's add does), then 2^24 finds
-    (50% hits). Algorithmic bytes (per key of k words): find 4k + 32 + 4k*hit + 4, insert 4k + 32 + 4k + 4."""
+    (50% hits). 16 stored items per bucket gives the configuration's 2^20 buckets. Algorithmic bytes (per key of k words): find 4k + 32 + 4k*hit + 4, insert 4k + 32 + 4k + 4."""
     n_unique = n_total // 2
     words, offs, sizes = c1_keys(n_unique)
     rng = np.random.default_rng(3)
@@ -650,7 +650,7 @@ def main():
     ap.add_argument("--no-hash", action="store_true")
     ap.add_argument("--hash-keys", type=int, default=1 << 24)
     ap.add_argument("--hash-lanes", type=int, default=1)
-    ap.add_argument("--hash-lf", type=int, default=20)
+    ap.add_argument("--hash-lf", type=int, default=16)
     ap.add_argument("--hash-reps", type=int, default=3)
     ap.add_argument("--hash-pool", type=int, default=6 << 30)
     args = ap.parse_args()

@@ -251,9 +251,15 @@ __device__ __forceinline__ void load_key(const Grp<G>& g, const uint32_t* p, uns
         // All ten words are requested at once (one memory round trip instead of two: the length is
         // only known from the first words) and trimmed to the key's length afterwards.
         uint32_t v[kItemStride];
+        if (limit >= kItemStride) { // all but the last keys of an array: no per-word bound
 #pragma unroll
-        for (uint32_t i = 0; i < kItemStride; ++i)
-            v[i] = i < limit ? ld<MODE>(p + i) : 0u;
+            for (uint32_t i = 0; i < kItemStride; ++i)
+                v[i] = ld<MODE>(p + i);
+        } else {
+#pragma unroll
+            for (uint32_t i = 0; i < kItemStride; ++i)
+                v[i] = i < limit ? ld<MODE>(p + i) : 0u;
+        }
         key.n = kind == SVDAG_KIND_NODE ? dev_node_words(v[0]) : dev_leaf_words(v[0], v[1]);
         uint32_t a = 0;
 #pragma unroll
@@ -324,26 +330,37 @@ struct HdrSnap {
 };
 
 // Loads the 8 header words of a slab. Returns the candidate mask of slots whose tag byte equals
-// `tag` (24 bits), with the body handle, the next header id and the mask of free slots; `snap`
-// (optional) receives the tag words.
-template <int G, bool CG = false>
+// `tag` (24 bits), with the body handle, the next header id and (EMPTY) the mask of free slots;
+// `snap` (optional) receives the tag words. A single thread reads the 32-byte header with one
+// 256-bit load (headers are 32-byte aligned).
+template <int G, bool CG = false, bool EMPTY = true>
 __device__ __forceinline__ uint32_t probe_header(const Grp<G>& g, const uint32_t* hdr, uint32_t tag, uint32_t& next, uint32_t& body,
     uint32_t& emptyMask, HdrSnap<G>* snap = nullptr)
 {
     const uint32_t tag4 = tag * 0x01010101u;
     uint32_t cand = 0, empty = 0;
-    // bytes of 0xFF/0x00 -> 4-bit mask: the multiply gathers bit 7 of every byte into bits 28..31
-    auto bytes = [](uint32_t v) { return ((v & 0x80808080u) * 0x00204081u) >> 28; };
+    // bit 7 of each byte set exactly where that byte of v is zero (the adds carry within a byte only)
+    auto zero_bytes = [](uint32_t v) { return ~(((v & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | v | 0x7F7F7F7Fu); };
+    // bits 7, 15, 23, 31 -> bits 28..31: the partial products of the multiply never overlap
+    auto gather = [](uint32_t m) { return (m * 0x00204081u) >> 28; };
     auto account = [&](uint32_t word, uint32_t x) {
         if (word < 6) {
-            cand |= bytes(__vcmpeq4(x, tag4)) << (4 * word);
-            empty |= bytes(__vcmpeq4(x, 0u)) << (4 * word);
+            cand |= gather(zero_bytes(x ^ tag4)) << (4 * word);
+            if constexpr (EMPTY)
+                empty |= gather(zero_bytes(x)) << (4 * word);
         }
     };
     uint32_t nx = 0, bd = 0;
     if constexpr (G == 1) {
-        const uint4 a = CG ? __ldcg(reinterpret_cast<const uint4*>(hdr)) : reinterpret_cast<const uint4*>(hdr)[0];
-        const uint4 b = CG ? __ldcg(reinterpret_cast<const uint4*>(hdr) + 1) : reinterpret_cast<const uint4*>(hdr)[1];
+        uint4 a, b;
+        if constexpr (CG) {
+            a = __ldcg(reinterpret_cast<const uint4*>(hdr));
+            b = __ldcg(reinterpret_cast<const uint4*>(hdr) + 1);
+        } else {
+            asm("ld.global.v8.u32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                : "=r"(a.x), "=r"(a.y), "=r"(a.z), "=r"(a.w), "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
+                : "l"(hdr));
+        }
         account(0, a.x);
         account(1, a.y);
         account(2, a.z);
@@ -517,7 +534,7 @@ __device__ __forceinline__ uint32_t table_find(const Grp<G>& g, const DevDag& d,
             return kNone;
         }
         uint32_t next, body, empty;
-        uint32_t cand = probe_header<G>(g, slab_ptr(d, slab), tag, next, body, empty);
+        uint32_t cand = probe_header<G, false, false>(g, slab_ptr(d, slab), tag, next, body, empty);
         while (cand) {
             const uint32_t s = __ffs(cand) - 1u;
             cand &= cand - 1u;
