@@ -184,6 +184,9 @@ _PROTOS = {
     "svdag_submit_undo": [_P, C.c_int, C.POINTER(_U64)],
     "svdag_replay_parse": [C.c_char_p, _U64, C.c_float, _P, _U64, C.POINTER(_U64), C.POINTER(_U64)],
     "svdag_server_replay_actions": [_P, _P, _U64, C.c_double, _P, _P],
+    "svdag_save_items": [_P, _P, _U64, _P, _P, C.POINTER(_U64), _P],
+    "svdag_load_items": [_P, _P, _P, _P, _P],
+    "svdag_basic_dag_to_items": [_P, _U64, _U32, _U32, _P, _U64, _P, _P, C.POINTER(_U64)],
 }
 EXPORTED = tuple(_PROTOS)
 
@@ -455,6 +458,134 @@ class MyGPUHashDAG:
             _check(lib().svdag_export_level(self.h, level, handles.ctypes.data, words.ctypes.data, cap, C.byref(n),
                                             None), "svdag_export_level")
         return handles[: n.value], words[: n.value]
+
+    def save_items(self, stream=None) -> "ItemSnapshot":
+        """The items reachable from the root as an item snapshot (svdag_save_items); stands in for
+        MyGPUHashDAG::writeTo (my_gpu_hash_dag.cu:158-165)."""
+        nl = self.levels - 1
+        lw, li, total = np.zeros(nl, np.uint64), np.zeros(nl, np.uint64), C.c_uint64()
+        words = np.zeros(0, np.uint32)
+        while True:
+            st = lib().svdag_save_items(self.h, words.ctypes.data if len(words) else None, len(words), lw.ctypes.data,
+                                        li.ctypes.data, C.byref(total), stream_ptr(stream))
+            if st == 2 and total.value > len(words):
+                words = np.zeros(total.value, np.uint32)
+                continue
+            _check(st, "svdag_save_items")
+            return ItemSnapshot(self.levels, words[: total.value], lw, li)
+
+    def load_items(self, snap: "ItemSnapshot", stream=None):
+        """Replaces the DAG by an item snapshot (svdag_load_items); stands in for
+        MyGPUHashDAG::readFrom (my_gpu_hash_dag.cu:167-177)."""
+        if snap.levels != self.levels:
+            raise SvdagError(1, f"svdag_load_items: snapshot of {snap.levels} levels, DAG of {self.levels}")
+        w = np.ascontiguousarray(snap.words, dtype=np.uint32)
+        lw = np.ascontiguousarray(snap.level_words, dtype=np.uint64)
+        li = np.ascontiguousarray(snap.level_items, dtype=np.uint64)
+        _check(lib().svdag_load_items(self.h, w.ctypes.data if len(w) else None, lw.ctypes.data, li.ctypes.data,
+                                      stream_ptr(stream)), "svdag_load_items")
+
+    def write_to(self, path: str):
+        self.save_items().write(path)
+
+    def read_from(self, path: str):
+        self.load_items(ItemSnapshot.read(path))
+
+    def load_basic_dag(self, path: str, material: int = 0) -> "BasicDAGFile":
+        """Loads a BasicDAG geometry file of the reference (BasicDAGFactory::load_dag_from_file,
+        basic_dag.cpp:108-122) with every voxel of `material`; returns the file's header."""
+        f = BasicDAGFile.read(path)
+        if f.levels != self.levels:
+            raise SvdagError(1, f"BasicDAG of {f.levels} levels, DAG of {self.levels}")
+        self.load_items(basic_dag_to_items(f.data, f.levels, material))
+        return f
+
+
+@dataclass
+class ItemSnapshot:
+    """Per-level item lists of a DAG (include/svdag.h, "import and export"). The file form is
+    b"SVDAGIT1", u32 version 1, u32 levels, u64 level_words[levels-1], u64 level_items[levels-1],
+    then the words, all little-endian."""
+    levels: int
+    words: np.ndarray
+    level_words: np.ndarray
+    level_items: np.ndarray
+
+    MAGIC = b"SVDAGIT1"
+
+    def write(self, path: str):
+        with open(path, "wb") as f:
+            f.write(self.MAGIC)
+            f.write(np.array([1, self.levels], dtype="<u4").tobytes())
+            f.write(np.asarray(self.level_words, dtype="<u8").tobytes())
+            f.write(np.asarray(self.level_items, dtype="<u8").tobytes())
+            f.write(np.asarray(self.words, dtype="<u4").tobytes())
+
+    @classmethod
+    def read(cls, path: str) -> "ItemSnapshot":
+        with open(path, "rb") as f:
+            data = f.read()
+        if data[:8] != cls.MAGIC:
+            raise SvdagError(1, f"{path}: not an item snapshot")
+        version, levels = np.frombuffer(data, "<u4", 2, 8)
+        if version != 1 or not 4 <= levels <= MAX_LEVELS:
+            raise SvdagError(1, f"{path}: version {version}, levels {levels}")
+        nl = int(levels) - 1
+        lw = np.frombuffer(data, "<u8", nl, 16).copy()
+        li = np.frombuffer(data, "<u8", nl, 16 + 8 * nl).copy()
+        at = 16 + 16 * nl
+        total = int(lw.sum())
+        if len(data) != at + 4 * total:
+            raise SvdagError(1, f"{path}: {len(data)} bytes, expected {at + 4 * total}")
+        return cls(int(levels), np.frombuffer(data, "<u4", total, at).copy(), lw, li)
+
+
+@dataclass
+class BasicDAGFile:
+    """The reference's BasicDAG file (BasicDAGFactory::save_dag_to_file, basic_dag.cpp:95-106, through
+    FileWriter, serializer.h:12-61): DAGInfo as six doubles (AABB min, max), u32 levels, u64 word
+    count, then the node words."""
+    bounds_min: tuple
+    bounds_max: tuple
+    levels: int
+    data: np.ndarray
+
+    def write(self, path: str):
+        with open(path, "wb") as f:
+            f.write(np.array(list(self.bounds_min) + list(self.bounds_max), dtype="<f8").tobytes())
+            f.write(np.array([self.levels], dtype="<u4").tobytes())
+            f.write(np.array([len(self.data)], dtype="<u8").tobytes())
+            f.write(np.asarray(self.data, dtype="<u4").tobytes())
+
+    @classmethod
+    def read(cls, path: str) -> "BasicDAGFile":
+        with open(path, "rb") as f:
+            data = f.read()
+        if len(data) < 60:
+            raise SvdagError(1, f"{path}: too short for a BasicDAG file")
+        b = np.frombuffer(data, "<f8", 6, 0)
+        levels = int(np.frombuffer(data, "<u4", 1, 48)[0])
+        n = int(np.frombuffer(data, "<u8", 1, 52)[0])
+        if len(data) != 60 + 4 * n:
+            raise SvdagError(1, f"{path}: {len(data)} bytes, expected {60 + 4 * n}")
+        return cls(tuple(float(v) for v in b[:3]), tuple(float(v) for v in b[3:]), levels,
+                   np.frombuffer(data, "<u4", n, 60).copy())
+
+
+def basic_dag_to_items(data, levels: int, material: int = 0) -> ItemSnapshot:
+    """BasicDAG node words -> item snapshot, every voxel of `material` (svdag_basic_dag_to_items, a
+    host function: create_dag_cpu without colour import, my_gpu_hash_dag_factory.cpp:316-418)."""
+    d = np.ascontiguousarray(data, dtype=np.uint32)
+    nl = levels - 1
+    lw, li, total = np.zeros(nl, np.uint64), np.zeros(nl, np.uint64), C.c_uint64()
+    st = lib().svdag_basic_dag_to_items(d.ctypes.data, len(d), levels, material, None, 0, lw.ctypes.data, li.ctypes.data,
+                                        C.byref(total))
+    if st not in (0, 2):
+        _check(st, "svdag_basic_dag_to_items")
+    words = np.zeros(max(total.value, 1), np.uint32)
+    _check(lib().svdag_basic_dag_to_items(d.ctypes.data, len(d), levels, material, words.ctypes.data, len(words),
+                                          lw.ctypes.data, li.ctypes.data, C.byref(total)), "svdag_basic_dag_to_items")
+    return ItemSnapshot(levels, words[: total.value], lw, li)
 
 
 class HashTable:

@@ -327,6 +327,35 @@ svdag_status svdag_get_stats(svdag_ctx* ctx, svdag_stats* out, void* stream);
 svdag_status svdag_export_level(svdag_ctx* ctx, uint32_t level, uint32_t* out_handles, uint32_t* out_words,
     uint64_t capacity, uint64_t* out_count, void* stream);
 
+/* ---------------------------------------------------------------- import and export */
+
+/* An item snapshot: level l (0 .. levels-2) holds level_items[l] items packed in level_words[l]
+ * words (nodes: header + one word per child; leaves: 2 mask words + packed 4-bit materials), the
+ * levels one after another. A node's child words are ordinals into the item list of the level below
+ * and item 0 of level 0 is the root; all counts 0 is the empty DAG. Snapshots stand in for
+ * MyGPUHashDAG::writeTo / readFrom (my_gpu_hash_dag.cu:158-177), whose raw table dump only the same
+ * table layout can read back. */
+
+/* Writes the items reachable from the current root, each level in ascending handle order. Fills
+ * level_words and level_items (levels - 1 entries each) and *total_words; writes the words when
+ * capacity suffices, else returns SVDAG_ERR_OOM (call again with capacity >= *total_words).
+ * Synchronous. */
+svdag_status svdag_save_items(svdag_ctx* ctx, uint32_t* out_words, uint64_t capacity, uint64_t* level_words,
+    uint64_t* level_items, uint64_t* total_words, void* stream);
+/* Replaces the DAG by a snapshot: history cleared, each level table sized for its distinct items,
+ * fully-filled items deduplicated against the canonical ones. A snapshot that does not parse (item
+ * sizes, counts, child ordinals) gives SVDAG_ERR_INVALID and leaves the DAG unchanged. Synchronous. */
+svdag_status svdag_load_items(svdag_ctx* ctx, const uint32_t* words, const uint64_t* level_words, const uint64_t* level_items,
+    void* stream);
+/* Host function: converts the node array of a BasicDAG (BasicDAG::data, basic_dag.h: root at index
+ * 0, inner nodes [child mask in bits 0-7 | child indices], 64-bit leaves {low, high} at level
+ * levels - 2) into a snapshot as create_dag_cpu converts it without colour import
+ * (my_gpu_hash_dag_factory.cpp:316-418): every voxel gets `material`, and a node whose 8 children are
+ * fully filled with one material carries the fully-filled header. Output as svdag_save_items; an
+ * index out of range or an empty item gives SVDAG_ERR_CORRUPT. */
+svdag_status svdag_basic_dag_to_items(const uint32_t* data, uint64_t n_words, uint32_t levels, uint32_t material,
+    uint32_t* out_words, uint64_t capacity, uint64_t* level_words, uint64_t* level_items, uint64_t* total_words);
+
 /* ---------------------------------------------------------------- autotuner
  *
  * Picks the settings of the batched form by measuring them on the device (no counterpart in the
