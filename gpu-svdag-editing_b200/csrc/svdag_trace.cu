@@ -9,6 +9,8 @@
 // a slab-table decode.
 #include <cuda_runtime.h>
 
+#include <cmath>
+
 #include "svdag_host.hpp"
 
 namespace svdag {
@@ -24,7 +26,7 @@ __device__ __forceinline__ float cminf(float a, float b) { return a < b ? a : b;
 // compute_intersection_mask, tracer.cu:56-173 (device max/min of two floats are fmaxf/fminf; the
 // vector max/min of cuda_math.h are the ternary forms).
 __device__ __forceinline__ uint32_t intersection_mask(bool isRoot, uint32_t level, uint32_t px, uint32_t py, uint32_t pz, uint32_t levels,
-    const RayF& r)
+    const RayF& r, float rayTmax = 3.402823466e+38f)
 {
     const uint32_t shift = levels - level;
     const float radius = float(1u << (shift - 1));
@@ -38,7 +40,7 @@ __device__ __forceinline__ uint32_t intersection_mask(bool isRoot, uint32_t leve
         tmax = cminf(tmx + sx, cminf(tmy + sy, tmz + sz));
     }
     tmin = fmaxf(tmin, 0.0f); // ray.tmin
-    tmax = fminf(tmax, 3.402823466e+38f); // ray.tmax
+    tmax = fminf(tmax, rayTmax); // ray.tmax
     if (isRoot && (tmin >= tmax))
         return 0;
     uint32_t mask;
@@ -232,6 +234,266 @@ __global__ void __launch_bounds__(256) k_trace(DevDag d, svdag_trace_params p, s
     out[(size_t)(p.height - 1 - y) * p.width + x] = h;
 }
 
+// ---------------------------------------------------------------- shading (tracer.cu:413-730)
+
+struct ShadeDev {
+    uint32_t palette[SVDAG_NUM_MATERIALS];
+    float sun[3];
+    float bias, aoLength, sunBrightness, fog;
+    uint32_t samples, flags;
+    unsigned long long seed;
+};
+
+// intersect_ray_node_out_of_order, tracer.cu:275-352: whether any voxel lies on the ray within
+// [0, tmax]; children are taken highest index first, whatever the ray's direction.
+__device__ bool any_hit(const DevDag& d, uint32_t root, const RayF& r, float tmax, uint32_t (*sIndex)[256], uint32_t (*sMasks)[256],
+    uint32_t tix)
+{
+    if (root == kNone)
+        return false;
+    const uint32_t levels = d.levels, LL = d.leafLevel;
+    uint32_t level = 0, px = 0, py = 0, pz = 0, leafLo = 0, leafHi = 0;
+    uint32_t cIndex = root;
+    uint32_t cChild = item_ptr(d, root)[0] & 0xFFu;
+    uint32_t cVisit = cChild & intersection_mask(true, 0, 0, 0, 0, levels, r, tmax);
+    for (;;) {
+        {
+            uint32_t newLevel = level;
+            while (newLevel > 0 && !cVisit) {
+                newLevel--;
+                cIndex = sIndex[newLevel][tix];
+                cChild = sMasks[newLevel][tix] & 0xFFu;
+                cVisit = sMasks[newLevel][tix] >> 8;
+            }
+            if (newLevel == 0 && !cVisit)
+                return false;
+            const uint32_t up = level - newLevel;
+            px >>= up;
+            py >>= up;
+            pz >>= up;
+            level = newLevel;
+        }
+        const uint32_t nextChild = 31u - (uint32_t)__clz(cVisit);
+        cVisit &= ~(1u << nextChild);
+        px = (px << 1) | ((nextChild >> 2) & 1u);
+        py = (py << 1) | ((nextChild >> 1) & 1u);
+        pz = (pz << 1) | (nextChild & 1u);
+        sIndex[level][tix] = cIndex;
+        sMasks[level][tix] = cChild | (cVisit << 8);
+        level++;
+        if (level == levels)
+            return true;
+        if (level < LL) {
+            const uint32_t* node = item_ptr(d, cIndex);
+            cIndex = node[1 + __popc(cChild & ((1u << nextChild) - 1u))];
+            cChild = item_ptr(d, cIndex)[0] & 0xFFu;
+            cVisit = cChild & intersection_mask(false, level, px, py, pz, levels, r, tmax);
+        } else {
+            uint32_t childMask;
+            if (level == LL) {
+                const uint32_t* node = item_ptr(d, cIndex);
+                const uint32_t* lp = item_ptr(d, node[1 + __popc(cChild & ((1u << nextChild) - 1u))]);
+                leafLo = lp[0];
+                leafHi = lp[1];
+                childMask = first_child_mask(leafLo, leafHi);
+            } else {
+                childMask = (((nextChild & 4u) ? leafHi : leafLo) >> ((nextChild & 3u) * 8u)) & 0xFFu;
+            }
+            cChild = childMask;
+            cVisit = cChild & intersection_mask(false, level, px, py, pz, levels, r, tmax);
+        }
+    }
+}
+
+__device__ __forceinline__ RayF make_rayf(float ox, float oy, float oz, float dx, float dy, float dz) // Ray::create, tracer.cu:32-41
+{
+    RayF r;
+    r.ox = ox;
+    r.oy = oy;
+    r.oz = oz;
+    r.dx = dx;
+    r.dy = dy;
+    r.dz = dz;
+    r.ix = 1.0f / dx;
+    r.iy = 1.0f / dy;
+    r.iz = 1.0f / dz;
+    return r;
+}
+
+// Utils::PCG_RNG (utils.h:45-78): PCG-XSH-RR 32 with the stream as increment.
+struct Pcg {
+    unsigned long long state = 0x853c49e6748fea9bull, inc;
+    __device__ explicit Pcg(unsigned long long stream)
+        : inc(stream)
+    {
+        next();
+        next();
+    }
+    __device__ uint32_t next()
+    {
+        const unsigned long long old = state;
+        state = old * 6364136223846793005ull + (inc | 1ull);
+        const uint32_t xorshifted = (uint32_t)(((old >> 18u) ^ old) >> 27u);
+        const uint32_t rot = (uint32_t)(old >> 59);
+        return (xorshifted >> rot) | (xorshifted << ((0xFFFFFFFFu - rot + 1u) & 31u));
+    }
+    __device__ float next_float() { return float(next()) / 4294967296.0f; } // float(UINT32_MAX) is 2^32
+};
+
+// sin and cos of x in [0, 2 pi]: reduction by the nearest multiple of pi/2 (in double, exact for
+// these arguments to well below float precision) and the Taylor polynomials of sin (degree 9) and
+// cos (degree 8) on [-pi/4, pi/4]. The oracle evaluates the same operations in the same order, so
+// AO sample directions agree bit for bit.
+__device__ __forceinline__ void sincos_quadrant(float x, float& s, float& c)
+{
+    const float k = rintf(x * 0.63661975f);
+    const float r = (float)((double)x - (double)k * 1.5707963267948966);
+    const float r2 = r * r;
+    const float sp = r + (r * r2) * (-0.16666667f + r2 * (0.008333334f + r2 * (-0.0001984127f + r2 * 2.7557319e-06f)));
+    const float cp = 1.0f + r2 * (-0.5f + r2 * (0.041666668f + r2 * (-0.0013888889f + r2 * 2.4801588e-05f)));
+    switch ((int)k & 3) {
+    case 0:
+        s = sp;
+        c = cp;
+        break;
+    case 1:
+        s = cp;
+        c = -sp;
+        break;
+    case 2:
+        s = -sp;
+        c = -cp;
+        break;
+    default:
+        s = -cp;
+        c = sp;
+        break;
+    }
+}
+
+__device__ __forceinline__ float srgb_to_linear(float v) // ColorUtils::accurateSRGBToLinear, color_utils.h:233-242
+{
+    const float lo = v / 12.92f;
+    const float hi = powf((v + 0.055f) / 1.055f, 2.4f);
+    return (v <= 0.04045f) ? lo : hi;
+}
+__device__ __forceinline__ float linear_to_srgb(float v) // ColorUtils::accurateLinearToSRGB, :243-252
+{
+    const float lo = v * 12.92f;
+    const float hi = (powf(fabsf(v), 1.0f / 2.4f) * 1.055f) - 0.055f;
+    return (v <= 0.0031308f) ? lo : hi;
+}
+__device__ __forceinline__ uint32_t to_rgb888(float r, float g, float b) // ColorUtils::float3_to_rgb888, :31-37
+{
+    r = fmaxf(0.f, fminf(r, 1.f));
+    g = fmaxf(0.f, fminf(g, 1.f));
+    b = fmaxf(0.f, fminf(b, 1.f));
+    return (uint32_t(r * 255.0f) << 0) | (uint32_t(g * 255.0f) << 8) | (uint32_t(b * 255.0f) << 16) | 0xff000000u;
+}
+
+// One pixel: diffuse colour (trace_colors), sun shadow (trace_shadows), ambient occlusion
+// (trace_ambient_occlusion) and lighting (trace_lighting), each step in the reference's order.
+__global__ void __launch_bounds__(256) k_shade(DevDag d, svdag_trace_params tp, ShadeDev sp, svdag_hit* hits, uint32_t* rgba, float* sunOut,
+    float* aoOut)
+{
+    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t y = blockIdx.y * blockDim.y + threadIdx.y;
+    __shared__ uint32_t sIndex[kMaxLevels][256];
+    __shared__ uint32_t sMasks[kMaxLevels][256];
+    if (x >= tp.width || y >= tp.height)
+        return;
+    const uint32_t tix = threadIdx.y * blockDim.x + threadIdx.x;
+    const size_t i = (size_t)y * tp.width + x;
+    svdag_hit& si = hits[i];
+    const bool hit = si.path[0] != 0 || si.path[1] != 0 || si.path[2] != 0;
+    const uint32_t root = d.ctl->root;
+    // computeColorAtSurface (tracer.cu:413-445): black for a miss, a checker for an unknown material
+    uint32_t diffuse;
+    if (!hit) {
+        diffuse = to_rgb888(0.f, 0.f, 0.f);
+    } else if (si.material < SVDAG_NUM_MATERIALS) {
+        diffuse = sp.palette[si.material] | 0xff000000u;
+    } else {
+        const float b = float((si.path[0] ^ si.path[1] ^ si.path[2]) & 1u);
+        diffuse = to_rgb888(1.f, b, 1.f - b);
+    }
+    si.color = diffuse;
+    const float px = si.position[0], py = si.position[1], pz = si.position[2];
+    const float nx = si.normal[0], ny = si.normal[1], nz = si.normal[2];
+    float sun = 0.f, ao = 0.f;
+    if (hit && (sp.flags & SVDAG_SHADE_SHADOWS)) {
+        const RayF r = make_rayf(px + sp.bias * sp.sun[0], py + sp.bias * sp.sun[1], pz + sp.bias * sp.sun[2], sp.sun[0], sp.sun[1], sp.sun[2]);
+        const bool occluded = any_hit(d, root, r, 3.402823466e+38f, sIndex, sMasks, tix);
+        const float ndotl = fmaxf((nx * r.dx + ny * r.dy) + nz * r.dz, 0.0f);
+        sun = occluded ? 0.0f : ndotl;
+    }
+    if (hit && (sp.flags & SVDAG_SHADE_AO) && sp.samples) {
+        const unsigned long long seed = (unsigned long long)(y * tp.width + x) * (sp.seed > 1ull ? sp.seed : 1ull);
+        Pcg rng(seed);
+        uint32_t samples = 0, open = 0;
+        const float ox = px + nx * sp.bias, oy = py + ny * sp.bias, oz = pz + nz * sp.bias;
+        for (uint32_t k = 0; k < sp.samples; ++k) {
+            const float ux = rng.next_float();
+            const float uy = rng.next_float();
+            // cosineSampleHemisphere (tracer.cu:643-655)
+            const float rr = sqrtf(ux);
+            const float theta = 6.2831855f * uy;
+            float sn, cs;
+            sincos_quadrant(theta, sn, cs);
+            const float lx = rr * cs, ly = rr * sn, lz = sqrtf(fmaxf(0.0f, 1 - ux));
+            // SurfaceInteraction::transformDirectionToWorld (tracer.h:106-109)
+            const float wx = (lx * si.dpdu[0] + ly * si.dpdv[0]) + lz * nx;
+            const float wy = (lx * si.dpdu[1] + ly * si.dpdv[1]) + lz * ny;
+            const float wz = (lx * si.dpdu[2] + ly * si.dpdv[2]) + lz * nz;
+            const RayF r = make_rayf(ox, oy, oz, wx, wy, wz);
+            if (!any_hit(d, root, r, sp.aoLength, sIndex, sMasks, tix))
+                open += 1;
+            samples += 1;
+        }
+        ao = (float)open / (float)samples;
+    }
+    if (sunOut)
+        sunOut[i] = sun;
+    if (aoOut)
+        aoOut[i] = ao;
+    // trace_lighting (tracer.cu:701-730)
+    const float skyR = 187.f / 255.f, skyG = 242.f / 255.f, skyB = 250.f / 255.f;
+    float sr, sg, sb;
+    if (!hit) {
+        sr = skyR;
+        sg = skyG;
+        sb = skyB;
+    } else {
+        const float kr = srgb_to_linear(float((diffuse >> 0) & 0xFFu) / 255.0f);
+        const float kg = srgb_to_linear(float((diffuse >> 8) & 0xFFu) / 255.0f);
+        const float kb = srgb_to_linear(float((diffuse >> 16) & 0xFFu) / 255.0f);
+        const float occl = (sp.flags & SVDAG_SHADE_AO) && sp.samples ? ao : 1.0f;
+        const float vis = (sp.flags & SVDAG_SHADE_SHADOWS) ? sun : 1.0f;
+        const float a = occl * 0.5f;
+        sr = ((a * skyR) + ((vis * 0.95f) * sp.sunBrightness)) * kr;
+        sg = ((a * skyG) + ((vis * 0.94f) * sp.sunBrightness)) * kg;
+        sb = ((a * skyB) + ((vis * 0.47f) * sp.sunBrightness)) * kb;
+        if (sp.fog > 0.0f) { // applyFog, tracer.cu:685-699, with the camera ray of this pixel
+            const double vx = ((tp.ray_min[0] + (double)x * tp.ray_ddx[0]) + (double)y * tp.ray_ddy[0]) - tp.camera[0];
+            const double vy = ((tp.ray_min[1] + (double)x * tp.ray_ddx[1]) + (double)y * tp.ray_ddy[1]) - tp.camera[1];
+            const double vz = ((tp.ray_min[2] + (double)x * tp.ray_ddx[2]) + (double)y * tp.ray_ddy[2]) - tp.camera[2];
+            const double inv = 1.0 / sqrt(vx * vx + vy * vy + vz * vz);
+            const float dx = (float)(vx * inv), dy = (float)(vy * inv), dz = (float)(vz * inv);
+            const float ex = (float)tp.camera[0] - px, ey = (float)tp.camera[1] - py, ez = (float)tp.camera[2] - pz;
+            const float density = sp.fog * 0.00001f;
+            const float amount = 1.0f - expf(-sqrtf((ex * ex + ey * ey) + ez * ez) * density);
+            const float sunAmount = 1.01f * fmaxf((dx * sp.sun[0] + dy * sp.sun[1]) + dz * sp.sun[2], 0.0f);
+            const float t = powf(sunAmount, 30.0f);
+            const float fr = skyR + t * (1.0f - skyR), fg = skyG + t * (1.0f - skyG), fb = skyB + t * (1.0f - skyB);
+            const float f = fmaxf(0.0f, fminf(amount, 1.0f));
+            sr = sr + f * (fr - sr);
+            sg = sg + f * (fg - sg);
+            sb = sb + f * (fb - sb);
+        }
+    }
+    rgba[i] = to_rgb888(linear_to_srgb(sr), linear_to_srgb(sg), linear_to_srgb(sb));
+}
+
 __global__ void k_sample(DevDag d, const uint32_t* xyz, uint32_t n, uint32_t* out)
 {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -288,6 +550,32 @@ svdag_status svdag_trace_primary(svdag_ctx* ctx, const svdag_trace_params* p, sv
     const dim3 block(32, 8);
     const dim3 grid((p->width + block.x - 1) / block.x, (p->height + block.y - 1) / block.y);
     k_trace<<<grid, block, 0, as_stream(stream)>>>(ctx->dag(), *p, out, nullptr);
+    SVDAG_CUDA(cudaGetLastError());
+    return SVDAG_OK;
+}
+
+svdag_status svdag_shade(svdag_ctx* ctx, const svdag_trace_params* tp, const svdag_shade_params* sp, svdag_hit* hits, uint32_t* rgba,
+    float* sun, float* ao, void* stream)
+{
+    if (!ctx || !tp || !sp || !hits || !rgba || tp->width == 0 || tp->height == 0 || (sp->flags & ~(SVDAG_SHADE_SHADOWS | SVDAG_SHADE_AO)))
+        return SVDAG_ERR_INVALID;
+    if (!(sp->ao_ray_length >= 0.0f) || !std::isfinite(sp->shadow_bias) || !std::isfinite(sp->sun_brightness) || !(sp->fog_density >= 0.0f))
+        return SVDAG_ERR_INVALID;
+    ShadeDev d {};
+    for (uint32_t m = 0; m < SVDAG_NUM_MATERIALS; ++m)
+        d.palette[m] = sp->material_srgb8[m] & 0x00FFFFFFu;
+    for (int a = 0; a < 3; ++a)
+        d.sun[a] = sp->sun_direction[a];
+    d.bias = sp->shadow_bias;
+    d.aoLength = sp->ao_ray_length;
+    d.sunBrightness = sp->sun_brightness;
+    d.fog = sp->fog_density;
+    d.samples = sp->ao_samples;
+    d.flags = sp->flags;
+    d.seed = sp->random_seed;
+    const dim3 block(32, 8);
+    const dim3 grid((tp->width + block.x - 1) / block.x, (tp->height + block.y - 1) / block.y);
+    k_shade<<<grid, block, 0, as_stream(stream)>>>(ctx->dag(), *tp, d, hits, rgba, sun, ao);
     SVDAG_CUDA(cudaGetLastError());
     return SVDAG_OK;
 }

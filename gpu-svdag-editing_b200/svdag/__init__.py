@@ -109,6 +109,39 @@ assert RESULT_DTYPE.itemsize == C.sizeof(RequestResult) == 48
 SERVE_PLAIN, SERVE_COPY_FRAMES = 1, 2
 
 
+class ShadeParams(C.Structure):
+    _fields_ = [("material_srgb8", C.c_uint32 * NUM_MATERIALS), ("sun_direction", C.c_float * 3),
+                ("shadow_bias", C.c_float), ("ao_ray_length", C.c_float), ("sun_brightness", C.c_float),
+                ("fog_density", C.c_float), ("ao_samples", C.c_uint32), ("flags", C.c_uint32), ("pad", C.c_uint32),
+                ("random_seed", C.c_uint64)]
+
+
+SHADE_SHADOWS, SHADE_AO = 1, 2
+# Diffuse sRGB8 colour per material (0x00BBGGRR): stands in for the reference's material textures.
+DEFAULT_PALETTE = (0x3C5A7A, 0x4A7F5B, 0x2E6B8C, 0x8C8C8C, 0x5E5E5E, 0x3B8FD4, 0x61A0A8, 0xD9D9D9,
+                   0x2F2FB0, 0x2E9AE8, 0x3DB86A, 0xB06A2F, 0x8A3DB8, 0x6AD4E0, 0x1F4E79, 0xF0F0F0)
+
+
+def shade_params(levels: int, shadows: bool = True, ao_samples: int = 0, ao_ray_length: float | None = None,
+                 shadow_bias: float = 1.0, sun_brightness: float = 1.0, fog_density: float = 0.0, seed: int = 1,
+                 palette=DEFAULT_PALETTE) -> ShadeParams:
+    """Shading parameters with the reference engine's defaults (engine.h:212-214): shadow bias 1, AO
+    ray length 2^(levels - 10), the sun towards normalize(0.3, 1, 0.5) (computed in double)."""
+    sun = np.array([0.3, 1.0, 0.5])
+    sun = sun / math.sqrt(float(np.dot(sun, sun)))
+    p = ShadeParams()
+    p.material_srgb8[:] = list(palette)
+    p.sun_direction[:] = [float(np.float32(v)) for v in sun]
+    p.shadow_bias = shadow_bias
+    p.ao_ray_length = float(1 << max(levels - 10, 0)) if ao_ray_length is None else ao_ray_length
+    p.sun_brightness = sun_brightness
+    p.fog_density = fog_density
+    p.ao_samples = ao_samples
+    p.flags = (SHADE_SHADOWS if shadows else 0) | (SHADE_AO if ao_samples else 0)
+    p.random_seed = seed
+    return p
+
+
 class Tuning(C.Structure):
     _fields_ = [("probe_lanes", C.c_uint32), ("load_factor", C.c_uint32), ("persistent_leaves", C.c_uint32),
                 ("trials", C.c_uint32), ("table_ns_per_key", C.c_double), ("graph_us_small", C.c_double),
@@ -185,6 +218,7 @@ _PROTOS = {
     "svdag_replay_parse": [C.c_char_p, _U64, C.c_float, _P, _U64, C.POINTER(_U64), C.POINTER(_U64)],
     "svdag_server_replay_actions": [_P, _P, _U64, C.c_double, _P, _P],
     "svdag_save_items": [_P, _P, _U64, _P, _P, C.POINTER(_U64), _P],
+    "svdag_shade": [_P, C.POINTER(TraceParams), C.POINTER(ShadeParams), _P, _P, _P, _P, _P],
     "svdag_load_items": [_P, _P, _P, _P, _P],
     "svdag_basic_dag_to_items": [_P, _U64, _U32, _U32, _P, _U64, _P, _P, C.POINTER(_U64)],
 }
@@ -691,6 +725,22 @@ class DAGTracer:
 
     def hits_numpy(self) -> np.ndarray:
         return self.hits.cpu().numpy().view(HIT_DTYPE)
+
+    def resolve_lighting(self, params: TraceParams, dag: MyGPUHashDAG, shade: ShadeParams, want_surfaces: bool = False,
+                         stream=None):
+        """Colours, shadows, ambient occlusion and lighting of the last resolve_paths
+        (DAGTracer::resolve_colors / resolve_shadows / resolve_ambient_occlusion / resolve_lighting,
+        dag_tracer.cu:136-250) in one launch: returns the sRGB8 image as a device tensor, plus the sun
+        and AO surfaces with want_surfaces."""
+        import torch
+        n = self.width * self.height
+        self.colors = torch.empty(n, dtype=torch.int32, device=self.hits.device)
+        sun = torch.empty(n, dtype=torch.float32, device=self.hits.device) if want_surfaces else None
+        ao = torch.empty(n, dtype=torch.float32, device=self.hits.device) if want_surfaces else None
+        _check(lib().svdag_shade(dag.h, C.byref(params), C.byref(shade), ptr(self.hits), ptr(self.colors),
+                                 ptr(sun) if sun is not None else None, ptr(ao) if ao is not None else None,
+                                 stream_ptr(stream)), "svdag_shade")
+        return (self.colors, sun, ao) if want_surfaces else self.colors
 
 
 class Server:

@@ -252,6 +252,35 @@ svdag_status svdag_trace_primary(svdag_ctx* ctx, const svdag_trace_params* param
 svdag_status svdag_sample_voxels(svdag_ctx* ctx, const uint32_t* xyz_dev, uint32_t count,
     uint32_t* out_dev, void* stream);
 
+/* Post-hit shading of a hit buffer, all four of the reference's passes in one kernel: the diffuse
+ * colour (Tracer::trace_colors, tracer.cu:413-593), the sun shadow ray (trace_shadows, :609-628),
+ * ambient occlusion (trace_ambient_occlusion, :654-683) and lighting (trace_lighting, :701-730). The
+ * output pixel (x, y) is hit record y * width + x, as the reference's surfaces index them. Material
+ * textures are files the reference loads; here each material has one sRGB8 diffuse colour. Shadow
+ * and AO rays use the any-hit traversal intersect_ray_node_out_of_order (tracer.cu:275-352). */
+#define SVDAG_SHADE_SHADOWS 1u
+#define SVDAG_SHADE_AO 2u
+
+typedef struct svdag_shade_params {
+    uint32_t material_srgb8[SVDAG_NUM_MATERIALS]; /* diffuse colour per material, 0x00BBGGRR */
+    float sun_direction[3]; /* unit vector towards the sun (the reference: normalize(0.3, 1, 0.5)) */
+    float shadow_bias; /* offset of shadow and AO ray origins (engine.h: 1) */
+    float ao_ray_length; /* AO ray tmax (engine.h: 2^(depth - 10)) */
+    float sun_brightness; /* direct light scale (the reference's resolve_lighting leaves it 0, dag_tracer.cu:232-245) */
+    float fog_density; /* 0 = no fog */
+    uint32_t ao_samples; /* cosine-weighted hemisphere samples per pixel */
+    uint32_t flags; /* SVDAG_SHADE_* */
+    uint32_t pad;
+    uint64_t random_seed; /* PCG stream of pixel i = i * max(random_seed, 1) */
+} svdag_shade_params;
+
+/* `hits_dev` holds the trace of `trace` (svdag_trace_primary); each hit's `color` receives its
+ * diffuse colour (SurfaceInteraction::diffuseColorSRGB8). Writes width*height packed sRGB8 pixels
+ * (0xFFBBGGRR) to out_rgba_dev and, when not NULL, the sun visibility (trace_shadows' sunLight
+ * surface) and the AO fraction per pixel; misses write 0 there. */
+svdag_status svdag_shade(svdag_ctx* ctx, const svdag_trace_params* trace, const svdag_shade_params* shade,
+    svdag_hit* hits_dev, uint32_t* out_rgba_dev, float* out_sun_dev, float* out_ao_dev, void* stream);
+
 /* ---------------------------------------------------------------- hash tables */
 
 /* The table of one DAG level (level leaf_level = levels-2 holds leaves). The handle stays owned by

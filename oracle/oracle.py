@@ -55,6 +55,12 @@ class TraceParams(C.Structure):
                 ("ray_ddy", C.c_double * 3), ("width", C.c_uint32), ("height", C.c_uint32)]
 
 
+class ShadeParams(C.Structure):
+    _fields_ = [("material_srgb8", C.c_uint32 * 16), ("sun_direction", C.c_float * 3), ("shadow_bias", C.c_float),
+                ("ao_ray_length", C.c_float), ("sun_brightness", C.c_float), ("fog_density", C.c_float),
+                ("ao_samples", C.c_uint32), ("flags", C.c_uint32), ("pad", C.c_uint32), ("random_seed", C.c_uint64)]
+
+
 HIT_DTYPE = np.dtype([("path", "<u4", (3,)), ("material", "u1"), ("pad", "u1", (3,)),
                       ("position", "<f4", (3,)), ("normal", "<f4", (3,)), ("dpdu", "<f4", (3,)),
                       ("dpdv", "<f4", (3,)), ("color", "<u4")])
@@ -98,6 +104,9 @@ def lib():
             getattr(L, f).restype = C.c_uint32
         L.oracle_sample_voxels.argtypes = [P, P, C.c_uint64, P]
         L.oracle_trace.argtypes = [P, C.POINTER(TraceParams), P, C.c_int]
+        L.oracle_shade.argtypes = [P, C.POINTER(TraceParams), C.POINTER(ShadeParams), P, P, P, P, C.c_int]
+        L.oracle_sincos.argtypes = [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        L.oracle_sincos.restype = None
         L.oracle_trace_counts.argtypes = [P, C.POINTER(TraceParams), C.POINTER(C.c_uint64),
                                           C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
         L.oracle_canonicalize.argtypes = [P, C.POINTER(Canon)]
@@ -224,6 +233,14 @@ class OracleDag:
         out = np.zeros(params.width * params.height, dtype=HIT_DTYPE)
         lib().oracle_trace(self.h, C.byref(params), _ptr(out), threads)
         return out
+
+    def shade(self, params: TraceParams, shade: ShadeParams, hits: np.ndarray, threads: int = 8):
+        """(hits with diffuse colours, rgba uint32, sun float32, ao float32) of a traced hit buffer."""
+        hits = hits.copy()
+        n = params.width * params.height
+        rgba, sun, ao = np.zeros(n, np.uint32), np.zeros(n, np.float32), np.zeros(n, np.float32)
+        lib().oracle_shade(self.h, C.byref(params), C.byref(shade), _ptr(hits), _ptr(rgba), _ptr(sun), _ptr(ao), threads)
+        return hits, rgba, sun, ao
 
     def trace_counts(self, params: TraceParams):
         a, b, c = C.c_uint64(), C.c_uint64(), C.c_uint64()

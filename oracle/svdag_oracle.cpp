@@ -1749,6 +1749,260 @@ int oracle_trace_counts(const oracle_dag* d, const svdag_trace_params* p, uint64
     return SVDAG_OK;
 }
 
+// ---------------------------------------------------------------- shading (tracer.cu:413-730)
+
+namespace {
+
+// intersect_ray_node_out_of_order, tracer.cu:275-352: any voxel on the ray within [tmin, tmax].
+bool any_hit(const Dag& dag, const Ray& ray)
+{
+    struct Entry {
+        uint32_t index;
+        uint32_t childMask;
+        uint32_t visitMask;
+    };
+    if (dag.root == kSentinel)
+        return false;
+    uint32_t level = 0;
+    Path path {};
+    Entry stack[SVDAG_MAX_LEVELS];
+    Entry cache;
+    uint32_t leafLo = 0, leafHi = 0;
+    cache.index = dag.root;
+    cache.childMask = header_child_mask(dag.ptr(0, cache.index)[0]);
+    cache.visitMask = cache.childMask & intersection_mask(true, 0, path, dag.levels, ray);
+    for (;;) {
+        {
+            uint32_t newLevel = level;
+            while (newLevel > 0 && !cache.visitMask) {
+                newLevel--;
+                cache = stack[newLevel];
+            }
+            if (newLevel == 0 && !cache.visitMask)
+                return false;
+            path.ascend(level - newLevel);
+            level = newLevel;
+        }
+        const uint32_t nextChild = 31u - (uint32_t)__builtin_clz(cache.visitMask);
+        cache.visitMask &= ~(1u << nextChild);
+        path.descend(nextChild);
+        stack[level] = cache;
+        level++;
+        if (level == dag.levels)
+            return true;
+        if (level < dag.leaf_level()) {
+            const uint32_t* node = dag.ptr(level - 1, cache.index);
+            cache.index = node[1 + child_offset(cache.childMask, nextChild)];
+            cache.childMask = header_child_mask(dag.ptr(level, cache.index)[0]);
+            cache.visitMask = cache.childMask & intersection_mask(false, level, path, dag.levels, ray);
+        } else {
+            uint32_t childMask;
+            if (level == dag.leaf_level()) {
+                const uint32_t* node = dag.ptr(level - 1, cache.index);
+                const uint32_t* leaf = dag.ptr(level, node[1 + child_offset(cache.childMask, nextChild)]);
+                leafLo = leaf[0];
+                leafHi = leaf[1];
+                childMask = leaf_first_child_mask(leafLo, leafHi);
+            } else {
+                childMask = leaf_second_child_mask(leafLo, leafHi, nextChild);
+            }
+            cache.childMask = childMask;
+            cache.visitMask = cache.childMask & intersection_mask(false, level, path, dag.levels, ray);
+        }
+    }
+}
+
+Ray ray_create(F3 o, F3 dir, float tmax) // Ray::create, tracer.cu:32-41
+{
+    Ray r;
+    r.o = o;
+    r.d = dir;
+    r.inv = { 1.0f / dir.x, 1.0f / dir.y, 1.0f / dir.z };
+    r.tmin = 0.0f;
+    r.tmax = tmax;
+    return r;
+}
+
+struct Pcg { // Utils::PCG_RNG, utils.h:45-78
+    uint64_t state = 0x853c49e6748fea9bull, inc;
+    explicit Pcg(uint64_t stream)
+        : inc(stream)
+    {
+        next();
+        next();
+    }
+    uint32_t next()
+    {
+        const uint64_t old = state;
+        state = old * 6364136223846793005ull + (inc | 1ull);
+        const uint32_t xorshifted = (uint32_t)(((old >> 18u) ^ old) >> 27u);
+        const uint32_t rot = (uint32_t)(old >> 59);
+        return (xorshifted >> rot) | (xorshifted << ((0xFFFFFFFFu - rot + 1u) & 31u));
+    }
+    float next_float() { return float(next()) / 4294967296.0f; }
+};
+
+// sin and cos of x in [0, 2 pi] by quadrant reduction and Taylor polynomials (the library evaluates
+// the same operations, so sample directions agree exactly).
+void sincos_quadrant(float x, float& s, float& c)
+{
+    const float k = std::rint(x * 0.63661975f);
+    const float r = (float)((double)x - (double)k * 1.5707963267948966);
+    const float r2 = r * r;
+    const float sp = r + (r * r2) * (-0.16666667f + r2 * (0.008333334f + r2 * (-0.0001984127f + r2 * 2.7557319e-06f)));
+    const float cp = 1.0f + r2 * (-0.5f + r2 * (0.041666668f + r2 * (-0.0013888889f + r2 * 2.4801588e-05f)));
+    switch ((int)k & 3) {
+    case 0:
+        s = sp;
+        c = cp;
+        break;
+    case 1:
+        s = cp;
+        c = -sp;
+        break;
+    case 2:
+        s = -sp;
+        c = -cp;
+        break;
+    default:
+        s = -cp;
+        c = sp;
+        break;
+    }
+}
+
+float srgb_to_linear(float v) // ColorUtils::accurateSRGBToLinear, color_utils.h:233-242
+{
+    const float lo = v / 12.92f;
+    const float hi = std::pow((v + 0.055f) / 1.055f, 2.4f);
+    return (v <= 0.04045f) ? lo : hi;
+}
+float linear_to_srgb(float v) // ColorUtils::accurateLinearToSRGB, :243-252
+{
+    const float lo = v * 12.92f;
+    const float hi = (std::pow(std::fabs(v), 1.0f / 2.4f) * 1.055f) - 0.055f;
+    return (v <= 0.0031308f) ? lo : hi;
+}
+uint32_t to_rgb888(float r, float g, float b) // ColorUtils::float3_to_rgb888, :31-37
+{
+    r = std::fmax(0.f, std::fmin(r, 1.f));
+    g = std::fmax(0.f, std::fmin(g, 1.f));
+    b = std::fmax(0.f, std::fmin(b, 1.f));
+    return (uint32_t(r * 255.0f) << 0) | (uint32_t(g * 255.0f) << 8) | (uint32_t(b * 255.0f) << 16) | 0xff000000u;
+}
+
+void shade_pixel(const Dag& dag, const svdag_trace_params& tp, const svdag_shade_params& sp, uint32_t x, uint32_t y, svdag_hit& si,
+    uint32_t& rgba, float& sunOut, float& aoOut)
+{
+    const bool hit = si.path[0] != 0 || si.path[1] != 0 || si.path[2] != 0;
+    uint32_t diffuse; // computeColorAtSurface, tracer.cu:413-445
+    if (!hit) {
+        diffuse = to_rgb888(0.f, 0.f, 0.f);
+    } else if (si.material < SVDAG_NUM_MATERIALS) {
+        diffuse = (sp.material_srgb8[si.material] & 0x00FFFFFFu) | 0xff000000u;
+    } else {
+        const float b = float((si.path[0] ^ si.path[1] ^ si.path[2]) & 1u);
+        diffuse = to_rgb888(1.f, b, 1.f - b);
+    }
+    si.color = diffuse;
+    const F3 pos { si.position[0], si.position[1], si.position[2] };
+    const F3 n { si.normal[0], si.normal[1], si.normal[2] };
+    const F3 sun { sp.sun_direction[0], sp.sun_direction[1], sp.sun_direction[2] };
+    float sunVis = 0.f, ao = 0.f;
+    if (hit && (sp.flags & SVDAG_SHADE_SHADOWS)) { // trace_shadows, tracer.cu:609-628
+        const Ray r = ray_create({ pos.x + sp.shadow_bias * sun.x, pos.y + sp.shadow_bias * sun.y, pos.z + sp.shadow_bias * sun.z }, sun,
+            std::numeric_limits<float>::max());
+        const bool occluded = any_hit(dag, r);
+        const float ndotl = std::fmax((n.x * r.d.x + n.y * r.d.y) + n.z * r.d.z, 0.0f);
+        sunVis = occluded ? 0.0f : ndotl;
+    }
+    if (hit && (sp.flags & SVDAG_SHADE_AO) && sp.ao_samples) { // trace_ambient_occlusion, tracer.cu:654-683
+        const uint64_t seed = (uint64_t)(y * tp.width + x) * (sp.random_seed > 1ull ? sp.random_seed : 1ull);
+        Pcg rng(seed);
+        uint32_t samples = 0, open = 0;
+        const F3 o { pos.x + n.x * sp.shadow_bias, pos.y + n.y * sp.shadow_bias, pos.z + n.z * sp.shadow_bias };
+        for (uint32_t k = 0; k < sp.ao_samples; ++k) {
+            const float ux = rng.next_float();
+            const float uy = rng.next_float();
+            const float rr = std::sqrt(ux);
+            const float theta = 6.2831855f * uy;
+            float sn, cs;
+            sincos_quadrant(theta, sn, cs);
+            const float lx = rr * cs, ly = rr * sn, lz = std::sqrt(std::fmax(0.0f, 1 - ux));
+            const F3 w { (lx * si.dpdu[0] + ly * si.dpdv[0]) + lz * n.x, (lx * si.dpdu[1] + ly * si.dpdv[1]) + lz * n.y,
+                (lx * si.dpdu[2] + ly * si.dpdv[2]) + lz * n.z };
+            if (!any_hit(dag, ray_create(o, w, sp.ao_ray_length)))
+                open += 1;
+            samples += 1;
+        }
+        ao = (float)open / (float)samples;
+    }
+    sunOut = sunVis;
+    aoOut = ao;
+    const float skyR = 187.f / 255.f, skyG = 242.f / 255.f, skyB = 250.f / 255.f; // trace_lighting, tracer.cu:701-730
+    float sr, sg, sb;
+    if (!hit) {
+        sr = skyR;
+        sg = skyG;
+        sb = skyB;
+    } else {
+        const float kr = srgb_to_linear(float((diffuse >> 0) & 0xFFu) / 255.0f);
+        const float kg = srgb_to_linear(float((diffuse >> 8) & 0xFFu) / 255.0f);
+        const float kb = srgb_to_linear(float((diffuse >> 16) & 0xFFu) / 255.0f);
+        const float occl = (sp.flags & SVDAG_SHADE_AO) && sp.ao_samples ? ao : 1.0f;
+        const float vis = (sp.flags & SVDAG_SHADE_SHADOWS) ? sunVis : 1.0f;
+        const float a = occl * 0.5f;
+        sr = ((a * skyR) + ((vis * 0.95f) * sp.sun_brightness)) * kr;
+        sg = ((a * skyG) + ((vis * 0.94f) * sp.sun_brightness)) * kg;
+        sb = ((a * skyB) + ((vis * 0.47f) * sp.sun_brightness)) * kb;
+        if (sp.fog_density > 0.0f) { // applyFog, tracer.cu:685-699
+            double v[3];
+            for (int i = 0; i < 3; ++i)
+                v[i] = ((tp.ray_min[i] + (double)x * tp.ray_ddx[i]) + (double)y * tp.ray_ddy[i]) - tp.camera[i];
+            const double inv = 1.0 / std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+            const float dx = (float)(v[0] * inv), dy = (float)(v[1] * inv), dz = (float)(v[2] * inv);
+            const float ex = (float)tp.camera[0] - pos.x, ey = (float)tp.camera[1] - pos.y, ez = (float)tp.camera[2] - pos.z;
+            const float density = sp.fog_density * 0.00001f;
+            const float amount = 1.0f - std::exp(-std::sqrt((ex * ex + ey * ey) + ez * ez) * density);
+            const float sunAmount = 1.01f * std::fmax((dx * sun.x + dy * sun.y) + dz * sun.z, 0.0f);
+            const float t = std::pow(sunAmount, 30.0f);
+            const float fr = skyR + t * (1.0f - skyR), fg = skyG + t * (1.0f - skyG), fb = skyB + t * (1.0f - skyB);
+            const float f = std::fmax(0.0f, std::fmin(amount, 1.0f));
+            sr = sr + f * (fr - sr);
+            sg = sg + f * (fg - sg);
+            sb = sb + f * (fb - sb);
+        }
+    }
+    rgba = to_rgb888(linear_to_srgb(sr), linear_to_srgb(sg), linear_to_srgb(sb));
+}
+
+} // namespace
+
+void oracle_sincos(float x, float* s, float* c) { sincos_quadrant(x, *s, *c); }
+
+int oracle_shade(const oracle_dag* d, const svdag_trace_params* tp, const svdag_shade_params* sp, svdag_hit* hits, uint32_t* rgba, float* sun,
+    float* ao, int threads)
+{
+    const uint32_t W = tp->width, H = tp->height;
+    const auto work = [&](uint32_t y0, uint32_t y1) {
+        for (uint32_t y = y0; y < y1; ++y)
+            for (uint32_t x = 0; x < W; ++x) {
+                const size_t i = (size_t)y * W + x;
+                shade_pixel(d->dag, *tp, *sp, x, y, hits[i], rgba[i], sun[i], ao[i]);
+            }
+    };
+    if (threads <= 1) {
+        work(0, H);
+    } else {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < threads; ++t)
+            pool.emplace_back(work, H * t / threads, H * (t + 1) / threads);
+        for (auto& th : pool)
+            th.join();
+    }
+    return SVDAG_OK;
+}
+
 int oracle_canonicalize(const oracle_dag* d, oracle_canon* out)
 {
     Canon c;

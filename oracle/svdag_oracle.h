@@ -60,6 +60,12 @@ uint32_t oracle_redo_count(const oracle_dag* dag);
 
 int oracle_sample_voxels(const oracle_dag* dag, const uint32_t* xyz, uint64_t count, uint32_t* out);
 int oracle_trace(const oracle_dag* dag, const svdag_trace_params* params, svdag_hit* out, int threads);
+/* Shading of a hit buffer (trace_colors, trace_shadows, trace_ambient_occlusion, trace_lighting,
+ * tracer.cu:413-730); hits[i].color receives the diffuse colour; rgba, sun and ao get width*height values. */
+/* sin and cos of the AO sample angle (quadrant reduction, Taylor polynomials), as the library computes them. */
+void oracle_sincos(float x, float* s, float* c);
+int oracle_shade(const oracle_dag* dag, const svdag_trace_params* trace, const svdag_shade_params* shade, svdag_hit* hits,
+    uint32_t* rgba, float* sun, float* ao, int threads);
 /* Node-visit counters of the trace (for the tracer's algorithmic bytes). */
 int oracle_trace_counts(const oracle_dag* dag, const svdag_trace_params* params, uint64_t* out_node_visits,
     uint64_t* out_leaf_visits, uint64_t* out_hits);
