@@ -144,6 +144,10 @@ __device__ __forceinline__ uint32_t should_edit(const DevEditor& e, uint32_t px,
         if (!box_overlap(e, nmin, nmax))
             return OP_KEEP;
         return state == ST_EMPTY ? OP_EMPTY : OP_SUBDIVIDE;
+    } else if constexpr (TOOL == SVDAG_TOOL_SPHERE_ERODE) { // MyGpuSphereErosionEditor::should_edit, :551-562
+        if (!sphere_overlap(e, nmin, nmax))
+            return OP_KEEP;
+        return state == ST_EMPTY ? OP_EMPTY : OP_SUBDIVIDE;
     } else if constexpr (TOOL == SVDAG_TOOL_COPY) { // stateless form, :166-172 (used for voxels)
         return box_overlap(e, nmin, nmax) ? OP_SUBDIVIDE : OP_KEEP;
     } else if constexpr (TOOL == kToolTerrain) {
@@ -375,6 +379,7 @@ template <uint32_t TOOL>
 __device__ void ph_build_leaves(const DevDag& d, const DevEditor& e, char* scratch, unsigned long long scratchBytes)
 {
     __shared__ __align__(16) uint32_t packBuf[16][16]; // per warp of a block of up to 512 threads: 64 material bytes
+    __shared__ uint2 erodeBuf[TOOL == SVDAG_TOOL_SPHERE_ERODE ? 16 : 1][27]; // erosion: per warp, the neighbour leaf masks
     EditCounters& E = d.ctl->edit;
     const uint32_t LL = d.leafLevel;
     const unsigned long long stride = work_stride(TOOL);
@@ -458,6 +463,33 @@ __device__ void ph_build_leaves(const DevDag& d, const DevEditor& e, char* scrat
                     corners[k] = __shfl_sync(0xFFFFFFFFu, mine, k);
             }
         }
+        // erosion: the 27 leaves around this one in the DAG before the edit (lane k: offset
+        // (k / 9, k / 3 % 3, k % 3) - 1, coordinates wrapping as the reference's unsigned paths do)
+        if constexpr (TOOL == SVDAG_TOOL_SPHERE_ERODE) {
+            uint32_t nlo = 0, nhi = 0;
+            if (lane < 27) {
+                const uint32_t lmask = (1u << LL) - 1u;
+                const uint32_t lx = (w.x + lane / 9u - 1u) & lmask, ly = (w.y + (lane / 3u) % 3u - 1u) & lmask, lz = (w.z + lane % 3u - 1u) & lmask;
+                uint32_t h = E.rootBefore;
+                for (uint32_t l = 0; l < LL && h != kNone; ++l) {
+                    const uint32_t s = LL - 1u - l;
+                    const uint32_t c = (((lx >> s) & 1u) << 2) | (((ly >> s) & 1u) << 1) | ((lz >> s) & 1u);
+                    const uint32_t* node = item_ptr(d, h);
+                    const uint32_t m = node[0] & 0xFFu;
+                    h = ((m >> c) & 1u) ? node[1 + __popc(m & ((1u << c) - 1u))] : kNone;
+                }
+                if (h != kNone) {
+                    const uint32_t* lp = item_ptr(d, h);
+                    nlo = lp[0];
+                    nhi = lp[1];
+                }
+            }
+            uint2* nb = erodeBuf[threadIdx.x >> 5];
+            __syncwarp();
+            if (lane < 27)
+                nb[lane] = make_uint2(nlo, nhi);
+            __syncwarp();
+        }
         uint32_t newMat[2];
         bool set[2];
 #pragma unroll
@@ -495,6 +527,24 @@ __device__ void ph_build_leaves(const DevDag& d, const DevEditor& e, char* scrat
                         out = true;
                         mat = e.noiseCellLog2 >= 2 ? noise_from_corners(corners, e.noiseCellLog2, vx, vy, vz)
                                                    : noise_material(e.noiseSeed, e.noiseCellLog2, vx, vy, vz);
+                    } else if constexpr (TOOL == SVDAG_TOOL_SPHERE_ERODE) { // get_new_value, :564-588
+                        const uint2* nb = erodeBuf[threadIdx.x >> 5];
+                        uint32_t count = 0;
+                        for (int oz = -1; oz <= 1; ++oz)
+                            for (int oy = -1; oy <= 1; ++oy)
+                                for (int ox = -1; ox <= 1; ++ox) {
+                                    if (ox == 0 && oy == 0 && oz == 0)
+                                        continue;
+                                    const int qx = (int)dx + ox, qy = (int)dy + oy, qz = (int)dz + oz; // -1 .. 4
+                                    const uint32_t li = (uint32_t)(((qx >> 2) + 1) * 9 + ((qy >> 2) + 1) * 3 + ((qz >> 2) + 1));
+                                    const uint32_t ix = (uint32_t)qx & 3u, iy = (uint32_t)qy & 3u, iz = (uint32_t)qz & 3u;
+                                    const uint32_t bit = ((ix & 1u) ? 4u : 0u) | ((iy & 1u) ? 2u : 0u) | ((iz & 1u) ? 1u : 0u) | ((ix & 2u) ? 32u : 0u)
+                                        | ((iy & 2u) ? 16u : 0u) | ((iz & 2u) ? 8u : 0u);
+                                    const uint2 m = nb[li];
+                                    count += ((bit < 32 ? m.x >> bit : m.y >> (bit - 32)) & 1u);
+                                }
+                        out = hasOld && count > e.noiseSeed;
+                        mat = oldMat;
                     } else if constexpr (TOOL == SVDAG_TOOL_COPY) { // get_new_value(uint3, optional, State), :225-252
                         out = hasOld;
                         mat = oldMat;
@@ -1071,6 +1121,9 @@ __global__ void __launch_bounds__(kBlockThreads, 1) k_edit_block(DevDag d, DevEd
         case SVDAG_TOOL_BOX_PAINT_NOISE:
             block_edit<SVDAG_TOOL_BOX_PAINT_NOISE>(d, ed, scratch, scratchBytes, rec);
             break;
+        case SVDAG_TOOL_SPHERE_ERODE:
+            block_edit<SVDAG_TOOL_SPHERE_ERODE>(d, ed, scratch, scratchBytes, rec);
+            break;
         default:
             break;
         }
@@ -1130,10 +1183,12 @@ DevEditor make_editor(const svdag_ctx* ctx, const svdag_edit& e)
     case SVDAG_TOOL_SPHERE_ADD:
     case SVDAG_TOOL_SPHERE_REMOVE:
     case SVDAG_TOOL_SPHERE_PAINT: // MyGpuSphereEditorBase constructor, :406-411
+    case SVDAG_TOOL_SPHERE_ERODE:
         for (int a = 0; a < 3; ++a)
             d.center[a] = c[a] + 0.5f;
         d.radius = std::max(e.radius, 0.1f);
         d.radiusSquared = d.radius * d.radius;
+        d.noiseSeed = e.noise_seed; // erosion threshold
         break;
     case SVDAG_TOOL_COPY: { // MyGpuCopyEditor constructor, :157-164
         float center[3];
@@ -1183,6 +1238,8 @@ svdag_status launch_build_any(svdag_ctx* ctx, uint32_t tool, cudaStream_t s)
         return launch_build<SVDAG_TOOL_COPY>(ctx, s);
     case SVDAG_TOOL_BOX_PAINT_NOISE:
         return launch_build<SVDAG_TOOL_BOX_PAINT_NOISE>(ctx, s);
+    case SVDAG_TOOL_SPHERE_ERODE:
+        return launch_build<SVDAG_TOOL_SPHERE_ERODE>(ctx, s);
     case kToolTerrain:
         return launch_build<kToolTerrain>(ctx, s);
     default:
@@ -1296,6 +1353,10 @@ double estimate_leaves(const DevEditor& e)
     case SVDAG_TOOL_SPHERE_PAINT: {
         const double r = e.radius / 4.0 + 1.0;
         return std::min(8.0 * r * r * r, 12.0 * M_PI * r * r);
+    }
+    case SVDAG_TOOL_SPHERE_ERODE: { // every filled leaf inside the sphere is rebuilt
+        const double r = e.radius / 4.0 + 1.0;
+        return 8.0 * r * r * r;
     }
     case kToolTerrain:
         return 1e12;

@@ -14,7 +14,7 @@ enum : uint32_t { OP_SUBDIVIDE = 0, OP_FILL = 1, OP_EMPTY = 2, OP_KEEP = 3 };
 enum : uint32_t { ST_PARTIAL = 0, ST_FILLED = 1, ST_EMPTY = 2 };
 constexpr uint32_t kToolTerrain = 100; // internal: the procedural scene builder
 constexpr uint32_t kEmptyRep = 0xFFFFFFFEu; // dedup result of an empty SVO item
-constexpr int kNumGraphs = 8; // CUDA graphs of the phase launches: one per tool, the last for the scene builder
+constexpr int kNumGraphs = 10; // CUDA graphs of the phase launches: one per tool, the last for the scene builder
 
 struct EditRecord;
 

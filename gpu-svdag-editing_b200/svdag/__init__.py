@@ -34,6 +34,7 @@ KIND_NODE, KIND_LEAF = 0, 1
 
 TOOL_SPHERE_ADD, TOOL_SPHERE_REMOVE, TOOL_BOX_ADD, TOOL_BOX_REMOVE = 0, 1, 2, 3
 TOOL_SPHERE_PAINT, TOOL_COPY, TOOL_BOX_PAINT_NOISE, TOOL_MOVE = 4, 5, 6, 7
+TOOL_SPHERE_ERODE = 8
 
 STATUS = {0: "SVDAG_OK", 1: "SVDAG_ERR_INVALID", 2: "SVDAG_ERR_OOM", 3: "SVDAG_ERR_TIMEOUT",
           4: "SVDAG_ERR_CORRUPT", 5: "SVDAG_ERR_CUDA", 6: "SVDAG_ERR_NO_DEVICE", 7: "SVDAG_ERR_UNSUPPORTED",
@@ -288,6 +289,21 @@ class MyGpuSphereEditor:
 
     def to_edit(self) -> Edit:
         e = Edit(tool=TOOL_SPHERE_ADD if self.is_adding else TOOL_SPHERE_REMOVE, material=self.material)
+        e.center[:] = [float(v) for v in self.center]
+        e.radius = float(self.radius)
+        return e
+
+
+@dataclass
+class MyGpuSphereErosionEditor:
+    """MyGpuSphereErosionEditor (my_gpu_dag_editors.h:538-589): inside the sphere, a filled voxel stays
+    when more than `threshold` of its 26 neighbours are filled in the DAG before the edit."""
+    center: tuple
+    radius: float
+    threshold: int
+
+    def to_edit(self) -> Edit:
+        e = Edit(tool=TOOL_SPHERE_ERODE, material=0, noise_seed=int(self.threshold))
         e.center[:] = [float(v) for v in self.center]
         e.radius = float(self.radius)
         return e

@@ -135,7 +135,10 @@ typedef enum svdag_tool {
     SVDAG_TOOL_COPY = 5, /* MyGpuCopyEditor           (my_gpu_dag_editors.h:129-253) */
     SVDAG_TOOL_BOX_PAINT_NOISE = 6, /* box paint with a per-voxel material from 3D value noise */
     SVDAG_TOOL_MOVE = 7, /* copy followed by removal of the source box */
-    SVDAG_NUM_TOOLS = 8
+    SVDAG_TOOL_SPHERE_ERODE = 8, /* MyGpuSphereErosionEditor (my_gpu_dag_editors.h:538-589): inside the
+                                    sphere a filled voxel stays when more than noise_seed of its 26
+                                    neighbours are filled in the DAG before the edit, else it is removed */
+    SVDAG_NUM_TOOLS = 9
 } svdag_tool;
 
 typedef struct svdag_edit {
@@ -145,7 +148,7 @@ typedef struct svdag_edit {
     float radius; /* sphere radius, or box half extent */
     float src[3]; /* copy/move: source anchor */
     float dst[3]; /* copy/move: destination anchor */
-    uint32_t noise_seed; /* BOX_PAINT_NOISE: lattice seed */
+    uint32_t noise_seed; /* BOX_PAINT_NOISE: lattice seed; SPHERE_ERODE: neighbour threshold */
     uint32_t noise_cell_log2; /* BOX_PAINT_NOISE: lattice cell size = 1 << noise_cell_log2 voxels */
 } svdag_edit;
 

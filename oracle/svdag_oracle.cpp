@@ -275,6 +275,7 @@ struct Editor {
     int32_t iDestToSource[3] {};
     const Dag* dagCopy = nullptr;
     uint32_t copyRoot = kSentinel;
+    const Dag* dagOld = nullptr; // erosion: the DAG the neighbour counts read (its root is unchanged until the merge)
 
     bool stateful() const { return tool == SVDAG_TOOL_COPY; }
 
@@ -329,6 +330,14 @@ struct Editor {
         } break;
         case SVDAG_TOOL_COPY: { // stateless MyGpuCopyEditor::should_edit, :166-172
             out.op = box.overlap(nmin, nmax) ? Op::Subdivide : Op::Keep;
+        } break;
+        case SVDAG_TOOL_SPHERE_ERODE: { // MyGpuSphereErosionEditor::should_edit, :551-562
+            if (!sphere.overlap(nmin, nmax))
+                out.op = Op::Keep;
+            else if (desc.state == State::Empty)
+                out.op = Op::Empty;
+            else
+                out.op = Op::Subdivide;
         } break;
         default:
             break;
@@ -530,6 +539,21 @@ std::optional<uint32_t> Editor::new_value(const Path& voxel, std::optional<uint3
         return e.material;
     case SVDAG_TOOL_BOX_PAINT_NOISE:
         return noise_material(e.noise_seed, e.noise_cell_log2, voxel.x, voxel.y, voxel.z);
+    case SVDAG_TOOL_SPHERE_ERODE: { // MyGpuSphereErosionEditor::get_new_value, :564-588
+        uint32_t count = 0;
+        for (int dz = -1; dz <= 1; ++dz)
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx) {
+                    if (dx == 0 && dy == 0 && dz == 0)
+                        continue;
+                    // unsigned coordinates: -1 wraps around the grid as the reference's Path does
+                    const Path nb { voxel.x + (uint32_t)dx, voxel.y + (uint32_t)dy, voxel.z + (uint32_t)dz };
+                    count += get_value(*dagOld, nb).has_value() ? 1u : 0u;
+                }
+        if (count > e.noise_seed)
+            return old;
+        return std::nullopt;
+    }
     case SVDAG_TOOL_COPY: { // get_new_value(uint3, optional, State), :225-252
         int32_t s[3] = { (int32_t)voxel.x + iDestToSource[0], (int32_t)voxel.y + iDestToSource[1],
             (int32_t)voxel.z + iDestToSource[2] };
@@ -572,6 +596,10 @@ Editor make_editor(const svdag_edit& e, const Dag& dag)
     case SVDAG_TOOL_SPHERE_REMOVE:
     case SVDAG_TOOL_SPHERE_PAINT:
         ed.sphere.init(c, e.radius);
+        break;
+    case SVDAG_TOOL_SPHERE_ERODE: // MyGpuSphereErosionEditor constructor, :542-548
+        ed.sphere.init(c, e.radius);
+        ed.dagOld = &dag;
         break;
     case SVDAG_TOOL_COPY: { // MyGpuCopyEditor constructor, my_gpu_dag_editors.h:157-164
         const F3 src { e.src[0], e.src[1], e.src[2] };

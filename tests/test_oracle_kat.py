@@ -171,3 +171,28 @@ def test_edit_then_inverse_edit(oracle_mod):
     e.tool = 1
     d.edit(e)
     assert (d.sample(xyz) == 0xFFFFFFFF).all()
+
+
+def test_erosion_semantics(oracle_mod):
+    """MyGpuSphereErosionEditor (my_gpu_dag_editors.h:538-589): threshold 25 keeps only voxels with all
+    26 neighbours filled inside the sphere; threshold 0 removes an isolated voxel; voxels outside the
+    sphere stay. A box of whole leaves builds no leaves and leaves the DAG unchanged
+    (my_gpu_hash_dag_edits.cu:651), so the box is offset by one voxel."""
+    import numpy as np
+
+    o = oracle_mod.OracleDag(8)
+
+    def edit(tool, center, radius, material=0, threshold=0):
+        e = oracle_mod.Edit()
+        e.tool, e.material, e.radius, e.noise_seed = tool, material, radius, threshold
+        e.center[:] = list(center)
+        assert o.edit(e).status == 0
+
+    edit(2, (128.0, 128.0, 128.0), 60.0, 3)  # [68, 188)^3: leaf aligned
+    assert o.root == 0xFFFFFFFF
+    edit(2, (129.0, 129.0, 129.0), 60.0, 3)  # [69, 189)^3
+    edit(2, (30.0, 30.0, 30.0), 0.0, 5)  # one voxel
+    edit(8, (129.0, 160.0, 129.0), 40.0, threshold=25)
+    edit(8, (30.0, 30.0, 30.0), 5.0, threshold=0)
+    xyz = np.array([[129, 160, 129], [129, 188, 129], [71, 188, 71], [30, 30, 30]], dtype=np.uint32)
+    assert o.sample(xyz).tolist() == [3, 0xFFFFFFFF, 3, 0xFFFFFFFF]
