@@ -170,27 +170,23 @@ __global__ void __launch_bounds__(256) k_trace(DevDag d, svdag_trace_params p, s
                 }
                 break;
             }
+            // The child's mask by level kind, then one intersection test for all lanes together (the
+            // branches only fetch; the mask arithmetic runs converged).
             if (level < LL) {
                 const uint32_t* node = item_ptr(d, cIndex);
                 cIndex = node[1 + __popc(cChild & ((1u << nextChild) - 1u))];
                 cChild = item_ptr(d, cIndex)[0] & 0xFFu;
-                cVisit = cChild & intersection_mask(false, level, px, py, pz, levels, r);
-            } else {
-                uint32_t childMask;
-                if (level == LL) {
-                    const uint32_t* node = item_ptr(d, cIndex);
-                    addr = node[1 + __popc(cChild & ((1u << nextChild) - 1u))];
-                    const uint32_t* lp = item_ptr(d, addr);
-                    const uint2 lh = make_uint2(lp[0], lp[1]);
-                    leafLo = lh.x;
-                    leafHi = lh.y;
-                    childMask = first_child_mask(leafLo, leafHi);
-                } else { // get_second_child_mask, base_dag.h:53-58
-                    childMask = (((nextChild & 4u) ? leafHi : leafLo) >> ((nextChild & 3u) * 8u)) & 0xFFu;
-                }
-                cChild = childMask;
-                cVisit = cChild & intersection_mask(false, level, px, py, pz, levels, r);
+            } else if (level == LL) {
+                const uint32_t* node = item_ptr(d, cIndex);
+                addr = node[1 + __popc(cChild & ((1u << nextChild) - 1u))];
+                const uint32_t* lp = item_ptr(d, addr);
+                leafLo = lp[0];
+                leafHi = lp[1];
+                cChild = first_child_mask(leafLo, leafHi);
+            } else { // get_second_child_mask, base_dag.h:53-58
+                cChild = (((nextChild & 4u) ? leafHi : leafLo) >> ((nextChild & 3u) * 8u)) & 0xFFu;
             }
+            cVisit = cChild & intersection_mask(false, level, px, py, pz, levels, r);
         }
     }
     if (px == 0 && py == 0 && pz == 0)
@@ -287,21 +283,16 @@ __device__ bool any_hit(const DevDag& d, uint32_t root, const RayF& r, float tma
             const uint32_t* node = item_ptr(d, cIndex);
             cIndex = node[1 + __popc(cChild & ((1u << nextChild) - 1u))];
             cChild = item_ptr(d, cIndex)[0] & 0xFFu;
-            cVisit = cChild & intersection_mask(false, level, px, py, pz, levels, r, tmax);
+        } else if (level == LL) {
+            const uint32_t* node = item_ptr(d, cIndex);
+            const uint32_t* lp = item_ptr(d, node[1 + __popc(cChild & ((1u << nextChild) - 1u))]);
+            leafLo = lp[0];
+            leafHi = lp[1];
+            cChild = first_child_mask(leafLo, leafHi);
         } else {
-            uint32_t childMask;
-            if (level == LL) {
-                const uint32_t* node = item_ptr(d, cIndex);
-                const uint32_t* lp = item_ptr(d, node[1 + __popc(cChild & ((1u << nextChild) - 1u))]);
-                leafLo = lp[0];
-                leafHi = lp[1];
-                childMask = first_child_mask(leafLo, leafHi);
-            } else {
-                childMask = (((nextChild & 4u) ? leafHi : leafLo) >> ((nextChild & 3u) * 8u)) & 0xFFu;
-            }
-            cChild = childMask;
-            cVisit = cChild & intersection_mask(false, level, px, py, pz, levels, r, tmax);
+            cChild = (((nextChild & 4u) ? leafHi : leafLo) >> ((nextChild & 3u) * 8u)) & 0xFFu;
         }
+        cVisit = cChild & intersection_mask(false, level, px, py, pz, levels, r, tmax);
     }
 }
 
