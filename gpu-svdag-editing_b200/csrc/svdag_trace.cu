@@ -132,19 +132,22 @@ __global__ void __launch_bounds__(256) k_trace(DevDag d, svdag_trace_params p, s
         uint32_t cIndex = root;
         uint32_t cChild = item_ptr(d, root)[0] & 0xFFu;
         uint32_t cVisit = cChild & intersection_mask(true, 0, 0, 0, 0, levels, r);
+        // Bit l of `live`: the stack entry of level l still has children to visit. Ascending to the
+        // deepest such level below the current one is what the reference's pop loop does one level
+        // at a time (entries in between have nothing left); here it is one bit scan.
+        uint32_t live = 0;
         for (;;) {
-            {
-                uint32_t newLevel = level;
-                while (newLevel > 0 && !cVisit) {
-                    newLevel--;
-                    cIndex = sIndex[newLevel][tix];
-                    cChild = sMasks[newLevel][tix] & 0xFFu;
-                    cVisit = sMasks[newLevel][tix] >> 8;
-                }
-                if (newLevel == 0 && !cVisit) {
+            if (!cVisit) {
+                const uint32_t cand = live & ((1u << level) - 1u);
+                if (!cand) {
                     px = py = pz = 0;
                     break;
                 }
+                const uint32_t newLevel = 31u - (uint32_t)__clz(cand);
+                cIndex = sIndex[newLevel][tix];
+                const uint32_t m = sMasks[newLevel][tix];
+                cChild = m & 0xFFu;
+                cVisit = m >> 8;
                 const uint32_t up = level - newLevel;
                 px >>= up;
                 py >>= up;
@@ -158,6 +161,7 @@ __global__ void __launch_bounds__(256) k_trace(DevDag d, svdag_trace_params p, s
             pz = (pz << 1) | (nextChild & 1u);
             sIndex[level][tix] = cIndex;
             sMasks[level][tix] = cChild | (cVisit << 8);
+            live = cVisit ? (live | (1u << level)) : (live & ~(1u << level));
             level++;
             if (level == levels) {
                 const uint32_t voxel = ((px & 1u) ? 4u : 0u) | ((py & 1u) ? 2u : 0u) | ((pz & 1u) ? 1u : 0u) | ((px & 2u) ? 32u : 0u)
@@ -252,17 +256,17 @@ __device__ bool any_hit(const DevDag& d, uint32_t root, const RayF& r, float tma
     uint32_t cIndex = root;
     uint32_t cChild = item_ptr(d, root)[0] & 0xFFu;
     uint32_t cVisit = cChild & intersection_mask(true, 0, 0, 0, 0, levels, r, tmax);
+    uint32_t live = 0; // as in k_trace: bit l set while stack level l has children left
     for (;;) {
-        {
-            uint32_t newLevel = level;
-            while (newLevel > 0 && !cVisit) {
-                newLevel--;
-                cIndex = sIndex[newLevel][tix];
-                cChild = sMasks[newLevel][tix] & 0xFFu;
-                cVisit = sMasks[newLevel][tix] >> 8;
-            }
-            if (newLevel == 0 && !cVisit)
+        if (!cVisit) {
+            const uint32_t cand = live & ((1u << level) - 1u);
+            if (!cand)
                 return false;
+            const uint32_t newLevel = 31u - (uint32_t)__clz(cand);
+            cIndex = sIndex[newLevel][tix];
+            const uint32_t m = sMasks[newLevel][tix];
+            cChild = m & 0xFFu;
+            cVisit = m >> 8;
             const uint32_t up = level - newLevel;
             px >>= up;
             py >>= up;
@@ -276,6 +280,7 @@ __device__ bool any_hit(const DevDag& d, uint32_t root, const RayF& r, float tma
         pz = (pz << 1) | (nextChild & 1u);
         sIndex[level][tix] = cIndex;
         sMasks[level][tix] = cChild | (cVisit << 8);
+        live = cVisit ? (live | (1u << level)) : (live & ~(1u << level));
         level++;
         if (level == levels)
             return true;
