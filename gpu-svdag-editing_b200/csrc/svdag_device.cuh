@@ -690,7 +690,10 @@ __device__ __forceinline__ uint32_t table_find_or_insert(const Grp<G>& g, const 
         const uint32_t item = claim_in_slab<G>(g, d, slab, body, empty, tag, key.n, true, s, key.ha >> 8, &snap);
         if (item != kNone) {
             write_item<G>(g, handle_ptr(d, item), key);
-            __threadfence();
+            if constexpr (G == 1)
+                fence_release(); // the writer publishes: a release orders its item before the tag
+            else
+                __threadfence();
             g.sync();
             if (g.lane == 0)
                 atomicXor(slab_ptr(d, slab) + (s >> 2), (kTagBusy ^ tag) << (8u * (s & 3u)));

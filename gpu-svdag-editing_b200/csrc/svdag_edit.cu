@@ -893,7 +893,8 @@ __device__ void ph_merge_level(const DevDag& d, uint32_t level, char* scratch)
 #pragma unroll
             for (uint32_t j = 0; j < kItemStride; ++j)
                 it[j] = key.w[j];
-            fence_release(); // the content is visible before the dedup entry that points at it
+            if (n > 1)
+                fence_release(); // the content is visible before the dedup entry that points at it
         }
         const bool isEmpty = isLeaf ? (key.w[0] == 0 && key.w[1] == 0) : ((key.w[0] & 0xFFu) == 0);
         if (isEmpty) {
@@ -902,7 +903,8 @@ __device__ void ph_merge_level(const DevDag& d, uint32_t level, char* scratch)
         }
         key.n = isLeaf ? dev_leaf_words(key.w[0], key.w[1]) : dev_node_words(key.w[0]);
         hash_words(key.w, key.n, key.ha, key.hb);
-        const uint32_t r = dedup_item(table, m.cap - 1u, items, i, key.w, key.n, key.ha, key.hb);
+        // a level of one item has no duplicates (the top levels of a small edit)
+        const uint32_t r = n > 1 ? dedup_item(table, m.cap - 1u, items, i, key.w, key.n, key.ha, key.hb) : i;
         rep[i] = r;
         if (r != i)
             continue;
