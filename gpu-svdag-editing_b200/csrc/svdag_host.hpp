@@ -110,6 +110,10 @@ svdag_status table_find_lanes(svdag_table* t, const uint32_t* keys, const uint32
 svdag_status launch_edits_at(svdag_ctx* ctx, const DevEditor* eds, uint32_t n, char* region, size_t regionBytes, cudaStream_t s);
 // A frame of the root stored at `root` (device word) instead of the current one (svdag_trace.cu).
 svdag_status trace_frame(svdag_ctx* ctx, const svdag_trace_params* p, svdag_hit* out, const uint32_t* root, cudaStream_t s);
+// The same frame over the previous frame of the same camera in `out`: only pixels whose ray meets one
+// of the boxes (6 floats each: min xyz, max xyz) are traced again.
+svdag_status trace_frame_incremental(svdag_ctx* ctx, const svdag_trace_params* p, svdag_hit* out, const uint32_t* root, const float* boxes,
+    uint32_t nBoxes, cudaStream_t s);
 // Procedural scene construction (svdag_scene.cu).
 svdag_status run_scene_build(svdag_ctx* ctx, const svdag_terrain_params* p, cudaStream_t s);
 

@@ -80,6 +80,38 @@ unsigned long long edit_reserve_bytes(const svdag_edit& e, uint32_t levels)
 
 double now_since(Clock::time_point t0) { return std::chrono::duration<double>(Clock::now() - t0).count(); }
 
+constexpr uint32_t kMaxFrameBoxes = 512; // changed regions one incremental frame tests; more: a whole frame
+
+// Boxes (min xyz, max xyz) holding every voxel an edit can change, grown by two voxels (the tracer
+// admits voxels within 1e-4 of a ray; the margin also covers float rounding of the box test).
+// Returns how many it wrote (a move changes its source and its destination).
+uint32_t edit_boxes(const svdag_edit& e, float* out)
+{
+    auto put = [&](float* b, float cx, float cy, float cz, float r) {
+        const float lo = r + 2.0f, hi = r + 3.0f; // the sphere centre is offset by +0.5, a box of radius 0 is one voxel
+        b[0] = cx - lo;
+        b[1] = cy - lo;
+        b[2] = cz - lo;
+        b[3] = cx + hi;
+        b[4] = cy + hi;
+        b[5] = cz + hi;
+    };
+    const float r = std::max(e.radius, 0.1f);
+    const float dx = e.dst[0] + (e.center[0] - e.src[0]), dy = e.dst[1] + (e.center[1] - e.src[1]), dz = e.dst[2] + (e.center[2] - e.src[2]);
+    switch (e.tool) {
+    case SVDAG_TOOL_COPY:
+        put(out, dx, dy, dz, r);
+        return 1;
+    case SVDAG_TOOL_MOVE:
+        put(out, e.center[0], e.center[1], e.center[2], r);
+        put(out + 6, dx, dy, dz, r);
+        return 2;
+    default:
+        put(out, e.center[0], e.center[1], e.center[2], r);
+        return 1;
+    }
+}
+
 } // namespace
 
 struct svdag_server {
@@ -99,6 +131,9 @@ struct svdag_server {
     std::vector<cudaEvent_t> events; // one per slot
     cudaEvent_t frameDone = nullptr;
     uint32_t* frameRoot = nullptr; // root the frame in flight shows (batches may commit meanwhile)
+    float* boxesDev = nullptr; // changed regions of an incremental frame
+    float* boxesHost = nullptr; // pinned staging (one frame in flight: reused only after it finished)
+    bool haveFrame = false; // `hits` holds a frame of lastFrame's camera
     unsigned long long capBytes = 0;
     unsigned long long usedBytes = 0; // item region in use after the last finished launch
 
@@ -116,7 +151,7 @@ struct svdag_server {
     uint32_t frameCovers = 0; // batches with launch < frameCovers are shown by the frame in flight
     uint32_t covered = 0; // batches with launch < covered have a frame launched behind them
     std::vector<Request> frameReqs, pendingFrames;
-    svdag_trace_params lastFrame {};
+    svdag_trace_params lastFrame {}; // camera of the last frame launched
     uint32_t launches = 0;
     std::thread worker;
 
@@ -168,7 +203,31 @@ struct svdag_server {
         if ((size_t)frame.width * frame.height > frameHits || frame.width == 0 || frame.height == 0)
             frame = cfg.frame;
         SVDAG_CUDA(cudaMemcpyAsync(frameRoot, &ctx->ctl->root, sizeof(uint32_t), cudaMemcpyDeviceToDevice, frameStream));
-        SVDAG_TRY(trace_frame(ctx, &frame, hits, frameRoot, frameStream));
+        // Incremental when the camera is the last frame's and only edits ran since (the batches from
+        // `covered` on are the ones launched after that frame).
+        bool whole = plain() || (cfg.flags & SVDAG_SERVE_FULL_FRAMES) || !haveFrame
+            || std::memcmp(&frame, &lastFrame, sizeof(frame)) != 0;
+        uint32_t nBoxes = 0;
+        for (auto it = batches.begin(); !whole && it != batches.end(); ++it) {
+            if (it->launch < covered)
+                continue;
+            for (auto& r : it->reqs) {
+                if (r.kind != 0 || nBoxes + 2 > kMaxFrameBoxes) {
+                    whole = true;
+                    break;
+                }
+                nBoxes += edit_boxes(r.edit, boxesHost + 6 * nBoxes);
+            }
+        }
+        if (whole) {
+            SVDAG_TRY(trace_frame(ctx, &frame, hits, frameRoot, frameStream));
+        } else {
+            if (nBoxes)
+                SVDAG_CUDA(cudaMemcpyAsync(boxesDev, boxesHost, nBoxes * 6 * sizeof(float), cudaMemcpyHostToDevice, frameStream));
+            SVDAG_TRY(trace_frame_incremental(ctx, &frame, hits, frameRoot, boxesDev, nBoxes, frameStream));
+        }
+        haveFrame = true;
+        lastFrame = frame;
         if (cfg.flags & SVDAG_SERVE_COPY_FRAMES)
             SVDAG_CUDA(cudaMemcpyAsync(hostHits, hits, (size_t)frame.width * frame.height * sizeof(svdag_hit), cudaMemcpyDeviceToHost,
                 frameStream));
@@ -421,6 +480,8 @@ svdag_status svdag_server_create(svdag_ctx* ctx, const svdag_server_config* conf
     fail(cudaStreamCreateWithFlags(&s->frameStream, cudaStreamNonBlocking));
     fail(cudaEventCreateWithFlags(&s->frameDone, cudaEventDisableTiming));
     fail(cudaMalloc(&s->frameRoot, 256));
+    fail(cudaMalloc(&s->boxesDev, kMaxFrameBoxes * 6 * sizeof(float)));
+    fail(cudaMallocHost(&s->boxesHost, kMaxFrameBoxes * 6 * sizeof(float)));
     fail(cudaMalloc(&s->hits, s->frameHits * sizeof(svdag_hit)));
     if (config->flags & SVDAG_SERVE_COPY_FRAMES)
         fail(cudaMallocHost(&s->hostHits, s->frameHits * sizeof(svdag_hit)));
@@ -488,6 +549,10 @@ svdag_status svdag_server_destroy(svdag_server* s)
         cudaFree(s->hits);
     if (s->frameRoot)
         cudaFree(s->frameRoot);
+    if (s->boxesDev)
+        cudaFree(s->boxesDev);
+    if (s->boxesHost)
+        cudaFreeHost(s->boxesHost);
     if (s->frameDone)
         cudaEventDestroy(s->frameDone);
     if (s->stream)

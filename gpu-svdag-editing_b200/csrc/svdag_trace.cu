@@ -94,7 +94,26 @@ __device__ __forceinline__ uint32_t first_child_mask(uint32_t lo, uint32_t hi) /
     return out;
 }
 
-__global__ void __launch_bounds__(256) k_trace(DevDag d, svdag_trace_params p, svdag_hit* out, const uint32_t* rootPtr)
+// Whether the ray meets the box [b0..b2] x [b3..b5] at some t >= 0 (slab test; a NaN from a zero
+// direction component on a slab boundary drops that slab's constraint, which only widens the test).
+__device__ __forceinline__ bool ray_meets_box(const RayF& r, const float* b)
+{
+    const float t1x = (b[0] - r.ox) * r.ix, t2x = (b[3] - r.ox) * r.ix;
+    const float t1y = (b[1] - r.oy) * r.iy, t2y = (b[4] - r.oy) * r.iy;
+    const float t1z = (b[2] - r.oz) * r.iz, t2z = (b[5] - r.oz) * r.iz;
+    const float tnear = fmaxf(fmaxf(fminf(t1x, t2x), fminf(t1y, t2y)), fmaxf(fminf(t1z, t2z), 0.0f));
+    const float tfar = fminf(fminf(fmaxf(t1x, t2x), fmaxf(t1y, t2y)), fmaxf(t1z, t2z));
+    return tnear <= tfar;
+}
+
+// Primary rays. With INCR the buffer holds the previous frame of the same camera and only pixels
+// whose ray meets one of `boxes` (the changed regions since that frame, grown by a margin) are traced
+// again. The traversal only ever inspects voxels within the intersection test's tolerance (1e-4) of
+// the ray, and which ones it admits depends on the ray alone, so a pixel whose ray meets no changed
+// region finds the same voxel as before: its record is already right.
+template <bool INCR>
+__global__ void __launch_bounds__(256) k_trace(DevDag d, svdag_trace_params p, svdag_hit* out, const uint32_t* rootPtr,
+    const float* boxes, uint32_t nBoxes)
 {
     const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t y = blockIdx.y * blockDim.y + threadIdx.y;
@@ -117,6 +136,13 @@ __global__ void __launch_bounds__(256) k_trace(DevDag d, svdag_trace_params p, s
     r.ix = 1.0f / r.dx;
     r.iy = 1.0f / r.dy;
     r.iz = 1.0f / r.dz;
+    if constexpr (INCR) {
+        bool touched = false;
+        for (uint32_t b = 0; b < nBoxes && !touched; ++b)
+            touched = ray_meets_box(r, boxes + 6 * b);
+        if (!touched)
+            return;
+    }
 
     // intersect_ray, tracer.cu:186-273.
     const uint32_t levels = d.levels, LL = d.leafLevel;
@@ -528,7 +554,17 @@ svdag_status trace_frame(svdag_ctx* ctx, const svdag_trace_params* p, svdag_hit*
 {
     const dim3 block(32, 8);
     const dim3 grid((p->width + block.x - 1) / block.x, (p->height + block.y - 1) / block.y);
-    k_trace<<<grid, block, 0, s>>>(ctx->dag(), *p, out, root);
+    k_trace<false><<<grid, block, 0, s>>>(ctx->dag(), *p, out, root, nullptr, 0);
+    SVDAG_CUDA(cudaGetLastError());
+    return SVDAG_OK;
+}
+
+svdag_status trace_frame_incremental(svdag_ctx* ctx, const svdag_trace_params* p, svdag_hit* out, const uint32_t* root, const float* boxes,
+    uint32_t nBoxes, cudaStream_t s)
+{
+    const dim3 block(32, 8);
+    const dim3 grid((p->width + block.x - 1) / block.x, (p->height + block.y - 1) / block.y);
+    k_trace<true><<<grid, block, 0, s>>>(ctx->dag(), *p, out, root, boxes, nBoxes);
     SVDAG_CUDA(cudaGetLastError());
     return SVDAG_OK;
 }
@@ -545,7 +581,7 @@ svdag_status svdag_trace_primary(svdag_ctx* ctx, const svdag_trace_params* p, sv
         return SVDAG_ERR_INVALID;
     const dim3 block(32, 8);
     const dim3 grid((p->width + block.x - 1) / block.x, (p->height + block.y - 1) / block.y);
-    k_trace<<<grid, block, 0, as_stream(stream)>>>(ctx->dag(), *p, out, nullptr);
+    k_trace<false><<<grid, block, 0, as_stream(stream)>>>(ctx->dag(), *p, out, nullptr, nullptr, 0);
     SVDAG_CUDA(cudaGetLastError());
     return SVDAG_OK;
 }

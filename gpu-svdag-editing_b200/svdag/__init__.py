@@ -107,7 +107,7 @@ RESULT_DTYPE = np.dtype([("ticket", "<u8"), ("kind", "<u4"), ("status", "<u4"), 
                          ("launch", "<u4"), ("edited_voxels", "<u8"), ("submit_s", "<f8"), ("visible_s", "<f8")])
 assert RESULT_DTYPE.itemsize == C.sizeof(RequestResult) == 48
 
-SERVE_PLAIN, SERVE_COPY_FRAMES = 1, 2
+SERVE_PLAIN, SERVE_COPY_FRAMES, SERVE_FULL_FRAMES = 1, 2, 4
 
 
 class ShadeParams(C.Structure):
@@ -764,11 +764,12 @@ class Server:
     plain=True it is the per-edit baseline: one request at a time, each edit followed by a frame."""
 
     def __init__(self, dag: MyGPUHashDAG, frame: TraceParams, max_batch: int = 256, max_inflight: int = 2,
-                 memory_cap_bytes: int = 0, plain: bool = False, copy_frames: bool = False):
+                 memory_cap_bytes: int = 0, plain: bool = False, copy_frames: bool = False, full_frames: bool = False):
         self.dag = dag
         self.frame_params = frame
+        flags = (SERVE_PLAIN if plain else 0) | (SERVE_COPY_FRAMES if copy_frames else 0) | (SERVE_FULL_FRAMES if full_frames else 0)
         cfg = ServerConfig(max_batch=max_batch, max_inflight=max_inflight, memory_cap_bytes=memory_cap_bytes,
-                           frame=frame, flags=(SERVE_PLAIN if plain else 0) | (SERVE_COPY_FRAMES if copy_frames else 0))
+                           frame=frame, flags=flags)
         h = C.c_void_p()
         _check(lib().svdag_server_create(dag.h, C.byref(cfg), C.byref(h)), "svdag_server_create")
         self.h = h

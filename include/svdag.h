@@ -431,6 +431,11 @@ svdag_status svdag_set_tuning(svdag_ctx* ctx, const svdag_tuning* tuning);
 
 #define SVDAG_SERVE_PLAIN 1u /* one request per launch, synchronously */
 #define SVDAG_SERVE_COPY_FRAMES 2u /* copy every rendered frame to host memory (svdag_server_frame) */
+/* Trace every frame whole. Without it, a frame of the same camera as the one before is traced only
+ * where a ray meets the bounding box of an edit made since (the other pixels keep their records,
+ * which a whole frame would reproduce bit for bit); undo and redo, a new camera and the first frame
+ * are traced whole. SVDAG_SERVE_PLAIN always traces whole frames, as the reference's loop does. */
+#define SVDAG_SERVE_FULL_FRAMES 4u
 
 typedef struct svdag_server_config {
     uint32_t max_batch; /* edits per launch; 0 = 256 */
