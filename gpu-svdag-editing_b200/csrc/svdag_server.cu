@@ -81,6 +81,41 @@ unsigned long long edit_reserve_bytes(const svdag_edit& e, uint32_t levels)
 double now_since(Clock::time_point t0) { return std::chrono::duration<double>(Clock::now() - t0).count(); }
 
 constexpr uint32_t kMaxFrameBoxes = 512; // changed regions one incremental frame tests; more: a whole frame
+constexpr uint32_t kMaxCopyRuns = 16; // row runs copied to the host after an incremental frame; more: the whole frame
+
+// Hit-buffer rows [row0, row1] that rays meeting `box` can come from. Pixel (x, y) looks along
+// ray_min + x * ddx + y * ddy - camera, so a point P is seen at the (x, y) solving
+// P - camera = s * (ray_min - camera) + (s x) * ddx + (s y) * ddy; the rays meeting a box in front of
+// the camera pass inside the projection of its corners. False when a corner is not in front.
+bool box_rows(const svdag_trace_params& p, const float* box, int64_t& row0, int64_t& row1)
+{
+    const double a[3] = { p.ray_min[0] - p.camera[0], p.ray_min[1] - p.camera[1], p.ray_min[2] - p.camera[2] };
+    const double* u = p.ray_ddx;
+    const double* v = p.ray_ddy;
+    auto det = [](const double* c0, const double* c1, const double* c2) {
+        return c0[0] * (c1[1] * c2[2] - c1[2] * c2[1]) - c1[0] * (c0[1] * c2[2] - c0[2] * c2[1]) + c2[0] * (c0[1] * c1[2] - c0[2] * c1[1]);
+    };
+    const double D = det(a, u, v);
+    if (!(std::fabs(D) > 0.0))
+        return false;
+    double ymin = 1e300, ymax = -1e300;
+    for (int k = 0; k < 8; ++k) {
+        const double q[3] = { (k & 1 ? box[3] : box[0]) - p.camera[0], (k & 2 ? box[4] : box[1]) - p.camera[1],
+            (k & 4 ? box[5] : box[2]) - p.camera[2] };
+        const double s = det(q, u, v) / D; // Cramer's rule for (s, s x, s y)
+        if (!(s > 1e-9))
+            return false;
+        const double y = (det(a, u, q) / D) / s;
+        ymin = std::min(ymin, y);
+        ymax = std::max(ymax, y);
+    }
+    const int64_t y0 = (int64_t)std::floor(std::max(ymin, -4.0)) - 2, y1 = (int64_t)std::ceil(std::min(ymax, (double)p.height + 4.0)) + 2;
+    row0 = (int64_t)p.height - 1 - y1;
+    row1 = (int64_t)p.height - 1 - y0;
+    row0 = std::max<int64_t>(row0, 0);
+    row1 = std::min<int64_t>(row1, (int64_t)p.height - 1);
+    return true;
+}
 
 // Boxes (min xyz, max xyz) holding every voxel an edit can change, grown by two voxels (the tracer
 // admits voxels within 1e-4 of a ray; the margin also covers float rounding of the box test).
@@ -228,9 +263,37 @@ struct svdag_server {
         }
         haveFrame = true;
         lastFrame = frame;
-        if (cfg.flags & SVDAG_SERVE_COPY_FRAMES)
-            SVDAG_CUDA(cudaMemcpyAsync(hostHits, hits, (size_t)frame.width * frame.height * sizeof(svdag_hit), cudaMemcpyDeviceToHost,
-                frameStream));
+        if (cfg.flags & SVDAG_SERVE_COPY_FRAMES) {
+            // After an incremental frame only the rows its boxes project to can differ from the host
+            // copy of the previous frame.
+            std::vector<std::pair<int64_t, int64_t>> runs;
+            bool all = whole;
+            for (uint32_t b = 0; b < nBoxes && !all; ++b) {
+                int64_t r0, r1;
+                if (!box_rows(frame, boxesHost + 6 * b, r0, r1))
+                    all = true;
+                else if (r0 <= r1)
+                    runs.emplace_back(r0, r1);
+            }
+            std::sort(runs.begin(), runs.end());
+            std::vector<std::pair<int64_t, int64_t>> merged;
+            for (auto& r : runs) {
+                if (!merged.empty() && r.first <= merged.back().second + 1)
+                    merged.back().second = std::max(merged.back().second, r.second);
+                else
+                    merged.push_back(r);
+            }
+            if (merged.size() > kMaxCopyRuns)
+                all = true;
+            const size_t rowBytes = (size_t)frame.width * sizeof(svdag_hit);
+            if (all) {
+                SVDAG_CUDA(cudaMemcpyAsync(hostHits, hits, rowBytes * frame.height, cudaMemcpyDeviceToHost, frameStream));
+            } else {
+                for (auto& r : merged)
+                    SVDAG_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(hostHits) + rowBytes * r.first, reinterpret_cast<const char*>(hits) + rowBytes * r.first,
+                        rowBytes * (size_t)(r.second - r.first + 1), cudaMemcpyDeviceToHost, frameStream));
+            }
+        }
         SVDAG_CUDA(cudaEventRecord(frameDone, frameStream));
         frameActive = true;
         frameCovers = covered = launches;
