@@ -83,11 +83,11 @@ double now_since(Clock::time_point t0) { return std::chrono::duration<double>(Cl
 constexpr uint32_t kMaxFrameBoxes = 512; // changed regions one incremental frame tests; more: a whole frame
 constexpr uint32_t kMaxCopyRuns = 16; // row runs copied to the host after an incremental frame; more: the whole frame
 
-// Hit-buffer rows [row0, row1] that rays meeting `box` can come from. Pixel (x, y) looks along
+// Hit-buffer rows [row0, row1] and columns [col0, col1] that rays meeting `box` can come from. Pixel (x, y) looks along
 // ray_min + x * ddx + y * ddy - camera, so a point P is seen at the (x, y) solving
 // P - camera = s * (ray_min - camera) + (s x) * ddx + (s y) * ddy; the rays meeting a box in front of
 // the camera pass inside the projection of its corners. False when a corner is not in front.
-bool box_rows(const svdag_trace_params& p, const float* box, int64_t& row0, int64_t& row1)
+bool box_rows(const svdag_trace_params& p, const float* box, int64_t& row0, int64_t& row1, int64_t& col0, int64_t& col1)
 {
     const double a[3] = { p.ray_min[0] - p.camera[0], p.ray_min[1] - p.camera[1], p.ray_min[2] - p.camera[2] };
     const double* u = p.ray_ddx;
@@ -98,7 +98,7 @@ bool box_rows(const svdag_trace_params& p, const float* box, int64_t& row0, int6
     const double D = det(a, u, v);
     if (!(std::fabs(D) > 0.0))
         return false;
-    double ymin = 1e300, ymax = -1e300;
+    double ymin = 1e300, ymax = -1e300, xmin = 1e300, xmax = -1e300;
     for (int k = 0; k < 8; ++k) {
         const double q[3] = { (k & 1 ? box[3] : box[0]) - p.camera[0], (k & 2 ? box[4] : box[1]) - p.camera[1],
             (k & 4 ? box[5] : box[2]) - p.camera[2] };
@@ -106,9 +106,14 @@ bool box_rows(const svdag_trace_params& p, const float* box, int64_t& row0, int6
         if (!(s > 1e-9))
             return false;
         const double y = (det(a, u, q) / D) / s;
+        const double x = (det(a, q, v) / D) / s;
         ymin = std::min(ymin, y);
         ymax = std::max(ymax, y);
+        xmin = std::min(xmin, x);
+        xmax = std::max(xmax, x);
     }
+    col0 = std::max<int64_t>((int64_t)std::floor(std::max(xmin, -4.0)) - 2, 0);
+    col1 = std::min<int64_t>((int64_t)std::ceil(std::min(xmax, (double)p.width + 4.0)) + 2, (int64_t)p.width - 1);
     const int64_t y0 = (int64_t)std::floor(std::max(ymin, -4.0)) - 2, y1 = (int64_t)std::ceil(std::min(ymax, (double)p.height + 4.0)) + 2;
     row0 = (int64_t)p.height - 1 - y1;
     row1 = (int64_t)p.height - 1 - y0;
@@ -264,24 +269,32 @@ struct svdag_server {
         haveFrame = true;
         lastFrame = frame;
         if (cfg.flags & SVDAG_SERVE_COPY_FRAMES) {
-            // After an incremental frame only the rows its boxes project to can differ from the host
-            // copy of the previous frame.
-            std::vector<std::pair<int64_t, int64_t>> runs;
+            // After an incremental frame only the pixels its boxes project to can differ from the host
+            // copy of the previous frame: runs of rows, each with the union of its boxes' columns,
+            // copied as one rectangle each.
+            struct Run {
+                int64_t r0, r1, c0, c1;
+            };
+            std::vector<Run> runs;
             bool all = whole;
             for (uint32_t b = 0; b < nBoxes && !all; ++b) {
-                int64_t r0, r1;
-                if (!box_rows(frame, boxesHost + 6 * b, r0, r1))
+                Run r {};
+                if (!box_rows(frame, boxesHost + 6 * b, r.r0, r.r1, r.c0, r.c1))
                     all = true;
-                else if (r0 <= r1)
-                    runs.emplace_back(r0, r1);
+                else if (r.r0 <= r.r1 && r.c0 <= r.c1)
+                    runs.push_back(r);
             }
-            std::sort(runs.begin(), runs.end());
-            std::vector<std::pair<int64_t, int64_t>> merged;
+            std::sort(runs.begin(), runs.end(), [](const Run& a, const Run& b) { return a.r0 < b.r0; });
+            std::vector<Run> merged;
             for (auto& r : runs) {
-                if (!merged.empty() && r.first <= merged.back().second + 1)
-                    merged.back().second = std::max(merged.back().second, r.second);
-                else
+                if (!merged.empty() && r.r0 <= merged.back().r1 + 1) {
+                    Run& m = merged.back();
+                    m.r1 = std::max(m.r1, r.r1);
+                    m.c0 = std::min(m.c0, r.c0);
+                    m.c1 = std::max(m.c1, r.c1);
+                } else {
                     merged.push_back(r);
+                }
             }
             if (merged.size() > kMaxCopyRuns)
                 all = true;
@@ -289,9 +302,12 @@ struct svdag_server {
             if (all) {
                 SVDAG_CUDA(cudaMemcpyAsync(hostHits, hits, rowBytes * frame.height, cudaMemcpyDeviceToHost, frameStream));
             } else {
-                for (auto& r : merged)
-                    SVDAG_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(hostHits) + rowBytes * r.first, reinterpret_cast<const char*>(hits) + rowBytes * r.first,
-                        rowBytes * (size_t)(r.second - r.first + 1), cudaMemcpyDeviceToHost, frameStream));
+                for (auto& r : merged) {
+                    const size_t off = rowBytes * (size_t)r.r0 + sizeof(svdag_hit) * (size_t)r.c0;
+                    SVDAG_CUDA(cudaMemcpy2DAsync(reinterpret_cast<char*>(hostHits) + off, rowBytes, reinterpret_cast<const char*>(hits) + off,
+                        rowBytes, sizeof(svdag_hit) * (size_t)(r.c1 - r.c0 + 1), (size_t)(r.r1 - r.r0 + 1), cudaMemcpyDeviceToHost,
+                        frameStream));
+                }
             }
         }
         SVDAG_CUDA(cudaEventRecord(frameDone, frameStream));
