@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
@@ -174,6 +175,7 @@ struct svdag_server {
     float* boxesDev = nullptr; // changed regions of an incremental frame
     float* boxesHost = nullptr; // pinned staging (one frame in flight: reused only after it finished)
     bool haveFrame = false; // `hits` holds a frame of lastFrame's camera
+    std::atomic<unsigned long long> framesWhole { 0 }, framesIncremental { 0 }, frameBytesToHost { 0 };
     unsigned long long capBytes = 0;
     unsigned long long usedBytes = 0; // item region in use after the last finished launch
 
@@ -268,6 +270,7 @@ struct svdag_server {
         }
         haveFrame = true;
         lastFrame = frame;
+        (whole ? framesWhole : framesIncremental).fetch_add(1);
         if (cfg.flags & SVDAG_SERVE_COPY_FRAMES) {
             // After an incremental frame only the pixels its boxes project to can differ from the host
             // copy of the previous frame: runs of rows, each with the union of its boxes' columns,
@@ -301,8 +304,10 @@ struct svdag_server {
             const size_t rowBytes = (size_t)frame.width * sizeof(svdag_hit);
             if (all) {
                 SVDAG_CUDA(cudaMemcpyAsync(hostHits, hits, rowBytes * frame.height, cudaMemcpyDeviceToHost, frameStream));
+                frameBytesToHost.fetch_add(rowBytes * frame.height);
             } else {
                 for (auto& r : merged) {
+                    frameBytesToHost.fetch_add(sizeof(svdag_hit) * (size_t)(r.c1 - r.c0 + 1) * (size_t)(r.r1 - r.r0 + 1));
                     const size_t off = rowBytes * (size_t)r.r0 + sizeof(svdag_hit) * (size_t)r.c0;
                     SVDAG_CUDA(cudaMemcpy2DAsync(reinterpret_cast<char*>(hostHits) + off, rowBytes, reinterpret_cast<const char*>(hits) + off,
                         rowBytes, sizeof(svdag_hit) * (size_t)(r.c1 - r.c0 + 1), (size_t)(r.r1 - r.r0 + 1), cudaMemcpyDeviceToHost,
@@ -702,6 +707,19 @@ svdag_status svdag_poll(svdag_server* s, uint64_t ticket, int wait, svdag_reques
     }
     *out = it->second;
     s->done.erase(it);
+    return SVDAG_OK;
+}
+
+svdag_status svdag_server_counters(svdag_server* s, uint64_t* whole, uint64_t* incremental, uint64_t* bytesToHost)
+{
+    if (!s)
+        return SVDAG_ERR_INVALID;
+    if (whole)
+        *whole = s->framesWhole.load();
+    if (incremental)
+        *incremental = s->framesIncremental.load();
+    if (bytesToHost)
+        *bytesToHost = s->frameBytesToHost.load();
     return SVDAG_OK;
 }
 

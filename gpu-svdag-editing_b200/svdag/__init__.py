@@ -214,6 +214,7 @@ _PROTOS = {
     "svdag_submit_frame": [_P, C.POINTER(TraceParams), C.POINTER(_U64)],
     "svdag_poll": [_P, _U64, C.c_int, C.POINTER(RequestResult)],
     "svdag_server_frame": [_P, _P, _U64],
+    "svdag_server_counters": [_P, C.POINTER(_U64), C.POINTER(_U64), C.POINTER(_U64)],
     "svdag_server_replay": [_P, C.POINTER(Edit), _P, _U32, _P, _U32, _P],
     "svdag_submit_undo": [_P, C.c_int, C.POINTER(_U64)],
     "svdag_replay_parse": [C.c_char_p, _U64, C.c_float, _P, _U64, C.POINTER(_U64), C.POINTER(_U64)],
@@ -811,6 +812,12 @@ class Server:
         _check(lib().svdag_server_replay(self.h, arr, et.ctypes.data, len(edits), ft.ctypes.data, len(ft),
                                          out.ctypes.data), "svdag_server_replay")
         return out
+
+    def counters(self) -> dict:
+        """Frames traced whole and incrementally so far, bytes of frames copied to the host."""
+        a, b, c = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        _check(lib().svdag_server_counters(self.h, C.byref(a), C.byref(b), C.byref(c)), "svdag_server_counters")
+        return {"frames_whole": a.value, "frames_incremental": b.value, "frame_bytes_to_host": c.value}
 
     def submit_undo(self, redo: bool = False) -> int:
         t = C.c_uint64()

@@ -468,6 +468,10 @@ svdag_status svdag_submit_frame(svdag_server* server, const svdag_trace_params* 
 /* Result of a request: with wait = 0 returns SVDAG_ERR_BUSY while it is not visible yet. A result is
  * handed out once. */
 svdag_status svdag_poll(svdag_server* server, uint64_t ticket, int wait, svdag_request_result* out);
+/* Frames launched so far, traced whole and incrementally, and the bytes of frames copied to host
+ * memory (SVDAG_SERVE_COPY_FRAMES). Any pointer may be NULL. No counterpart in the reference. */
+svdag_status svdag_server_counters(svdag_server* server, uint64_t* frames_whole, uint64_t* frames_incremental,
+    uint64_t* frame_bytes_to_host);
 /* Copies the most recent frame (SVDAG_SERVE_COPY_FRAMES) to `out` (width * height hits). */
 svdag_status svdag_server_frame(svdag_server* server, svdag_hit* out, uint64_t capacity);
 /* Replays a timed request stream (the reference's replay of recorded edits, replay.h): edit i is

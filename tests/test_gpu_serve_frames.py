@@ -94,4 +94,9 @@ def test_incremental_frames_equal_whole_frames(svdag_lib, oracle_mod):
             for tk in tickets:
                 assert srv.poll(tk).status == 0
             compare_hits(srv.frame(), o.trace(po, threads=8))
+        c = srv.counters()
+        # the first frame and the undo/redo waves are whole, the other waves incremental
+        assert c["frames_whole"] >= 3 and c["frames_incremental"] >= 8
+        whole_bytes = 256 * 192 * 68
+        assert whole_bytes * c["frames_whole"] <= c["frame_bytes_to_host"] < whole_bytes * (c["frames_whole"] + c["frames_incremental"])
     g.free()
