@@ -111,9 +111,10 @@ __device__ __forceinline__ bool ray_meets_box(const RayF& r, const float* b)
 // again. The traversal only ever inspects voxels within the intersection test's tolerance (1e-4) of
 // the ray, and which ones it admits depends on the ray alone, so a pixel whose ray meets no changed
 // region finds the same voxel as before: its record is already right. That holds while the inverse
-// direction is finite: with an infinite component (a zero or denormal direction component) the
-// intersection test computes 0 * inf = NaN on node planes through the origin and can admit voxels
-// off the ray, so such pixels are always traced again.
+// direction stays far from overflow: with an infinite component (a zero or denormal direction
+// component) the intersection test computes 0 * inf = NaN on node planes through the origin and can
+// admit voxels off the ray, and a component above 1e30 can overflow its products to infinity, so
+// such pixels are always traced again.
 template <bool INCR>
 __global__ void __launch_bounds__(256) k_trace(DevDag d, svdag_trace_params p, svdag_hit* out, const uint32_t* rootPtr,
     const float* boxes, uint32_t nBoxes)
@@ -140,7 +141,7 @@ __global__ void __launch_bounds__(256) k_trace(DevDag d, svdag_trace_params p, s
     r.iy = 1.0f / r.dy;
     r.iz = 1.0f / r.dz;
     if constexpr (INCR) {
-        bool touched = isinf(r.ix) || isinf(r.iy) || isinf(r.iz);
+        bool touched = !(fabsf(r.ix) <= 1e30f && fabsf(r.iy) <= 1e30f && fabsf(r.iz) <= 1e30f);
         for (uint32_t b = 0; b < nBoxes && !touched; ++b)
             touched = ray_meets_box(r, boxes + 6 * b);
         if (!touched)
