@@ -1,0 +1,407 @@
+// svdag_alt_tables.cu - kernels and C ABI of the alternative table layouts (svdag_alt_tables.cuh).
+//
+// Two launch forms per operation, as the reference's table benchmark has them
+// (extras/hashmap_bench/src/main.cu:125-200):
+//  * thread per key (lanes = 1): the layout functions of svdag_alt_tables.cuh as they are;
+//  * warp-hybrid (lanes = 32; addAsWarpHybrid / findAsWarpHybrid): every lane holds a key, and the
+//    warp serves the lanes' keys one at a time, each lane inspecting one slot of the slab, so a slab
+//    is read with one coalesced load of its slot words (128 to 256 bytes) instead of 31 dependent ones.
+// Layouts are template arguments: a kernel's copy of the table descriptor gets its layout field
+// set to the constant, so the layout branches of the shared functions fold at compile time.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <new>
+
+#include "svdag_alt_tables.cuh"
+#include "svdag_host.hpp"
+
+using namespace svdag;
+using namespace svdag::alt;
+
+struct svdag_alt_table {
+    svdag_ctx* ctx = nullptr;
+    AltTable t {};
+    void* mem = nullptr;
+    unsigned long long* countDev = nullptr; // stats scratch
+};
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+__device__ __forceinline__ const uint32_t* shfl_ptr(const uint32_t* p, int src)
+{
+    return (const uint32_t*)__shfl_sync(kFull, (unsigned long long)p, src);
+}
+__device__ __forceinline__ uint64_t shfl64(uint64_t v, int src) { return __shfl_sync(kFull, (unsigned long long)v, src); }
+
+template <uint32_t L>
+__device__ __forceinline__ AltTable with_layout(const AltTable& t)
+{
+    AltTable c = t;
+    c.layout = L;
+    return c;
+}
+
+// Slot match of lane `lane` in slab s for the broadcast key (warp-hybrid find).
+template <uint32_t L>
+__device__ __forceinline__ bool lane_match(const AltTable& t, const uint32_t* s, uint32_t lane, const uint32_t* key, uint32_t tag,
+    uint64_t prefix)
+{
+    const uint32_t k = t.k;
+    if (L == kTicketBoard)
+        return ((s[0] >> lane) & 1u) && words_equal(s + body_word(L, k, lane), key, k);
+    if (L == kAtomic64)
+        return lane < 31u && ((const uint64_t*)s)[lane] == prefix && words_equal(s + body_word(L, k, lane), key + 2, k - 2u);
+    return lane >= 1u && s[lane] == tag && words_equal(s + body_word(L, k, lane), key, k);
+}
+
+// findAsWarpHybrid: returns this lane's result (kInvalid for a miss or an invalid lane).
+template <uint32_t L>
+__device__ uint32_t warp_find(const AltTable& t, const uint32_t* key, bool valid)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t tag = 0, slab = 0, result = kInvalid;
+    uint64_t prefix = 0;
+    if (valid) {
+        const uint32_t acc = key_acc(key, t.k);
+        tag = acc_tag32(acc);
+        prefix = L == kAtomic64 ? key_prefix(key) : 0;
+        slab = bucket_index(bucket_hash(acc), t.numBuckets);
+        valid = !(L == kAtomic64 && prefix == 0);
+    }
+    bool active = valid;
+    uint32_t steps = 0;
+    for (uint32_t mask; (mask = __ballot_sync(kFull, active)) != 0;) {
+        if (++steps > kMaxSteps) { // warp-uniform
+            if (active)
+                set_status(t, SVDAG_ERR_TIMEOUT);
+            break;
+        }
+        const int src = __ffs(mask) - 1;
+        const uint32_t sSlab = __shfl_sync(kFull, slab, src);
+        const uint32_t sTag = __shfl_sync(kFull, tag, src);
+        const uint64_t sPrefix = shfl64(prefix, src);
+        const uint32_t* sKey = shfl_ptr(key, src);
+        const uint32_t* s = slab_at(t, sSlab);
+        const uint32_t hits = __ballot_sync(kFull, lane_match<L>(t, s, lane, sKey, sTag, sPrefix));
+        if (lane == (uint32_t)src) {
+            if (hits) {
+                result = sSlab * 32u + (__ffs(hits) - 1u);
+                active = false;
+            } else {
+                const uint32_t nx = s[next_word(L)];
+                if (nx == 0) {
+                    active = false;
+                } else if (nx < t.numBuckets || nx >= t.slabCount) {
+                    set_status(t, SVDAG_ERR_CORRUPT);
+                    active = false;
+                } else {
+                    slab = nx;
+                }
+            }
+        }
+    }
+    return result;
+}
+
+// addAsWarpHybrid: returns this lane's handle (kInvalid for an invalid lane or on failure).
+template <uint32_t L>
+__device__ uint32_t warp_add(const AltTable& t, const uint32_t* key, bool valid)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t k = t.k;
+    uint32_t tag = 0, slab = 0, result = kInvalid;
+    uint64_t prefix = 0;
+    if (valid) {
+        const uint32_t acc = key_acc(key, k);
+        tag = acc_tag32(acc);
+        prefix = L == kAtomic64 ? key_prefix(key) : 0;
+        slab = bucket_index(bucket_hash(acc), t.numBuckets);
+        if (L == kAtomic64 && prefix == 0) {
+            set_status(t, SVDAG_ERR_INVALID);
+            valid = false;
+        }
+    }
+    bool active = valid;
+    uint32_t steps = 0;
+    for (uint32_t mask; (mask = __ballot_sync(kFull, active)) != 0;) {
+        if (++steps > kMaxSteps) { // warp-uniform
+            if (active)
+                set_status(t, SVDAG_ERR_TIMEOUT);
+            break;
+        }
+        const int src = __ffs(mask) - 1;
+        const uint32_t sSlab = __shfl_sync(kFull, slab, src);
+        const uint32_t sTag = __shfl_sync(kFull, tag, src);
+        const uint64_t sPrefix = shfl64(prefix, src);
+        const uint32_t* sKey = shfl_ptr(key, src);
+        uint32_t* s = slab_at(t, sSlab);
+        uint32_t slot = kInvalid;
+        if (L == kTicketBoard) {
+            // one lane claims on the slot mask (at most 32 failed ORs)
+            if (lane == (uint32_t)src)
+                slot = try_claim(t, s, sTag, sPrefix);
+            slot = __shfl_sync(kFull, slot, src);
+        } else {
+            // every lane reads its slot word; the free ones are tried in order (each failed CAS is a
+            // slot another warp took)
+            const bool mine = L == kAtomic64 ? lane < 31u : lane >= 1u;
+            const bool isFree = mine && (L == kAtomic64 ? ld_relaxed64((const uint64_t*)s + lane) == 0 : ld_relaxed(s + lane) == 0);
+            uint32_t freeMask = __ballot_sync(kFull, isFree);
+            while (freeMask) {
+                const uint32_t d = __ffs(freeMask) - 1u;
+                bool won = false;
+                if (lane == d)
+                    won = L == kAtomic64 ? cas64((uint64_t*)s + d, 0, sPrefix) == 0 : cas32(s + d, 0u, sTag) == 0;
+                if (__shfl_sync(kFull, won, d)) {
+                    slot = d;
+                    break;
+                }
+                freeMask &= freeMask - 1u;
+            }
+        }
+        if (slot != kInvalid) {
+            const uint32_t first = L == kAtomic64 ? 2u : 0u;
+            if (lane < k - first)
+                s[body_word(L, k, slot) + lane] = sKey[first + lane];
+            if (lane == (uint32_t)src) {
+                result = sSlab * 32u + slot;
+                active = false;
+            }
+        } else if (lane == (uint32_t)src) {
+            const uint32_t nx = next_or_link(t, s);
+            if (nx == kNoSlab)
+                active = false;
+            else
+                slab = nx;
+        }
+    }
+    return result;
+}
+
+template <uint32_t L>
+__global__ void k_alt_add(AltTable t0, const uint32_t* __restrict__ keys, uint32_t n, uint32_t* __restrict__ handles)
+{
+    const AltTable t = with_layout<L>(t0);
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        handles[i] = add(t, keys + (uint64_t)i * t.k);
+}
+
+template <uint32_t L>
+__global__ void k_alt_find(AltTable t0, const uint32_t* __restrict__ keys, uint32_t n, uint32_t* __restrict__ handles)
+{
+    const AltTable t = with_layout<L>(t0);
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        handles[i] = find(t, keys + (uint64_t)i * t.k);
+}
+
+// Warp-hybrid forms: the loop bound is warp-uniform (every lane of a warp shares `base`).
+template <uint32_t L, bool ADD>
+__global__ void k_alt_warp(AltTable t0, const uint32_t* __restrict__ keys, uint32_t n, uint32_t* __restrict__ handles)
+{
+    const AltTable t = with_layout<L>(t0);
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
+        const uint64_t i = base + lane;
+        const bool valid = i < n;
+        const uint32_t* key = keys + (valid ? i : 0) * t.k;
+        const uint32_t h = ADD ? warp_add<L>(t, key, valid) : warp_find<L>(t, key, valid);
+        if (valid)
+            handles[i] = h;
+    }
+}
+
+__global__ void k_alt_read(AltTable t, const uint32_t* __restrict__ handles, uint32_t n, uint32_t* __restrict__ out)
+{
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        read(t, handles[i], out + (uint64_t)i * t.k);
+}
+
+__global__ void k_alt_count(AltTable t, uint32_t slabs, unsigned long long* count)
+{
+    unsigned long long n = 0;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < slabs; i += stride)
+        n += slab_items(t.layout, slab_at(t, i));
+    for (int o = 16; o; o >>= 1)
+        n += __shfl_xor_sync(kFull, n, o);
+    if ((threadIdx.x & 31u) == 0 && n)
+        atomicAdd(count, n);
+}
+
+int grid_of(const svdag_alt_table* at, unsigned long long threads)
+{
+    static int smCount = 0;
+    if (!smCount) {
+        cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount, at->ctx->device);
+        if (smCount <= 0)
+            smCount = 148;
+    }
+    const unsigned long long need = (threads + kThreads - 1) / kThreads;
+    return (int)std::max<unsigned long long>(1, std::min<unsigned long long>(need, (unsigned long long)smCount * 8));
+}
+
+template <bool ADD>
+svdag_status launch_op(svdag_alt_table* at, const uint32_t* keys, uint32_t n, uint32_t* handles, uint32_t lanes, void* stream)
+{
+    if (!at || (n && (!keys || !handles)) || (lanes != 0 && lanes != 1 && lanes != 32))
+        return SVDAG_ERR_INVALID;
+    if (!n)
+        return SVDAG_OK;
+    cudaSetDevice(at->ctx->device);
+    const cudaStream_t s = (cudaStream_t)stream;
+    const AltTable& t = at->t;
+    const int grid = grid_of(at, n);
+    if (lanes != 1) {
+        switch (t.layout) {
+        case kTicketBoard: k_alt_warp<kTicketBoard, ADD><<<grid, kThreads, 0, s>>>(t, keys, n, handles); break;
+        case kAtomic64: k_alt_warp<kAtomic64, ADD><<<grid, kThreads, 0, s>>>(t, keys, n, handles); break;
+        default: k_alt_warp<kAcceleration, ADD><<<grid, kThreads, 0, s>>>(t, keys, n, handles); break;
+        }
+    } else if (ADD) {
+        switch (t.layout) {
+        case kTicketBoard: k_alt_add<kTicketBoard><<<grid, kThreads, 0, s>>>(t, keys, n, handles); break;
+        case kAtomic64: k_alt_add<kAtomic64><<<grid, kThreads, 0, s>>>(t, keys, n, handles); break;
+        default: k_alt_add<kAcceleration><<<grid, kThreads, 0, s>>>(t, keys, n, handles); break;
+        }
+    } else {
+        switch (t.layout) {
+        case kTicketBoard: k_alt_find<kTicketBoard><<<grid, kThreads, 0, s>>>(t, keys, n, handles); break;
+        case kAtomic64: k_alt_find<kAtomic64><<<grid, kThreads, 0, s>>>(t, keys, n, handles); break;
+        default: k_alt_find<kAcceleration><<<grid, kThreads, 0, s>>>(t, keys, n, handles); break;
+        }
+    }
+    SVDAG_CUDA(cudaGetLastError());
+    return SVDAG_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+svdag_status svdag_alt_table_create(svdag_ctx* ctx, uint32_t layout, uint32_t itemWords, uint32_t numBuckets,
+    uint64_t reservedItems, svdag_alt_table** out)
+{
+    if (!ctx || !out || !layout_ok(layout, itemWords) || numBuckets == 0)
+        return SVDAG_ERR_INVALID;
+    *out = nullptr;
+    const uint32_t slabs = arena_slabs(layout, numBuckets, reservedItems);
+    if (!slabs)
+        return SVDAG_ERR_INVALID;
+    const uint32_t sw = slab_words(layout, itemWords);
+    const unsigned long long bytes = 256ull + (unsigned long long)slabs * sw * 4ull;
+    cudaSetDevice(ctx->device);
+    auto* at = new (std::nothrow) svdag_alt_table();
+    if (!at)
+        return SVDAG_ERR_OOM;
+    at->ctx = ctx;
+    if (cudaMalloc(&at->mem, bytes) != cudaSuccess || cudaMalloc(&at->countDev, sizeof(unsigned long long)) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(at->mem);
+        delete at;
+        return SVDAG_ERR_OOM;
+    }
+    AltTable& t = at->t;
+    t.layout = layout;
+    t.k = itemWords;
+    t.numBuckets = numBuckets;
+    t.slabWords = sw;
+    t.slabCount = slabs;
+    t.ctl = (uint32_t*)at->mem;
+    t.slabs = (uint32_t*)((char*)at->mem + 256);
+    const uint32_t ctlInit[kCtlWords] = { numBuckets };
+    svdag_status st = SVDAG_OK;
+    if (cudaMemset(at->mem, 0, bytes) != cudaSuccess
+        || cudaMemcpy(t.ctl, ctlInit, sizeof(ctlInit), cudaMemcpyHostToDevice) != cudaSuccess)
+        st = SVDAG_ERR_CUDA;
+    if (st) {
+        cudaGetLastError();
+        cudaFree(at->countDev);
+        cudaFree(at->mem);
+        delete at;
+        return st;
+    }
+    *out = at;
+    return SVDAG_OK;
+}
+
+svdag_status svdag_alt_table_destroy(svdag_alt_table* at)
+{
+    if (!at)
+        return SVDAG_ERR_INVALID;
+    cudaSetDevice(at->ctx->device);
+    cudaFree(at->countDev);
+    cudaFree(at->mem);
+    delete at;
+    return SVDAG_OK;
+}
+
+svdag_status svdag_alt_table_add(svdag_alt_table* at, const uint32_t* keys, uint32_t n, uint32_t* handles, uint32_t lanes, void* stream)
+{
+    return launch_op<true>(at, keys, n, handles, lanes, stream);
+}
+
+svdag_status svdag_alt_table_find(svdag_alt_table* at, const uint32_t* keys, uint32_t n, uint32_t* handles, uint32_t lanes, void* stream)
+{
+    return launch_op<false>(at, keys, n, handles, lanes, stream);
+}
+
+svdag_status svdag_alt_table_read(svdag_alt_table* at, const uint32_t* handles, uint32_t n, uint32_t* outWords, void* stream)
+{
+    if (!at || (n && (!handles || !outWords)))
+        return SVDAG_ERR_INVALID;
+    if (!n)
+        return SVDAG_OK;
+    cudaSetDevice(at->ctx->device);
+    k_alt_read<<<grid_of(at, n), kThreads, 0, (cudaStream_t)stream>>>(at->t, handles, n, outWords);
+    SVDAG_CUDA(cudaGetLastError());
+    return SVDAG_OK;
+}
+
+svdag_status svdag_alt_table_sync(svdag_alt_table* at, void* stream)
+{
+    if (!at)
+        return SVDAG_ERR_INVALID;
+    cudaSetDevice(at->ctx->device);
+    const cudaStream_t s = (cudaStream_t)stream;
+    uint32_t st = 0;
+    SVDAG_CUDA(cudaMemcpyAsync(&st, &at->t.ctl[kCtlStatus], sizeof(st), cudaMemcpyDeviceToHost, s));
+    SVDAG_CUDA(cudaStreamSynchronize(s));
+    if (st) {
+        SVDAG_CUDA(cudaMemsetAsync(&at->t.ctl[kCtlStatus], 0, sizeof(uint32_t), s));
+        SVDAG_CUDA(cudaStreamSynchronize(s));
+    }
+    return (svdag_status)st;
+}
+
+svdag_status svdag_alt_table_get_stats(svdag_alt_table* at, svdag_table_stats* out, void* stream)
+{
+    if (!at || !out)
+        return SVDAG_ERR_INVALID;
+    cudaSetDevice(at->ctx->device);
+    const cudaStream_t s = (cudaStream_t)stream;
+    uint32_t next = 0;
+    SVDAG_CUDA(cudaMemcpyAsync(&next, &at->t.ctl[kCtlNextSlab], sizeof(next), cudaMemcpyDeviceToHost, s));
+    SVDAG_CUDA(cudaStreamSynchronize(s));
+    const uint32_t used = std::min(next, at->t.slabCount);
+    SVDAG_CUDA(cudaMemsetAsync(at->countDev, 0, sizeof(unsigned long long), s));
+    k_alt_count<<<grid_of(at, used), kThreads, 0, s>>>(at->t, used, at->countDev);
+    SVDAG_CUDA(cudaGetLastError());
+    unsigned long long items = 0;
+    SVDAG_CUDA(cudaMemcpyAsync(&items, at->countDev, sizeof(items), cudaMemcpyDeviceToHost, s));
+    SVDAG_CUDA(cudaStreamSynchronize(s));
+    out->items = items;
+    out->buckets = at->t.numBuckets;
+    out->overflow_slabs = used - at->t.numBuckets;
+    out->bytes = (unsigned long long)used * at->t.slabWords * 4ull;
+    return svdag_alt_table_sync(at, stream);
+}
+
+} // extern "C"

@@ -1,0 +1,345 @@
+// svdag_alt_tables.cuh - the reference's alternative slab layouts for fixed-size items, as tables of
+// their own: TicketBoard (ticket_board_hash_table.h), Atomic64 (atomic64_hash_table.h) and
+// Acceleration (acceleration_hash_table.h). The compact 8-bit-tag layout is the level tables'
+// (svdag_device.cuh). These serve the fixed-size hashmap workload of the reference's table
+// benchmark (extras/hashmap_bench/src/main.cu) so the layouts can be measured against each other.
+//
+// One table is one device allocation: a control block and an arena of equal-sized slabs. Slabs
+// 0..numBuckets-1 are the buckets' first slabs; overflow slabs are taken from a bump counter and
+// linked at the tail of a chain. The arena is zeroed when the table is created and slabs are never
+// reused, so a fresh slab needs no initialisation and a next word of 0 ends a chain (no overflow
+// slab has id 0; kLinkBusy marks a link being made). A handle is slab * 32 + slot.
+//
+// Slab layouts (32-bit words; a slab's stride is rounded up to 8 words, 32 bytes):
+//   TicketBoard : [0] occupied-slot mask, [1] next, [2..7] unused, items of slots 0..31 from word 8.
+//                 A slot is claimed by an atomic OR of its bit, then the item is written.
+//   Atomic64    : words 2s, 2s+1 = the first 8 bytes of slot s's item (s = 0..30, 0 = free),
+//                 [62] next, [63] unused, the other k-2 words of slot s's item from word 64.
+//                 A slot is claimed by a 64-bit CAS of its first 8 bytes; items whose first two
+//                 words are both 0 cannot be stored (the reference requires the same).
+//   Acceleration: [0] next, [s] = 32-bit tag of slot s (s = 1..31, 0 = free), items of slots
+//                 1..31 from word 32. A slot is claimed by a CAS of its tag.
+//
+// The thread-per-key functions below compile for the device and, unchanged, for the host (the
+// atomics are GCC builtins there), so their claim and chain logic can be exercised by host threads.
+// Adds and finds must not overlap in time (the reference's bulk phases do the same): a finder may
+// see a claimed slot before its item is written.
+#pragma once
+#include <cstdint>
+
+#include "../../include/svdag.h"
+#include "svdag_hash.h"
+
+namespace svdag {
+namespace alt {
+
+enum Layout : uint32_t { kTicketBoard = 1, kAtomic64 = 2, kAcceleration = 3 };
+
+constexpr uint32_t kInvalid = 0xFFFFFFFFu;
+constexpr uint32_t kNoSlab = 0xFFFFFFFFu;
+constexpr uint32_t kMaxItemWords = 32;
+constexpr uint32_t kMaxSlabs = 1u << 27; // handles slab * 32 + slot stay below 2^32 - 1
+constexpr uint32_t kMaxSteps = 1u << 22; // slabs one add or find may visit before it gives up
+constexpr uint32_t kLinkBusy = 0xFFFFFFFFu; // next word of a slab whose successor is being linked
+constexpr uint32_t kMaxSpin = 1u << 20; // reads of a busy next word before a wait gives up
+
+// Control block words.
+enum Ctl : uint32_t { kCtlNextSlab = 0, kCtlStatus = 1, kCtlWords = 8 };
+
+struct AltTable {
+    uint32_t layout;
+    uint32_t k; // item words
+    uint32_t numBuckets;
+    uint32_t slabWords; // stride of a slab in words, a multiple of 8
+    uint32_t slabCount; // slabs in the arena
+    uint32_t pad;
+    uint32_t* slabs;
+    uint32_t* ctl;
+};
+
+SVDAG_HD uint32_t round8(uint32_t w) { return (w + 7u) & ~7u; }
+SVDAG_HD uint32_t slab_words(uint32_t layout, uint32_t k)
+{
+    return layout == kTicketBoard ? round8(8u + 32u * k) : layout == kAtomic64 ? round8(64u + 31u * (k - 2u)) : round8(32u + 31u * k);
+}
+SVDAG_HD uint32_t slots_per_slab(uint32_t layout) { return layout == kTicketBoard ? 32u : 31u; }
+SVDAG_HD uint32_t next_word(uint32_t layout) { return layout == kTicketBoard ? 1u : layout == kAtomic64 ? 62u : 0u; }
+SVDAG_HD bool layout_ok(uint32_t layout, uint32_t k)
+{
+    return (layout == kTicketBoard || layout == kAcceleration) ? (k >= 1 && k <= kMaxItemWords)
+         : layout == kAtomic64 ? (k >= 2 && k <= kMaxItemWords) : false;
+}
+// Slabs of a table's arena: the bucket slabs and overflow slabs for `reserved` more items, or 0 when
+// that exceeds kMaxSlabs.
+inline uint32_t arena_slabs(uint32_t layout, uint32_t numBuckets, uint64_t reserved)
+{
+    const uint64_t overflow = (reserved + slots_per_slab(layout) - 1) / slots_per_slab(layout);
+    const uint64_t slabs = (uint64_t)numBuckets + overflow;
+    return slabs > kMaxSlabs ? 0u : (uint32_t)slabs;
+}
+// Slot numbers a layout uses: 0..31, 0..30 or 1..31.
+SVDAG_HD bool slot_ok(uint32_t layout, uint32_t slot)
+{
+    return layout == kTicketBoard ? slot < 32u : layout == kAtomic64 ? slot < 31u : (slot >= 1u && slot < 32u);
+}
+// Word offset (in its slab) of the stored part of slot s's item: all k words, or the last k-2 for Atomic64.
+SVDAG_HD uint32_t body_word(uint32_t layout, uint32_t k, uint32_t s)
+{
+    return layout == kTicketBoard ? 8u + s * k : layout == kAtomic64 ? 64u + s * (k - 2u) : 32u + (s - 1u) * k;
+}
+
+// ---------------------------------------------------------------- atomics (device / host builtins)
+
+#ifdef __CUDA_ARCH__
+__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p) { return *(const volatile uint32_t*)p; }
+__device__ __forceinline__ uint64_t ld_relaxed64(const uint64_t* p) { return *(const volatile uint64_t*)p; }
+__device__ __forceinline__ uint32_t cas32(uint32_t* p, uint32_t cmp, uint32_t v) { return atomicCAS(p, cmp, v); }
+__device__ __forceinline__ uint64_t cas64(uint64_t* p, uint64_t cmp, uint64_t v)
+{
+    return atomicCAS((unsigned long long*)p, (unsigned long long)cmp, (unsigned long long)v);
+}
+__device__ __forceinline__ uint32_t or32(uint32_t* p, uint32_t v) { return atomicOr(p, v); }
+__device__ __forceinline__ uint32_t add32(uint32_t* p, uint32_t v) { return atomicAdd(p, v); }
+__device__ __forceinline__ uint32_t exch32(uint32_t* p, uint32_t v) { return atomicExch(p, v); }
+__device__ __forceinline__ uint32_t ctz32(uint32_t v) { return __ffs(v) - 1u; }
+#else
+inline uint32_t ld_relaxed(const uint32_t* p) { return __atomic_load_n(p, __ATOMIC_RELAXED); }
+inline uint64_t ld_relaxed64(const uint64_t* p) { return __atomic_load_n(p, __ATOMIC_RELAXED); }
+inline uint32_t cas32(uint32_t* p, uint32_t cmp, uint32_t v)
+{
+    __atomic_compare_exchange_n(p, &cmp, v, false, __ATOMIC_ACQ_REL, __ATOMIC_ACQUIRE);
+    return cmp;
+}
+inline uint64_t cas64(uint64_t* p, uint64_t cmp, uint64_t v)
+{
+    __atomic_compare_exchange_n(p, &cmp, v, false, __ATOMIC_ACQ_REL, __ATOMIC_ACQUIRE);
+    return cmp;
+}
+inline uint32_t or32(uint32_t* p, uint32_t v) { return __atomic_fetch_or(p, v, __ATOMIC_ACQ_REL); }
+inline uint32_t add32(uint32_t* p, uint32_t v) { return __atomic_fetch_add(p, v, __ATOMIC_ACQ_REL); }
+inline uint32_t exch32(uint32_t* p, uint32_t v) { return __atomic_exchange_n(p, v, __ATOMIC_ACQ_REL); }
+inline uint32_t ctz32(uint32_t v) { return (uint32_t)__builtin_ctz(v); }
+#endif
+
+SVDAG_HD void set_status(const AltTable& t, uint32_t st) { cas32(&t.ctl[kCtlStatus], 0u, st); }
+SVDAG_HD uint32_t* slab_at(const AltTable& t, uint32_t slab) { return t.slabs + (uint64_t)slab * t.slabWords; }
+
+// Key hash over the k words (the level tables' hash, svdag_hash.h).
+SVDAG_HD uint32_t key_acc(const uint32_t* key, uint32_t k)
+{
+    uint32_t acc = 0;
+    for (uint32_t i = 0; i < k; ++i)
+        acc ^= word_term(key[i], i);
+    return acc;
+}
+SVDAG_HD uint32_t acc_tag32(uint32_t acc)
+{
+    const uint32_t t = tag_hash(acc);
+    return t ? t : 1u;
+}
+SVDAG_HD uint64_t key_prefix(const uint32_t* key) { return (uint64_t)key[0] | ((uint64_t)key[1] << 32); }
+SVDAG_HD bool words_equal(const uint32_t* a, const uint32_t* b, uint32_t n)
+{
+    bool eq = true;
+    for (uint32_t i = 0; i < n; ++i)
+        eq &= a[i] == b[i];
+    return eq;
+}
+
+// Claims a free slot of slab s for the key (tag / prefix already computed); the slot or kInvalid if
+// the slab is full. Each failed claim is a slot another thread took, so the loops are bounded by 32.
+SVDAG_HD uint32_t try_claim(const AltTable& t, uint32_t* s, uint32_t tag, uint64_t prefix)
+{
+    if (t.layout == kTicketBoard) {
+        uint32_t m = ld_relaxed(&s[0]);
+        while (m != 0xFFFFFFFFu) {
+            const uint32_t slot = ctz32(~m);
+            const uint32_t old = or32(&s[0], 1u << slot);
+            if (!(old & (1u << slot)))
+                return slot;
+            m = old | (1u << slot);
+        }
+        return kInvalid;
+    }
+    if (t.layout == kAtomic64) {
+        uint64_t* pre = (uint64_t*)s;
+        for (uint32_t slot = 0; slot < 31u; ++slot)
+            if (ld_relaxed64(&pre[slot]) == 0 && cas64(&pre[slot], 0, prefix) == 0)
+                return slot;
+        return kInvalid;
+    }
+    for (uint32_t slot = 1; slot < 32u; ++slot)
+        if (ld_relaxed(&s[slot]) == 0 && cas32(&s[slot], 0u, tag) == 0)
+            return slot;
+    return kInvalid;
+}
+
+// Slot of slab s holding the key, or kInvalid.
+SVDAG_HD uint32_t match_slab(const AltTable& t, const uint32_t* s, const uint32_t* key, uint32_t tag, uint64_t prefix)
+{
+    const uint32_t k = t.k;
+    if (t.layout == kTicketBoard) {
+        uint32_t m = s[0];
+        while (m) {
+            const uint32_t slot = ctz32(m);
+            m &= m - 1u;
+            if (words_equal(s + body_word(kTicketBoard, k, slot), key, k))
+                return slot;
+        }
+        return kInvalid;
+    }
+    if (t.layout == kAtomic64) {
+        const uint64_t* pre = (const uint64_t*)s;
+        for (uint32_t slot = 0; slot < 31u; ++slot)
+            if (pre[slot] == prefix && words_equal(s + body_word(kAtomic64, k, slot), key + 2, k - 2u))
+                return slot;
+        return kInvalid;
+    }
+    for (uint32_t slot = 1; slot < 32u; ++slot)
+        if (s[slot] == tag && words_equal(s + body_word(kAcceleration, k, slot), key, k))
+            return slot;
+    return kInvalid;
+}
+
+// Next slab of a chain after slab s, linking a new one when the chain ends there. The thread that
+// turns the next word from 0 to kLinkBusy takes a slab from the bump counter and stores its id;
+// threads that meet kLinkBusy wait for the id (the holder waits for nothing in between, so the wait
+// is short; it is bounded all the same). One slab is taken per link and none is lost, where taking
+// a slab before the race for the link would strand the losers' slabs (the reference frees them,
+// gpu_hash_table_base.h:128-219). kNoSlab with the status latched on exhaustion, a bad link or a
+// wait that gave up.
+SVDAG_HD uint32_t next_or_link(const AltTable& t, uint32_t* s)
+{
+    uint32_t* link = &s[next_word(t.layout)];
+    uint32_t nx = ld_relaxed(link);
+    for (uint32_t spin = 0; nx == 0 || nx == kLinkBusy; ++spin) {
+        if (spin >= kMaxSpin) {
+            set_status(t, SVDAG_ERR_TIMEOUT);
+            return kNoSlab;
+        }
+        if (nx == 0) {
+            nx = cas32(link, 0u, kLinkBusy);
+            if (nx == 0) {
+                const uint32_t fresh = add32(&t.ctl[kCtlNextSlab], 1u);
+                if (fresh >= t.slabCount) {
+                    exch32(link, 0u); // the chain ends here again; later arrivals fail the same way
+                    set_status(t, SVDAG_ERR_OOM);
+                    return kNoSlab;
+                }
+                exch32(link, fresh);
+                return fresh;
+            }
+        } else {
+            nx = ld_relaxed(link);
+        }
+    }
+    if (nx < t.numBuckets || nx >= t.slabCount) {
+        set_status(t, SVDAG_ERR_CORRUPT);
+        return kNoSlab;
+    }
+    return nx;
+}
+
+// add (ticket_board_hash_table.h:24-60, atomic64_hash_table.h:36-64, acceleration_hash_table.h:31-72):
+// stores the key in a fresh slot, duplicates included, and returns its handle.
+SVDAG_HD uint32_t add(const AltTable& t, const uint32_t* key)
+{
+    const uint32_t k = t.k;
+    const uint32_t acc = key_acc(key, k);
+    const uint32_t tag = acc_tag32(acc);
+    const uint64_t prefix = t.layout == kAtomic64 ? key_prefix(key) : 0;
+    if (t.layout == kAtomic64 && prefix == 0) {
+        set_status(t, SVDAG_ERR_INVALID);
+        return kInvalid;
+    }
+    uint32_t slab = bucket_index(bucket_hash(acc), t.numBuckets);
+    for (uint32_t step = 0; step < kMaxSteps; ++step) {
+        uint32_t* s = slab_at(t, slab);
+        const uint32_t slot = try_claim(t, s, tag, prefix);
+        if (slot != kInvalid) {
+            const uint32_t first = t.layout == kAtomic64 ? 2u : 0u;
+            uint32_t* dst = s + body_word(t.layout, k, slot);
+            for (uint32_t i = first; i < k; ++i)
+                dst[i - first] = key[i];
+            return slab * 32u + slot;
+        }
+        slab = next_or_link(t, s);
+        if (slab == kNoSlab)
+            return kInvalid;
+    }
+    set_status(t, SVDAG_ERR_TIMEOUT);
+    return kInvalid;
+}
+
+// find (ticket_board_hash_table.h:176-197, atomic64_hash_table.h:194-214, acceleration_hash_table.h):
+// handle of a stored copy of the key, or kInvalid.
+SVDAG_HD uint32_t find(const AltTable& t, const uint32_t* key)
+{
+    const uint32_t k = t.k;
+    const uint32_t acc = key_acc(key, k);
+    const uint32_t tag = acc_tag32(acc);
+    const uint64_t prefix = t.layout == kAtomic64 ? key_prefix(key) : 0;
+    if (t.layout == kAtomic64 && prefix == 0)
+        return kInvalid;
+    uint32_t slab = bucket_index(bucket_hash(acc), t.numBuckets);
+    for (uint32_t step = 0; step < kMaxSteps; ++step) {
+        const uint32_t* s = slab_at(t, slab);
+        const uint32_t slot = match_slab(t, s, key, tag, prefix);
+        if (slot != kInvalid)
+            return slab * 32u + slot;
+        const uint32_t nx = s[next_word(t.layout)];
+        if (nx == 0)
+            return kInvalid;
+        if (nx < t.numBuckets || nx >= t.slabCount) {
+            set_status(t, SVDAG_ERR_CORRUPT);
+            return kInvalid;
+        }
+        slab = nx;
+    }
+    set_status(t, SVDAG_ERR_TIMEOUT);
+    return kInvalid;
+}
+
+// Whether slot `slot` of slab s is occupied.
+SVDAG_HD bool slot_used(uint32_t layout, const uint32_t* s, uint32_t slot)
+{
+    return layout == kTicketBoard ? ((s[0] >> slot) & 1u) != 0
+         : layout == kAtomic64 ? ((const uint64_t*)s)[slot] != 0 : s[slot] != 0;
+}
+
+// decodePointer: the k words of a handle's item into out[0..k); false for a handle that names no
+// stored item (out is then zeroed).
+SVDAG_HD bool read(const AltTable& t, uint32_t h, uint32_t* out)
+{
+    const uint32_t slab = h >> 5, slot = h & 31u, k = t.k;
+    const bool ok = h != kInvalid && slab < t.slabCount && slot_ok(t.layout, slot) && slot_used(t.layout, slab_at(t, slab), slot);
+    if (!ok) {
+        for (uint32_t i = 0; i < k; ++i)
+            out[i] = 0;
+        return false;
+    }
+    const uint32_t* s = slab_at(t, slab);
+    const uint32_t* body = s + body_word(t.layout, k, slot);
+    if (t.layout == kAtomic64) {
+        out[0] = s[2 * slot];
+        out[1] = s[2 * slot + 1];
+        for (uint32_t i = 2; i < k; ++i)
+            out[i] = body[i - 2];
+    } else {
+        for (uint32_t i = 0; i < k; ++i)
+            out[i] = body[i];
+    }
+    return true;
+}
+
+// Occupied slots of slab s.
+SVDAG_HD uint32_t slab_items(uint32_t layout, const uint32_t* s)
+{
+    uint32_t n = 0;
+    for (uint32_t slot = 0; slot < 32u; ++slot)
+        n += slot_ok(layout, slot) && slot_used(layout, s, slot);
+    return n;
+}
+
+} // namespace alt
+} // namespace svdag

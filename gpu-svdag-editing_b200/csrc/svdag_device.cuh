@@ -26,6 +26,7 @@
 #include <cstdint>
 
 #include "../../include/svdag.h"
+#include "svdag_hash.h"
 
 namespace svdag {
 
@@ -131,32 +132,8 @@ __device__ __forceinline__ bool slab_ok(const DevDag& d, uint32_t slab) { return
 __device__ __forceinline__ uint32_t* slab_ptr(const DevDag& d, uint32_t slab) { return d.headers + 8ull * slab; }
 __device__ __forceinline__ uint32_t* handle_ptr(const DevDag& d, uint32_t h) { return d.items + 2ull * h; }
 
-// ---------------------------------------------------------------- hashing (ours; the bucket
-// function of the reference is xorHash32xN, utils.h:395-403, which uses a 32-bit modulo per word)
+// ---------------------------------------------------------------- hashing: svdag_hash.h
 
-__host__ __device__ __forceinline__ uint32_t fmix32(uint32_t h)
-{
-    h ^= h >> 16;
-    h *= 0x85ebca6bu;
-    h ^= h >> 13;
-    h *= 0xc2b2ae35u;
-    h ^= h >> 16;
-    return h;
-}
-// Per-word term of the key hash: an odd multiply of the word offset by a position constant (a
-// bijection of the word; the terms of a key are combined by XOR, so lanes that hold different words
-// of one key can combine theirs). The finalisers below turn the sum into the bucket and tag hashes.
-__host__ __device__ __forceinline__ uint32_t word_term(uint32_t w, uint32_t i)
-{
-    return (w ^ (i * 0x9E3779B9u + 0x7F4A7C15u)) * (0x85EBCA6Bu + 2u * i);
-}
-__host__ __device__ __forceinline__ uint32_t bucket_hash(uint32_t acc) { return fmix32(acc); }
-__host__ __device__ __forceinline__ uint32_t tag_hash(uint32_t acc) { return fmix32(acc ^ 0x5BD1E995u); }
-__host__ __device__ __forceinline__ uint32_t tag_of(uint32_t hb)
-{
-    uint32_t t = hb >> 24;
-    return t == 0 ? 1u : (t == 0xFFu ? 0xFEu : t);
-}
 __device__ __forceinline__ uint32_t bucket_of(uint32_t ha, uint32_t numBuckets) { return __umulhi(ha, numBuckets); }
 
 // Key length from the first words (my_gpu_base_dag.h:195-203).

@@ -203,6 +203,13 @@ _PROTOS = {
     "svdag_table_find_or_add_static": [_P, _P, _P, _U32, _U64, _P, _U32, _P],
     "svdag_table_read": [_P, _P, _U32, _P, _P],
     "svdag_table_get_stats": [_P, C.POINTER(TableStats), _P],
+    "svdag_alt_table_create": [_P, _U32, _U32, _U32, _U64, C.POINTER(_P)],
+    "svdag_alt_table_destroy": [_P],
+    "svdag_alt_table_add": [_P, _P, _U32, _P, _U32, _P],
+    "svdag_alt_table_find": [_P, _P, _U32, _P, _U32, _P],
+    "svdag_alt_table_read": [_P, _P, _U32, _P, _P],
+    "svdag_alt_table_sync": [_P, _P],
+    "svdag_alt_table_get_stats": [_P, C.POINTER(TableStats), _P],
     "svdag_get_stats": [_P, C.POINTER(Stats), _P],
     "svdag_export_level": [_P, _U32, _P, _P, _U64, C.POINTER(_U64), _P],
     "svdag_autotune": [_P, C.POINTER(Edit), _U32, _P, _P, _U32, _U64, _U32, C.POINTER(Tuning), _P],
@@ -675,6 +682,65 @@ class HashTable:
         if self.owned and self.h:
             lib().svdag_table_destroy(self.h)
             self.h = None
+
+
+TABLE_LAYOUT_TICKET_BOARD, TABLE_LAYOUT_ATOMIC64, TABLE_LAYOUT_ACCELERATION = 1, 2, 3
+
+
+class AltHashTable:
+    """A table of fixed-size items in one of the reference's alternative slab layouts
+    (TicketBoardHashTable, Atomic64HashTable, AccelerationHashTable), on the GPU of `dag`, in an
+    allocation of its own. Keys are `item_words` words back to back; add stores every key in a
+    fresh slot, duplicates included; adds and finds must not overlap in time."""
+
+    def __init__(self, dag: MyGPUHashDAG, layout: int, item_words: int, num_buckets: int, reserved_items: int):
+        self.dag, self.layout, self.item_words = dag, layout, item_words
+        t = C.c_void_p()
+        _check(lib().svdag_alt_table_create(dag.h, layout, item_words, num_buckets, reserved_items, C.byref(t)),
+               "svdag_alt_table_create")
+        self.h = t
+
+    @classmethod
+    def allocate(cls, dag: MyGPUHashDAG, layout: int, numBuckets: int, numReservedElements: int, itemSizeInU32: int):
+        """Table::allocate(numBuckets, numReservedElements, itemSizeInU32)."""
+        return cls(dag, layout, itemSizeInU32, numBuckets, numReservedElements)
+
+    def add(self, keys, count, out, lanes=0, stream=None):
+        _check(lib().svdag_alt_table_add(self.h, ptr(keys), count, ptr(out), lanes, stream_ptr(stream)), "svdag_alt_table_add")
+
+    def find(self, keys, count, out, lanes=0, stream=None):
+        _check(lib().svdag_alt_table_find(self.h, ptr(keys), count, ptr(out), lanes, stream_ptr(stream)),
+               "svdag_alt_table_find")
+
+    def read(self, handles, count, out_words, stream=None):
+        _check(lib().svdag_alt_table_read(self.h, ptr(handles), count, ptr(out_words), stream_ptr(stream)),
+               "svdag_alt_table_read")
+
+    def sync(self, stream=None):
+        """Waits for the stream; raises the first device-side error latched since the last sync."""
+        _check(lib().svdag_alt_table_sync(self.h, stream_ptr(stream)), "svdag_alt_table_sync")
+
+    def stats(self, stream=None) -> TableStats:
+        s = TableStats()
+        _check(lib().svdag_alt_table_get_stats(self.h, C.byref(s), stream_ptr(stream)), "svdag_alt_table_get_stats")
+        return s
+
+    def destroy(self):
+        if self.h:
+            lib().svdag_alt_table_destroy(self.h)
+            self.h = None
+
+
+def TicketBoardHashTable(dag, numBuckets, numReservedElements, itemSizeInU32):
+    return AltHashTable.allocate(dag, TABLE_LAYOUT_TICKET_BOARD, numBuckets, numReservedElements, itemSizeInU32)
+
+
+def Atomic64HashTable(dag, numBuckets, numReservedElements, itemSizeInU32):
+    return AltHashTable.allocate(dag, TABLE_LAYOUT_ATOMIC64, numBuckets, numReservedElements, itemSizeInU32)
+
+
+def AccelerationHashTable(dag, numBuckets, numReservedElements, itemSizeInU32):
+    return AltHashTable.allocate(dag, TABLE_LAYOUT_ACCELERATION, numBuckets, numReservedElements, itemSizeInU32)
 
 
 class MyGPUHashDAGUndoRedo:

@@ -335,6 +335,47 @@ typedef struct svdag_table_stats {
 } svdag_table_stats;
 svdag_status svdag_table_get_stats(svdag_table* table, svdag_table_stats* out, void* stream);
 
+/* ---------------------------------------------------------------- alternative table layouts */
+
+/* The reference's other slab layouts, for items of a fixed size (the workload of its table benchmark,
+ * extras/hashmap_bench/src/main.cu): the DAG's level tables keep the compact 8-bit-tag layout above.
+ * TICKET_BOARD: 32 slots per slab, a slot-occupancy mask claimed by atomic OR
+ * (TicketBoardHashTable, ticket_board_hash_table.h:10-347). ATOMIC64: 31 slots, each claimed by a
+ * 64-bit CAS of its item's first 8 bytes, which makes items with two zero first words unstorable
+ * (Atomic64HashTable, atomic64_hash_table.h:11-414). ACCELERATION: 31 slots with a 32-bit tag each,
+ * claimed by CAS (AccelerationHashTable, acceleration_hash_table.h:17-491). */
+#define SVDAG_TABLE_LAYOUT_TICKET_BOARD 1u
+#define SVDAG_TABLE_LAYOUT_ATOMIC64 2u
+#define SVDAG_TABLE_LAYOUT_ACCELERATION 3u
+typedef struct svdag_alt_table svdag_alt_table;
+/* Table::allocate(numBuckets, numReservedElements, itemSizeInU32) (gpu_hash_table_base.h,
+ * ticket_board_hash_table.h:19): one device allocation on the context's GPU holding num_buckets
+ * first slabs and overflow slabs for reserved_items more items. item_words 1..32 (2..32 for
+ * ATOMIC64). More than 2^27 slabs in all gives SVDAG_ERR_INVALID. */
+svdag_status svdag_alt_table_create(svdag_ctx* ctx, uint32_t layout, uint32_t item_words, uint32_t num_buckets,
+    uint64_t reserved_items, svdag_alt_table** out_table);
+svdag_status svdag_alt_table_destroy(svdag_alt_table* table);
+/* add / addAsWarpHybrid: keys_dev holds count items of item_words words back to back; each is stored
+ * in a fresh slot, duplicates included. lanes 1 = a thread per key; 32 or 0 = warp-hybrid (every lane
+ * holds a key and the warp inspects one slab for one lane's key at a time). Asynchronous: exhausted
+ * overflow slabs (SVDAG_ERR_OOM), an unstorable ATOMIC64 item (SVDAG_ERR_INVALID) or a bad link
+ * (SVDAG_ERR_CORRUPT) give that key SVDAG_INVALID_HANDLE and are latched for svdag_alt_table_sync.
+ * Adds and finds on one table must not overlap in time. */
+svdag_status svdag_alt_table_add(svdag_alt_table* table, const uint32_t* keys_dev, uint32_t count, uint32_t* handles_dev,
+    uint32_t lanes, void* stream);
+/* find / findAsWarpHybrid: handle of a stored copy of each key, or SVDAG_INVALID_HANDLE. */
+svdag_status svdag_alt_table_find(svdag_alt_table* table, const uint32_t* keys_dev, uint32_t count, uint32_t* handles_dev,
+    uint32_t lanes, void* stream);
+/* decodePointer: the item_words words of each handle to out_words_dev[i * item_words ...]; a handle
+ * that names no stored item reads as zeros. */
+svdag_status svdag_alt_table_read(svdag_alt_table* table, const uint32_t* handles_dev, uint32_t count,
+    uint32_t* out_words_dev, void* stream);
+/* Waits for the stream and returns (and clears) the first latched device-side error. */
+svdag_status svdag_alt_table_sync(svdag_alt_table* table, void* stream);
+/* Occupied slots, bucket slabs, linked or lost overflow slabs taken, bytes of those slabs; synchronous,
+ * returns like svdag_alt_table_sync. */
+svdag_status svdag_alt_table_get_stats(svdag_alt_table* table, svdag_table_stats* out, void* stream);
+
 /* ---------------------------------------------------------------- inspection */
 
 typedef struct svdag_stats {

@@ -1,0 +1,154 @@
+"""The alternative table layouts on the GPU, thread-per-key and warp-hybrid, through the C ABI.
+
+Same set semantics as tests/test_alt_tables_cpu.py (the reference's hash_table_test.cpp:158-240 and
+the verification of extras/hashmap_bench/src/main.cu:640-700): every add gets its own slot,
+duplicates included; added keys are found and read back as themselves; keys never added are not
+found; exhausting the reserved overflow slabs latches SVDAG_ERR_OOM and stores nothing beyond them.
+The file sorts after the other GPU tests so that they run first.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TB, A64, ACC = 1, 2, 3
+INVALID = 0xFFFFFFFF
+
+
+def dev(a):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.uint32).view(np.int32)).cuda()
+
+
+def host(t):
+    return t.cpu().numpy().view(np.uint32)
+
+
+def unique_keys(rng, n, k, exclude=None):
+    keys = rng.integers(0, 1 << 32, (2 * n + 16, k), dtype=np.uint64).astype(np.uint32)
+    if k >= 2:
+        keys = keys[(keys[:, 0] != 0) | (keys[:, 1] != 0)]
+    keys = np.unique(keys, axis=0)
+    if exclude is not None:
+        ex = {tuple(r) for r in exclude}
+        keys = np.array([r for r in keys if tuple(r) not in ex], dtype=np.uint32).reshape(-1, k)
+    keys = keys[rng.permutation(len(keys))[:n]]
+    assert len(keys) == n
+    return keys
+
+
+@pytest.fixture(scope="module")
+def dag(svdag_lib):
+    d = svdag_lib.MyGPUHashDAG(6, pool_bytes=64 << 20, scratch_bytes=16 << 20)
+    yield d
+    d.free()
+
+
+@pytest.mark.parametrize("lanes", [1, 32])
+@pytest.mark.parametrize("buckets", [7, 1000])
+@pytest.mark.parametrize("layout,k", [(TB, 1), (TB, 2), (TB, 5), (A64, 2), (A64, 3), (A64, 9), (ACC, 1), (ACC, 2),
+                                      (ACC, 7), (TB, 32), (A64, 32), (ACC, 32)])
+def test_add_find_read(svdag_lib, dag, layout, k, buckets, lanes):
+    import torch
+
+    rng = np.random.default_rng(1000 * layout + 10 * k + lanes + buckets)
+    n = 20000
+    keys = unique_keys(rng, n, k)
+    ins = keys[rng.permutation(np.concatenate([np.arange(n), np.arange(n)]))]
+    t = svdag_lib.AltHashTable(dag, layout, k, buckets, 3 * n)
+    try:
+        h = torch.empty(2 * n, dtype=torch.int32, device="cuda")
+        t.add(dev(ins), 2 * n, h, lanes=lanes)
+        t.sync()
+        hh = host(h)
+        assert np.all(hh != INVALID) and len(np.unique(hh)) == 2 * n
+        words = torch.empty((2 * n, k), dtype=torch.int32, device="cuda")
+        t.read(h, 2 * n, words)
+        assert np.array_equal(host(words), ins)
+        st = t.stats()
+        assert st.items == 2 * n and st.buckets == buckets
+        absent = unique_keys(rng, n, k, exclude=keys)
+        q = np.concatenate([keys, absent])
+        f = torch.empty(2 * n, dtype=torch.int32, device="cuda")
+        t.find(dev(q), 2 * n, f, lanes=lanes)
+        t.read(f, 2 * n, words)
+        t.sync()
+        fh, got = host(f), host(words)
+        assert np.all(fh[:n] != INVALID) and np.all(fh[n:] == INVALID)
+        assert np.array_equal(got[:n], keys) and np.all(got[n:] == 0)
+    finally:
+        t.destroy()
+
+
+@pytest.mark.parametrize("lanes", [1, 32])
+@pytest.mark.parametrize("layout", [TB, A64, ACC])
+def test_exhausted_overflow_latches_oom(svdag_lib, dag, layout, lanes):
+    import torch
+
+    rng = np.random.default_rng(50 + layout + lanes)
+    keys = unique_keys(rng, 2000, 3)
+    t = svdag_lib.AltHashTable(dag, layout, 3, 1, 64)
+    try:
+        h = torch.empty(2000, dtype=torch.int32, device="cuda")
+        t.add(dev(keys), 2000, h, lanes=lanes)
+        with pytest.raises(svdag_lib.SvdagError) as e:
+            t.sync()
+        assert e.value.status == 2  # SVDAG_ERR_OOM
+        ok = host(h) != INVALID
+        slots = 32 if layout == TB else 31
+        assert ok.sum() == (1 + -(-64 // slots)) * slots
+        f = torch.empty(2000, dtype=torch.int32, device="cuda")
+        t.find(dev(keys), 2000, f, lanes=lanes)
+        t.sync()
+        assert np.array_equal(host(f) != INVALID, ok)
+    finally:
+        t.destroy()
+
+
+@pytest.mark.parametrize("lanes", [1, 32])
+def test_atomic64_rejects_zero_first_words(svdag_lib, dag, lanes):
+    import torch
+
+    t = svdag_lib.AltHashTable(dag, A64, 3, 4, 0)
+    try:
+        h = torch.empty(3, dtype=torch.int32, device="cuda")
+        t.add(dev(np.array([[0, 0, 5], [0, 1, 5], [1, 0, 5]])), 3, h, lanes=lanes)
+        with pytest.raises(svdag_lib.SvdagError) as e:
+            t.sync()
+        assert e.value.status == 1  # SVDAG_ERR_INVALID
+        hh = host(h)
+        assert hh[0] == INVALID and hh[1] != INVALID and hh[2] != INVALID
+    finally:
+        t.destroy()
+
+
+def test_hashmap_benchmark_shape(svdag_lib, dag):
+    """The reference benchmark's flow at a reduced size: items of 2 words, an initial bulk add,
+    searches at hit rates 0..100 %, a second bulk add, then every key of both adds is found."""
+    import torch
+
+    rng = np.random.default_rng(9)
+    n0, n1, ns = 1 << 16, 1 << 13, 1 << 13
+    allk = unique_keys(rng, n0 + n1 + ns, 2)
+    init, more, never = allk[:n0], allk[n0:n0 + n1], allk[n0 + n1:]
+    for layout in (TB, A64, ACC):
+        t = svdag_lib.AltHashTable(dag, layout, 2, (n0 + n1) // 64 + 1, 2 * (n0 + n1))
+        try:
+            h = torch.empty(n0, dtype=torch.int32, device="cuda")
+            t.add(dev(init), n0, h)
+            f = torch.empty(ns, dtype=torch.int32, device="cuda")
+            for pct in (0, 25, 50, 75, 100):
+                hits = ns * pct // 100
+                q = np.concatenate([init[rng.permutation(n0)[:hits]], never[:ns - hits]])
+                t.find(dev(q), ns, f)
+                t.sync()
+                assert int((host(f) != INVALID).sum()) == hits
+            h1 = torch.empty(n1, dtype=torch.int32, device="cuda")
+            t.add(dev(more), n1, h1)
+            g = torch.empty(n0 + n1, dtype=torch.int32, device="cuda")
+            t.find(dev(np.concatenate([init, more])), n0 + n1, g)
+            t.sync()
+            assert np.all(host(g) != INVALID)
+        finally:
+            t.destroy()
