@@ -12,7 +12,7 @@ frame); `value` is the served p99 edit-to-visible latency, with the plain path's
 A step is one window of `--window` seconds of the stream; W windows are replayed untimed first, then
 K windows in one continuous replay. Other modes (profiling entry points): c0 (depth-10 per-edit
 path), c2 (the at-scale edit sequence), c3 (256 uneven edits, batched vs plain), hash (the 2^24-key
-slab-hash microbenchmark).
+slab-hash microbenchmark), hashmap (the reference's table benchmark over every slab layout).
 
 --impl reference times the reference algorithm on the host cores: the CPU restatement of the
 MyGpuDag pipeline (the reference has no CPU implementation of it) on a bounded sample of the same
@@ -511,6 +511,89 @@ def run_mode_hash(args):
     print(json.dumps(r))
 
 
+def run_mode_hashmap(args):
+    """The reference's table benchmark (extras/hashmap_bench/src/main.cu:560-720, defaults :850-873)
+    over every slab layout: items of 2 words, a bulk add of 8M items, 1M finds at hit rates
+    0/25/50/75/100 %, a second bulk add of 1M items, 64 items per bucket, room reserved for twice the
+    items. Layouts: ticket_board, atomic64, acceleration (svdag_alt_table_*) and compact (the level
+    tables' layout; its keys are 2-word node keys, a one-bit child mask then a word). Each runs thread
+    per key (lanes 1) and warp-hybrid / 32 lanes per key (lanes 32). Every phase is checked: all adds
+    stored, exactly the expected finds hit."""
+    import torch
+
+    import svdag
+
+    k = 2
+    n0, n1, ns = args.hashmap_initial, args.hashmap_insert, args.hashmap_search
+    rng = np.random.default_rng(11)
+    keys = rng.integers(0, 1 << 32, (n0 + n1 + ns, k), dtype=np.uint64).astype(np.uint32)
+    keys[:, 0] = (keys[:, 0] & 0xFFFFFF00) | (np.uint32(1) << (keys[:, 0] & 7))  # valid 2-word node keys
+    init, more, never = keys[:n0], keys[n0:n0 + n1], keys[n0 + n1:]
+    buckets = (n0 + n1) // 64 + 1
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.uint32).reshape(-1).view(np.int32)).cuda()
+    d_init, d_more = d(init), d(more)
+    searches = {}
+    for pct in (0, 25, 50, 75, 100):
+        hits = ns * pct // 100
+        searches[pct] = (d(np.concatenate([init[rng.permutation(n0)[:hits]], never[:ns - hits]])), hits)
+    offs = {n: torch.arange(0, k * n, k, dtype=torch.int32, device="cuda") for n in {n0, n1, ns}}
+    stream = torch.cuda.Stream()
+    dag = svdag.MyGPUHashDAG(6, pool_bytes=max(1 << 30, 64 * (n0 + n1) * 4), scratch_bytes=64 << 20)
+    results = []
+    for layout in ("ticket_board", "atomic64", "acceleration", "compact"):
+        for lanes in (1, 32):
+            if layout == "compact":
+                per_size = np.zeros(svdag.NUM_SIZE_CLASSES, np.uint32)
+                per_size[0] = buckets
+                tbl = dag.create_table(svdag.KIND_NODE, per_size)
+                add = lambda kd, n, out: tbl.add(kd, offs[n], n, k * n, out, lanes=lanes, stream=stream)
+                find = lambda kd, n, out: tbl.find(kd, offs[n], n, k * n, out, lanes=lanes, stream=stream)
+            else:
+                code = {"ticket_board": svdag.TABLE_LAYOUT_TICKET_BOARD, "atomic64": svdag.TABLE_LAYOUT_ATOMIC64,
+                        "acceleration": svdag.TABLE_LAYOUT_ACCELERATION}[layout]
+                tbl = svdag.AltHashTable(dag, code, k, buckets, 2 * (n0 + n1))
+                add = lambda kd, n, out: tbl.add(kd, n, out, lanes=lanes, stream=stream)
+                find = lambda kd, n, out: tbl.find(kd, n, out, lanes=lanes, stream=stream)
+            out0 = torch.empty(n0, dtype=torch.int32, device="cuda")
+            out1 = torch.empty(n1, dtype=torch.int32, device="cuda")
+            outs = torch.empty(ns, dtype=torch.int32, device="cuda")
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(14)]
+            torch.cuda.synchronize()
+            found = {}
+            with torch.cuda.stream(stream):
+                ev[0].record(stream)
+                add(d_init, n0, out0)
+                ev[1].record(stream)
+                for j, pct in enumerate(searches):
+                    ev[2 + 2 * j].record(stream)
+                    find(searches[pct][0], ns, outs)
+                    ev[3 + 2 * j].record(stream)
+                    found[pct] = (outs != -1).sum()
+                ev[12].record(stream)
+                add(d_more, n1, out1)
+                ev[13].record(stream)
+            stream.synchronize()
+            if layout == "compact":
+                dag.sync()
+            else:
+                tbl.sync(stream)
+            r = {"layout": layout, "lanes": lanes, "bulk_add1_ms": ev[0].elapsed_time(ev[1]),
+                 "bulk_add2_ms": ev[12].elapsed_time(ev[13])}
+            for j, pct in enumerate(searches):
+                r[f"search_hit{pct}_ms"] = ev[2 + 2 * j].elapsed_time(ev[3 + 2 * j])
+                assert int(found[pct]) == searches[pct][1], (layout, lanes, pct, int(found[pct]))
+            assert bool((out0 != -1).all()) and bool((out1 != -1).all()), (layout, lanes)
+            r["bulk_add1_mitems_s"] = n0 / r["bulk_add1_ms"] / 1e3
+            r["search_hit50_mitems_s"] = ns / r["search_hit50_ms"] / 1e3
+            st = tbl.stats(stream) if layout != "compact" else tbl.stats()
+            r["items"], r["slab_bytes"] = int(st.items), int(st.bytes)
+            results.append(r)
+            tbl.destroy()
+    dag.free()
+    print(json.dumps({"mode": "hashmap", "item_words": k, "initial_items": n0, "insert_items": n1, "search_items": ns,
+                      "buckets": buckets, "results": results}))
+
+
 def run_mode_c0(args):
     """Depth-10 terrain, then K sphere edits of the C0 stream each followed by a 256x256 frame."""
     import torch
@@ -644,7 +727,7 @@ def main():
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
-    ap.add_argument("--mode", default="serve", choices=["serve", "c0", "c2", "c3", "hash", "trace"],
+    ap.add_argument("--mode", default="serve", choices=["serve", "c0", "c2", "c3", "hash", "hashmap", "trace"],
                     help="serve = the benchmark line; the others run one sub-workload (profiling)")
     ap.add_argument("--rate", type=float, default=1000.0, help="edit arrivals per second")
     ap.add_argument("--window", type=float, default=0.5, help="seconds of the stream per step")
@@ -659,12 +742,17 @@ def main():
     ap.add_argument("--hash-lf", type=int, default=16)
     ap.add_argument("--hash-reps", type=int, default=3)
     ap.add_argument("--hash-pool", type=int, default=6 << 30)
+    ap.add_argument("--hashmap-initial", type=int, default=8 << 20)
+    ap.add_argument("--hashmap-insert", type=int, default=1 << 20)
+    ap.add_argument("--hashmap-search", type=int, default=1 << 20)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         run_reference(args)
     elif args.mode == "hash":
         run_mode_hash(args)
+    elif args.mode == "hashmap":
+        run_mode_hashmap(args)
     elif args.mode == "c0":
         run_mode_c0(args)
     elif args.mode == "c2":
