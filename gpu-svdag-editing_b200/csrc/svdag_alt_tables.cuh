@@ -230,6 +230,9 @@ SVDAG_HD uint32_t next_or_link(const AltTable& t, uint32_t* s)
                 return fresh;
             }
         } else {
+#ifdef __CUDA_ARCH__
+            __nanosleep(32); // yield: the link's holder may be a thread of this warp
+#endif
             nx = ld_relaxed(link);
         }
     }
