@@ -372,8 +372,8 @@ svdag_status svdag_alt_table_read(svdag_alt_table* table, const uint32_t* handle
     uint32_t* out_words_dev, void* stream);
 /* Waits for the stream and returns (and clears) the first latched device-side error. */
 svdag_status svdag_alt_table_sync(svdag_alt_table* table, void* stream);
-/* Occupied slots, bucket slabs, linked or lost overflow slabs taken, bytes of those slabs; synchronous,
- * returns like svdag_alt_table_sync. */
+/* Occupied slots, bucket slabs, overflow slabs linked, bytes of those slabs; synchronous, returns like
+ * svdag_alt_table_sync. */
 svdag_status svdag_alt_table_get_stats(svdag_alt_table* table, svdag_table_stats* out, void* stream);
 
 /* ---------------------------------------------------------------- inspection */
