@@ -404,4 +404,75 @@ svdag_status svdag_alt_table_get_stats(svdag_alt_table* at, svdag_table_stats* o
     return svdag_alt_table_sync(at, stream);
 }
 
+svdag_status svdag_alt_table_tune(svdag_ctx* ctx, const uint32_t* keys, uint32_t n, uint32_t itemWords, uint32_t itemsPerBucket,
+    svdag_alt_tuning* best, svdag_alt_tuning* all, void* stream)
+{
+    if (!ctx || !keys || !n || !best || itemWords < 1 || itemWords > alt::kMaxItemWords)
+        return SVDAG_ERR_INVALID;
+    const uint32_t ipb = itemsPerBucket ? itemsPerBucket : 64u;
+    const uint32_t buckets = n / ipb + 1;
+    const cudaStream_t s = (cudaStream_t)stream;
+    cudaSetDevice(ctx->device);
+    uint32_t* handles = nullptr;
+    cudaEvent_t ev[3] = {};
+    if (cudaMalloc(&handles, (size_t)n * sizeof(uint32_t)) != cudaSuccess) {
+        cudaGetLastError();
+        return SVDAG_ERR_OOM;
+    }
+    svdag_status st = SVDAG_OK;
+    for (auto& e : ev)
+        if (cudaEventCreate(&e) != cudaSuccess)
+            st = SVDAG_ERR_CUDA;
+    svdag_alt_tuning cand[SVDAG_ALT_TUNING_CANDIDATES] = {};
+    int bestIdx = -1;
+    const uint32_t layouts[3] = { kTicketBoard, kAtomic64, kAcceleration };
+    for (uint32_t c = 0; c < SVDAG_ALT_TUNING_CANDIDATES && st == SVDAG_OK; ++c) {
+        svdag_alt_tuning& r = cand[c];
+        r.layout = layouts[c / 2];
+        r.lanes = (c & 1) ? 32u : 1u;
+        r.add_ms = r.find_ms = -1.0f;
+        if (!layout_ok(r.layout, itemWords))
+            continue;
+        svdag_alt_table* t = nullptr;
+        const svdag_status cs = svdag_alt_table_create(ctx, r.layout, itemWords, buckets, 2ull * n, &t);
+        if (cs == SVDAG_ERR_OOM)
+            continue;
+        if (cs != SVDAG_OK) {
+            st = cs;
+            break;
+        }
+        svdag_status ts = SVDAG_OK;
+        if (cudaEventRecord(ev[0], s) != cudaSuccess || (ts = svdag_alt_table_add(t, keys, n, handles, r.lanes, stream)) != SVDAG_OK
+            || cudaEventRecord(ev[1], s) != cudaSuccess || (ts = svdag_alt_table_find(t, keys, n, handles, r.lanes, stream)) != SVDAG_OK
+            || cudaEventRecord(ev[2], s) != cudaSuccess)
+            ts = ts ? ts : SVDAG_ERR_CUDA;
+        const svdag_status ds = ts ? ts : svdag_alt_table_sync(t, stream); // a latched error: the sample does not fit this layout
+        if (ds == SVDAG_OK) {
+            float a = 0, f = 0;
+            cudaEventElapsedTime(&a, ev[0], ev[1]);
+            cudaEventElapsedTime(&f, ev[1], ev[2]);
+            r.add_ms = a;
+            r.find_ms = f;
+            if (bestIdx < 0 || a + f < cand[bestIdx].add_ms + cand[bestIdx].find_ms)
+                bestIdx = (int)c;
+        } else if (ds == SVDAG_ERR_CUDA) {
+            st = ds;
+        }
+        svdag_alt_table_destroy(t);
+    }
+    for (auto& e : ev)
+        if (e)
+            cudaEventDestroy(e);
+    cudaFree(handles);
+    if (st != SVDAG_OK)
+        return st;
+    if (bestIdx < 0)
+        return SVDAG_ERR_OOM;
+    *best = cand[bestIdx];
+    if (all)
+        for (uint32_t c = 0; c < SVDAG_ALT_TUNING_CANDIDATES; ++c)
+            all[c] = cand[c];
+    return SVDAG_OK;
+}
+
 } // extern "C"

@@ -210,6 +210,7 @@ _PROTOS = {
     "svdag_alt_table_read": [_P, _P, _U32, _P, _P],
     "svdag_alt_table_sync": [_P, _P],
     "svdag_alt_table_get_stats": [_P, C.POINTER(TableStats), _P],
+    "svdag_alt_table_tune": [_P, _P, _U32, _U32, _U32, _P, _P, _P],
     "svdag_get_stats": [_P, C.POINTER(Stats), _P],
     "svdag_export_level": [_P, _U32, _P, _P, _U64, C.POINTER(_U64), _P],
     "svdag_autotune": [_P, C.POINTER(Edit), _U32, _P, _P, _U32, _U64, _U32, C.POINTER(Tuning), _P],
@@ -729,6 +730,23 @@ class AltHashTable:
         if self.h:
             lib().svdag_alt_table_destroy(self.h)
             self.h = None
+
+
+class AltTuning(C.Structure):
+    _fields_ = [("layout", _U32), ("lanes", _U32), ("add_ms", C.c_float), ("find_ms", C.c_float)]
+
+
+ALT_TUNING_CANDIDATES = 6
+
+
+def alt_table_tune(dag: MyGPUHashDAG, keys, count: int, item_words: int, items_per_bucket: int = 0, stream=None):
+    """svdag_alt_table_tune: (best candidate, all candidates) among the alternative layouts and launch
+    forms, measured on `count` keys of `item_words` words (a device array)."""
+    best = AltTuning()
+    every = (AltTuning * ALT_TUNING_CANDIDATES)()
+    _check(lib().svdag_alt_table_tune(dag.h, ptr(keys), count, item_words, items_per_bucket, C.addressof(best),
+                                      C.addressof(every), stream_ptr(stream)), "svdag_alt_table_tune")
+    return best, list(every)
 
 
 def TicketBoardHashTable(dag, numBuckets, numReservedElements, itemSizeInU32):

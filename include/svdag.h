@@ -376,6 +376,23 @@ svdag_status svdag_alt_table_sync(svdag_alt_table* table, void* stream);
  * svdag_alt_table_sync. */
 svdag_status svdag_alt_table_get_stats(svdag_alt_table* table, svdag_table_stats* out, void* stream);
 
+/* One measured candidate of svdag_alt_table_tune. */
+typedef struct svdag_alt_tuning {
+    uint32_t layout; /* SVDAG_TABLE_LAYOUT_* */
+    uint32_t lanes; /* 1 or 32 */
+    float add_ms; /* bulk add of the sample into a fresh table; < 0: the layout cannot hold the sample */
+    float find_ms; /* find of every sample key afterwards */
+} svdag_alt_tuning;
+#define SVDAG_ALT_TUNING_CANDIDATES 6u
+/* Measured choice among the alternative layouts for fixed-size items, with no counterpart in the
+ * reference (which compares them offline, extras/hashmap_bench). For each layout and launch form
+ * (lanes 1 and 32) a fresh table of count / items_per_bucket + 1 buckets (items_per_bucket 0 = 64)
+ * is filled with the count keys of keys_dev and searched for all of them, timed with CUDA events on
+ * `stream`. *best receives the candidate with the least add + find time; all[] (NULL, or room for
+ * SVDAG_ALT_TUNING_CANDIDATES) every candidate. Synchronous; the tables are freed again. */
+svdag_status svdag_alt_table_tune(svdag_ctx* ctx, const uint32_t* keys_dev, uint32_t count, uint32_t item_words,
+    uint32_t items_per_bucket, svdag_alt_tuning* best, svdag_alt_tuning* all, void* stream);
+
 /* ---------------------------------------------------------------- inspection */
 
 typedef struct svdag_stats {

@@ -40,6 +40,7 @@ def test_struct_layouts(svdag_lib):
     assert C.sizeof(s.ServerConfig) == 128
     assert C.sizeof(s.RequestResult) == 48
     assert C.sizeof(s.Tuning) == 40
+    assert C.sizeof(s.AltTuning) == 16  # svdag_alt_tuning
 
 
 def test_invalid_arguments_are_rejected(svdag_lib):
@@ -51,6 +52,16 @@ def test_invalid_arguments_are_rejected(svdag_lib):
     assert L.svdag_create(C.byref(cfg), C.byref(h)) == 1
     assert L.svdag_destroy(None) == 1
     assert L.svdag_edit_apply(None, None, None) == 1
+    # alternative-layout tables: null handles are rejected before any CUDA call
+    t = C.c_void_p()
+    assert L.svdag_alt_table_create(None, 1, 2, 16, 0, C.byref(t)) == 1
+    for f in (L.svdag_alt_table_add, L.svdag_alt_table_find):
+        assert f(None, None, 0, None, 1, None) == 1
+    assert L.svdag_alt_table_read(None, None, 0, None, None) == 1
+    assert L.svdag_alt_table_sync(None, None) == 1
+    assert L.svdag_alt_table_get_stats(None, None, None) == 1
+    assert L.svdag_alt_table_destroy(None) == 1
+    assert L.svdag_alt_table_tune(None, None, 0, 2, 0, None, None, None) == 1
 
 
 def test_no_cpu_fallback_without_device(svdag_lib):

@@ -152,3 +152,28 @@ def test_hashmap_benchmark_shape(svdag_lib, dag):
             assert np.all(host(g) != INVALID)
         finally:
             t.destroy()
+
+
+@pytest.mark.parametrize("k", [1, 3])
+def test_tune_picks_the_fastest_measured_candidate(svdag_lib, dag, k):
+    import torch
+
+    rng = np.random.default_rng(70 + k)
+    n = 1 << 15
+    keys = unique_keys(rng, n, k)
+    best, every = svdag_lib.alt_table_tune(dag, dev(keys), n, k)
+    assert [(c.layout, c.lanes) for c in every] == [(1, 1), (1, 32), (2, 1), (2, 32), (3, 1), (3, 32)]
+    measured = [c for c in every if c.add_ms >= 0]
+    # Atomic64 needs two words per item
+    assert len(measured) == (4 if k == 1 else 6)
+    assert all(c.find_ms >= 0 for c in measured)
+    assert min(c.add_ms + c.find_ms for c in measured) == best.add_ms + best.find_ms
+    t = svdag_lib.AltHashTable(dag, best.layout, k, n // 64 + 1, 2 * n)
+    try:
+        h = torch.empty(n, dtype=torch.int32, device="cuda")
+        t.add(dev(keys), n, h, lanes=best.lanes)
+        t.find(dev(keys), n, h, lanes=best.lanes)
+        t.sync()
+        assert np.all(host(h) != INVALID)
+    finally:
+        t.destroy()
