@@ -6,8 +6,10 @@
 //  * warp-hybrid (lanes = 32; addAsWarpHybrid / findAsWarpHybrid): every lane holds a key, and the
 //    warp serves the lanes' keys one at a time, each lane inspecting one slot of the slab, so a slab
 //    is read with one coalesced load of its slot words (128 to 256 bytes) instead of 31 dependent ones.
-// Layouts are template arguments: a kernel's copy of the table descriptor gets its layout field
-// set to the constant, so the layout branches of the shared functions fold at compile time.
+// The warp-hybrid functions live in svdag_alt_tables.cuh beside the thread-per-key ones, written
+// against a warp type (here the intrinsics) so that the host can run them too. Layouts are template
+// arguments: a kernel's copy of the table descriptor gets its layout field set to the constant, so
+// the layout branches of the shared functions fold at compile time.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -31,11 +33,17 @@ namespace {
 constexpr int kThreads = 256;
 constexpr unsigned kFull = 0xFFFFFFFFu;
 
-__device__ __forceinline__ const uint32_t* shfl_ptr(const uint32_t* p, int src)
-{
-    return (const uint32_t*)__shfl_sync(kFull, (unsigned long long)p, src);
-}
-__device__ __forceinline__ uint64_t shfl64(uint64_t v, int src) { return __shfl_sync(kFull, (unsigned long long)v, src); }
+// The warp collectives of the warp-hybrid forms (svdag_alt_tables.cuh), every lane taking part.
+// The call-site argument only serves the host's emulated warp.
+struct DeviceWarp {
+    __device__ __forceinline__ uint32_t lane() const { return threadIdx.x & 31u; }
+    __device__ __forceinline__ uint32_t ballot(bool p, uint32_t) const { return __ballot_sync(kFull, p); }
+    __device__ __forceinline__ uint32_t shfl(uint32_t v, uint32_t src, uint32_t) const { return __shfl_sync(kFull, v, (int)src); }
+    __device__ __forceinline__ uint64_t shfl64(uint64_t v, uint32_t src, uint32_t) const
+    {
+        return __shfl_sync(kFull, (unsigned long long)v, (int)src);
+    }
+};
 
 template <uint32_t L>
 __device__ __forceinline__ AltTable with_layout(const AltTable& t)
@@ -43,143 +51,6 @@ __device__ __forceinline__ AltTable with_layout(const AltTable& t)
     AltTable c = t;
     c.layout = L;
     return c;
-}
-
-// Slot match of lane `lane` in slab s for the broadcast key (warp-hybrid find).
-template <uint32_t L>
-__device__ __forceinline__ bool lane_match(const AltTable& t, const uint32_t* s, uint32_t lane, const uint32_t* key, uint32_t tag,
-    uint64_t prefix)
-{
-    const uint32_t k = t.k;
-    if (L == kTicketBoard)
-        return ((s[0] >> lane) & 1u) && words_equal(s + body_word(L, k, lane), key, k);
-    if (L == kAtomic64)
-        return lane < 31u && ((const uint64_t*)s)[lane] == prefix && words_equal(s + body_word(L, k, lane), key + 2, k - 2u);
-    return lane >= 1u && s[lane] == tag && words_equal(s + body_word(L, k, lane), key, k);
-}
-
-// findAsWarpHybrid: returns this lane's result (kInvalid for a miss or an invalid lane).
-template <uint32_t L>
-__device__ uint32_t warp_find(const AltTable& t, const uint32_t* key, bool valid)
-{
-    const uint32_t lane = threadIdx.x & 31u;
-    uint32_t tag = 0, slab = 0, result = kInvalid;
-    uint64_t prefix = 0;
-    if (valid) {
-        const uint32_t acc = key_acc(key, t.k);
-        tag = acc_tag32(acc);
-        prefix = L == kAtomic64 ? key_prefix(key) : 0;
-        slab = bucket_index(bucket_hash(acc), t.numBuckets);
-        valid = !(L == kAtomic64 && prefix == 0);
-    }
-    bool active = valid;
-    uint32_t steps = 0;
-    for (uint32_t mask; (mask = __ballot_sync(kFull, active)) != 0;) {
-        if (++steps > kMaxSteps) { // warp-uniform
-            if (active)
-                set_status(t, SVDAG_ERR_TIMEOUT);
-            break;
-        }
-        const int src = __ffs(mask) - 1;
-        const uint32_t sSlab = __shfl_sync(kFull, slab, src);
-        const uint32_t sTag = __shfl_sync(kFull, tag, src);
-        const uint64_t sPrefix = shfl64(prefix, src);
-        const uint32_t* sKey = shfl_ptr(key, src);
-        const uint32_t* s = slab_at(t, sSlab);
-        const uint32_t hits = __ballot_sync(kFull, lane_match<L>(t, s, lane, sKey, sTag, sPrefix));
-        if (lane == (uint32_t)src) {
-            if (hits) {
-                result = sSlab * 32u + (__ffs(hits) - 1u);
-                active = false;
-            } else {
-                const uint32_t nx = s[next_word(L)];
-                if (nx == 0) {
-                    active = false;
-                } else if (nx < t.numBuckets || nx >= t.slabCount) {
-                    set_status(t, SVDAG_ERR_CORRUPT);
-                    active = false;
-                } else {
-                    slab = nx;
-                }
-            }
-        }
-    }
-    return result;
-}
-
-// addAsWarpHybrid: returns this lane's handle (kInvalid for an invalid lane or on failure).
-template <uint32_t L>
-__device__ uint32_t warp_add(const AltTable& t, const uint32_t* key, bool valid)
-{
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t k = t.k;
-    uint32_t tag = 0, slab = 0, result = kInvalid;
-    uint64_t prefix = 0;
-    if (valid) {
-        const uint32_t acc = key_acc(key, k);
-        tag = acc_tag32(acc);
-        prefix = L == kAtomic64 ? key_prefix(key) : 0;
-        slab = bucket_index(bucket_hash(acc), t.numBuckets);
-        if (L == kAtomic64 && prefix == 0) {
-            set_status(t, SVDAG_ERR_INVALID);
-            valid = false;
-        }
-    }
-    bool active = valid;
-    uint32_t steps = 0;
-    for (uint32_t mask; (mask = __ballot_sync(kFull, active)) != 0;) {
-        if (++steps > kMaxSteps) { // warp-uniform
-            if (active)
-                set_status(t, SVDAG_ERR_TIMEOUT);
-            break;
-        }
-        const int src = __ffs(mask) - 1;
-        const uint32_t sSlab = __shfl_sync(kFull, slab, src);
-        const uint32_t sTag = __shfl_sync(kFull, tag, src);
-        const uint64_t sPrefix = shfl64(prefix, src);
-        const uint32_t* sKey = shfl_ptr(key, src);
-        uint32_t* s = slab_at(t, sSlab);
-        uint32_t slot = kInvalid;
-        if (L == kTicketBoard) {
-            // one lane claims on the slot mask (at most 32 failed ORs)
-            if (lane == (uint32_t)src)
-                slot = try_claim(t, s, sTag, sPrefix);
-            slot = __shfl_sync(kFull, slot, src);
-        } else {
-            // every lane reads its slot word; the free ones are tried in order (each failed CAS is a
-            // slot another warp took)
-            const bool mine = L == kAtomic64 ? lane < 31u : lane >= 1u;
-            const bool isFree = mine && (L == kAtomic64 ? ld_relaxed64((const uint64_t*)s + lane) == 0 : ld_relaxed(s + lane) == 0);
-            uint32_t freeMask = __ballot_sync(kFull, isFree);
-            while (freeMask) {
-                const uint32_t d = __ffs(freeMask) - 1u;
-                bool won = false;
-                if (lane == d)
-                    won = L == kAtomic64 ? cas64((uint64_t*)s + d, 0, sPrefix) == 0 : cas32(s + d, 0u, sTag) == 0;
-                if (__shfl_sync(kFull, won, d)) {
-                    slot = d;
-                    break;
-                }
-                freeMask &= freeMask - 1u;
-            }
-        }
-        if (slot != kInvalid) {
-            const uint32_t first = L == kAtomic64 ? 2u : 0u;
-            if (lane < k - first)
-                s[body_word(L, k, slot) + lane] = sKey[first + lane];
-            if (lane == (uint32_t)src) {
-                result = sSlab * 32u + slot;
-                active = false;
-            }
-        } else if (lane == (uint32_t)src) {
-            const uint32_t nx = next_or_link(t, s);
-            if (nx == kNoSlab)
-                active = false;
-            else
-                slab = nx;
-        }
-    }
-    return result;
 }
 
 template <uint32_t L>
@@ -211,7 +82,8 @@ __global__ void k_alt_warp(AltTable t0, const uint32_t* __restrict__ keys, uint3
         const uint64_t i = base + lane;
         const bool valid = i < n;
         const uint32_t* key = keys + (valid ? i : 0) * t.k;
-        const uint32_t h = ADD ? warp_add<L>(t, key, valid) : warp_find<L>(t, key, valid);
+        const DeviceWarp w;
+        const uint32_t h = ADD ? warp_add<L>(w, t, key, valid) : warp_find<L>(w, t, key, valid);
         if (valid)
             handles[i] = h;
     }

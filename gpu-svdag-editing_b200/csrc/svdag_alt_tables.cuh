@@ -344,5 +344,163 @@ SVDAG_HD uint32_t slab_items(uint32_t layout, const uint32_t* s)
     return n;
 }
 
+// ---------------------------------------------------------------- warp-hybrid forms
+//
+// addAsWarpHybrid / findAsWarpHybrid (atomic64_hash_table.h:125-185, 245-300 and the same pair in
+// ticket_board_hash_table.h and acceleration_hash_table.h): every lane of a warp holds a key (or
+// none), and the warp serves the lanes' keys one at a time, each lane inspecting one slot of the
+// slab, so a slab's slot words are read by one coalesced load. W supplies the collectives lane(),
+// ballot(p, site), shfl(v, src, site) and shfl64(v, src, site); every lane takes part in every call,
+// in the same order (the loop conditions below are warp-uniform). `site` names the call (its source
+// line): the CUDA kernels pass the warp intrinsics, which ignore it; the host tests pass an emulated
+// warp that checks that all lanes of a warp stand at the same site.
+#ifdef __CUDACC__
+#define SVDAG_WARP_FN __device__ __forceinline__
+#else
+#define SVDAG_WARP_FN inline
+#endif
+
+// Whether slot `lane` of slab s holds the broadcast key.
+template <uint32_t L>
+SVDAG_HD bool lane_match(const AltTable& t, const uint32_t* s, uint32_t lane, const uint32_t* key, uint32_t tag, uint64_t prefix)
+{
+    const uint32_t k = t.k;
+    if (L == kTicketBoard)
+        return ((s[0] >> lane) & 1u) && words_equal(s + body_word(L, k, lane), key, k);
+    if (L == kAtomic64)
+        return lane < 31u && ((const uint64_t*)s)[lane] == prefix && words_equal(s + body_word(L, k, lane), key + 2, k - 2u);
+    return lane >= 1u && s[lane] == tag && words_equal(s + body_word(L, k, lane), key, k);
+}
+
+template <class W>
+SVDAG_WARP_FN const uint32_t* shfl_ptr(const W& w, const uint32_t* p, uint32_t src, uint32_t site)
+{
+    return (const uint32_t*)(uintptr_t)w.shfl64((uint64_t)(uintptr_t)p, src, site);
+}
+
+// This lane's result: the handle of a stored copy of its key, or kInvalid (a miss or no key).
+template <uint32_t L, class W>
+SVDAG_WARP_FN uint32_t warp_find(const W& w, const AltTable& t, const uint32_t* key, bool valid)
+{
+    const uint32_t lane = w.lane();
+    uint32_t tag = 0, slab = 0, result = kInvalid;
+    uint64_t prefix = 0;
+    if (valid) {
+        const uint32_t acc = key_acc(key, t.k);
+        tag = acc_tag32(acc);
+        prefix = L == kAtomic64 ? key_prefix(key) : 0;
+        slab = bucket_index(bucket_hash(acc), t.numBuckets);
+        valid = !(L == kAtomic64 && prefix == 0);
+    }
+    bool active = valid;
+    uint32_t steps = 0;
+    for (uint32_t mask; (mask = w.ballot(active, __LINE__)) != 0;) {
+        if (++steps > kMaxSteps) { // warp-uniform
+            if (active)
+                set_status(t, SVDAG_ERR_TIMEOUT);
+            break;
+        }
+        const uint32_t src = ctz32(mask);
+        const uint32_t sSlab = w.shfl(slab, src, __LINE__);
+        const uint32_t sTag = w.shfl(tag, src, __LINE__);
+        const uint64_t sPrefix = w.shfl64(prefix, src, __LINE__);
+        const uint32_t* sKey = shfl_ptr(w, key, src, __LINE__);
+        const uint32_t* s = slab_at(t, sSlab);
+        const uint32_t hits = w.ballot(lane_match<L>(t, s, lane, sKey, sTag, sPrefix), __LINE__);
+        if (lane == src) {
+            if (hits) {
+                result = sSlab * 32u + ctz32(hits);
+                active = false;
+            } else {
+                const uint32_t nx = s[next_word(L)];
+                if (nx == 0) {
+                    active = false;
+                } else if (nx < t.numBuckets || nx >= t.slabCount) {
+                    set_status(t, SVDAG_ERR_CORRUPT);
+                    active = false;
+                } else {
+                    slab = nx;
+                }
+            }
+        }
+    }
+    return result;
+}
+
+// This lane's handle: its key stored in a fresh slot (kInvalid for no key or on failure).
+template <uint32_t L, class W>
+SVDAG_WARP_FN uint32_t warp_add(const W& w, const AltTable& t, const uint32_t* key, bool valid)
+{
+    const uint32_t lane = w.lane();
+    const uint32_t k = t.k;
+    uint32_t tag = 0, slab = 0, result = kInvalid;
+    uint64_t prefix = 0;
+    if (valid) {
+        const uint32_t acc = key_acc(key, k);
+        tag = acc_tag32(acc);
+        prefix = L == kAtomic64 ? key_prefix(key) : 0;
+        slab = bucket_index(bucket_hash(acc), t.numBuckets);
+        if (L == kAtomic64 && prefix == 0) {
+            set_status(t, SVDAG_ERR_INVALID);
+            valid = false;
+        }
+    }
+    bool active = valid;
+    uint32_t steps = 0;
+    for (uint32_t mask; (mask = w.ballot(active, __LINE__)) != 0;) {
+        if (++steps > kMaxSteps) { // warp-uniform
+            if (active)
+                set_status(t, SVDAG_ERR_TIMEOUT);
+            break;
+        }
+        const uint32_t src = ctz32(mask);
+        const uint32_t sSlab = w.shfl(slab, src, __LINE__);
+        const uint32_t sTag = w.shfl(tag, src, __LINE__);
+        const uint64_t sPrefix = w.shfl64(prefix, src, __LINE__);
+        const uint32_t* sKey = shfl_ptr(w, key, src, __LINE__);
+        uint32_t* s = slab_at(t, sSlab);
+        uint32_t slot = kInvalid;
+        if (L == kTicketBoard) {
+            // one lane claims on the slot mask (at most 32 failed ORs)
+            if (lane == src)
+                slot = try_claim(t, s, sTag, sPrefix);
+            slot = w.shfl(slot, src, __LINE__);
+        } else {
+            // every lane reads its slot word; the free ones are tried in order (each failed CAS is a
+            // slot another warp took)
+            const bool mine = L == kAtomic64 ? lane < 31u : lane >= 1u;
+            const bool isFree = mine && (L == kAtomic64 ? ld_relaxed64((const uint64_t*)s + lane) == 0 : ld_relaxed(s + lane) == 0);
+            uint32_t freeMask = w.ballot(isFree, __LINE__);
+            while (freeMask) {
+                const uint32_t d = ctz32(freeMask);
+                uint32_t won = 0;
+                if (lane == d)
+                    won = L == kAtomic64 ? cas64((uint64_t*)s + d, 0, sPrefix) == 0 : cas32(s + d, 0u, sTag) == 0;
+                if (w.shfl(won, d, __LINE__)) {
+                    slot = d;
+                    break;
+                }
+                freeMask &= freeMask - 1u;
+            }
+        }
+        if (slot != kInvalid) {
+            const uint32_t first = L == kAtomic64 ? 2u : 0u;
+            if (lane < k - first)
+                s[body_word(L, k, slot) + lane] = sKey[first + lane];
+            if (lane == src) {
+                result = sSlab * 32u + slot;
+                active = false;
+            }
+        } else if (lane == src) {
+            const uint32_t nx = next_or_link(t, s);
+            if (nx == kNoSlab)
+                active = false;
+            else
+                slab = nx;
+        }
+    }
+    return result;
+}
+
 } // namespace alt
 } // namespace svdag

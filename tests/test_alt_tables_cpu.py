@@ -213,3 +213,21 @@ print("ok")
         pytest.skip("ThreadSanitizer could not run here: " + r.stderr[-300:])
     assert "WARNING: ThreadSanitizer" not in r.stderr, r.stderr[-3000:]
     assert r.returncode == 0 and "ok" in r.stdout, r.stderr[-2000:]
+
+
+@pytest.fixture(scope="module")
+def host_so(tmp_path_factory):
+    if shutil.which("g++") is None:
+        pytest.skip("no host C++ compiler")
+    return _compile(str(tmp_path_factory.mktemp("altw")))
+
+
+@pytest.mark.parametrize("warps", [1, 4])
+@pytest.mark.parametrize("layout,k,buckets", [(TB, 1, 5), (TB, 3, 40), (TB, 32, 5), (A64, 2, 5), (A64, 3, 40),
+                                              (A64, 32, 5), (ACC, 1, 5), (ACC, 3, 40), (ACC, 32, 5)])
+def test_warp_hybrid_forms_on_emulated_warps(host_so, layout, k, buckets, warps):
+    """The warp-hybrid add and find (the lanes = 32 kernels) run by emulated warps of 32 threads,
+    several warps at once: same set semantics, exact exhaustion and no lane missing a collective."""
+    r = subprocess.run(["python", os.path.join(HERE, "alt_warp_child.py"), host_so, str(layout), str(k), str(buckets),
+                        str(warps)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), (r.stdout[-1000:], r.stderr[-3000:])
