@@ -19,6 +19,7 @@ def load(so):
     lib.alt_host_create.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64]
     lib.alt_host_destroy.argtypes = [C.c_void_p]
     lib.alt_host_warp_op.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_int]
+    lib.alt_host_find.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32]
     lib.alt_host_read.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
     lib.alt_host_status.restype = C.c_uint32
     lib.alt_host_status.argtypes = [C.c_void_p]
@@ -91,6 +92,11 @@ def main():
         f = t.op(np.concatenate([keys, absent]), add=False)
         assert np.all(f[:n] != INVALID) and np.all(f[n:] == INVALID)
         assert np.array_equal(t.read(f[:n]), keys)
+        # the thread-per-key find agrees with the warp-hybrid one (same hash, same slot order)
+        q = np.ascontiguousarray(np.concatenate([keys, absent]), dtype=np.uint32)
+        g = np.empty(2 * n, dtype=np.uint32)
+        lib.alt_host_find(t.h, q.ctypes.data, 2 * n, g.ctypes.data, 8)
+        assert np.array_equal(g, f)
         assert t.status() == 0
     finally:
         t.free()

@@ -90,6 +90,33 @@ def test_add_then_find(svdag_lib, dag, lanes, kind):
     assert st.overflow_slabs > 0
 
 
+@pytest.mark.parametrize("add_lanes,find_lanes", [(1, 32), (32, 1), (8, 2), (2, 16)])
+def test_lane_counts_agree_on_buckets_and_tags(svdag_lib, dag, add_lanes, find_lanes):
+    """A key hashed by G cooperating lanes (each lane's word terms combined by a group XOR) lands in
+    the bucket and carries the tag of the one-thread hash, so a table filled with one lane count is
+    searched with another (the reference's warp == thread hash test, utils_tests.cu:204-233)."""
+    import torch
+
+    rng = np.random.default_rng(300 + add_lanes * 40 + find_lanes)
+    n = 8000
+    for kind, gen in ((0, node_keys), (1, leaf_keys)):
+        words, offs = gen(rng, 2 * n)
+        keys = key_list(words, offs)
+        tbl = dag.create_table(kind, [97] * 9)
+        h = torch.empty(2 * n, dtype=torch.int32, device="cuda")
+        tbl.add(dev(words[: offs[n]]), dev(offs[:n]), n, int(offs[n]), h, lanes=add_lanes)
+        tbl.find(dev(words), dev(offs), 2 * n, len(words), h, lanes=find_lanes)
+        out = torch.empty((2 * n, 10), dtype=torch.int32, device="cuda")
+        tbl.read(h, 2 * n, out)
+        dag.sync()
+        hf, got = h.cpu().numpy().view(np.uint32), out.cpu().numpy().view(np.uint32)
+        assert np.all(hf[:n] != 0xFFFFFFFF)
+        assert all(tuple(got[i][: len(keys[i])]) == keys[i] for i in range(n))
+        inserted = set(keys[:n])
+        assert all(hf[i] == 0xFFFFFFFF for i in range(n, 2 * n) if keys[i] not in inserted)
+        tbl.destroy()
+
+
 @pytest.mark.parametrize("lanes", [1, 8, 32])
 def test_find_or_add_dedups(svdag_lib, dag, lanes):
     import torch

@@ -177,3 +177,26 @@ def test_tune_picks_the_fastest_measured_candidate(svdag_lib, dag, k):
         assert np.all(host(h) != INVALID)
     finally:
         t.destroy()
+
+
+@pytest.mark.parametrize("add_lanes,find_lanes", [(1, 32), (32, 1)])
+@pytest.mark.parametrize("layout", [TB, A64, ACC])
+def test_launch_forms_interoperate(svdag_lib, dag, layout, add_lanes, find_lanes):
+    """Keys added thread per key are found warp-hybrid and the other way round: both forms hash,
+    place and compare alike."""
+    import torch
+
+    rng = np.random.default_rng(90 + layout + add_lanes)
+    n = 10000
+    keys = unique_keys(rng, n, 4)
+    absent = unique_keys(rng, n, 4, exclude=keys)
+    t = svdag_lib.AltHashTable(dag, layout, 4, 11, 2 * n)
+    try:
+        h = torch.empty(n, dtype=torch.int32, device="cuda")
+        t.add(dev(keys), n, h, lanes=add_lanes)
+        f = torch.empty(2 * n, dtype=torch.int32, device="cuda")
+        t.find(dev(np.concatenate([keys, absent])), 2 * n, f, lanes=find_lanes)
+        t.sync()
+        assert np.array_equal(host(f)[:n], host(h)) and np.all(host(f)[n:] == INVALID)
+    finally:
+        t.destroy()
