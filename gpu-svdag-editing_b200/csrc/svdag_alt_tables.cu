@@ -190,8 +190,11 @@ svdag_status svdag_alt_table_create(svdag_ctx* ctx, uint32_t layout, uint32_t it
     t.slabs = (uint32_t*)((char*)at->mem + 256);
     const uint32_t ctlInit[kCtlWords] = { numBuckets };
     svdag_status st = SVDAG_OK;
+    // Both run on the legacy default stream and may still be in flight when they return; the wait
+    // orders them before work on any stream, non-blocking streams included.
     if (cudaMemset(at->mem, 0, bytes) != cudaSuccess
-        || cudaMemcpy(t.ctl, ctlInit, sizeof(ctlInit), cudaMemcpyHostToDevice) != cudaSuccess)
+        || cudaMemcpy(t.ctl, ctlInit, sizeof(ctlInit), cudaMemcpyHostToDevice) != cudaSuccess
+        || cudaStreamSynchronize(0) != cudaSuccess)
         st = SVDAG_ERR_CUDA;
     if (st) {
         cudaGetLastError();

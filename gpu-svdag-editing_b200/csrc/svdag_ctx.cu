@@ -211,6 +211,10 @@ svdag_status svdag_create(const svdag_config* cfg, svdag_ctx** out)
                 m = kNone;
         e = cudaMemcpy(ctx->ctl, &init, sizeof(init), cudaMemcpyHostToDevice);
     }
+    // The memset and the copy run on the legacy default stream and may still be in flight when they
+    // return; waiting here orders them before the caller's work on any stream (non-blocking included).
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(0);
     if (e != cudaSuccess) {
         cudaFree(ctx->pool);
         delete ctx;
