@@ -538,6 +538,7 @@ def run_mode_hashmap(args):
         searches[pct] = (d(np.concatenate([init[rng.permutation(n0)[:hits]], never[:ns - hits]])), hits)
     offs = {n: torch.arange(0, k * n, k, dtype=torch.int32, device="cuda") for n in {n0, n1, ns}}
     stream = torch.cuda.Stream()
+    peak, peak_kind = measured_peak_gbs()
     dag = svdag.MyGPUHashDAG(6, pool_bytes=max(1 << 30, 64 * (n0 + n1) * 4), scratch_bytes=64 << 20)
     results = []
     for layout in ("ticket_board", "atomic64", "acceleration", "compact"):
@@ -585,13 +586,22 @@ def run_mode_hashmap(args):
             assert bool((out0 != -1).all()) and bool((out1 != -1).all()), (layout, lanes)
             r["bulk_add1_mitems_s"] = n0 / r["bulk_add1_ms"] / 1e3
             r["search_hit50_mitems_s"] = ns / r["search_hit50_ms"] / 1e3
+            # algorithmic bytes, the same fixed formulas for every layout: add 4k + 32 + 4k + 4,
+            # find 4k + 32 + 4k*hit + 4 per key of k words
+            add_b = n0 * (8 * k + 36)
+            r["bulk_add1_gbs"] = add_b / r["bulk_add1_ms"] / 1e6
+            r["bulk_add1_frac"] = r["bulk_add1_gbs"] / peak
+            for pct in searches:
+                find_b = ns * (4 * k + 36) + searches[pct][1] * 4 * k
+                r[f"search_hit{pct}_gbs"] = find_b / r[f"search_hit{pct}_ms"] / 1e6
+            r["search_hit50_frac"] = r["search_hit50_gbs"] / peak
             st = tbl.stats(stream) if layout != "compact" else tbl.stats()
             r["items"], r["slab_bytes"] = int(st.items), int(st.bytes)
             results.append(r)
             tbl.destroy()
     dag.free()
     print(json.dumps({"mode": "hashmap", "item_words": k, "initial_items": n0, "insert_items": n1, "search_items": ns,
-                      "buckets": buckets, "results": results}))
+                      "buckets": buckets, "hbm_peak_gbs": peak, "peak": peak_kind, "results": results}))
 
 
 def run_mode_c0(args):
