@@ -72,3 +72,37 @@ def test_no_cpu_fallback_without_device(svdag_lib):
     with pytest.raises(svdag_lib.SvdagError) as e:
         svdag_lib.MyGPUHashDAG(10)
     assert e.value.status == 6  # SVDAG_ERR_NO_DEVICE
+
+
+def test_header_is_c11_and_the_binding_lays_out_structs_alike(svdag_lib, tmp_path):
+    """include/svdag.h compiles as strict C11, every ctypes structure of the Python binding has the
+    size and field offsets a C compiler gives the header's struct, and a C program that takes the
+    address of every exported function links against libsvdag.so."""
+    import shutil
+
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    s = svdag_lib
+    pairs = {"svdag_config": s.Config, "svdag_terrain_params": s.TerrainParams, "svdag_edit": s.Edit,
+             "svdag_edit_stats": s.EditStats, "svdag_edit_record": s.EditRecord, "svdag_trace_params": s.TraceParams,
+             "svdag_server_config": s.ServerConfig, "svdag_request_result": s.RequestResult,
+             "svdag_replay_action": s.ReplayAction, "svdag_shade_params": s.ShadeParams, "svdag_tuning": s.Tuning,
+             "svdag_stats": s.Stats, "svdag_table_stats": s.TableStats, "svdag_alt_tuning": s.AltTuning}
+    lines = ["#include <stddef.h>", '#include "svdag.h"']
+    for cname, cls in pairs.items():
+        lines.append(f'_Static_assert(sizeof({cname}) == {C.sizeof(cls)}, "size of {cname}");')
+        for fname, *_ in cls._fields_:
+            off = getattr(cls, fname).offset
+            lines.append(f'_Static_assert(offsetof({cname}, {fname}) == {off}, "{cname}.{fname}");')
+    lines.append(f'_Static_assert(sizeof(svdag_hit) == {s.HIT_DTYPE.itemsize}, "size of svdag_hit");')
+    lines.append("typedef void (*any_fn)(void);")
+    lines.append("any_fn const every_function[] = {" + ", ".join(f"(any_fn)&{f}" for f in s.EXPORTED) + "};")
+    lines.append("int main(void) { return every_function[0] == 0; }")
+    src = tmp_path / "abi.c"
+    src.write_text("\n".join(lines) + "\n")
+    inc = os.path.join(ROOT, "include")
+    libdir = os.path.dirname(s.LIB_PATH)
+    r = subprocess.run(["gcc", "-std=c11", "-pedantic", "-Wall", "-Werror", "-I", inc, str(src), "-L", libdir, "-lsvdag",
+                        "-Wl,--unresolved-symbols=ignore-in-shared-libs", "-o", str(tmp_path / "abi")],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
