@@ -515,9 +515,10 @@ def run_mode_hashmap(args):
     """The reference's table benchmark (extras/hashmap_bench/src/main.cu:560-720, defaults :850-873)
     over every slab layout: items of 2 words, a bulk add of 8M items, 1M finds at hit rates
     0/25/50/75/100 %, a second bulk add of 1M items, 64 items per bucket, room reserved for twice the
-    items. Layouts: ticket_board, atomic64, acceleration (svdag_alt_table_*) and compact (the level
-    tables' layout; its keys are 2-word node keys, a one-bit child mask then a word). Each runs thread
-    per key (lanes 1) and warp-hybrid / 32 lanes per key (lanes 32). Every phase is checked: all adds
+    items. Layouts: ticket_board, atomic64, acceleration, individual_chaining (svdag_alt_table_*) and
+    compact (the level tables' layout; its keys are 2-word node keys, a one-bit child mask then a
+    word). Each runs thread per key (lanes 1) and warp-hybrid / 32 lanes per key (lanes 32), except
+    individual_chaining, which has only the thread-per-key form. Every phase is checked: all adds
     stored, exactly the expected finds hit."""
     import torch
 
@@ -541,8 +542,8 @@ def run_mode_hashmap(args):
     peak, peak_kind = measured_peak_gbs()
     dag = svdag.MyGPUHashDAG(6, pool_bytes=max(1 << 30, 64 * (n0 + n1) * 4), scratch_bytes=64 << 20)
     results = []
-    for layout in ("ticket_board", "atomic64", "acceleration", "compact"):
-        for lanes in (1, 32):
+    for layout in ("ticket_board", "atomic64", "acceleration", "individual_chaining", "compact"):
+        for lanes in ((1,) if layout == "individual_chaining" else (1, 32)):
             if layout == "compact":
                 per_size = np.zeros(svdag.NUM_SIZE_CLASSES, np.uint32)
                 per_size[0] = buckets
@@ -551,7 +552,8 @@ def run_mode_hashmap(args):
                 find = lambda kd, n, out: tbl.find(kd, offs[n], n, k * n, out, lanes=lanes, stream=stream)
             else:
                 code = {"ticket_board": svdag.TABLE_LAYOUT_TICKET_BOARD, "atomic64": svdag.TABLE_LAYOUT_ATOMIC64,
-                        "acceleration": svdag.TABLE_LAYOUT_ACCELERATION}[layout]
+                        "acceleration": svdag.TABLE_LAYOUT_ACCELERATION,
+                        "individual_chaining": svdag.TABLE_LAYOUT_INDIVIDUAL_CHAINING}[layout]
                 tbl = svdag.AltHashTable(dag, code, k, buckets, 2 * (n0 + n1))
                 add = lambda kd, n, out: tbl.add(kd, n, out, lanes=lanes, stream=stream)
                 find = lambda kd, n, out: tbl.find(kd, n, out, lanes=lanes, stream=stream)

@@ -96,6 +96,22 @@ __global__ void k_alt_read(AltTable t, const uint32_t* __restrict__ handles, uin
         read(t, handles[i], out + (uint64_t)i * t.k);
 }
 
+// Nodes reachable from the IndividualChaining heads (thread per bucket, walks bounded by the arena).
+__global__ void k_chain_count(AltTable t, unsigned long long* count)
+{
+    unsigned long long n = 0;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < t.numBuckets; b += stride)
+        for (uint32_t cur = t.heads[b], steps = 0; cur != 0 && cur <= t.slabCount && steps < t.slabCount; ++steps) {
+            ++n;
+            cur = slab_at(t, cur - 1u)[t.k];
+        }
+    for (int o = 16; o; o >>= 1)
+        n += __shfl_xor_sync(kFull, n, o);
+    if ((threadIdx.x & 31u) == 0 && n)
+        atomicAdd(count, n);
+}
+
 __global__ void k_alt_count(AltTable t, uint32_t slabs, unsigned long long* count)
 {
     unsigned long long n = 0;
@@ -131,7 +147,7 @@ svdag_status launch_op(svdag_alt_table* at, const uint32_t* keys, uint32_t n, ui
     const cudaStream_t s = (cudaStream_t)stream;
     const AltTable& t = at->t;
     const int grid = grid_of(at, n);
-    if (lanes != 1) {
+    if (lanes != 1 && t.layout != kIndividualChaining) { // a chain walk is one key's: no warp form
         switch (t.layout) {
         case kTicketBoard: k_alt_warp<kTicketBoard, ADD><<<grid, kThreads, 0, s>>>(t, keys, n, handles); break;
         case kAtomic64: k_alt_warp<kAtomic64, ADD><<<grid, kThreads, 0, s>>>(t, keys, n, handles); break;
@@ -141,12 +157,14 @@ svdag_status launch_op(svdag_alt_table* at, const uint32_t* keys, uint32_t n, ui
         switch (t.layout) {
         case kTicketBoard: k_alt_add<kTicketBoard><<<grid, kThreads, 0, s>>>(t, keys, n, handles); break;
         case kAtomic64: k_alt_add<kAtomic64><<<grid, kThreads, 0, s>>>(t, keys, n, handles); break;
+        case kIndividualChaining: k_alt_add<kIndividualChaining><<<grid, kThreads, 0, s>>>(t, keys, n, handles); break;
         default: k_alt_add<kAcceleration><<<grid, kThreads, 0, s>>>(t, keys, n, handles); break;
         }
     } else {
         switch (t.layout) {
         case kTicketBoard: k_alt_find<kTicketBoard><<<grid, kThreads, 0, s>>>(t, keys, n, handles); break;
         case kAtomic64: k_alt_find<kAtomic64><<<grid, kThreads, 0, s>>>(t, keys, n, handles); break;
+        case kIndividualChaining: k_alt_find<kIndividualChaining><<<grid, kThreads, 0, s>>>(t, keys, n, handles); break;
         default: k_alt_find<kAcceleration><<<grid, kThreads, 0, s>>>(t, keys, n, handles); break;
         }
     }
@@ -164,11 +182,9 @@ svdag_status svdag_alt_table_create(svdag_ctx* ctx, uint32_t layout, uint32_t it
     if (!ctx || !out || !layout_ok(layout, itemWords) || numBuckets == 0)
         return SVDAG_ERR_INVALID;
     *out = nullptr;
-    const uint32_t slabs = arena_slabs(layout, numBuckets, reservedItems);
-    if (!slabs)
+    const unsigned long long bytes = table_layout(layout, itemWords, numBuckets, reservedItems, nullptr, nullptr);
+    if (!bytes)
         return SVDAG_ERR_INVALID;
-    const uint32_t sw = slab_words(layout, itemWords);
-    const unsigned long long bytes = 256ull + (unsigned long long)slabs * sw * 4ull;
     cudaSetDevice(ctx->device);
     auto* at = new (std::nothrow) svdag_alt_table();
     if (!at)
@@ -181,14 +197,8 @@ svdag_status svdag_alt_table_create(svdag_ctx* ctx, uint32_t layout, uint32_t it
         return SVDAG_ERR_OOM;
     }
     AltTable& t = at->t;
-    t.layout = layout;
-    t.k = itemWords;
-    t.numBuckets = numBuckets;
-    t.slabWords = sw;
-    t.slabCount = slabs;
-    t.ctl = (uint32_t*)at->mem;
-    t.slabs = (uint32_t*)((char*)at->mem + 256);
-    const uint32_t ctlInit[kCtlWords] = { numBuckets };
+    table_layout(layout, itemWords, numBuckets, reservedItems, at->mem, &t);
+    const uint32_t ctlInit[kCtlWords] = { initial_counter(layout, numBuckets) };
     svdag_status st = SVDAG_OK;
     // Both run on the legacy default stream and may still be in flight when they return; the wait
     // orders them before work on any stream, non-blocking streams included.
@@ -266,16 +276,21 @@ svdag_status svdag_alt_table_get_stats(svdag_alt_table* at, svdag_table_stats* o
     SVDAG_CUDA(cudaMemcpyAsync(&next, &at->t.ctl[kCtlNextSlab], sizeof(next), cudaMemcpyDeviceToHost, s));
     SVDAG_CUDA(cudaStreamSynchronize(s));
     const uint32_t used = std::min(next, at->t.slabCount);
+    const bool chain = at->t.layout == kIndividualChaining;
     SVDAG_CUDA(cudaMemsetAsync(at->countDev, 0, sizeof(unsigned long long), s));
-    k_alt_count<<<grid_of(at, used), kThreads, 0, s>>>(at->t, used, at->countDev);
+    if (chain)
+        k_chain_count<<<grid_of(at, at->t.numBuckets), kThreads, 0, s>>>(at->t, at->countDev);
+    else
+        k_alt_count<<<grid_of(at, used), kThreads, 0, s>>>(at->t, used, at->countDev);
     SVDAG_CUDA(cudaGetLastError());
     unsigned long long items = 0;
     SVDAG_CUDA(cudaMemcpyAsync(&items, at->countDev, sizeof(items), cudaMemcpyDeviceToHost, s));
     SVDAG_CUDA(cudaStreamSynchronize(s));
     out->items = items;
     out->buckets = at->t.numBuckets;
-    out->overflow_slabs = used - at->t.numBuckets;
-    out->bytes = (unsigned long long)used * at->t.slabWords * 4ull;
+    out->overflow_slabs = chain ? 0 : used - at->t.numBuckets;
+    out->bytes = (chain ? ((unsigned long long)at->t.numBuckets * 4ull + 255ull) / 256ull * 256ull : 0ull)
+        + (unsigned long long)used * at->t.slabWords * 4ull;
     return svdag_alt_table_sync(at, stream);
 }
 
@@ -300,11 +315,14 @@ svdag_status svdag_alt_table_tune(svdag_ctx* ctx, const uint32_t* keys, uint32_t
             st = SVDAG_ERR_CUDA;
     svdag_alt_tuning cand[SVDAG_ALT_TUNING_CANDIDATES] = {};
     int bestIdx = -1;
-    const uint32_t layouts[3] = { kTicketBoard, kAtomic64, kAcceleration };
+    // (layout, lanes): each slab layout thread per key and warp-hybrid, IndividualChaining thread per key
+    const uint32_t layouts[SVDAG_ALT_TUNING_CANDIDATES] = { kTicketBoard, kTicketBoard, kAtomic64, kAtomic64, kAcceleration,
+        kAcceleration, kIndividualChaining };
+    const uint32_t laneCounts[SVDAG_ALT_TUNING_CANDIDATES] = { 1, 32, 1, 32, 1, 32, 1 };
     for (uint32_t c = 0; c < SVDAG_ALT_TUNING_CANDIDATES && st == SVDAG_OK; ++c) {
         svdag_alt_tuning& r = cand[c];
-        r.layout = layouts[c / 2];
-        r.lanes = (c & 1) ? 32u : 1u;
+        r.layout = layouts[c];
+        r.lanes = laneCounts[c];
         r.add_ms = r.find_ms = -1.0f;
         if (!layout_ok(r.layout, itemWords))
             continue;

@@ -19,6 +19,9 @@
 //                 words are both 0 cannot be stored (the reference requires the same).
 //   Acceleration: [0] next, [s] = 32-bit tag of slot s (s = 1..31, 0 = free), items of slots
 //                 1..31 from word 32. A slot is claimed by a CAS of its tag.
+// IndividualChaining (individual_chaining_hash_table.h) has no slabs: a head word per bucket and an
+// arena of nodes of k + 1 words (the item, then the next node's id + 1, 0 = end), taken from a bump
+// counter and pushed onto the bucket's head by CAS. Its handle is the node's id.
 //
 // The thread-per-key functions below compile for the device and, unchanged, for the host (the
 // atomics are GCC builtins there), so their claim and chain logic can be exercised by host threads.
@@ -33,12 +36,13 @@
 namespace svdag {
 namespace alt {
 
-enum Layout : uint32_t { kTicketBoard = 1, kAtomic64 = 2, kAcceleration = 3 };
+enum Layout : uint32_t { kTicketBoard = 1, kAtomic64 = 2, kAcceleration = 3, kIndividualChaining = 4 };
 
 constexpr uint32_t kInvalid = 0xFFFFFFFFu;
 constexpr uint32_t kNoSlab = 0xFFFFFFFFu;
 constexpr uint32_t kMaxItemWords = 32;
 constexpr uint32_t kMaxSlabs = 1u << 27; // handles slab * 32 + slot stay below 2^32 - 1
+constexpr uint32_t kMaxNodes = 1u << 30; // IndividualChaining nodes (handles are node ids)
 constexpr uint32_t kMaxSteps = 1u << 22; // slabs one add or find may visit before it gives up
 constexpr uint32_t kLinkBusy = 0xFFFFFFFFu; // next word of a slab whose successor is being linked
 constexpr uint32_t kMaxSpin = 1u << 20; // reads of a busy next word before a wait gives up
@@ -50,11 +54,12 @@ struct AltTable {
     uint32_t layout;
     uint32_t k; // item words
     uint32_t numBuckets;
-    uint32_t slabWords; // stride of a slab in words, a multiple of 8
-    uint32_t slabCount; // slabs in the arena
+    uint32_t slabWords; // stride of a slab in words, a multiple of 8 (IndividualChaining: of a node, k + 1)
+    uint32_t slabCount; // slabs in the arena (IndividualChaining: nodes)
     uint32_t pad;
-    uint32_t* slabs;
+    uint32_t* slabs; // the arena (IndividualChaining: the nodes)
     uint32_t* ctl;
+    uint32_t* heads; // IndividualChaining: first node id + 1 of each bucket (0 = empty); else null
 };
 
 SVDAG_HD uint32_t round8(uint32_t w) { return (w + 7u) & ~7u; }
@@ -66,7 +71,7 @@ SVDAG_HD uint32_t slots_per_slab(uint32_t layout) { return layout == kTicketBoar
 SVDAG_HD uint32_t next_word(uint32_t layout) { return layout == kTicketBoard ? 1u : layout == kAtomic64 ? 62u : 0u; }
 SVDAG_HD bool layout_ok(uint32_t layout, uint32_t k)
 {
-    return (layout == kTicketBoard || layout == kAcceleration) ? (k >= 1 && k <= kMaxItemWords)
+    return (layout == kTicketBoard || layout == kAcceleration || layout == kIndividualChaining) ? (k >= 1 && k <= kMaxItemWords)
          : layout == kAtomic64 ? (k >= 2 && k <= kMaxItemWords) : false;
 }
 // Slabs of a table's arena: the bucket slabs and overflow slabs for `reserved` more items, or 0 when
@@ -77,6 +82,41 @@ inline uint32_t arena_slabs(uint32_t layout, uint32_t numBuckets, uint64_t reser
     const uint64_t slabs = (uint64_t)numBuckets + overflow;
     return slabs > kMaxSlabs ? 0u : (uint32_t)slabs;
 }
+// Bytes of a table's single allocation, 0 when the sizes exceed the handle space. With `base` set,
+// *t becomes the descriptor of a table in that allocation: a 256-byte control block, then the
+// IndividualChaining heads (rounded to 256 bytes), then the arena.
+inline uint64_t table_layout(uint32_t layout, uint32_t k, uint32_t numBuckets, uint64_t reserved, void* base, AltTable* t)
+{
+    AltTable d {};
+    d.layout = layout;
+    d.k = k;
+    d.numBuckets = numBuckets;
+    uint64_t headBytes = 0, count = 0;
+    if (layout == kIndividualChaining) {
+        count = reserved ? reserved : 1;
+        if (count > kMaxNodes)
+            return 0;
+        headBytes = ((uint64_t)numBuckets * 4u + 255u) & ~255ull;
+        d.slabWords = k + 1;
+    } else {
+        count = arena_slabs(layout, numBuckets, reserved);
+        if (!count)
+            return 0;
+        d.slabWords = slab_words(layout, k);
+    }
+    d.slabCount = (uint32_t)count;
+    if (base) {
+        d.ctl = (uint32_t*)base;
+        d.heads = headBytes ? (uint32_t*)((char*)base + 256) : nullptr;
+        d.slabs = (uint32_t*)((char*)base + 256 + headBytes);
+        *t = d;
+    }
+    return 256 + headBytes + count * d.slabWords * 4ull;
+}
+// Initial value of the control block's bump counter: overflow slabs follow the bucket slabs; nodes
+// start at 0.
+inline uint32_t initial_counter(uint32_t layout, uint32_t numBuckets) { return layout == kIndividualChaining ? 0u : numBuckets; }
+
 // Slot numbers a layout uses: 0..31, 0..30 or 1..31.
 SVDAG_HD bool slot_ok(uint32_t layout, uint32_t slot)
 {
@@ -243,10 +283,61 @@ SVDAG_HD uint32_t next_or_link(const AltTable& t, uint32_t* s)
     return nx;
 }
 
+// IndividualChaining add (individual_chaining_hash_table.h:271-296): a node from the counter, the
+// item written, then pushed onto the bucket's head by CAS with its next word set to the head it
+// replaces. Each failed CAS is another push that succeeded; the loop is bounded all the same.
+SVDAG_HD uint32_t chain_add(const AltTable& t, const uint32_t* key)
+{
+    const uint32_t k = t.k;
+    uint32_t* head = &t.heads[bucket_index(bucket_hash(key_acc(key, k)), t.numBuckets)];
+    const uint32_t id = add32(&t.ctl[kCtlNextSlab], 1u);
+    if (id >= t.slabCount) {
+        set_status(t, SVDAG_ERR_OOM);
+        return kInvalid;
+    }
+    uint32_t* node = slab_at(t, id);
+    for (uint32_t i = 0; i < k; ++i)
+        node[i] = key[i];
+    uint32_t old = ld_relaxed(head);
+    for (uint32_t spin = 0; spin < kMaxSpin; ++spin) {
+        node[k] = old;
+        const uint32_t seen = cas32(head, old, id + 1u);
+        if (seen == old)
+            return id;
+        old = seen;
+    }
+    set_status(t, SVDAG_ERR_TIMEOUT);
+    return kInvalid;
+}
+
+// IndividualChaining find (individual_chaining_hash_table.h:236-248): the first node of the chain
+// holding the key (the most recently added copy).
+SVDAG_HD uint32_t chain_find(const AltTable& t, const uint32_t* key)
+{
+    const uint32_t k = t.k;
+    uint32_t cur = t.heads[bucket_index(bucket_hash(key_acc(key, k)), t.numBuckets)];
+    for (uint32_t step = 0; step < kMaxSteps; ++step) {
+        if (cur == 0)
+            return kInvalid;
+        if (cur > t.slabCount) {
+            set_status(t, SVDAG_ERR_CORRUPT);
+            return kInvalid;
+        }
+        const uint32_t* node = slab_at(t, cur - 1u);
+        if (words_equal(node, key, k))
+            return cur - 1u;
+        cur = node[k];
+    }
+    set_status(t, SVDAG_ERR_TIMEOUT);
+    return kInvalid;
+}
+
 // add (ticket_board_hash_table.h:24-60, atomic64_hash_table.h:36-64, acceleration_hash_table.h:31-72):
 // stores the key in a fresh slot, duplicates included, and returns its handle.
 SVDAG_HD uint32_t add(const AltTable& t, const uint32_t* key)
 {
+    if (t.layout == kIndividualChaining)
+        return chain_add(t, key);
     const uint32_t k = t.k;
     const uint32_t acc = key_acc(key, k);
     const uint32_t tag = acc_tag32(acc);
@@ -278,6 +369,8 @@ SVDAG_HD uint32_t add(const AltTable& t, const uint32_t* key)
 // handle of a stored copy of the key, or kInvalid.
 SVDAG_HD uint32_t find(const AltTable& t, const uint32_t* key)
 {
+    if (t.layout == kIndividualChaining)
+        return chain_find(t, key);
     const uint32_t k = t.k;
     const uint32_t acc = key_acc(key, k);
     const uint32_t tag = acc_tag32(acc);
@@ -314,6 +407,12 @@ SVDAG_HD bool slot_used(uint32_t layout, const uint32_t* s, uint32_t slot)
 // stored item (out is then zeroed).
 SVDAG_HD bool read(const AltTable& t, uint32_t h, uint32_t* out)
 {
+    if (t.layout == kIndividualChaining) {
+        const bool ok = h < t.slabCount && h < ld_relaxed(&t.ctl[kCtlNextSlab]);
+        for (uint32_t i = 0; i < t.k; ++i)
+            out[i] = ok ? slab_at(t, h)[i] : 0u;
+        return ok;
+    }
     const uint32_t slab = h >> 5, slot = h & 31u, k = t.k;
     const bool ok = h != kInvalid && slab < t.slabCount && slot_ok(t.layout, slot) && slot_used(t.layout, slab_at(t, slab), slot);
     if (!ok) {

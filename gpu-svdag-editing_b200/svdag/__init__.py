@@ -685,12 +685,12 @@ class HashTable:
             self.h = None
 
 
-TABLE_LAYOUT_TICKET_BOARD, TABLE_LAYOUT_ATOMIC64, TABLE_LAYOUT_ACCELERATION = 1, 2, 3
+TABLE_LAYOUT_TICKET_BOARD, TABLE_LAYOUT_ATOMIC64, TABLE_LAYOUT_ACCELERATION, TABLE_LAYOUT_INDIVIDUAL_CHAINING = 1, 2, 3, 4
 
 
 class AltHashTable:
-    """A table of fixed-size items in one of the reference's alternative slab layouts
-    (TicketBoardHashTable, Atomic64HashTable, AccelerationHashTable), on the GPU of `dag`, in an
+    """A table of fixed-size items in one of the reference's alternative layouts (TicketBoardHashTable,
+    Atomic64HashTable, AccelerationHashTable, IndividualChainingHashTable), on the GPU of `dag`, in an
     allocation of its own. Keys are `item_words` words back to back; add stores every key in a
     fresh slot, duplicates included; adds and finds must not overlap in time."""
 
@@ -736,7 +736,7 @@ class AltTuning(C.Structure):
     _fields_ = [("layout", _U32), ("lanes", _U32), ("add_ms", C.c_float), ("find_ms", C.c_float)]
 
 
-ALT_TUNING_CANDIDATES = 6
+ALT_TUNING_CANDIDATES = 7
 
 
 def alt_table_tune(dag: MyGPUHashDAG, keys, count: int, item_words: int, items_per_bucket: int = 0, stream=None):
@@ -759,6 +759,10 @@ def Atomic64HashTable(dag, numBuckets, numReservedElements, itemSizeInU32):
 
 def AccelerationHashTable(dag, numBuckets, numReservedElements, itemSizeInU32):
     return AltHashTable.allocate(dag, TABLE_LAYOUT_ACCELERATION, numBuckets, numReservedElements, itemSizeInU32)
+
+
+def IndividualChainingHashTable(dag, numBuckets, numReservedElements, itemSizeInU32):
+    return AltHashTable.allocate(dag, TABLE_LAYOUT_INDIVIDUAL_CHAINING, numBuckets, numReservedElements, itemSizeInU32)
 
 
 class MyGPUHashDAGUndoRedo:

@@ -343,15 +343,20 @@ svdag_status svdag_table_get_stats(svdag_table* table, svdag_table_stats* out, v
  * (TicketBoardHashTable, ticket_board_hash_table.h:10-347). ATOMIC64: 31 slots, each claimed by a
  * 64-bit CAS of its item's first 8 bytes, which makes items with two zero first words unstorable
  * (Atomic64HashTable, atomic64_hash_table.h:11-414). ACCELERATION: 31 slots with a 32-bit tag each,
- * claimed by CAS (AccelerationHashTable, acceleration_hash_table.h:17-491). */
+ * claimed by CAS (AccelerationHashTable, acceleration_hash_table.h:17-491). INDIVIDUAL_CHAINING: no
+ * slabs; a node per item pushed onto its bucket's list by CAS, found by walking the list
+ * (IndividualChainingHashTable, individual_chaining_hash_table.h:181-336); it has no warp form, so
+ * lanes 32 runs a thread per key too, and a find returns the most recently added copy. */
 #define SVDAG_TABLE_LAYOUT_TICKET_BOARD 1u
 #define SVDAG_TABLE_LAYOUT_ATOMIC64 2u
 #define SVDAG_TABLE_LAYOUT_ACCELERATION 3u
+#define SVDAG_TABLE_LAYOUT_INDIVIDUAL_CHAINING 4u
 typedef struct svdag_alt_table svdag_alt_table;
 /* Table::allocate(numBuckets, numReservedElements, itemSizeInU32) (gpu_hash_table_base.h,
  * ticket_board_hash_table.h:19): one device allocation on the context's GPU holding num_buckets
- * first slabs and overflow slabs for reserved_items more items. item_words 1..32 (2..32 for
- * ATOMIC64). More than 2^27 slabs in all gives SVDAG_ERR_INVALID. */
+ * first slabs and overflow slabs for reserved_items more items (INDIVIDUAL_CHAINING: num_buckets
+ * heads and reserved_items nodes). item_words 1..32 (2..32 for ATOMIC64). More than 2^27 slabs or
+ * 2^30 nodes gives SVDAG_ERR_INVALID. */
 svdag_status svdag_alt_table_create(svdag_ctx* ctx, uint32_t layout, uint32_t item_words, uint32_t num_buckets,
     uint64_t reserved_items, svdag_alt_table** out_table);
 svdag_status svdag_alt_table_destroy(svdag_alt_table* table);
@@ -383,10 +388,10 @@ typedef struct svdag_alt_tuning {
     float add_ms; /* bulk add of the sample into a fresh table; < 0: the layout cannot hold the sample */
     float find_ms; /* find of every sample key afterwards */
 } svdag_alt_tuning;
-#define SVDAG_ALT_TUNING_CANDIDATES 6u
+#define SVDAG_ALT_TUNING_CANDIDATES 7u
 /* Measured choice among the alternative layouts for fixed-size items, with no counterpart in the
- * reference (which compares them offline, extras/hashmap_bench). For each layout and launch form
- * (lanes 1 and 32) a fresh table of count / items_per_bucket + 1 buckets (items_per_bucket 0 = 64)
+ * reference (which compares them offline, extras/hashmap_bench). For each slab layout and launch form
+ * (lanes 1 and 32) and for INDIVIDUAL_CHAINING (lanes 1) a fresh table of count / items_per_bucket + 1 buckets (items_per_bucket 0 = 64)
  * is filled with the count keys of keys_dev and searched for all of them, timed with CUDA events on
  * `stream`. *best receives the candidate with the least add + find time; all[] (NULL, or room for
  * SVDAG_ALT_TUNING_CANDIDATES) every candidate. Synchronous; the tables are freed again. */

@@ -167,25 +167,17 @@ void* alt_host_create(uint32_t layout, uint32_t k, uint32_t numBuckets, uint64_t
 {
     if (!layout_ok(layout, k) || numBuckets == 0)
         return nullptr;
-    const uint32_t slabs = arena_slabs(layout, numBuckets, reserved);
-    if (!slabs)
+    const uint64_t bytes = table_layout(layout, k, numBuckets, reserved, nullptr, nullptr);
+    if (!bytes)
         return nullptr;
-    const uint32_t sw = slab_words(layout, k);
-    const size_t bytes = 256 + (size_t)slabs * sw * 4;
-    void* mem = std::aligned_alloc(256, (bytes + 255) & ~(size_t)255);
+    void* mem = std::aligned_alloc(256, (bytes + 255) & ~(uint64_t)255);
     if (!mem)
         return nullptr;
     std::memset(mem, 0, bytes);
     auto* h = new HostTable();
     h->mem = mem;
-    h->t.layout = layout;
-    h->t.k = k;
-    h->t.numBuckets = numBuckets;
-    h->t.slabWords = sw;
-    h->t.slabCount = slabs;
-    h->t.ctl = (uint32_t*)mem;
-    h->t.slabs = (uint32_t*)((char*)mem + 256);
-    h->t.ctl[kCtlNextSlab] = numBuckets;
+    table_layout(layout, k, numBuckets, reserved, mem, &h->t);
+    h->t.ctl[kCtlNextSlab] = initial_counter(layout, numBuckets);
     return h;
 }
 
@@ -227,10 +219,26 @@ void alt_host_warp_op(void* p, const uint32_t* keys, uint32_t n, uint32_t* handl
 
 uint32_t alt_host_status(void* p) { return ((HostTable*)p)->t.ctl[kCtlStatus]; }
 
-// Occupied slots over the slabs taken so far, and the overflow slabs taken.
+// Nodes reachable from the IndividualChaining heads.
+static uint64_t chain_nodes(const AltTable& t)
+{
+    uint64_t n = 0;
+    for (uint32_t b = 0; b < t.numBuckets; ++b)
+        for (uint32_t cur = t.heads[b]; cur != 0 && cur <= t.slabCount; cur = slab_at(t, cur - 1u)[t.k])
+            ++n;
+    return n;
+}
+
+// Occupied slots over the slabs taken so far, and the overflow slabs taken (IndividualChaining:
+// linked nodes, and 0).
 void alt_host_stats(void* p, uint64_t* items, uint64_t* overflow)
 {
     const AltTable t = ((HostTable*)p)->t;
+    if (t.layout == kIndividualChaining) {
+        *items = chain_nodes(t);
+        *overflow = 0;
+        return;
+    }
     const uint32_t used = t.ctl[kCtlNextSlab] < t.slabCount ? t.ctl[kCtlNextSlab] : t.slabCount;
     uint64_t n = 0;
     for (uint32_t s = 0; s < used; ++s)
@@ -243,6 +251,8 @@ void alt_host_stats(void* p, uint64_t* items, uint64_t* overflow)
 uint64_t alt_host_linked_overflow(void* p)
 {
     const AltTable t = ((HostTable*)p)->t;
+    if (t.layout == kIndividualChaining)
+        return 0;
     uint64_t n = 0;
     for (uint32_t b = 0; b < t.numBuckets; ++b)
         for (uint32_t s = slab_at(t, b)[next_word(t.layout)]; s != 0 && s < t.slabCount; s = slab_at(t, s)[next_word(t.layout)])

@@ -15,7 +15,7 @@ import numpy as np
 import pytest
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-TB, A64, ACC = 1, 2, 3
+TB, A64, ACC, IC = 1, 2, 3, 4
 INVALID = 0xFFFFFFFF
 ERR_INVALID, ERR_OOM = 1, 2
 
@@ -104,7 +104,7 @@ def unique_keys(rng, n, k, exclude=None):
 
 
 CASES = [(TB, 1), (TB, 2), (TB, 5), (TB, 32), (A64, 2), (A64, 3), (A64, 9), (A64, 32), (ACC, 1), (ACC, 2), (ACC, 7),
-         (ACC, 32)]
+         (ACC, 32), (IC, 1), (IC, 3), (IC, 32)]
 
 
 @pytest.mark.parametrize("buckets", [5, 300])
@@ -122,9 +122,12 @@ def test_add_find_read_set_semantics(host, layout, k, buckets):
         assert len(np.unique(h)) == 2 * n, "two adds got the same slot"
         assert np.array_equal(t.read(h), ins)
         items, overflow = t.stats()
-        slots = 32 if layout == TB else 31
-        assert items == 2 * n and overflow >= -(-2 * n // slots) - buckets
-        assert t.lib.alt_host_linked_overflow(t.h) == overflow  # no slab taken and left unlinked
+        if layout != IC:
+            slots = 32 if layout == TB else 31
+            assert items == 2 * n and overflow >= -(-2 * n // slots) - buckets
+            assert t.lib.alt_host_linked_overflow(t.h) == overflow  # no slab taken and left unlinked
+        else:
+            assert items == 2 * n and overflow == 0  # every node taken is linked
         absent = unique_keys(rng, n, k, exclude=keys)
         fh = t.find(np.concatenate([keys, absent]))
         assert np.all(fh[:n] != INVALID) and np.all(fh[n:] == INVALID)
@@ -134,7 +137,7 @@ def test_add_find_read_set_semantics(host, layout, k, buckets):
         t.free()
 
 
-@pytest.mark.parametrize("layout,k", [(TB, 3), (A64, 3), (ACC, 3)])
+@pytest.mark.parametrize("layout,k", [(TB, 3), (A64, 3), (ACC, 3), (IC, 3)])
 def test_exhausted_overflow_latches_oom(host, layout, k):
     rng = np.random.default_rng(7)
     keys = unique_keys(rng, 400, k)
@@ -143,8 +146,11 @@ def test_exhausted_overflow_latches_oom(host, layout, k):
         h = t.add(keys)
         assert t.status() == ERR_OOM
         ok = h != INVALID
-        slots = 32 if layout == TB else 31
-        assert ok.sum() == (1 + -(-64 // slots)) * slots  # every slot of those slabs, nothing beyond
+        if layout == IC:
+            assert ok.sum() == 64  # the reserved nodes, nothing beyond
+        else:
+            slots = 32 if layout == TB else 31
+            assert ok.sum() == (1 + -(-64 // slots)) * slots  # every slot of those slabs, nothing beyond
         assert np.array_equal(t.read(h[ok]), keys[ok])
         fh = t.find(keys)
         assert np.all((fh != INVALID) == ok)
@@ -163,13 +169,16 @@ def test_atomic64_rejects_items_with_zero_first_words(host):
         t.free()
 
 
-@pytest.mark.parametrize("layout", [TB, A64, ACC])
+@pytest.mark.parametrize("layout", [TB, A64, ACC, IC])
 def test_handles_that_name_no_item_read_as_zeros(host, layout):
     t = Table(host, layout, 4, 3, reserved=31)
     try:
         h = t.add(np.array([[9, 8, 7, 6]], np.uint32), threads=1)
         h0 = int(h[0])
-        bad = np.array([INVALID, h0 ^ 1, 3 * 32 + 5, 1 << 30, (h0 & 0xFFFFFFE0) | 31], np.uint32)
+        if layout == IC:  # node ids: the one node taken is 0
+            bad = np.array([INVALID, 1, 30, 31, 1 << 30], np.uint32)
+        else:
+            bad = np.array([INVALID, h0 ^ 1, 3 * 32 + 5, 1 << 30, (h0 & 0xFFFFFFE0) | 31], np.uint32)
         out = t.read(bad)
         assert np.all(out == 0)
         assert np.array_equal(t.read(h), [[9, 8, 7, 6]])
@@ -196,7 +205,7 @@ lib.alt_host_add.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c
 lib.alt_host_status.restype = C.c_uint32
 lib.alt_host_status.argtypes = [C.c_void_p]
 rng = np.random.default_rng(5)
-for layout in (1, 2, 3):
+for layout in (1, 2, 3, 4):
     keys = rng.integers(1, 1 << 32, (2000, 3), dtype=np.uint64).astype(np.uint32)
     t = lib.alt_host_create(layout, 3, 3, 4000)
     out = np.empty(2000, np.uint32)

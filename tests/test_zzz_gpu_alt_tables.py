@@ -11,7 +11,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-TB, A64, ACC = 1, 2, 3
+TB, A64, ACC, IC = 1, 2, 3, 4
 INVALID = 0xFFFFFFFF
 
 
@@ -48,7 +48,7 @@ def dag(svdag_lib):
 @pytest.mark.parametrize("lanes", [1, 32])
 @pytest.mark.parametrize("buckets", [7, 1000])
 @pytest.mark.parametrize("layout,k", [(TB, 1), (TB, 2), (TB, 5), (A64, 2), (A64, 3), (A64, 9), (ACC, 1), (ACC, 2),
-                                      (ACC, 7), (TB, 32), (A64, 32), (ACC, 32)])
+                                      (ACC, 7), (TB, 32), (A64, 32), (ACC, 32), (IC, 1), (IC, 3), (IC, 32)])
 def test_add_find_read(svdag_lib, dag, layout, k, buckets, lanes):
     import torch
 
@@ -68,6 +68,7 @@ def test_add_find_read(svdag_lib, dag, layout, k, buckets, lanes):
         assert np.array_equal(host(words), ins)
         st = t.stats()
         assert st.items == 2 * n and st.buckets == buckets
+        assert layout != IC or st.overflow_slabs == 0
         absent = unique_keys(rng, n, k, exclude=keys)
         q = np.concatenate([keys, absent])
         f = torch.empty(2 * n, dtype=torch.int32, device="cuda")
@@ -82,7 +83,7 @@ def test_add_find_read(svdag_lib, dag, layout, k, buckets, lanes):
 
 
 @pytest.mark.parametrize("lanes", [1, 32])
-@pytest.mark.parametrize("layout", [TB, A64, ACC])
+@pytest.mark.parametrize("layout", [TB, A64, ACC, IC])
 def test_exhausted_overflow_latches_oom(svdag_lib, dag, layout, lanes):
     import torch
 
@@ -96,8 +97,11 @@ def test_exhausted_overflow_latches_oom(svdag_lib, dag, layout, lanes):
             t.sync()
         assert e.value.status == 2  # SVDAG_ERR_OOM
         ok = host(h) != INVALID
-        slots = 32 if layout == TB else 31
-        assert ok.sum() == (1 + -(-64 // slots)) * slots
+        if layout == IC:
+            assert ok.sum() == 64
+        else:
+            slots = 32 if layout == TB else 31
+            assert ok.sum() == (1 + -(-64 // slots)) * slots
         f = torch.empty(2000, dtype=torch.int32, device="cuda")
         t.find(dev(keys), 2000, f, lanes=lanes)
         t.sync()
@@ -132,7 +136,7 @@ def test_hashmap_benchmark_shape(svdag_lib, dag):
     n0, n1, ns = 1 << 16, 1 << 13, 1 << 13
     allk = unique_keys(rng, n0 + n1 + ns, 2)
     init, more, never = allk[:n0], allk[n0:n0 + n1], allk[n0 + n1:]
-    for layout in (TB, A64, ACC):
+    for layout in (TB, A64, ACC, IC):
         t = svdag_lib.AltHashTable(dag, layout, 2, (n0 + n1) // 64 + 1, 2 * (n0 + n1))
         try:
             h = torch.empty(n0, dtype=torch.int32, device="cuda")
@@ -162,10 +166,10 @@ def test_tune_picks_the_fastest_measured_candidate(svdag_lib, dag, k):
     n = 1 << 15
     keys = unique_keys(rng, n, k)
     best, every = svdag_lib.alt_table_tune(dag, dev(keys), n, k)
-    assert [(c.layout, c.lanes) for c in every] == [(1, 1), (1, 32), (2, 1), (2, 32), (3, 1), (3, 32)]
+    assert [(c.layout, c.lanes) for c in every] == [(1, 1), (1, 32), (2, 1), (2, 32), (3, 1), (3, 32), (4, 1)]
     measured = [c for c in every if c.add_ms >= 0]
     # Atomic64 needs two words per item
-    assert len(measured) == (4 if k == 1 else 6)
+    assert len(measured) == (5 if k == 1 else 7)
     assert all(c.find_ms >= 0 for c in measured)
     assert min(c.add_ms + c.find_ms for c in measured) == best.add_ms + best.find_ms
     t = svdag_lib.AltHashTable(dag, best.layout, k, n // 64 + 1, 2 * n)
@@ -180,7 +184,7 @@ def test_tune_picks_the_fastest_measured_candidate(svdag_lib, dag, k):
 
 
 @pytest.mark.parametrize("add_lanes,find_lanes", [(1, 32), (32, 1)])
-@pytest.mark.parametrize("layout", [TB, A64, ACC])
+@pytest.mark.parametrize("layout", [TB, A64, ACC, IC])
 def test_launch_forms_interoperate(svdag_lib, dag, layout, add_lanes, find_lanes):
     """Keys added thread per key are found warp-hybrid and the other way round: both forms hash,
     place and compare alike."""
