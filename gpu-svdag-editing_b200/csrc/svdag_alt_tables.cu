@@ -96,6 +96,27 @@ __global__ void k_alt_read(AltTable t, const uint32_t* __restrict__ handles, uin
         read(t, handles[i], out + (uint64_t)i * t.k);
 }
 
+__global__ void k_alt_mark(AltTable t, const uint32_t* __restrict__ handles, uint32_t n)
+{
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        mark_active(t, handles[i]);
+}
+
+// freeInactiveItems: thread per slab (slab layouts) or per bucket list (IndividualChaining), the
+// freed count summed per warp into *count.
+__global__ void k_alt_free(AltTable t, uint32_t units, unsigned long long* count)
+{
+    unsigned long long n = 0;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < units; i += stride)
+        n += t.layout == kIndividualChaining ? free_inactive_chain(t, i) : free_inactive_slab(t, i);
+    for (int o = 16; o; o >>= 1)
+        n += __shfl_xor_sync(kFull, n, o);
+    if ((threadIdx.x & 31u) == 0 && n)
+        atomicAdd(count, n);
+}
+
 // Nodes reachable from the IndividualChaining heads (thread per bucket, walks bounded by the arena).
 __global__ void k_chain_count(AltTable t, unsigned long long* count)
 {
@@ -291,6 +312,51 @@ svdag_status svdag_alt_table_get_stats(svdag_alt_table* at, svdag_table_stats* o
     out->overflow_slabs = chain ? 0 : used - at->t.numBuckets;
     out->bytes = (chain ? ((unsigned long long)at->t.numBuckets * 4ull + 255ull) / 256ull * 256ull : 0ull)
         + (unsigned long long)used * at->t.slabWords * 4ull;
+    return svdag_alt_table_sync(at, stream);
+}
+
+svdag_status svdag_alt_table_clear_active(svdag_alt_table* at, void* stream)
+{
+    if (!at)
+        return SVDAG_ERR_INVALID;
+    cudaSetDevice(at->ctx->device);
+    SVDAG_CUDA(cudaMemsetAsync(at->t.active, 0, (size_t)active_words(at->t) * 4u, (cudaStream_t)stream));
+    return SVDAG_OK;
+}
+
+svdag_status svdag_alt_table_mark_active(svdag_alt_table* at, const uint32_t* handles, uint32_t n, void* stream)
+{
+    if (!at || (n && !handles))
+        return SVDAG_ERR_INVALID;
+    if (!n)
+        return SVDAG_OK;
+    cudaSetDevice(at->ctx->device);
+    k_alt_mark<<<grid_of(at, n), kThreads, 0, (cudaStream_t)stream>>>(at->t, handles, n);
+    SVDAG_CUDA(cudaGetLastError());
+    return SVDAG_OK;
+}
+
+svdag_status svdag_alt_table_free_inactive(svdag_alt_table* at, uint64_t* freed, void* stream)
+{
+    if (!at)
+        return SVDAG_ERR_INVALID;
+    cudaSetDevice(at->ctx->device);
+    const cudaStream_t s = (cudaStream_t)stream;
+    const bool chain = at->t.layout == kIndividualChaining;
+    uint32_t next = 0;
+    if (!chain) {
+        SVDAG_CUDA(cudaMemcpyAsync(&next, &at->t.ctl[kCtlNextSlab], sizeof(next), cudaMemcpyDeviceToHost, s));
+        SVDAG_CUDA(cudaStreamSynchronize(s));
+    }
+    const uint32_t units = chain ? at->t.numBuckets : std::min(next, at->t.slabCount);
+    SVDAG_CUDA(cudaMemsetAsync(at->countDev, 0, sizeof(unsigned long long), s));
+    k_alt_free<<<grid_of(at, units), kThreads, 0, s>>>(at->t, units, at->countDev);
+    SVDAG_CUDA(cudaGetLastError());
+    unsigned long long n = 0;
+    SVDAG_CUDA(cudaMemcpyAsync(&n, at->countDev, sizeof(n), cudaMemcpyDeviceToHost, s));
+    SVDAG_CUDA(cudaStreamSynchronize(s));
+    if (freed)
+        *freed = n;
     return svdag_alt_table_sync(at, stream);
 }
 

@@ -60,6 +60,7 @@ struct AltTable {
     uint32_t* slabs; // the arena (IndividualChaining: the nodes)
     uint32_t* ctl;
     uint32_t* heads; // IndividualChaining: first node id + 1 of each bucket (0 = empty); else null
+    uint32_t* active; // garbage-collection flags: bit (h & 31) of word (h >> 5) for handle h
 };
 
 SVDAG_HD uint32_t round8(uint32_t w) { return (w + 7u) & ~7u; }
@@ -82,9 +83,13 @@ inline uint32_t arena_slabs(uint32_t layout, uint32_t numBuckets, uint64_t reser
     const uint64_t slabs = (uint64_t)numBuckets + overflow;
     return slabs > kMaxSlabs ? 0u : (uint32_t)slabs;
 }
+// Words of a table's active-flag bitmap: one per slab, or one per 32 nodes.
+SVDAG_HD uint32_t active_words(const AltTable& t) { return t.layout == kIndividualChaining ? (t.slabCount + 31u) / 32u : t.slabCount; }
+
 // Bytes of a table's single allocation, 0 when the sizes exceed the handle space. With `base` set,
 // *t becomes the descriptor of a table in that allocation: a 256-byte control block, then the
-// IndividualChaining heads (rounded to 256 bytes), then the arena.
+// IndividualChaining heads (rounded to 256 bytes), the arena (rounded to 256 bytes) and the
+// active-flag bitmap.
 inline uint64_t table_layout(uint32_t layout, uint32_t k, uint32_t numBuckets, uint64_t reserved, void* base, AltTable* t)
 {
     AltTable d {};
@@ -105,13 +110,16 @@ inline uint64_t table_layout(uint32_t layout, uint32_t k, uint32_t numBuckets, u
         d.slabWords = slab_words(layout, k);
     }
     d.slabCount = (uint32_t)count;
+    const uint64_t arenaBytes = (count * d.slabWords * 4ull + 255u) & ~255ull;
+    const uint64_t activeBytes = active_words(d) * 4ull;
     if (base) {
         d.ctl = (uint32_t*)base;
         d.heads = headBytes ? (uint32_t*)((char*)base + 256) : nullptr;
         d.slabs = (uint32_t*)((char*)base + 256 + headBytes);
+        d.active = (uint32_t*)((char*)base + 256 + headBytes + arenaBytes);
         *t = d;
     }
-    return 256 + headBytes + count * d.slabWords * 4ull;
+    return 256 + headBytes + arenaBytes + activeBytes;
 }
 // Initial value of the control block's bump counter: overflow slabs follow the bucket slabs; nodes
 // start at 0.
@@ -142,6 +150,7 @@ __device__ __forceinline__ uint32_t or32(uint32_t* p, uint32_t v) { return atomi
 __device__ __forceinline__ uint32_t add32(uint32_t* p, uint32_t v) { return atomicAdd(p, v); }
 __device__ __forceinline__ uint32_t exch32(uint32_t* p, uint32_t v) { return atomicExch(p, v); }
 __device__ __forceinline__ uint32_t ctz32(uint32_t v) { return __ffs(v) - 1u; }
+__device__ __forceinline__ uint32_t popc32(uint32_t v) { return __popc(v); }
 #else
 inline uint32_t ld_relaxed(const uint32_t* p) { return __atomic_load_n(p, __ATOMIC_RELAXED); }
 inline uint64_t ld_relaxed64(const uint64_t* p) { return __atomic_load_n(p, __ATOMIC_RELAXED); }
@@ -159,6 +168,7 @@ inline uint32_t or32(uint32_t* p, uint32_t v) { return __atomic_fetch_or(p, v, _
 inline uint32_t add32(uint32_t* p, uint32_t v) { return __atomic_fetch_add(p, v, __ATOMIC_ACQ_REL); }
 inline uint32_t exch32(uint32_t* p, uint32_t v) { return __atomic_exchange_n(p, v, __ATOMIC_ACQ_REL); }
 inline uint32_t ctz32(uint32_t v) { return (uint32_t)__builtin_ctz(v); }
+inline uint32_t popc32(uint32_t v) { return (uint32_t)__builtin_popcount(v); }
 #endif
 
 SVDAG_HD void set_status(const AltTable& t, uint32_t st) { cas32(&t.ctl[kCtlStatus], 0u, st); }
@@ -441,6 +451,72 @@ SVDAG_HD uint32_t slab_items(uint32_t layout, const uint32_t* s)
     for (uint32_t slot = 0; slot < 32u; ++slot)
         n += slot_ok(layout, slot) && slot_used(layout, s, slot);
     return n;
+}
+
+// ---------------------------------------------------------------- garbage collection
+//
+// clearActiveFlags / markAsActive / freeInactiveItems (gpu_hash_table_base.h:102-112,
+// gpu_hash_table_base.cu:231-330): the caller clears the flags, marks the handles it keeps, and the
+// table frees every stored item left unmarked. A freed slot is free for later adds; the reference
+// also unlinks overflow slabs left empty and returns them to its allocator, which this bump
+// allocator has no use for: they stay linked and their slots are reused in place. Freed
+// IndividualChaining nodes are unlinked from their lists (the reference's node allocator does not
+// free either). These phases must not overlap adds or finds.
+
+// markAsActive: sets the flag of handle h (handles outside the table are ignored).
+SVDAG_HD void mark_active(const AltTable& t, uint32_t h)
+{
+    if (h != kInvalid && (h >> 5) < active_words(t))
+        or32(&t.active[h >> 5], 1u << (h & 31u));
+}
+
+// Frees the unmarked items of slab `slab` (a slab layout); returns how many.
+SVDAG_HD uint32_t free_inactive_slab(const AltTable& t, uint32_t slab)
+{
+    uint32_t* s = slab_at(t, slab);
+    const uint32_t act = t.active[slab];
+    if (t.layout == kTicketBoard) {
+        const uint32_t dead = s[0] & ~act;
+        s[0] &= ~dead;
+        return popc32(dead);
+    }
+    uint32_t freed = 0;
+    if (t.layout == kAtomic64) {
+        uint64_t* pre = (uint64_t*)s;
+        for (uint32_t slot = 0; slot < 31u; ++slot)
+            if (!((act >> slot) & 1u) && pre[slot] != 0) {
+                pre[slot] = 0;
+                ++freed;
+            }
+        return freed;
+    }
+    for (uint32_t slot = 1; slot < 32u; ++slot)
+        if (!((act >> slot) & 1u) && s[slot] != 0) {
+            s[slot] = 0;
+            ++freed;
+        }
+    return freed;
+}
+
+// Unlinks the unmarked nodes of bucket b's list (IndividualChaining); returns how many.
+SVDAG_HD uint32_t free_inactive_chain(const AltTable& t, uint32_t b)
+{
+    uint32_t* link = &t.heads[b];
+    uint32_t freed = 0;
+    for (uint32_t steps = 0; steps < t.slabCount; ++steps) {
+        const uint32_t cur = *link;
+        if (cur == 0 || cur > t.slabCount)
+            break;
+        const uint32_t id = cur - 1u;
+        uint32_t* node = slab_at(t, id);
+        if ((t.active[id >> 5] >> (id & 31u)) & 1u) {
+            link = &node[t.k];
+        } else {
+            *link = node[t.k];
+            ++freed;
+        }
+    }
+    return freed;
 }
 
 // ---------------------------------------------------------------- warp-hybrid forms

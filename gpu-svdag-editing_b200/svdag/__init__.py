@@ -211,6 +211,9 @@ _PROTOS = {
     "svdag_alt_table_sync": [_P, _P],
     "svdag_alt_table_get_stats": [_P, C.POINTER(TableStats), _P],
     "svdag_alt_table_tune": [_P, _P, _U32, _U32, _U32, _P, _P, _P],
+    "svdag_alt_table_clear_active": [_P, _P],
+    "svdag_alt_table_mark_active": [_P, _P, _U32, _P],
+    "svdag_alt_table_free_inactive": [_P, C.POINTER(_U64), _P],
     "svdag_get_stats": [_P, C.POINTER(Stats), _P],
     "svdag_export_level": [_P, _U32, _P, _P, _U64, C.POINTER(_U64), _P],
     "svdag_autotune": [_P, C.POINTER(Edit), _U32, _P, _P, _U32, _U64, _U32, C.POINTER(Tuning), _P],
@@ -725,6 +728,19 @@ class AltHashTable:
         s = TableStats()
         _check(lib().svdag_alt_table_get_stats(self.h, C.byref(s), stream_ptr(stream)), "svdag_alt_table_get_stats")
         return s
+
+    def clearActiveFlags(self, stream=None):
+        _check(lib().svdag_alt_table_clear_active(self.h, stream_ptr(stream)), "svdag_alt_table_clear_active")
+
+    def markAsActive(self, handles, count, stream=None):
+        _check(lib().svdag_alt_table_mark_active(self.h, ptr(handles), count, stream_ptr(stream)),
+               "svdag_alt_table_mark_active")
+
+    def freeInactiveItems(self, stream=None) -> int:
+        """Frees every stored item not marked since clearActiveFlags; returns how many."""
+        n = C.c_uint64()
+        _check(lib().svdag_alt_table_free_inactive(self.h, C.byref(n), stream_ptr(stream)), "svdag_alt_table_free_inactive")
+        return n.value
 
     def destroy(self):
         if self.h:

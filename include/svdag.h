@@ -381,6 +381,16 @@ svdag_status svdag_alt_table_sync(svdag_alt_table* table, void* stream);
  * svdag_alt_table_sync. */
 svdag_status svdag_alt_table_get_stats(svdag_alt_table* table, svdag_table_stats* out, void* stream);
 
+/* The table half of garbage collection: clearActiveFlags / markAsActive / freeInactiveItems
+ * (gpu_hash_table_base.h:102-112, gpu_hash_table_base.cu:231-330). Clear the flags, mark the handles
+ * to keep (handles that name nothing are ignored), then free every stored item left unmarked:
+ * *freed (may be NULL) receives how many. Kept items keep their handles; freed slots are reused by
+ * later adds (overflow slabs stay linked; IndividualChaining unlinks freed nodes). Must not overlap
+ * adds or finds. free_inactive is synchronous and returns like svdag_alt_table_sync. */
+svdag_status svdag_alt_table_clear_active(svdag_alt_table* table, void* stream);
+svdag_status svdag_alt_table_mark_active(svdag_alt_table* table, const uint32_t* handles_dev, uint32_t count, void* stream);
+svdag_status svdag_alt_table_free_inactive(svdag_alt_table* table, uint64_t* freed, void* stream);
+
 /* One measured candidate of svdag_alt_table_tune. */
 typedef struct svdag_alt_tuning {
     uint32_t layout; /* SVDAG_TABLE_LAYOUT_* */

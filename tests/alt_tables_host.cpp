@@ -217,6 +217,34 @@ void alt_host_warp_op(void* p, const uint32_t* keys, uint32_t n, uint32_t* handl
     }
 }
 
+void alt_host_clear_active(void* p)
+{
+    const AltTable& t = ((HostTable*)p)->t;
+    std::memset(t.active, 0, (size_t)active_words(t) * 4u);
+}
+
+void alt_host_mark_active(void* p, const uint32_t* handles, uint32_t n, uint32_t threads)
+{
+    const AltTable t = ((HostTable*)p)->t;
+    run_threads(n, threads, [&](uint32_t i) { mark_active(t, handles[i]); });
+}
+
+// freeInactiveItems over every slab taken (or every bucket list); returns the items freed.
+uint64_t alt_host_free_inactive(void* p)
+{
+    const AltTable& t = ((HostTable*)p)->t;
+    uint64_t n = 0;
+    if (t.layout == kIndividualChaining) {
+        for (uint32_t b = 0; b < t.numBuckets; ++b)
+            n += free_inactive_chain(t, b);
+    } else {
+        const uint32_t used = t.ctl[kCtlNextSlab] < t.slabCount ? t.ctl[kCtlNextSlab] : t.slabCount;
+        for (uint32_t s = 0; s < used; ++s)
+            n += free_inactive_slab(t, s);
+    }
+    return n;
+}
+
 uint32_t alt_host_status(void* p) { return ((HostTable*)p)->t.ctl[kCtlStatus]; }
 
 // Nodes reachable from the IndividualChaining heads.

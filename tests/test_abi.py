@@ -62,6 +62,9 @@ def test_invalid_arguments_are_rejected(svdag_lib):
     assert L.svdag_alt_table_get_stats(None, None, None) == 1
     assert L.svdag_alt_table_destroy(None) == 1
     assert L.svdag_alt_table_tune(None, None, 0, 2, 0, None, None, None) == 1
+    assert L.svdag_alt_table_clear_active(None, None) == 1
+    assert L.svdag_alt_table_mark_active(None, None, 0, None) == 1
+    assert L.svdag_alt_table_free_inactive(None, None, None) == 1
 
 
 def test_no_cpu_fallback_without_device(svdag_lib):

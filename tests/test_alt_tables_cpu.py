@@ -41,6 +41,10 @@ def _load(so):
     lib.alt_host_stats.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
     lib.alt_host_linked_overflow.restype = C.c_uint64
     lib.alt_host_linked_overflow.argtypes = [C.c_void_p]
+    lib.alt_host_clear_active.argtypes = [C.c_void_p]
+    lib.alt_host_mark_active.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32]
+    lib.alt_host_free_inactive.restype = C.c_uint64
+    lib.alt_host_free_inactive.argtypes = [C.c_void_p]
     return lib
 
 
@@ -156,6 +160,44 @@ def test_exhausted_overflow_latches_oom(host, layout, k):
         assert np.all((fh != INVALID) == ok)
     finally:
         t.free()
+
+
+@pytest.mark.parametrize("layout", [TB, A64, ACC, IC])
+def test_delete_frees_unmarked_items_and_keeps_handles(host, layout):
+    """The reference's "GPUHashTable Delete" case (hash_table_test.cpp:262-303): 1024 + 512 items
+    of 2 words in 64 buckets, the first 1024 marked active, freeInactiveItems frees exactly the 512
+    others; every kept item is found at its original handle, any other find decodes to its key. Ten
+    random item sets, as GENERATE(take(10, ...)) draws. Freed slots are then reused by new adds."""
+    rng = np.random.default_rng(400 + layout)
+    n_keep, n_drop = 1024, 512
+    for _ in range(10):
+        items = unique_keys(rng, n_keep + n_drop, 2)
+        t = Table(host, layout, 2, 64, reserved=2 * (n_keep + n_drop))
+        try:
+            h = t.add(items)
+            assert np.all(h != INVALID)
+            before = t.stats()[0]
+            t.lib.alt_host_clear_active(t.h)
+            keep = np.ascontiguousarray(h[:n_keep])
+            t.lib.alt_host_mark_active(t.h, keep.ctypes.data, n_keep, 8)
+            assert t.lib.alt_host_free_inactive(t.h) == n_drop
+            assert t.stats()[0] == before - n_drop
+            f = t.find(items)
+            assert np.array_equal(f[:n_keep], h[:n_keep])
+            found = f != INVALID
+            assert np.array_equal(t.read(f[found]), items[found])
+            assert not found[n_keep:].any()  # distinct random items: the freed ones are gone
+            # adding the freed items again fills exactly the slots they left (same buckets), so the
+            # slab layouts need no new slab; IndividualChaining takes fresh nodes. All are found.
+            again = np.ascontiguousarray(items[n_keep:])
+            taken = t.lib.alt_host_linked_overflow(t.h)
+            g = t.add(again)
+            assert np.all(g != INVALID) and t.status() == 0
+            if layout != IC:
+                assert t.lib.alt_host_linked_overflow(t.h) == taken
+            assert np.array_equal(t.find(again), g) and np.array_equal(t.find(items[:n_keep]), h[:n_keep])
+        finally:
+            t.free()
 
 
 def test_atomic64_rejects_items_with_zero_first_words(host):

@@ -204,3 +204,39 @@ def test_launch_forms_interoperate(svdag_lib, dag, layout, add_lanes, find_lanes
         assert np.array_equal(host(f)[:n], host(h)) and np.all(host(f)[n:] == INVALID)
     finally:
         t.destroy()
+
+
+@pytest.mark.parametrize("layout", [TB, A64, ACC, IC])
+def test_delete_frees_unmarked_items_and_keeps_handles(svdag_lib, dag, layout):
+    """The reference's "GPUHashTable Delete GPU" case (hash_table_test.cpp:306-346): 1024 + 512
+    items of 2 words added warp-hybrid into 64 buckets, the first 1024 marked active on the GPU,
+    freeInactiveItems frees the other 512; kept items are found at their handles, freed ones not at
+    all, and adding the freed items again fits them into the slots they left."""
+    import torch
+
+    rng = np.random.default_rng(500 + layout)
+    n_keep, n_drop = 1024, 512
+    for _ in range(10):
+        items = unique_keys(rng, n_keep + n_drop, 2)
+        t = svdag_lib.AltHashTable(dag, layout, 2, 64, 2 * (n_keep + n_drop))
+        try:
+            h = torch.empty(n_keep + n_drop, dtype=torch.int32, device="cuda")
+            t.add(dev(items), n_keep + n_drop, h, lanes=32)
+            t.clearActiveFlags()
+            t.markAsActive(h[:n_keep], n_keep)
+            assert t.freeInactiveItems() == n_drop
+            assert t.stats().items == n_keep
+            f = torch.empty(n_keep + n_drop, dtype=torch.int32, device="cuda")
+            t.find(dev(items), n_keep + n_drop, f)
+            t.sync()
+            hf = host(f)
+            assert np.array_equal(hf[:n_keep], host(h)[:n_keep]) and np.all(hf[n_keep:] == INVALID)
+            slabs = t.stats().overflow_slabs
+            g = torch.empty(n_drop, dtype=torch.int32, device="cuda")
+            t.add(dev(items[n_keep:]), n_drop, g)
+            t.find(dev(items), n_keep + n_drop, f)
+            t.sync()
+            assert np.all(host(f) != INVALID) and np.array_equal(host(f)[n_keep:], host(g))
+            assert t.stats().items == n_keep + n_drop and t.stats().overflow_slabs == slabs
+        finally:
+            t.destroy()
