@@ -1,14 +1,16 @@
-// svdag_alt_tables.cuh - the reference's alternative slab layouts for fixed-size items, as tables of
-// their own: TicketBoard (ticket_board_hash_table.h), Atomic64 (atomic64_hash_table.h) and
-// Acceleration (acceleration_hash_table.h). The compact 8-bit-tag layout is the level tables'
-// (svdag_device.cuh). These serve the fixed-size hashmap workload of the reference's table
-// benchmark (extras/hashmap_bench/src/main.cu) so the layouts can be measured against each other.
+// svdag_alt_tables.cuh - the reference's alternative table layouts for fixed-size items, as tables
+// of their own: TicketBoard (ticket_board_hash_table.h), Atomic64 (atomic64_hash_table.h),
+// Acceleration (acceleration_hash_table.h) and IndividualChaining (individual_chaining_hash_table.h).
+// The compact 8-bit-tag layout is the level tables' (svdag_device.cuh). These serve the fixed-size
+// hashmap workload of the reference's table benchmark (extras/hashmap_bench/src/main.cu) so the
+// layouts can be measured against each other.
 //
 // One table is one device allocation: a control block and an arena of equal-sized slabs. Slabs
 // 0..numBuckets-1 are the buckets' first slabs; overflow slabs are taken from a bump counter and
-// linked at the tail of a chain. The arena is zeroed when the table is created and slabs are never
-// reused, so a fresh slab needs no initialisation and a next word of 0 ends a chain (no overflow
-// slab has id 0; kLinkBusy marks a link being made). A handle is slab * 32 + slot.
+// linked at the tail of a chain. The arena is zeroed when the table is created and a slab is never
+// given back to the counter (slots freed by garbage collection are reused in place), so a fresh
+// slab needs no initialisation and a next word of 0 ends a chain (no overflow slab has id 0;
+// kLinkBusy marks a link being made). A handle is slab * 32 + slot.
 //
 // Slab layouts (32-bit words; a slab's stride is rounded up to 8 words, 32 bytes):
 //   TicketBoard : [0] occupied-slot mask, [1] next, [2..7] unused, items of slots 0..31 from word 8.
