@@ -513,7 +513,7 @@ svdag_status svdag_set_tuning(svdag_ctx* ctx, const svdag_tuning* tuning);
 typedef struct svdag_server_config {
     uint32_t max_batch; /* edits per launch; 0 = 256 */
     uint32_t max_inflight; /* launches queued on the GPU; 0 = 2 */
-    uint64_t memory_cap_bytes; /* item-region budget for admission; 0 = the whole item region */
+    uint64_t memory_cap_bytes; /* item-region bytes that admitted edits may fill; 0 = the whole item region */
     svdag_trace_params frame; /* camera and resolution of the frames rendered after each launch */
     uint32_t flags; /* SVDAG_SERVE_* */
     uint32_t reserved;
