@@ -392,6 +392,16 @@ svdag_status svdag_alt_table_tune(svdag_ctx* ctx, const uint32_t* keys, uint32_t
         r.add_ms = r.find_ms = -1.0f;
         if (!layout_ok(r.layout, itemWords))
             continue;
+        { // untimed warm-up on a small table: a kernel's first launch also loads it (lazy module loading)
+            svdag_alt_table* w = nullptr;
+            const uint32_t wn = std::min(n, 1024u);
+            if (svdag_alt_table_create(ctx, r.layout, itemWords, 64, 2ull * wn, &w) == SVDAG_OK) {
+                svdag_alt_table_add(w, keys, wn, handles, r.lanes, stream);
+                svdag_alt_table_find(w, keys, wn, handles, r.lanes, stream);
+                svdag_alt_table_sync(w, stream); // a latched error here shows again in the timed run
+                svdag_alt_table_destroy(w);
+            }
+        }
         svdag_alt_table* t = nullptr;
         const svdag_status cs = svdag_alt_table_create(ctx, r.layout, itemWords, buckets, 2ull * n, &t);
         if (cs == SVDAG_ERR_OOM)
