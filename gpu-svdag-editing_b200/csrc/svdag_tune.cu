@@ -63,7 +63,28 @@ svdag_status tune_tables(svdag_ctx* ctx, const uint32_t* keys, const uint32_t* o
     Timer t0, t1;
     double best = 1e300;
     svdag_status st = SVDAG_OK;
+    // Untimed warm-up of each lane count's kernels on a small scratch table: a kernel's first launch
+    // also loads it (lazy module loading), which would count against the first load factor timed.
+    for (uint32_t lanes : { 1u, 2u, 4u, 8u }) {
+        uint32_t buckets[kNumClasses];
+        for (auto& b : buckets)
+            b = 1;
+        svdag_table t;
+        st = alloc_table(ctx, &t, kind, buckets, s);
+        if (st != SVDAG_OK)
+            break;
+        const uint32_t wn = std::min(n, 256u);
+        st = table_add_lanes(&t, keys, offsets, wn, totalWords, handles, lanes, s);
+        if (st == SVDAG_OK)
+            st = table_find_lanes(&t, keys, offsets, wn, totalWords, handles, lanes, s);
+        SVDAG_CUDA(cudaMemcpyAsync(&ctx->ctl->itemTop, tops, sizeof(tops), cudaMemcpyHostToDevice, s));
+        SVDAG_CUDA(cudaStreamSynchronize(s));
+        if (st != SVDAG_OK)
+            break;
+    }
     for (uint32_t lf : { 8u, 12u, 16u, 24u, 32u }) {
+        if (st != SVDAG_OK)
+            break;
         for (uint32_t lanes : { 1u, 2u, 4u, 8u }) {
             uint32_t buckets[kNumClasses];
             for (uint32_t c = 0; c < kNumClasses; ++c)
