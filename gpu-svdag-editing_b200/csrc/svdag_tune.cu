@@ -135,6 +135,9 @@ svdag_status tune_edits(svdag_ctx* ctx, const svdag_edit* edits, uint32_t n, svd
     double sum[kBuckets][2] = {}, cnt[kBuckets][2] = {};
     std::vector<Timer> timers(2 * (size_t)n);
     std::vector<int> bucketOf(2 * (size_t)n, -1), formOf(2 * (size_t)n, 0);
+    // The first launch of a tool in a form may capture and instantiate its graph or load the kernel:
+    // it is applied like the others but left out of the statistics (bucket -1).
+    bool seen[2][SVDAG_NUM_TOOLS] = {};
     size_t used = 0;
     for (uint32_t i = 0; i < n; ++i) {
         DevEditor eds[2];
@@ -149,18 +152,22 @@ svdag_status tune_edits(svdag_ctx* ctx, const svdag_edit* edits, uint32_t n, svd
             cudaEventRecord(t.a, s);
             SVDAG_TRY(form ? launch_single_fused(ctx, eds[j], s) : launch_pipeline(ctx, eds[j], s, nullptr, true));
             cudaEventRecord(t.b, s);
-            bucketOf[used] = b;
+            const uint32_t tool = eds[j].tool < SVDAG_NUM_TOOLS ? eds[j].tool : 0u;
+            bucketOf[used] = seen[form][tool] ? b : -1;
+            seen[form][tool] = true;
             formOf[used] = form;
             ++used;
         }
     }
     SVDAG_CUDA(cudaStreamSynchronize(s));
     for (size_t k = 0; k < used; ++k) {
+        ++out.trials;
+        if (bucketOf[k] < 0)
+            continue;
         float ms = 0;
         cudaEventElapsedTime(&ms, timers[k].a, timers[k].b);
         sum[bucketOf[k]][formOf[k]] += ms * 1e3;
         cnt[bucketOf[k]][formOf[k]] += 1;
-        ++out.trials;
     }
     // Persistent kernel for the buckets, from the smallest up, where it is faster.
     double threshold = 0;
