@@ -1,6 +1,7 @@
-// svdag_frames.h - host-side geometry of incremental served frames: the boxes holding every voxel an
-// edit can change, and the hit-buffer rectangle whose rays can meet such a box. Plain C++ (no CUDA),
-// so the tests compile the same functions for the host.
+// svdag_serve_geometry.h - host-side geometry of the serving loop: an edit's admission estimate (the
+// item-region bytes it can add), the boxes holding every voxel it can change, and the hit-buffer
+// rectangle whose rays can meet such a box. Plain C++ (no CUDA), so the tests compile the same
+// functions for the host.
 #pragma once
 #include <algorithm>
 #include <cmath>
@@ -9,7 +10,38 @@
 #include "../../include/svdag.h"
 
 namespace svdag {
-namespace frames {
+namespace serve {
+
+// Upper estimate of the item-region bytes an edit can add: its intermediate SVO bounds the new items.
+// Leaves: the footprint's bounding volume in 4^3 bricks, or for spheres and boxes whose volume is
+// large, a shell of three bricks' thickness around the surface (interior nodes are filled or emptied
+// whole). Nodes above the leaves add at most a seventh; each item takes at most 48 bytes with its
+// share of the slab header.
+inline unsigned long long edit_reserve_bytes(const svdag_edit& e, uint32_t levels)
+{
+    const double r = std::max(1.0, (double)e.radius);
+    const double side = 2.0 * r / 4.0 + 2.0; // bricks per axis
+    const double volume = side * side * side;
+    double leaves = volume;
+    switch (e.tool) {
+    case SVDAG_TOOL_SPHERE_ADD:
+    case SVDAG_TOOL_SPHERE_REMOVE:
+    case SVDAG_TOOL_SPHERE_PAINT:
+        leaves = std::min(volume, 3.0 * 4.0 * M_PI * (r / 4.0 + 1.0) * (r / 4.0 + 1.0));
+        break;
+    case SVDAG_TOOL_BOX_ADD:
+    case SVDAG_TOOL_BOX_REMOVE:
+        leaves = std::min(volume, 3.0 * 6.0 * side * side);
+        break;
+    case SVDAG_TOOL_MOVE:
+        leaves = 2.0 * volume;
+        break;
+    default:
+        break;
+    }
+    const double items = leaves * 8.0 / 7.0 + 8.0 * levels;
+    return (unsigned long long)(items * 48.0);
+}
 
 // Hit-buffer rows [row0, row1] and columns [col0, col1] that rays meeting `box` can come from. Pixel (x, y) looks along
 // ray_min + x * ddx + y * ddy - camera, so a point P is seen at the (x, y) solving
@@ -80,5 +112,5 @@ inline uint32_t edit_boxes(const svdag_edit& e, float* out)
     }
 }
 
-} // namespace frames
+} // namespace serve
 } // namespace svdag

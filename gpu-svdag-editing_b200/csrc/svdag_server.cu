@@ -18,7 +18,7 @@
 #include <vector>
 
 #include "svdag_edit.cuh"
-#include "svdag_frames.h"
+#include "svdag_serve_geometry.h"
 #include "svdag_host.hpp"
 
 using namespace svdag;
@@ -49,44 +49,14 @@ struct Batch {
     bool finished = false;
 };
 
-// Upper estimate of the item-region bytes an edit can add: its intermediate SVO bounds the new items.
-// Leaves: the footprint's bounding volume in 4^3 bricks, or for spheres and boxes whose volume is
-// large, a shell of three bricks' thickness around the surface (interior nodes are filled or emptied
-// whole). Nodes above the leaves add at most a seventh; each item takes at most 48 bytes with its
-// share of the slab header.
-unsigned long long edit_reserve_bytes(const svdag_edit& e, uint32_t levels)
-{
-    const double r = std::max(1.0, (double)e.radius);
-    const double side = 2.0 * r / 4.0 + 2.0; // bricks per axis
-    const double volume = side * side * side;
-    double leaves = volume;
-    switch (e.tool) {
-    case SVDAG_TOOL_SPHERE_ADD:
-    case SVDAG_TOOL_SPHERE_REMOVE:
-    case SVDAG_TOOL_SPHERE_PAINT:
-        leaves = std::min(volume, 3.0 * 4.0 * M_PI * (r / 4.0 + 1.0) * (r / 4.0 + 1.0));
-        break;
-    case SVDAG_TOOL_BOX_ADD:
-    case SVDAG_TOOL_BOX_REMOVE:
-        leaves = std::min(volume, 3.0 * 6.0 * side * side);
-        break;
-    case SVDAG_TOOL_MOVE:
-        leaves = 2.0 * volume;
-        break;
-    default:
-        break;
-    }
-    const double items = leaves * 8.0 / 7.0 + 8.0 * levels;
-    return (unsigned long long)(items * 48.0);
-}
-
 double now_since(Clock::time_point t0) { return std::chrono::duration<double>(Clock::now() - t0).count(); }
 
 constexpr uint32_t kMaxFrameBoxes = 512; // changed regions one incremental frame tests; more: a whole frame
 constexpr uint32_t kMaxCopyRuns = 16; // row runs copied to the host after an incremental frame; more: the whole frame
 
-using frames::box_rows;
-using frames::edit_boxes;
+using serve::box_rows;
+using serve::edit_boxes;
+using serve::edit_reserve_bytes;
 
 } // namespace
 

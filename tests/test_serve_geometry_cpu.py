@@ -1,8 +1,9 @@
-"""The serving loop's incremental-frame geometry, compiled from its own header for the host
-(tests/frames_host.cpp over svdag_frames.h): edit_boxes gives exactly the boxes the CPU claim tests
-use (tests/test_incremental_frames_cpu.py, tests/test_edit_boxes_cpu.py check those boxes against the
-oracle), and box_rows' rectangle holds every hit-buffer pixel whose ray meets the box, so copying
-only those rows and columns of an incremental frame misses no changed pixel."""
+"""The serving loop's host geometry, compiled from its own header for the host
+(tests/serve_geometry_host.cpp over svdag_serve_geometry.h): the admission estimate bounds the items
+an edit adds (checked against the oracle's counts); edit_boxes gives exactly the boxes the CPU claim
+tests use (tests/test_incremental_frames_cpu.py, tests/test_edit_boxes_cpu.py check those boxes
+against the oracle); box_rows' rectangle holds every hit-buffer pixel whose ray meets the box, so
+copying only those rows and columns of an incremental frame misses no changed pixel."""
 import ctypes as C
 import os
 import shutil
@@ -20,13 +21,15 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 def frames(tmp_path_factory):
     if shutil.which("g++") is None:
         pytest.skip("no host C++ compiler")
-    so = str(tmp_path_factory.mktemp("frames") / "frames_host.so")
-    subprocess.check_call(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", os.path.join(HERE, "frames_host.cpp"), "-o", so])
+    so = str(tmp_path_factory.mktemp("frames") / "serve_geometry_host.so")
+    subprocess.check_call(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", os.path.join(HERE, "serve_geometry_host.cpp"), "-o", so])
     lib = C.CDLL(so)
     lib.frames_edit_boxes.restype = C.c_uint32
     lib.frames_edit_boxes.argtypes = [C.c_void_p, C.c_void_p]
     lib.frames_box_rows.restype = C.c_int
     lib.frames_box_rows.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.frames_edit_reserve_bytes.restype = C.c_ulonglong
+    lib.frames_edit_reserve_bytes.argtypes = [C.c_void_p, C.c_uint32]
     return lib
 
 
@@ -77,3 +80,40 @@ def test_box_rows_hold_every_pixel_whose_ray_meets_the_box(svdag_lib, oracle_mod
         covered += int(hit.any())
         small += int((row1 - row0 + 1) * (col1 - col0 + 1) < p.width * p.height // 4)
     assert covered > 50 and small > 50  # the rectangles do cut the copy down
+
+
+@pytest.mark.parametrize("tool", range(9))
+def test_admission_estimate_bounds_the_new_items(svdag_lib, oracle_mod, frames, tool):
+    """edit_reserve_bytes (what the server reserves before admitting an edit) is at least 48 bytes
+    per item the edit adds, for edits of every tool and radii from 1 to 120 voxels near the surface
+    of a depth-10 terrain, one after another (the oracle's new-item counts)."""
+    levels = 10
+    terrain = dict(seed=7, octaves=5, num_materials=8, min_height_pct=35, max_height_pct=65)
+    L = oracle_mod.lib()
+    o = oracle_mod.OracleDag(levels)
+    o.build_terrain(oracle_mod.TerrainParams(**terrain))
+    rng = np.random.default_rng(900 + tool)
+    g = 1 << levels
+    tight = 0.0
+    for _ in range(14):
+        x, z = (int(v) for v in rng.integers(130, g - 130, 2))
+        h = L.oracle_terrain_height(oracle_mod.TerrainParams(**terrain), levels, x, z)
+        e = oracle_mod.Edit(tool=tool, material=int(rng.integers(0, 16)))
+        e.radius = float(np.exp(rng.uniform(0, np.log(120))))
+        e.center[:] = [float(x), float(h + rng.integers(-8, 9)), float(z)]
+        if tool in (5, 7):
+            e.src[:] = list(e.center)
+            e.dst[:] = [e.center[0] + float(rng.integers(-100, 101)), e.center[1] + float(rng.integers(-20, 21)),
+                        e.center[2] + float(rng.integers(-100, 101))]
+        if tool == 6:
+            e.noise_seed, e.noise_cell_log2 = int(rng.integers(1, 99)), int(rng.integers(0, 4))
+        if tool == 8:
+            e.noise_seed = int(rng.integers(12, 22))
+        se = svdag_lib.Edit()
+        C.memmove(C.addressof(se), C.addressof(e), C.sizeof(se))
+        reserve = frames.frames_edit_reserve_bytes(C.addressof(se), levels)
+        st = o.edit(e)
+        assert st.status == 0
+        assert 48 * st.new_items <= reserve, (tool, e.radius, st.new_items, reserve)
+        tight = max(tight, 48 * st.new_items / reserve)
+    assert tight > 0.0  # the edits did add items
