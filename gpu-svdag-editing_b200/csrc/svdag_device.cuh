@@ -136,13 +136,7 @@ __device__ __forceinline__ uint32_t* handle_ptr(const DevDag& d, uint32_t h) { r
 
 __device__ __forceinline__ uint32_t bucket_of(uint32_t ha, uint32_t numBuckets) { return __umulhi(ha, numBuckets); }
 
-// Key length from the first words (my_gpu_base_dag.h:195-203).
-__host__ __device__ __forceinline__ uint32_t node_words(uint32_t header) { return 1u + __builtin_popcount(header & 0xFFu); }
-__host__ __device__ __forceinline__ uint32_t leaf_words(uint32_t lo, uint32_t hi)
-{
-    const uint32_t v = __builtin_popcount(lo) + __builtin_popcount(hi);
-    return 2u + ((v * 4u + 31u) >> 5);
-}
+// Key length from the first words: node_words / leaf_words in svdag_hash.h.
 __device__ __forceinline__ uint32_t dev_node_words(uint32_t header) { return 1u + __popc(header & 0xFFu); }
 __device__ __forceinline__ uint32_t dev_leaf_words(uint32_t lo, uint32_t hi) { return 2u + (((__popc(lo) + __popc(hi)) * 4u + 31u) >> 5); }
 

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "svdag_device.cuh"
+#include "svdag_snapshot.h"
 #include "svdag_host.hpp"
 
 using namespace svdag;
@@ -26,37 +27,8 @@ namespace {
 
 uint32_t host_popc(uint32_t v) { return (uint32_t)__builtin_popcount(v); }
 
-// Words of the item starting at p (avail words readable), or 0 when it does not fit or is invalid.
-uint32_t item_words(bool leaf, const uint32_t* p, uint64_t avail)
-{
-    if (avail < 2)
-        return 0;
-    const uint32_t n = leaf ? leaf_words(p[0], p[1]) : node_words(p[0]);
-    if (leaf ? (p[0] == 0 && p[1] == 0) : (p[0] & 0xFFu) == 0)
-        return 0; // an empty item never occurs in a DAG
-    return n <= avail ? n : 0;
-}
-
-// Offsets of the items of one level of a snapshot; false when the words do not split into exactly
-// `count` items or a child ordinal is out of range.
-bool split_level(bool leaf, const uint32_t* w, uint64_t nWords, uint64_t count, uint64_t childCount, std::vector<uint64_t>& offs)
-{
-    offs.clear();
-    offs.reserve(count);
-    uint64_t at = 0;
-    while (at < nWords) {
-        const uint32_t n = item_words(leaf, w + at, nWords - at);
-        if (!n)
-            return false;
-        if (!leaf)
-            for (uint32_t i = 1; i < n; ++i)
-                if (w[at + i] >= childCount)
-                    return false;
-        offs.push_back(at);
-        at += n;
-    }
-    return offs.size() == count;
-}
+using snapshot::item_words;
+using snapshot::split_level;
 
 struct KeyRef {
     const std::vector<uint32_t>* words;
