@@ -260,8 +260,9 @@ def max_over_ranks(values, dist=None, device="cuda"):
     return [float(x) for x in t.cpu()]
 
 
-def summarize(res, n_edits):
-    """Latency (ms) and throughput of a replay; res = edits then frames."""
+def summarize(res, n_edits, duration_s=None):
+    """Latency (ms) and throughput of a replay; res = edits then frames. `sustained`: the last edit
+    became visible within 10 % (+0.25 s) of the end of the stream, so no backlog built up."""
     ed = res[:n_edits]
     lat = (ed["visible_s"] - ed["submit_s"]) * 1e3
     fr = res[n_edits:]
@@ -269,19 +270,35 @@ def summarize(res, n_edits):
     span = float(res["visible_s"].max() - res["submit_s"].min()) if len(res) else 0.0
     vox = float(ed["edited_voxels"].sum())
     launches = len(set(res["launch"].tolist()))
-    return {"edits": int(n_edits), "ok": int((ed["status"] == 0).sum()), "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99),
-            "max_ms": float(lat.max()) if len(lat) else None, "frame_p99_ms": pct(flat, 99),
-            "edited_mvox_s": vox / span / 1e6 if span > 0 else None, "launches": launches,
-            "mean_edits_per_launch": float(n_edits) / max(1, len(set(ed["launch"].tolist()))), "span_s": span}
+    out = {"edits": int(n_edits), "ok": int((ed["status"] == 0).sum()), "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99),
+           "max_ms": float(lat.max()) if len(lat) else None, "frame_p99_ms": pct(flat, 99),
+           "edited_mvox_s": vox / span / 1e6 if span > 0 else None, "launches": launches,
+           "mean_edits_per_launch": float(n_edits) / max(1, len(set(ed["launch"].tolist()))), "span_s": span}
+    if duration_s is not None:
+        out["sustained"] = bool(span <= 1.1 * duration_s + 0.25)
+    return out
 
 
-def replay(svdag, dag, cam, edits, times, frames, plain=False, copy_frames=False, counters=None):
-    """Serves a timed stream; `counters` (a dict) receives the server's frame counters."""
+def require_ok(res, n_edits, what):
+    """Every edit of a replay must have succeeded: a latency over failed edits measures nothing."""
+    st = res["status"][:n_edits]
+    bad = np.nonzero(st != 0)[0]
+    if len(bad):
+        i = int(bad[0])
+        raise SystemExit(f"bench: {what}: {len(bad)} of {n_edits} edits failed; first: edit {i} with status "
+                         f"{int(st[i])} (launch {int(res['launch'][i])})")
+
+
+def replay(svdag, dag, cam, edits, times, frames, plain=False, copy_frames=False, counters=None, memory=None):
+    """Serves a timed stream; `counters` and `memory` (dicts) receive the server's frame counters and
+    memory accounting (in-loop collections)."""
     with svdag.Server(dag, cam, max_batch=256, max_inflight=2, memory_cap_bytes=POOL_CAP, plain=plain,
                       copy_frames=copy_frames) as srv:
         res = srv.replay(edits, times, frames)
         if counters is not None:
             counters.update(srv.counters())
+        if memory is not None:
+            memory.update(srv.memory())
         return res
 
 
@@ -290,6 +307,31 @@ def edit_algorithmic_bytes(records):
     ones (44 + 44 bytes with its representative and handle), one table find per distinct item (a
     32-byte slab header and a 40-byte candidate), 40 bytes per inserted item."""
     return float(sum(r.svo_items * 88 + r.unique_items * 72 + r.new_items * 40 for r in records))
+
+
+def stream_of(w, levels, rate, duration, seed, height=None):
+    rmax = 2048.0 * (1 << levels) / 131072
+    return w.c4_stream(rate, duration, seed=seed, levels=levels, rmax=rmax, terrain=make_terrain(w, levels),
+                       copy_offset=int(1024 * (1 << levels) / 131072), height=height)
+
+
+def trace_rays_s(svdag, torch, dag, cam, frames=10):
+    """Whole 1920x1080 frames of the scene (CUDA events on the tracer's stream)."""
+    tracer = svdag.DAGTracer(cam.width, cam.height)
+    stream = torch.cuda.Stream()
+    for _ in range(3):
+        tracer.resolve_paths(cam, dag, stream=stream.cuda_stream)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(frames)]
+    torch.cuda.synchronize()
+    for a, b in ev:
+        a.record(stream)
+        tracer.resolve_paths(cam, dag, stream=stream.cuda_stream)
+        b.record(stream)
+    torch.cuda.synchronize()
+    ms = statistics.median(a.elapsed_time(b) for a, b in ev)
+    hits = tracer.hits_numpy()
+    return {"frame_ms": ms, "rays_s": cam.width * cam.height / (ms / 1e3),
+            "hit_fraction": float((hits["material"] != 255).mean())}
 
 
 def run_serve(args):
@@ -310,70 +352,113 @@ def run_serve(args):
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     levels = args.levels
-    rmax = 2048.0 * (1 << levels) / 131072
     dur_w, dur_k = args.warmup * args.window, args.steps * args.window
     # warm-up and timed streams (different seeds, so the timed edits are new work)
-    tw, ew, fw = w.c4_stream(args.rate, dur_w, seed=40 + rank, levels=levels, rmax=rmax,
-                             terrain=make_terrain(w, levels), copy_offset=int(1024 * (1 << levels) / 131072))
-    tk, ek, fk = w.c4_stream(args.rate, dur_k, seed=4 + rank, levels=levels, rmax=rmax,
-                             terrain=make_terrain(w, levels), copy_offset=int(1024 * (1 << levels) / 131072))
+    tw, ew, fw = stream_of(w, levels, args.rate, dur_w, 40 + rank)
+    tk, ek, fk = stream_of(w, levels, args.rate, dur_k, 4 + rank)
     cam = c2_camera(svdag, levels)
     out = {}
-    # served and plain paths, each on its own copy of the scene
+    dags = {}
+    # served and plain paths, each on its own copy of the scene (both resident)
     for name, plain in (("served", False), ("plain", True)):
         dag, _ = make_scene(svdag, w, levels, persistent=args.persistent)
         # the autotuner times the first warm-up edits (applied for real) and picks the launch form
         tuning = dag.autotune(edits=ew[:64])
-        replay(svdag, dag, cam, ew[64:], [t - tw[64] for t in tw[64:]] if len(ew) > 64 else [], fw, plain=plain)
+        res = replay(svdag, dag, cam, ew[64:], [t - tw[64] for t in tw[64:]] if len(ew) > 64 else [], fw, plain=plain)
+        require_ok(res, max(0, len(ew) - 64), f"{name} warm-up")
+        # the timed stream starts from a collected region (undo history kept)
+        dag.garbage_collect(keep_history=True)
+        dags[name] = dag
+        out[name] = {"tuning": {"persistent_leaves": tuning.persistent_leaves, "graph_us_small": tuning.graph_us_small,
+                                "persistent_us_small": tuning.persistent_us_small}}
+    for name, plain in (("served", False), ("plain", True)):
+        dag = dags[name]
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
+        mem, frames = {}, {}
         with ClockSampler(local) as clocks, profiled():
             t0 = time.perf_counter()
-            res = replay(svdag, dag, cam, ek, tk, fk, plain=plain)
+            res = replay(svdag, dag, cam, ek, tk, fk, plain=plain, memory=mem, counters=frames)
             wall = time.perf_counter() - t0
         torch.cuda.synchronize()
-        out[name] = summarize(res, len(ek))
+        require_ok(res, len(ek), f"{name} timed stream")
+        out[name].update(summarize(res, len(ek), dur_k))
         out[name]["wall_s"] = wall
-        out[name]["tuning"] = {"persistent_leaves": tuning.persistent_leaves, "graph_us_small": tuning.graph_us_small,
-                               "persistent_us_small": tuning.persistent_us_small}
+        out[name]["memory"] = mem
+        out[name]["frames"] = frames
         if name == "served":
             out["clocks"] = clocks.summary()
-            out["launches_timed"] = out[name]["launches"]
-            # e2e: the same timed stream again (after GC) with every frame copied to pinned host memory
-            dag.garbage_collect()
-            replay(svdag, dag, cam, ew, tw, fw)
-            frame_counters = {}
-            res_e2e = replay(svdag, dag, cam, ek, tk, fk, copy_frames=True, counters=frame_counters)
-            out["e2e"] = summarize(res_e2e, len(ek))
-            out["e2e"]["frames"] = frame_counters
-            # the dominant kernel: one window of the stream as one persistent batched launch
-            dag.garbage_collect()
-            nwin = max(1, len(ek) // max(1, args.steps))
-            batch = ek[:nwin]
-            stream = torch.cuda.Stream()
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            torch.cuda.synchronize()
-            a.record(stream)
-            nrec = dag.edit_batch(batch, stream=stream.cuda_stream)
-            b.record(stream)
-            torch.cuda.synchronize()
-            recs = dag.edit_records(nrec)
-            out["batch"] = {"edits": len(batch), "ms": a.elapsed_time(b), "bytes": edit_algorithmic_bytes(recs),
-                            "svo_items": int(sum(r.svo_items for r in recs))}
-            out["used_gb"] = dag.stats().item_region_used_bytes / 1e9
-        dag.free()
-        del dag
-    hash_res = None
+    # offered-load sweep: the same stream shape at other rates, served and plain, each from a
+    # collected region
+    out["sweep"] = []
+    for i, rate in enumerate(float(r) for r in args.sweep.split(",") if r):
+        dur = min(8.0, max(2.0, 400.0 / rate))
+        ts, es, fs = stream_of(w, levels, rate, dur, 200 + 10 * i + rank)
+        point = {"rate_edits_per_s": rate, "duration_s": dur}
+        for name, plain in (("served", False), ("plain", True)):
+            dags[name].garbage_collect(keep_history=True)
+            mem = {}
+            res = replay(svdag, dags[name], cam, es, ts, fs, plain=plain, memory=mem)
+            require_ok(res, len(es), f"{name} at {rate:g} edits/s")
+            point[name] = summarize(res, len(es), dur)
+            point[name]["gc_runs"] = mem.get("gc_runs")
+        point["p99_served_over_plain"] = point["served"]["p99_ms"] / point["plain"]["p99_ms"]
+        out["sweep"].append(point)
+    dags["plain"].free()
+    del dags["plain"]
+    dag = dags["served"]
+    # e2e: the timed stream again with every frame copied to pinned host memory
+    dag.garbage_collect(keep_history=True)
+    frame_counters = {}
+    res_e2e = replay(svdag, dag, cam, ek, tk, fk, copy_frames=True, counters=frame_counters)
+    require_ok(res_e2e, len(ek), "e2e stream")
+    out["e2e"] = summarize(res_e2e, len(ek), dur_k)
+    out["e2e"]["frames"] = frame_counters
+    # the dominant kernel: one window of the stream as one batched launch
+    dag.garbage_collect(keep_history=True)
+    nwin = max(1, len(ek) // max(1, args.steps))
+    batch = ek[:nwin]
+    stream = torch.cuda.Stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    nrec = dag.edit_batch(batch, stream=stream.cuda_stream)
+    b.record(stream)
+    torch.cuda.synchronize()
+    recs = dag.edit_records(nrec)
+    bad = [i for i, r in enumerate(recs) if r.status != 0]
+    if bad:
+        raise SystemExit(f"bench: batched window: edit record {bad[0]} has status {recs[bad[0]].status}")
+    out["batch"] = {"edits": len(batch), "ms": a.elapsed_time(b), "bytes": edit_algorithmic_bytes(recs),
+                    "svo_items": int(sum(r.svo_items for r in recs))}
+    st = dag.stats()
+    out["used_gb"] = st.item_region_used_bytes / 1e9
+    out["trace"] = trace_rays_s(svdag, torch, dag, cam)
+    dag.free()
+    del dags["served"]
+    peak, peak_kind = measured_peak_gbs()
+    trace_c0 = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu_c0, cpu_hits = cpu_trace_c0()
+        trace_c0 = {"gpu": gpu_trace_c0(svdag, torch, cpu_c0, cpu_hits, peak), "cpu": cpu_c0}
+    hash_res = []
     if not args.no_hash:
-        hash_res = run_hash_bench(svdag, torch, torch.cuda.Stream(), lanes=args.hash_lanes, load_factor=args.hash_lf)
+        for lf in (16, 96):
+            for lanes in (1, 32):
+                hash_res.append(run_hash_bench(svdag, torch, torch.cuda.Stream(), lanes=lanes, load_factor=lf))
     p99 = out["served"]["p99_ms"]
     p99, out["plain"]["p99_ms"], out["e2e"]["p99_ms"] = max_over_ranks([p99, out["plain"]["p99_ms"], out["e2e"]["p99_ms"]], dist)
-    peak, peak_kind = measured_peak_gbs()
     bt = out["batch"]
     achieved = bt["bytes"] / (bt["ms"] / 1e3) / 1e9
     # frame bytes the server copied to host memory (incremental frames copy only their changed pixels)
-    frame_d2h = out["e2e"].get("frames", {}).get("frame_bytes_to_host", cam.width * cam.height * 68 * out["e2e"]["launches"])
+    frame_d2h = out["e2e"]["frames"].get("frame_bytes_to_host", cam.width * cam.height * 68 * out["e2e"]["launches"])
+    # the served/plain ratio at the highest offered load both paths sustain (the plain loop's p99 at a
+    # load it cannot keep up with measures its queue, not its kernels)
+    points = [(args.rate, out["served"], out["plain"])] + [(p["rate_edits_per_s"], p["served"], p["plain"]) for p in out["sweep"]]
+    both = [pt for pt in points if pt[1]["sustained"] and pt[2]["sustained"]]
+    head = max(both, key=lambda pt: pt[0]) if both else None
+    fr = out["served"]["frames"]
     line = {
         "metric": METRIC,
         "value": p99,
@@ -394,6 +479,10 @@ def run_serve(args):
                    "l2": "inputs larger than L2 (the DAG holds > 20 GB; edits land at random places)"},
         "served": out["served"], "plain": out["plain"],
         "p99_served_over_plain": p99 / out["plain"]["p99_ms"] if out["plain"]["p99_ms"] else None,
+        "p99_served_over_plain_sustained": ({"rate_edits_per_s": head[0], "ratio": head[1]["p99_ms"] / head[2]["p99_ms"],
+                                             "served_p99_ms": head[1]["p99_ms"], "plain_p99_ms": head[2]["p99_ms"]}
+                                            if head else None),
+        "sweep": out["sweep"],
         "edited_mvox_s_served": out["served"]["edited_mvox_s"],
         "e2e": {"value": out["e2e"]["p99_ms"], "unit": "ms (served p99 edit-to-visible, frames copied to host)",
                 "h2d_bytes_per_step": int(56 * len(ek) / args.steps),
@@ -403,15 +492,23 @@ def run_serve(args):
                                "the phase kernels, small edits in the single-CTA persistent kernel)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind, "traffic": None, "launch": bt},
+        "trace_1080p": dict(out["trace"], bytes_per_ray_lower_bound=68 + 8 * levels,
+                            hbm_frac_lower_bound=out["trace"]["rays_s"] * (68 + 8 * levels) / 1e9 / peak),
+        "trace_c0": trace_c0,
         "clocks": out["clocks"],
-        "gpu_launches": 2 * out["launches_timed"],
+        # launch calls of the timed served replay: one per batch (a CUDA-graph replay or one persistent
+        # kernel per run of small edits) and one per frame
+        "gpu_launches": out["served"]["launches"] + fr.get("frames_whole", 0) + fr.get("frames_incremental", 0),
         "item_region_used_gb": out["used_gb"],
     }
     if hash_res:
         line["hash_c1"] = hash_res
-        line["hash_roofline"] = {"kernel": f"slab-hash find (2^24 keys, {args.hash_lanes} lane(s)/key)",
-                                 "achieved": hash_res["find_gbs"], "peak": peak, "unit": "GB/s",
-                                 "frac": hash_res["find_gbs"] / peak}
+        primary = hash_res[0]
+        line["hash_roofline"] = {"kernel": f"slab-hash find (2^24 keys, load factor {primary['load_factor']}, "
+                                           f"{primary['lanes']} lane(s)/key)",
+                                 "achieved": primary["find_gbs"], "peak": peak, "unit": "GB/s",
+                                 "frac": primary["find_gbs"] / peak,
+                                 "insert_achieved": primary["insert_gbs"], "insert_frac": primary["insert_gbs"] / peak}
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_sample(args, levels)["cpu_baseline"]
     if rank == 0:
@@ -439,60 +536,159 @@ def edit_box(e):
     return [int(np.floor(v)) for v in lo], [int(np.ceil(v)) + 1 for v in hi]
 
 
-def cpu_sample(args, levels, budget_s=25.0):
-    """The oracle (CPU restatement of the reference pipeline, one core) on the leading edits of the
-    timed stream, each on the scene clipped to the edit's box (the result inside the box equals the
-    full scene's: edits are local). Times the edit only; the region build is not timed."""
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_sample(args, levels, budget_s=25.0, min_edits=64, hard_s=90.0):
+    """The oracle (the CPU restatement of the reference pipeline; the reference's MyGpuDag path has no
+    CPU implementation) on the leading edits of the timed stream, one edit per host thread at a time
+    on every host core, each edit on the scene clipped to its box (the result inside the box equals
+    the full scene's: edits are local). Times the edit only; the region build is not timed. At least
+    `min_edits` edits, more while `budget_s` lasts. Loads no CUDA library: the stream's surface heights
+    come from the oracle's own terrain function."""
+    import concurrent.futures as cf
+    import threading
+
     import svdag.workloads as w
     from oracle import oracle
 
-    rmax = 2048.0 * (1 << levels) / 131072
-    tk, ek, _ = w.c4_stream(args.rate, args.steps * args.window, seed=4, levels=levels, rmax=rmax,
-                            terrain=make_terrain(w, levels), copy_offset=int(1024 * (1 << levels) / 131072))
+    L = oracle.lib()
     params = oracle.TerrainParams(**make_terrain(w, levels))
-    lat, vox, radii = [], 0, []
+    height = lambda lv, x, z, terrain: L.oracle_terrain_height(params, lv, x, z)
+    _, ek, _ = stream_of(w, levels, args.rate, args.steps * args.window, 4, height=height)
+    threads = host_threads()
+    lock = threading.Lock()
+    state = {"next": 0}
     start = time.perf_counter()
-    for e in ek:
-        if time.perf_counter() - start > budget_s and len(lat) >= 8:
-            break
-        d = oracle.OracleDag(levels)
-        lo, hi = edit_box(e)
-        d.build_scene_region(params, lo, hi)
-        oe = oracle.Edit(tool=e.tool, material=e.material, radius=e.radius, noise_seed=e.noise_seed,
-                         noise_cell_log2=e.noise_cell_log2)
-        oe.center[:], oe.src[:], oe.dst[:] = list(e.center), list(e.src), list(e.dst)
-        t0 = time.perf_counter()
-        st = d.edit(oe)
-        lat.append((time.perf_counter() - t0) * 1e3)
-        vox += st.edited_voxels
-        radii.append(float(e.radius))
-        del d
+    results = []
+
+    def worker():
+        while True:
+            with lock:
+                i = state["next"]
+                el = time.perf_counter() - start
+                if i >= len(ek) or (i >= min_edits and el > budget_s) or el > hard_s:
+                    return
+                state["next"] = i + 1
+            e = ek[i]
+            d = oracle.OracleDag(levels)
+            lo, hi = edit_box(e)
+            d.build_scene_region(params, lo, hi)
+            oe = oracle.Edit(tool=e.tool, material=e.material, radius=e.radius, noise_seed=e.noise_seed,
+                             noise_cell_log2=e.noise_cell_log2)
+            oe.center[:], oe.src[:], oe.dst[:] = list(e.center), list(e.src), list(e.dst)
+            t0 = time.perf_counter()
+            st = d.edit(oe)
+            ms = (time.perf_counter() - t0) * 1e3
+            with lock:
+                results.append((i, ms, st.edited_voxels, float(e.radius)))
+            del d
+
+    with cf.ThreadPoolExecutor(threads) as ex:
+        for f in [ex.submit(worker) for _ in range(threads)]:
+            f.result()
+    wall = time.perf_counter() - start
+    results.sort()
+    lat = [r[1] for r in results]
+    vox = sum(r[2] for r in results)
+    radii = [r[3] for r in results]
     p99 = pct(lat, 99)
     return {"p99_ms": p99, "p50_ms": pct(lat, 50), "mean_ms": float(np.mean(lat)), "edits": len(lat),
-            "edited_mvox_s": vox / (sum(lat) / 1e3) / 1e6,
-            "cpu_baseline": {"value": p99, "unit": "ms (p99 edit latency, edit only)", "cores": 1, "kind": "port",
+            "edited_mvox_s": vox / (sum(lat) / 1e3) / 1e6, "threads": threads,
+            "cpu_baseline": {"value": p99, "unit": "ms (p99 edit latency, edit only)", "cores": threads, "kind": "port",
                              "sample": f"first {len(lat)} edits of the timed stream (radius {min(radii):.0f}..{max(radii):.0f}), "
-                                       "each on the scene clipped to its box; edit time only, no frame, no queueing",
-                             "p50_ms": pct(lat, 50)}}
+                                       f"one edit per thread on {threads} host threads, each on the scene clipped to its "
+                                       "box; edit time only, no frame, no queueing",
+                             "p50_ms": pct(lat, 50), "edits_per_s_all_threads": len(lat) / wall,
+                             "edited_mvox_s_all_threads": vox / wall / 1e6}}
+
+
+def c0_trace_params(svdag):
+    """The C0 frame: 256x256 primary rays of the depth-10 terrain from (512, 900, 512) towards the
+    grid centre (get_trace_params is host Python: no CUDA library is loaded)."""
+    return svdag.get_trace_params((512.0, 900.0, 512.0), (512.0, 512.0, 512.0), C0_FRAME, C0_FRAME)
+
+
+def cpu_trace_c0(reps=3):
+    """The oracle's tracer (a restatement of tracer.cu; the reference has no CPU tracer) on the C0
+    frame, row bands on every host thread. Returns rays/s, the hit buffer and the visit counts the
+    algorithmic bytes of the trace roofline come from."""
+    import svdag
+    import svdag.workloads as w
+    from oracle import oracle
+
+    threads = host_threads()
+    o = oracle.OracleDag(w.C0_LEVELS)
+    o.build_terrain(oracle.TerrainParams(**w.C0_TERRAIN))
+    p = c0_trace_params(svdag)
+    po = oracle.TraceParams()
+    for f in ("camera", "ray_min", "ray_ddx", "ray_ddy"):
+        getattr(po, f)[:] = list(getattr(p, f))
+    po.width, po.height = p.width, p.height
+    best, hits = None, None
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        hits = o.trace(po, threads)
+        dt = time.perf_counter() - t0
+        best = dt if best is None else min(best, dt)
+    nodes, leaves, nhits = o.trace_counts(po)
+    return {"rays_s": p.width * p.height / best, "threads": threads, "frame_ms": best * 1e3,
+            "node_visits": nodes, "leaf_visits": leaves, "hits": nhits}, hits
+
+
+def gpu_trace_c0(svdag, torch, cpu, cpu_hits, peak, frames=50):
+    """The same C0 frame on the GPU (CUDA events over `frames` launches on the tracer's stream),
+    checked pixel for pixel against the oracle's hit buffer. Algorithmic bytes per frame: 8 per node
+    visit (header + child pointer), 12 per leaf visit, 68 per hit record written."""
+    import svdag.workloads as w
+
+    dag = svdag.MyGPUHashDAG(w.C0_LEVELS, pool_bytes=4 << 30, scratch_bytes=1 << 30)
+    dag.build_terrain(**w.C0_TERRAIN)
+    p = c0_trace_params(svdag)
+    tracer = svdag.DAGTracer(p.width, p.height)
+    stream = torch.cuda.Stream()
+    for _ in range(3):
+        tracer.resolve_paths(p, dag, stream=stream.cuda_stream)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(frames):
+        tracer.resolve_paths(p, dag, stream=stream.cuda_stream)
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / frames
+    hits = tracer.hits_numpy()
+    exact = bool(np.array_equal(hits["path"], cpu_hits["path"]) and np.array_equal(hits["material"], cpu_hits["material"]))
+    dag.free()
+    rays = p.width * p.height
+    alg = 8.0 * cpu["node_visits"] + 12.0 * cpu["leaf_visits"] + 68.0 * rays
+    return {"rays_s": rays / (ms / 1e3), "frame_us": ms * 1e3, "bit_exact_vs_oracle": exact,
+            "bytes_per_frame": alg, "hbm_frac": alg / (ms / 1e3) / 1e9 / peak}
 
 
 def run_reference(args):
-    """Reference arm: the CPU restatement of the reference path timed on the host, rank 0 only."""
+    """Reference arm: the CPU restatement of the reference path timed on the host cores, rank 0 only.
+    No CUDA library is loaded (libsvdag.so stays unmapped)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     r = cpu_sample(args, args.levels)
     cb = r["cpu_baseline"]
-    cb["cores"] = 1
+    trace, _ = cpu_trace_c0()
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": r["p99_ms"], "unit": "ms (p99 edit latency, edit only)",
         "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": r["mean_ms"], "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded procedural scene and seeded request stream)",
-        "config": {"workload": f"c4 stream edits on the c2 scene (depth {args.levels}), one at a time on the CPU",
+        "config": {"workload": f"c4 stream edits on the c2 scene (depth {args.levels}), one edit per host thread on the CPU",
                    "levels": args.levels, "rate_edits_per_s": args.rate},
         "p50_ms": r["p50_ms"], "edits": r["edits"], "edited_mvox_s": r["edited_mvox_s"],
         "cpu_baseline": cb,
+        "trace_c0_cpu": trace,
         "e2e": {"value": r["p99_ms"], "unit": "ms (p99 edit latency, edit only)", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }))
@@ -755,6 +951,7 @@ def main():
                     help="serve = the benchmark line; the others run one sub-workload (profiling)")
     ap.add_argument("--rate", type=float, default=1000.0, help="edit arrivals per second")
     ap.add_argument("--window", type=float, default=0.5, help="seconds of the stream per step")
+    ap.add_argument("--sweep", default="50,200,500,2000", help="other offered loads (edits/s) served and plain")
     ap.add_argument("--levels", type=int, default=17)
     ap.add_argument("--phase-kernels", action="store_true", help="one launch per edit phase (profiling)")
     ap.add_argument("--persistent", action="store_true", help="small edits in the persistent cooperative kernel")

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 
@@ -16,37 +17,78 @@ constexpr unsigned long long kCtlBytes = 64 * 1024;
 constexpr unsigned long long kBatchBytes = 2 * 1024 * 1024;
 
 // ---------------------------------------------------------------- garbage collection
-// MyGPUHashDAG::garbageCollect (my_gpu_hash_dag.cu:365-475) marks level by level from the root set
-// (the root and the level-0 fully-filled nodes) and, with CAPTURE_MEMORY_STATS_SLOW, frees the
-// unmarked slots (gpu_hash_table_base.cu:304-374). Here marking is a bitmap with one bit per handle
-// (an 8-byte unit of the item region) and the frontier is deduplicated by the test-and-set on it.
+// MyGPUHashDAG::garbageCollect(activeRootNodes) (my_gpu_hash_dag.cu:373-463) marks level by level
+// from the active roots and the canonical fully-filled nodes; freeInactiveItems
+// (gpu_hash_table_base.cu:265-374) then clears every unmarked slot and hands every overflow slab it
+// leaves empty back to the slab allocator. Here marking is a bitmap with one bit per handle (an
+// 8-byte unit of the item region) and the frontier is deduplicated by the test-and-set on it; the
+// sweep unlinks empty overflow slabs and pushes them on the free list of their size class.
+// MyGPUHashDAGUndoRedo::garbageCollect (my_gpu_base_dag.h:66-77) passes the current root alone and
+// clears the history (svdag_gc); svdag_gc_keep_history passes the current root and every undo and
+// redo root, and keeps the history.
 
 __device__ __forceinline__ bool mark_once(uint32_t* bits, uint32_t handle)
 {
     const uint32_t m = 1u << (handle & 31u);
+    if (__ldcg(&bits[handle >> 5]) & m) // most children of a shared DAG are marked already
+        return false;
     return !(atomicOr(&bits[handle >> 5], m) & m);
 }
 
-__global__ void k_gc_roots(DevDag d, uint32_t* bits, uint32_t* frontier, uint32_t* count)
+__device__ __forceinline__ void push_root(const DevDag& d, uint32_t* bits, uint32_t h, uint32_t* frontier, uint32_t& n)
+{
+    if (h == kNone)
+        return;
+    if (!handle_ok(d, h)) {
+        set_status(d.ctl, SVDAG_ERR_CORRUPT);
+        return;
+    }
+    if (mark_once(bits, h))
+        frontier[n++] = h;
+}
+
+// Level-0 frontier: the root, the canonical fully-filled nodes of level 0 and, with `history`,
+// every root of the undo ring and the redo stack (at most 1 + 16 + 64 + 64 entries).
+__global__ void k_gc_roots(DevDag d, uint32_t* bits, uint32_t* frontier, uint32_t* count, uint32_t history)
 {
     if (threadIdx.x != 0 || blockIdx.x != 0)
         return;
+    const Control* c = d.ctl;
     uint32_t n = 0;
-    const uint32_t root = d.ctl->root;
-    if (root != kNone && mark_once(bits, root))
-        frontier[n++] = root;
-    for (uint32_t m = 0; m < SVDAG_NUM_MATERIALS; ++m) {
-        const uint32_t h = d.ctl->fullyFilled[0][m];
-        if (h != kNone && mark_once(bits, h))
-            frontier[n++] = h;
+    push_root(d, bits, c->root, frontier, n);
+    for (uint32_t m = 0; m < SVDAG_NUM_MATERIALS; ++m)
+        push_root(d, bits, c->fullyFilled[0][m], frontier, n);
+    if (history) {
+        const uint32_t nu = c->undoCount < 64u ? c->undoCount : 64u;
+        for (uint32_t i = 0; i < nu; ++i)
+            push_root(d, bits, c->undo[(c->undoHead + 63u - i) & 63u], frontier, n);
+        const uint32_t nr = c->redoCount < 64u ? c->redoCount : 64u;
+        for (uint32_t i = 0; i < nr; ++i)
+            push_root(d, bits, c->redo[i], frontier, n);
     }
     count[0] = n;
 }
 
-__global__ void k_gc_mark(DevDag d, uint32_t* bits, const uint32_t* in, const uint32_t* inCount, uint32_t* out, uint32_t* outCount,
-    unsigned long long outCap)
+// Marks the children of the level's frontier and gathers the newly marked ones (plus the canonical
+// fully-filled items of the level below) as the next frontier. A frontier longer than `cap` latches
+// SVDAG_ERR_OOM; the next level then reads only the first `cap` entries and the host leaves the
+// tables untouched (no sweep runs after an incomplete mark).
+__global__ void k_gc_mark(DevDag d, uint32_t* bits, uint32_t level, const uint32_t* in, const uint32_t* inCount, uint32_t* out,
+    uint32_t* outCount, uint32_t cap)
 {
-    const uint32_t n = *inCount;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        for (uint32_t m = 0; m < SVDAG_NUM_MATERIALS; ++m) {
+            const uint32_t h = d.ctl->fullyFilled[level + 1][m];
+            if (h == kNone || !handle_ok(d, h) || !mark_once(bits, h))
+                continue;
+            const uint32_t at = atomicAdd(outCount, 1u);
+            if (at < cap)
+                out[at] = h;
+            else
+                set_status(d.ctl, SVDAG_ERR_OOM);
+        }
+    }
+    const uint32_t n = min(*inCount, cap);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t* node = item_ptr(d, in[i]);
         const uint32_t mask = node[0] & 0xFFu;
@@ -59,7 +101,7 @@ __global__ void k_gc_mark(DevDag d, uint32_t* bits, const uint32_t* in, const ui
             }
             if (mark_once(bits, c)) {
                 const uint32_t at = atomicAdd(outCount, 1u);
-                if (at < outCap)
+                if (at < cap)
                     out[at] = c;
                 else
                     set_status(d.ctl, SVDAG_ERR_OOM);
@@ -68,26 +110,34 @@ __global__ void k_gc_mark(DevDag d, uint32_t* bits, const uint32_t* in, const ui
     }
 }
 
-// Clears unmarked occupied slots (tag and item words) of one table; returns freed items in *freed.
+// One thread per bucket: clears the unmarked occupied slots (tag and item words) of its chain and
+// unlinks every overflow slab left without an occupied slot (the bucket's own slab stays); the
+// unlinked slabs of a thread are pushed on their class's free list as one chain.
 __global__ void k_gc_sweep(DevDag d, DevTable t, const uint32_t* bits, unsigned long long* freed)
 {
-    unsigned long long nfreed = 0;
+    unsigned long long nfreed = 0, nslabs = 0;
     for (uint32_t c = 0; c < kNumClasses; ++c) {
         const uint32_t k = c + 2;
+        uint32_t first = kEnd, last = kEnd, count = 0; // unlinked slabs, linked through word 7
         for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < t.numBuckets[c]; b += gridDim.x * blockDim.x) {
             uint32_t slab = t.bucketBase[c] + b;
+            uint32_t* prevLink = nullptr; // the link word that leads to `slab` (none for the bucket's slab)
             for (uint32_t steps = 0; steps < kMaxChain; ++steps) {
                 uint32_t* h = slab_ptr(d, slab);
                 const uint32_t body = h[6];
+                uint32_t live = 0;
                 for (uint32_t s = 0; s < kSlots; ++s) {
                     const uint32_t tag = header_tag(h, s);
-                    if (tag == 0 || tag == kTagBusy)
+                    if (tag == 0)
                         continue;
                     const uint32_t item = slot_handle(body, s, k);
-                    if ((bits[item >> 5] >> (item & 31u)) & 1u)
+                    if (tag == kTagBusy || ((bits[item >> 5] >> (item & 31u)) & 1u)) {
+                        ++live;
                         continue;
+                    }
                     if (!handle_ok(d, item)) {
                         set_status(d.ctl, SVDAG_ERR_CORRUPT);
+                        ++live;
                         continue;
                     }
                     uint32_t* ip = handle_ptr(d, item);
@@ -96,24 +146,94 @@ __global__ void k_gc_sweep(DevDag d, DevTable t, const uint32_t* bits, unsigned 
                     h[s >> 2] &= ~(0xFFu << (8u * (s & 3u)));
                     ++nfreed;
                 }
-                if (h[7] == kEnd)
-                    break;
-                if (!slab_ok(d, h[7])) {
+                const uint32_t next = h[7];
+                if (next != kEnd && !slab_ok(d, next)) {
                     set_status(d.ctl, SVDAG_ERR_CORRUPT);
                     break;
                 }
-                slab = h[7];
+                if (live == 0 && prevLink) { // an empty overflow slab: out of the chain, onto the free list
+                    *prevLink = next;
+                    h[7] = first;
+                    first = slab;
+                    if (last == kEnd)
+                        last = slab;
+                    ++count;
+                } else {
+                    prevLink = h + 7;
+                }
+                if (next == kEnd)
+                    break;
+                slab = next;
             }
+        }
+        if (count) {
+            push_free_chain(d, c, first, last, count);
+            nslabs += count;
         }
     }
     if (nfreed)
-        atomicAdd(freed, nfreed);
+        atomicAdd(&freed[0], nfreed);
+    if (nslabs)
+        atomicAdd(&freed[1], nslabs);
 }
 
-__global__ void k_gc_clear_history(Control* c)
+__global__ void k_gc_finish(Control* c, const unsigned long long* freed, uint32_t clearHistory)
 {
-    c->undoCount = 0;
-    c->redoCount = 0;
+    c->gcFreedItems = freed[0];
+    c->gcFreedSlabs = freed[1];
+    if (clearHistory) {
+        c->undoCount = 0;
+        c->redoCount = 0;
+    }
+}
+
+svdag_status collect(svdag_ctx* ctx, bool keepHistory, cudaStream_t s)
+{
+    SVDAG_TRY(ensure_level_tables(ctx, s));
+    // A collection reports its own errors: an error latched by earlier work (which its own call or
+    // record reported) is cleared first.
+    (void)read_status(ctx, s);
+    unsigned long long top = 0;
+    SVDAG_CUDA(cudaMemcpyAsync(&top, &ctx->ctl->itemTop, sizeof(top), cudaMemcpyDeviceToHost, s));
+    SVDAG_CUDA(cudaStreamSynchronize(s));
+    top = std::min<unsigned long long>(top, ctx->itemWords);
+    const unsigned long long bitmapBytes = align256(((top / 2) + 64) / 8 + 8); // one bit per 8-byte unit
+    const unsigned long long rest = ctx->scratchBytes > bitmapBytes + 4096 ? ctx->scratchBytes - bitmapBytes - 4096 : 0;
+    uint32_t frontierCap = (uint32_t)std::min<unsigned long long>(rest / 8, 0xFFFFFFFFull); // two frontiers of u32
+    // SVDAG_GC_MAX_FRONTIER lowers the frontier capacity (tests reach the overflow path with it
+    // without a DAG larger than the scratch arena).
+    if (const char* cap = std::getenv("SVDAG_GC_MAX_FRONTIER"))
+        frontierCap = (uint32_t)std::min<unsigned long long>(frontierCap, std::strtoull(cap, nullptr, 10));
+    if (frontierCap < 1024)
+        return SVDAG_ERR_OOM;
+    auto* bits = reinterpret_cast<uint32_t*>(ctx->scratch);
+    auto* counts = reinterpret_cast<uint32_t*>(ctx->scratch + bitmapBytes);
+    auto* fa = reinterpret_cast<uint32_t*>(ctx->scratch + bitmapBytes + 4096);
+    auto* fb = fa + frontierCap;
+    ctx->scratchHighWater = std::max(ctx->scratchHighWater, bitmapBytes + 4096);
+    SVDAG_CUDA(cudaMemsetAsync(ctx->scratch, 0, bitmapBytes + 4096, s));
+    const DevDag d = ctx->dag();
+    k_gc_roots<<<1, 32, 0, s>>>(d, bits, fa, counts + 0, keepHistory ? 1u : 0u);
+    const uint32_t LL = d.leafLevel;
+    for (uint32_t level = 0; level < LL; ++level) {
+        uint32_t* in = (level & 1) ? fb : fa;
+        uint32_t* out = (level & 1) ? fa : fb;
+        k_gc_mark<<<grid_for(ctx, 1ull << 24, 256), 256, 0, s>>>(d, bits, level, in, counts + level, out, counts + level + 1, frontierCap);
+    }
+    SVDAG_CUDA(cudaGetLastError());
+    // An incomplete mark (frontier overflow, a corrupt handle) must not free anything.
+    SVDAG_TRY(read_status(ctx, s));
+    auto* freed = reinterpret_cast<unsigned long long*>(counts + 64);
+    for (uint32_t level = 0; level <= LL; ++level) {
+        const DevTable t = ctx->levelTables[level].dev;
+        unsigned long long nb = 0;
+        for (uint32_t c = 0; c < kNumClasses; ++c)
+            nb = std::max<unsigned long long>(nb, t.numBuckets[c]);
+        k_gc_sweep<<<grid_for(ctx, nb, 256), 256, 0, s>>>(d, t, bits, freed);
+    }
+    k_gc_finish<<<1, 1, 0, s>>>(ctx->ctl, freed, keepHistory ? 0u : 1u);
+    SVDAG_CUDA(cudaGetLastError());
+    return read_status(ctx, s);
 }
 
 } // namespace
@@ -261,40 +381,14 @@ svdag_status svdag_gc(svdag_ctx* ctx, void* stream)
 {
     if (!ctx)
         return SVDAG_ERR_INVALID;
-    cudaStream_t s = as_stream(stream);
-    SVDAG_TRY(ensure_level_tables(ctx, s));
-    unsigned long long top = 0;
-    SVDAG_CUDA(cudaMemcpyAsync(&top, &ctx->ctl->itemTop, sizeof(top), cudaMemcpyDeviceToHost, s));
-    SVDAG_CUDA(cudaStreamSynchronize(s));
-    const unsigned long long bitmapBytes = align256(((top / 2) + 64) / 8 + 8); // one bit per 8-byte unit
-    const unsigned long long rest = ctx->scratchBytes > bitmapBytes + 4096 ? ctx->scratchBytes - bitmapBytes - 4096 : 0;
-    const unsigned long long frontierCap = rest / 8; // two frontiers of u32
-    if (frontierCap < 1024)
-        return SVDAG_ERR_OOM;
-    auto* bits = reinterpret_cast<uint32_t*>(ctx->scratch);
-    auto* counts = reinterpret_cast<uint32_t*>(ctx->scratch + bitmapBytes);
-    auto* fa = reinterpret_cast<uint32_t*>(ctx->scratch + bitmapBytes + 4096);
-    auto* fb = fa + frontierCap;
-    SVDAG_CUDA(cudaMemsetAsync(ctx->scratch, 0, bitmapBytes + 4096, s));
-    const DevDag d = ctx->dag();
-    k_gc_roots<<<1, 32, 0, s>>>(d, bits, fa, counts + 0);
-    const uint32_t LL = d.leafLevel;
-    for (uint32_t level = 0; level < LL; ++level) {
-        uint32_t* in = (level & 1) ? fb : fa;
-        uint32_t* out = (level & 1) ? fa : fb;
-        k_gc_mark<<<grid_for(ctx, 1ull << 24, 256), 256, 0, s>>>(d, bits, in, counts + level, out, counts + level + 1, frontierCap);
-    }
-    unsigned long long* freed = reinterpret_cast<unsigned long long*>(counts + 64);
-    for (uint32_t level = 0; level <= LL; ++level) {
-        const DevTable t = ctx->levelTables[level].dev;
-        unsigned long long nb = 0;
-        for (uint32_t c = 0; c < kNumClasses; ++c)
-            nb = std::max<unsigned long long>(nb, t.numBuckets[c]);
-        k_gc_sweep<<<grid_for(ctx, nb, 256), 256, 0, s>>>(d, t, bits, freed);
-    }
-    k_gc_clear_history<<<1, 1, 0, s>>>(ctx->ctl);
-    SVDAG_CUDA(cudaGetLastError());
-    return read_status(ctx, s);
+    return collect(ctx, false, as_stream(stream));
+}
+
+svdag_status svdag_gc_keep_history(svdag_ctx* ctx, void* stream)
+{
+    if (!ctx)
+        return SVDAG_ERR_INVALID;
+    return collect(ctx, true, as_stream(stream));
 }
 
 svdag_status svdag_get_stats(svdag_ctx* ctx, svdag_stats* out, void* stream)
@@ -310,7 +404,12 @@ svdag_status svdag_get_stats(svdag_ctx* ctx, svdag_stats* out, void* stream)
     out->root = c.root;
     out->pool_bytes = ctx->poolBytes;
     out->item_region_bytes = ctx->itemWords * 4 + ctx->headerCount * 32;
-    out->item_region_used_bytes = c.itemTop * 4 + c.headerTop * 32;
+    out->item_region_used_bytes = used_region_bytes(ctx, c.itemTop, c.headerTop, c.freeBytes);
+    out->free_list_bytes = c.freeBytes;
+    for (uint32_t k = 0; k < kNumClasses; ++k)
+        out->free_list_slabs += c.freeSlabs[k];
+    out->gc_freed_items = c.gcFreedItems;
+    out->gc_freed_slabs = c.gcFreedSlabs;
     out->scratch_bytes = ctx->scratchBytes;
     out->scratch_high_water_bytes = ctx->scratchHighWater;
     out->undo_count = c.undoCount;

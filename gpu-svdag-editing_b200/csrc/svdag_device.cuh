@@ -20,9 +20,18 @@
 // header with each slab's items (compact_acceleration_hash_table.h:519-541). The first slab of each
 // bucket is allocated with the table (HASH_TABLE_STORE_SLABS_IN_TABLE, gpu_hash_table_base.h:30-49);
 // overflow slabs come from bump allocators over the two regions and are linked at the chain's tail.
+//
+// Free list (DynamicSlabAllocator::free, dynamic_slab_alloc.h:187-208, and the sweep's unlinking of
+// empty slabs, gpu_hash_table_base.cu:265-281,320-336): garbage collection unlinks every overflow
+// slab of a level table that it leaves empty and pushes it on the free list of its size class, a
+// stack of header ids linked through header word 7 whose head carries a 32-bit version count beside
+// the id (so a pop racing a push cannot take a stale link). Overflow allocations of level tables pop
+// from that list before they bump. Tables whose space is given back by rewinding the bump pointers
+// (the autotuner's scratch tables) neither pop nor push.
 #pragma once
 #include <cooperative_groups.h>
 #include <cooperative_groups/scan.h>
+#include <cstddef>
 #include <cstdint>
 
 #include "../../include/svdag.h"
@@ -53,6 +62,7 @@ struct DevTable {
     uint32_t numBuckets[kNumClasses];
     uint32_t bucketBase[kNumClasses]; // header id of bucket 0
     uint32_t bodyBase[kNumClasses]; // body handle of bucket 0 (bucket b's body follows at b * body size)
+    uint32_t recycle; // overflow slabs come from and go back to the free lists (level tables)
 };
 
 // Device control block (lives at the start of the scratch side of the pool).
@@ -78,6 +88,7 @@ struct Control {
     unsigned long long headerTop; // bump pointer of the header region, in headers (0 is never used)
     uint32_t status; // latched svdag_status
     uint32_t root; // current root handle (kNone = empty DAG)
+    unsigned long long freeBytes; // bytes (headers and bodies) of the slabs on the free lists
     uint32_t undo[64];
     uint32_t redo[64];
     uint32_t undoHead, undoCount, redoCount, undoDepth;
@@ -89,7 +100,25 @@ struct Control {
     unsigned long long phaseTimes[64]; // GPU global-timer stamps at the phase barriers of the last fused edit
     uint32_t phaseCount;
     uint32_t pad1;
+    unsigned long long freeHead[kNumClasses]; // per size class: version << 32 | header id of the first free slab (0 = none)
+    unsigned long long freeSlabs[kNumClasses]; // slabs on each free list
+    unsigned long long gcFreedItems; // items the last collection freed
+    unsigned long long gcFreedSlabs; // overflow slabs the last collection put on the free lists
 };
+
+// The first 32 bytes of the control block, copied to the host after every served launch.
+struct MemSnapshot {
+    unsigned long long itemTop, headerTop;
+    uint32_t status, root;
+    unsigned long long freeBytes;
+};
+static_assert(offsetof(Control, itemTop) == offsetof(MemSnapshot, itemTop) && offsetof(Control, headerTop) == offsetof(MemSnapshot, headerTop)
+        && offsetof(Control, status) == offsetof(MemSnapshot, status) && offsetof(Control, root) == offsetof(MemSnapshot, root)
+        && offsetof(Control, freeBytes) == offsetof(MemSnapshot, freeBytes),
+    "MemSnapshot mirrors the head of Control");
+
+// Bytes of item and header region a slab of k-word items occupies.
+__host__ __device__ constexpr unsigned long long slab_bytes(uint32_t k) { return 32ull + 4ull * body_words(k); }
 
 struct DevDag {
     uint32_t* items;
@@ -426,13 +455,74 @@ __device__ __forceinline__ uint32_t first_slab(const DevTable& t, uint32_t cls, 
     return t.bucketBase[cls] + bucket_of(ha, t.numBuckets[cls]);
 }
 
+constexpr uint32_t kFreeListTries = 64; // pops that lose this many races fall back to the bump allocator
+
+// Takes a slab off the free list of size class `cls`; kNone when the list is empty (or contended).
+// The head's version count changes with every pop and push, so a pop whose head is stale fails its
+// compare-and-swap even when the same id is back on top.
+__device__ __forceinline__ uint32_t pop_free_slab(const DevDag& d, uint32_t cls)
+{
+    unsigned long long* head = &d.ctl->freeHead[cls];
+    unsigned long long cur = __ldcg(head);
+    for (uint32_t tries = 0; tries < kFreeListTries; ++tries) {
+        const uint32_t id = (uint32_t)cur;
+        if (id == kEnd)
+            return kNone;
+        if (!slab_ok(d, id)) {
+            set_status(d.ctl, SVDAG_ERR_CORRUPT);
+            return kNone;
+        }
+        const uint32_t next = __ldcg(slab_ptr(d, id) + 7);
+        const unsigned long long want = (((cur >> 32) + 1ull) << 32) | next;
+        const unsigned long long old = atomicCAS(head, cur, want);
+        if (old == cur) {
+            atomicAdd(&d.ctl->freeSlabs[cls], ~0ull); // minus one (two's complement)
+            atomicAdd(&d.ctl->freeBytes, 0ull - slab_bytes(cls + 2));
+            return id;
+        }
+        cur = old;
+    }
+    return kNone;
+}
+
+// Pushes a chain of `count` free slabs (first .. last, linked through header word 7) on the free
+// list of size class `cls`.
+__device__ __forceinline__ void push_free_chain(const DevDag& d, uint32_t cls, uint32_t first, uint32_t last, uint32_t count)
+{
+    unsigned long long* head = &d.ctl->freeHead[cls];
+    unsigned long long cur = __ldcg(head);
+    for (uint32_t tries = 0; tries < (1u << 20); ++tries) {
+        slab_ptr(d, last)[7] = (uint32_t)cur;
+        __threadfence(); // the link is visible before the slab is reachable from the head
+        const unsigned long long want = (((cur >> 32) + 1ull) << 32) | first;
+        const unsigned long long old = atomicCAS(head, cur, want);
+        if (old == cur) {
+            atomicAdd(&d.ctl->freeSlabs[cls], (unsigned long long)count);
+            atomicAdd(&d.ctl->freeBytes, (unsigned long long)count * slab_bytes(cls + 2));
+            return;
+        }
+        cur = old;
+    }
+    set_status(d.ctl, SVDAG_ERR_TIMEOUT); // the chain stays allocated (lost to reuse, never corrupt)
+}
+
 // Allocates and initialises an overflow slab of class k (a header and a cleared body); returns its
-// header id, or kNone when a region is full.
+// header id, or kNone when a region is full. `recycle`: try the free list of class k first.
 template <int G>
-__device__ __forceinline__ uint32_t alloc_slab(const Grp<G>& g, const DevDag& d, uint32_t k)
+__device__ __forceinline__ uint32_t alloc_slab(const Grp<G>& g, const DevDag& d, uint32_t k, uint32_t recycle)
 {
     uint32_t id = kNone, body = 0;
-    if (g.lane == 0) {
+    if (g.lane == 0 && recycle) {
+        id = pop_free_slab(d, k - 2u);
+        if (id != kNone) {
+            body = __ldcg(slab_ptr(d, id) + 6); // a free slab keeps its body
+            if (2ull * body + body_words(k) > d.itemWords) {
+                set_status(d.ctl, SVDAG_ERR_CORRUPT);
+                id = kNone; // dropped from the list: never handed out
+            }
+        }
+    }
+    if (g.lane == 0 && id == kNone) {
         // The groups of a warp that allocate at the same time share one atomic per region (the
         // bump pointers are single addresses every allocation in the launch goes through).
         namespace cg = cooperative_groups;
@@ -486,6 +576,26 @@ struct Spare {
     uint32_t slab = kNone;
     uint32_t k = 0;
 };
+
+// Gives an unused spare back: a level table's goes on its class's free list; other tables' spares
+// stay allocated (their space comes back when the bump pointers are rewound or never).
+template <int G>
+__device__ __forceinline__ void release_spare(const Grp<G>& g, const DevDag& d, const DevTable& t, Spare& spare)
+{
+    if (spare.slab != kNone && t.recycle && g.lane == 0)
+        push_free_chain(d, spare.k - 2u, spare.slab, spare.slab, 1);
+    spare.slab = kNone;
+}
+// A spare of another size class than `k` is released before a new one is allocated.
+template <int G>
+__device__ __forceinline__ void take_spare(const Grp<G>& g, const DevDag& d, const DevTable& t, Spare& spare, uint32_t k)
+{
+    if (spare.slab == kNone || spare.k != k) {
+        release_spare<G>(g, d, t, spare);
+        spare.slab = alloc_slab<G>(g, d, k, t.recycle);
+        spare.k = k;
+    }
+}
 
 constexpr uint32_t kMaxChain = 1u << 14; // bound on chain walks (16K slabs in one bucket only happens on a corrupt chain)
 
@@ -587,10 +697,7 @@ __device__ __forceinline__ uint32_t table_add(const Grp<G>& g, const DevDag& d, 
             return item;
         }
         if (next == kEnd) {
-            if (spare.slab == kNone || spare.k != key.n) {
-                spare.slab = alloc_slab<G>(g, d, key.n); // a spare of another class is abandoned
-                spare.k = key.n;
-            }
+            take_spare<G>(g, d, t, spare, key.n);
             if (spare.slab == kNone)
                 return kNone;
             uint32_t linked = kNone;
@@ -627,6 +734,7 @@ __device__ __forceinline__ uint32_t table_find_or_insert(const Grp<G>& g, const 
     const uint32_t tag = tag_of(key.hb);
     uint32_t slab = first_slab(t, cls, key.ha);
     uint32_t tail = slab, tailEmpty = 0, tailBody = 0;
+    uint32_t open = kNone, openEmpty = 0, openBody = 0; // first slab of the chain with a free slot
     HdrSnap<G> snap;
     for (uint32_t steps = 0;; ++steps) {
         if (steps >= kMaxChain) {
@@ -645,6 +753,11 @@ __device__ __forceinline__ uint32_t table_find_or_insert(const Grp<G>& g, const 
         tail = slab;
         tailEmpty = empty;
         tailBody = body;
+        if (open == kNone && empty) {
+            open = slab;
+            openEmpty = empty;
+            openBody = body;
+        }
         if (next == kEnd)
             break;
         if (!slab_ok(d, next)) {
@@ -653,12 +766,16 @@ __device__ __forceinline__ uint32_t table_find_or_insert(const Grp<G>& g, const 
         }
         slab = next;
     }
-    // Not present: claim a slot at the tail of the chain (earlier slabs were full or hold other keys).
-    slab = tail;
-    uint32_t empty = tailEmpty, body = tailBody;
+    // Not present: claim a slot in the first slab that had one free (slots freed by garbage
+    // collection are reused before the chain grows), else at the tail of the chain.
+    const bool atTail = open == kNone || open == tail;
+    slab = atTail ? tail : open;
+    uint32_t empty = atTail ? tailEmpty : openEmpty, body = atTail ? tailBody : openBody;
+    bool snapValid = atTail; // `snap` holds the tag words of the tail, the last slab probed
     for (uint32_t steps = 0; steps < kMaxChain; ++steps) {
         uint32_t s = 0;
-        const uint32_t item = claim_in_slab<G>(g, d, slab, body, empty, tag, key.n, true, s, key.ha >> 8, &snap);
+        const uint32_t item = claim_in_slab<G>(g, d, slab, body, empty, tag, key.n, true, s, key.ha >> 8, snapValid ? &snap : nullptr);
+        snapValid = true;
         if (item != kNone) {
             write_item<G>(g, handle_ptr(d, item), key);
             if constexpr (G == 1)
@@ -676,10 +793,7 @@ __device__ __forceinline__ uint32_t table_find_or_insert(const Grp<G>& g, const 
         if (empty)
             continue; // a slot was freed up meanwhile (cannot happen during edits, kept for safety)
         if (next == kEnd) {
-            if (spare.slab == kNone || spare.k != key.n) {
-                spare.slab = alloc_slab<G>(g, d, key.n); // a spare of another class is abandoned
-                spare.k = key.n;
-            }
+            take_spare<G>(g, d, t, spare, key.n);
             if (spare.slab == kNone)
                 return kNone;
             uint32_t linked = kNone;

@@ -915,6 +915,7 @@ __device__ void ph_merge_level(const DevDag& d, uint32_t level, char* scratch)
         handle[i] = table_find_or_insert<1>(g, d, t, key, spare, ins);
         added += ins ? 1u : 0u;
     }
+    release_spare<1>(g, d, t, spare);
     if (full)
         atomicAdd(&E.ffCount[level], full);
     if (reps)
@@ -952,6 +953,7 @@ __device__ void ph_insert_level(const DevDag& d, const DevTable& t, uint32_t lev
             added += ins ? 1u : 0u;
         }
     }
+    release_spare<G>(g, d, t, spare);
     if (added)
         atomicAdd(&E.added, (unsigned long long)added);
 }
@@ -1542,7 +1544,7 @@ svdag_status build_scene_untiled(svdag_ctx* ctx, const DevEditor& ed, cudaStream
             buckets[c] = (uint32_t)std::max<unsigned long long>(1, (items + ctx->loadFactor - 1) / ctx->loadFactor);
         }
         svdag_table& t = ctx->levelTables[level];
-        SVDAG_TRY(alloc_table(ctx, &t, level == (int)LL ? SVDAG_KIND_LEAF : SVDAG_KIND_NODE, buckets, s));
+        SVDAG_TRY(alloc_table(ctx, &t, level == (int)LL ? SVDAG_KIND_LEAF : SVDAG_KIND_NODE, buckets, s, true));
         t.level = level;
         SVDAG_TRY(upload_tables(ctx, s));
         SVDAG_TRY(insert_canonical(ctx, (uint32_t)level, s));

@@ -69,11 +69,22 @@ inline svdag_status cuda_status(cudaError_t e)
 
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// Item and header region bytes in use: what the bump pointers handed out (a failed allocation may
+// leave a pointer past the end), less the slabs on the free lists.
+inline unsigned long long used_region_bytes(const svdag_ctx* ctx, unsigned long long itemTop, unsigned long long headerTop,
+    unsigned long long freeBytes)
+{
+    const unsigned long long used = (itemTop < ctx->itemWords ? itemTop : ctx->itemWords) * 4ull
+        + (headerTop < ctx->headerCount ? headerTop : ctx->headerCount) * 32ull;
+    return used > freeBytes ? used - freeBytes : 0ull;
+}
+
 // Number of resident-CTA-sized grid for grid-stride kernels: a multiple of the SM count.
 int grid_for(const svdag_ctx* ctx, unsigned long long work, int threadsPerBlock, int blocksPerSm = 8);
 
 // Table management (svdag_tables.cu).
-svdag_status alloc_table(svdag_ctx* ctx, svdag_table* t, uint32_t kind, const uint32_t* bucketsPerClass, cudaStream_t s);
+// `recycle`: a level table, whose overflow slabs come from and go back to the free lists.
+svdag_status alloc_table(svdag_ctx* ctx, svdag_table* t, uint32_t kind, const uint32_t* bucketsPerClass, cudaStream_t s, bool recycle = false);
 svdag_status ensure_level_tables(svdag_ctx* ctx, cudaStream_t s);
 svdag_status insert_canonical(svdag_ctx* ctx, uint32_t level, cudaStream_t s);
 svdag_status upload_tables(svdag_ctx* ctx, cudaStream_t s);

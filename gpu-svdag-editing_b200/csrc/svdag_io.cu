@@ -138,7 +138,7 @@ svdag_status load_snapshot(svdag_ctx* ctx, const uint32_t* words, const uint64_t
         for (uint32_t c = 0; c < kNumClasses; ++c)
             buckets[c] = (uint32_t)std::max<unsigned long long>(1, (perClass[c] + SVDAG_NUM_MATERIALS + ctx->loadFactor - 1) / ctx->loadFactor);
         svdag_table& t = ctx->levelTables[level];
-        SVDAG_TRY(alloc_table(ctx, &t, leaf ? SVDAG_KIND_LEAF : SVDAG_KIND_NODE, buckets, s));
+        SVDAG_TRY(alloc_table(ctx, &t, leaf ? SVDAG_KIND_LEAF : SVDAG_KIND_NODE, buckets, s, true));
         t.level = (uint32_t)level;
         SVDAG_TRY(upload_tables(ctx, s));
         SVDAG_TRY(insert_canonical(ctx, (uint32_t)level, s));

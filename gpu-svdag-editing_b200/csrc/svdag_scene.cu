@@ -225,7 +225,7 @@ struct TiledBuild {
         const uint32_t LL = ctx->cfg.levels - 2;
         for (int level = (int)LL; level >= 0; --level) {
             svdag_table& t = ctx->levelTables[level];
-            SVDAG_TRY(alloc_table(ctx, &t, level == (int)LL ? SVDAG_KIND_LEAF : SVDAG_KIND_NODE, buckets[level].data(), s));
+            SVDAG_TRY(alloc_table(ctx, &t, level == (int)LL ? SVDAG_KIND_LEAF : SVDAG_KIND_NODE, buckets[level].data(), s, true));
             t.level = level;
             SVDAG_TRY(insert_canonical(ctx, (uint32_t)level, s));
         }

@@ -1,8 +1,9 @@
 // svdag_server.cu - the serving form: a request loop on its own host thread with continuous batching
 // of edits into batched launches on one stream, frames on a second stream (one in flight at a time,
 // each behind every batch launched before it, so the GPU renders while the next batch edits),
-// admission by reserved item-region memory, and a timed replay driver. SVDAG_SERVE_PLAIN turns the
-// loop into the per-edit baseline (one request at a time: an edit, then its frame, synchronously).
+// admission by reserved item-region memory, garbage collection in the loop when that memory fills,
+// and a timed replay driver. SVDAG_SERVE_PLAIN turns the loop into the per-edit baseline (one
+// request at a time: an edit, then its frame, synchronously).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -72,7 +73,7 @@ struct svdag_server {
     uint32_t nslots = 0;
     size_t slotBytes = 0;
     std::vector<EditRecord*> hostRecords; // pinned, one array per slot
-    std::vector<unsigned long long*> hostTop; // pinned item-region top after each launch
+    std::vector<MemSnapshot*> hostMem; // pinned head of the control block after each launch
     std::vector<uint32_t*> hostRoot; // pinned root after each undo/redo launch
     std::vector<cudaEvent_t> events; // one per slot
     cudaEvent_t frameDone = nullptr;
@@ -82,7 +83,14 @@ struct svdag_server {
     bool haveFrame = false; // `hits` holds a frame of lastFrame's camera
     std::atomic<unsigned long long> framesWhole { 0 }, framesIncremental { 0 }, frameBytesToHost { 0 };
     unsigned long long capBytes = 0;
-    unsigned long long usedBytes = 0; // item region in use after the last finished launch
+    std::atomic<unsigned long long> usedBytes { 0 }; // item and header region in use after the last finished launch
+    unsigned long long gcThreshold = 0; // configured threshold
+    unsigned long long gcTrigger = 0; // bytes in use that start the next collection
+    bool dirtySinceGc = true; // a launch finished since the last collection (one could free something)
+    bool gcWanted = false; // admit nothing until the GPU is idle, then collect
+    // Memory counters: written by the worker thread, read by svdag_server_memory_stats.
+    std::atomic<unsigned long long> gcRuns { 0 }, gcFreedBytes { 0 }, rejectedEdits { 0 }, failedEdits { 0 };
+    std::atomic<double> gcSeconds { 0.0 };
 
     std::mutex m;
     std::condition_variable cv, doneCv;
@@ -103,6 +111,30 @@ struct svdag_server {
     std::thread worker;
 
     bool plain() const { return cfg.flags & SVDAG_SERVE_PLAIN; }
+    bool gcAllowed() const { return !(cfg.flags & SVDAG_SERVE_NO_GC); }
+
+    // A collection that keeps every undo/redo root (nothing of the context may be on the GPU), then
+    // the bytes in use it left. Runs on the worker thread; the loop admits nothing meanwhile.
+    svdag_status collect_garbage()
+    {
+        const Clock::time_point a = Clock::now();
+        const svdag_status st = svdag_gc_keep_history(ctx, stream);
+        MemSnapshot ms {};
+        SVDAG_CUDA(cudaMemcpyAsync(&ms, &ctx->ctl->itemTop, sizeof(ms), cudaMemcpyDeviceToHost, stream));
+        SVDAG_CUDA(cudaStreamSynchronize(stream));
+        const unsigned long long before = usedBytes;
+        usedBytes = used_region_bytes(ctx, ms.itemTop, ms.headerTop, ms.freeBytes);
+        gcSeconds.store(gcSeconds.load() + std::chrono::duration<double>(Clock::now() - a).count());
+        ++gcRuns;
+        gcFreedBytes += before > usedBytes ? before - usedBytes : 0ull;
+        // The next collection waits until a quarter of the room left above what this one kept has
+        // filled, so that live data near the threshold does not start a collection per launch.
+        const unsigned long long kept = usedBytes;
+        gcTrigger = std::max(gcThreshold, kept < capBytes ? kept + (capBytes - kept) / 4 : capBytes);
+        dirtySinceGc = false;
+        gcWanted = false;
+        return st;
+    }
 
     svdag_status launch_batch(std::vector<Request>& reqs, unsigned long long reserved)
     {
@@ -114,7 +146,7 @@ struct svdag_server {
         if (reqs.size() == 1 && reqs[0].kind >= 2) { // an undo or redo is a launch of its own
             SVDAG_TRY(reqs[0].kind == 2 ? svdag_undo(ctx, stream) : svdag_redo(ctx, stream));
             SVDAG_CUDA(cudaMemcpyAsync(hostRoot[b.slot], &ctx->ctl->root, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
-            SVDAG_CUDA(cudaMemcpyAsync(hostTop[b.slot], &ctx->ctl->itemTop, sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream));
+            SVDAG_CUDA(cudaMemcpyAsync(hostMem[b.slot], &ctx->ctl->itemTop, sizeof(MemSnapshot), cudaMemcpyDeviceToHost, stream));
             SVDAG_CUDA(cudaEventRecord(b.done, stream));
             b.reqs = std::move(reqs);
             batches.push_back(std::move(b));
@@ -132,7 +164,7 @@ struct svdag_server {
         const size_t edBytes = align256(eds.size() * sizeof(DevEditor));
         b.records.resize(eds.size());
         SVDAG_CUDA(cudaMemcpyAsync(hostRecords[b.slot], region + edBytes, eds.size() * sizeof(EditRecord), cudaMemcpyDeviceToHost, stream));
-        SVDAG_CUDA(cudaMemcpyAsync(hostTop[b.slot], &ctx->ctl->itemTop, sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream));
+        SVDAG_CUDA(cudaMemcpyAsync(hostMem[b.slot], &ctx->ctl->itemTop, sizeof(MemSnapshot), cudaMemcpyDeviceToHost, stream));
         SVDAG_CUDA(cudaEventRecord(b.done, stream));
         b.reqs = std::move(reqs);
         batches.push_back(std::move(b));
@@ -235,7 +267,11 @@ struct svdag_server {
         std::memcpy(b.records.data(), hostRecords[b.slot], b.records.size() * sizeof(EditRecord));
         if (b.records.empty())
             b.root = *hostRoot[b.slot];
-        usedBytes = *hostTop[b.slot] * 4ull;
+        const MemSnapshot& ms = *hostMem[b.slot];
+        usedBytes = used_region_bytes(ctx, ms.itemTop, ms.headerTop, ms.freeBytes);
+        for (size_t i = 0; i < b.lastRecord.size(); ++i)
+            failedEdits += b.records[b.lastRecord[i]].status != 0 ? 1u : 0u;
+        dirtySinceGc = true;
         b.finished = true;
     }
 
@@ -344,6 +380,14 @@ struct svdag_server {
             }
             std::vector<Request> one { r };
             svdag_status st = SVDAG_OK;
+            if (r.kind == 0 && gcAllowed() && dirtySinceGc && (usedBytes > gcTrigger || usedBytes + r.reserve > capBytes))
+                collect_garbage(); // a failed collection frees nothing; the edit is then judged as it is
+            if (r.kind == 0 && usedBytes + r.reserve > capBytes) {
+                std::lock_guard<std::mutex> lk(m);
+                ++rejectedEdits;
+                fail_requests(one, SVDAG_ERR_OOM);
+                continue;
+            }
             if (r.kind != 1) // an edit, undo or redo
                 st = launch_batch(one, r.reserve);
             else
@@ -379,13 +423,21 @@ struct svdag_server {
                     finish_batch(b);
             if (frameActive && cudaEventQuery(frameDone) == cudaSuccess)
                 complete_frame();
+            // Memory: past the threshold, admit nothing until the launches and the frame in flight
+            // are done, then collect (every undo/redo root kept).
+            if (gcAllowed() && dirtySinceGc && usedBytes > gcTrigger)
+                gcWanted = true;
+            if (gcWanted && unfinished() == 0 && !frameActive) {
+                collect_garbage(); // a failed collection frees nothing; admission then judges edits as they are
+                continue;
+            }
             std::vector<Request> take;
             unsigned long long reserve = 0;
             {
                 std::unique_lock<std::mutex> lk(m);
                 if (stop && queue.empty() && batches.empty() && !frameActive && pendingFrames.empty())
                     break;
-                const bool canLaunch = unfinished() < maxInflight;
+                const bool canLaunch = unfinished() < maxInflight && !gcWanted;
                 const unsigned long long inUse = usedBytes + reserved_in_flight();
                 uint32_t edits = 0;
                 for (auto it = queue.begin(); it != queue.end();) {
@@ -403,9 +455,21 @@ struct svdag_server {
                     }
                     if (!canLaunch || edits == maxBatch)
                         break;
-                    const bool first = unfinished() == 0 && edits == 0; // always make progress
-                    if (!first && inUse + reserve + it->reserve > capBytes)
+                    if (inUse + reserve + it->reserve > capBytes) {
+                        // Does not fit. With launches in flight, wait for them; with nothing in flight
+                        // only a collection can make room, and after one the edit fails up front.
+                        if (edits == 0 && unfinished() == 0) {
+                            if (gcAllowed() && dirtySinceGc) {
+                                gcWanted = true;
+                            } else {
+                                ++rejectedEdits;
+                                fail_requests({ *it }, SVDAG_ERR_OOM);
+                                it = queue.erase(it);
+                                continue;
+                            }
+                        }
                         break;
+                    }
                     reserve += it->reserve;
                     ++edits;
                     take.push_back(*it);
@@ -422,8 +486,9 @@ struct svdag_server {
                 launched = true;
             }
             // One frame in flight at a time, behind everything launched so far.
+            // (While a collection waits, frames run only to show launched edits.)
             const bool uncovered = !batches.empty() && batches.back().launch >= covered;
-            if (!frameActive && (uncovered || !pendingFrames.empty())) {
+            if (!frameActive && (uncovered || (!pendingFrames.empty() && !gcWanted))) {
                 if (launch_frame() != SVDAG_OK) {
                     fail_everything(SVDAG_ERR_CUDA);
                     continue;
@@ -477,23 +542,25 @@ svdag_status svdag_server_create(svdag_ctx* ctx, const svdag_server_config* conf
     const size_t maxRecords = s->slotBytes / (sizeof(DevEditor) + sizeof(EditRecord));
     for (uint32_t i = 0; i < s->nslots; ++i) {
         EditRecord* r = nullptr;
-        unsigned long long* t = nullptr;
+        MemSnapshot* t = nullptr;
         uint32_t* root = nullptr;
         cudaEvent_t ev = nullptr;
         fail(cudaMallocHost(&r, maxRecords * sizeof(EditRecord)));
-        fail(cudaMallocHost(&t, sizeof(unsigned long long)));
+        fail(cudaMallocHost(&t, sizeof(MemSnapshot)));
         fail(cudaMallocHost(&root, sizeof(uint32_t)));
         fail(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
         s->hostRecords.push_back(r);
-        s->hostTop.push_back(t);
+        s->hostMem.push_back(t);
         s->hostRoot.push_back(root);
         s->events.push_back(ev);
     }
     {
-        unsigned long long top = 0;
-        fail(cudaMemcpy(&top, &ctx->ctl->itemTop, sizeof(top), cudaMemcpyDeviceToHost));
-        s->usedBytes = top * 4ull;
+        MemSnapshot ms {};
+        fail(cudaMemcpy(&ms, &ctx->ctl->itemTop, sizeof(ms), cudaMemcpyDeviceToHost));
+        s->usedBytes = used_region_bytes(ctx, ms.itemTop, ms.headerTop, ms.freeBytes);
     }
+    s->gcThreshold = config->gc_threshold_bytes ? config->gc_threshold_bytes : s->capBytes - s->capBytes / 8;
+    s->gcTrigger = s->gcThreshold;
     if (st != SVDAG_OK) {
         s->stop = true;
         svdag_server_destroy(s);
@@ -526,7 +593,7 @@ svdag_status svdag_server_destroy(svdag_server* s)
         cudaStreamSynchronize(s->frameStream);
     for (auto* r : s->hostRecords)
         cudaFreeHost(r);
-    for (auto* t : s->hostTop)
+    for (auto* t : s->hostMem)
         cudaFreeHost(t);
     for (auto* r : s->hostRoot)
         cudaFreeHost(r);
@@ -625,6 +692,23 @@ svdag_status svdag_server_counters(svdag_server* s, uint64_t* whole, uint64_t* i
         *incremental = s->framesIncremental.load();
     if (bytesToHost)
         *bytesToHost = s->frameBytesToHost.load();
+    return SVDAG_OK;
+}
+
+svdag_status svdag_server_memory_stats(svdag_server* s, svdag_server_memory* out)
+{
+    if (!s || !out)
+        return SVDAG_ERR_INVALID;
+    svdag_server_memory r {};
+    r.used_bytes = s->usedBytes.load();
+    r.cap_bytes = s->capBytes;
+    r.gc_threshold_bytes = s->gcThreshold;
+    r.gc_runs = s->gcRuns.load();
+    r.gc_freed_bytes = s->gcFreedBytes.load();
+    r.gc_seconds = s->gcSeconds.load();
+    r.rejected_edits = s->rejectedEdits.load();
+    r.failed_edits = s->failedEdits.load();
+    *out = r;
     return SVDAG_OK;
 }
 

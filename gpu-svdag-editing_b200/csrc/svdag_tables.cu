@@ -53,13 +53,14 @@ __global__ void k_init_bucket_headers(DevDag d, DevTable t)
 
 // Reserves a table's bucket headers at the top of the header region and its first slab bodies at the
 // top of the item region, clears them and links each header to its body.
-svdag_status alloc_table(svdag_ctx* ctx, svdag_table* t, uint32_t kind, const uint32_t* bucketsPerClass, cudaStream_t s)
+svdag_status alloc_table(svdag_ctx* ctx, svdag_table* t, uint32_t kind, const uint32_t* bucketsPerClass, cudaStream_t s, bool recycle)
 {
     unsigned long long tops[2] = { 0, 0 }; // itemTop (words), headerTop (headers)
     SVDAG_CUDA(cudaMemcpyAsync(tops, &ctx->ctl->itemTop, sizeof(tops), cudaMemcpyDeviceToHost, s));
     SVDAG_CUDA(cudaStreamSynchronize(s));
     DevTable dev {};
     dev.kind = kind;
+    dev.recycle = recycle ? 1u : 0u;
     unsigned long long words = 0, headers = 0, buckets = 0;
     for (uint32_t c = 0; c < kNumClasses; ++c) {
         dev.numBuckets[c] = bucketsPerClass[c];
@@ -108,6 +109,7 @@ __global__ void k_insert_canonical(DevDag d, DevTable t, uint32_t level)
         bool inserted;
         d.ctl->fullyFilled[level][m] = table_find_or_insert<1>(g, d, t, key, spare, inserted);
     }
+    release_spare<1>(g, d, t, spare);
 }
 
 svdag_status insert_canonical(svdag_ctx* ctx, uint32_t level, cudaStream_t s)
@@ -137,7 +139,7 @@ svdag_status ensure_level_tables(svdag_ctx* ctx, cudaStream_t s)
         uint32_t buckets[kNumClasses];
         for (uint32_t c = 0; c < kNumClasses; ++c)
             buckets[c] = (uint32_t)std::max<unsigned long long>(1, expect / (4ull * ctx->loadFactor));
-        SVDAG_TRY(alloc_table(ctx, &t, level == (int)leaf ? SVDAG_KIND_LEAF : SVDAG_KIND_NODE, buckets, s));
+        SVDAG_TRY(alloc_table(ctx, &t, level == (int)leaf ? SVDAG_KIND_LEAF : SVDAG_KIND_NODE, buckets, s, true));
         t.level = level;
         SVDAG_TRY(insert_canonical(ctx, (uint32_t)level, s));
         created = true;
@@ -196,6 +198,7 @@ __global__ void __launch_bounds__(256) k_table_op(DevDag d, DevTable t, const ui
         if (g.lane == 0)
             out[i] = h;
     }
+    release_spare<G>(g, d, t, spare);
 }
 
 // Batch dedup into an open-addressing scratch table of 64-bit entries (tag hash << 32 | index+1).
@@ -504,6 +507,12 @@ extern "C" svdag_status svdag_table_find_or_add_static(svdag_table* t, const uin
     if (!n)
         return SVDAG_OK;
     svdag_ctx* ctx = t->ctx;
+    // The kernels run on the calling thread's current device; the fixed array's address is that of
+    // the table's device, so the two must be the same.
+    int current = -1;
+    SVDAG_CUDA(cudaGetDevice(&current));
+    if (current != ctx->device)
+        return SVDAG_ERR_INVALID;
     unsigned char* base = nullptr;
     SVDAG_TRY(static_scratch(ctx->device, &base));
     cudaStream_t s = as_stream(stream);

@@ -85,7 +85,15 @@ class TraceParams(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("max_batch", C.c_uint32), ("max_inflight", C.c_uint32), ("memory_cap_bytes", C.c_uint64),
-                ("frame", TraceParams), ("flags", C.c_uint32), ("reserved", C.c_uint32)]
+                ("frame", TraceParams), ("flags", C.c_uint32), ("reserved", C.c_uint32),
+                ("gc_threshold_bytes", C.c_uint64)]
+
+
+class ServerMemory(C.Structure):
+    """svdag_server_memory: the serving loop's memory accounting and in-loop collections."""
+    _fields_ = [("used_bytes", C.c_uint64), ("cap_bytes", C.c_uint64), ("gc_threshold_bytes", C.c_uint64),
+                ("gc_runs", C.c_uint64), ("gc_freed_bytes", C.c_uint64), ("gc_seconds", C.c_double),
+                ("rejected_edits", C.c_uint64), ("failed_edits", C.c_uint64)]
 
 
 class RequestResult(C.Structure):
@@ -107,7 +115,7 @@ RESULT_DTYPE = np.dtype([("ticket", "<u8"), ("kind", "<u4"), ("status", "<u4"), 
                          ("launch", "<u4"), ("edited_voxels", "<u8"), ("submit_s", "<f8"), ("visible_s", "<f8")])
 assert RESULT_DTYPE.itemsize == C.sizeof(RequestResult) == 48
 
-SERVE_PLAIN, SERVE_COPY_FRAMES, SERVE_FULL_FRAMES = 1, 2, 4
+SERVE_PLAIN, SERVE_COPY_FRAMES, SERVE_FULL_FRAMES, SERVE_NO_GC = 1, 2, 4, 8
 
 
 class ShadeParams(C.Structure):
@@ -154,7 +162,8 @@ class Stats(C.Structure):
                 ("item_region_bytes", C.c_uint64), ("item_region_used_bytes", C.c_uint64),
                 ("scratch_bytes", C.c_uint64), ("scratch_high_water_bytes", C.c_uint64),
                 ("level_items", C.c_uint64 * MAX_LEVELS), ("level_buckets", C.c_uint64 * MAX_LEVELS),
-                ("undo_count", C.c_uint32), ("redo_count", C.c_uint32)]
+                ("undo_count", C.c_uint32), ("redo_count", C.c_uint32), ("free_list_bytes", C.c_uint64),
+                ("free_list_slabs", C.c_uint64), ("gc_freed_items", C.c_uint64), ("gc_freed_slabs", C.c_uint64)]
 
 
 class TableStats(C.Structure):
@@ -191,6 +200,7 @@ _PROTOS = {
     "svdag_undo": [_P, _P],
     "svdag_redo": [_P, _P],
     "svdag_gc": [_P, _P],
+    "svdag_gc_keep_history": [_P, _P],
     "svdag_get_root": [_P, C.POINTER(_U32), _P],
     "svdag_trace_primary": [_P, C.POINTER(TraceParams), _P, _P],
     "svdag_sample_voxels": [_P, _P, _U32, _P, _P],
@@ -226,6 +236,7 @@ _PROTOS = {
     "svdag_poll": [_P, _U64, C.c_int, C.POINTER(RequestResult)],
     "svdag_server_frame": [_P, _P, _U64],
     "svdag_server_counters": [_P, C.POINTER(_U64), C.POINTER(_U64), C.POINTER(_U64)],
+    "svdag_server_memory_stats": [_P, C.POINTER(ServerMemory)],
     "svdag_server_replay": [_P, C.POINTER(Edit), _P, _U32, _P, _U32, _P],
     "svdag_submit_undo": [_P, C.c_int, C.POINTER(_U64)],
     "svdag_replay_parse": [C.c_char_p, _U64, C.c_float, _P, _U64, C.POINTER(_U64), C.POINTER(_U64)],
@@ -464,8 +475,13 @@ class MyGPUHashDAG:
     def redo(self, stream=None):
         _check(lib().svdag_redo(self.h, stream_ptr(stream)), "svdag_redo")
 
-    def garbage_collect(self, stream=None):
-        _check(lib().svdag_gc(self.h, stream_ptr(stream)), "svdag_gc")
+    def garbage_collect(self, stream=None, keep_history: bool = False):
+        """MyGPUHashDAGUndoRedo::garbageCollect: frees what the root cannot reach and clears the
+        history; keep_history=True marks from every undo/redo root too and keeps the history."""
+        if keep_history:
+            _check(lib().svdag_gc_keep_history(self.h, stream_ptr(stream)), "svdag_gc_keep_history")
+        else:
+            _check(lib().svdag_gc(self.h, stream_ptr(stream)), "svdag_gc")
 
     def stats(self, stream=None) -> Stats:
         s = Stats()
@@ -869,12 +885,14 @@ class Server:
     plain=True it is the per-edit baseline: one request at a time, each edit followed by a frame."""
 
     def __init__(self, dag: MyGPUHashDAG, frame: TraceParams, max_batch: int = 256, max_inflight: int = 2,
-                 memory_cap_bytes: int = 0, plain: bool = False, copy_frames: bool = False, full_frames: bool = False):
+                 memory_cap_bytes: int = 0, plain: bool = False, copy_frames: bool = False, full_frames: bool = False,
+                 gc_threshold_bytes: int = 0, gc: bool = True):
         self.dag = dag
         self.frame_params = frame
-        flags = (SERVE_PLAIN if plain else 0) | (SERVE_COPY_FRAMES if copy_frames else 0) | (SERVE_FULL_FRAMES if full_frames else 0)
+        flags = ((SERVE_PLAIN if plain else 0) | (SERVE_COPY_FRAMES if copy_frames else 0)
+                 | (SERVE_FULL_FRAMES if full_frames else 0) | (0 if gc else SERVE_NO_GC))
         cfg = ServerConfig(max_batch=max_batch, max_inflight=max_inflight, memory_cap_bytes=memory_cap_bytes,
-                           frame=frame, flags=flags)
+                           frame=frame, flags=flags, gc_threshold_bytes=gc_threshold_bytes)
         h = C.c_void_p()
         _check(lib().svdag_server_create(dag.h, C.byref(cfg), C.byref(h)), "svdag_server_create")
         self.h = h
@@ -922,6 +940,12 @@ class Server:
         a, b, c = C.c_uint64(), C.c_uint64(), C.c_uint64()
         _check(lib().svdag_server_counters(self.h, C.byref(a), C.byref(b), C.byref(c)), "svdag_server_counters")
         return {"frames_whole": a.value, "frames_incremental": b.value, "frame_bytes_to_host": c.value}
+
+    def memory(self) -> dict:
+        """Bytes in use, cap and threshold, in-loop collections, edits rejected and failed."""
+        m = ServerMemory()
+        _check(lib().svdag_server_memory_stats(self.h, C.byref(m)), "svdag_server_memory_stats")
+        return {f: getattr(m, f) for f, _ in ServerMemory._fields_}
 
     def submit_undo(self, redo: bool = False) -> int:
         t = C.c_uint64()

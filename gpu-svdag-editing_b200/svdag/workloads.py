@@ -2,7 +2,9 @@
 
 The reference measures on scene files and recorded edit replays that are not available here; these
 seeded procedural stand-ins have the stated depths, sizes and edit mixes. Edits are placed on the
-terrain surface with the library's own height function (svdag_scene_height).
+terrain surface with the library's own height function (svdag_scene_height, host code) unless the
+caller passes another `height(levels, x, z, terrain)` with the same values (the CPU baseline passes
+the oracle's, so that it runs without the CUDA library).
 """
 import math
 
@@ -80,6 +82,10 @@ def c2_edits(levels=C2_LEVELS, terrain=C2_TERRAIN):
     return [carve, copy, paint]
 
 
+def _library_height(levels, x, z, terrain):
+    return scene_height(levels, x, z, **terrain)
+
+
 def _log_uniform(rng, lo, hi):
     return float(math.exp(rng.uniform(math.log(lo), math.log(hi))))
 
@@ -110,11 +116,12 @@ def c3_edits(n=256, seed=3, levels=C2_LEVELS, terrain=C2_TERRAIN, rmax=4096.0):
 
 
 def c4_stream(rate, duration_s, seed=4, levels=C2_LEVELS, terrain=C2_TERRAIN, rmax=2048.0, frame_hz=60.0,
-              copy_offset=1024):
+              copy_offset=1024, height=None):
     """Served request stream: edit arrivals Poisson at `rate` per second, mix add / remove / paint /
     copy 35/35/20/10, radius log-uniform in [2, rmax], centres within +-32 voxels of the surface,
     copies moved by up to +-copy_offset in x and z; frame requests every 1/frame_hz s. Returns
     (edit_times, edits, frame_times), times in seconds."""
+    height = height or _library_height
     rng = np.random.default_rng(seed)
     g = 1 << levels
     times, edits = [], []
@@ -124,7 +131,7 @@ def c4_stream(rate, duration_s, seed=4, levels=C2_LEVELS, terrain=C2_TERRAIN, rm
         if t >= duration_s:
             break
         x, z = (int(v) for v in rng.integers(0, g, 2))
-        h = scene_height(levels, x, z, **terrain)
+        h = height(levels, x, z, terrain)
         c = (float(x + rng.integers(-32, 33)), float(h + rng.integers(-32, 33)), float(z + rng.integers(-32, 33)))
         r = float(max(int(_log_uniform(rng, 2.0, rmax)), 2))
         u = rng.uniform()

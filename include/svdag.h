@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define SVDAG_ABI_VERSION 1u
+#define SVDAG_ABI_VERSION 2u
 
 typedef enum svdag_status {
     SVDAG_OK = 0,
@@ -213,9 +213,19 @@ svdag_status svdag_edit_copy(svdag_ctx* ctx, const float src[3], const float dst
 svdag_status svdag_undo(svdag_ctx* ctx, void* stream);
 svdag_status svdag_redo(svdag_ctx* ctx, void* stream);
 /* MyGPUHashDAGUndoRedo::garbageCollect (my_gpu_base_dag.h:66-77) -> MyGPUHashDAG::garbageCollect
- * (my_gpu_hash_dag.cu:365-475): clears the history, marks everything reachable from the root and
- * the canonical fully-filled nodes, frees the rest. Synchronous. */
+ * (my_gpu_hash_dag.cu:365-475) and freeInactiveItems (gpu_hash_table_base.cu:265-374): clears the
+ * history, marks everything reachable from the root and the canonical fully-filled nodes, frees the
+ * rest and puts every overflow slab it leaves empty on the free list of its size class, from which
+ * later overflow allocations are served. Synchronous. The collection first clears the context's
+ * latched status (errors of earlier calls were reported by those calls or their edit records) and
+ * returns only its own errors; when marking fails (SVDAG_ERR_OOM: the scratch arena cannot hold a
+ * level's frontier) nothing is freed and the history is kept. No other work on the context (edits,
+ * traces) may run while it does. */
 svdag_status svdag_gc(svdag_ctx* ctx, void* stream);
+/* MyGPUHashDAG::garbageCollect(activeRootNodes) (my_gpu_hash_dag.cu:373-463) with the active roots
+ * = the current root and every root of the undo and redo history: the same collection as svdag_gc,
+ * but undo and redo keep working afterwards. The serving loop runs it when its memory fills. */
+svdag_status svdag_gc_keep_history(svdag_ctx* ctx, void* stream);
 /* MyGPUHashDAG::get_first_node_index (my_gpu_hash_dag.h:290-293); synchronises `stream`. */
 svdag_status svdag_get_root(svdag_ctx* ctx, uint32_t* out_root, void* stream);
 
@@ -318,7 +328,8 @@ svdag_status svdag_table_find_or_add(svdag_table* table, const uint32_t* keys_de
  * The first call on a device looks up the array's address (with that device made current), so make
  * that first call before any stream capture. All calls share the one array: calls whose work
  * overlaps on the GPU (different streams, or different contexts on the same device) race on it and
- * must be serialised by the caller. Results are the same as svdag_table_find_or_add's. */
+ * must be serialised by the caller. The calling thread's current device must be the table's device
+ * (else SVDAG_ERR_INVALID). Results are the same as svdag_table_find_or_add's. */
 svdag_status svdag_table_find_or_add_static(svdag_table* table, const uint32_t* keys_dev,
     const uint32_t* offsets_dev, uint32_t count, uint64_t total_words, uint32_t* handles_dev,
     uint32_t lanes, void* stream);
@@ -422,6 +433,10 @@ typedef struct svdag_stats {
     uint64_t level_buckets[SVDAG_MAX_LEVELS];
     uint32_t undo_count;
     uint32_t redo_count;
+    uint64_t free_list_bytes; /* slabs on the free lists (counted as not in use above) */
+    uint64_t free_list_slabs;
+    uint64_t gc_freed_items; /* items the last collection freed */
+    uint64_t gc_freed_slabs; /* overflow slabs the last collection put on the free lists */
 } svdag_stats;
 /* MyGPUHashDAG::report (my_gpu_hash_dag.cu:217-230). Synchronises `stream`. */
 svdag_status svdag_get_stats(svdag_ctx* ctx, svdag_stats* out, void* stream);
@@ -498,7 +513,11 @@ svdag_status svdag_set_tuning(svdag_ctx* ctx, const svdag_tuning* tuning);
  * the frame requests pending when it started, and the next batch edits while it renders.
  * An edit is admitted when the item-region bytes in use plus those reserved by admitted, unfinished
  * edits (an upper estimate from the tool's footprint) stay under the memory cap; a queue head that
- * does not fit waits until launches complete. With SVDAG_SERVE_PLAIN the same loop serves one request
+ * does not fit waits until launches complete. Memory is reclaimed in the loop: once the bytes in use
+ * pass gc_threshold_bytes, or when the queue head does not fit with nothing in flight, the loop lets
+ * the launches and the frame in flight finish, then runs svdag_gc_keep_history (the undo history
+ * survives) before it admits more. An edit that does not fit even after a collection fails with
+ * SVDAG_ERR_OOM without being launched. With SVDAG_SERVE_PLAIN the same loop serves one request
  * at a time, synchronously, as the reference's engine does (an edit, then a frame: engine.h:104-163,
  * engine.cpp:627-629): the per-edit baseline. No counterpart in the reference beyond that loop. */
 
@@ -509,6 +528,8 @@ svdag_status svdag_set_tuning(svdag_ctx* ctx, const svdag_tuning* tuning);
  * which a whole frame would reproduce bit for bit); undo and redo, a new camera and the first frame
  * are traced whole. SVDAG_SERVE_PLAIN always traces whole frames, as the reference's loop does. */
 #define SVDAG_SERVE_FULL_FRAMES 4u
+/* Never collect garbage in the loop (edits that do not fit then fail with SVDAG_ERR_OOM). */
+#define SVDAG_SERVE_NO_GC 8u
 
 typedef struct svdag_server_config {
     uint32_t max_batch; /* edits per launch; 0 = 256 */
@@ -517,6 +538,7 @@ typedef struct svdag_server_config {
     svdag_trace_params frame; /* camera and resolution of the frames rendered after each launch */
     uint32_t flags; /* SVDAG_SERVE_* */
     uint32_t reserved;
+    uint64_t gc_threshold_bytes; /* bytes in use that start a collection; 0 = 7/8 of the cap */
 } svdag_server_config;
 
 typedef struct svdag_server svdag_server;
@@ -545,6 +567,18 @@ svdag_status svdag_poll(svdag_server* server, uint64_t ticket, int wait, svdag_r
  * memory (SVDAG_SERVE_COPY_FRAMES). Any pointer may be NULL. No counterpart in the reference. */
 svdag_status svdag_server_counters(svdag_server* server, uint64_t* frames_whole, uint64_t* frames_incremental,
     uint64_t* frame_bytes_to_host);
+/* Memory accounting of the loop. No counterpart in the reference. */
+typedef struct svdag_server_memory {
+    uint64_t used_bytes; /* item and header region in use after the last finished launch (free lists excluded) */
+    uint64_t cap_bytes; /* admission cap */
+    uint64_t gc_threshold_bytes;
+    uint64_t gc_runs; /* collections the loop ran */
+    uint64_t gc_freed_bytes; /* drop of used_bytes over those collections */
+    double gc_seconds; /* host time they took (the loop admits nothing meanwhile) */
+    uint64_t rejected_edits; /* failed with SVDAG_ERR_OOM before launch: they did not fit after a collection */
+    uint64_t failed_edits; /* launched edits whose record reported an error */
+} svdag_server_memory;
+svdag_status svdag_server_memory_stats(svdag_server* server, svdag_server_memory* out);
 /* Copies the most recent frame (SVDAG_SERVE_COPY_FRAMES) to `out` (width * height hits). */
 svdag_status svdag_server_frame(svdag_server* server, svdag_hit* out, uint64_t capacity);
 /* Replays a timed request stream (the reference's replay of recorded edits, replay.h): edit i is

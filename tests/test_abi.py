@@ -26,7 +26,7 @@ def test_every_declared_symbol_is_exported(svdag_lib):
 
 def test_library_loads_and_reports_version(svdag_lib):
     L = svdag_lib.lib()
-    assert L.svdag_abi_version() == 1
+    assert L.svdag_abi_version() == 2
     assert L.svdag_status_string(2).decode().startswith("out of memory")
 
 
@@ -37,7 +37,8 @@ def test_struct_layouts(svdag_lib):
     assert C.sizeof(s.Config) == 40
     assert C.sizeof(s.TraceParams) == 104
     assert C.sizeof(s.TerrainParams) == 32
-    assert C.sizeof(s.ServerConfig) == 128
+    assert C.sizeof(s.ServerConfig) == 136
+    assert C.sizeof(s.ServerMemory) == 64
     assert C.sizeof(s.RequestResult) == 48
     assert C.sizeof(s.Tuning) == 40
     assert C.sizeof(s.AltTuning) == 16  # svdag_alt_tuning
@@ -90,7 +91,8 @@ def test_header_is_c11_and_the_binding_lays_out_structs_alike(svdag_lib, tmp_pat
              "svdag_edit_stats": s.EditStats, "svdag_edit_record": s.EditRecord, "svdag_trace_params": s.TraceParams,
              "svdag_server_config": s.ServerConfig, "svdag_request_result": s.RequestResult,
              "svdag_replay_action": s.ReplayAction, "svdag_shade_params": s.ShadeParams, "svdag_tuning": s.Tuning,
-             "svdag_stats": s.Stats, "svdag_table_stats": s.TableStats, "svdag_alt_tuning": s.AltTuning}
+             "svdag_stats": s.Stats, "svdag_table_stats": s.TableStats, "svdag_alt_tuning": s.AltTuning,
+             "svdag_server_memory": s.ServerMemory}
     lines = ["#include <stddef.h>", '#include "svdag.h"']
     for cname, cls in pairs.items():
         lines.append(f'_Static_assert(sizeof({cname}) == {C.sizeof(cls)}, "size of {cname}");')

@@ -67,7 +67,10 @@ def test_static_find_or_add_matches_arena_version(svdag_lib, lanes):
         [base[i] for i in rng.permutation(np.concatenate([np.arange(30000), np.arange(0, 30000, 2)]))],
         # second call in a row: half already stored, half new, with duplicates
         [k for k in (base[:12000] + node_keys(rng, 18000)) for _ in range(2)],
+        # third call: exactly the largest batch, so the probe table fills the whole fixed array
+        [k for k in (base[20000:28000] + node_keys(rng, 24768)) for _ in range(2)],
     ]
+    assert len(batches[2]) == MAX_KEYS
     for keys in batches:
         assert len(keys) <= MAX_KEYS
         rng.shuffle(keys)
@@ -79,7 +82,7 @@ def test_static_find_or_add_matches_arena_version(svdag_lib, lanes):
             assert tuple(w_s[i][: len(k)]) == k
         assert np.array_equal(labels(h_a), labels(h_s))  # the same keys share a slot in both tables
         assert arena.stats().items == static.stats().items
-    assert static.stats().items == len(set(base) | set(batches[1]))
+    assert static.stats().items == len(set(base) | set(batches[1]) | set(batches[2]))
     dag.free()
 
 
