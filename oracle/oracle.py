@@ -103,6 +103,8 @@ def lib():
             getattr(L, f).argtypes = [P]
             getattr(L, f).restype = C.c_uint32
         L.oracle_sample_voxels.argtypes = [P, P, C.c_uint64, P]
+        L.oracle_export_items.argtypes = [P, P, C.c_uint64, C.POINTER(C.c_uint64)]
+        L.oracle_should_edit_many.argtypes = [C.c_void_p, P, P, P, P, C.c_uint64, P, P]
         L.oracle_trace.argtypes = [P, C.POINTER(TraceParams), P, C.c_int]
         L.oracle_shade.argtypes = [P, C.POINTER(TraceParams), C.POINTER(ShadeParams), P, P, P, P, C.c_int]
         L.oracle_sincos.argtypes = [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]
@@ -222,6 +224,15 @@ class OracleDag:
 
     def redo_count(self) -> int:
         return lib().oracle_redo_count(self.h)
+
+    def export_items(self) -> np.ndarray:
+        """Items reachable from the root, (n, 10) uint32, children as row indices, row 0 = root."""
+        n = C.c_uint64()
+        lib().oracle_export_items(self.h, None, 0, C.byref(n))
+        out = np.zeros((n.value, 10), dtype=np.uint32)
+        if n.value:
+            lib().oracle_export_items(self.h, _ptr(out), n.value, C.byref(n))
+        return out
 
     def sample(self, xyz: np.ndarray) -> np.ndarray:
         xyz = np.ascontiguousarray(xyz, dtype=np.uint32).reshape(-1, 3)

@@ -1734,6 +1734,53 @@ int oracle_sample_voxels(const oracle_dag* d, const uint32_t* xyz, uint64_t coun
     return SVDAG_OK;
 }
 
+int oracle_export_items(const oracle_dag* d, uint32_t* out, uint64_t capacity, uint64_t* count)
+{
+    const Dag& g = d->dag;
+    *count = 0;
+    if (g.root == kSentinel)
+        return 0;
+    // Breadth first, level by level: ids are assigned in order of first appearance.
+    std::vector<std::vector<uint32_t>> order(g.levels - 1);
+    std::vector<std::unordered_map<uint32_t, uint64_t>> id(g.levels - 1);
+    order[0].push_back(g.root);
+    id[0][g.root] = 0;
+    uint64_t next = 1;
+    for (uint32_t level = 0; level < g.leaf_level(); ++level) {
+        for (uint32_t h : order[level]) {
+            const uint32_t* p = g.ptr(level, h);
+            const uint32_t n = (uint32_t)__builtin_popcount(header_child_mask(p[0]));
+            for (uint32_t j = 0; j < n; ++j)
+                if (id[level + 1].emplace(p[1 + j], 0).second)
+                    order[level + 1].push_back(p[1 + j]);
+        }
+        uint64_t base = next;
+        for (uint32_t c : order[level + 1])
+            id[level + 1][c] = base++;
+        next = base;
+    }
+    *count = next;
+    if (capacity < next)
+        return 1;
+    for (uint32_t level = 0; level <= g.leaf_level(); ++level) {
+        for (uint32_t h : order[level]) {
+            uint32_t* o = out + id[level][h] * 10ull;
+            for (uint32_t j = 0; j < 10; ++j)
+                o[j] = 0;
+            const uint32_t* p = g.ptr(level, h);
+            const uint32_t n = g.item_size(level, p);
+            for (uint32_t j = 0; j < n; ++j)
+                o[j] = p[j];
+            if (level < g.leaf_level()) {
+                const uint32_t k = (uint32_t)__builtin_popcount(header_child_mask(p[0]));
+                for (uint32_t j = 0; j < k; ++j)
+                    o[1 + j] = (uint32_t)id[level + 1][p[1 + j]];
+            }
+        }
+    }
+    return 0;
+}
+
 int oracle_trace(const oracle_dag* d, const svdag_trace_params* p, svdag_hit* out, int threads)
 {
     const uint32_t W = p->width, H = p->height;
@@ -2121,6 +2168,14 @@ int oracle_should_edit(const svdag_edit* e, const uint32_t path[3], uint32_t dep
     if (out_fill)
         *out_fill = d.fillMaterial;
     return (int)d.op;
+}
+
+int oracle_should_edit_many(const svdag_edit* e, const uint32_t* paths, const uint32_t* depths, const uint32_t* states,
+    const uint32_t* fills, uint64_t n, int32_t* ops, uint32_t* out_fills)
+{
+    for (uint64_t i = 0; i < n; ++i)
+        ops[i] = oracle_should_edit(e, paths + 3 * i, depths[i], states[i], fills[i], out_fills + i);
+    return 0;
 }
 
 void oracle_camera_params(const double pos[3], const double target[3], double fovDeg, uint32_t W, uint32_t H,

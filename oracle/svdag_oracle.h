@@ -59,6 +59,14 @@ uint32_t oracle_undo_count(const oracle_dag* dag);
 uint32_t oracle_redo_count(const oracle_dag* dag);
 
 int oracle_sample_voxels(const oracle_dag* dag, const uint32_t* xyz, uint64_t count, uint32_t* out);
+/* The items reachable from the root as one array of items at a stride of 10 words (zero padded),
+ * level by level, every child word rewritten to the index of the child's item in that array; item 0
+ * is the root. Writes *count items when capacity (in items) suffices, else only sets *count and
+ * returns 1. An empty DAG gives *count = 0. For feeding the reference's own decoding code. */
+/* oracle_should_edit over n nodes of one edit (paths: 3 words each). */
+int oracle_should_edit_many(const svdag_edit* e, const uint32_t* paths, const uint32_t* depths, const uint32_t* states,
+    const uint32_t* fills, uint64_t n, int32_t* ops, uint32_t* out_fills);
+int oracle_export_items(const oracle_dag* dag, uint32_t* out, uint64_t capacity, uint64_t* count);
 int oracle_trace(const oracle_dag* dag, const svdag_trace_params* params, svdag_hit* out, int threads);
 /* Shading of a hit buffer (trace_colors, trace_shadows, trace_ambient_occlusion, trace_lighting,
  * tracer.cu:413-730); hits[i].color receives the diffuse colour; rgba, sun and ao get width*height values. */

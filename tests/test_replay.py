@@ -200,7 +200,21 @@ def test_view_trace_params_equal_look_at(svdag_lib):
     assert len(frames) == 2 and list(frames[1].camera) == [1.0, 2.0, 3.0]
 
 
-REPLAYS = "/root/reference/replays"
+def _replays_dir():
+    """The reference's replays/ folder: SVDAG_REFERENCE_REPLAYS, else beside the reference sources
+    the oracle/_ref recipe compiles (absent on machines without the reference)."""
+    if os.environ.get("SVDAG_REFERENCE_REPLAYS"):
+        return os.environ["SVDAG_REFERENCE_REPLAYS"]
+    import importlib.util
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    spec = importlib.util.spec_from_file_location("build_ref", os.path.join(root, "oracle", "build_ref.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return os.path.join(os.path.dirname(mod.REFERENCE_SRC), "replays")
+
+
+REPLAYS = _replays_dir()
 
 
 @pytest.mark.skipif(not os.path.isdir(REPLAYS), reason="the reference's replay files are not on this machine")
