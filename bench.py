@@ -237,10 +237,11 @@ def c2_camera(svdag, levels, width=1920, height=1080):
 
 
 def make_scene(svdag, w, levels, phase_kernels=False, pool_gb=0.0, persistent=False):
-    # 52 GB at depth 17 (a 32 GiB item region, 16 GiB scratch); smaller scenes get a share of it by
-    # surface area (4^(levels-17)), at least 2 GB
+    # 86 GiB at depth 17 (the 64 GiB item region the 32-bit handle reaches, its slab headers and a
+    # 16 GiB scratch arena); smaller scenes get a share of it by surface area (4^(levels-17)), at
+    # least 2 GiB
     shrink = 4 ** max(0, w.C2_LEVELS - levels)
-    pool = int(pool_gb * (1 << 30)) if pool_gb else max(2 << 30, min(POOL_CAP, 52 << 30) // shrink)
+    pool = int(pool_gb * (1 << 30)) if pool_gb else max(2 << 30, min(POOL_CAP, 86 << 30) // shrink)
     dag = svdag.MyGPUHashDAG(levels, pool_bytes=pool, scratch_bytes=max(512 << 20, (16 << 30) // shrink),
                              undo_depth=32, phase_kernels=phase_kernels, persistent=persistent)
     terrain = make_terrain(w, levels)
@@ -279,14 +280,14 @@ def summarize(res, n_edits, duration_s=None):
     return out
 
 
-def require_ok(res, n_edits, what):
+def require_ok(res, n_edits, what, memory=None):
     """Every edit of a replay must have succeeded: a latency over failed edits measures nothing."""
     st = res["status"][:n_edits]
     bad = np.nonzero(st != 0)[0]
     if len(bad):
         i = int(bad[0])
         raise SystemExit(f"bench: {what}: {len(bad)} of {n_edits} edits failed; first: edit {i} with status "
-                         f"{int(st[i])} (launch {int(res['launch'][i])})")
+                         f"{int(st[i])} (launch {int(res['launch'][i])}); server memory: {memory}")
 
 
 def replay(svdag, dag, cam, edits, times, frames, plain=False, copy_frames=False, counters=None, memory=None):
@@ -358,21 +359,25 @@ def run_serve(args):
     tk, ek, fk = stream_of(w, levels, args.rate, dur_k, 4 + rank)
     cam = c2_camera(svdag, levels)
     out = {}
-    dags = {}
-    # served and plain paths, each on its own copy of the scene (both resident)
-    for name, plain in (("served", False), ("plain", True)):
+
+    def prepared_scene(plain):
+        """The scene built on the GPU, the launch form tuned on the first warm-up edits (applied for
+        real), the rest of the warm-up stream served, then a collection (undo history kept)."""
         dag, _ = make_scene(svdag, w, levels, persistent=args.persistent)
-        # the autotuner times the first warm-up edits (applied for real) and picks the launch form
         tuning = dag.autotune(edits=ew[:64])
-        res = replay(svdag, dag, cam, ew[64:], [t - tw[64] for t in tw[64:]] if len(ew) > 64 else [], fw, plain=plain)
-        require_ok(res, max(0, len(ew) - 64), f"{name} warm-up")
-        # the timed stream starts from a collected region (undo history kept)
+        mem = {}
+        res = replay(svdag, dag, cam, ew[64:], [t - tw[64] for t in tw[64:]] if len(ew) > 64 else [], fw, plain=plain,
+                     memory=mem)
+        require_ok(res, max(0, len(ew) - 64), f"{'plain' if plain else 'served'} warm-up", mem)
         dag.garbage_collect(keep_history=True)
-        dags[name] = dag
-        out[name] = {"tuning": {"persistent_leaves": tuning.persistent_leaves, "graph_us_small": tuning.graph_us_small,
-                                "persistent_us_small": tuning.persistent_us_small}}
+        return dag, {"persistent_leaves": tuning.persistent_leaves, "graph_us_small": tuning.graph_us_small,
+                     "persistent_us_small": tuning.persistent_us_small}
+
+    # Each replay below runs on a scene of its own: a depth-17 DAG keeps growing with the detail the
+    # edits add (undo history and garbage are collected, live data is not), and its 32 GiB item region
+    # holds the warm-up, a timed stream and some more, not every stream of the run.
     for name, plain in (("served", False), ("plain", True)):
-        dag = dags[name]
+        dag, tuning = prepared_scene(plain)
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
@@ -382,61 +387,62 @@ def run_serve(args):
             res = replay(svdag, dag, cam, ek, tk, fk, plain=plain, memory=mem, counters=frames)
             wall = time.perf_counter() - t0
         torch.cuda.synchronize()
-        require_ok(res, len(ek), f"{name} timed stream")
-        out[name].update(summarize(res, len(ek), dur_k))
-        out[name]["wall_s"] = wall
-        out[name]["memory"] = mem
-        out[name]["frames"] = frames
+        require_ok(res, len(ek), f"{name} timed stream", mem)
+        out[name] = summarize(res, len(ek), dur_k)
+        out[name].update(wall_s=wall, memory=mem, frames=frames, tuning=tuning)
         if name == "served":
             out["clocks"] = clocks.summary()
-    # offered-load sweep: the same stream shape at other rates, served and plain, each from a
-    # collected region
-    out["sweep"] = []
-    for i, rate in enumerate(float(r) for r in args.sweep.split(",") if r):
-        dur = min(8.0, max(2.0, 400.0 / rate))
-        ts, es, fs = stream_of(w, levels, rate, dur, 200 + 10 * i + rank)
-        point = {"rate_edits_per_s": rate, "duration_s": dur}
-        for name, plain in (("served", False), ("plain", True)):
-            dags[name].garbage_collect(keep_history=True)
-            mem = {}
-            res = replay(svdag, dags[name], cam, es, ts, fs, plain=plain, memory=mem)
-            require_ok(res, len(es), f"{name} at {rate:g} edits/s")
-            point[name] = summarize(res, len(es), dur)
-            point[name]["gc_runs"] = mem.get("gc_runs")
-        point["p99_served_over_plain"] = point["served"]["p99_ms"] / point["plain"]["p99_ms"]
-        out["sweep"].append(point)
-    dags["plain"].free()
-    del dags["plain"]
-    dag = dags["served"]
-    # e2e: the timed stream again with every frame copied to pinned host memory
-    dag.garbage_collect(keep_history=True)
-    frame_counters = {}
-    res_e2e = replay(svdag, dag, cam, ek, tk, fk, copy_frames=True, counters=frame_counters)
-    require_ok(res_e2e, len(ek), "e2e stream")
+            # the dominant kernel: one window of the stream as one batched launch
+            dag.garbage_collect(keep_history=True)
+            nwin = max(1, len(ek) // max(1, args.steps))
+            batch = ek[:nwin]
+            stream = torch.cuda.Stream()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            a.record(stream)
+            nrec = dag.edit_batch(batch, stream=stream.cuda_stream)
+            b.record(stream)
+            torch.cuda.synchronize()
+            recs = dag.edit_records(nrec)
+            bad = [i for i, r in enumerate(recs) if r.status != 0]
+            if bad:
+                raise SystemExit(f"bench: batched window: edit record {bad[0]} has status {recs[bad[0]].status}")
+            out["batch"] = {"edits": len(batch), "ms": a.elapsed_time(b), "bytes": edit_algorithmic_bytes(recs),
+                            "svo_items": int(sum(r.svo_items for r in recs))}
+            out["used_gb"] = dag.stats().item_region_used_bytes / 1e9
+            out["trace"] = trace_rays_s(svdag, torch, dag, cam)
+        dag.free()
+        del dag
+    # e2e: the timed stream served again, on a fresh scene, with every frame copied to pinned host memory
+    dag, _ = prepared_scene(False)
+    frame_counters, mem = {}, {}
+    res_e2e = replay(svdag, dag, cam, ek, tk, fk, copy_frames=True, counters=frame_counters, memory=mem)
+    require_ok(res_e2e, len(ek), "e2e stream", mem)
     out["e2e"] = summarize(res_e2e, len(ek), dur_k)
-    out["e2e"]["frames"] = frame_counters
-    # the dominant kernel: one window of the stream as one batched launch
-    dag.garbage_collect(keep_history=True)
-    nwin = max(1, len(ek) // max(1, args.steps))
-    batch = ek[:nwin]
-    stream = torch.cuda.Stream()
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    a.record(stream)
-    nrec = dag.edit_batch(batch, stream=stream.cuda_stream)
-    b.record(stream)
-    torch.cuda.synchronize()
-    recs = dag.edit_records(nrec)
-    bad = [i for i, r in enumerate(recs) if r.status != 0]
-    if bad:
-        raise SystemExit(f"bench: batched window: edit record {bad[0]} has status {recs[bad[0]].status}")
-    out["batch"] = {"edits": len(batch), "ms": a.elapsed_time(b), "bytes": edit_algorithmic_bytes(recs),
-                    "svo_items": int(sum(r.svo_items for r in recs))}
-    st = dag.stats()
-    out["used_gb"] = st.item_region_used_bytes / 1e9
-    out["trace"] = trace_rays_s(svdag, torch, dag, cam)
+    out["e2e"].update(frames=frame_counters, memory=mem)
     dag.free()
-    del dags["served"]
+    del dag
+    # offered-load sweep: the same stream shape at other rates, served then plain, each from a
+    # collected region of one more fresh scene
+    out["sweep"] = []
+    sweep = [float(r) for r in args.sweep.split(",") if r]
+    if sweep:
+        dag, _ = prepared_scene(False)
+        for i, rate in enumerate(sweep):
+            dur = min(8.0, max(2.0, 400.0 / rate))
+            ts, es, fs = stream_of(w, levels, rate, dur, 200 + 10 * i + rank)
+            point = {"rate_edits_per_s": rate, "duration_s": dur}
+            for name, plain in (("served", False), ("plain", True)):
+                dag.garbage_collect(keep_history=True)
+                mem = {}
+                res = replay(svdag, dag, cam, es, ts, fs, plain=plain, memory=mem)
+                require_ok(res, len(es), f"{name} at {rate:g} edits/s", mem)
+                point[name] = summarize(res, len(es), dur)
+                point[name]["gc_runs"] = mem.get("gc_runs")
+            point["p99_served_over_plain"] = point["served"]["p99_ms"] / point["plain"]["p99_ms"]
+            out["sweep"].append(point)
+        dag.free()
+        del dag
     peak, peak_kind = measured_peak_gbs()
     trace_c0 = None
     if rank == 0 and not args.no_cpu_baseline:

@@ -21,7 +21,7 @@ constexpr unsigned long long kBatchBytes = 2 * 1024 * 1024;
 // from the active roots and the canonical fully-filled nodes; freeInactiveItems
 // (gpu_hash_table_base.cu:265-374) then clears every unmarked slot and hands every overflow slab it
 // leaves empty back to the slab allocator. Here marking is a bitmap with one bit per handle (an
-// 8-byte unit of the item region) and the frontier is deduplicated by the test-and-set on it; the
+// 16-byte handle unit of the item region) and the frontier is deduplicated by the test-and-set on it; the
 // sweep unlinks empty overflow slabs and pushes them on the free list of their size class.
 // MyGPUHashDAGUndoRedo::garbageCollect (my_gpu_base_dag.h:66-77) passes the current root alone and
 // clears the history (svdag_gc); svdag_gc_keep_history passes the current root and every undo and
@@ -89,23 +89,44 @@ __global__ void k_gc_mark(DevDag d, uint32_t* bits, uint32_t level, const uint32
         }
     }
     const uint32_t n = min(*inCount, cap);
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t* node = item_ptr(d, in[i]);
-        const uint32_t mask = node[0] & 0xFFu;
-        const uint32_t k = __popc(mask);
-        for (uint32_t j = 0; j < k; ++j) {
-            const uint32_t c = node[1 + j];
-            if (!handle_ok(d, c)) {
-                set_status(d.ctl, SVDAG_ERR_CORRUPT);
-                continue;
+    // Whole warps iterate together (the bound is rounded up to a warp multiple) so that the
+    // children a warp marks in one step take a single atomic on the frontier counter.
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < n; base += stride) {
+        const uint32_t i = base + lane;
+        const uint32_t* node = i < n ? item_ptr(d, in[i]) : nullptr;
+        const uint32_t mask = node ? node[0] & 0xFFu : 0u;
+        uint32_t children[8];
+        uint32_t mine = 0; // children this lane marked first
+#pragma unroll
+        for (uint32_t j = 0; j < 8; ++j) {
+            if (j < (uint32_t)__popc(mask)) {
+                const uint32_t c = node[1 + j];
+                if (!handle_ok(d, c))
+                    set_status(d.ctl, SVDAG_ERR_CORRUPT);
+                else if (mark_once(bits, c))
+                    children[mine++] = c;
             }
-            if (mark_once(bits, c)) {
-                const uint32_t at = atomicAdd(outCount, 1u);
-                if (at < cap)
-                    out[at] = c;
-                else
-                    set_status(d.ctl, SVDAG_ERR_OOM);
-            }
+        }
+        // warp-wide exclusive scan of `mine`
+        uint32_t prefix = mine;
+#pragma unroll
+        for (uint32_t o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, prefix, o);
+            if (lane >= o)
+                prefix += v;
+        }
+        const uint32_t total = __shfl_sync(0xFFFFFFFFu, prefix, 31);
+        uint32_t first = 0;
+        if (lane == 31 && total)
+            first = atomicAdd(outCount, total);
+        first = __shfl_sync(0xFFFFFFFFu, first, 31) + prefix - mine;
+        for (uint32_t j = 0; j < mine; ++j) {
+            if (first + j < cap)
+                out[first + j] = children[j];
+            else
+                set_status(d.ctl, SVDAG_ERR_OOM);
         }
     }
 }
@@ -177,8 +198,12 @@ __global__ void k_gc_sweep(DevDag d, DevTable t, const uint32_t* bits, unsigned 
         atomicAdd(&freed[1], nslabs);
 }
 
-__global__ void k_gc_finish(Control* c, const unsigned long long* freed, uint32_t clearHistory)
+__global__ void k_gc_finish(Control* c, const unsigned long long* freed, const uint32_t* counts, uint32_t levels, uint32_t clearHistory)
 {
+    unsigned long long live = 0;
+    for (uint32_t l = 0; l < levels; ++l) // counts[l]: the frontier of level l, every item marked once
+        live += counts[l];
+    c->gcLiveItems = live;
     c->gcFreedItems = freed[0];
     c->gcFreedSlabs = freed[1];
     if (clearHistory) {
@@ -197,7 +222,7 @@ svdag_status collect(svdag_ctx* ctx, bool keepHistory, cudaStream_t s)
     SVDAG_CUDA(cudaMemcpyAsync(&top, &ctx->ctl->itemTop, sizeof(top), cudaMemcpyDeviceToHost, s));
     SVDAG_CUDA(cudaStreamSynchronize(s));
     top = std::min<unsigned long long>(top, ctx->itemWords);
-    const unsigned long long bitmapBytes = align256(((top / 2) + 64) / 8 + 8); // one bit per 8-byte unit
+    const unsigned long long bitmapBytes = align256(((top / kUnitWords) + 64) / 8 + 8); // one bit per handle unit
     const unsigned long long rest = ctx->scratchBytes > bitmapBytes + 4096 ? ctx->scratchBytes - bitmapBytes - 4096 : 0;
     uint32_t frontierCap = (uint32_t)std::min<unsigned long long>(rest / 8, 0xFFFFFFFFull); // two frontiers of u32
     // SVDAG_GC_MAX_FRONTIER lowers the frontier capacity (tests reach the overflow path with it
@@ -231,7 +256,7 @@ svdag_status collect(svdag_ctx* ctx, bool keepHistory, cudaStream_t s)
             nb = std::max<unsigned long long>(nb, t.numBuckets[c]);
         k_gc_sweep<<<grid_for(ctx, nb, 256), 256, 0, s>>>(d, t, bits, freed);
     }
-    k_gc_finish<<<1, 1, 0, s>>>(ctx->ctl, freed, keepHistory ? 0u : 1u);
+    k_gc_finish<<<1, 1, 0, s>>>(ctx->ctl, freed, counts, LL + 1, keepHistory ? 0u : 1u);
     SVDAG_CUDA(cudaGetLastError());
     return read_status(ctx, s);
 }
@@ -311,13 +336,14 @@ svdag_status svdag_create(const svdag_config* cfg, svdag_ctx** out)
     static_assert(sizeof(EditQueue) <= 4096, "editor queue too large");
     ctx->scratch = ctx->pool + kCtlBytes + kBatchBytes;
     ctx->scratchBytes = scratch;
-    // The rest: slab headers (a ninth: 32 bytes per slab of 24 items of 2..10 words) then items.
+    // The rest: slab headers (a thirteenth: 32 bytes per slab, whose body of 24 items takes at least
+    // 24 * 16 = 384 bytes) then items.
     const unsigned long long rest = pool - kCtlBytes - kBatchBytes - scratch;
-    const unsigned long long headerBytes = align256(rest / 9);
+    const unsigned long long headerBytes = align256(rest / 13);
     ctx->headers = reinterpret_cast<uint32_t*>(ctx->pool + kCtlBytes + kBatchBytes + scratch);
     ctx->headerCount = std::min<unsigned long long>(headerBytes / 32, 0xFFFFFFF0ull);
     ctx->items = reinterpret_cast<uint32_t*>(ctx->pool + kCtlBytes + kBatchBytes + scratch + headerBytes);
-    ctx->itemWords = std::min<unsigned long long>((rest - headerBytes) / 4 - 64, kMaxItemWords) & ~7ull;
+    ctx->itemWords = std::min<unsigned long long>((rest - headerBytes) / 4 - 64, kMaxItemWords) & ~31ull;
     static_assert(sizeof(Control) <= kCtlBytes, "control block too large");
     cudaError_t e = cudaMemset(ctx->pool, 0, pool);
     if (e == cudaSuccess) {
@@ -410,6 +436,7 @@ svdag_status svdag_get_stats(svdag_ctx* ctx, svdag_stats* out, void* stream)
         out->free_list_slabs += c.freeSlabs[k];
     out->gc_freed_items = c.gcFreedItems;
     out->gc_freed_slabs = c.gcFreedSlabs;
+    out->gc_live_items = c.gcLiveItems;
     out->scratch_bytes = ctx->scratchBytes;
     out->scratch_high_water_bytes = ctx->scratchHighWater;
     out->undo_count = c.undoCount;

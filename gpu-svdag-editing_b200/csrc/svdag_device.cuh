@@ -1,8 +1,8 @@
 // svdag_device.cuh - device-side data layout and the slab hash table probes.
 //
-// Item region: one array inside the context's HBM pool. A handle is the index of an item in 8-byte
-// units (items are 8-byte aligned), so decoding a handle is a shift and an add and 32-bit handles
-// reach 32 GiB (the reference decodes through a table descriptor and the slab allocator's super-block
+// Item region: one array inside the context's HBM pool. A handle is the index of an item in 16-byte
+// units (items are 16-byte aligned), so decoding a handle is a shift and an add and 32-bit handles
+// reach 64 GiB (the reference decodes through a table descriptor and the slab allocator's super-block
 // table, gpu_hash_table_base.h:275-294). Slabs are 32-byte aligned and named by their index in
 // 32-byte units (the "slab id").
 //
@@ -13,7 +13,7 @@
 //   header words 0..5 : 24 one-byte tags, slot s at word s / 4, byte s % 4; 0 = free, 0xFF = being written
 //   header word 6     : handle of the body (item of slot 0)
 //   header word 7     : header id of the next slab in the bucket's chain, 0 = end (header 0 is unused)
-//   body              : 24 items of k words at a stride of k rounded up to even (slot s at body + s*stride)
+//   body              : 24 items of k words at a stride of k rounded up to a multiple of 4 (slot s at body + s*stride)
 // A probe reads one 32-byte header sector per slab plus the candidate item. Headers are dense (a
 // table's headers are about a tenth of its bytes), so the headers a lookup stream touches stay in
 // the 126 MB L2 while the items it compares are read once; the reference interleaves a 10-word
@@ -42,7 +42,8 @@ namespace svdag {
 constexpr uint32_t kNone = 0xFFFFFFFFu; // empty child / missing handle
 constexpr uint32_t kEnd = 0u; // end of a slab chain
 constexpr uint32_t kFillMarker = 0xFFFFFF00u; // SVO child "canonical fully-filled node of material m" = kFillMarker | m
-constexpr unsigned long long kMaxItemWords = 2ull * 0xFFFFFF00ull - 64; // item region limit (just under 32 GiB)
+constexpr uint32_t kUnitWords = 4; // a handle counts 16-byte units
+constexpr unsigned long long kMaxItemWords = (unsigned long long)kUnitWords * 0xFFFFFF00ull - 64; // item region limit (just under 64 GiB)
 constexpr uint32_t kSlots = 24;
 constexpr uint32_t kHeaderWords = 8;
 constexpr uint32_t kTagBusy = 0xFFu;
@@ -50,10 +51,10 @@ constexpr uint32_t kMaxLevels = SVDAG_MAX_LEVELS;
 constexpr uint32_t kItemStride = 10; // padded stride of items in scratch arrays
 constexpr uint32_t kNumClasses = 9; // item sizes 2..10
 
-__host__ __device__ constexpr uint32_t item_stride(uint32_t k) { return (k + 1u) & ~1u; } // words, even
-__host__ __device__ constexpr uint32_t body_words(uint32_t k) { return kSlots * item_stride(k); } // a multiple of 8
+__host__ __device__ constexpr uint32_t item_stride(uint32_t k) { return (k + kUnitWords - 1u) & ~(kUnitWords - 1u); } // words
+__host__ __device__ constexpr uint32_t body_words(uint32_t k) { return kSlots * item_stride(k); } // a multiple of 32
 // Handle of slot s of the slab whose body starts at handle `body`, for items of k words.
-__host__ __device__ constexpr uint32_t slot_handle(uint32_t body, uint32_t s, uint32_t k) { return body + s * (item_stride(k) >> 1); }
+__host__ __device__ constexpr uint32_t slot_handle(uint32_t body, uint32_t s, uint32_t k) { return body + s * (item_stride(k) / kUnitWords); }
 __host__ __device__ inline uint32_t header_tag(const uint32_t* h, uint32_t s) { return (h[s >> 2] >> (8u * (s & 3u))) & 0xFFu; }
 
 // Per-table descriptor, passed by value to kernels.
@@ -104,6 +105,7 @@ struct Control {
     unsigned long long freeSlabs[kNumClasses]; // slabs on each free list
     unsigned long long gcFreedItems; // items the last collection freed
     unsigned long long gcFreedSlabs; // overflow slabs the last collection put on the free lists
+    unsigned long long gcLiveItems; // items the last collection marked (reachable from its roots)
 };
 
 // The first 32 bytes of the control block, copied to the host after every served launch.
@@ -148,18 +150,18 @@ __device__ __forceinline__ void set_status(Control* ctl, uint32_t code)
 __device__ const uint32_t kZeroItem[16] = {};
 __device__ __forceinline__ bool handle_ok(const DevDag& d, uint32_t h)
 {
-    return 2ull * h + 16ull <= d.itemWords;
+    return (unsigned long long)kUnitWords * h + 16ull <= d.itemWords;
 }
 __device__ __forceinline__ const uint32_t* item_ptr(const DevDag& d, uint32_t h)
 {
     if (handle_ok(d, h))
-        return d.items + 2ull * h;
+        return d.items + (unsigned long long)kUnitWords * h;
     set_status(d.ctl, SVDAG_ERR_CORRUPT);
     return kZeroItem;
 }
 __device__ __forceinline__ bool slab_ok(const DevDag& d, uint32_t slab) { return slab != 0 && slab < d.headerCount; }
 __device__ __forceinline__ uint32_t* slab_ptr(const DevDag& d, uint32_t slab) { return d.headers + 8ull * slab; }
-__device__ __forceinline__ uint32_t* handle_ptr(const DevDag& d, uint32_t h) { return d.items + 2ull * h; }
+__device__ __forceinline__ uint32_t* handle_ptr(const DevDag& d, uint32_t h) { return d.items + (unsigned long long)kUnitWords * h; }
 
 // ---------------------------------------------------------------- hashing: svdag_hash.h
 
@@ -516,7 +518,7 @@ __device__ __forceinline__ uint32_t alloc_slab(const Grp<G>& g, const DevDag& d,
         id = pop_free_slab(d, k - 2u);
         if (id != kNone) {
             body = __ldcg(slab_ptr(d, id) + 6); // a free slab keeps its body
-            if (2ull * body + body_words(k) > d.itemWords) {
+            if ((unsigned long long)kUnitWords * body + body_words(k) > d.itemWords) {
                 set_status(d.ctl, SVDAG_ERR_CORRUPT);
                 id = kNone; // dropped from the list: never handed out
             }
@@ -539,7 +541,7 @@ __device__ __forceinline__ uint32_t alloc_slab(const Grp<G>& g, const DevDag& d,
         const unsigned long long o = leaders.shfl(obase, 0) + before;
         if (hid < d.headerCount && o + w <= d.itemWords) {
             id = (uint32_t)hid;
-            body = (uint32_t)(o >> 1); // itemTop stays a multiple of 8 words
+            body = (uint32_t)(o / kUnitWords); // itemTop stays a multiple of 32 words
         } else {
             set_status(d.ctl, SVDAG_ERR_OOM);
         }

@@ -15,7 +15,7 @@ namespace serve {
 // Upper estimate of the item-region bytes an edit can add: its intermediate SVO bounds the new items.
 // Leaves: the footprint's bounding volume in 4^3 bricks, or for spheres and boxes whose volume is
 // large, a shell of three bricks' thickness around the surface (interior nodes are filled or emptied
-// whole). Nodes above the leaves add at most a seventh; each item takes at most 48 bytes with its
+// whole). Nodes above the leaves add at most a seventh; each item takes at most 50 bytes with its
 // share of the slab header.
 inline unsigned long long edit_reserve_bytes(const svdag_edit& e, uint32_t levels)
 {
@@ -40,7 +40,7 @@ inline unsigned long long edit_reserve_bytes(const svdag_edit& e, uint32_t level
         break;
     }
     const double items = leaves * 8.0 / 7.0 + 8.0 * levels;
-    return (unsigned long long)(items * 48.0);
+    return (unsigned long long)(items * 50.0); // a 48-byte slot (10 words at a 16-byte stride) and 1/24 of a 32-byte header
 }
 
 // Hit-buffer rows [row0, row1] and columns [col0, col1] that rays meeting `box` can come from. Pixel (x, y) looks along

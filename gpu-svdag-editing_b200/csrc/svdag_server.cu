@@ -86,6 +86,11 @@ struct svdag_server {
     std::atomic<unsigned long long> usedBytes { 0 }; // item and header region in use after the last finished launch
     unsigned long long gcThreshold = 0; // configured threshold
     unsigned long long gcTrigger = 0; // bytes in use that start the next collection
+    // Slots a collection frees stay in their slabs (only overflow slabs left empty go back), so the
+    // bump-pointer bytes in use stay high after it while inserts fill those slots. The credit is
+    // the slot bytes the last collection freed (16 per item, the smallest slot) less 50 per item
+    // inserted since (the largest); memory pressure is the bytes in use less the credit.
+    std::atomic<unsigned long long> reuseCredit { 0 };
     bool dirtySinceGc = true; // a launch finished since the last collection (one could free something)
     bool gcWanted = false; // admit nothing until the GPU is idle, then collect
     // Memory counters: written by the worker thread, read by svdag_server_memory_stats.
@@ -111,6 +116,11 @@ struct svdag_server {
     std::thread worker;
 
     bool plain() const { return cfg.flags & SVDAG_SERVE_PLAIN; }
+    unsigned long long pressure() const
+    {
+        const unsigned long long u = usedBytes.load(), c = reuseCredit.load();
+        return u > c ? u - c : 0ull;
+    }
     bool gcAllowed() const { return !(cfg.flags & SVDAG_SERVE_NO_GC); }
 
     // A collection that keeps every undo/redo root (nothing of the context may be on the GPU), then
@@ -120,8 +130,12 @@ struct svdag_server {
         const Clock::time_point a = Clock::now();
         const svdag_status st = svdag_gc_keep_history(ctx, stream);
         MemSnapshot ms {};
+        unsigned long long freedItems = 0;
         SVDAG_CUDA(cudaMemcpyAsync(&ms, &ctx->ctl->itemTop, sizeof(ms), cudaMemcpyDeviceToHost, stream));
+        SVDAG_CUDA(cudaMemcpyAsync(&freedItems, &ctx->ctl->gcFreedItems, sizeof(freedItems), cudaMemcpyDeviceToHost, stream));
         SVDAG_CUDA(cudaStreamSynchronize(stream));
+        if (st == SVDAG_OK)
+            reuseCredit = freedItems * 16ull;
         const unsigned long long before = usedBytes;
         usedBytes = used_region_bytes(ctx, ms.itemTop, ms.headerTop, ms.freeBytes);
         gcSeconds.store(gcSeconds.load() + std::chrono::duration<double>(Clock::now() - a).count());
@@ -129,7 +143,7 @@ struct svdag_server {
         gcFreedBytes += before > usedBytes ? before - usedBytes : 0ull;
         // The next collection waits until a quarter of the room left above what this one kept has
         // filled, so that live data near the threshold does not start a collection per launch.
-        const unsigned long long kept = usedBytes;
+        const unsigned long long kept = pressure();
         gcTrigger = std::max(gcThreshold, kept < capBytes ? kept + (capBytes - kept) / 4 : capBytes);
         dirtySinceGc = false;
         gcWanted = false;
@@ -271,6 +285,11 @@ struct svdag_server {
         usedBytes = used_region_bytes(ctx, ms.itemTop, ms.headerTop, ms.freeBytes);
         for (size_t i = 0; i < b.lastRecord.size(); ++i)
             failedEdits += b.records[b.lastRecord[i]].status != 0 ? 1u : 0u;
+        unsigned long long added = 0;
+        for (const EditRecord& r : b.records)
+            added += r.added;
+        const unsigned long long c = reuseCredit.load();
+        reuseCredit = c > 50ull * added ? c - 50ull * added : 0ull;
         dirtySinceGc = true;
         b.finished = true;
     }
@@ -380,9 +399,9 @@ struct svdag_server {
             }
             std::vector<Request> one { r };
             svdag_status st = SVDAG_OK;
-            if (r.kind == 0 && gcAllowed() && dirtySinceGc && (usedBytes > gcTrigger || usedBytes + r.reserve > capBytes))
+            if (r.kind == 0 && gcAllowed() && dirtySinceGc && (pressure() > gcTrigger || pressure() + r.reserve > capBytes))
                 collect_garbage(); // a failed collection frees nothing; the edit is then judged as it is
-            if (r.kind == 0 && usedBytes + r.reserve > capBytes) {
+            if (r.kind == 0 && pressure() + r.reserve > capBytes) {
                 std::lock_guard<std::mutex> lk(m);
                 ++rejectedEdits;
                 fail_requests(one, SVDAG_ERR_OOM);
@@ -425,7 +444,7 @@ struct svdag_server {
                 complete_frame();
             // Memory: past the threshold, admit nothing until the launches and the frame in flight
             // are done, then collect (every undo/redo root kept).
-            if (gcAllowed() && dirtySinceGc && usedBytes > gcTrigger)
+            if (gcAllowed() && dirtySinceGc && pressure() > gcTrigger)
                 gcWanted = true;
             if (gcWanted && unfinished() == 0 && !frameActive) {
                 collect_garbage(); // a failed collection frees nothing; admission then judges edits as they are
@@ -438,7 +457,7 @@ struct svdag_server {
                 if (stop && queue.empty() && batches.empty() && !frameActive && pendingFrames.empty())
                     break;
                 const bool canLaunch = unfinished() < maxInflight && !gcWanted;
-                const unsigned long long inUse = usedBytes + reserved_in_flight();
+                const unsigned long long inUse = pressure() + reserved_in_flight();
                 uint32_t edits = 0;
                 for (auto it = queue.begin(); it != queue.end();) {
                     if (it->kind == 1) { // answered by the next frame
@@ -559,7 +578,9 @@ svdag_status svdag_server_create(svdag_ctx* ctx, const svdag_server_config* conf
         fail(cudaMemcpy(&ms, &ctx->ctl->itemTop, sizeof(ms), cudaMemcpyDeviceToHost));
         s->usedBytes = used_region_bytes(ctx, ms.itemTop, ms.headerTop, ms.freeBytes);
     }
-    s->gcThreshold = config->gc_threshold_bytes ? config->gc_threshold_bytes : s->capBytes - s->capBytes / 8;
+    // Default: collect when less than 1/32 of the cap (at least 1 GiB, at most an eighth) is left.
+    const unsigned long long room = std::min(s->capBytes / 8, std::max(s->capBytes / 32, 1ull << 30));
+    s->gcThreshold = config->gc_threshold_bytes ? config->gc_threshold_bytes : s->capBytes - room;
     s->gcTrigger = s->gcThreshold;
     if (st != SVDAG_OK) {
         s->stop = true;
@@ -708,6 +729,7 @@ svdag_status svdag_server_memory_stats(svdag_server* s, svdag_server_memory* out
     r.gc_seconds = s->gcSeconds.load();
     r.rejected_edits = s->rejectedEdits.load();
     r.failed_edits = s->failedEdits.load();
+    r.reuse_credit_bytes = s->reuseCredit.load();
     *out = r;
     return SVDAG_OK;
 }

@@ -42,7 +42,7 @@ svdag_status read_status(svdag_ctx* ctx, cudaStream_t s)
 __global__ void k_init_bucket_headers(DevDag d, DevTable t)
 {
     for (uint32_t c = 0; c < kNumClasses; ++c) {
-        const uint32_t units = body_words(c + 2) >> 1;
+        const uint32_t units = body_words(c + 2) / kUnitWords;
         for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < t.numBuckets[c]; b += gridDim.x * blockDim.x) {
             uint4* h = reinterpret_cast<uint4*>(slab_ptr(d, t.bucketBase[c] + b));
             h[0] = make_uint4(0, 0, 0, 0);
@@ -65,7 +65,7 @@ svdag_status alloc_table(svdag_ctx* ctx, svdag_table* t, uint32_t kind, const ui
     for (uint32_t c = 0; c < kNumClasses; ++c) {
         dev.numBuckets[c] = bucketsPerClass[c];
         dev.bucketBase[c] = (uint32_t)(tops[1] + headers);
-        dev.bodyBase[c] = (uint32_t)((tops[0] + words) >> 1); // tops[0] and body sizes are multiples of 8 words
+        dev.bodyBase[c] = (uint32_t)((tops[0] + words) / kUnitWords); // tops[0] and body sizes are multiples of 32 words
         words += (unsigned long long)bucketsPerClass[c] * body_words(c + 2);
         headers += bucketsPerClass[c];
         buckets = std::max<unsigned long long>(buckets, bucketsPerClass[c]);

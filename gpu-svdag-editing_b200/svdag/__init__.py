@@ -93,7 +93,7 @@ class ServerMemory(C.Structure):
     """svdag_server_memory: the serving loop's memory accounting and in-loop collections."""
     _fields_ = [("used_bytes", C.c_uint64), ("cap_bytes", C.c_uint64), ("gc_threshold_bytes", C.c_uint64),
                 ("gc_runs", C.c_uint64), ("gc_freed_bytes", C.c_uint64), ("gc_seconds", C.c_double),
-                ("rejected_edits", C.c_uint64), ("failed_edits", C.c_uint64)]
+                ("rejected_edits", C.c_uint64), ("failed_edits", C.c_uint64), ("reuse_credit_bytes", C.c_uint64)]
 
 
 class RequestResult(C.Structure):
@@ -163,7 +163,8 @@ class Stats(C.Structure):
                 ("scratch_bytes", C.c_uint64), ("scratch_high_water_bytes", C.c_uint64),
                 ("level_items", C.c_uint64 * MAX_LEVELS), ("level_buckets", C.c_uint64 * MAX_LEVELS),
                 ("undo_count", C.c_uint32), ("redo_count", C.c_uint32), ("free_list_bytes", C.c_uint64),
-                ("free_list_slabs", C.c_uint64), ("gc_freed_items", C.c_uint64), ("gc_freed_slabs", C.c_uint64)]
+                ("free_list_slabs", C.c_uint64), ("gc_freed_items", C.c_uint64), ("gc_freed_slabs", C.c_uint64),
+                ("gc_live_items", C.c_uint64)]
 
 
 class TableStats(C.Structure):

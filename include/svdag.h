@@ -37,7 +37,7 @@ typedef enum svdag_status {
     SVDAG_ERR_BUSY = 8 /* serving queue full / admission refused */
 } svdag_status;
 
-/* Item handles are 32-bit indices of items in 8-byte units of the context's item region (up to 32 GiB). */
+/* Item handles are 32-bit indices of items in 16-byte units of the context's item region (up to 64 GiB). */
 #define SVDAG_INVALID_HANDLE 0xFFFFFFFFu
 /* Voxel sampling and hit records use this value for "no voxel". */
 #define SVDAG_NO_MATERIAL 0xFFFFFFFFu
@@ -437,6 +437,7 @@ typedef struct svdag_stats {
     uint64_t free_list_slabs;
     uint64_t gc_freed_items; /* items the last collection freed */
     uint64_t gc_freed_slabs; /* overflow slabs the last collection put on the free lists */
+    uint64_t gc_live_items; /* items the last collection found reachable */
 } svdag_stats;
 /* MyGPUHashDAG::report (my_gpu_hash_dag.cu:217-230). Synchronises `stream`. */
 svdag_status svdag_get_stats(svdag_ctx* ctx, svdag_stats* out, void* stream);
@@ -511,10 +512,11 @@ svdag_status svdag_set_tuning(svdag_ctx* ctx, const svdag_tuning* tuning);
  * are queued on the GPU ahead of their completion). Frames run on a second stream, one at a time,
  * each behind every batch launched before it: its completion makes those edits visible and answers
  * the frame requests pending when it started, and the next batch edits while it renders.
- * An edit is admitted when the item-region bytes in use plus those reserved by admitted, unfinished
- * edits (an upper estimate from the tool's footprint) stay under the memory cap; a queue head that
- * does not fit waits until launches complete. Memory is reclaimed in the loop: once the bytes in use
- * pass gc_threshold_bytes, or when the queue head does not fit with nothing in flight, the loop lets
+ * An edit is admitted when the memory pressure (item-region bytes in use, less the slots the last
+ * collection freed) plus the bytes reserved by admitted, unfinished edits (an upper estimate from
+ * the tool's footprint) stays under the memory cap; a queue head that does not fit waits until
+ * launches complete. Memory is reclaimed in the loop: once the pressure passes gc_threshold_bytes,
+ * or when the queue head does not fit with nothing in flight, the loop lets
  * the launches and the frame in flight finish, then runs svdag_gc_keep_history (the undo history
  * survives) before it admits more. An edit that does not fit even after a collection fails with
  * SVDAG_ERR_OOM without being launched. With SVDAG_SERVE_PLAIN the same loop serves one request
@@ -538,7 +540,10 @@ typedef struct svdag_server_config {
     svdag_trace_params frame; /* camera and resolution of the frames rendered after each launch */
     uint32_t flags; /* SVDAG_SERVE_* */
     uint32_t reserved;
-    uint64_t gc_threshold_bytes; /* bytes in use that start a collection; 0 = 7/8 of the cap */
+    /* Memory pressure that starts a collection; 0 = the cap less 1/32 of it (at least 1 GiB, at most
+     * an eighth). Pressure = item and header bytes in use less the slot bytes the last collection
+     * freed and inserts have not filled yet (16 bytes per freed item, less 50 per item inserted). */
+    uint64_t gc_threshold_bytes;
 } svdag_server_config;
 
 typedef struct svdag_server svdag_server;
@@ -577,6 +582,7 @@ typedef struct svdag_server_memory {
     double gc_seconds; /* host time they took (the loop admits nothing meanwhile) */
     uint64_t rejected_edits; /* failed with SVDAG_ERR_OOM before launch: they did not fit after a collection */
     uint64_t failed_edits; /* launched edits whose record reported an error */
+    uint64_t reuse_credit_bytes; /* freed slot bytes counted as available (see gc_threshold_bytes) */
 } svdag_server_memory;
 svdag_status svdag_server_memory_stats(svdag_server* server, svdag_server_memory* out);
 /* Copies the most recent frame (SVDAG_SERVE_COPY_FRAMES) to `out` (width * height hits). */

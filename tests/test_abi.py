@@ -38,7 +38,7 @@ def test_struct_layouts(svdag_lib):
     assert C.sizeof(s.TraceParams) == 104
     assert C.sizeof(s.TerrainParams) == 32
     assert C.sizeof(s.ServerConfig) == 136
-    assert C.sizeof(s.ServerMemory) == 64
+    assert C.sizeof(s.ServerMemory) == 72
     assert C.sizeof(s.RequestResult) == 48
     assert C.sizeof(s.Tuning) == 40
     assert C.sizeof(s.AltTuning) == 16  # svdag_alt_tuning

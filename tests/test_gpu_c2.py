@@ -112,7 +112,7 @@ def test_c2_sequence_regions_undo_redo_gc(svdag_lib, oracle_mod, c2):
     cam = (0.30 * (1 << LEVELS) + 3000.0, 0.62 * (1 << LEVELS), 0.30 * (1 << LEVELS) - 2500.0)
     p = svdag_lib.get_trace_params(cam, tuple(edits[0].center), 1920, 1080)
     before = gpu_trace(svdag_lib, g, p)
-    used = g.stats().item_region_used_bytes
+    used, free_before = g.stats().item_region_used_bytes, g.stats().free_list_bytes
     items = [g.table(l).stats().items for l in range(LEVELS - 1)]
     g.garbage_collect()
     after_items = [g.table(l).stats().items for l in range(LEVELS - 1)]
@@ -120,7 +120,7 @@ def test_c2_sequence_regions_undo_redo_gc(svdag_lib, oracle_mod, c2):
     st = g.stats()
     # freed slots stay in their slabs for reuse; overflow slabs left empty go on the free lists and
     # count as free
-    assert st.item_region_used_bytes == used - st.free_list_bytes
+    assert st.item_region_used_bytes == used - (st.free_list_bytes - free_before)
     assert st.gc_freed_items == sum(items) - sum(after_items)
     assert g.stats().undo_count == 0 and g.stats().redo_count == 0
     after = gpu_trace(svdag_lib, g, p)
@@ -130,3 +130,40 @@ def test_c2_sequence_regions_undo_redo_gc(svdag_lib, oracle_mod, c2):
     assert compare_region(oracle_mod, g, oracles[2], lo, hi) > 0
     g.undo()
     assert g.get_first_node_index() == roots[3]
+
+
+def test_c2_1080p_frame_equals_the_oracle_in_a_clipped_region(svdag_lib, oracle_mod, c2):
+    """A 1920x1080 frame of the depth-17 scene, pixel for pixel against the oracle. The camera looks
+    steeply down at the terrain away from the edited regions, and the oracle builds the scene clipped
+    to a box around it that holds every voxel the frame's rays reach first: every ray hits inside the
+    box (checked), so the clipped scene and the whole one give the same frame."""
+    from gpu_util import compare_hits
+    from oracle import oracle as om
+
+    g, _, params = c2
+    L = oracle_mod.lib()
+    gsz = 1 << LEVELS
+    x0, z0 = int(0.80 * gsz), int(0.20 * gsz)
+    h0 = L.oracle_terrain_height(params, LEVELS, x0, z0)
+    cam = (float(x0), float(h0 + 160), float(z0))
+    target = (float(x0 + 110), float(h0 - 120), float(z0 + 80))
+    p = svdag_lib.get_trace_params(cam, target, 1920, 1080)
+    hits = gpu_trace(svdag_lib, g, p)
+    lo = [x0 - 2048, h0 - 2048, z0 - 2048]
+    hi = [x0 + 2048, h0 + 1024, z0 + 2048]
+    o = oracle_mod.OracleDag(LEVELS)
+    o.build_scene_region(params, lo, hi)
+    po = oracle_mod.TraceParams()
+    for f in ("camera", "ray_min", "ray_ddx", "ray_ddy"):
+        getattr(po, f)[:] = list(getattr(p, f))
+    po.width, po.height = p.width, p.height
+    import os
+
+    ref = o.trace(po, max(1, len(os.sched_getaffinity(0))))
+    path = hits["path"].astype(np.int64)
+    assert np.all(np.any(path != 0, axis=1)), "every ray hits the terrain"
+    inside = np.all((path >= np.array(lo) + 1) & (path < np.array(hi) - 1), axis=1)
+    assert inside.all(), "every hit lies inside the clipped box"
+    compare_hits(hits, ref)
+    assert len(np.unique(hits["material"])) > 1
+    del om
