@@ -420,10 +420,38 @@ __device__ __forceinline__ uint32_t probe_header(const Grp<G>& g, const uint32_t
     return g.reduce_or(cand);
 }
 
-// Compares the key with the item at `item`; all lanes of the group get the same answer.
+template <int MODE>
+__device__ __forceinline__ uint4 ld4(const uint4* p)
+{
+    if constexpr (MODE == LD_L2)
+        return __ldcg(p);
+    else if constexpr (MODE == LD_STREAM)
+        return __ldcs(p);
+    else
+        return *p;
+}
+
+// Word i of a single thread's key (zero past its ten words).
+__device__ __forceinline__ uint32_t key_word(const Key<1>& key, uint32_t i) { return i < kItemStride ? key.w[i] : 0u; }
+
+// Compares the key with the item at `item`; all lanes of the group get the same answer. A single
+// thread compares 16-byte chunks (items are 16-byte aligned; words past the key's length are not
+// compared).
 template <int G, int MODE = LD_DEFAULT>
 __device__ __forceinline__ bool item_equals(const Grp<G>& g, const uint32_t* item, const Key<G>& key)
 {
+    if constexpr (G == 1) {
+        bool eq = true;
+#pragma unroll
+        for (uint32_t c = 0; c < 3; ++c) {
+            if (4u * c < key.n) {
+                const uint4 v = ld4<MODE>(reinterpret_cast<const uint4*>(item) + c);
+                eq &= (4u * c + 0 >= key.n || v.x == key_word(key, 4u * c + 0)) && (4u * c + 1 >= key.n || v.y == key_word(key, 4u * c + 1))
+                    && (4u * c + 2 >= key.n || v.z == key_word(key, 4u * c + 2)) && (4u * c + 3 >= key.n || v.w == key_word(key, 4u * c + 3));
+            }
+        }
+        return eq;
+    }
     bool eq = true;
 #pragma unroll
     for (int i = 0; i < Grp<G>::KW; ++i) {
@@ -437,11 +465,13 @@ __device__ __forceinline__ bool item_equals(const Grp<G>& g, const uint32_t* ite
 template <int G>
 __device__ __forceinline__ void write_item(const Grp<G>& g, uint32_t* item, const Key<G>& key)
 {
-    if constexpr (G == 1) { // word pairs; the pad word of an odd-length item is written as zero
+    if constexpr (G == 1) { // 16-byte chunks; pad words (inside the slot's stride) are written as zero
 #pragma unroll
-        for (uint32_t i = 0; i < kItemStride; i += 2)
-            if (i < key.n)
-                *reinterpret_cast<uint2*>(item + i) = make_uint2(key.w[i], i + 1 < key.n ? key.w[i + 1] : 0u);
+        for (uint32_t c = 0; c < 3; ++c)
+            if (4u * c < key.n) {
+                auto word = [&](uint32_t i) { return i < key.n ? key_word(key, i) : 0u; };
+                *reinterpret_cast<uint4*>(item + 4u * c) = make_uint4(word(4u * c), word(4u * c + 1), word(4u * c + 2), word(4u * c + 3));
+            }
     } else {
 #pragma unroll
         for (int i = 0; i < Grp<G>::KW; ++i) {
