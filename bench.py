@@ -261,9 +261,10 @@ def max_over_ranks(values, dist=None, device="cuda"):
     return [float(x) for x in t.cpu()]
 
 
-def summarize(res, n_edits, duration_s=None):
+def summarize(res, n_edits, duration_s=None, edits=None):
     """Latency (ms) and throughput of a replay; res = edits then frames. `sustained`: the last edit
-    became visible within 10 % (+0.25 s) of the end of the stream, so no backlog built up."""
+    became visible within 10 % (+0.25 s) of the end of the stream, so no backlog built up. With the
+    edits given, the p99 per radius band too."""
     ed = res[:n_edits]
     lat = (ed["visible_s"] - ed["submit_s"]) * 1e3
     fr = res[n_edits:]
@@ -277,6 +278,10 @@ def summarize(res, n_edits, duration_s=None):
            "mean_edits_per_launch": float(n_edits) / max(1, len(set(ed["launch"].tolist()))), "span_s": span}
     if duration_s is not None:
         out["sustained"] = bool(span <= 1.1 * duration_s + 0.25)
+    if edits is not None and len(edits) == n_edits:
+        radius = np.array([e.radius for e in edits])
+        out["p99_ms_by_radius"] = {f"{lo:g}-{hi:g}": pct(lat[(radius >= lo) & (radius < hi)], 99)
+                                   for lo, hi in ((0, 64), (64, 512), (512, 1e9)) if ((radius >= lo) & (radius < hi)).any()}
     return out
 
 
@@ -388,7 +393,7 @@ def run_serve(args):
             wall = time.perf_counter() - t0
         torch.cuda.synchronize()
         require_ok(res, len(ek), f"{name} timed stream", mem)
-        out[name] = summarize(res, len(ek), dur_k)
+        out[name] = summarize(res, len(ek), dur_k, ek)
         out[name].update(wall_s=wall, memory=mem, frames=frames, tuning=tuning)
         if name == "served":
             out["clocks"] = clocks.summary()
