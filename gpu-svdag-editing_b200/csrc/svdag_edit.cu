@@ -1217,10 +1217,10 @@ svdag_status launch_build(svdag_ctx* ctx, cudaStream_t s)
     const uint32_t LL = d.leafLevel;
     for (uint32_t level = 0; level < LL; ++level) {
         const unsigned long long bound = level < 8 ? (1ull << (3 * level)) : (1ull << 24);
-        k_build_level<TOOL><<<grid_resident(ctx, k_build_level<TOOL>, bound * 8, 256), 256, 0, s>>>(d, q, level, ctx->scratch, ctx->scratchBytes);
+        k_build_level<TOOL><<<grid_for(ctx, bound * 8, 256), 256, 0, s>>>(d, q, level, ctx->scratch, ctx->scratchBytes);
     }
     const unsigned long long bound = LL < 8 ? (1ull << (3 * LL)) : (1ull << 24);
-    k_build_leaves<TOOL><<<grid_resident(ctx, k_build_leaves<TOOL>, bound * 32, 256), 256, 0, s>>>(d, q, ctx->scratch, ctx->scratchBytes);
+    k_build_leaves<TOOL><<<grid_for(ctx, bound * 32, 256), 256, 0, s>>>(d, q, ctx->scratch, ctx->scratchBytes);
     SVDAG_CUDA(cudaGetLastError());
     return SVDAG_OK;
 }
@@ -1293,7 +1293,7 @@ svdag_status launch_phases(svdag_ctx* ctx, uint32_t tool, cudaStream_t s)
     SVDAG_TRY(launch_build_any(ctx, tool, s));
     const uint32_t LL = d.leafLevel;
     for (int level = (int)LL; level >= 0; --level)
-        k_merge_level<<<grid_resident(ctx, k_merge_level, level_bound(level), 256), 256, 0, s>>>(d, level, ctx->scratch);
+        k_merge_level<<<grid_for(ctx, level_bound(level), 256), 256, 0, s>>>(d, level, ctx->scratch);
     k_edit_end<<<1, 32, 0, s>>>(d, ctx->scratch, ctx->queue);
     SVDAG_CUDA(cudaGetLastError());
     return SVDAG_OK;

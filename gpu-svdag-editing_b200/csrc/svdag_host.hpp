@@ -81,16 +81,6 @@ inline unsigned long long used_region_bytes(const svdag_ctx* ctx, unsigned long 
 
 // Number of resident-CTA-sized grid for grid-stride kernels: a multiple of the SM count.
 int grid_for(const svdag_ctx* ctx, unsigned long long work, int threadsPerBlock, int blocksPerSm = 8);
-// Blocks of `threadsPerBlock` threads one SM holds at once for this kernel (its registers and shared
-// memory decide), queried once per kernel.
-int resident_blocks(const void* kernel, int threadsPerBlock);
-// A grid-stride kernel's grid: no more blocks than are resident at once, so that no partial second
-// wave runs the last part of the work at a fraction of the occupancy.
-template <typename K>
-int grid_resident(const svdag_ctx* ctx, K kernel, unsigned long long work, int threadsPerBlock)
-{
-    return grid_for(ctx, work, threadsPerBlock, resident_blocks(reinterpret_cast<const void*>(kernel), threadsPerBlock));
-}
 
 // Table management (svdag_tables.cu).
 // `recycle`: a level table, whose overflow slabs come from and go back to the free lists.

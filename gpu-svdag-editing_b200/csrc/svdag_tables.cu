@@ -5,8 +5,6 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
-#include <utility>
-#include <vector>
 
 #include "svdag_host.hpp"
 
@@ -25,24 +23,6 @@ int grid_for(const svdag_ctx* ctx, unsigned long long work, int threadsPerBlock,
     const unsigned long long maxBlocks = (unsigned long long)smCount * blocksPerSm;
     const unsigned long long need = (work + threadsPerBlock - 1) / threadsPerBlock;
     return (int)std::max<unsigned long long>(1, std::min(maxBlocks, need));
-}
-
-int resident_blocks(const void* kernel, int threadsPerBlock)
-{
-    static std::mutex m;
-    static std::vector<std::pair<std::pair<const void*, int>, int>> known;
-    std::lock_guard<std::mutex> lk(m);
-    for (auto& k : known)
-        if (k.first.first == kernel && k.first.second == threadsPerBlock)
-            return k.second;
-    int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threadsPerBlock, 0) != cudaSuccess || n < 1) {
-        cudaGetLastError();
-        n = 1;
-    }
-    n = std::min(n, 8);
-    known.push_back({ { kernel, threadsPerBlock }, n });
-    return n;
 }
 
 svdag_status read_status(svdag_ctx* ctx, cudaStream_t s)
@@ -343,18 +323,6 @@ __global__ void k_table_walk(DevDag d, DevTable t, unsigned long long* counters,
     }
 }
 
-// Grid-stride table kernels get exactly as many blocks as are resident at once (their register use
-// decides how many fit on an SM): a grid larger than that leaves a partial second wave that runs the
-// last part of the keys at a fraction of the occupancy.
-template <int G, int OP>
-void launch_op(const svdag_ctx* ctx, unsigned long long workThreads, cudaStream_t s, const DevDag& d, const DevTable& t,
-    const uint32_t* keys, const uint32_t* offsets, uint32_t n, unsigned long long totalWords, const uint32_t* reps, uint32_t* out)
-{
-    constexpr int threads = 256;
-    const int grid = grid_resident(ctx, k_table_op<G, OP>, workThreads, threads);
-    k_table_op<G, OP><<<grid, threads, 0, s>>>(d, t, keys, offsets, n, totalWords, reps, out);
-}
-
 template <int OP>
 svdag_status launch_table_op(svdag_table* t, const uint32_t* keys, const uint32_t* offsets, uint32_t n,
     unsigned long long totalWords, const uint32_t* reps, uint32_t* out, uint32_t lanes, cudaStream_t s)
@@ -362,26 +330,28 @@ svdag_status launch_table_op(svdag_table* t, const uint32_t* keys, const uint32_
     svdag_ctx* ctx = t->ctx;
     if (!lanes)
         lanes = ctx->probeLanes;
+    const int threads = 256;
     const unsigned long long workThreads = (unsigned long long)n * lanes;
+    const int grid = grid_for(ctx, workThreads, threads, 8);
     const DevDag d = ctx->dag();
     switch (lanes) {
     case 1:
-        launch_op<1, OP>(ctx, workThreads, s, d, t->dev, keys, offsets, n, totalWords, reps, out);
+        k_table_op<1, OP><<<grid, threads, 0, s>>>(d, t->dev, keys, offsets, n, totalWords, reps, out);
         break;
     case 2:
-        launch_op<2, OP>(ctx, workThreads, s, d, t->dev, keys, offsets, n, totalWords, reps, out);
+        k_table_op<2, OP><<<grid, threads, 0, s>>>(d, t->dev, keys, offsets, n, totalWords, reps, out);
         break;
     case 4:
-        launch_op<4, OP>(ctx, workThreads, s, d, t->dev, keys, offsets, n, totalWords, reps, out);
+        k_table_op<4, OP><<<grid, threads, 0, s>>>(d, t->dev, keys, offsets, n, totalWords, reps, out);
         break;
     case 8:
-        launch_op<8, OP>(ctx, workThreads, s, d, t->dev, keys, offsets, n, totalWords, reps, out);
+        k_table_op<8, OP><<<grid, threads, 0, s>>>(d, t->dev, keys, offsets, n, totalWords, reps, out);
         break;
     case 16:
-        launch_op<16, OP>(ctx, workThreads, s, d, t->dev, keys, offsets, n, totalWords, reps, out);
+        k_table_op<16, OP><<<grid, threads, 0, s>>>(d, t->dev, keys, offsets, n, totalWords, reps, out);
         break;
     case 32:
-        launch_op<32, OP>(ctx, workThreads, s, d, t->dev, keys, offsets, n, totalWords, reps, out);
+        k_table_op<32, OP><<<grid, threads, 0, s>>>(d, t->dev, keys, offsets, n, totalWords, reps, out);
         break;
     default:
         return SVDAG_ERR_INVALID;

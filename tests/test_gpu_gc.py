@@ -186,3 +186,39 @@ def test_long_served_stream_reclaims_memory(svdag_lib, oracle_mod, plain):
         o.edit(to_oracle(oracle_mod, e))
     assert gpu_canon(oracle_mod, g) == o.canon()
     g.free()
+
+
+def test_serving_loop_rejects_an_edit_that_cannot_fit(svdag_lib, oracle_mod):
+    """Admission never launches an edit whose reserve exceeds the room left after a collection: it
+    fails with SVDAG_ERR_OOM up front (counted as rejected), the DAG is left as it was, and the edits
+    around it are served. With collection switched off the same holds without a collection."""
+    for gc in (True, False):
+        g = svdag_lib.MyGPUHashDAG(LEVELS, pool_bytes=1 << 30)
+        g.build_terrain(**SCENE)
+        used0 = g.stats().item_region_used_bytes
+        cam = svdag_lib.get_trace_params((512.0, 950.0, 150.0), (512.0, 550.0, 512.0), 160, 90)
+        L = oracle_mod.lib()
+        p = oracle_mod.TerrainParams(**SCENE)
+        h = L.oracle_terrain_height(p, LEVELS, 300, 300)
+        small = to_svdag_edit(svdag_lib, 0, 3, (300.0, float(h), 300.0), 6.0)
+        huge = to_svdag_edit(svdag_lib, 0, 5, (512.0, 512.0, 512.0), 2000.0)  # reserve of gigabytes
+        with svdag_lib.Server(g, cam, memory_cap_bytes=used0 + (64 << 20), gc=gc) as srv:
+            t1 = srv.submit_edit(small)
+            r1 = srv.poll(t1)
+            root1 = r1.root_after
+            t2 = srv.submit_edit(huge)
+            r2 = srv.poll(t2)
+            t3 = srv.submit_edit(to_svdag_edit(svdag_lib, 1, 0, (300.0, float(h), 300.0), 6.0))
+            r3 = srv.poll(t3)
+            mem = srv.memory()
+        assert r1.status == 0 and r3.status == 0
+        assert r2.status == 2  # SVDAG_ERR_OOM, before launch
+        assert mem["rejected_edits"] == 1 and mem["failed_edits"] == 0
+        assert (mem["gc_runs"] >= 1) == gc
+        assert r3.root_after != root1
+        o = oracle_mod.OracleDag(LEVELS)
+        o.build_terrain(oracle_mod.TerrainParams(**SCENE))
+        o.edit(to_oracle(oracle_mod, small))
+        o.edit(to_oracle(oracle_mod, to_svdag_edit(svdag_lib, 1, 0, (300.0, float(h), 300.0), 6.0)))
+        assert gpu_canon(oracle_mod, g) == o.canon()  # the huge edit left no trace
+        g.free()
