@@ -158,6 +158,34 @@ __device__ __forceinline__ uint32_t should_edit(const DevEditor& e, uint32_t px,
     }
 }
 
+// should_edit for one voxel (depth 0) in the leaf phase. For the sphere and box add/remove tools and
+// the sphere paint, Fill and Subdivide of a voxel end in the same get_new_value (the fill material,
+// nothing, or the paint material), and a node that is contained also overlaps, so the overlap test
+// alone decides the voxel: Keep when it does not overlap, Empty for paint on an empty voxel, else
+// Subdivide. The containment test is skipped; every other tool takes should_edit.
+template <uint32_t TOOL>
+__device__ __forceinline__ uint32_t voxel_op(const DevEditor& e, uint32_t vx, uint32_t vy, uint32_t vz, uint32_t state, uint32_t& fillMaterial)
+{
+    if constexpr (TOOL == SVDAG_TOOL_SPHERE_ADD || TOOL == SVDAG_TOOL_SPHERE_REMOVE || TOOL == SVDAG_TOOL_SPHERE_PAINT
+        || TOOL == SVDAG_TOOL_BOX_ADD || TOOL == SVDAG_TOOL_BOX_REMOVE) {
+        const float nmin[3] = { float(vx), float(vy), float(vz) }; // Path::as_position at depth 0
+        const float nmax[3] = { nmin[0] + 1.0f, nmin[1] + 1.0f, nmin[2] + 1.0f };
+        bool overlaps;
+        if constexpr (TOOL == SVDAG_TOOL_BOX_ADD || TOOL == SVDAG_TOOL_BOX_REMOVE)
+            overlaps = box_overlap(e, nmin, nmax);
+        else
+            overlaps = sphere_overlap(e, nmin, nmax);
+        fillMaterial = e.material;
+        if (!overlaps)
+            return OP_KEEP;
+        if (TOOL == SVDAG_TOOL_SPHERE_PAINT && state == ST_EMPTY)
+            return OP_EMPTY;
+        return OP_SUBDIVIDE;
+    } else {
+        return should_edit<TOOL>(e, vx, vy, vz, 0, state, fillMaterial);
+    }
+}
+
 // MyGpuCopyEditor::should_edit with state (the "#if 1" form, my_gpu_dag_editors.h:173-217).
 __device__ uint32_t copy_should_edit(const DevEditor& e, const DevDag& d, uint32_t px, uint32_t py, uint32_t pz, uint32_t depth,
     const CopyParent* in, CopyParent* out)
@@ -516,7 +544,7 @@ __device__ void ph_build_leaves(const DevDag& d, const DevEditor& e, char* scrat
                 ++edited;
             } else {
                 uint32_t fm = 0;
-                const uint32_t op = should_edit<TOOL>(e, vx, vy, vz, 0, hasOld ? ST_FILLED : ST_EMPTY, fm);
+                const uint32_t op = voxel_op<TOOL>(e, vx, vy, vz, hasOld ? ST_FILLED : ST_EMPTY, fm);
                 if (op != OP_KEEP)
                     ++edited;
                 if (op == OP_FILL || op == OP_SUBDIVIDE) {

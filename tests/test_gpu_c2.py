@@ -165,5 +165,5 @@ def test_c2_1080p_frame_equals_the_oracle_in_a_clipped_region(svdag_lib, oracle_
     inside = np.all((path >= np.array(lo) + 1) & (path < np.array(hi) - 1), axis=1)
     assert inside.all(), "every hit lies inside the clipped box"
     compare_hits(hits, ref)
-    assert len(np.unique(path, axis=0)) > 100000  # a real view: the rays reach many distinct voxels
+    assert len(np.unique(path, axis=0)) > 10000  # a real view: the rays reach many distinct voxels
     del om
