@@ -9,7 +9,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libsvdag.so")
-SOURCES = ["svdag_ctx.cu", "svdag_tables.cu", "svdag_edit.cu", "svdag_scene.cu", "svdag_server.cu", "svdag_trace.cu", "svdag_tune.cu", "svdag_replay.cu", "svdag_io.cu", "svdag_alt_tables.cu"]
+SOURCES = ["svdag_ctx.cu", "svdag_tables.cu", "svdag_edit.cu", "svdag_scene.cu", "svdag_server.cu", "svdag_trace.cu", "svdag_tune.cu", "svdag_replay.cu", "svdag_io.cu", "svdag_v3.cu", "svdag_alt_tables.cu"]
 HEADERS = ["svdag_device.cuh", "svdag_edit.cuh", "svdag_scene.cuh", "svdag_host.hpp", "svdag_hash.h", "svdag_alt_tables.cuh", "svdag_serve_geometry.h", "svdag_snapshot.h"]
 NVCC = os.environ.get("NVCC", "nvcc")
 

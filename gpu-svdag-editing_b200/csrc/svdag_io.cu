@@ -3,8 +3,9 @@
 // Items of a DAG travel as per-level item lists ("item snapshots"): level l holds its items packed
 // one after another (nodes: header + one word per child; leaves: 2 mask words + packed 4-bit
 // materials), and a node's child words are ordinals into the item list of level l + 1. Item 0 of
-// level 0 is the root. Snapshots stand in for MyGPUHashDAG::writeTo/readFrom (my_gpu_hash_dag.cu:
-// 158-177), which dump the raw hash tables and can only be read back by the same table layout.
+// level 0 is the root. Snapshots are the portable form; the reference's own file
+// (MyGPUHashDAG::writeTo/readFrom, my_gpu_hash_dag.cu:158-177, a dump of its raw hash tables)
+// converts to and from them in svdag_v3.cu.
 //
 // The reference's BasicDAG geometry files (BasicDAGFactory::load_dag_from_file, basic_dag.cpp:
 // 108-122) convert into a snapshot as MyGPUHashDAGFactory's create_dag_cpu converts them without

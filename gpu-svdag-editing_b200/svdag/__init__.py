@@ -24,6 +24,7 @@ PKG_ROOT = os.path.dirname(HERE)
 LIB_PATH = os.path.join(PKG_ROOT, "libsvdag.so")
 
 MAX_LEVELS = 17
+V3_GPU_MANAGED, V3_GPU_MALLOC, V3_GPU_ASYNC, V3_CPU = 0, 1, 2, 3  # EMemoryType values of a v3 file, memory.h:17-23
 MAX_ITEM_WORDS = 10
 NUM_SIZE_CLASSES = 9
 NUM_MATERIALS = 16
@@ -246,6 +247,8 @@ _PROTOS = {
     "svdag_shade": [_P, C.POINTER(TraceParams), C.POINTER(ShadeParams), _P, _P, _P, _P, _P],
     "svdag_load_items": [_P, _P, _P, _P, _P],
     "svdag_basic_dag_to_items": [_P, _U64, _U32, _U32, _P, _U64, _P, _P, C.POINTER(_U64)],
+    "svdag_v3_to_items": [_P, _U64, _U32, _P, _U64, _P, _P, C.POINTER(_U64)],
+    "svdag_items_to_v3": [_P, _P, _P, _U32, _U32, C.c_char_p],
 }
 EXPORTED = tuple(_PROTOS)
 
@@ -539,8 +542,8 @@ class MyGPUHashDAG:
         return handles[: n.value], words[: n.value]
 
     def save_items(self, stream=None) -> "ItemSnapshot":
-        """The items reachable from the root as an item snapshot (svdag_save_items); stands in for
-        MyGPUHashDAG::writeTo (my_gpu_hash_dag.cu:158-165)."""
+        """The items reachable from the root as an item snapshot (svdag_save_items), the portable form
+        that writeTo converts to the reference's file."""
         nl = self.levels - 1
         lw, li, total = np.zeros(nl, np.uint64), np.zeros(nl, np.uint64), C.c_uint64()
         words = np.zeros(0, np.uint32)
@@ -554,8 +557,8 @@ class MyGPUHashDAG:
             return ItemSnapshot(self.levels, words[: total.value], lw, li)
 
     def load_items(self, snap: "ItemSnapshot", stream=None):
-        """Replaces the DAG by an item snapshot (svdag_load_items); stands in for
-        MyGPUHashDAG::readFrom (my_gpu_hash_dag.cu:167-177)."""
+        """Replaces the DAG by an item snapshot (svdag_load_items), the portable form that readFrom
+        converts the reference's file to."""
         if snap.levels != self.levels:
             raise SvdagError(1, f"svdag_load_items: snapshot of {snap.levels} levels, DAG of {self.levels}")
         w = np.ascontiguousarray(snap.words, dtype=np.uint32)
@@ -565,10 +568,22 @@ class MyGPUHashDAG:
                                       stream_ptr(stream)), "svdag_load_items")
 
     def write_to(self, path: str):
+        """Writes the DAG as a portable item snapshot file (ItemSnapshot.write)."""
         self.save_items().write(path)
 
     def read_from(self, path: str):
+        """Replaces the DAG by an item snapshot file (ItemSnapshot.read)."""
         self.load_items(ItemSnapshot.read(path))
+
+    def writeTo(self, path: str, memory_type: int = V3_GPU_MALLOC):
+        """MyGPUHashDAG::writeTo (my_gpu_hash_dag.cu:158-165): the DAG as the reference's own version-3
+        file, which the reference's readFrom loads (svdag_save_items, then svdag_items_to_v3)."""
+        items_to_v3(self.save_items(), path, memory_type)
+
+    def readFrom(self, path: str):
+        """MyGPUHashDAG::readFrom (my_gpu_hash_dag.cu:167-177): replaces the DAG by a version-3 file
+        the reference wrote (svdag_v3_to_items, then svdag_load_items)."""
+        self.load_items(v3_to_items(path, self.levels))
 
     def load_basic_dag(self, path: str, material: int = 0) -> "BasicDAGFile":
         """Loads a BasicDAG geometry file of the reference (BasicDAGFactory::load_dag_from_file,
@@ -665,6 +680,34 @@ def basic_dag_to_items(data, levels: int, material: int = 0) -> ItemSnapshot:
     _check(lib().svdag_basic_dag_to_items(d.ctypes.data, len(d), levels, material, words.ctypes.data, len(words),
                                           lw.ctypes.data, li.ctypes.data, C.byref(total)), "svdag_basic_dag_to_items")
     return ItemSnapshot(levels, words[: total.value], lw, li)
+
+
+def v3_to_items(path: str, levels: int) -> ItemSnapshot:
+    """A version-3 DAG file of the reference (MyGPUHashDAG::writeTo) -> item snapshot
+    (svdag_v3_to_items, a host function). The file is mapped, not read into memory."""
+    size = os.path.getsize(path)
+    data = np.memmap(path, dtype=np.uint8, mode="r") if size else np.zeros(0, np.uint8)
+    base = data.ctypes.data if size else None
+    nl = levels - 1
+    lw, li, total = np.zeros(nl, np.uint64), np.zeros(nl, np.uint64), C.c_uint64()
+    st = lib().svdag_v3_to_items(base, size, levels, None, 0, lw.ctypes.data, li.ctypes.data, C.byref(total))
+    if st not in (0, 2):
+        _check(st, "svdag_v3_to_items")
+    words = np.zeros(max(total.value, 1), np.uint32)
+    _check(lib().svdag_v3_to_items(base, size, levels, words.ctypes.data, len(words), lw.ctypes.data, li.ctypes.data,
+                                   C.byref(total)), "svdag_v3_to_items")
+    del data
+    return ItemSnapshot(levels, words[: total.value], lw, li)
+
+
+def items_to_v3(snap: ItemSnapshot, path: str, memory_type: int = V3_GPU_MALLOC):
+    """Item snapshot -> the reference's version-3 DAG file (svdag_items_to_v3, a host function);
+    `memory_type` is the EMemoryType the file records (V3_*)."""
+    words = np.ascontiguousarray(snap.words, dtype=np.uint32)
+    lw = np.ascontiguousarray(snap.level_words, dtype=np.uint64)
+    li = np.ascontiguousarray(snap.level_items, dtype=np.uint64)
+    _check(lib().svdag_items_to_v3(words.ctypes.data if len(words) else None, lw.ctypes.data, li.ctypes.data, snap.levels,
+                                   memory_type, os.fsencode(path)), "svdag_items_to_v3")
 
 
 class HashTable:

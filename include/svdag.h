@@ -453,9 +453,9 @@ svdag_status svdag_export_level(svdag_ctx* ctx, uint32_t level, uint32_t* out_ha
 /* An item snapshot: level l (0 .. levels-2) holds level_items[l] items packed in level_words[l]
  * words (nodes: header + one word per child; leaves: 2 mask words + packed 4-bit materials), the
  * levels one after another. A node's child words are ordinals into the item list of the level below
- * and item 0 of level 0 is the root; all counts 0 is the empty DAG. Snapshots stand in for
- * MyGPUHashDAG::writeTo / readFrom (my_gpu_hash_dag.cu:158-177), whose raw table dump only the same
- * table layout can read back. */
+ * and item 0 of level 0 is the root; all counts 0 is the empty DAG. Snapshots are the portable
+ * form; the reference's own file (MyGPUHashDAG::writeTo / readFrom, my_gpu_hash_dag.cu:158-177)
+ * converts to and from them with svdag_v3_to_items / svdag_items_to_v3 below. */
 
 /* Writes the items reachable from the current root, each level in ascending handle order. Fills
  * level_words and level_items (levels - 1 entries each) and *total_words; writes the words when
@@ -476,6 +476,33 @@ svdag_status svdag_load_items(svdag_ctx* ctx, const uint32_t* words, const uint6
  * index out of range or an empty item gives SVDAG_ERR_CORRUPT. */
 svdag_status svdag_basic_dag_to_items(const uint32_t* data, uint64_t n_words, uint32_t levels, uint32_t material,
     uint32_t* out_words, uint64_t capacity, uint64_t* level_words, uint64_t* level_items, uint64_t* total_words);
+
+/* The reference's own DAG file: what MyGPUHashDAG::writeTo writes and readFrom reads, format
+ * version 3 (my_gpu_hash_dag.cu:158-177), in the reference's default configuration
+ * (configuration/gpu_hash_dag_definitions.h: CompactAccelerationHash tables, SlabHashXor buckets,
+ * first slabs stored in the table, 4 material bits). Values of EMemoryType (memory.h:17-23) as the
+ * file records them: */
+#define SVDAG_V3_GPU_MANAGED 0u
+#define SVDAG_V3_GPU_MALLOC 1u /* the engine's MyGPUHashDAG<EMemoryType::GPU_Malloc> */
+#define SVDAG_V3_GPU_ASYNC 2u
+#define SVDAG_V3_CPU 3u /* MyGPUHashDAG<EMemoryType::CPU> */
+/* Host function: converts a version-3 file held in `data` (n_bytes, 4-byte aligned) into a snapshot,
+ * following the handles from its root; output as svdag_save_items. The file's scene depth (the
+ * width of its fully-filled node array, the reference's SCENE_DEPTH) must equal `levels`
+ * (SVDAG_ERR_INVALID otherwise); another version or table configuration gives
+ * SVDAG_ERR_UNSUPPORTED; a truncated file or a handle that does not name an occupied slot holding an
+ * item of the handle's size gives SVDAG_ERR_CORRUPT. An empty DAG (root 0xFFFFFFFF) gives all
+ * counts 0. */
+svdag_status svdag_v3_to_items(const void* data, uint64_t n_bytes, uint32_t levels, uint32_t* out_words,
+    uint64_t capacity, uint64_t* level_words, uint64_t* level_items, uint64_t* total_words);
+/* Host function: writes a snapshot (as svdag_load_items takes it) to `path` as a version-3 file
+ * whose arrays record `memory_type` (SVDAG_V3_*): the fully-filled items of every level and material
+ * that MyGPUHashDAG::allocate inserts (my_gpu_hash_dag.cu:29-65), then the snapshot's distinct
+ * items, each table sized to 96 items per bucket (TARGET_LOAD_FACTOR) and every item in a slot of
+ * its bucket's slab chain, where the reference's find looks for it. A snapshot that does not parse gives
+ * SVDAG_ERR_INVALID; one whose handles would not fit the reference's 29-bit index SVDAG_ERR_OOM. */
+svdag_status svdag_items_to_v3(const uint32_t* words, const uint64_t* level_words, const uint64_t* level_items,
+    uint32_t levels, uint32_t memory_type, const char* path);
 
 /* ---------------------------------------------------------------- autotuner
  *

@@ -1,5 +1,6 @@
 """ctypes binding of oracle/_ref/libref.so: the reference's own editors, item codecs and
-DAGUtils::get_value (oracle/ref_harness.cu), built by oracle/build_ref.py.
+DAGUtils::get_value (oracle/ref_harness.cu), and its host DAG with the writeTo / readFrom file
+format (oracle/ref_v3_harness.cu), built by oracle/build_ref.py.
 
 TEST INFRASTRUCTURE ONLY: the tests use it to check the oracle (and, on a GPU, the CUDA library's
 exported DAG) against reference code. `lib()` returns None where the library is neither built nor
@@ -54,6 +55,17 @@ def lib():
         getattr(L, f).restype = C.c_uint32
         getattr(L, f).argtypes = [C.c_uint32, C.c_uint32]
     L.ref_header_fully_filled.argtypes = [C.c_uint32, C.POINTER(C.c_uint32)]
+    L.ref_v3_levels.restype = C.c_uint32
+    L.ref_v3_levels.argtypes = []
+    L.ref_v3_write.argtypes = [P, P, P, C.c_char_p]
+    L.ref_v3_open.restype = P
+    L.ref_v3_open.argtypes = [C.c_char_p]
+    L.ref_v3_close.restype = None
+    L.ref_v3_close.argtypes = [P]
+    L.ref_v3_root.restype = C.c_uint32
+    L.ref_v3_root.argtypes = [P]
+    L.ref_v3_items.argtypes = [P, P, C.c_uint64, P, P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+    L.ref_v3_get_values.argtypes = [P, P, C.c_uint64, P]
     _lib = L
     return _lib
 
@@ -118,3 +130,59 @@ def items_from_dumps(levels: int, root: int, dumps) -> np.ndarray:
             k = bin(int(out[r, 0]) & 0xFF).count("1")
             out[r, 1:1 + k] = [where[(level + 1, int(c))] for c in out[r, 1:1 + k]]
     return out
+
+
+def v3_levels() -> int:
+    """The scene depth the reference's DAG was compiled with (SCENE_DEPTH)."""
+    return int(lib().ref_v3_levels())
+
+
+def v3_write(words: np.ndarray, level_words: np.ndarray, level_items: np.ndarray, path: str):
+    """Builds the reference's host DAG from an item snapshot of v3_levels() levels and writes it
+    with MyGPUHashDAG::writeTo. Needs a CUDA driver (the reference's host arrays are copied with
+    cudaMemcpy)."""
+    w = np.ascontiguousarray(words, dtype=np.uint32)
+    lw = np.ascontiguousarray(level_words, dtype=np.uint64)
+    li = np.ascontiguousarray(level_items, dtype=np.uint64)
+    if lib().ref_v3_write(_p(w) if len(w) else None, _p(lw), _p(li), os.fsencode(path)) != 0:
+        raise ValueError("the snapshot does not parse")
+
+
+class RefV3Dag:
+    """A version-3 DAG file loaded by the reference's MyGPUHashDAG::readFrom (host memory; needs a
+    CUDA driver, like v3_write)."""
+
+    def __init__(self, path: str):
+        self.h = lib().ref_v3_open(os.fsencode(path))
+
+    def close(self):
+        if self.h:
+            lib().ref_v3_close(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def root(self) -> int:
+        return int(lib().ref_v3_root(self.h))
+
+    def items(self):
+        """(words, level_words, level_items, found): the reachable items as a snapshot read through
+        the reference's accessors, and how many of them its find locates at their own handle."""
+        nl = v3_levels() - 1
+        lw, li = np.zeros(nl, np.uint64), np.zeros(nl, np.uint64)
+        total, found = C.c_uint64(), C.c_uint64()
+        lib().ref_v3_items(self.h, None, 0, _p(lw), _p(li), C.byref(total), C.byref(found))
+        words = np.zeros(max(total.value, 1), np.uint32)
+        assert lib().ref_v3_items(self.h, _p(words), len(words), _p(lw), _p(li), C.byref(total), C.byref(found)) == 0
+        return words[: total.value], lw, li, found.value
+
+    def get_values(self, xyz: np.ndarray) -> np.ndarray:
+        xyz = np.ascontiguousarray(xyz, dtype=np.uint32).reshape(-1, 3)
+        out = np.empty(len(xyz), dtype=np.uint32)
+        lib().ref_v3_get_values(self.h, _p(xyz), len(xyz), _p(out))
+        return out
