@@ -920,19 +920,13 @@ def run_mode_trace(args):
                       "hit_fraction": float((hits["material"] != 255).mean())}))
 
 
-def run_mode_c3(args):
-    """256 edits of uneven footprint: one batched persistent launch against the plain per-edit path,
-    each on its own copy of the scene; the stored item sets must be equal."""
-    import torch
-
-    import svdag
-    import svdag.workloads as w
-
-    edits = w.c3_edits(levels=args.levels, terrain=make_terrain(w, args.levels), rmax=4096.0 * (1 << args.levels) / 131072)
-    res = {}
-    items = {}
+def c3_compare(svdag, w, torch, levels, edits):
+    """The edits through the plain per-edit path and through one batch (the persistent kernel for small
+    edits, subtree groups for runs of small edits in disjoint nodes), each on its own copy of the
+    scene; the stored item sets must be equal."""
+    res, items = {}, {}
     for name in ("plain", "batched"):
-        dag, _ = make_scene(svdag, w, args.levels)
+        dag, _ = make_scene(svdag, w, levels, persistent=name == "batched")
         stream = torch.cuda.Stream()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
@@ -946,10 +940,27 @@ def run_mode_c3(args):
         torch.cuda.synchronize()
         dag.sync()
         res[name] = a.elapsed_time(b)
-        items[name] = [dag.table(l).stats().items for l in range(args.levels - 1)]
+        items[name] = [dag.table(l).stats().items for l in range(levels - 1)]
         dag.free()
-    print(json.dumps({"edits": len(edits), "plain_ms": res["plain"], "batched_ms": res["batched"],
-                      "items_equal": items["plain"] == items["batched"]}))
+    return {"edits": len(edits), "plain_ms": res["plain"], "batched_ms": res["batched"],
+            "items_equal": items["plain"] == items["batched"]}
+
+
+def run_mode_c3(args):
+    """256 edits of uneven footprint (radius log-uniform up to 4096 at depth 17), and 256 small edits
+    of the same mix (radius 4..16) scattered over the surface: the batched form against the plain
+    per-edit path."""
+    import torch
+
+    import svdag
+    import svdag.workloads as w
+
+    terrain = make_terrain(w, args.levels)
+    c3 = w.c3_edits(levels=args.levels, terrain=terrain, rmax=4096.0 * (1 << args.levels) / 131072)
+    small = w.c3_edits(levels=args.levels, terrain=terrain, rmax=16.0, seed=5)
+    out = c3_compare(svdag, w, torch, args.levels, c3)
+    out["small_scattered"] = c3_compare(svdag, w, torch, args.levels, small)
+    print(json.dumps(out))
 
 
 def main():

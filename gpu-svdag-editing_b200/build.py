@@ -10,7 +10,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libsvdag.so")
 SOURCES = ["svdag_ctx.cu", "svdag_tables.cu", "svdag_edit.cu", "svdag_scene.cu", "svdag_server.cu", "svdag_trace.cu", "svdag_tune.cu", "svdag_replay.cu", "svdag_io.cu", "svdag_v3.cu", "svdag_alt_tables.cu"]
-HEADERS = ["svdag_device.cuh", "svdag_edit.cuh", "svdag_scene.cuh", "svdag_host.hpp", "svdag_hash.h", "svdag_alt_tables.cuh", "svdag_serve_geometry.h", "svdag_snapshot.h"]
+HEADERS = ["svdag_device.cuh", "svdag_edit.cuh", "svdag_scene.cuh", "svdag_host.hpp", "svdag_hash.h", "svdag_alt_tables.cuh", "svdag_serve_geometry.h", "svdag_snapshot.h", "svdag_subtree.h"]
 NVCC = os.environ.get("NVCC", "nvcc")
 
 # -fmad=false: the editors' float predicates decide the DAG structure and the tracer's decide the

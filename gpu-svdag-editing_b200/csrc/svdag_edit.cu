@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "svdag_edit.cuh"
+#include "svdag_subtree.h"
 #include "svdag_host.hpp"
 
 
@@ -249,17 +250,24 @@ __device__ __forceinline__ bool leaf_get_material(uint32_t lo, uint32_t hi, cons
 
 __device__ __forceinline__ unsigned long long work_stride(uint32_t tool) { return tool == SVDAG_TOOL_COPY ? 16ull + 128ull : 16ull; }
 
+// Child index, at level l, of the node on the path from the root to the node (L0, path).
+__device__ __forceinline__ uint32_t spine_child(const uint32_t* path, uint32_t L0, uint32_t l)
+{
+    const uint32_t s = L0 - 1u - l;
+    return (((path[0] >> s) & 1u) << 2) | (((path[1] >> s) & 1u) << 1) | ((path[2] >> s) & 1u);
+}
+
 __device__ void ph_edit_begin(const DevDag& d, const DevEditor& e, char* scratch)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0)
+    if (threadIdx.x != 0 || ph_block(d) != 0)
         return;
     Control* c = d.ctl;
     if (e.saveRoot)
         c->savedRoot = c->root;
-    EditCounters& E = c->edit;
+    EditCounters& E = *d.edit;
     const uint32_t root = c->root;
     E.rootBefore = root;
-    if (!e.builder) { // MyGPUHashDAGUndoRedo::add_frame (my_gpu_base_dag.h:23-34), ring of undoDepth frames
+    if (!e.builder && !e.subtree) { // MyGPUHashDAGUndoRedo::add_frame (my_gpu_base_dag.h:23-34), ring of undoDepth frames
         const bool same = c->undoCount > 0 && c->undo[(c->undoHead + 63u) & 63u] == root;
         if (!same) {
             c->redoCount = 0;
@@ -274,7 +282,18 @@ __device__ void ph_edit_begin(const DevDag& d, const DevEditor& e, char* scratch
     E.count[L0] = 1;
     E.offW[L0] = 0;
     WorkItem* w = reinterpret_cast<WorkItem*>(scratch);
-    w[0] = WorkItem { e.startPath[0], e.startPath[1], e.startPath[2], L0 == 0 ? root : kNone };
+    uint32_t start = L0 == 0 ? root : kNone;
+    if (e.subtree) { // the node (L0, startPath) of the current DAG, reached from the root
+        start = root;
+        for (uint32_t l = 0; l < L0 && start != kNone; ++l) {
+            const uint32_t* node = item_ptr(d, start);
+            const uint32_t c = spine_child(e.startPath, L0, l);
+            const uint32_t mask = node[0] & 0xFFu;
+            start = (mask >> c) & 1u ? node[1 + __popc(mask & ((1u << c) - 1u))] : kNone;
+        }
+        *e.tileOut = kKeep;
+    }
+    w[0] = WorkItem { e.startPath[0], e.startPath[1], e.startPath[2], start };
     if (e.tool == SVDAG_TOOL_COPY) { // createInitialState, my_gpu_dag_editors.h:148-155
         CopyParent* st = reinterpret_cast<CopyParent*>(scratch + 16);
         for (int i = 0; i < 8; ++i)
@@ -289,13 +308,13 @@ __device__ void ph_edit_begin(const DevDag& d, const DevEditor& e, char* scratch
 template <uint32_t TOOL>
 __device__ void ph_build_level(const DevDag& d, const DevEditor& e, uint32_t level, char* scratch, unsigned long long scratchBytes)
 {
-    EditCounters& E = d.ctl->edit;
+    EditCounters& E = *d.edit;
     const unsigned long long stride = work_stride(TOOL);
     const uint32_t n = E.count[level];
     const unsigned long long offW = E.offW[level];
     const unsigned long long offN = align256(offW + n * stride);
     const unsigned long long offWn = align256(offN + (unsigned long long)n * 4 * kItemStride);
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (ph_block(d) == 0 && threadIdx.x == 0) {
         E.offN[level] = offN;
         E.offW[level + 1] = offWn;
     }
@@ -308,9 +327,9 @@ __device__ void ph_build_level(const DevDag& d, const DevEditor& e, uint32_t lev
     }
     const uint32_t lane = threadIdx.x & 31u, c = lane & 7u, grp = lane >> 3;
     const uint32_t childLevel = level + 1, childDepth = d.levels - childLevel;
-    const uint32_t warpsTotal = gridDim.x * (blockDim.x >> 5);
+    const uint32_t warpsTotal = ph_grid(d) * (blockDim.x >> 5);
     unsigned long long edited = 0, oldRead = 0;
-    for (uint32_t base = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 4; base < n; base += warpsTotal * 4) {
+    for (uint32_t base = (ph_block(d) * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 4; base < n; base += warpsTotal * 4) {
         const uint32_t i = base + grp;
         const bool active = i < n;
         WorkItem w { 0, 0, 0, kNone };
@@ -408,14 +427,14 @@ __device__ void ph_build_leaves(const DevDag& d, const DevEditor& e, char* scrat
 {
     __shared__ __align__(16) uint32_t packBuf[16][16]; // per warp of a block of up to 512 threads: 64 material bytes
     __shared__ uint2 erodeBuf[TOOL == SVDAG_TOOL_SPHERE_ERODE ? 16 : 1][27]; // erosion: per warp, the neighbour leaf masks
-    EditCounters& E = d.ctl->edit;
+    EditCounters& E = *d.edit;
     const uint32_t LL = d.leafLevel;
     const unsigned long long stride = work_stride(TOOL);
     const uint32_t n = E.count[LL];
     const unsigned long long offW = E.offW[LL];
     const unsigned long long offN = align256(offW + n * stride);
     const unsigned long long buildTop = align256(offN + (unsigned long long)n * 4 * kItemStride);
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (ph_block(d) == 0 && threadIdx.x == 0) {
         E.offN[LL] = offN;
         E.buildTop = buildTop;
     }
@@ -431,8 +450,8 @@ __device__ void ph_build_leaves(const DevDag& d, const DevEditor& e, char* scrat
             atomicExch(&E.overflow, 1u);
         return;
     }
-    const unsigned long long tid = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
-    const unsigned long long nthreads = (unsigned long long)gridDim.x * blockDim.x;
+    const unsigned long long tid = ph_block(d) * (unsigned long long)blockDim.x + threadIdx.x;
+    const unsigned long long nthreads = (unsigned long long)ph_grid(d) * blockDim.x;
     {
         unsigned long long off = buildTop;
         for (int l = (int)LL; l >= 0; --l) {
@@ -449,7 +468,7 @@ __device__ void ph_build_leaves(const DevDag& d, const DevEditor& e, char* scrat
     }
 
     const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t warpsTotal = gridDim.x * (blockDim.x >> 5);
+    const uint32_t warpsTotal = ph_grid(d) * (blockDim.x >> 5);
     unsigned long long edited = 0, oldRead = 0;
     uint32_t fullLeaves = 0;
     // Software pipeline over the warp's leaves: the work item two ahead and the old leaf one ahead are
@@ -459,7 +478,7 @@ __device__ void ph_build_leaves(const DevDag& d, const DevEditor& e, char* scrat
         return k < n ? *reinterpret_cast<const WorkItem*>(scratch + offW + k * stride) : WorkItem { 0, 0, 0, kNone };
     };
     auto leaf_word = [&](uint32_t h) { return (h != kNone && lane < kItemStride) ? item_ptr(d, h)[lane] : 0u; };
-    uint32_t i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    uint32_t i = ph_block(d) * (blockDim.x >> 5) + (threadIdx.x >> 5);
     WorkItem w = work_at(i), wn = work_at(i + warpsTotal);
     uint32_t owRaw = leaf_word(w.handle);
     for (; i < n; i += warpsTotal) {
@@ -667,7 +686,7 @@ __device__ void ph_build_leaves(const DevDag& d, const DevEditor& e, char* scrat
 // untouched, my_gpu_hash_dag_edits.cu:651) or, for the scene builder, always.
 __device__ __forceinline__ bool merge_live(const DevDag& d)
 {
-    const EditCounters& E = d.ctl->edit;
+    const EditCounters& E = *d.edit;
     return (E.count[d.leafLevel] != 0 || E.builder) && !E.overflow;
 }
 
@@ -710,18 +729,23 @@ __device__ __forceinline__ bool fix_node(const DevDag& d, uint32_t level, bool g
         rem &= rem - 1u;
         h[j] = w[1 + j];
     }
-    // Children built in this edit: their representative, then its handle.
-    uint32_t r[8];
+    // Children built in this edit: their representative and, loaded beside it, the handle stored
+    // under the child's own index, which is the answer when the child is its own representative
+    // (only a duplicate needs the second, dependent load of its representative's handle).
+    uint32_t r[8], own[8];
 #pragma unroll
-    for (uint32_t j = 0; j < 8; ++j)
-        r[j] = (j < n && ((interm >> cbit[j]) & 1u)) ? repC[h[j]] : kEmptyRep;
+    for (uint32_t j = 0; j < 8; ++j) {
+        const bool built = j < n && ((interm >> cbit[j]) & 1u);
+        r[j] = built ? repC[h[j]] : kEmptyRep;
+        own[j] = built ? hC[h[j]] : kNone;
+    }
     const uint32_t* ff = d.ctl->fullyFilled[level + 1];
 #pragma unroll
     for (uint32_t j = 0; j < 8; ++j) {
         if (j >= n)
             h[j] = kNone;
         else if ((interm >> cbit[j]) & 1u)
-            h[j] = r[j] == kEmptyRep ? kNone : hC[r[j]];
+            h[j] = r[j] == kEmptyRep ? kNone : (r[j] == h[j] ? own[j] : hC[r[j]]);
         else if (h[j] >= kFillMarker && h[j] != kNone)
             h[j] = ff[h[j] & 0xFu];
     }
@@ -819,20 +843,20 @@ __device__ __forceinline__ uint32_t dedup_item(unsigned long long* table, uint32
 
 __device__ void ph_fix_level(const DevDag& d, uint32_t level, uint32_t builder, char* scratch)
 {
-    EditCounters& E = d.ctl->edit;
+    EditCounters& E = *d.edit;
     if (!merge_live(d))
         return;
     const uint32_t LL = d.leafLevel;
     const uint32_t n = E.count[level];
     const bool gate = discovery_gate(E, level, LL, builder);
-    if (blockIdx.x == 0 && threadIdx.x == 0)
+    if (ph_block(d) == 0 && threadIdx.x == 0)
         E.ffRan[level] = gate ? 1u : 0u;
     const MergeLayout ch = merge_layout(E.count, E.buildTop, level + 1, LL);
     const uint32_t* repC = reinterpret_cast<const uint32_t*>(scratch + ch.rep);
     const uint32_t* hC = reinterpret_cast<const uint32_t*>(scratch + ch.handle);
     uint32_t* nodes = reinterpret_cast<uint32_t*>(scratch + E.offN[level]);
     uint32_t full = 0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    for (uint32_t i = ph_block(d) * blockDim.x + threadIdx.x; i < n; i += ph_grid(d) * blockDim.x) {
         uint32_t* node = nodes + (size_t)i * kItemStride;
         uint32_t w[kItemStride];
 #pragma unroll
@@ -852,7 +876,7 @@ __device__ void ph_fix_level(const DevDag& d, uint32_t level, uint32_t builder, 
 // representative, kEmptyRep for an empty item.
 __device__ void ph_dedup_level(const DevDag& d, uint32_t level, char* scratch)
 {
-    EditCounters& E = d.ctl->edit;
+    EditCounters& E = *d.edit;
     if (!merge_live(d))
         return;
     const uint32_t LL = d.leafLevel;
@@ -861,7 +885,7 @@ __device__ void ph_dedup_level(const DevDag& d, uint32_t level, char* scratch)
     uint32_t* rep = reinterpret_cast<uint32_t*>(scratch + m.rep);
     unsigned long long* table = reinterpret_cast<unsigned long long*>(scratch + m.table);
     const uint32_t* items = reinterpret_cast<const uint32_t*>(scratch + E.offN[level]);
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    for (uint32_t i = ph_block(d) * blockDim.x + threadIdx.x; i < n; i += ph_grid(d) * blockDim.x) {
         const uint32_t* it = items + (size_t)i * kItemStride;
         uint32_t w[kItemStride];
 #pragma unroll
@@ -884,19 +908,102 @@ __device__ void ph_dedup_level(const DevDag& d, uint32_t level, char* scratch)
     }
 }
 
+// The bottom-up step of one SVO item held in w (one thread; the item is alone on its level, so it has
+// no duplicates): gated fully-filled discovery and child fix-up (children built in this edit are
+// looked up in repC / hC), then find-or-insert in the level table. Leaves w fixed; returns the item's
+// handle, or kNone when the item came out empty.
+__device__ uint32_t merge_single(const DevDag& d, uint32_t level, uint32_t* w, const uint32_t* repC, const uint32_t* hC,
+    const Grp<1>& g, Spare& spare, unsigned long long& added)
+{
+    EditCounters& E = *d.edit;
+    const uint32_t LL = d.leafLevel;
+    const bool isLeaf = level == LL;
+    Key<1> key;
+#pragma unroll
+    for (uint32_t j = 0; j < kItemStride; ++j)
+        key.w[j] = w[j];
+    if (!isLeaf) {
+        const bool gate = discovery_gate(E, level, LL, E.builder);
+        E.ffRan[level] = gate ? 1u : 0u;
+        if (fix_node(d, level, gate, repC, hC, key.w))
+            E.ffCount[level] = 1;
+#pragma unroll
+        for (uint32_t j = 0; j < kItemStride; ++j)
+            w[j] = key.w[j];
+    }
+    const bool isEmpty = isLeaf ? (key.w[0] == 0 && key.w[1] == 0) : ((key.w[0] & 0xFFu) == 0);
+    if (isEmpty)
+        return kNone;
+    key.n = isLeaf ? dev_leaf_words(key.w[0], key.w[1]) : dev_node_words(key.w[0]);
+    hash_words(key.w, key.n, key.ha, key.hb);
+    E.repCount[level] = 1;
+    if (E.builder)
+        atomicAdd(&E.repPerClass[level][key.n - 2], 1u);
+    const DevTable t = d.ctl->tables[level];
+    bool ins = false;
+    const uint32_t h = table_find_or_insert<1, false>(g, d, t, key, spare, ins);
+    release_spare<1>(g, d, t, spare);
+    added += ins ? 1u : 0u;
+    return h;
+}
+
+// The path from the root down to a subtree edit's node (L0, path), rebuilt bottom-up over the current
+// DAG with the subtree's new handle `sub` (kNone: emptied) in place of the old child: level by level
+// the SVO item the edit's own pass would have built there (the old node's children kept, the path
+// child subdivided) goes through merge_single with the counters of that edit. Returns the new root.
+__device__ uint32_t rebuild_spine(const DevDag& d, uint32_t L0, const uint32_t* path, uint32_t root, uint32_t sub,
+    unsigned long long& added)
+{
+    uint32_t nodes[kMaxLevels];
+    uint32_t h = root;
+    for (uint32_t l = 0; l < L0; ++l) {
+        nodes[l] = h;
+        if (h != kNone) {
+            const uint32_t* node = item_ptr(d, h);
+            const uint32_t c = spine_child(path, L0, l);
+            const uint32_t mask = node[0] & 0xFFu;
+            h = (mask >> c) & 1u ? node[1 + __popc(mask & ((1u << c) - 1u))] : kNone;
+        }
+    }
+    Grp<1> g;
+    Spare spare;
+    uint32_t childRep = sub == kNone ? kEmptyRep : 0u, childHandle = sub;
+    for (int li = (int)L0 - 1; li >= 0; --li) {
+        const uint32_t l = (uint32_t)li;
+        const uint32_t ci = spine_child(path, L0, l);
+        uint32_t w[kItemStride] = {};
+        const uint32_t* old = nodes[l] != kNone ? item_ptr(d, nodes[l]) : nullptr;
+        const uint32_t oldMask = old ? old[0] & 0xFFu : 0u;
+        const uint32_t mask = oldMask | (1u << ci);
+        uint32_t j = 0;
+        for (uint32_t b = 0; b < 8; ++b)
+            if ((mask >> b) & 1u)
+                w[1 + j++] = b == ci ? 0u : old[1 + __popc(oldMask & ((1u << b) - 1u))];
+        w[0] = mask | (1u << (13 + ci));
+        const uint32_t regRep[1] = { childRep }, regHandle[1] = { childHandle };
+        const uint32_t hn = merge_single(d, l, w, regRep, regHandle, g, spare, added);
+        childRep = hn == kNone ? kEmptyRep : 0u;
+        childHandle = hn;
+    }
+    return childHandle;
+}
+
 // One bottom-up level in a single pass (used by edits): child fix-up and gated discovery, intra-level
 // dedup, and find-or-insert of the representative in the level table. Duplicates only record their
-// representative; the parent level reads the representative's handle after the next barrier.
+// representative; the parent level reads the representative's handle after the next barrier. With
+// SHARED (the blocks of a group of subtree edits), other blocks may insert the same items at the
+// same time (table_find_or_insert's shared mode).
+template <bool SHARED>
 __device__ void ph_merge_level(const DevDag& d, uint32_t level, char* scratch)
 {
-    EditCounters& E = d.ctl->edit;
+    EditCounters& E = *d.edit;
     if (!merge_live(d))
         return;
     const uint32_t LL = d.leafLevel;
     const uint32_t n = E.count[level];
     const bool isLeaf = level == LL;
     const bool gate = isLeaf ? false : discovery_gate(E, level, LL, E.builder);
-    if (!isLeaf && blockIdx.x == 0 && threadIdx.x == 0)
+    if (!isLeaf && ph_block(d) == 0 && threadIdx.x == 0)
         E.ffRan[level] = gate ? 1u : 0u;
     const MergeLayout m = merge_layout(E.count, E.buildTop, level, LL);
     const MergeLayout ch = isLeaf ? m : merge_layout(E.count, E.buildTop, level + 1, LL);
@@ -910,7 +1017,7 @@ __device__ void ph_merge_level(const DevDag& d, uint32_t level, char* scratch)
     Grp<1> g;
     Spare spare;
     uint32_t full = 0, reps = 0, added = 0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    for (uint32_t i = ph_block(d) * blockDim.x + threadIdx.x; i < n; i += ph_grid(d) * blockDim.x) {
         uint32_t* it = items + (size_t)i * kItemStride;
         Key<1> key;
 #pragma unroll
@@ -940,7 +1047,7 @@ __device__ void ph_merge_level(const DevDag& d, uint32_t level, char* scratch)
         if (E.builder) // the scene builder sizes the level tables from these
             atomicAdd(&E.repPerClass[level][key.n - 2], 1u);
         bool ins = false;
-        handle[i] = table_find_or_insert<1>(g, d, t, key, spare, ins);
+        handle[i] = table_find_or_insert<1, SHARED>(g, d, t, key, spare, ins);
         added += ins ? 1u : 0u;
     }
     release_spare<1>(g, d, t, spare);
@@ -957,7 +1064,7 @@ __device__ void ph_merge_level(const DevDag& d, uint32_t level, char* scratch)
 template <int G>
 __device__ void ph_insert_level(const DevDag& d, const DevTable& t, uint32_t level, char* scratch)
 {
-    EditCounters& E = d.ctl->edit;
+    EditCounters& E = *d.edit;
     if (!merge_live(d))
         return;
     const uint32_t n = E.count[level];
@@ -969,7 +1076,7 @@ __device__ void ph_insert_level(const DevDag& d, const DevTable& t, uint32_t lev
     const uint32_t groupsPerBlock = blockDim.x / G;
     Spare spare;
     uint32_t added = 0;
-    for (uint32_t i = blockIdx.x * groupsPerBlock + threadIdx.x / G; i < n; i += gridDim.x * groupsPerBlock) {
+    for (uint32_t i = ph_block(d) * groupsPerBlock + threadIdx.x / G; i < n; i += ph_grid(d) * groupsPerBlock) {
         if (rep[i] != i)
             continue;
         Key<G> key;
@@ -988,14 +1095,15 @@ __device__ void ph_insert_level(const DevDag& d, const DevTable& t, uint32_t lev
 
 __device__ void ph_edit_end(const DevDag& d, char* scratch, uint32_t builder, uint32_t* tileOut, EditRecord* record)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0)
+    if (threadIdx.x != 0 || ph_block(d) != 0)
         return;
     Control* c = d.ctl;
-    EditCounters& E = c->edit;
+    EditCounters& E = *d.edit;
     // An edit that failed (scratch exhausted, or an error raised while it ran) leaves the root as it
     // was; later edits of a batch still run.
     if (E.overflow) {
-        set_status(c, SVDAG_ERR_OOM);
+        if (!d.solo) // a subtree edit's overflow is reported by k_edit_spines, for that edit alone
+            set_status(c, SVDAG_ERR_OOM);
     } else if ((E.count[d.leafLevel] != 0 || builder) && E.err == 0) {
         const MergeLayout m = merge_layout(E.count, E.buildTop, E.startLevel, d.leafLevel);
         const uint32_t r = reinterpret_cast<const uint32_t*>(scratch + m.rep)[0];
@@ -1024,9 +1132,9 @@ __device__ void ph_edit_end(const DevDag& d, char* scratch, uint32_t builder, ui
 
 __device__ void ph_reset_counters(const DevDag& d)
 {
-    if (blockIdx.x != 0)
+    if (ph_block(d) != 0)
         return;
-    uint32_t* w = reinterpret_cast<uint32_t*>(&d.ctl->edit);
+    uint32_t* w = reinterpret_cast<uint32_t*>(d.edit);
     for (uint32_t i = threadIdx.x; i < sizeof(EditCounters) / 4; i += blockDim.x)
         w[i] = 0;
 }
@@ -1063,7 +1171,7 @@ __global__ void __launch_bounds__(256) k_fix_level(DevDag d, uint32_t level, uin
     ph_fix_level(d, level, builder, scratch);
 }
 __global__ void __launch_bounds__(256) k_dedup_level(DevDag d, uint32_t level, char* scratch) { ph_dedup_level(d, level, scratch); }
-__global__ void __launch_bounds__(256) k_merge_level(DevDag d, uint32_t level, char* scratch) { ph_merge_level(d, level, scratch); }
+__global__ void __launch_bounds__(256) k_merge_level(DevDag d, uint32_t level, char* scratch) { ph_merge_level<false>(d, level, scratch); }
 template <int G>
 __global__ void __launch_bounds__(256) k_insert_level(DevDag d, DevTable t, uint32_t level, char* scratch)
 {
@@ -1086,7 +1194,7 @@ constexpr uint32_t kBlockThreads = 512;
 
 __device__ __forceinline__ void stamp(const DevDag& d, uint32_t& k)
 {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (!d.solo && blockIdx.x == 0 && threadIdx.x == 0) {
         unsigned long long t;
         asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
         if (k < 64)
@@ -1095,7 +1203,7 @@ __device__ __forceinline__ void stamp(const DevDag& d, uint32_t& k)
     }
 }
 
-template <uint32_t TOOL>
+template <uint32_t TOOL, bool SHARED = false>
 __device__ __forceinline__ void block_edit(const DevDag& d, const DevEditor& ed, char* scratch, unsigned long long scratchBytes,
     EditRecord* record)
 {
@@ -1116,7 +1224,7 @@ __device__ __forceinline__ void block_edit(const DevDag& d, const DevEditor& ed,
     __syncthreads();
     stamp(d, k);
     for (int level = (int)LL; level >= 0; --level) {
-        ph_merge_level(d, (uint32_t)level, scratch);
+        ph_merge_level<SHARED>(d, (uint32_t)level, scratch);
         __syncthreads();
         stamp(d, k);
     }
@@ -1158,6 +1266,104 @@ __global__ void __launch_bounds__(kBlockThreads, 1) k_edit_block(DevDag d, DevEd
             break;
         default:
             break;
+        }
+    }
+}
+
+// A group of subtree edits (DevEditor::subtree) whose nodes are pairwise disjoint: block k builds and
+// merges edit k's subtree against the DAG as the group found it, with counters and a slice of the
+// scratch arena of its own. Their footprints do not meet, so each block reads exactly the nodes the
+// edit's own pass would read after its predecessors; only the path from the root to each subtree
+// depends on the order, and k_edit_spines rebuilds it in submission order afterwards.
+__global__ void __launch_bounds__(kBlockThreads, 1) k_edit_subtrees(DevDag d, const DevEditor* eds, uint32_t numEdits, char* parts,
+    unsigned long long partBytes, EditCounters* counters)
+{
+    const uint32_t k = blockIdx.x;
+    if (k >= numEdits)
+        return;
+    DevDag dk = d;
+    dk.edit = counters + k;
+    dk.solo = 1;
+    const DevEditor ed = eds[k];
+    char* scratch = parts + (unsigned long long)k * partBytes;
+    switch (ed.tool) {
+    case SVDAG_TOOL_SPHERE_ADD:
+        block_edit<SVDAG_TOOL_SPHERE_ADD, true>(dk, ed, scratch, partBytes, nullptr);
+        break;
+    case SVDAG_TOOL_SPHERE_REMOVE:
+        block_edit<SVDAG_TOOL_SPHERE_REMOVE, true>(dk, ed, scratch, partBytes, nullptr);
+        break;
+    case SVDAG_TOOL_BOX_ADD:
+        block_edit<SVDAG_TOOL_BOX_ADD, true>(dk, ed, scratch, partBytes, nullptr);
+        break;
+    case SVDAG_TOOL_BOX_REMOVE:
+        block_edit<SVDAG_TOOL_BOX_REMOVE, true>(dk, ed, scratch, partBytes, nullptr);
+        break;
+    case SVDAG_TOOL_SPHERE_PAINT:
+        block_edit<SVDAG_TOOL_SPHERE_PAINT, true>(dk, ed, scratch, partBytes, nullptr);
+        break;
+    case SVDAG_TOOL_BOX_PAINT_NOISE:
+        block_edit<SVDAG_TOOL_BOX_PAINT_NOISE, true>(dk, ed, scratch, partBytes, nullptr);
+        break;
+    default:
+        break;
+    }
+}
+
+// Commits a group of subtree edits in submission order (one thread): per edit, the undo frame of
+// ph_edit_begin, the path from the root to its subtree rebuilt over the current DAG (rebuild_spine),
+// the new root and the edit's record. An edit that changed nothing or ran out of its scratch slice
+// leaves the root as it is, as in its own pass; an error raised while the group's subtrees were
+// built fails every edit of the group.
+__global__ void k_edit_spines(DevDag d, const DevEditor* eds, uint32_t numEdits, EditCounters* counters)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0)
+        return;
+    Control* c = d.ctl;
+    const uint32_t groupErr = c->edit.err;
+    for (uint32_t k = 0; k < numEdits; ++k) {
+        const DevEditor& e = eds[k];
+        EditCounters& E = counters[k];
+        const uint32_t root = c->root;
+        { // MyGPUHashDAGUndoRedo::add_frame (my_gpu_base_dag.h:23-34), as ph_edit_begin
+            const bool same = c->undoCount > 0 && c->undo[(c->undoHead + 63u) & 63u] == root;
+            if (!same) {
+                c->redoCount = 0;
+                c->undo[c->undoHead] = root;
+                c->undoHead = (c->undoHead + 1u) & 63u;
+                c->undoCount = c->undoCount < c->undoDepth ? c->undoCount + 1u : c->undoDepth;
+            }
+        }
+        const uint32_t sub = *e.tileOut;
+        unsigned long long added = 0;
+        uint32_t status = E.overflow ? (uint32_t)SVDAG_ERR_OOM : groupErr;
+        if (status == 0 && sub != kKeep) {
+            DevDag dk = d;
+            dk.edit = &E;
+            dk.solo = 1;
+            const uint32_t errBefore = c->edit.err;
+            const uint32_t after = rebuild_spine(dk, e.startLevel, e.startPath, root, sub, added);
+            if (c->edit.err == errBefore)
+                c->root = after;
+            else
+                status = c->edit.err;
+        }
+        if (E.overflow)
+            set_status(c, SVDAG_ERR_OOM);
+        if (e.record) {
+            EditRecord* r = e.record;
+            r->rootBefore = root;
+            r->rootAfter = c->root;
+            r->status = status;
+            r->edited = E.edited;
+            r->added = E.added + added;
+            unsigned long long svo = e.startLevel, reps = 0;
+            for (uint32_t l = 0; l < kMaxLevels; ++l) {
+                svo += E.count[l];
+                reps += E.repCount[l];
+            }
+            r->svoItems = svo;
+            r->unique = reps;
         }
     }
 }
@@ -1400,9 +1606,44 @@ double estimate_leaves(const DevEditor& e)
     }
 }
 
-// Launches expanded editors with their editors and records in `region`: runs of small edits in one
-// persistent launch each (grid barriers are cheaper than launches for small SVOs), large edits as one
-// launch per phase at full occupancy (the persistent kernel holds 16 warps per SM).
+// Node of a subtree edit (svdag_subtree.h) from its editor's footprint box: the sphere's bounding box
+// (centre with the +0.5 applied, radius) or the box; false for tools whose reads or writes reach
+// outside their footprint (copy, move, erosion) and for the scene builder.
+bool subtree_node(const svdag_ctx* ctx, const DevEditor& e, uint32_t& level, uint32_t path[3])
+{
+    float lo[3], hi[3];
+    switch (e.tool) {
+    case SVDAG_TOOL_SPHERE_ADD:
+    case SVDAG_TOOL_SPHERE_REMOVE:
+    case SVDAG_TOOL_SPHERE_PAINT:
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = e.center[a] - e.radius;
+            hi[a] = e.center[a] + e.radius;
+        }
+        break;
+    case SVDAG_TOOL_BOX_ADD:
+    case SVDAG_TOOL_BOX_REMOVE:
+    case SVDAG_TOOL_BOX_PAINT_NOISE:
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = e.bmin[a];
+            hi[a] = e.bmax[a];
+        }
+        break;
+    default:
+        return false;
+    }
+    if (e.saveRoot || e.useSavedSource || e.builder)
+        return false;
+    return subtree::node_of(lo, hi, ctx->cfg.levels, level, path);
+}
+
+constexpr unsigned long long kSubtreeScratch = 16ull << 20; // scratch slice of one subtree edit
+
+// Launches expanded editors with their editors and records in `region`. Large edits run as one launch
+// per phase at full occupancy. Runs of small edits are cut into groups of subtree edits whose nodes
+// are pairwise disjoint (one block per edit builds its subtree, then one thread commits the group in
+// order: k_edit_subtrees, k_edit_spines) and the edits between them, which run one after another in
+// one persistent launch (block barriers are cheaper than launches for small SVOs).
 svdag_status launch_edits_at(svdag_ctx* ctx, const DevEditor* eds, uint32_t n, char* region, size_t regionBytes, cudaStream_t s)
 {
     const size_t edBytes = align256((size_t)n * sizeof(DevEditor));
@@ -1410,40 +1651,82 @@ svdag_status launch_edits_at(svdag_ctx* ctx, const DevEditor* eds, uint32_t n, c
         return SVDAG_ERR_INVALID;
     const DevEditor* devEds = reinterpret_cast<const DevEditor*>(region);
     EditRecord* records = reinterpret_cast<EditRecord*>(region + edBytes);
-    {
-        std::vector<DevEditor> withRecords(eds, eds + n);
-        for (uint32_t k = 0; k < n; ++k)
-            withRecords[k].record = records + k;
-        // a pageable source is staged before the call returns, so the vector may go
-        SVDAG_CUDA(cudaMemcpyAsync(region, withRecords.data(), (size_t)n * sizeof(DevEditor), cudaMemcpyHostToDevice, s));
-    }
     auto small = [&](uint32_t k) { return ctx->persistentLeaves > 0 && estimate_leaves(eds[k]) <= ctx->persistentLeaves; };
-    uint32_t i = 0;
-    while (i < n) {
-        if (!small(i)) { // a run of editors through the queue: the first phase takes eds[cursor]
-            uint32_t j = i + 1;
-            while (j < n && !small(j))
-                ++j;
-            const EditQueue head { devEds + i, 0, 0, {} };
-            SVDAG_CUDA(cudaMemcpyAsync(ctx->queue, &head, offsetof(EditQueue, slot), cudaMemcpyHostToDevice, s));
-            for (uint32_t k = i; k < j; ++k)
-                SVDAG_TRY(run_phases(ctx, eds[k].tool, s, true));
-            i = j;
+    // plan: [begin, end) segments of one kind each
+    enum Kind { LARGE, SEQUENTIAL, GROUP };
+    struct Seg {
+        uint32_t begin, end;
+        Kind kind;
+    };
+    std::vector<Seg> segs;
+    std::vector<DevEditor> withRecords(eds, eds + n);
+    for (uint32_t k = 0; k < n; ++k)
+        withRecords[k].record = records + k;
+    const unsigned long long maxGroup = std::min<unsigned long long>(148, ctx->scratchBytes / kSubtreeScratch);
+    auto extend = [&](uint32_t k, Kind kind) {
+        if (!segs.empty() && segs.back().kind == kind && kind != GROUP && segs.back().end == k)
+            segs.back().end = k + 1;
+        else
+            segs.push_back(Seg { k, k + 1, kind });
+    };
+    for (uint32_t k = 0; k < n;) {
+        if (!small(k)) {
+            extend(k++, LARGE);
             continue;
         }
-        uint32_t j = i + 1;
-        while (j < n && small(j))
-            ++j;
-        DevDag d = ctx->dag();
-        DevEditor single = eds[i];
-        const DevEditor* segEds = devEds + i;
-        EditRecord* segRec = records + i;
-        uint32_t m = j - i;
-        char* scratch = ctx->scratch;
-        unsigned long long scratchBytes = ctx->scratchBytes;
-        k_edit_block<<<1, kBlockThreads, 0, s>>>(d, single, segEds, m, scratch, scratchBytes, segRec);
-        SVDAG_CUDA(cudaGetLastError());
-        i = j;
+        uint32_t e = k, lv[148], pt[148][3];
+        while (e < n && e - k < maxGroup && small(e)) {
+            const uint32_t m = e - k;
+            if (!subtree_node(ctx, eds[e], lv[m], pt[m]))
+                break;
+            bool ok = true;
+            for (uint32_t q = 0; q < m && ok; ++q)
+                ok = subtree::disjoint(lv[q], pt[q], lv[m], pt[m]);
+            if (!ok)
+                break;
+            ++e;
+        }
+        const uint32_t m = e - k;
+        if (m < 2) {
+            extend(k++, SEQUENTIAL);
+            continue;
+        }
+        uint32_t* results = reinterpret_cast<uint32_t*>(ctx->scratch + align256((size_t)m * sizeof(EditCounters)));
+        for (uint32_t q = 0; q < m; ++q) {
+            DevEditor& ed = withRecords[k + q];
+            ed.subtree = 1;
+            ed.startLevel = lv[q];
+            for (int a = 0; a < 3; ++a)
+                ed.startPath[a] = pt[q][a];
+            ed.tileOut = results + q;
+        }
+        segs.push_back(Seg { k, e, GROUP });
+        k = e;
+    }
+    // a pageable source is staged before the call returns, so the vector may go
+    SVDAG_CUDA(cudaMemcpyAsync(region, withRecords.data(), (size_t)n * sizeof(DevEditor), cudaMemcpyHostToDevice, s));
+    const DevDag d = ctx->dag();
+    for (const Seg& g : segs) {
+        const uint32_t m = g.end - g.begin;
+        if (g.kind == LARGE) { // a run of editors through the queue: the first phase takes eds[cursor]
+            const EditQueue head { devEds + g.begin, 0, 0, {} };
+            SVDAG_CUDA(cudaMemcpyAsync(ctx->queue, &head, offsetof(EditQueue, slot), cudaMemcpyHostToDevice, s));
+            for (uint32_t k = g.begin; k < g.end; ++k)
+                SVDAG_TRY(run_phases(ctx, eds[k].tool, s, true));
+        } else if (g.kind == SEQUENTIAL) {
+            k_edit_block<<<1, kBlockThreads, 0, s>>>(d, eds[g.begin], devEds + g.begin, m, ctx->scratch, ctx->scratchBytes,
+                records + g.begin);
+            SVDAG_CUDA(cudaGetLastError());
+        } else {
+            const size_t cntBytes = align256((size_t)m * sizeof(EditCounters));
+            const size_t head = cntBytes + align256((size_t)m * 4);
+            EditCounters* counters = reinterpret_cast<EditCounters*>(ctx->scratch);
+            const unsigned long long partBytes = ((ctx->scratchBytes - head) / m) & ~255ull;
+            SVDAG_CUDA(cudaMemsetAsync(&ctx->ctl->edit.err, 0, sizeof(uint32_t), s));
+            k_edit_subtrees<<<m, kBlockThreads, 0, s>>>(d, devEds + g.begin, m, ctx->scratch + head, partBytes, counters);
+            k_edit_spines<<<1, 32, 0, s>>>(d, devEds + g.begin, m, counters);
+            SVDAG_CUDA(cudaGetLastError());
+        }
     }
     return SVDAG_OK;
 }

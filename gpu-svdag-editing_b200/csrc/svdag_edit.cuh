@@ -36,7 +36,14 @@ struct DevEditor {
     uint32_t useSavedSource; // copy: read the source from the saved root (move)
     uint32_t saveRoot; // remember the root before this edit as the source of a later copy (move)
     uint32_t builder; // scene build: fully-filled discovery on every level, no undo frame
+    // Subtree edit: the edit covers the subtree of the node (startLevel, startPath) of the DAG as the
+    // batch found it (that node's region holds the edit's whole footprint and no other edit of its
+    // group touches it); no undo frame; the subtree's new handle goes to *tileOut (kNone when it
+    // empties, kKeep while the edit has changed nothing), and the path above is rebuilt afterwards in
+    // submission order.
+    uint32_t subtree;
 };
+constexpr uint32_t kKeep = 0xFFFFFFFDu; // subtree edit: nothing committed
 
 // Summary of one edit of a batch (written on the device, read by the host after the batch).
 struct EditRecord {
@@ -68,13 +75,22 @@ struct MergeLayout {
     uint32_t cap;
 };
 
-// Scratch layout of the bottom-up phase; every thread recomputes it from the final level counts.
+// Scratch layout of the bottom-up phase; every thread recomputes it from the final level counts
+// (count has kMaxLevels entries). The counts are all loaded before the walk over the levels, and the
+// walk is unrolled, so the counts stay in registers and cost one round trip.
 __host__ __device__ inline MergeLayout merge_layout(const uint32_t* count, unsigned long long buildTop, uint32_t level, uint32_t leafLevel)
 {
+    uint32_t c[kMaxLevels];
+#pragma unroll
+    for (uint32_t l = 0; l < kMaxLevels; ++l)
+        c[l] = count[l];
     unsigned long long off = buildTop;
     MergeLayout m {};
-    for (int l = (int)leafLevel; l >= 0; --l) {
-        const unsigned long long n = count[l];
+#pragma unroll
+    for (int l = (int)kMaxLevels - 1; l >= 0; --l) {
+        if (l > (int)leafLevel)
+            continue;
+        const unsigned long long n = c[l];
         uint32_t cap = 2;
         while (cap < 2ull * n)
             cap <<= 1;
