@@ -132,7 +132,9 @@ struct DevDag {
     uint32_t leafLevel;
     EditCounters* edit; // counters of the running edit: &ctl->edit, or a subtree edit's own
     uint32_t solo; // each block runs an edit of its own (a subtree edit): phases see one block of a one-block grid
+    uint32_t* locks; // kLockStripes bucket lock words of a group of subtree edits (null otherwise)
 };
+constexpr uint32_t kLockStripes = 1u << 16;
 
 // Block index and block count of an edit phase: the launch's own, or 0 of 1 for a block that runs an
 // edit of its own.
@@ -757,54 +759,52 @@ __device__ __forceinline__ uint32_t table_add(const Grp<G>& g, const DevDag& d, 
     return kNone;
 }
 
-constexpr uint32_t kBusyWaitTries = 1u << 20; // bound on waiting for another thread's in-flight slot (about 30 ms)
+constexpr uint32_t kLockTries = 1u << 20; // bound on waiting for a bucket lock (about 30 ms)
 
-// The first slot of the key's chain, before slot `mySlot` of `mySlab`, that holds an item equal to the
-// key (one thread). A slot in flight (claimed, not yet published) is waited for, within a bound: its
-// owner only writes its item and publishes or gives the slot back, and an owner waits only for slots
-// before its own, so no two threads wait for each other.
-__device__ inline uint32_t first_equal_before(const Grp<1>& g, const DevDag& d, const DevTable& t, const Key<1>& key, uint32_t tag,
-    uint32_t mySlab, uint32_t mySlot)
+// Find-or-insert for keys that no other group of the same launch looks up (the DAG merge inserts
+// each distinct item once). A slot is claimed with the in-flight tag, the item written, then the
+// final tag published, so concurrent probes of other keys never compare a half-written item.
+template <int G>
+__device__ __forceinline__ uint32_t table_find_or_insert_one(const Grp<G>& g, const DevDag& d, const DevTable& t, const Key<G>& key,
+    Spare& spare, bool& inserted);
+
+// Find-or-insert. With SHARED (one thread per key, G = 1), several blocks may look up and insert the
+// same key at once (the blocks of a group of subtree edits): the lookup and insert then run under
+// the bucket's lock (a striped lock word in d.locks), so the second of two equal keys finds the
+// first's published item. A holder only probes and inserts into its own chain, so no lock waits on
+// another; the wait for a lock is bounded and ends with SVDAG_ERR_TIMEOUT.
+template <int G, bool SHARED = false>
+__device__ __forceinline__ uint32_t table_find_or_insert(const Grp<G>& g, const DevDag& d, const DevTable& t, const Key<G>& key,
+    Spare& spare, bool& inserted)
 {
-    uint32_t slab = first_slab(t, key.n - 2u, key.ha);
-    for (uint32_t steps = 0; steps < kMaxChain; ++steps) {
-        const uint32_t* hdr = slab_ptr(d, slab);
-        const uint32_t body = __ldcg(hdr + 6), next = __ldcg(hdr + 7);
-        const uint32_t last = slab == mySlab ? mySlot : kSlots;
-        for (uint32_t sl = 0; sl < last; ++sl) {
-            const uint32_t shift = 8u * (sl & 3u);
-            uint32_t tb = (__ldcg(hdr + (sl >> 2)) >> shift) & 0xFFu;
-            for (uint32_t spin = 0; tb == kTagBusy && spin < kBusyWaitTries; ++spin) {
-                __nanosleep(32);
-                tb = (*reinterpret_cast<const volatile uint32_t*>(hdr + (sl >> 2)) >> shift) & 0xFFu;
-            }
-            if (tb == kTagBusy) {
+    if constexpr (SHARED && G == 1) {
+        inserted = false;
+        const uint32_t cls = key.n - 2u;
+        if (key.n < 2u || key.n > 10u || t.numBuckets[cls] == 0 || !d.locks) {
+            set_status(d.ctl, SVDAG_ERR_INVALID);
+            return kNone;
+        }
+        uint32_t* lock = d.locks + (first_slab(t, cls, key.ha) & (kLockStripes - 1u));
+        uint32_t tries = 0;
+        while (atomicCAS(lock, 0u, 1u) != 0u) {
+            if (++tries >= kLockTries) {
                 set_status(d.ctl, SVDAG_ERR_TIMEOUT);
                 return kNone;
             }
-            if (tb == tag) {
-                const uint32_t item = slot_handle(body, sl, key.n);
-                if (item_equals<1, LD_L2>(g, handle_ptr(d, item), key))
-                    return item;
-            }
+            __nanosleep(32);
         }
-        if (slab == mySlab || next == kEnd || !slab_ok(d, next))
-            return kNone;
-        slab = next;
+        __threadfence(); // acquire: the previous holder's item and tag are visible
+        const uint32_t h = table_find_or_insert_one<G>(g, d, t, key, spare, inserted);
+        __threadfence(); // release: this holder's item and tag are visible before the lock is free
+        atomicExch(lock, 0u);
+        return h;
+    } else {
+        return table_find_or_insert_one<G>(g, d, t, key, spare, inserted);
     }
-    return kNone;
 }
 
-// Find-or-insert. Without `shared`, for keys that no other group of the same launch looks up (the DAG
-// merge inserts each distinct item once). A slot is claimed with the in-flight tag, the item written,
-// then the final tag published, so concurrent probes of other keys never compare a half-written
-// item. With SHARED (one thread per key, G = 1; several blocks may insert the same key at once),
-// the chain is read again before publishing: when an equal item sits in a slot before the fresh one,
-// that item is the answer and the fresh slot goes back cleared. Of concurrent inserts of one key
-// exactly the first slot in chain order survives, and the others were never published, so nobody
-// read them.
-template <int G, bool SHARED = false>
-__device__ __forceinline__ uint32_t table_find_or_insert(const Grp<G>& g, const DevDag& d, const DevTable& t, const Key<G>& key,
+template <int G>
+__device__ __forceinline__ uint32_t table_find_or_insert_one(const Grp<G>& g, const DevDag& d, const DevTable& t, const Key<G>& key,
     Spare& spare, bool& inserted)
 {
     inserted = false;
@@ -860,24 +860,10 @@ __device__ __forceinline__ uint32_t table_find_or_insert(const Grp<G>& g, const 
         snapValid = true;
         if (item != kNone) {
             write_item<G>(g, handle_ptr(d, item), key);
-            if constexpr (G == 1) {
+            if constexpr (G == 1)
                 fence_release(); // the writer publishes: a release orders its item before the tag
-                if constexpr (SHARED) {
-                    const uint32_t other = first_equal_before(g, d, t, key, tag, slab, s);
-                    if (other != kNone) { // give the slot back as a free one: zero words, then no tag
-                        uint32_t* p = handle_ptr(d, item);
-#pragma unroll
-                        for (uint32_t c = 0; c < 3; ++c)
-                            if (4u * c < key.n)
-                                *reinterpret_cast<uint4*>(p + 4u * c) = make_uint4(0, 0, 0, 0);
-                        fence_release();
-                        atomicAnd(slab_ptr(d, slab) + (s >> 2), ~(0xFFu << (8u * (s & 3u))));
-                        return other;
-                    }
-                }
-            } else {
+            else
                 __threadfence();
-            }
             g.sync();
             if (g.lane == 0)
                 atomicXor(slab_ptr(d, slab) + (s >> 2), (kTagBusy ^ tag) << (8u * (s & 3u)));

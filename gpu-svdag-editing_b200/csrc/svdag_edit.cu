@@ -1718,12 +1718,17 @@ svdag_status launch_edits_at(svdag_ctx* ctx, const DevEditor* eds, uint32_t n, c
                 records + g.begin);
             SVDAG_CUDA(cudaGetLastError());
         } else {
+            // scratch: the group's counters, its result handles, the bucket locks, then one slice per edit
             const size_t cntBytes = align256((size_t)m * sizeof(EditCounters));
-            const size_t head = cntBytes + align256((size_t)m * 4);
+            const size_t lockAt = cntBytes + align256((size_t)m * 4);
+            const size_t head = lockAt + (size_t)kLockStripes * 4;
             EditCounters* counters = reinterpret_cast<EditCounters*>(ctx->scratch);
             const unsigned long long partBytes = ((ctx->scratchBytes - head) / m) & ~255ull;
+            DevDag dg = d;
+            dg.locks = reinterpret_cast<uint32_t*>(ctx->scratch + lockAt);
+            SVDAG_CUDA(cudaMemsetAsync(dg.locks, 0, (size_t)kLockStripes * 4, s));
             SVDAG_CUDA(cudaMemsetAsync(&ctx->ctl->edit.err, 0, sizeof(uint32_t), s));
-            k_edit_subtrees<<<m, kBlockThreads, 0, s>>>(d, devEds + g.begin, m, ctx->scratch + head, partBytes, counters);
+            k_edit_subtrees<<<m, kBlockThreads, 0, s>>>(dg, devEds + g.begin, m, ctx->scratch + head, partBytes, counters);
             k_edit_spines<<<1, 32, 0, s>>>(d, devEds + g.begin, m, counters);
             SVDAG_CUDA(cudaGetLastError());
         }

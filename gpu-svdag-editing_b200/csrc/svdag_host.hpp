@@ -40,7 +40,7 @@ struct svdag_ctx {
     double persistentLeaves = 0; // edits estimated at or below this many SVO leaves run in the persistent kernel (0 = none)
     uint32_t loadFactor = 16;
     unsigned long long scratchHighWater = 0;
-    svdag::DevDag dag() const { return svdag::DevDag { items, itemWords, headers, headerCount, ctl, cfg.levels, cfg.levels - 2, &ctl->edit, 0u }; }
+    svdag::DevDag dag() const { return svdag::DevDag { items, itemWords, headers, headerCount, ctl, cfg.levels, cfg.levels - 2, &ctl->edit, 0u, nullptr }; }
 };
 
 namespace svdag {

@@ -6,7 +6,9 @@ submission order, rebuilding the path from the root to each subtree over the cur
 Against the same edits applied one at a time:
  - the DAG after the batch equals the oracle's;
  - every edit's record chains: its root_before is the previous edit's root_after;
- - undo steps back through the same DAGs as the per-edit path, edit by edit.
+ - undo steps back through the same DAGs as the per-edit path, edit by edit;
+ - the tables store each distinct item once, as many items per level as the per-edit path stores, even
+   when many blocks make equal items at once.
 A batch that mixes groups with overlapping edits, a large edit and a copy is checked the same way.
 """
 import numpy as np
@@ -61,6 +63,15 @@ def run_both(svdag_lib, oracle_mod, edits):
     return batched, recs, o
 
 
+def stored_items(dag):
+    """Per level: the number of stored items, and how many of them repeat another's words."""
+    out = []
+    for level in range(LEVELS - 1):
+        _, words = dag.export_level(level)
+        out.append((len(words), len(words) - len(np.unique(words, axis=0)) if len(words) else 0))
+    return out
+
+
 def test_disjoint_small_edits_equal_the_oracle_and_chain(svdag_lib, oracle_mod):
     edits = scattered(svdag_lib, 96, seed=11)
     batched, recs, o = run_both(svdag_lib, oracle_mod, edits)
@@ -70,6 +81,35 @@ def test_disjoint_small_edits_equal_the_oracle_and_chain(svdag_lib, oracle_mod):
     assert recs[-1].root_after == batched.get_first_node_index()
     assert sum(1 for r in recs if r.root_after != r.root_before) > 60
     assert gpu_canon(oracle_mod, batched) == o.canon()
+    # the tables hold each distinct item once, exactly the items the per-edit path stores
+    plain = svdag_lib.MyGPUHashDAG(LEVELS, pool_bytes=4 << 30, scratch_bytes=1 << 30, undo_depth=64)
+    plain.build_terrain(**TERRAIN)
+    for e in edits:
+        plain.edit(e)
+    plain.sync()
+    got, want = stored_items(batched), stored_items(plain)
+    assert all(dup == 0 for _, dup in got), got
+    assert [n for n, _ in got] == [n for n, _ in want]
+    batched.free()
+    plain.free()
+
+
+def test_equal_new_items_from_many_edits_are_stored_once(svdag_lib, oracle_mod):
+    """Many edits of one tool and material in scattered places produce many equal leaves and nodes
+    at the same time; each must be stored once."""
+    import svdag.workloads as w
+
+    rng = np.random.default_rng(14)
+    g = 1 << LEVELS
+    edits = []
+    for _ in range(120):
+        x, z = (int(v) for v in rng.integers(16, g - 16, 2))
+        c = (float(x), float(w.scene_height(LEVELS, x, z, **TERRAIN) + 6), float(z))
+        edits.append(w.make_edit(svdag_lib.TOOL_BOX_ADD, 5, c, 7.0))
+    batched, recs, o = run_both(svdag_lib, oracle_mod, edits)
+    assert all(r.status == 0 for r in recs)
+    assert gpu_canon(oracle_mod, batched) == o.canon()
+    assert all(dup == 0 for _, dup in stored_items(batched))
     batched.free()
 
 
