@@ -448,6 +448,12 @@ def run_serve(args):
             out["sweep"].append(point)
         dag.free()
         del dag
+    # the batched form on scattered small edits (runs of them land in disjoint subtrees, built side by
+    # side), against the per-edit path
+    batching = None
+    if not args.no_batching:
+        small = w.c3_edits(levels=levels, terrain=make_terrain(w, levels), rmax=16.0, seed=5)
+        batching = {"small_scattered_256": c3_compare(svdag, w, torch, levels, small)}
     peak, peak_kind = measured_peak_gbs()
     trace_c0 = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -500,12 +506,13 @@ def run_serve(args):
                 "d2h_bytes_per_step": int((frame_d2h + 48 * len(ek)) / args.steps),
                 "detail": out["e2e"]},
         "roofline": {"bound": "hbm", "kernel": "edit pipeline: one window of the stream as one batch (per-tool CUDA graphs of "
-                               "the phase kernels, small edits in the single-CTA persistent kernel)",
+                               "the phase kernels, small edits in the persistent kernel or in subtree groups)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind, "traffic": None, "launch": bt},
         "trace_1080p": dict(out["trace"], bytes_per_ray_lower_bound=68 + 8 * levels,
                             hbm_frac_lower_bound=out["trace"]["rays_s"] * (68 + 8 * levels) / 1e9 / peak),
         "trace_c0": trace_c0,
+        "batching": batching,
         "clocks": out["clocks"],
         # launch calls of the timed served replay: one per batch (a CUDA-graph replay or one persistent
         # kernel per run of small edits) and one per frame
@@ -980,6 +987,7 @@ def main():
     ap.add_argument("--pool-gb", type=float, default=0.0, help="pool size of the c2 mode's scene (0 = by depth)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-hash", action="store_true")
+    ap.add_argument("--no-batching", action="store_true", help="skip the batched-form comparison on small edits")
     ap.add_argument("--hash-keys", type=int, default=1 << 24)
     ap.add_argument("--hash-lanes", type=int, default=1)
     ap.add_argument("--hash-lf", type=int, default=16)
