@@ -169,10 +169,13 @@ typedef struct svdag_edit_stats {
  * (my_gpu_hash_dag_edits.h:12-13, body my_gpu_hash_dag_edits.cu:633-671). Asynchronous on
  * `stream`; the root handle, undo history and counters stay on the device. */
 svdag_status svdag_edit_apply(svdag_ctx* ctx, const svdag_edit* edit, void* stream);
-/* Batched form: applies the edits in order with no host round trip between them (runs of small edits
- * in one persistent launch, the others replayed through the tool's CUDA graph, all reading their
- * editors from device memory); the result equals applying them one by one. Each edit gets an
- * svdag_edit_record. A move counts as two records (removal, then paste). */
+/* Batched form: applies the edits in order with no host round trip between them, all reading their
+ * editors from device memory. Consecutive small sphere/box add, remove and paint edits whose
+ * footprints lie in pairwise disjoint subtrees are built side by side (one block each) and committed
+ * in order; other small edits run one after another in one persistent launch; the others are
+ * replayed through the tool's CUDA graph. The result, the undo frames and the records equal applying
+ * the edits one by one. Each edit gets an svdag_edit_record. A move counts as two records (removal,
+ * then paste). */
 svdag_status svdag_edit_apply_many(svdag_ctx* ctx, const svdag_edit* edits, uint32_t count, void* stream);
 
 typedef struct svdag_edit_record {
