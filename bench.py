@@ -963,10 +963,13 @@ def run_mode_c3(args):
     import svdag.workloads as w
 
     terrain = make_terrain(w, args.levels)
-    c3 = w.c3_edits(levels=args.levels, terrain=terrain, rmax=4096.0 * (1 << args.levels) / 131072)
-    small = w.c3_edits(levels=args.levels, terrain=terrain, rmax=16.0, seed=5)
-    out = c3_compare(svdag, w, torch, args.levels, c3)
-    out["small_scattered"] = c3_compare(svdag, w, torch, args.levels, small)
+    out = {}
+    if args.c3_set in ("both", "c3"):
+        c3 = w.c3_edits(levels=args.levels, terrain=terrain, rmax=4096.0 * (1 << args.levels) / 131072)
+        out = c3_compare(svdag, w, torch, args.levels, c3)
+    if args.c3_set in ("both", "small"):
+        small = w.c3_edits(levels=args.levels, terrain=terrain, rmax=16.0, seed=5)
+        out["small_scattered"] = c3_compare(svdag, w, torch, args.levels, small)
     print(json.dumps(out))
 
 
@@ -988,6 +991,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-hash", action="store_true")
     ap.add_argument("--no-batching", action="store_true", help="skip the batched-form comparison on small edits")
+    ap.add_argument("--c3-set", default="both", choices=["both", "c3", "small"], help="--mode c3: which edit sets")
     ap.add_argument("--hash-keys", type=int, default=1 << 24)
     ap.add_argument("--hash-lanes", type=int, default=1)
     ap.add_argument("--hash-lf", type=int, default=16)
