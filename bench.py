@@ -937,13 +937,14 @@ def c3_compare(svdag, w, torch, levels, edits):
         stream = torch.cuda.Stream()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
-        a.record(stream)
-        if name == "plain":
-            for e in edits:
-                dag.edit(e, stream=stream.cuda_stream)
-        else:
-            dag.edit_batch(edits, stream=stream.cuda_stream)
-        b.record(stream)
+        with profiled():
+            a.record(stream)
+            if name == "plain":
+                for e in edits:
+                    dag.edit(e, stream=stream.cuda_stream)
+            else:
+                dag.edit_batch(edits, stream=stream.cuda_stream)
+            b.record(stream)
         torch.cuda.synchronize()
         dag.sync()
         res[name] = a.elapsed_time(b)
