@@ -290,3 +290,48 @@ def test_snapshot_that_does_not_parse(svdag_lib, tmp_path):
     with pytest.raises(svdag_lib.SvdagError) as e:
         svdag_lib.items_to_v3(bad, str(tmp_path / "x.v3"), svdag_lib.V3_CPU)
     assert e.value.status == 1
+
+
+def test_corrupted_files_never_crash_the_reader(svdag_lib, tmp_path):
+    """Random byte changes anywhere in a file: the reader returns a status or a snapshot that parses;
+    it never reads outside the buffer (the buffer is exactly the file, no slack)."""
+    import ctypes as C
+
+    levels = 6
+    snap = svdag_lib.basic_dag_to_items(build_basic_dag(random_grid(np.random.default_rng(8), levels), levels), levels, 4)
+    p = str(tmp_path / "dag.v3")
+    svdag_lib.items_to_v3(snap, p, svdag_lib.V3_CPU)
+    good = np.fromfile(p, np.uint8)
+    f = V3File(p)
+    # the bytes that matter most: headers, the fully-filled array, the root, the first slabs' tags and
+    # items; and anywhere at all
+    hot = list(range(0, 4 + 8 + 4 + 4 * levels * 16 + 16 + 12 + 8))
+    for T in f.tables:
+        base = T["first"].ctypes.data - f.b.ctypes.data
+        hot += list(range(base, base + min(T["first"].nbytes, 512)))
+    rng = np.random.default_rng(9)
+    L = svdag_lib.lib()
+    nl = levels - 1
+    lw, li, total = np.zeros(nl, np.uint64), np.zeros(nl, np.uint64), C.c_uint64()
+    statuses = set()
+    rewritten = 0
+    for trial in range(80):
+        bad = good.copy()
+        where = rng.choice(hot, 3) if trial % 2 == 0 else rng.integers(0, len(bad), 3)
+        for w_ in where:
+            bad[int(w_)] = rng.integers(0, 256)
+        cut = len(bad) if trial % 5 else int(rng.integers(0, len(bad)))
+        buf = np.ascontiguousarray(bad[:cut])
+        st = L.svdag_v3_to_items(buf.ctypes.data if cut else None, cut, levels, None, 0, lw.ctypes.data, li.ctypes.data,
+                                 C.byref(total))
+        statuses.add(int(st))
+        if st in (0, 2):  # a snapshot came out: it must be one the loader accepts
+            words = np.zeros(max(total.value, 1), np.uint32)
+            assert L.svdag_v3_to_items(buf.ctypes.data, cut, levels, words.ctypes.data, len(words), lw.ctypes.data,
+                                       li.ctypes.data, C.byref(total)) == 0
+            if rewritten < 2:
+                back = svdag_lib.ItemSnapshot(levels, words[: total.value], lw.copy(), li.copy())
+                svdag_lib.items_to_v3(back, str(tmp_path / "re.v3"), svdag_lib.V3_CPU)
+                rewritten += 1
+    assert statuses - {0, 1, 2, 4, 7} == set()
+    assert 4 in statuses
