@@ -912,6 +912,7 @@ __device__ void ph_dedup_level(const DevDag& d, uint32_t level, char* scratch)
 // no duplicates): gated fully-filled discovery and child fix-up (children built in this edit are
 // looked up in repC / hC), then find-or-insert in the level table. Leaves w fixed; returns the item's
 // handle, or kNone when the item came out empty.
+template <bool SHARED>
 __device__ uint32_t merge_single(const DevDag& d, uint32_t level, uint32_t* w, const uint32_t* repC, const uint32_t* hC,
     const Grp<1>& g, Spare& spare, unsigned long long& added)
 {
@@ -941,17 +942,19 @@ __device__ uint32_t merge_single(const DevDag& d, uint32_t level, uint32_t* w, c
         atomicAdd(&E.repPerClass[level][key.n - 2], 1u);
     const DevTable t = d.ctl->tables[level];
     bool ins = false;
-    const uint32_t h = table_find_or_insert<1, false>(g, d, t, key, spare, ins);
+    const uint32_t h = table_find_or_insert<1, SHARED>(g, d, t, key, spare, ins);
     release_spare<1>(g, d, t, spare);
     added += ins ? 1u : 0u;
     return h;
 }
 
-// The path from the root down to a subtree edit's node (L0, path), rebuilt bottom-up over the current
-// DAG with the subtree's new handle `sub` (kNone: emptied) in place of the old child: level by level
-// the SVO item the edit's own pass would have built there (the old node's children kept, the path
-// child subdivided) goes through merge_single with the counters of that edit. Returns the new root.
-__device__ uint32_t rebuild_spine(const DevDag& d, uint32_t L0, const uint32_t* path, uint32_t root, uint32_t sub,
+// Levels L0-1 .. stop of the path from the root down to the node (L0, path), rebuilt bottom-up over
+// the DAG under `root` with the node's new handle `sub` (kNone: emptied) in place of the old child:
+// level by level the SVO item the edit's own pass would have built there (the old node's children
+// kept, the path child subdivided) goes through merge_single with the counters of that edit. Returns
+// the new handle at level `stop` (kNone when it emptied); with stop 0, the new root.
+template <bool SHARED>
+__device__ uint32_t rebuild_spine(const DevDag& d, uint32_t L0, const uint32_t* path, uint32_t root, uint32_t sub, uint32_t stop,
     unsigned long long& added)
 {
     uint32_t nodes[kMaxLevels];
@@ -968,7 +971,7 @@ __device__ uint32_t rebuild_spine(const DevDag& d, uint32_t L0, const uint32_t* 
     Grp<1> g;
     Spare spare;
     uint32_t childRep = sub == kNone ? kEmptyRep : 0u, childHandle = sub;
-    for (int li = (int)L0 - 1; li >= 0; --li) {
+    for (int li = (int)L0 - 1; li >= (int)stop; --li) {
         const uint32_t l = (uint32_t)li;
         const uint32_t ci = spine_child(path, L0, l);
         uint32_t w[kItemStride] = {};
@@ -981,7 +984,7 @@ __device__ uint32_t rebuild_spine(const DevDag& d, uint32_t L0, const uint32_t* 
                 w[1 + j++] = b == ci ? 0u : old[1 + __popc(oldMask & ((1u << b) - 1u))];
         w[0] = mask | (1u << (13 + ci));
         const uint32_t regRep[1] = { childRep }, regHandle[1] = { childHandle };
-        const uint32_t hn = merge_single(d, l, w, regRep, regHandle, g, spare, added);
+        const uint32_t hn = merge_single<SHARED>(d, l, w, regRep, regHandle, g, spare, added);
         childRep = hn == kNone ? kEmptyRep : 0u;
         childHandle = hn;
     }
@@ -1310,11 +1313,33 @@ __global__ void __launch_bounds__(kBlockThreads, 1) k_edit_subtrees(DevDag d, co
     }
 }
 
+// The private part of each subtree edit's path (levels spineSplit .. startLevel-1, which no other
+// path of the group passes through, so no earlier edit of the group changes them), rebuilt for all
+// the group's edits at once: thread k over the DAG as the group found it, with edit k's counters.
+// Two edits can make equal path items, so the find-or-inserts take the bucket locks. The handle at
+// level spineSplit replaces the subtree's in `results` (kKeep stays).
+__global__ void k_edit_spines_private(DevDag d, const DevEditor* eds, uint32_t numEdits, EditCounters* counters)
+{
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= numEdits)
+        return;
+    const DevEditor& e = eds[k];
+    EditCounters& E = counters[k];
+    const uint32_t sub = *e.tileOut;
+    if (E.overflow || sub == kKeep || d.ctl->edit.err != 0 || e.spineSplit >= e.startLevel)
+        return;
+    DevDag dk = d;
+    dk.edit = &E;
+    unsigned long long added = 0;
+    *e.tileOut = rebuild_spine<true>(dk, e.startLevel, e.startPath, d.ctl->root, sub, e.spineSplit, added);
+    E.added += added;
+}
+
 // Commits a group of subtree edits in submission order (one thread): per edit, the undo frame of
-// ph_edit_begin, the path from the root to its subtree rebuilt over the current DAG (rebuild_spine),
-// the new root and the edit's record. An edit that changed nothing or ran out of its scratch slice
-// leaves the root as it is, as in its own pass; an error raised while the group's subtrees were
-// built fails every edit of the group.
+// ph_edit_begin, the shared part of the path (levels spineSplit-1 .. 0) rebuilt over the current DAG
+// (rebuild_spine), the new root and the edit's record. An edit that changed nothing or ran out of
+// its scratch slice leaves the root as it is, as in its own pass; an error raised while the group's
+// subtrees or private path parts were built fails every edit of the group.
 __global__ void k_edit_spines(DevDag d, const DevEditor* eds, uint32_t numEdits, EditCounters* counters)
 {
     if (threadIdx.x != 0 || blockIdx.x != 0)
@@ -1334,15 +1359,19 @@ __global__ void k_edit_spines(DevDag d, const DevEditor* eds, uint32_t numEdits,
                 c->undoCount = c->undoCount < c->undoDepth ? c->undoCount + 1u : c->undoDepth;
             }
         }
-        const uint32_t sub = *e.tileOut;
+        const uint32_t sub = *e.tileOut; // the handle at level spineSplit (the subtree's when no private part)
         unsigned long long added = 0;
         uint32_t status = E.overflow ? (uint32_t)SVDAG_ERR_OOM : groupErr;
         if (status == 0 && sub != kKeep) {
             DevDag dk = d;
             dk.edit = &E;
             dk.solo = 1;
+            const uint32_t L = e.spineSplit < e.startLevel ? e.spineSplit : e.startLevel;
+            uint32_t path[3];
+            for (int a = 0; a < 3; ++a)
+                path[a] = e.startPath[a] >> (e.startLevel - L);
             const uint32_t errBefore = c->edit.err;
-            const uint32_t after = rebuild_spine(dk, e.startLevel, e.startPath, root, sub, added);
+            const uint32_t after = rebuild_spine<false>(dk, L, path, root, sub, 0, added);
             if (c->edit.err == errBefore)
                 c->root = after;
             else
@@ -1699,6 +1728,13 @@ svdag_status launch_edits_at(svdag_ctx* ctx, const DevEditor* eds, uint32_t n, c
             for (int a = 0; a < 3; ++a)
                 ed.startPath[a] = pt[q][a];
             ed.tileOut = results + q;
+            // the deepest level at which another edit's path meets this one's; the levels below it
+            // down to the node are this edit's alone
+            uint32_t meet = 0;
+            for (uint32_t o = 0; o < m; ++o)
+                if (o != q)
+                    meet = std::max(meet, subtree::meet_level(lv[q], pt[q], lv[o], pt[o]));
+            ed.spineSplit = meet + 1;
         }
         segs.push_back(Seg { k, e, GROUP });
         k = e;
@@ -1729,6 +1765,7 @@ svdag_status launch_edits_at(svdag_ctx* ctx, const DevEditor* eds, uint32_t n, c
             SVDAG_CUDA(cudaMemsetAsync(dg.locks, 0, (size_t)kLockStripes * 4, s));
             SVDAG_CUDA(cudaMemsetAsync(&ctx->ctl->edit.err, 0, sizeof(uint32_t), s));
             k_edit_subtrees<<<m, kBlockThreads, 0, s>>>(dg, devEds + g.begin, m, ctx->scratch + head, partBytes, counters);
+            k_edit_spines_private<<<(m + 31) / 32, 32, 0, s>>>(dg, devEds + g.begin, m, counters);
             k_edit_spines<<<1, 32, 0, s>>>(d, devEds + g.begin, m, counters);
             SVDAG_CUDA(cudaGetLastError());
         }

@@ -42,6 +42,9 @@ struct DevEditor {
     // empties, kKeep while the edit has changed nothing), and the path above is rebuilt afterwards in
     // submission order.
     uint32_t subtree;
+    // Subtree edit: path levels spineSplit .. startLevel-1 lie on no other path of the group (rebuilt
+    // for all the group's edits at once); levels 0 .. spineSplit-1 are shared and rebuilt in order.
+    uint32_t spineSplit;
 };
 constexpr uint32_t kKeep = 0xFFFFFFFDu; // subtree edit: nothing committed
 
