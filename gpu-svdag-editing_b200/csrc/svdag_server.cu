@@ -400,7 +400,7 @@ struct svdag_server {
             std::vector<Request> one { r };
             svdag_status st = SVDAG_OK;
             if (r.kind == 0 && gcAllowed() && dirtySinceGc && (pressure() > gcTrigger || pressure() + r.reserve > capBytes))
-                collect_garbage(); // a failed collection frees nothing; the edit is then judged as it is
+                collect_garbage(); // a failed collection frees nothing; the edit is then admitted or refused as it is
             if (r.kind == 0 && pressure() + r.reserve > capBytes) {
                 std::lock_guard<std::mutex> lk(m);
                 ++rejectedEdits;
@@ -447,7 +447,7 @@ struct svdag_server {
             if (gcAllowed() && dirtySinceGc && pressure() > gcTrigger)
                 gcWanted = true;
             if (gcWanted && unfinished() == 0 && !frameActive) {
-                collect_garbage(); // a failed collection frees nothing; admission then judges edits as they are
+                collect_garbage(); // a failed collection frees nothing; admission then weighs edits as they are
                 continue;
             }
             std::vector<Request> take;
