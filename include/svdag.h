@@ -502,7 +502,8 @@ svdag_status svdag_v3_to_items(const void* data, uint64_t n_bytes, uint32_t leve
  * whose arrays record `memory_type` (SVDAG_V3_*): the fully-filled items of every level and material
  * that MyGPUHashDAG::allocate inserts (my_gpu_hash_dag.cu:29-65), then the snapshot's distinct
  * items, each table sized to 96 items per bucket (TARGET_LOAD_FACTOR) and every item in a slot of
- * its bucket's slab chain, where the reference's find looks for it. A snapshot that does not parse gives
+ * its bucket's slab chain, where the reference's find looks for it. The tables are laid out in host
+ * memory before they are written (about the file's size). A snapshot that does not parse gives
  * SVDAG_ERR_INVALID; one whose handles would not fit the reference's 29-bit index SVDAG_ERR_OOM. */
 svdag_status svdag_items_to_v3(const uint32_t* words, const uint64_t* level_words, const uint64_t* level_items,
     uint32_t levels, uint32_t memory_type, const char* path);
