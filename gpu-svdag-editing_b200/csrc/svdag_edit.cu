@@ -912,7 +912,7 @@ __device__ void ph_dedup_level(const DevDag& d, uint32_t level, char* scratch)
 // no duplicates): gated fully-filled discovery and child fix-up (children built in this edit are
 // looked up in repC / hC), then find-or-insert in the level table. Leaves w fixed; returns the item's
 // handle, or kNone when the item came out empty.
-template <bool SHARED>
+template <int MODE>
 __device__ uint32_t merge_single(const DevDag& d, uint32_t level, uint32_t* w, const uint32_t* repC, const uint32_t* hC,
     const Grp<1>& g, Spare& spare, unsigned long long& added)
 {
@@ -942,7 +942,7 @@ __device__ uint32_t merge_single(const DevDag& d, uint32_t level, uint32_t* w, c
         atomicAdd(&E.repPerClass[level][key.n - 2], 1u);
     const DevTable t = d.ctl->tables[level];
     bool ins = false;
-    const uint32_t h = table_find_or_insert<1, SHARED>(g, d, t, key, spare, ins);
+    const uint32_t h = table_find_or_insert<1, MODE>(g, d, t, key, spare, ins);
     release_spare<1>(g, d, t, spare);
     added += ins ? 1u : 0u;
     return h;
@@ -953,7 +953,7 @@ __device__ uint32_t merge_single(const DevDag& d, uint32_t level, uint32_t* w, c
 // level by level the SVO item the edit's own pass would have built there (the old node's children
 // kept, the path child subdivided) goes through merge_single with the counters of that edit. Returns
 // the new handle at level `stop` (kNone when it emptied); with stop 0, the new root.
-template <bool SHARED>
+template <int MODE>
 __device__ uint32_t rebuild_spine(const DevDag& d, uint32_t L0, const uint32_t* path, uint32_t root, uint32_t sub, uint32_t stop,
     unsigned long long& added)
 {
@@ -984,7 +984,7 @@ __device__ uint32_t rebuild_spine(const DevDag& d, uint32_t L0, const uint32_t* 
                 w[1 + j++] = b == ci ? 0u : old[1 + __popc(oldMask & ((1u << b) - 1u))];
         w[0] = mask | (1u << (13 + ci));
         const uint32_t regRep[1] = { childRep }, regHandle[1] = { childHandle };
-        const uint32_t hn = merge_single<SHARED>(d, l, w, regRep, regHandle, g, spare, added);
+        const uint32_t hn = merge_single<MODE>(d, l, w, regRep, regHandle, g, spare, added);
         childRep = hn == kNone ? kEmptyRep : 0u;
         childHandle = hn;
     }
@@ -1050,7 +1050,7 @@ __device__ void ph_merge_level(const DevDag& d, uint32_t level, char* scratch)
         if (E.builder) // the scene builder sizes the level tables from these
             atomicAdd(&E.repPerClass[level][key.n - 2], 1u);
         bool ins = false;
-        handle[i] = table_find_or_insert<1, SHARED>(g, d, t, key, spare, ins);
+        handle[i] = table_find_or_insert<1, SHARED ? kInsertShared : kInsertLaunch>(g, d, t, key, spare, ins);
         added += ins ? 1u : 0u;
     }
     release_spare<1>(g, d, t, spare);
@@ -1331,7 +1331,7 @@ __global__ void k_edit_spines_private(DevDag d, const DevEditor* eds, uint32_t n
     DevDag dk = d;
     dk.edit = &E;
     unsigned long long added = 0;
-    *e.tileOut = rebuild_spine<true>(dk, e.startLevel, e.startPath, d.ctl->root, sub, e.spineSplit, added);
+    *e.tileOut = rebuild_spine<kInsertShared>(dk, e.startLevel, e.startPath, d.ctl->root, sub, e.spineSplit, added);
     E.added += added;
 }
 
@@ -1371,7 +1371,8 @@ __global__ void k_edit_spines(DevDag d, const DevEditor* eds, uint32_t numEdits,
             for (int a = 0; a < 3; ++a)
                 path[a] = e.startPath[a] >> (e.startLevel - L);
             const uint32_t errBefore = c->edit.err;
-            const uint32_t after = rebuild_spine<false>(dk, L, path, root, sub, 0, added);
+            const uint32_t after = rebuild_spine<kInsertSole>(dk, L, path, root, sub, 0, added);
+            __threadfence(); // the items of the rebuilt path are visible before the root that reaches them
             if (c->edit.err == errBefore)
                 c->root = after;
             else
