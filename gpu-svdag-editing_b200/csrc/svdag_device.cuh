@@ -764,28 +764,24 @@ constexpr uint32_t kLockTries = 1u << 20; // bound on waiting for a bucket lock 
 // Find-or-insert for keys that no other group of the same launch looks up (the DAG merge inserts
 // each distinct item once). A slot is claimed with the in-flight tag, the item written, then the
 // final tag published, so concurrent probes of other keys never compare a half-written item.
-template <int G, bool FENCE = true>
+template <int G>
 __device__ __forceinline__ uint32_t table_find_or_insert_one(const Grp<G>& g, const DevDag& d, const DevTable& t, const Key<G>& key,
     Spare& spare, bool& inserted);
 
 // Insert modes of table_find_or_insert: the default (keys that no other group of the launch looks
-// up), shared (several blocks may insert the same key at once: under the bucket lock) and sole (the
-// only thread probing the tables; no release fence before a slot's tag, the caller fences once
-// before it publishes a handle that reaches the new items).
-enum : int { kInsertLaunch = 0, kInsertShared = 1, kInsertSole = 2 };
+// up) and shared (several threads may insert the same key at once: under the bucket lock).
+enum : int { kInsertLaunch = 0, kInsertShared = 1 };
 
-// Find-or-insert. In the shared mode (one thread per key, G = 1), several blocks may look up and insert the
-// same key at once (the blocks of a group of subtree edits): the lookup and insert then run under
-// the bucket's lock (a striped lock word in d.locks), so the second of two equal keys finds the
-// first's published item. A holder only probes and inserts into its own chain, so no lock waits on
+// Find-or-insert. In the shared mode (one thread per key, G = 1), several threads may look up and
+// insert the same key at once (the blocks and the path threads of a group of subtree edits): the
+// lookup and insert then run under the bucket's lock (a striped lock word in d.locks), so the
+// second of two equal keys finds the first's published item. A holder only probes and inserts into its own chain, so no lock waits on
 // another; the wait for a lock is bounded and ends with SVDAG_ERR_TIMEOUT.
 template <int G, int MODE = kInsertLaunch>
 __device__ __forceinline__ uint32_t table_find_or_insert(const Grp<G>& g, const DevDag& d, const DevTable& t, const Key<G>& key,
     Spare& spare, bool& inserted)
 {
-    if constexpr (MODE == kInsertSole && G == 1) {
-        return table_find_or_insert_one<G, false>(g, d, t, key, spare, inserted);
-    } else if constexpr (MODE == kInsertShared && G == 1) {
+    if constexpr (MODE == kInsertShared && G == 1) {
         inserted = false;
         const uint32_t cls = key.n - 2u;
         if (key.n < 2u || key.n > 10u || t.numBuckets[cls] == 0 || !d.locks) {
@@ -811,7 +807,7 @@ __device__ __forceinline__ uint32_t table_find_or_insert(const Grp<G>& g, const 
     }
 }
 
-template <int G, bool FENCE>
+template <int G>
 __device__ __forceinline__ uint32_t table_find_or_insert_one(const Grp<G>& g, const DevDag& d, const DevTable& t, const Key<G>& key,
     Spare& spare, bool& inserted)
 {
@@ -868,12 +864,10 @@ __device__ __forceinline__ uint32_t table_find_or_insert_one(const Grp<G>& g, co
         snapValid = true;
         if (item != kNone) {
             write_item<G>(g, handle_ptr(d, item), key);
-            if constexpr (FENCE) { // (the sole writer fences once, before it publishes what it built)
-                if constexpr (G == 1)
-                    fence_release(); // the writer publishes: a release orders its item before the tag
-                else
-                    __threadfence();
-            }
+            if constexpr (G == 1)
+                fence_release(); // the writer publishes: a release orders its item before the tag
+            else
+                __threadfence();
             g.sync();
             if (g.lane == 0)
                 atomicXor(slab_ptr(d, slab) + (s >> 2), (kTagBusy ^ tag) << (8u * (s & 3u)));

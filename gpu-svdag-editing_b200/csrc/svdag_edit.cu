@@ -948,49 +948,6 @@ __device__ uint32_t merge_single(const DevDag& d, uint32_t level, uint32_t* w, c
     return h;
 }
 
-// Levels L0-1 .. stop of the path from the root down to the node (L0, path), rebuilt bottom-up over
-// the DAG under `root` with the node's new handle `sub` (kNone: emptied) in place of the old child:
-// level by level the SVO item the edit's own pass would have built there (the old node's children
-// kept, the path child subdivided) goes through merge_single with the counters of that edit. Returns
-// the new handle at level `stop` (kNone when it emptied); with stop 0, the new root.
-template <int MODE>
-__device__ uint32_t rebuild_spine(const DevDag& d, uint32_t L0, const uint32_t* path, uint32_t root, uint32_t sub, uint32_t stop,
-    unsigned long long& added)
-{
-    uint32_t nodes[kMaxLevels];
-    uint32_t h = root;
-    for (uint32_t l = 0; l < L0; ++l) {
-        nodes[l] = h;
-        if (h != kNone) {
-            const uint32_t* node = item_ptr(d, h);
-            const uint32_t c = spine_child(path, L0, l);
-            const uint32_t mask = node[0] & 0xFFu;
-            h = (mask >> c) & 1u ? node[1 + __popc(mask & ((1u << c) - 1u))] : kNone;
-        }
-    }
-    Grp<1> g;
-    Spare spare;
-    uint32_t childRep = sub == kNone ? kEmptyRep : 0u, childHandle = sub;
-    for (int li = (int)L0 - 1; li >= (int)stop; --li) {
-        const uint32_t l = (uint32_t)li;
-        const uint32_t ci = spine_child(path, L0, l);
-        uint32_t w[kItemStride] = {};
-        const uint32_t* old = nodes[l] != kNone ? item_ptr(d, nodes[l]) : nullptr;
-        const uint32_t oldMask = old ? old[0] & 0xFFu : 0u;
-        const uint32_t mask = oldMask | (1u << ci);
-        uint32_t j = 0;
-        for (uint32_t b = 0; b < 8; ++b)
-            if ((mask >> b) & 1u)
-                w[1 + j++] = b == ci ? 0u : old[1 + __popc(oldMask & ((1u << b) - 1u))];
-        w[0] = mask | (1u << (13 + ci));
-        const uint32_t regRep[1] = { childRep }, regHandle[1] = { childHandle };
-        const uint32_t hn = merge_single<MODE>(d, l, w, regRep, regHandle, g, spare, added);
-        childRep = hn == kNone ? kEmptyRep : 0u;
-        childHandle = hn;
-    }
-    return childHandle;
-}
-
 // One bottom-up level in a single pass (used by edits): child fix-up and gated discovery, intra-level
 // dedup, and find-or-insert of the representative in the level table. Duplicates only record their
 // representative; the parent level reads the representative's handle after the next barrier. With
@@ -1277,7 +1234,7 @@ __global__ void __launch_bounds__(kBlockThreads, 1) k_edit_block(DevDag d, DevEd
 // merges edit k's subtree against the DAG as the group found it, with counters and a slice of the
 // scratch arena of its own. Their footprints do not meet, so each block reads exactly the nodes the
 // edit's own pass would read after its predecessors; only the path from the root to each subtree
-// depends on the order, and k_edit_spines rebuilds it in submission order afterwards.
+// depends on the order, and k_edit_spines rebuilds it afterwards.
 __global__ void __launch_bounds__(kBlockThreads, 1) k_edit_subtrees(DevDag d, const DevEditor* eds, uint32_t numEdits, char* parts,
     unsigned long long partBytes, EditCounters* counters)
 {
@@ -1313,43 +1270,127 @@ __global__ void __launch_bounds__(kBlockThreads, 1) k_edit_subtrees(DevDag d, co
     }
 }
 
-// The private part of each subtree edit's path (levels spineSplit .. startLevel-1, which no other
-// path of the group passes through, so no earlier edit of the group changes them), rebuilt for all
-// the group's edits at once: thread k over the DAG as the group found it, with edit k's counters.
-// Two edits can make equal path items, so the find-or-inserts take the bucket locks. The handle at
-// level spineSplit replaces the subtree's in `results` (kKeep stays).
-__global__ void k_edit_spines_private(DevDag d, const DevEditor* eds, uint32_t numEdits, EditCounters* counters)
-{
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= numEdits)
-        return;
-    const DevEditor& e = eds[k];
-    EditCounters& E = counters[k];
-    const uint32_t sub = *e.tileOut;
-    if (E.overflow || sub == kKeep || d.ctl->edit.err != 0 || e.spineSplit >= e.startLevel)
-        return;
-    DevDag dk = d;
-    dk.edit = &E;
-    unsigned long long added = 0;
-    *e.tileOut = rebuild_spine<kInsertShared>(dk, e.startLevel, e.startPath, d.ctl->root, sub, e.spineSplit, added);
-    E.added += added;
-}
+// Commits a group of subtree edits: each edit's path from its node up to the root (levels
+// startLevel-1 .. 0), then in submission order the undo frames, roots and records.
+// One thread per edit, `spread` threads apart so that few edits share a warp (their finds and
+// inserts take different branches, which a warp would run one after another); the path levels are
+// built bottom-up, one level for all edits at a time. Edit k's version of the node N on its path at level l holds, in each child slot, the
+// version of the latest edit j <= k of the group whose path passes through that child, and the
+// group's DAG's child where none does. Each edit changes only the nodes on its own path (the
+// subtrees are disjoint), so that is the node the edits 0..k applied one after another leave at N:
+// the SVO item edit k's own pass would build there (the old node's children kept, the path child
+// subdivided) over the DAG of its predecessors. It goes through merge_single with edit k's
+// counters, as in that pass. Equal versions made by two edits at once take the bucket locks.
+// An edit that changed nothing or ran out of its scratch slice leaves the root as it is, as in its
+// own pass. An error raised while the group's subtrees were built fails every edit of the group;
+// an insert that fails here fails its edit and every later edit of the group (the later versions
+// include the failed one), and the root stays at the last edit before it.
+constexpr uint32_t kMaxGroup = 148; // edits of one group of subtree edits (one block)
 
-// Commits a group of subtree edits in submission order (one thread): per edit, the undo frame of
-// ph_edit_begin, the shared part of the path (levels spineSplit-1 .. 0) rebuilt over the current DAG
-// (rebuild_spine), the new root and the edit's record. An edit that changed nothing or ran out of
-// its scratch slice leaves the root as it is, as in its own pass; an error raised while the group's
-// subtrees or private path parts were built fails every edit of the group.
-__global__ void k_edit_spines(DevDag d, const DevEditor* eds, uint32_t numEdits, EditCounters* counters)
+__global__ void __launch_bounds__(1024) k_edit_spines(DevDag d, const DevEditor* eds, uint32_t numEdits, uint32_t spread,
+    EditCounters* counters)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0)
-        return;
+    __shared__ uint32_t px[kMaxGroup], py[kMaxGroup], pz[kMaxGroup], top[kMaxGroup];
+    __shared__ uint32_t ver[kMaxLevels][kMaxGroup];
+    __shared__ uint32_t maxTop, failAt;
     Control* c = d.ctl;
+    const uint32_t k = threadIdx.x % spread == 0 ? threadIdx.x / spread : numEdits; // numEdits: no edit
+    const uint32_t root0 = c->root;
     const uint32_t groupErr = c->edit.err;
-    for (uint32_t k = 0; k < numEdits; ++k) {
+    if (k == 0) {
+        maxTop = 0;
+        failAt = numEdits;
+    }
+    __syncthreads();
+    bool live = false;
+    uint32_t nodes[kMaxLevels]; // the group's DAG along this edit's path, levels 0 .. top-1
+    if (k < numEdits) {
         const DevEditor& e = eds[k];
-        EditCounters& E = counters[k];
-        const uint32_t root = c->root;
+        const uint32_t sub = *e.tileOut; // the subtree's new handle
+        live = groupErr == 0 && !counters[k].overflow && sub != kKeep;
+        const uint32_t L = e.startLevel;
+        px[k] = e.startPath[0];
+        py[k] = e.startPath[1];
+        pz[k] = e.startPath[2];
+        top[k] = live ? L : 0u; // an edit that commits nothing has no versions
+        if (live) {
+            ver[L][k] = sub;
+            atomicMax(&maxTop, L);
+            const uint32_t path[3] = { px[k], py[k], pz[k] };
+            uint32_t h = root0;
+            for (uint32_t l = 0; l < L; ++l) {
+                nodes[l] = h;
+                if (h != kNone) {
+                    const uint32_t* node = item_ptr(d, h);
+                    const uint32_t ch = spine_child(path, L, l);
+                    const uint32_t mask = node[0] & 0xFFu;
+                    h = (mask >> ch) & 1u ? node[1 + __popc(mask & ((1u << ch) - 1u))] : kNone;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    DevDag dk = d;
+    dk.solo = 1;
+    Grp<1> g;
+    Spare spare;
+    unsigned long long added = 0;
+    for (int li = (int)maxTop - 1; li >= 0; --li) {
+        const uint32_t l = (uint32_t)li;
+        if (live && top[k] > l) {
+            dk.edit = counters + k;
+            const uint32_t sh = top[k] - l; // node coordinates at level l are the path's >> sh
+            const uint32_t nx = px[k] >> sh, ny = py[k] >> sh, nz = pz[k] >> sh;
+            const uint32_t ck = (((px[k] >> (sh - 1u)) & 1u) << 2) | (((py[k] >> (sh - 1u)) & 1u) << 1) | ((pz[k] >> (sh - 1u)) & 1u);
+            // the group's DAG's children of N, then the latest earlier edit's version per child slot
+            uint32_t kid[8];
+            const uint32_t* old = nodes[l] != kNone ? item_ptr(d, nodes[l]) : nullptr;
+            const uint32_t oldMask = old ? old[0] & 0xFFu : 0u;
+#pragma unroll
+            for (uint32_t b = 0; b < 8; ++b)
+                kid[b] = (oldMask >> b) & 1u ? old[1 + __popc(oldMask & ((1u << b) - 1u))] : kNone;
+            for (uint32_t j = 0; j < k; ++j) {
+                const uint32_t tj = top[j];
+                if (tj <= l)
+                    continue;
+                const uint32_t sj = tj - l;
+                if ((px[j] >> sj) != nx || (py[j] >> sj) != ny || (pz[j] >> sj) != nz)
+                    continue;
+                const uint32_t cj = (((px[j] >> (sj - 1u)) & 1u) << 2) | (((py[j] >> (sj - 1u)) & 1u) << 1) | ((pz[j] >> (sj - 1u)) & 1u);
+                const uint32_t v = ver[l + 1][j];
+#pragma unroll
+                for (uint32_t b = 0; b < 8; ++b)
+                    kid[b] = cj == b ? v : kid[b];
+            }
+            // the SVO item of the edit's own pass: the other children kept, the path child to be fixed up
+            uint32_t w[kItemStride] = {};
+            uint32_t mask = 1u << ck, j = 0;
+#pragma unroll
+            for (uint32_t b = 0; b < 8; ++b)
+                mask |= kid[b] != kNone ? 1u << b : 0u;
+#pragma unroll
+            for (uint32_t b = 0; b < 8; ++b)
+                if ((mask >> b) & 1u)
+                    w[1 + j++] = b == ck ? 0u : kid[b];
+            w[0] = mask | (1u << (13 + ck));
+            const uint32_t childHandle = ver[l + 1][k];
+            const uint32_t regRep[1] = { childHandle == kNone ? kEmptyRep : 0u }, regHandle[1] = { childHandle };
+            const uint32_t hn = merge_single<kInsertShared>(dk, l, w, regRep, regHandle, g, spare, added);
+            if (hn == kNone && (w[0] & 0xFFu) != 0) // not emptied: the insert failed
+                atomicMin(&failAt, k);
+            ver[l][k] = hn;
+        }
+        __syncthreads();
+    }
+    if (live)
+        counters[k].added += added;
+    __syncthreads();
+    if (k != 0)
+        return;
+    uint32_t root = root0;
+    for (uint32_t q = 0; q < numEdits; ++q) {
+        const DevEditor& e = eds[q];
+        EditCounters& E = counters[q];
         { // MyGPUHashDAGUndoRedo::add_frame (my_gpu_base_dag.h:23-34), as ph_edit_begin
             const bool same = c->undoCount > 0 && c->undo[(c->undoHead + 63u) & 63u] == root;
             if (!same) {
@@ -1359,34 +1400,23 @@ __global__ void k_edit_spines(DevDag d, const DevEditor* eds, uint32_t numEdits,
                 c->undoCount = c->undoCount < c->undoDepth ? c->undoCount + 1u : c->undoDepth;
             }
         }
-        const uint32_t sub = *e.tileOut; // the handle at level spineSplit (the subtree's when no private part)
-        unsigned long long added = 0;
+        const uint32_t before = root;
         uint32_t status = E.overflow ? (uint32_t)SVDAG_ERR_OOM : groupErr;
-        if (status == 0 && sub != kKeep) {
-            DevDag dk = d;
-            dk.edit = &E;
-            dk.solo = 1;
-            const uint32_t L = e.spineSplit < e.startLevel ? e.spineSplit : e.startLevel;
-            uint32_t path[3];
-            for (int a = 0; a < 3; ++a)
-                path[a] = e.startPath[a] >> (e.startLevel - L);
-            const uint32_t errBefore = c->edit.err;
-            const uint32_t after = rebuild_spine<kInsertSole>(dk, L, path, root, sub, 0, added);
-            __threadfence(); // the items of the rebuilt path are visible before the root that reaches them
-            if (c->edit.err == errBefore)
-                c->root = after;
+        if (status == 0 && *e.tileOut != kKeep) {
+            if (q >= failAt)
+                status = c->edit.err != 0 ? c->edit.err : (uint32_t)SVDAG_ERR_OOM;
             else
-                status = c->edit.err;
+                root = ver[0][q];
         }
         if (E.overflow)
             set_status(c, SVDAG_ERR_OOM);
         if (e.record) {
             EditRecord* r = e.record;
-            r->rootBefore = root;
-            r->rootAfter = c->root;
+            r->rootBefore = before;
+            r->rootAfter = root;
             r->status = status;
             r->edited = E.edited;
-            r->added = E.added + added;
+            r->added = E.added;
             unsigned long long svo = e.startLevel, reps = 0;
             for (uint32_t l = 0; l < kMaxLevels; ++l) {
                 svo += E.count[l];
@@ -1396,6 +1426,8 @@ __global__ void k_edit_spines(DevDag d, const DevEditor* eds, uint32_t numEdits,
             r->unique = reps;
         }
     }
+    __threadfence(); // the items of the rebuilt paths are visible before the root that reaches them
+    c->root = root;
 }
 
 __global__ void k_undo_redo(Control* c, uint32_t redo)
@@ -1671,8 +1703,9 @@ constexpr unsigned long long kSubtreeScratch = 16ull << 20; // scratch slice of 
 
 // Launches expanded editors with their editors and records in `region`. Large edits run as one launch
 // per phase at full occupancy. Runs of small edits are cut into groups of subtree edits whose nodes
-// are pairwise disjoint (one block per edit builds its subtree, then one thread commits the group in
-// order: k_edit_subtrees, k_edit_spines) and the edits between them, which run one after another in
+// are pairwise disjoint (one block per edit builds its subtree, then the paths from the root to the
+// subtrees are rebuilt and committed in order: k_edit_subtrees, k_edit_spines)
+// and the edits between them, which run one after another in
 // one persistent launch (block barriers are cheaper than launches for small SVOs).
 svdag_status launch_edits_at(svdag_ctx* ctx, const DevEditor* eds, uint32_t n, char* region, size_t regionBytes, cudaStream_t s)
 {
@@ -1692,7 +1725,7 @@ svdag_status launch_edits_at(svdag_ctx* ctx, const DevEditor* eds, uint32_t n, c
     std::vector<DevEditor> withRecords(eds, eds + n);
     for (uint32_t k = 0; k < n; ++k)
         withRecords[k].record = records + k;
-    const unsigned long long maxGroup = std::min<unsigned long long>(148, ctx->scratchBytes / kSubtreeScratch);
+    const unsigned long long maxGroup = std::min<unsigned long long>(kMaxGroup, ctx->scratchBytes / kSubtreeScratch);
     auto extend = [&](uint32_t k, Kind kind) {
         if (!segs.empty() && segs.back().kind == kind && kind != GROUP && segs.back().end == k)
             segs.back().end = k + 1;
@@ -1704,7 +1737,7 @@ svdag_status launch_edits_at(svdag_ctx* ctx, const DevEditor* eds, uint32_t n, c
             extend(k++, LARGE);
             continue;
         }
-        uint32_t e = k, lv[148], pt[148][3];
+        uint32_t e = k, lv[kMaxGroup], pt[kMaxGroup][3];
         while (e < n && e - k < maxGroup && small(e)) {
             const uint32_t m = e - k;
             if (!subtree_node(ctx, eds[e], lv[m], pt[m]))
@@ -1729,13 +1762,6 @@ svdag_status launch_edits_at(svdag_ctx* ctx, const DevEditor* eds, uint32_t n, c
             for (int a = 0; a < 3; ++a)
                 ed.startPath[a] = pt[q][a];
             ed.tileOut = results + q;
-            // the deepest level at which another edit's path meets this one's; the levels below it
-            // down to the node are this edit's alone
-            uint32_t meet = 0;
-            for (uint32_t o = 0; o < m; ++o)
-                if (o != q)
-                    meet = std::max(meet, subtree::meet_level(lv[q], pt[q], lv[o], pt[o]));
-            ed.spineSplit = meet + 1;
         }
         segs.push_back(Seg { k, e, GROUP });
         k = e;
@@ -1766,8 +1792,8 @@ svdag_status launch_edits_at(svdag_ctx* ctx, const DevEditor* eds, uint32_t n, c
             SVDAG_CUDA(cudaMemsetAsync(dg.locks, 0, (size_t)kLockStripes * 4, s));
             SVDAG_CUDA(cudaMemsetAsync(&ctx->ctl->edit.err, 0, sizeof(uint32_t), s));
             k_edit_subtrees<<<m, kBlockThreads, 0, s>>>(dg, devEds + g.begin, m, ctx->scratch + head, partBytes, counters);
-            k_edit_spines_private<<<(m + 31) / 32, 32, 0, s>>>(dg, devEds + g.begin, m, counters);
-            k_edit_spines<<<1, 32, 0, s>>>(d, devEds + g.begin, m, counters);
+            const uint32_t spread = std::min(32u, 1024u / m);
+            k_edit_spines<<<1, (m * spread + 31) / 32 * 32, 0, s>>>(dg, devEds + g.begin, m, spread, counters);
             SVDAG_CUDA(cudaGetLastError());
         }
     }

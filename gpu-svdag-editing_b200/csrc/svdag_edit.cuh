@@ -39,12 +39,9 @@ struct DevEditor {
     // Subtree edit: the edit covers the subtree of the node (startLevel, startPath) of the DAG as the
     // batch found it (that node's region holds the edit's whole footprint and no other edit of its
     // group touches it); no undo frame; the subtree's new handle goes to *tileOut (kNone when it
-    // empties, kKeep while the edit has changed nothing), and the path above is rebuilt afterwards in
-    // submission order.
+    // empties, kKeep while the edit has changed nothing), and the path above is rebuilt afterwards
+    // with the edits before it in the group applied.
     uint32_t subtree;
-    // Subtree edit: path levels spineSplit .. startLevel-1 lie on no other path of the group (rebuilt
-    // for all the group's edits at once); levels 0 .. spineSplit-1 are shared and rebuilt in order.
-    uint32_t spineSplit;
 };
 constexpr uint32_t kKeep = 0xFFFFFFFDu; // subtree edit: nothing committed
 

@@ -52,20 +52,5 @@ inline bool disjoint(uint32_t la, const uint32_t* pa, uint32_t lb, const uint32_
     return (pb[0] >> sh) != pa[0] || (pb[1] >> sh) != pa[1] || (pb[2] >> sh) != pa[2];
 }
 
-// Deepest level of a node that lies on both the path from the root to node (la, pa) and the path to
-// node (lb, pb): 0 when they part below the root. For disjoint nodes it is above both.
-inline uint32_t meet_level(uint32_t la, const uint32_t* pa, uint32_t lb, const uint32_t* pb)
-{
-    const uint32_t top = std::min(la, lb);
-    uint32_t meet = 0;
-    for (uint32_t l = 1; l <= top; ++l) {
-        const uint32_t sa = la - l, sb = lb - l;
-        if ((pa[0] >> sa) != (pb[0] >> sb) || (pa[1] >> sa) != (pb[1] >> sb) || (pa[2] >> sa) != (pb[2] >> sb))
-            break;
-        meet = l;
-    }
-    return meet;
-}
-
 } // namespace subtree
 } // namespace svdag

@@ -59,6 +59,7 @@ constexpr uint32_t kVersion = 3;
 constexpr uint32_t kMinItem = 2, kTables = 9; // item sizes 2..10
 constexpr uint32_t kMaterials = 16;
 constexpr uint32_t kTagWords = 8, kNextWord = 8, kItemsAt = 10, kSlots = 32;
+static_assert(kTagWords * 4 == kSlots && kNextWord == kTagWords, "one tag byte per slot, then the next pointer");
 constexpr uint32_t kEnd = 0xFFFFFFFFu; // next_sentinel; also the empty DAG's root
 constexpr uint32_t kBitmapWords = 512, kUnitsPerSuper = 16384;
 constexpr uint32_t kPtrBits = 29, kPtrMask = (1u << kPtrBits) - 1u;

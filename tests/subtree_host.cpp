@@ -11,8 +11,4 @@ int subtree_disjoint(uint32_t la, const uint32_t* pa, uint32_t lb, const uint32_
 {
     return svdag::subtree::disjoint(la, pa, lb, pb) ? 1 : 0;
 }
-uint32_t subtree_meet_level(uint32_t la, const uint32_t* pa, uint32_t lb, const uint32_t* pb)
-{
-    return svdag::subtree::meet_level(la, pa, lb, pb);
-}
 }

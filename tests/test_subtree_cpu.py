@@ -30,8 +30,6 @@ def geo(tmp_path_factory):
     lib = C.CDLL(so)
     lib.subtree_node_of.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32), C.c_void_p]
     lib.subtree_disjoint.argtypes = [C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p]
-    lib.subtree_meet_level.restype = C.c_uint32
-    lib.subtree_meet_level.argtypes = [C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p]
     return lib
 
 
@@ -131,23 +129,3 @@ def test_disjointness_is_ancestry(geo):
     assert not d(3, p, 4, child) and not d(4, child, 3, p)
     assert not d(3, p, 3, p)
     assert d(3, p, 4, other) and d(4, child, 4, other)
-
-
-def test_meet_level_is_the_deepest_common_ancestor(geo):
-    """Against a brute force over the nodes' ancestor chains, for random node pairs."""
-    rng = np.random.default_rng(10)
-    for _ in range(2000):
-        la, lb = (int(v) for v in rng.integers(1, 14, 2))
-        pa = rng.integers(0, 1 << la, 3).astype(np.uint32)
-        pb = rng.integers(0, 1 << lb, 3).astype(np.uint32)
-        if rng.random() < 0.5:  # make them share a deeper ancestor
-            m = int(rng.integers(0, min(la, lb) + 1))
-            pb = ((pa >> (la - m)) << (lb - m)) | (pb & ((1 << (lb - m)) - 1))
-            pb = pb.astype(np.uint32)
-        want = 0
-        for l in range(1, min(la, lb) + 1):
-            if np.array_equal(pa >> (la - l), pb >> (lb - l)):
-                want = l
-            else:
-                break
-        assert geo.subtree_meet_level(la, pa.ctypes.data, lb, pb.ctypes.data) == want
