@@ -6,7 +6,10 @@ The grouped form builds each edit's subtree against the DAG as the group found i
 edits' own passes because:
  - an edit changes no voxel outside its node's region;
  - edits whose nodes are disjoint commute: the DAG after them, in either order, is the same, item for
-   item (canonical digests per level).
+   item (canonical digests per level);
+ - after each edit of a group, every child of every node on its path is what the latest edit of the
+   group through that child left there, which is how the batch rebuilds all paths one level at a
+   time (k_edit_spines).
 """
 import ctypes as C
 import os
@@ -129,3 +132,50 @@ def test_disjointness_is_ancestry(geo):
     assert not d(3, p, 4, child) and not d(4, child, 3, p)
     assert not d(3, p, 3, p)
     assert d(3, p, 4, other) and d(4, child, 4, other)
+
+
+def test_path_versions_follow_the_latest_edit_per_child(geo, oracle_mod):
+    """The rule by which a group's paths are rebuilt one level for all edits at once: applied one
+    after another, after edit k every child of every node on k's path is that child as the latest
+    edit j <= k whose path passes through it left it, or as the group found it where none does.
+    Checked by handle (the oracle stores each distinct item once) on groups of consecutive edits in
+    one 64-voxel region whose nodes are pairwise disjoint, as the batch planner forms them."""
+    rng = np.random.default_rng(7)
+    g = 1 << LEVELS
+    shared = groups = 0
+    while groups < 6:
+        base = rng.integers(0, g - 64, 3)
+        group = []
+        for _ in range(200):
+            if len(group) == 10:
+                break
+            tool, mat = int(rng.choice([0, 1, 2, 3, 4])), int(rng.integers(0, 16))
+            c = tuple(float(v) for v in base + rng.uniform(0, 64, 3))
+            r = float(rng.integers(0, 7))
+            s = node_of(geo, tool, c, r)
+            if s is None or not all(geo.subtree_disjoint(s[0], s[1].ctypes.data, q[0], q[1].ctypes.data)
+                                    for _, q in group):
+                continue
+            group.append(((tool, mat, c, r), s))
+        if len(group) < 4:
+            continue
+        o = scene(oracle_mod)
+        kids = [np.array([(b >> 2) & 1, (b >> 1) & 1, b & 1], np.uint32) for b in range(8)]
+        watch = {(l + 1, tuple(int(v) for v in (p >> (lv - l)) * 2 + kid))
+                 for _, (lv, p) in group for l in range(lv) for kid in kids}
+        snap = lambda: {key: o.node_at(key[0], np.array(key[1], np.uint32)) for key in watch}
+        states = [snap()]
+        for (tool, mat, c, r), _ in group:
+            assert o.edit(edit(oracle_mod, tool, mat, c, r)).status == 0
+            states.append(snap())
+        for k, (_, (lk, pk)) in enumerate(group):
+            for l in range(lk):
+                for kid in kids:
+                    child = tuple(int(v) for v in (pk >> (lk - l)) * 2 + kid)
+                    through = [j for j, (_, (lj, pj)) in enumerate(group[:k + 1])
+                               if lj > l and tuple(int(v) for v in pj >> (lj - l - 1)) == child]
+                    want = states[through[-1] + 1] if through else states[0]
+                    assert states[k + 1][(l + 1, child)] == want[(l + 1, child)], (k, l, child)
+                    shared += bool(through) and through[-1] != k
+        groups += 1
+    assert shared > 50  # children last changed by an earlier edit of the group, not by edit k
