@@ -1,7 +1,8 @@
 """Groups of subtree edits in the batched form. Small edits whose footprints lie in pairwise disjoint
-subtrees are built side by side, one block each (k_edit_subtrees). One thread then commits them in
-submission order, rebuilding the path from the root to each subtree over the current DAG
-(k_edit_spines).
+subtrees are built side by side, one block each (k_edit_subtrees). Then every edit's path from its
+subtree to the root is rebuilt, one level for all edits at a time, each edit's version of a node
+taking the latest earlier edit's child where that edit's path passes, and the roots, records and
+undo frames are committed in submission order (k_edit_spines).
 
 Against the same edits applied one at a time:
  - the DAG after the batch equals the oracle's;
